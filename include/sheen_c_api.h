@@ -1,0 +1,215 @@
+/*
+ * sheen_c_api.h -- C-ABI of the B200 renderer core (libsheen_c_api.so).
+ *
+ * The first four entry points and the SheenScene struct are the drop-in
+ * boundary: same names, argument meaning, return codes and struct layout as
+ * the reference's sheen_c_api.h (sheen_c_api.h:18-107), so the Blender
+ * add-on's ctypes path (addon_sheen/sheen_render/engine.py:88-147) and the
+ * native module (api/sheen_py_module.cpp:57-87) load this library unchanged.
+ *
+ * Everything after them is new and stands beside the drop-in: an RGBA (float)
+ * output path for parity checks, device-resident scene handles with a choice
+ * of renderer form, the .sheen loader and synthetic scene generators behind a
+ * C view, and a continuous-batching request loop.
+ *
+ * Conventions for the new entry points: return 0 on success and -1 on error
+ * (message via sheen_get_last_error(), which is per thread for them); no
+ * torch or CUDA types in the signatures; pointers documented as host or
+ * device.
+ */
+#ifndef SHEEN_C_API_H
+#define SHEEN_C_API_H
+
+#include <stddef.h>
+#include "sheen_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* sheen_c_api.h:18-87 -- flat scene description, 352 bytes.  Pointers are
+ * host pointers owned by the caller for the duration of a call; NULL when the
+ * matching count is 0. */
+typedef struct SheenScene {
+    CameraData camera;
+
+    const Object* objects;
+    int num_objects;
+
+    const SweepPoint* sweep_points;
+    int num_sweep_points;
+    const SweepStrand* sweep_strands;
+    int num_sweep_strands;
+
+    const Triangle* triangles;
+    int num_triangles;
+
+    const HeightField* heightfields;
+    int num_heightfields;
+
+    const Superellipsoid* superellipsoids;
+    int num_superellipsoids;
+
+    const LathePoint* lathe_points;
+    int num_lathe_points;
+    const Lathe* lathes;
+    int num_lathes;
+
+    const PrismPoint* prism_points;
+    int num_prism_points;
+    const Prism* prisms;
+    int num_prisms;
+
+    const CSGNode* csg_nodes;
+    int csg_root;               /* -1: no CSG tree */
+    int num_csg_nodes;
+
+    const Plane* planes;
+    int num_planes;
+
+    const Material* materials;
+    int num_materials;
+
+    const unsigned char* const* texture_pixels;   /* [num_textures], RGB8 */
+    const int* texture_widths;
+    const int* texture_heights;
+    int num_textures;
+
+    const Light* lights;
+    int num_lights;
+
+    int photons;                /* photons emitted per light; 0 disables the caustic pass */
+    float photon_cell;          /* hash-grid cell size (<= 0: 0.25) */
+    float caustics;             /* caustic gain; 0 disables the gather */
+
+    const Medium* media;
+    int num_media;
+} SheenScene;
+
+/* ------------------------------------------------------------------ */
+/* Drop-in entry points                                                */
+/* ------------------------------------------------------------------ */
+
+/* Replaces sheen_init (sheen_c_api.h:91-93, api/sheen_c_api.cu:160-180).
+ * Selects the CUDA device.  cuda_arch is accepted and ignored: the library is
+ * built for sm_100a only.  Unlike the reference no 16 KB per-thread stack
+ * reservation is needed (no kernel here recurses).  0 / -1. */
+int sheen_init(int device_id, int cuda_arch);
+
+/* Replaces sheen_cleanup (sheen_c_api.h:95-96, api/sheen_c_api.cu:182-185).
+ * Frees every resident scene, server and pooled buffer, then resets this
+ * process's context on the device. */
+void sheen_cleanup(void);
+
+/* Replaces sheen_render_scene (sheen_c_api.h:98-105, api/sheen_c_api.cu:187-361).
+ * Renders with the plain FP32 form and writes an 8-bit sRGB PNG.  Parameter
+ * checks and messages follow the reference: w, h > 0, 1 <= aa <= 64,
+ * output_path != NULL, num_materials > 0.  0 / -1. */
+int sheen_render_scene(const SheenScene* scene, int width, int height,
+                       int aa_samples, const char* output_path);
+
+/* Replaces sheen_get_last_error (sheen_c_api.h:107, api/sheen_c_api.cu:363-365). */
+const char* sheen_get_last_error(void);
+
+/* ------------------------------------------------------------------ */
+/* Additions                                                           */
+/* ------------------------------------------------------------------ */
+
+/* Renderer forms. */
+enum {
+    SHEEN_FORM_PLAIN = 0,      /* one thread per pixel megakernel, FP32 32-byte nodes, median BVH */
+    SHEEN_FORM_WAVEFRONT = 1   /* persistent wavefront integrator, SAH BVH4 with 8-bit child boxes */
+};
+
+/* Render flags. */
+enum {
+    SHEEN_RENDER_COUNT_RAYS = 1   /* fill SheenRenderStats ray and node counters */
+};
+
+typedef struct SheenRenderStats {
+    unsigned long long primary_rays;     /* W*H*spp */
+    unsigned long long shadow_rays;      /* each glass pass counts */
+    unsigned long long secondary_rays;   /* reflection + refraction + photon-gather-free bounces */
+    unsigned long long total_rays;
+    unsigned long long node_visits;      /* box tests issued (counting builds only) */
+    unsigned long long prim_tests;       /* primitive tests issued (counting builds only) */
+    double build_ms;                     /* host BVH build */
+    double upload_ms;                    /* host -> device copies */
+    double photon_ms;                    /* photon emission + map build */
+    double render_ms;                    /* device time of the render launches */
+    unsigned long long device_bytes;     /* resident scene footprint */
+} SheenRenderStats;
+
+/* Render into a caller-owned HOST buffer of width*height float4 (RGBA, linear,
+ * alpha = 1), the same values the reference kernel writes into its float4
+ * output before the sRGB conversion.  Uploads, renders and frees like
+ * sheen_render_scene.  stats may be NULL. */
+int sheen_render_scene_rgba(const SheenScene* scene, int width, int height,
+                            int aa_samples, int form, float* out_rgba_host,
+                            SheenRenderStats* stats);
+
+/* Device-resident scenes.  create copies and packs every array to the device
+ * (BVH build included) and keeps it until destroy. */
+typedef struct SheenDeviceScene_* SheenDeviceScene;
+int  sheen_scene_create(const SheenScene* scene, int form, SheenDeviceScene* out);
+void sheen_scene_destroy(SheenDeviceScene scene);
+unsigned long long sheen_scene_device_bytes(SheenDeviceScene scene);
+int  sheen_scene_form(SheenDeviceScene scene);
+
+/* Render a resident scene into a DEVICE buffer (width*height float4) on the
+ * given CUDA stream (cudaStream_t passed as void*, NULL = legacy default
+ * stream).  Asynchronous unless flags has SHEEN_RENDER_COUNT_RAYS or stats
+ * is non-NULL, in which case it synchronises the stream before returning. */
+int sheen_scene_render_device(SheenDeviceScene scene, int width, int height,
+                              int aa_samples, float* out_rgba_device,
+                              void* stream, int flags, SheenRenderStats* stats);
+
+/* Same, into a HOST buffer; includes the device -> host copy. */
+int sheen_scene_render_host(SheenDeviceScene scene, int width, int height,
+                            int aa_samples, float* out_rgba_host, int flags,
+                            SheenRenderStats* stats);
+
+/* Owned host scenes: the .sheen loader and the synthetic generators return
+ * one.  sheen_owned_view points into storage owned by the handle. */
+typedef struct SheenOwnedScene_* SheenOwnedScene;
+
+typedef struct SheenSceneSettings {
+    int width;
+    int height;
+    int aa;
+    int photons;
+    float photon_cell;
+    float caustics;
+    char output[512];
+} SheenSceneSettings;
+
+/* Replaces load_scene_file (api/scene_io.h:20, api/scene_io.cpp:931-968):
+ * parses a .sheen text file with the reference's grammar.  On a parse error
+ * returns -1 with "line N: <text>" in the error message. */
+int  sheen_load_scene_file(const char* path, SheenOwnedScene* out);
+const SheenScene* sheen_owned_view(SheenOwnedScene scene);
+const SheenSceneSettings* sheen_owned_settings(SheenOwnedScene scene);
+void sheen_owned_free(SheenOwnedScene scene);
+
+/* Seeded synthetic scene generators for the benchmark workloads.
+ *   0: 64 spheres + ground plane + 1 point light, reflect 0.3
+ *   1: displaced level-`level` icosphere + 16 displaced 50k-triangle tori,
+ *      4 point lights, 4 glass tori (ior 1.5), reflect 0.2 elsewhere
+ *   2: analytic primitives + one CSG tree (superellipsoids, lathes, prisms,
+ *      sweeps, procedural heightfield)
+ *   3: glass sphere + glass lathe over a diffuse plane, one spot light,
+ *      caustics on (photons per light = `photons`)
+ * `detail` scales the geometry: for config 1 it is the icosphere subdivision
+ * level (8 = 1,310,720 triangles) and the torus grid is scaled with it; for
+ * the others it is ignored unless > 0 where noted. */
+int sheen_generate_scene(int config, unsigned int seed, int detail, int photons,
+                         SheenOwnedScene* out);
+
+/* 8-bit sRGB PNG writer used by sheen_render_scene (png_color.h:11-20 conversion). */
+int sheen_write_png_srgb(const char* path, const float* rgba, int width, int height);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHEEN_C_API_H */
