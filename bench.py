@@ -1,0 +1,330 @@
+"""Throughput benchmark of the ray-casting path (one JSON line on rank 0).
+
+Workload (default): the triangle-mesh scene -- a level-8 displaced
+icosphere (1,310,720 triangles) plus 16 displaced 50k-triangle tori, 4 point
+lights with shadow rays, mirror bounce (reflect 0.2) and refraction through
+the 4 glass tori (ior 1.5), 1920x1080 at 4 samples per pixel.  A step is
+one frame of that scene with the scene resident in HBM.
+
+metric: Mrays/s -- every scene query counts (primary, each glass pass of a
+shadow ray, each reflection/refraction segment); the per-frame ray count
+comes from the renderer's own device counters (a counting frame before the
+timed region; the path is deterministic, every frame issues the same rays).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--form wavefront|plain]
+                  [--impl ours|reference]
+
+--gpus N > 1 runs under torchrun: every rank renders its own replica of the
+frame on its own GPU (the path has no data exchange: "replicas only",
+weak scaling), timing is the max over ranks.
+
+--impl reference times the reference's own per-pixel code compiled for the
+host cores (oracle/_ref/libsheen_ref_host.so) on a bounded band of rows of
+the same frame, all host threads; its ray count is that band's count from
+this renderer's counters (same queries by construction).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+W, H, SPP = 1920, 1080, 4
+CPU_BAND = (480, 512)      # pixel rows of the CPU samples (two 16-row blocks)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": d["hbm_gbs"], "src": "measured", "sm_max_mhz": d.get("sm_max_mhz", 1965.0)}
+    return {"hbm_gbs": 6650.0, "src": "fallback", "sm_max_mhz": 1965.0}
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup(n):
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def make_scene(args):
+    import sheen_b200 as sb
+    return sb.generate_scene(args.config, args.seed, args.detail, args.photons)
+
+
+def run_ours(args):
+    import torch
+
+    import sheen_b200 as sb
+    rank, world, local = dist_setup(args.gpus)
+    sb.init(local, 100)
+    form = sb.FORM_WAVEFRONT if args.form == "wavefront" else sb.FORM_PLAIN
+    scene = make_scene(args)
+    t0 = time.perf_counter()
+    ds = sb.DeviceScene(scene, form)
+    create_s = time.perf_counter() - t0
+    out = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # > 126 MB L2
+    stream = torch.cuda.current_stream().cuda_stream
+
+    # counting frame: rays per frame and the traversal counters
+    st = ds.render_device(W, H, SPP, out.data_ptr(), stream, count_rays=True)
+    rays = st["total_rays"]
+    nodes, prims = st["node_visits"], st["prim_tests"]
+
+    for _ in range(args.warmup):
+        ds.render_device(W, H, SPP, out.data_ptr(), stream)
+    torch.cuda.synchronize()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.fill_(float(i))                      # evict L2 between frames (outside the events)
+            starts[i].record()
+            ds.render_device(W, H, SPP, out.data_ptr(), stream)
+            ends[i].record()
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    ms = max_over_ranks(ms, world)
+    frame_ms = ms / args.steps
+    value = rays * args.steps * world / (ms / 1e3) / 1e6
+
+    # end to end through the drop-in call: host scene arrays in, host RGBA
+    # out, per step: BVH build + scene upload + render + read back
+    img = np.empty((H, W, 4), np.float32)
+    e2e_steps = max(1, min(args.steps, 2))
+    sb.render_rgba(scene, W, H, SPP, form)          # warm the allocation paths
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        img, st2 = sb.render_rgba(scene, W, H, SPP, form)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e = rays * e2e_steps * world / e2e_s / 1e6
+
+    pk = peaks()
+    # algorithmic bytes: 32 B ray in + 16 B hit out per
+    # ray, B_node per box test, B_prim per primitive test
+    b_node, b_prim = (32, 48) if form == sb.FORM_PLAIN else (64, 48)
+    bytes_alg = rays * 48 + nodes * b_node + prims * b_prim
+    achieved_gbs = bytes_alg / (frame_ms / 1e3) / 1e9
+    fp32_flops = nodes * 14 + prims * 35
+    fp32_peak = 148 * 128 * 2 * pk["sm_max_mhz"] * 1e6
+    clocks = clk.summary()
+
+    line = {
+        "metric": "Mrays/s", "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(frame_ms, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": "mesh: displaced icosphere L8 (1,310,720 tris) + 16 displaced 50k-tri tori, "
+                               "1920x1080, 4 spp, 4 point lights, reflect 0.2, 4 glass tori ior 1.5",
+                   "triangles": scene.view.num_triangles, "width": W, "height": H, "spp": SPP,
+                   "form": args.form, "parallelism": f"replicas{world}",
+                   "l2": "256 MB buffer written between timed frames; scene arrays exceed L2",
+                   "rays_per_frame": rays, "box_tests_per_frame": nodes, "prim_tests_per_frame": prims,
+                   "scene_create_s": round(create_s, 3), "device_bytes": ds.device_bytes},
+        "e2e": {"value": round(e2e, 2), "unit": "Mrays/s",
+                "h2d_bytes_per_step": int(st2["device_bytes"]),
+                "d2h_bytes_per_step": W * H * 16,
+                "call": "sheen_render_scene_rgba (host BVH build + upload + render + readback)"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": round(achieved_gbs / pk["hbm_gbs"], 4), "traffic": None,
+                     "peak_source": pk["src"],
+                     "algorithmic_bytes_per_frame": int(bytes_alg),
+                     "fp32": {"flops_per_frame": int(fp32_flops),
+                              "achieved_tflops": round(fp32_flops / (frame_ms / 1e3) / 1e12, 2),
+                              "peak_tflops_nominal": round(fp32_peak / 1e12, 1)}},
+        "gpu_launches": args.steps * launches_per_frame(form),
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(ds, scene, stream, out)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ds.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def launches_per_frame(form):
+    import sheen_b200 as sb
+    return 1 if form == sb.FORM_PLAIN else int(os.environ.get("SHEEN_WAVE_LAUNCHES", "1"))
+
+
+def band_rays(ds, stream, out):
+    st = ds.render_region(W, H, SPP, 0, CPU_BAND[0], W, CPU_BAND[1], out.data_ptr(), stream, count_rays=True)
+    return st["total_rays"]
+
+
+def cpu_baseline(ds, scene, stream, out, steps=1):
+    """The reference's own code on the host cores over a band of rows."""
+    from oracle_bindings import RefHost
+    if not RefHost.available():
+        return {"value": None, "unit": "Mrays/s", "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    ref = RefHost()
+    threads = ref.lib.sheen_ref_max_threads()
+    h = ref.scene(scene.view_ptr, threads)
+    rays = band_rays(ds, stream, out)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ref.render(h, W, H, SPP, threads, CPU_BAND[0] // 16, CPU_BAND[1] // 16)
+    dt = time.perf_counter() - t0
+    return {"value": round(rays * steps / dt / 1e6, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
+            "sample": f"rows {CPU_BAND[0]}-{CPU_BAND[1]} of the 1920x1080 4 spp frame ({rays} rays), "
+                      f"{steps} pass(es), {dt:.1f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import torch
+
+    import sheen_b200 as sb
+    from oracle_bindings import RefHost
+    if not RefHost.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libsheen_ref_host.so not built"}))
+        return
+    sb.init(int(os.environ.get("LOCAL_RANK", "0")), 100)
+    scene = make_scene(args)
+    ref = RefHost()
+    threads = ref.lib.sheen_ref_max_threads()
+    h = ref.scene(scene.view_ptr, threads)
+    # ray count of the band: this renderer's counters (bookkeeping only; the
+    # timed work below is the reference's code alone)
+    ds = sb.DeviceScene(scene, sb.FORM_PLAIN)
+    out = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
+    rays = band_rays(ds, torch.cuda.current_stream().cuda_stream, out)
+    ds.close()
+    by0, by1 = CPU_BAND[0] // 16, CPU_BAND[1] // 16
+    for _ in range(args.warmup):
+        ref.render(h, W, H, SPP, threads, by0, by0 + 1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ref.render(h, W, H, SPP, threads, by0, by1)
+    dt = time.perf_counter() - t0
+    value = rays * args.steps / dt / 1e6
+    sample = (f"rows {CPU_BAND[0]}-{CPU_BAND[1]} of the 1920x1080 4 spp frame per step ({rays} rays), "
+              f"host-compiled reference render_kernel, {threads} threads")
+    print(json.dumps({
+        "impl": "reference", "metric": "Mrays/s", "value": round(value, 3), "unit": "Mrays/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": "mesh: displaced icosphere L8 + 16 tori, 1920x1080, 4 spp (row band sample)",
+                   "rays_per_step": rays},
+        "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="wavefront", choices=["wavefront", "plain"])
+    ap.add_argument("--config", type=int, default=1)
+    ap.add_argument("--detail", type=int, default=8)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--photons", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -164,10 +164,27 @@ int sheen_scene_render_device(SheenDeviceScene scene, int width, int height,
                               int aa_samples, float* out_rgba_device,
                               void* stream, int flags, SheenRenderStats* stats);
 
+/* Render only the pixel rectangle [x0, x1) x [y0, y1) of a width x height
+ * image (tiles, progressive refinement, bounded samples).  The DEVICE buffer
+ * holds the whole image; pixels outside the rectangle are left unchanged.
+ * Same synchronisation rules as sheen_scene_render_device. */
+int sheen_scene_render_region(SheenDeviceScene scene, int width, int height, int aa_samples,
+                              int x0, int y0, int x1, int y1, float* out_rgba_device,
+                              void* stream, int flags, SheenRenderStats* stats);
+
 /* Same, into a HOST buffer; includes the device -> host copy. */
 int sheen_scene_render_host(SheenDeviceScene scene, int width, int height,
                             int aa_samples, float* out_rgba_host, int flags,
                             SheenRenderStats* stats);
+
+/* Primary-ray closest hits of a resident scene, for hit-identity checks:
+ * for every pixel (x, y) and sample s of clamp(aa, 1, 64) samples, at index
+ * (y*width + x)*ns + s of the HOST arrays: the hit's object_id and
+ * material_id as the reference's scene_intersect sets them
+ * (integrator/raycast.h:14-70; 0x80000000 on a miss) and its t (-1 on a
+ * miss).  Uses the scene's form's own traversal. */
+int sheen_scene_primary_hits(SheenDeviceScene scene, int width, int height, int aa_samples,
+                             int* obj_id_host, int* mat_id_host, float* t_host);
 
 /* Owned host scenes: the .sheen loader and the synthetic generators return
  * one.  sheen_owned_view points into storage owned by the handle. */

@@ -314,3 +314,66 @@ int sheen_ref_scene_primary_hits(void* h, int width, int height, int aa,
 int sheen_ref_max_threads(void) { return omp_get_max_threads(); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------
+// The reference's .sheen loader (api/scene_io.cpp:931-968), for loader
+// parity: returns a handle whose SheenScene view points into the loaded
+// reference Scene.  settings_out: width, height, aa, photons (ints).
+// ---------------------------------------------------------------------
+#include "api/scene_io.h"
+
+namespace {
+struct RefLoaded {
+    Scene scene;
+    SceneSettings settings;
+    SheenScene view;
+    std::vector<const unsigned char*> tex_ptrs;
+    std::vector<int> tex_w, tex_h;
+    std::vector<int> hidden;
+};
+}  // namespace
+
+extern "C" {
+
+void* sheen_ref_load_scene_file(const char* path) {
+    RefLoaded* r = new RefLoaded();
+    if (!load_scene_file(path, r->scene, r->settings)) { delete r; return nullptr; }
+    Scene& s = r->scene;
+    SheenScene& v = r->view;
+    std::memset(&v, 0, sizeof(v));
+    v.camera = s.camera;
+#define V(field, vec) v.field = vec.empty() ? nullptr : vec.data(); v.num_##field = (int)vec.size();
+    V(objects, s.objects) V(sweep_points, s.sweep_points) V(sweep_strands, s.sweep_strands)
+    V(triangles, s.triangles) V(heightfields, s.heightfields) V(superellipsoids, s.superellipsoids)
+    V(lathe_points, s.lathe_points) V(lathes, s.lathes) V(prism_points, s.prism_points) V(prisms, s.prisms)
+    V(planes, s.planes) V(materials, s.materials) V(lights, s.lights) V(media, s.media)
+#undef V
+    v.csg_nodes = s.csg_nodes.empty() ? nullptr : s.csg_nodes.data();
+    v.num_csg_nodes = (int)s.csg_nodes.size();
+    v.csg_root = s.csg_root;
+    for (auto& t : s.textures) {   // level 0 of each mip chain
+        r->tex_ptrs.push_back(t.pixels.empty() ? nullptr : t.pixels.data());
+        r->tex_w.push_back(t.w);
+        r->tex_h.push_back(t.h);
+    }
+    v.texture_pixels = r->tex_ptrs.empty() ? nullptr : r->tex_ptrs.data();
+    v.texture_widths = r->tex_w.empty() ? nullptr : r->tex_w.data();
+    v.texture_heights = r->tex_h.empty() ? nullptr : r->tex_h.data();
+    v.num_textures = (int)s.textures.size();
+    v.photons = r->settings.photons;
+    v.photon_cell = r->settings.photon_cell;
+    v.caustics = r->settings.caustics;
+    r->hidden = s.se_hidden;
+    return r;
+}
+
+const SheenScene* sheen_ref_loaded_view(void* h) { return &static_cast<RefLoaded*>(h)->view; }
+
+void sheen_ref_loaded_settings(void* h, int* out4) {
+    const SceneSettings& st = static_cast<RefLoaded*>(h)->settings;
+    out4[0] = st.width; out4[1] = st.height; out4[2] = st.aa; out4[3] = st.photons;
+}
+
+void sheen_ref_loaded_free(void* h) { delete static_cast<RefLoaded*>(h); }
+
+}  // extern "C"

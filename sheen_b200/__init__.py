@@ -1,0 +1,268 @@
+"""sheen_b200 -- B200 renderer core for Sheen's per-pixel ray-casting path.
+
+Host-side mirror of the reference's Python entry points.  The reference's
+native module (api/sheen_py_module.cpp:57-87) exposes ``init(device_id,
+cuda_arch)``, ``cleanup()`` and ``render_scene(scene, width, height, aa,
+output_path)`` over libsheen_c_api.so; the same three functions are here with
+the same argument meaning and errors (RuntimeError carrying
+sheen_get_last_error()).  Beside them: RGBA output, resident device scenes
+with a choice of renderer form, the .sheen loader, the synthetic workload
+generators, and the request loop (``sheen_b200.serve``).
+
+Everything goes through the C-ABI of the in-tree ``libsheen_c_api.so``
+(built for sm_100a by ``__graft_entry__.build()`` / ``make -C
+sheen_b200/csrc``).  There is no CPU fallback: if the library is missing,
+loading fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import contract
+from .contract import SceneArrays, SheenScene
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsheen_c_api.so")
+
+FORM_PLAIN = 0
+FORM_WAVEFRONT = 1
+RENDER_COUNT_RAYS = 1
+
+_lib = None
+
+
+class RenderStats(ctypes.Structure):
+    _fields_ = [("primary_rays", ctypes.c_ulonglong), ("shadow_rays", ctypes.c_ulonglong),
+                ("secondary_rays", ctypes.c_ulonglong), ("total_rays", ctypes.c_ulonglong),
+                ("node_visits", ctypes.c_ulonglong), ("prim_tests", ctypes.c_ulonglong),
+                ("build_ms", ctypes.c_double), ("upload_ms", ctypes.c_double),
+                ("photon_ms", ctypes.c_double), ("render_ms", ctypes.c_double),
+                ("device_bytes", ctypes.c_ulonglong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class SceneSettings(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int), ("height", ctypes.c_int), ("aa", ctypes.c_int),
+                ("photons", ctypes.c_int), ("photon_cell", ctypes.c_float),
+                ("caustics", ctypes.c_float), ("output", ctypes.c_char * 512)]
+
+
+def lib():
+    """The loaded C-ABI library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libsheen_c_api.so not built ({LIB_PATH}); run __graft_entry__.build()")
+    L = ctypes.CDLL(LIB_PATH)
+    P, I, U, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint, ctypes.c_float
+    L.sheen_init.argtypes = [I, I]
+    L.sheen_init.restype = I
+    L.sheen_cleanup.argtypes = []
+    L.sheen_cleanup.restype = None
+    L.sheen_render_scene.argtypes = [P, I, I, I, ctypes.c_char_p]
+    L.sheen_render_scene.restype = I
+    L.sheen_get_last_error.argtypes = []
+    L.sheen_get_last_error.restype = ctypes.c_char_p
+    L.sheen_render_scene_rgba.argtypes = [P, I, I, I, I, P, ctypes.POINTER(RenderStats)]
+    L.sheen_render_scene_rgba.restype = I
+    L.sheen_scene_create.argtypes = [P, I, ctypes.POINTER(P)]
+    L.sheen_scene_create.restype = I
+    L.sheen_scene_destroy.argtypes = [P]
+    L.sheen_scene_destroy.restype = None
+    L.sheen_scene_device_bytes.argtypes = [P]
+    L.sheen_scene_device_bytes.restype = ctypes.c_ulonglong
+    L.sheen_scene_form.argtypes = [P]
+    L.sheen_scene_form.restype = I
+    L.sheen_scene_render_device.argtypes = [P, I, I, I, P, P, I, ctypes.POINTER(RenderStats)]
+    L.sheen_scene_render_device.restype = I
+    L.sheen_scene_render_region.argtypes = [P, I, I, I, I, I, I, I, P, P, I, ctypes.POINTER(RenderStats)]
+    L.sheen_scene_render_region.restype = I
+    L.sheen_scene_render_host.argtypes = [P, I, I, I, P, I, ctypes.POINTER(RenderStats)]
+    L.sheen_scene_render_host.restype = I
+    L.sheen_load_scene_file.argtypes = [ctypes.c_char_p, ctypes.POINTER(P)]
+    L.sheen_load_scene_file.restype = I
+    L.sheen_owned_view.argtypes = [P]
+    L.sheen_owned_view.restype = P
+    L.sheen_owned_settings.argtypes = [P]
+    L.sheen_owned_settings.restype = ctypes.POINTER(SceneSettings)
+    L.sheen_owned_free.argtypes = [P]
+    L.sheen_owned_free.restype = None
+    L.sheen_generate_scene.argtypes = [I, U, I, I, ctypes.POINTER(P)]
+    L.sheen_generate_scene.restype = I
+    L.sheen_scene_primary_hits.argtypes = [P, I, I, I, P, P, P]
+    L.sheen_scene_primary_hits.restype = I
+    L.sheen_write_png_srgb.argtypes = [ctypes.c_char_p, P, I, I]
+    L.sheen_write_png_srgb.restype = I
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return lib().sheen_get_last_error().decode("utf-8", "replace")
+
+
+def _check(rc):
+    if rc != 0:
+        raise RuntimeError(last_error())
+
+
+def _scene_ptr(scene):
+    """Accepts a ctypes SheenScene, SceneArrays, OwnedScene or a raw address."""
+    if isinstance(scene, SceneArrays):
+        v = scene.view()
+        return ctypes.addressof(v), v
+    if isinstance(scene, OwnedScene):
+        return scene.view_ptr, scene
+    if isinstance(scene, SheenScene):
+        return ctypes.addressof(scene), scene
+    if isinstance(scene, int):
+        return scene, None
+    raise TypeError("scene must be a SheenScene, SceneArrays, OwnedScene or address")
+
+
+# --- reference-compatible entry points (api/sheen_py_module.cpp:33-87) ---
+
+def init(device_id: int = 0, cuda_arch: int = 100) -> None:
+    _check(lib().sheen_init(device_id, cuda_arch))
+
+
+def cleanup() -> None:
+    lib().sheen_cleanup()
+
+
+def render_scene(scene, width: int, height: int, aa: int, output_path: str) -> None:
+    ptr, keep = _scene_ptr(scene)
+    _check(lib().sheen_render_scene(ptr, width, height, aa, output_path.encode()))
+    del keep
+
+
+# --- additions ---
+
+def render_rgba(scene, width: int, height: int, aa: int, form: int = FORM_PLAIN):
+    """Linear RGBA float32 image (height, width, 4) and the render stats."""
+    ptr, keep = _scene_ptr(scene)
+    out = np.empty((height, width, 4), np.float32)
+    st = RenderStats()
+    _check(lib().sheen_render_scene_rgba(ptr, width, height, aa, form, out.ctypes.data, ctypes.byref(st)))
+    del keep
+    return out, st.as_dict()
+
+
+class DeviceScene:
+    """A scene resident in HBM (SheenDeviceScene)."""
+
+    def __init__(self, scene, form: int = FORM_PLAIN):
+        ptr, keep = _scene_ptr(scene)
+        h = ctypes.c_void_p()
+        _check(lib().sheen_scene_create(ptr, form, ctypes.byref(h)))
+        del keep
+        self.handle = h.value
+        self.form = form
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().sheen_scene_device_bytes(self.handle))
+
+    def render_host(self, width, height, aa, count_rays=False):
+        out = np.empty((height, width, 4), np.float32)
+        st = RenderStats()
+        _check(lib().sheen_scene_render_host(self.handle, width, height, aa, out.ctypes.data,
+                                             RENDER_COUNT_RAYS if count_rays else 0, ctypes.byref(st)))
+        return out, st.as_dict()
+
+    def render_device(self, width, height, aa, out_ptr: int, stream: int = 0, count_rays=False, stats=False):
+        """Render into a device buffer (width*height float4).  With count_rays
+        or stats the call synchronises and returns the stats dict."""
+        st = RenderStats() if (stats or count_rays) else None
+        _check(lib().sheen_scene_render_device(self.handle, width, height, aa, out_ptr, stream,
+                                               RENDER_COUNT_RAYS if count_rays else 0,
+                                               ctypes.byref(st) if st is not None else None))
+        return st.as_dict() if st is not None else None
+
+    def render_region(self, width, height, aa, x0, y0, x1, y1, out_ptr: int, stream: int = 0,
+                      count_rays=False, stats=False):
+        """Render pixels [x0, x1) x [y0, y1) of a width x height image into the
+        device buffer at out_ptr (whole image, width*height float4)."""
+        st = RenderStats() if (stats or count_rays) else None
+        _check(lib().sheen_scene_render_region(self.handle, width, height, aa, x0, y0, x1, y1, out_ptr, stream,
+                                               RENDER_COUNT_RAYS if count_rays else 0,
+                                               ctypes.byref(st) if st is not None else None))
+        return st.as_dict() if st is not None else None
+
+    def primary_hits(self, width, height, aa):
+        """Per-sample primary closest hits: object id, material id, t."""
+        ns = max(1, min(aa, 64))
+        n = width * height * ns
+        obj = np.zeros(n, np.int32)
+        mat = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        _check(lib().sheen_scene_primary_hits(self.handle, width, height, aa, obj.ctypes.data,
+                                              mat.ctypes.data, t.ctypes.data))
+        return obj, mat, t
+
+    def close(self):
+        if self.handle:
+            lib().sheen_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class OwnedScene:
+    """Host scene owned by the library (.sheen loader or generator)."""
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    @property
+    def view_ptr(self) -> int:
+        return lib().sheen_owned_view(self.handle)
+
+    @property
+    def view(self) -> SheenScene:
+        return SheenScene.from_address(self.view_ptr)
+
+    @property
+    def settings(self) -> dict:
+        s = lib().sheen_owned_settings(self.handle).contents
+        return {"width": s.width, "height": s.height, "aa": s.aa, "photons": s.photons,
+                "photon_cell": s.photon_cell, "caustics": s.caustics,
+                "output": s.output.decode("utf-8", "replace")}
+
+    def close(self):
+        if self.handle:
+            lib().sheen_owned_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def load_scene_file(path: str) -> OwnedScene:
+    h = ctypes.c_void_p()
+    _check(lib().sheen_load_scene_file(path.encode(), ctypes.byref(h)))
+    return OwnedScene(h.value)
+
+
+def generate_scene(config: int, seed: int = 1, detail: int = 0, photons: int = 0) -> OwnedScene:
+    h = ctypes.c_void_p()
+    _check(lib().sheen_generate_scene(config, seed, detail, photons, ctypes.byref(h)))
+    return OwnedScene(h.value)
+
+
+def write_png(path: str, rgba: np.ndarray) -> None:
+    rgba = np.ascontiguousarray(rgba, np.float32)
+    _check(lib().sheen_write_png_srgb(path.encode(), rgba.ctypes.data, rgba.shape[1], rgba.shape[0]))

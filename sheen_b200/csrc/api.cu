@@ -1,0 +1,230 @@
+// api.cu -- the C-ABI of libsheen_c_api.so (include/sheen_c_api.h).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <set>
+#include <vector>
+
+#include "engine.h"
+
+namespace sheen {
+void release_all_servers();
+}
+
+namespace {
+
+std::mutex g_mu;
+std::set<sheen::DeviceScene*> g_scenes;
+
+int fail_cuda(cudaError_t e) {
+    sheen::set_error(cudaGetErrorString(e));
+    return -1;
+}
+
+// Parameter rules of sheen_render_scene (api/sheen_c_api.cu:189-193).
+int check_params(const SheenScene* s, int w, int h, int aa) {
+    if (!s) { sheen::set_error("null scene"); return -1; }
+    if (w <= 0 || h <= 0 || aa < 1 || aa > 64) { sheen::set_error("bad render params"); return -1; }
+    if (!s->num_materials) { sheen::set_error("no materials"); return -1; }
+    return 0;
+}
+
+void fill_stats(const sheen::DeviceScene& s, const unsigned long long* t, double render_ms, SheenRenderStats* st) {
+    if (!st) return;
+    std::memset(st, 0, sizeof(*st));
+    if (t) {
+        st->primary_rays = t[0];
+        st->shadow_rays = t[1];
+        st->secondary_rays = t[2];
+        st->node_visits = t[3];
+        st->prim_tests = t[4];
+        st->total_rays = t[0] + t[1] + t[2];
+    }
+    st->build_ms = s.build_ms;
+    st->upload_ms = s.upload_ms;
+    st->photon_ms = s.photon_ms;
+    st->render_ms = render_ms;
+    st->device_bytes = s.arena_bytes + s.extra_bytes;
+}
+
+// Launch one frame of `s` into device buffer `out`; optionally count rays
+// and time it with events on `stream`.
+int render_device(sheen::DeviceScene& s, int W, int H, int aa, sheen::Region rg, float4* out, cudaStream_t stream,
+                  int flags, SheenRenderStats* stats) {
+    if (rg.x0 < 0 || rg.y0 < 0 || rg.x1 > W || rg.y1 > H || rg.x0 >= rg.x1 || rg.y0 >= rg.y1) {
+        sheen::set_error("bad render region");
+        return -1;
+    }
+    const bool want_stats = stats != nullptr || (flags & SHEEN_RENDER_COUNT_RAYS);
+    cudaError_t e;
+    if (want_stats) {
+        e = cudaMemsetAsync(s.d_tally, 0, 8 * sizeof(unsigned long long), stream);
+        if (e != cudaSuccess) return fail_cuda(e);
+    }
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    if (want_stats) {
+        cudaEventCreate(&ev0);
+        cudaEventCreate(&ev1);
+        cudaEventRecord(ev0, stream);
+    }
+    if (s.form == SHEEN_FORM_PLAIN)
+        e = sheen::launch_plain(s, W, H, aa, rg, out, stream, (flags & SHEEN_RENDER_COUNT_RAYS) != 0);
+    else
+        e = sheen::launch_wavefront(s, W, H, aa, rg, out, stream);
+    if (e != cudaSuccess) return fail_cuda(e);
+    if (want_stats) {
+        cudaEventRecord(ev1, stream);
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return fail_cuda(e);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+        unsigned long long t[8] = {0};
+        e = cudaMemcpy(t, s.d_tally, sizeof(t), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return fail_cuda(e);
+        fill_stats(s, t, ms, stats);
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sheen_init(int device_id, int cuda_arch) {
+    (void)cuda_arch;
+    cudaError_t e = cudaSetDevice(device_id);
+    if (e != cudaSuccess) return fail_cuda(e);
+    e = cudaFree(0);
+    if (e != cudaSuccess) return fail_cuda(e);
+    return 0;
+}
+
+void sheen_cleanup(void) {
+    sheen::release_all_servers();
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        for (auto* s : g_scenes) sheen::scene_release(s);
+        g_scenes.clear();
+    }
+    cudaDeviceSynchronize();
+    cudaDeviceReset();
+}
+
+int sheen_scene_create(const SheenScene* scene, int form, SheenDeviceScene* out) {
+    if (!out) { sheen::set_error("null output handle"); return -1; }
+    *out = nullptr;
+    if (!scene) { sheen::set_error("null scene"); return -1; }
+    if (!scene->num_materials) { sheen::set_error("no materials"); return -1; }
+    sheen::DeviceScene* s = nullptr;
+    if (sheen::scene_upload(scene, form, &s) != 0) return -1;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_scenes.insert(s);
+    }
+    *out = reinterpret_cast<SheenDeviceScene>(s);
+    return 0;
+}
+
+void sheen_scene_destroy(SheenDeviceScene h) {
+    auto* s = reinterpret_cast<sheen::DeviceScene*>(h);
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        if (!g_scenes.erase(s)) return;
+    }
+    cudaDeviceSynchronize();
+    sheen::scene_release(s);
+}
+
+unsigned long long sheen_scene_device_bytes(SheenDeviceScene h) {
+    auto* s = reinterpret_cast<sheen::DeviceScene*>(h);
+    return s ? (unsigned long long)(s->arena_bytes + s->extra_bytes) : 0ull;
+}
+
+int sheen_scene_form(SheenDeviceScene h) {
+    auto* s = reinterpret_cast<sheen::DeviceScene*>(h);
+    return s ? s->form : -1;
+}
+
+int sheen_scene_render_device(SheenDeviceScene h, int W, int H, int aa, float* out, void* stream, int flags,
+                              SheenRenderStats* stats) {
+    auto* s = reinterpret_cast<sheen::DeviceScene*>(h);
+    if (!s) { sheen::set_error("null scene handle"); return -1; }
+    if (W <= 0 || H <= 0 || aa < 1 || aa > 64 || !out) { sheen::set_error("bad render params"); return -1; }
+    return render_device(*s, W, H, aa, sheen::Region{0, 0, W, H}, reinterpret_cast<float4*>(out),
+                         (cudaStream_t)stream, flags, stats);
+}
+
+int sheen_scene_render_region(SheenDeviceScene h, int W, int H, int aa, int x0, int y0, int x1, int y1, float* out,
+                              void* stream, int flags, SheenRenderStats* stats) {
+    auto* s = reinterpret_cast<sheen::DeviceScene*>(h);
+    if (!s) { sheen::set_error("null scene handle"); return -1; }
+    if (W <= 0 || H <= 0 || aa < 1 || aa > 64 || !out) { sheen::set_error("bad render params"); return -1; }
+    return render_device(*s, W, H, aa, sheen::Region{x0, y0, x1, y1}, reinterpret_cast<float4*>(out),
+                         (cudaStream_t)stream, flags, stats);
+}
+
+int sheen_scene_render_host(SheenDeviceScene h, int W, int H, int aa, float* out_host, int flags,
+                            SheenRenderStats* stats) {
+    auto* s = reinterpret_cast<sheen::DeviceScene*>(h);
+    if (!s) { sheen::set_error("null scene handle"); return -1; }
+    if (W <= 0 || H <= 0 || aa < 1 || aa > 64 || !out_host) { sheen::set_error("bad render params"); return -1; }
+    float4* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, (size_t)W * H * sizeof(float4));
+    if (e != cudaSuccess) return fail_cuda(e);
+    int rc = render_device(*s, W, H, aa, sheen::Region{0, 0, W, H}, d, 0, flags, stats);
+    if (rc == 0) {
+        e = cudaMemcpy(out_host, d, (size_t)W * H * sizeof(float4), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = fail_cuda(e);
+    }
+    cudaFree(d);
+    return rc;
+}
+
+int sheen_scene_primary_hits(SheenDeviceScene h, int W, int H, int aa, int* obj, int* mat, float* t) {
+    auto* s = reinterpret_cast<sheen::DeviceScene*>(h);
+    if (!s) { sheen::set_error("null scene handle"); return -1; }
+    if (W <= 0 || H <= 0 || !obj || !mat || !t) { sheen::set_error("bad render params"); return -1; }
+    const int ns = aa < 1 ? 1 : (aa > 64 ? 64 : aa);
+    const size_t n = (size_t)W * H * ns;
+    int *dobj = nullptr, *dmat = nullptr;
+    float* dt = nullptr;
+    cudaError_t e = cudaMalloc(&dobj, n * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&dmat, n * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&dt, n * sizeof(float));
+    if (e == cudaSuccess)
+        e = s->form == SHEEN_FORM_PLAIN ? sheen::launch_primary_hits_plain(*s, W, H, ns, dobj, dmat, dt, 0)
+                                        : sheen::launch_primary_hits_bvh4(*s, W, H, ns, dobj, dmat, dt, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(obj, dobj, n * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(mat, dmat, n * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(t, dt, n * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(dobj);
+    cudaFree(dmat);
+    cudaFree(dt);
+    return e == cudaSuccess ? 0 : fail_cuda(e);
+}
+
+int sheen_render_scene_rgba(const SheenScene* scene, int W, int H, int aa, int form, float* out_host,
+                            SheenRenderStats* stats) {
+    if (check_params(scene, W, H, aa) != 0) return -1;
+    if (!out_host) { sheen::set_error("null output buffer"); return -1; }
+    sheen::DeviceScene* s = nullptr;
+    if (sheen::scene_upload(scene, form, &s) != 0) return -1;
+    int rc = sheen_scene_render_host(reinterpret_cast<SheenDeviceScene>(s), W, H, aa, out_host, 0, stats);
+    sheen::scene_release(s);
+    return rc;
+}
+
+int sheen_render_scene(const SheenScene* scene, int W, int H, int aa, const char* path) {
+    if (check_params(scene, W, H, aa) != 0) return -1;
+    if (!path) { sheen::set_error("bad render params"); return -1; }
+    std::vector<float> rgba((size_t)W * H * 4);
+    if (sheen_render_scene_rgba(scene, W, H, aa, SHEEN_FORM_PLAIN, rgba.data(), nullptr) != 0) return -1;
+    return sheen_write_png_srgb(path, rgba.data(), W, H);
+}
+
+}  // extern "C"

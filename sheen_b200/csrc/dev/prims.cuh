@@ -1,0 +1,531 @@
+// prims.cuh -- ray/primitive tests with the reference's semantics.
+//
+// Each function states the reference lines whose results it reproduces.
+// They are shared by every renderer form: the forms differ in how they find
+// candidate primitives, never in how a primitive answers.
+#pragma once
+#include "scene.cuh"
+#include "vec.cuh"
+
+namespace sheen {
+namespace dev {
+
+// Slab test of bvh.h:578-600.  Note the reference's final check uses the
+// interval merged over x and y only (z only rejects disjoint slabs).
+__device__ __forceinline__ bool box_hit_ref(const Ray& r, float3 lo, float3 hi) {
+    float ix = 1.0f / r.d.x;
+    float tminX = (lo.x - r.o.x) * ix, tmaxX = (hi.x - r.o.x) * ix;
+    if (tminX > tmaxX) { float t = tminX; tminX = tmaxX; tmaxX = t; }
+    float iy = 1.0f / r.d.y;
+    float tminY = (lo.y - r.o.y) * iy, tmaxY = (hi.y - r.o.y) * iy;
+    if (tminY > tmaxY) { float t = tminY; tminY = tmaxY; tmaxY = t; }
+    if (tminX > tmaxY || tminY > tmaxX) return false;
+    if (tminY > tminX) tminX = tminY;
+    if (tmaxY < tmaxX) tmaxX = tmaxY;
+    float iz = 1.0f / r.d.z;
+    float tminZ = (lo.z - r.o.z) * iz, tmaxZ = (hi.z - r.o.z) * iz;
+    if (tminZ > tmaxZ) { float t = tminZ; tminZ = tmaxZ; tmaxZ = t; }
+    if (tminX > tmaxZ || tminZ > tmaxX) return false;
+    return (tmaxX >= r.tmin) && (tminX <= r.tmax);
+}
+
+// primitives/sphere.h:33-53: near root, else far root, inside [tmin, tmax].
+__device__ __forceinline__ bool sphere_test(const Ray& r, float3 c, float rad, Hit& h) {
+    float3 oc = r.o - c;
+    float a = dot(r.d, r.d);
+    float b = 2.0f * dot(oc, r.d);
+    float cc = dot(oc, oc) - rad * rad;
+    float disc = b * b - 4.0f * a * cc;
+    if (disc < 0.0f) return false;
+    float sq = sqrtf(disc);
+    float t = (-b - sq) / (2.0f * a);
+    if (t < r.tmin || t > r.tmax) {
+        t = (-b + sq) / (2.0f * a);
+        if (t < r.tmin || t > r.tmax) return false;
+    }
+    h.t = t;
+    h.p = r.o + t * r.d;
+    h.n = normalize(h.p - c);
+    h.tan = f3(0.0f, 0.0f, 0.0f);
+    h.uv = make_float2(0.0f, 0.0f);
+    return true;
+}
+
+// primitives/sphere.h:11-28: [t_enter, t_exit] clipped to [t0, t1].
+__device__ __forceinline__ bool sphere_span(const Ray& r, float3 c, float rad, float t0, float t1,
+                                            float& te, float& tx) {
+    float3 oc = r.o - c;
+    float a = dot(r.d, r.d);
+    float b = 2.0f * dot(oc, r.d);
+    float cc = dot(oc, oc) - rad * rad;
+    float disc = b * b - 4.0f * a * cc;
+    if (disc < 0.0f) return false;
+    float sq = sqrtf(disc);
+    float ta = (-b - sq) / (2.0f * a);
+    float tb = (-b + sq) / (2.0f * a);
+    if (tb < t0 || ta > t1) return false;
+    te = fmaxf(ta, t0);
+    tx = fminf(tb, t1);
+    return te <= tx;
+}
+
+// primitives/plane.h:7-24
+__device__ __forceinline__ bool plane_test(const Ray& r, float3 n, float d, Hit& h) {
+    float den = dot(n, r.d);
+    if (fabsf(den) > 1e-6f) {
+        float t = -(dot(r.o, n) + d) / den;
+        if (t >= r.tmin && t <= r.tmax) {
+            h.t = t;
+            h.p = r.o + t * r.d;
+            h.n = dot(n, r.d) > 0.0f ? -n : n;
+            h.tan = f3(0.0f, 0.0f, 0.0f);
+            h.uv = make_float2(0.0f, 0.0f);
+            return true;
+        }
+    }
+    return false;
+}
+
+// primitives/triangle.h:8-47, positions only (Moller-Trumbore, det eps 1e-8,
+// u, v in [0, 1]).  Returns t and barycentrics; the hit record is completed
+// by tri_finish() once the closest triangle is known.
+__device__ __forceinline__ bool tri_test(const Ray& r, float3 v0, float3 v1, float3 v2,
+                                         float& t, float& u, float& v) {
+    float3 e1 = v1 - v0, e2 = v2 - v0;
+    float3 pv = cross(r.d, e2);
+    float det = dot(e1, pv);
+    if (fabsf(det) < 1e-8f) return false;
+    float inv = 1.0f / det;
+    float3 tv = r.o - v0;
+    u = dot(tv, pv) * inv;
+    if (u < 0.0f || u > 1.0f) return false;
+    float3 qv = cross(tv, e1);
+    v = dot(r.d, qv) * inv;
+    if (v < 0.0f || u + v > 1.0f) return false;
+    t = dot(e2, qv) * inv;
+    return !(t < r.tmin || t > r.tmax);
+}
+
+__device__ __forceinline__ void tri_finish(const Ray& r, const Triangle& tr, float t, float u, float v, Hit& h) {
+    float3 v0 = f3(tr.v0), e1 = f3(tr.v1) - v0, e2 = f3(tr.v2) - v0;
+    h.t = t;
+    h.p = r.o + t * r.d;
+    float w = 1.0f - u - v;
+    float3 nv = f3(tr.n0) * w + f3(tr.n1) * u + f3(tr.n2) * v;
+    h.n = dot(nv, nv) > 1e-12f ? normalize(nv) : normalize(cross(e1, e2));
+    h.tan = normalize(e1);
+    h.uv = make_float2(tr.uv0.x * w + tr.uv1.x * u + tr.uv2.x * v, tr.uv0.y * w + tr.uv1.y * u + tr.uv2.y * v);
+    if (dot(h.n, r.d) > 0.0f) h.n = -h.n;
+    h.mat = tr.material_id;
+}
+
+// primitives/cone.h:11-73: truncated cone between two sweep points, radial
+// normal (no axial term), first root inside the ray range and the segment.
+__device__ __forceinline__ bool cone_test(const Ray& r, float3 p0, float r0, float3 p1, float r1, Hit& h) {
+    float3 axis = p1 - p0;
+    float L2 = dot(axis, axis);
+    if (L2 < 1e-12f) return false;
+    float L = sqrtf(L2);
+    float3 da = axis / L;
+    float k = (r1 - r0) / L;
+    float3 Q = r.o - p0;
+    float u = dot(r.d, da), v = dot(Q, da);
+    float3 Dp = r.d - u * da, Qp = Q - v * da;
+    float A = dot(Dp, Dp) - k * k * u * u;
+    float B = 2.0f * (dot(Dp, Qp) - k * r0 * u - k * k * v * u);
+    float C = dot(Qp, Qp) - k * k * v * v - 2.0f * k * r0 * v - r0 * r0;
+    float disc = B * B - 4.0f * A * C;
+    if (disc < 0.0f) return false;
+    float sq = sqrtf(disc);
+    float i2a = 1.0f / (2.0f * A);
+    float s1 = (-B - sq) * i2a, s2 = (-B + sq) * i2a;
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        float s = i == 0 ? s1 : s2;
+        if (s < r.tmin || s > r.tmax) continue;
+        float tp = v + s * u;
+        if (tp < 0.0f || tp > L) continue;
+        h.t = s;
+        h.p = r.o + s * r.d;
+        h.n = normalize(Qp + s * Dp);
+        h.tan = da;
+        if (dot(h.n, r.d) > 0.0f) h.n = -h.n;
+        return true;
+    }
+    return false;
+}
+
+// primitives/cone.h:78-121: sphere cap kept on the side of `axis`.  The
+// reference leaves the tangent unset here; it is zero in this renderer.
+__device__ __forceinline__ bool cap_test(const Ray& r, float3 c, float rad, float3 axis, Hit& h) {
+    float3 oc = r.o - c;
+    float a = dot(r.d, r.d);
+    float b = 2.0f * dot(oc, r.d);
+    float cc = dot(oc, oc) - rad * rad;
+    float disc = b * b - 4.0f * a * cc;
+    if (disc < 0.0f) return false;
+    float sq = sqrtf(disc);
+    float i2a = 1.0f / (2.0f * a);
+    float t1 = (-b - sq) * i2a, t2 = (-b + sq) * i2a;
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        float t = i == 0 ? t1 : t2;
+        if (t < r.tmin || t > r.tmax) continue;
+        float3 p = r.o + t * r.d;
+        float3 n = normalize(p - c);
+        if (dot(n, axis) < 0.0f) continue;
+        h.t = t; h.p = p; h.n = dot(n, r.d) > 0.0f ? -n : n;
+        h.tan = f3(0.0f, 0.0f, 0.0f);
+        return true;
+    }
+    return false;
+}
+
+// primitives/sweep.h:13-90: a strand = caps at both ends + cone pieces with
+// caps at the joints; closest of all against the unchanged ray range.
+__device__ __forceinline__ bool strand_test(const Ray& r, const SweepStrand& st, const SweepPoint* pts, Hit& h) {
+    const int n = st.point_count;
+    if (n < 2) return false;
+    const SweepPoint* P = pts + st.point_offset;
+    bool any = false;
+    float best = r.tmax;
+    Hit tmp;
+    if (cap_test(r, f3(P[0].position), P[0].radius, normalize(f3(P[0].position) - f3(P[1].position)), tmp) &&
+        tmp.t < best) { h = tmp; best = tmp.t; any = true; }
+    for (int i = 0; i < n - 1; i++) {
+        float3 a = f3(P[i].position), b = f3(P[i + 1].position);
+        if (cone_test(r, a, P[i].radius, b, P[i + 1].radius, tmp) && tmp.t < best) { h = tmp; best = tmp.t; any = true; }
+        if (i < n - 2) {
+            float3 ax = normalize(f3(P[i + 2].position) - b);
+            if (cap_test(r, b, P[i + 1].radius, ax, tmp) && tmp.t < best) { h = tmp; best = tmp.t; any = true; }
+        }
+    }
+    float3 pl = f3(P[n - 1].position), pp = f3(P[n - 2].position);
+    if (cap_test(r, pl, P[n - 1].radius, normalize(pl - pp), tmp) && tmp.t < best) { h = tmp; best = tmp.t; any = true; }
+    if (any) { h.mat = st.material_id; h.uv = make_float2(0.0f, 0.0f); }
+    return any;
+}
+
+// primitives/sweep.h:96-137: optical depth of one strand piece for a ray.
+__device__ __forceinline__ float piece_tau(const Ray& r, const SweepPoint& a, const SweepPoint& b, float sigma) {
+    float3 u = f3(b.position) - f3(a.position);
+    float A = dot(u, u);
+    if (A < 1e-12f) return 0.0f;
+    float3 v = r.d, w = r.o - f3(a.position);
+    float B = dot(u, v), C = dot(v, v), D = dot(u, w), E = dot(v, w);
+    float den = A * C - B * B;
+    float s = (den > 1e-9f) ? (B * E - C * D) / den : 0.0f;
+    s = fminf(fmaxf(s, 0.0f), 1.0f);
+    float t = (B * s + E) / C;
+    if (t < 0.0f) { t = 0.0f; s = fminf(fmaxf(-D / A, 0.0f), 1.0f); }
+    if (t > r.tmax) return 0.0f;
+    float3 cl = w + u * s - v * t;
+    float d2 = dot(cl, cl);
+    float rr = a.radius + (b.radius - a.radius) * s;
+    float r2 = rr * rr;
+    if (d2 >= r2) return 0.0f;
+    return sigma * (2.0f * sqrtf(fmaxf(r2 - d2, 0.0f)));
+}
+
+__device__ __forceinline__ float strand_tau(const Ray& r, const SweepStrand& st, const SweepPoint* pts, float sigma) {
+    float tau = 0.0f;
+    for (int i = 0; i < st.point_count - 1; i++) {
+        tau += piece_tau(r, pts[st.point_offset + i], pts[st.point_offset + i + 1], sigma);
+        if (tau > 6.0f) break;
+    }
+    return tau;
+}
+
+// primitives/lathe.h:14-63.  The profile turns about the world Y axis
+// (x = z = 0): Lathe.center does not move the surface, as in the reference.
+__device__ __forceinline__ bool lathe_test(const Ray& r, const Lathe& l, const LathePoint* pts, Hit& h) {
+    if (l.point_count < 2) return false;
+    bool any = false;
+    float best = r.tmax;
+    Hit tmp;
+    for (int i = 0; i < l.point_count - 1; i++) {
+        const LathePoint a = pts[l.point_offset + i], b = pts[l.point_offset + i + 1];
+        if (a.radius <= 0.0f && b.radius <= 0.0f) continue;
+        if (cone_test(r, f3(0.0f, a.y, 0.0f), a.radius, f3(0.0f, b.y, 0.0f), b.radius, tmp) && tmp.t < best) {
+            tmp.p = r.o + tmp.t * r.d;
+            h = tmp; best = tmp.t; any = true;
+        }
+    }
+    if (any) { h.mat = l.material_id; h.uv = make_float2(0.0f, 0.0f); }
+    return any;
+}
+
+// primitives/prism.h:18-63: even-odd containment of (x, z) over the closed
+// sub-contours (a contour ends where its first point repeats).
+__device__ __forceinline__ bool prism_contains(float x, float z, const Prism& p, const PrismPoint* all) {
+    const int base = p.point_offset, cnt = p.point_count;
+    bool inside = false;
+    int i = 0;
+    while (i < cnt) {
+        const int start = i;
+        const float sx = all[base + start].x, sz = all[base + start].z;
+        int j = i + 1;
+        while (j < cnt && !(all[base + j].x == sx && all[base + j].z == sz)) j++;
+        const int len = j - start;
+        if (len >= 3) {
+            bool in = false;
+            int q = len - 1;
+            for (int k = 0; k < len; k++) {
+                const PrismPoint pk = all[base + start + k], pq = all[base + start + q];
+                if ((pk.z > z) != (pq.z > z)) {
+                    float xint = (pq.x - pk.x) * (z - pk.z) / (pq.z - pk.z) + pk.x;
+                    if (x < xint) in = !in;
+                }
+                q = k;
+            }
+            if (in) inside = !inside;
+        }
+        i = j < cnt ? j + 1 : j;
+    }
+    return inside;
+}
+
+// primitives/prism.h:68-133: caps (y_min, y_max) and vertical walls.
+__device__ __forceinline__ bool prism_test(const Ray& r, const Prism& p, const PrismPoint* pts, Hit& h) {
+    const float y0 = p.center.y + p.y_min, y1 = p.center.y + p.y_max;
+    float ty0 = (y0 - r.o.y) / r.d.y, ty1 = (y1 - r.o.y) / r.d.y;
+    if (ty0 > ty1) { float t = ty0; ty0 = ty1; ty1 = t; }
+    if (fmaxf(ty0, r.tmin) > fminf(ty1, r.tmax)) return false;
+    bool any = false;
+    float best = r.tmax;
+    for (int face = 0; face < 2; face++) {
+        float yf = face == 0 ? y0 : y1;
+        float t = (yf - r.o.y) / r.d.y;
+        if (t < r.tmin || t > r.tmax) continue;
+        float3 P = r.o + t * r.d;
+        if (!prism_contains(P.x - p.center.x, P.z - p.center.z, p, pts)) continue;
+        if (t < best) {
+            float3 n = f3(0.0f, face == 0 ? -1.0f : 1.0f, 0.0f);
+            h.t = t; h.p = P; h.n = dot(n, r.d) > 0.0f ? -n : n;
+            h.tan = f3(1.0f, 0.0f, 0.0f);
+            best = t; any = true;
+        }
+    }
+    const float dx = r.d.x, dy = r.d.y, dz = r.d.z, ox = r.o.x, oz = r.o.z;
+    const int base = p.point_offset, cnt = p.point_count;
+    for (int i = 0; i < cnt; i++) {
+        const PrismPoint a = pts[base + i], b = pts[base + (i + 1) % cnt];
+        if (a.x == b.x && a.z == b.z) continue;
+        float ax = a.x + p.center.x, az = a.z + p.center.z;
+        float bx = b.x + p.center.x, bz = b.z + p.center.z;
+        float ex = bx - ax, ez = bz - az;
+        float den = ex * dz - ez * dx;
+        if (fabsf(den) < 1e-9f) continue;
+        float s = (dx * (az - oz) - dz * (ax - ox)) / den;
+        if (s < -0.001f || s > 1.001f) continue;
+        float t;
+        if (fabsf(dx) > 1e-9f) t = (ax + s * ex - ox) / dx;
+        else if (fabsf(dz) > 1e-9f) t = (az + s * ez - oz) / dz;
+        else continue;
+        if (t < r.tmin || t > r.tmax) continue;
+        float yy = r.o.y + dy * t;
+        if (yy < y0 - 0.001f || yy > y1 + 0.001f) continue;
+        if (t < best) {
+            float3 n = normalize(f3(ez, 0.0f, -ex));
+            h.t = t; h.p = r.o + t * r.d; h.n = dot(n, r.d) > 0.0f ? -n : n;
+            h.tan = f3(0.0f, 1.0f, 0.0f);
+            best = t; any = true;
+        }
+    }
+    if (any) { h.mat = p.material_id; h.uv = make_float2(0.0f, 0.0f); }
+    return any;
+}
+
+// primitives/superellipsoid.h:12-28
+__device__ __forceinline__ float se_value(const Superellipsoid& s, float3 p) {
+    float qx = (p.x - s.center.x) / s.a, qy = (p.y - s.center.y) / s.b, qz = (p.z - s.center.z) / s.c;
+    return powf(fabsf(qx), s.n) + powf(fabsf(qy), s.n) + powf(fabsf(qz), s.n);
+}
+__device__ __forceinline__ float3 se_gradient(const Superellipsoid& s, float3 p) {
+    float qx = (p.x - s.center.x) / s.a, qy = (p.y - s.center.y) / s.b, qz = (p.z - s.center.z) / s.c;
+    return f3(s.n * powf(fabsf(qx), s.n - 1.0f) * (qx >= 0.0f ? 1.0f : -1.0f) / s.a,
+              s.n * powf(fabsf(qy), s.n - 1.0f) * (qy >= 0.0f ? 1.0f : -1.0f) / s.b,
+              s.n * powf(fabsf(qz), s.n - 1.0f) * (qz >= 0.0f ? 1.0f : -1.0f) / s.c);
+}
+
+__device__ __forceinline__ void se_chord(const Ray& r, const Superellipsoid& s, float& tA, float& tB) {
+    const float3 lo = f3(s.center.x - s.a, s.center.y - s.b, s.center.z - s.c);
+    const float3 hi = f3(s.center.x + s.a, s.center.y + s.b, s.center.z + s.c);
+    float ix = 1.0f / r.d.x;
+    float tx0 = (lo.x - r.o.x) * ix, tx1 = (hi.x - r.o.x) * ix;
+    if (tx0 > tx1) { float t = tx0; tx0 = tx1; tx1 = t; }
+    float iy = 1.0f / r.d.y;
+    float ty0 = (lo.y - r.o.y) * iy, ty1 = (hi.y - r.o.y) * iy;
+    if (ty0 > ty1) { float t = ty0; ty0 = ty1; ty1 = t; }
+    float iz = 1.0f / r.d.z;
+    float tz0 = (lo.z - r.o.z) * iz, tz1 = (hi.z - r.o.z) * iz;
+    if (tz0 > tz1) { float t = tz0; tz0 = tz1; tz1 = t; }
+    tA = fmaxf(fmaxf(tx0, ty0), tz0);
+    tB = fminf(fminf(tx1, ty1), tz1);
+}
+
+// primitives/superellipsoid.h:41-117: 32 samples of F along the clipped
+// chord, 20 bisection steps for the exit.  As in the reference an entry
+// found by sampling is not refined (its bisection interval is empty), so
+// the entry lies on a sample.
+__device__ __forceinline__ bool se_span(const Ray& r, const Superellipsoid& s, float t0, float t1,
+                                        float& te, float& tx) {
+    float tA, tB;
+    se_chord(r, s, tA, tB);
+    if (tB < t0 || tA > t1 || tB < tA) return false;
+    t0 = fmaxf(t0, tA);
+    t1 = fminf(t1, tB);
+    const float step = (t1 - t0) / 32.0f;
+    float tp = t0;
+    bool inside = se_value(s, r.o + tp * r.d) <= 1.0f;
+    bool found_in = inside, found_out = false;
+    te = inside ? t0 : -1e30f;
+    tx = -1e30f;
+    for (int i = 1; i <= 32 && !found_out; i++) {
+        float t = fminf(t0 + step * (float)i, t1);
+        float F = se_value(s, r.o + t * r.d);
+        if (inside && F > 1.0f) {
+            float lo = tp, hi = t;
+            for (int b = 0; b < 20; b++) {
+                float mid = 0.5f * (lo + hi);
+                if (se_value(s, r.o + mid * r.d) > 1.0f) hi = mid; else lo = mid;
+            }
+            tx = fminf(0.5f * (lo + hi), t1);
+            found_out = true;
+            break;
+        }
+        tp = t;
+        if (!inside && F <= 1.0f) {
+            te = fmaxf(t, t0);   // bisection over [t, t] in the reference
+            found_in = true;
+            inside = true;
+        }
+    }
+    if (!found_in) return false;
+    if (!found_out) tx = t1;
+    return te <= tx;
+}
+
+// primitives/superellipsoid.h:123-161
+__device__ __forceinline__ bool se_test(const Ray& r, const Superellipsoid& s, Hit& h) {
+    float t0, t1;
+    se_chord(r, s, t0, t1);
+    if (t1 < r.tmin || t0 > r.tmax || t1 < t0) return false;
+    t0 = fmaxf(t0, r.tmin);
+    t1 = fminf(t1, r.tmax);
+    float te, tx;
+    if (!se_span(r, s, t0, t1, te, tx)) return false;
+    h.t = te;
+    h.p = r.o + te * r.d;
+    h.n = normalize(se_gradient(s, h.p));
+    h.tan = f3(1.0f, 0.0f, 0.0f);
+    h.uv = make_float2(h.p.x, h.p.y);
+    if (dot(h.n, r.d) > 0.0f) h.n = -h.n;
+    h.mat = s.material_id;
+    return true;
+}
+
+// primitives/heightfield.h:13-56: lattice hash, smoothed value noise, fBm.
+__device__ __forceinline__ float hf_hash(int xi, int zi, int seed) {
+    unsigned h = (unsigned)(xi * 374761393 + zi * 668265263 + seed * 974634097);
+    h = (h ^ (h >> 13)) * 1274126177u;
+    h = h ^ (h >> 16);
+    return float(h & 0xffffffu) / 16777216.0f;
+}
+__device__ __forceinline__ float hf_noise(float fx, float fz, int seed) {
+    int x0 = (int)floorf(fx), z0 = (int)floorf(fz);
+    float tx = fx - (float)x0, tz = fz - (float)z0;
+    tx = tx * tx * (3.0f - 2.0f * tx);
+    tz = tz * tz * (3.0f - 2.0f * tz);
+    float v00 = hf_hash(x0, z0, seed), v10 = hf_hash(x0 + 1, z0, seed);
+    float v01 = hf_hash(x0, z0 + 1, seed), v11 = hf_hash(x0 + 1, z0 + 1, seed);
+    float a = v00 + (v10 - v00) * tx, b = v01 + (v11 - v01) * tx;
+    return a + (b - a) * tz;
+}
+
+// primitives/heightfield.h:58-116: height above the tile base.
+__device__ __forceinline__ float hf_height(const HeightField& hf, float x, float z) {
+    float lx = (x - hf.center.x) / hf.size_x + 0.5f;
+    float lz = (z - hf.center.z) / hf.size_z + 0.5f;
+    if (lx < 0.0f || lx > 1.0f || lz < 0.0f || lz > 1.0f) return 0.0f;
+    if (hf.image) {
+        if (hf.img_w < 1 || hf.img_h < 1) return 0.0f;
+        float fu = lx * (float)(hf.img_w - 1), fv = lz * (float)(hf.img_h - 1);
+        int u0 = (int)fu, v0 = (int)fv;
+        int u1 = u0 < hf.img_w - 1 ? u0 + 1 : u0, v1 = v0 < hf.img_h - 1 ? v0 + 1 : v0;
+        float tx = fu - (float)u0, ty = fv - (float)v0;
+        float h00 = (float)hf.image[v0 * hf.img_w + u0] / 255.0f, h10 = (float)hf.image[v0 * hf.img_w + u1] / 255.0f;
+        float h01 = (float)hf.image[v1 * hf.img_w + u0] / 255.0f, h11 = (float)hf.image[v1 * hf.img_w + u1] / 255.0f;
+        float hh = h00 * (1.0f - tx) * (1.0f - ty) + h10 * tx * (1.0f - ty) + h01 * (1.0f - tx) * ty + h11 * tx * ty;
+        return hh * hf.height;
+    }
+    float fx = lx * hf.freq, fz = lz * hf.freq, amp = 0.5f, sum = 0.0f, nz = 0.0f;
+    for (int o = 0; o < hf.octaves; o++) {
+        sum += amp * hf_noise(fx, fz, hf.seed + o * 131);
+        nz += amp;
+        amp *= 0.5f;
+        fx *= 2.0f; fz *= 2.0f;
+    }
+    float t = sum / nz;
+    float detail = hf_noise(lx * 7.0f, lz * 7.0f, hf.seed + 7777) * 0.06f;
+    t = fminf(t + detail - 0.03f, 1.0f);
+    return t * hf.height;
+}
+
+// primitives/heightfield.h:121-183: march (diagonal/64 steps, <= 256) then
+// 10 bisection steps; finite-difference normal.
+__device__ __forceinline__ bool hf_test(const Ray& r, const HeightField& hf, Hit& h) {
+    const float3 lo = f3(hf.center.x - 0.5f * hf.size_x, hf.center.y, hf.center.z - 0.5f * hf.size_z);
+    const float3 hi = f3(hf.center.x + 0.5f * hf.size_x, hf.center.y + hf.height, hf.center.z + 0.5f * hf.size_z);
+    float ix = 1.0f / r.d.x, iy = 1.0f / r.d.y, iz = 1.0f / r.d.z;
+    float tx0 = (lo.x - r.o.x) * ix, tx1 = (hi.x - r.o.x) * ix;
+    float ty0 = (lo.y - r.o.y) * iy, ty1 = (hi.y - r.o.y) * iy;
+    float tz0 = (lo.z - r.o.z) * iz, tz1 = (hi.z - r.o.z) * iz;
+    if (tx0 > tx1) { float t = tx0; tx0 = tx1; tx1 = t; }
+    if (ty0 > ty1) { float t = ty0; ty0 = ty1; ty1 = t; }
+    if (tz0 > tz1) { float t = tz0; tz0 = tz1; tz1 = t; }
+    float t0 = fmaxf(fmaxf(tx0, ty0), tz0), t1 = fminf(fminf(tx1, ty1), tz1);
+    if (t1 < r.tmin || t0 > r.tmax || t1 < t0) return false;
+    t0 = fmaxf(t0, r.tmin);
+    t1 = fminf(t1, r.tmax);
+    const float diag = sqrtf(hf.size_x * hf.size_x + hf.size_z * hf.size_z);
+    const float step = fmaxf(diag / 64.0f, 1e-4f);
+    float t = t0;
+    bool inside = false;
+    for (int i = 0; i < 256; i++) {
+        float3 p = r.o + t * r.d;
+        bool below = p.y <= hf_height(hf, p.x, p.z) + hf.center.y;
+        if (below != inside) {
+            float a = t - step, b = t;
+            if (a < t0) a = t0;
+            for (int k = 0; k < 10; k++) {
+                float mid = 0.5f * (a + b);
+                float3 pm = r.o + mid * r.d;
+                if ((pm.y <= hf_height(hf, pm.x, pm.z) + hf.center.y) == below) b = mid; else a = mid;
+            }
+            float tt = 0.5f * (a + b);
+            float3 P = r.o + tt * r.d;
+            if (tt >= r.tmin && tt <= r.tmax) {
+                const float e = fmaxf(hf.size_x, hf.size_z) / 256.0f;
+                float hxp = hf_height(hf, P.x + e, P.z), hxm = hf_height(hf, P.x - e, P.z);
+                float hzp = hf_height(hf, P.x, P.z + e), hzm = hf_height(hf, P.x, P.z - e);
+                h.t = tt;
+                h.p = P;
+                h.n = normalize(f3(-(hxp - hxm) / (2.0f * e), 1.0f, -(hzp - hzm) / (2.0f * e)));
+                h.tan = f3(1.0f, 0.0f, 0.0f);
+                h.uv = make_float2(P.x, P.z);
+                if (dot(h.n, r.d) > 0.0f) h.n = -h.n;
+                h.mat = hf.material_id;
+                return true;
+            }
+            return false;
+        }
+        inside = below;
+        t += step;
+        if (t > t1) break;
+    }
+    return false;
+}
+
+}  // namespace dev
+}  // namespace sheen

@@ -1,0 +1,89 @@
+// scene.cuh -- device view of a resident scene, shared by every renderer form.
+//
+// All arrays live in HBM for the lifetime of a SheenDeviceScene.  The ABI
+// records (Material, Light, Object, ...) are uploaded unchanged; what the
+// traversal reads in its inner loops is repacked into 16-byte-aligned
+// records loaded with 128-bit loads:
+//   BvhNode   32 B  {lo.xyz, left}, {hi.xyz, right}   (plain form, one per
+//                   box, leaf: left = right = ~primitive, the reference
+//                   encoding of bvh.h:14-19)
+//   TriVerts  48 B  {v0.xyz, -}, {v1.xyz, -}, {v2.xyz, -} positions only;
+//                   normals/UVs stay in the 112-byte Triangle record that is
+//                   read once per shaded hit.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector_types.h>
+
+#include "sheen_c_api.h"
+
+namespace sheen {
+namespace dev {
+
+struct __align__(16) BvhNode {
+    float4 a;   // lo.xyz, left child (or ~prim)
+    float4 b;   // hi.xyz, right child (or ~prim)
+};
+
+struct PhotonMapView {
+    const float4* pos;      // xyz position, w unused        (stored by cell)
+    const float4* nrm;      // xyz normal
+    const float4* flux;     // xyz flux
+    const int* cell_start;  // [num_cells + 1]
+    const int* cell_count;  // [num_cells]
+    int num_cells;          // 2^18, or 0 when there is no map
+    float cell_size;
+};
+
+// Wide BVH of the wavefront form: 4 children with 8-bit boxes quantised in
+// a per-node frame (see bvh4.h for the encoding).
+struct __align__(16) QNode4 {
+    float4 origin_exp;      // origin.xyz, exponents packed in w (3 x int8 + child count)
+    uint4 child;            // child index / leaf (offset<<4 | count) per slot
+    uint4 qbox;             // 4 x {qlo.x, qhi.x, qlo.y, qhi.y}
+    uint2 qz;               // 4 x {qlo.z, qhi.z}
+    uint2 pad;
+};
+
+struct DevScene {
+    CameraData cam;
+
+    const Object* objects; int num_objects;  const BvhNode* sphere_bvh;
+    const SweepStrand* strands; const SweepPoint* sweep_points; int num_strands; const BvhNode* strand_bvh;
+    const Triangle* tris; const float4* tri_verts; int num_tris; const BvhNode* mesh_bvh;
+    const HeightField* hfs; int num_hfs; const BvhNode* hf_bvh;
+    const Superellipsoid* ses; int num_ses; const BvhNode* se_bvh;
+    const Lathe* lathes; const LathePoint* lathe_points; int num_lathes; const BvhNode* lathe_bvh;
+    const Prism* prisms; const PrismPoint* prism_points; int num_prisms; const BvhNode* prism_bvh;
+    const CSGNode* csg_nodes; int csg_root;
+    const Plane* planes; int num_planes;
+    const Material* materials; int num_materials;
+    const TextureRef* textures; int num_textures;
+    const Light* lights; int num_lights;
+    const Medium* media; int num_media;
+    PhotonMapView pmap;
+    float caustics;
+
+    // Wavefront form: triangles re-ordered into BVH4 leaf order.
+    const QNode4* mesh_qbvh;       // root at 0 (null when the scene has no triangles)
+    const float4* qtri;            // 3 float4 per triangle slot: v0 | e1 | e2, w of the first = original index
+    int num_qnodes;
+    int has_glass;                 // any material with transmission > 0
+};
+
+struct Ray {
+    float3 o, d;
+    float tmin, tmax;
+};
+
+// Closest hit: the reference's HitRecord fields (types.h:34-44).
+struct Hit {
+    float t;
+    int mat;
+    int obj;
+    float3 p, n, tan;
+    float2 uv;
+};
+
+}  // namespace dev
+}  // namespace sheen

@@ -1,0 +1,98 @@
+// engine.h -- internal interface between the C-ABI layer and the device code.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "sheen_c_api.h"
+#include "dev/scene.cuh"
+
+namespace sheen {
+
+void set_error(const char* msg);
+void set_errorf(const char* fmt, const char* a);
+
+// Host mirror of dev::BvhNode.
+struct HostNode {
+    float lo[3];
+    int left;
+    float hi[3];
+    int right;
+};
+static_assert(sizeof(HostNode) == 32, "BVH node is 32 bytes");
+
+// Median-split BVH with the reference's rules (bvh.h:71-576): object
+// median on the largest axis, one primitive per leaf (leaf = ~index in both
+// child slots).  `axis_from_centroids` selects the sphere/strand variant
+// (axis from the centroid extent) over the mesh/HF/SE/lathe/prism variant
+// (axis from the extent of the primitive boxes).
+void build_median_bvh(const std::vector<float>& lo, const std::vector<float>& hi,
+                      const std::vector<int>& prims, bool axis_from_centroids,
+                      std::vector<HostNode>& out);
+
+// Binned-SAH BVH4 over triangles with 8-bit child boxes (bvh4.cpp).
+struct QBvh {
+    std::vector<dev::QNode4> nodes;
+    std::vector<float4> tris;      // 3 float4 per triangle slot in leaf order
+    int leaf_size_max = 0;
+};
+void build_qbvh4(const Triangle* tris, int n, QBvh& out);
+
+// Result/accounting of one render call.
+struct RenderTally {
+    unsigned long long primary = 0, shadow = 0, secondary = 0, nodes = 0, prims = 0;
+};
+
+// A resident scene (behind SheenDeviceScene).
+struct DeviceScene {
+    int form = SHEEN_FORM_PLAIN;
+    int device = 0;
+    dev::DevScene view{};
+    void* arena = nullptr;                 // one allocation holding every array
+    size_t arena_bytes = 0;
+    std::vector<void*> extra;              // photon map buffers
+    size_t extra_bytes = 0;
+    unsigned long long* d_tally = nullptr; // 8 counters
+    double build_ms = 0.0, upload_ms = 0.0, photon_ms = 0.0;
+    int photons_stored = 0;
+    // Wavefront form state (queues sized for the last render).
+    struct Wave* wave = nullptr;
+};
+
+int scene_upload(const SheenScene* in, int form, DeviceScene** out);
+void scene_release(DeviceScene* s);
+
+// Pixel rectangle [x0, x1) x [y0, y1) of a W x H image; the output buffer
+// always holds the whole image (W*H float4), pixels outside are untouched.
+struct Region {
+    int x0, y0, x1, y1;
+};
+
+// Plain form: one thread per pixel.  Asynchronous on `stream`.
+cudaError_t launch_plain(const DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
+                         bool count_nodes);
+
+// Primary closest hits (object id, material id, t) per pixel sample.
+cudaError_t launch_primary_hits_plain(const DeviceScene& s, int W, int H, int ns, int* obj, int* mat, float* t,
+                                      cudaStream_t stream);
+cudaError_t launch_primary_hits_bvh4(const DeviceScene& s, int W, int H, int ns, int* obj, int* mat, float* t,
+                                     cudaStream_t stream);
+
+// Megakernel over the BVH4 mesh traversal (wavefront form's queries, one
+// thread per pixel); used by the wavefront form for scenes outside its
+// queue pipeline and as a measurement point.
+cudaError_t launch_mega_bvh4(const DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream);
+
+// Wavefront form.
+cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream);
+void wave_release(DeviceScene& s);
+
+// Photon pass on the device (emission + hash-grid build), called by
+// scene_upload when the scene asks for photons.
+int build_photon_map_device(DeviceScene& s, int per_light, float cell);
+
+double now_ms();
+
+}  // namespace sheen

@@ -1,0 +1,335 @@
+// upload.cu -- SheenScene (host arrays) -> resident DevScene in HBM.
+//
+// Does what the reference's sheen_render_scene does before its launch
+// (api/sheen_c_api.cu:92-266: copy arrays, build texture mips and the
+// per-class BVHs, patch height-map pointers) but into ONE device arena sized
+// up front (one cudaMalloc, one pinned staging buffer, one H2D copy), and
+// keeps it resident until the handle is released.  The wavefront form also
+// gets the SAH BVH4 with quantised child boxes over the triangles.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "engine.h"
+
+namespace sheen {
+
+double now_ms() {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+namespace {
+
+// Texture mip chain: 2x2 box filter with edge clamping and rounding, levels
+// stored back to back (the layout of scene.h:230-261 that tex_fetch walks).
+std::vector<uint8_t> build_mip_chain(const uint8_t* px, int w, int h, int& mips) {
+    std::vector<uint8_t> chain(px, px + (size_t)w * h * 3);
+    mips = 1;
+    if (w < 2 && h < 2) return chain;
+    int sw = w, sh = h;
+    size_t src = 0;
+    while (sw > 1 || sh > 1) {
+        const int nw = sw > 1 ? sw / 2 : 1, nh = sh > 1 ? sh / 2 : 1;
+        const size_t dst = chain.size();
+        chain.resize(dst + (size_t)nw * nh * 3);
+        for (int y = 0; y < nh; y++) {
+            const int y0 = std::min(2 * y, sh - 1), y1 = std::min(2 * y + 1, sh - 1);
+            for (int x = 0; x < nw; x++) {
+                const int x0 = std::min(2 * x, sw - 1), x1 = std::min(2 * x + 1, sw - 1);
+                for (int c = 0; c < 3; c++) {
+                    const int s = chain[src + ((size_t)y0 * sw + x0) * 3 + c] + chain[src + ((size_t)y0 * sw + x1) * 3 + c] +
+                                  chain[src + ((size_t)y1 * sw + x0) * 3 + c] + chain[src + ((size_t)y1 * sw + x1) * 3 + c];
+                    chain[dst + ((size_t)y * nw + x) * 3 + c] = (uint8_t)((s + 2) / 4);
+                }
+            }
+        }
+        src = dst;
+        sw = nw;
+        sh = nh;
+        mips++;
+    }
+    return chain;
+}
+
+// Arena layout builder: records (host source, size) pairs at 256-byte
+// aligned offsets, then copies everything with one staging buffer.
+struct Arena {
+    struct Item { const void* src; size_t bytes; size_t off; };
+    std::vector<Item> items;
+    size_t size = 0;
+    size_t add(const void* src, size_t bytes) {
+        size = (size + 255) & ~(size_t)255;
+        items.push_back({src, bytes, size});
+        size += bytes;
+        return size - bytes;
+    }
+};
+
+template <class T>
+void push_box(std::vector<float>& lo, std::vector<float>& hi, const T a[3], const T b[3]) {
+    for (int k = 0; k < 3; k++) { lo.push_back(a[k]); hi.push_back(b[k]); }
+}
+
+}  // namespace
+
+int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
+    *out = nullptr;
+    if (!in) { set_error("null scene"); return -1; }
+    if (form != SHEEN_FORM_PLAIN && form != SHEEN_FORM_WAVEFRONT) { set_error("unknown renderer form"); return -1; }
+    DeviceScene* s = new DeviceScene();
+    s->form = form;
+    cudaGetDevice(&s->device);
+    const double t0 = now_ms();
+
+    // ---- host-side derived data -------------------------------------
+    std::vector<float> lo, hi;
+    std::vector<int> prims;
+    std::vector<HostNode> sph_bvh, strand_bvh, mesh_bvh, hf_bvh, se_bvh, lathe_bvh, prism_bvh;
+
+    for (int i = 0; i < in->num_objects; i++) {   // bvh.h:24-35 (type 0 only)
+        const Object& o = in->objects[i];
+        float a[3] = {0, 0, 0}, b[3] = {0, 0, 0};
+        if (o.type == 0) {
+            a[0] = o.param1.x - o.param2; a[1] = o.param1.y - o.param2; a[2] = o.param1.z - o.param2;
+            b[0] = o.param1.x + o.param2; b[1] = o.param1.y + o.param2; b[2] = o.param1.z + o.param2;
+            prims.push_back(i);
+        }
+        push_box(lo, hi, a, b);
+    }
+    build_median_bvh(lo, hi, prims, true, sph_bvh);
+
+    lo.clear(); hi.clear(); prims.clear();
+    for (int i = 0; i < in->num_sweep_strands; i++) {   // bvh.h:40-62
+        const SweepStrand& st = in->sweep_strands[i];
+        float a[3] = {1e10f, 1e10f, 1e10f}, b[3] = {-1e10f, -1e10f, -1e10f};
+        for (int k = 0; k < st.point_count; k++) {
+            const SweepPoint& p = in->sweep_points[st.point_offset + k];
+            a[0] = fminf(a[0], p.position.x - p.radius); a[1] = fminf(a[1], p.position.y - p.radius);
+            a[2] = fminf(a[2], p.position.z - p.radius);
+            b[0] = fmaxf(b[0], p.position.x + p.radius); b[1] = fmaxf(b[1], p.position.y + p.radius);
+            b[2] = fmaxf(b[2], p.position.z + p.radius);
+        }
+        push_box(lo, hi, a, b);
+        prims.push_back(i);
+    }
+    build_median_bvh(lo, hi, prims, true, strand_bvh);
+
+    lo.clear(); hi.clear(); prims.clear();
+    std::vector<float4> tri_verts((size_t)in->num_triangles * 3);
+    lo.reserve((size_t)in->num_triangles * 3);
+    hi.reserve((size_t)in->num_triangles * 3);
+    for (int i = 0; i < in->num_triangles; i++) {   // bvh.h:235-242
+        const Triangle& t = in->triangles[i];
+        float a[3] = {fminf(t.v0.x, fminf(t.v1.x, t.v2.x)), fminf(t.v0.y, fminf(t.v1.y, t.v2.y)),
+                      fminf(t.v0.z, fminf(t.v1.z, t.v2.z))};
+        float b[3] = {fmaxf(t.v0.x, fmaxf(t.v1.x, t.v2.x)), fmaxf(t.v0.y, fmaxf(t.v1.y, t.v2.y)),
+                      fmaxf(t.v0.z, fmaxf(t.v1.z, t.v2.z))};
+        push_box(lo, hi, a, b);
+        prims.push_back(i);
+        tri_verts[3 * (size_t)i] = make_float4(t.v0.x, t.v0.y, t.v0.z, 0.0f);
+        tri_verts[3 * (size_t)i + 1] = make_float4(t.v1.x, t.v1.y, t.v1.z, 0.0f);
+        tri_verts[3 * (size_t)i + 2] = make_float4(t.v2.x, t.v2.y, t.v2.z, 0.0f);
+    }
+    build_median_bvh(lo, hi, prims, false, mesh_bvh);
+
+    lo.clear(); hi.clear(); prims.clear();
+    for (int i = 0; i < in->num_heightfields; i++) {   // bvh.h:304-309
+        const HeightField& f = in->heightfields[i];
+        float a[3] = {f.center.x - 0.5f * f.size_x, f.center.y, f.center.z - 0.5f * f.size_z};
+        float b[3] = {f.center.x + 0.5f * f.size_x, f.center.y + f.height, f.center.z + 0.5f * f.size_z};
+        push_box(lo, hi, a, b);
+        prims.push_back(i);
+    }
+    build_median_bvh(lo, hi, prims, false, hf_bvh);
+
+    lo.clear(); hi.clear(); prims.clear();
+    for (int i = 0; i < in->num_superellipsoids; i++) {   // superellipsoid.h:31-36
+        const Superellipsoid& e = in->superellipsoids[i];
+        float a[3] = {e.center.x - e.a, e.center.y - e.b, e.center.z - e.c};
+        float b[3] = {e.center.x + e.a, e.center.y + e.b, e.center.z + e.c};
+        push_box(lo, hi, a, b);
+        prims.push_back(i);
+    }
+    build_median_bvh(lo, hi, prims, false, se_bvh);
+
+    lo.clear(); hi.clear(); prims.clear();
+    for (int i = 0; i < in->num_lathes; i++) {   // bvh.h:394-407 (x/z start at +-1e30 about the centre)
+        const Lathe& l = in->lathes[i];
+        float a[3] = {l.center.x - 1e30f, 1e30f, l.center.z - 1e30f};
+        float b[3] = {l.center.x + 1e30f, -1e30f, l.center.z + 1e30f};
+        for (int k = 0; k < l.point_count; k++) {
+            const LathePoint& p = in->lathe_points[l.point_offset + k];
+            if (p.radius < 0.0f) continue;
+            a[0] = fminf(a[0], l.center.x - p.radius); a[1] = fminf(a[1], l.center.y + p.y - p.radius);
+            a[2] = fminf(a[2], l.center.z - p.radius);
+            b[0] = fmaxf(b[0], l.center.x + p.radius); b[1] = fmaxf(b[1], l.center.y + p.y + p.radius);
+            b[2] = fmaxf(b[2], l.center.z + p.radius);
+        }
+        if (a[0] > b[0]) { for (int k = 0; k < 3; k++) a[k] = b[k] = 0.0f; }
+        push_box(lo, hi, a, b);
+        prims.push_back(i);
+    }
+    build_median_bvh(lo, hi, prims, false, lathe_bvh);
+
+    lo.clear(); hi.clear(); prims.clear();
+    for (int i = 0; i < in->num_prisms; i++) {   // bvh.h:321-332
+        const Prism& p = in->prisms[i];
+        float a[3] = {1e30f, p.center.y + p.y_min, 1e30f}, b[3] = {-1e30f, p.center.y + p.y_max, -1e30f};
+        for (int k = 0; k < p.point_count; k++) {
+            const PrismPoint& q = in->prism_points[p.point_offset + k];
+            a[0] = fminf(a[0], p.center.x + q.x); b[0] = fmaxf(b[0], p.center.x + q.x);
+            a[2] = fminf(a[2], p.center.z + q.z); b[2] = fmaxf(b[2], p.center.z + q.z);
+        }
+        if (a[0] > b[0]) { a[0] = b[0] = 0.0f; a[1] = b[1] = p.center.y; a[2] = b[2] = 0.0f; }
+        push_box(lo, hi, a, b);
+        prims.push_back(i);
+    }
+    build_median_bvh(lo, hi, prims, false, prism_bvh);
+
+    QBvh qb;
+    if (form == SHEEN_FORM_WAVEFRONT && in->num_triangles > 0) build_qbvh4(in->triangles, in->num_triangles, qb);
+
+    // Textures with mips; TextureRef pixel pointers are patched after the
+    // arena address is known.
+    std::vector<std::vector<uint8_t>> chains((size_t)std::max(in->num_textures, 0));
+    std::vector<TextureRef> texrefs((size_t)std::max(in->num_textures, 0));
+    for (int i = 0; i < in->num_textures; i++) {
+        std::memset(&texrefs[(size_t)i], 0, sizeof(TextureRef));
+        const int w = in->texture_widths ? in->texture_widths[i] : 0;
+        const int h = in->texture_heights ? in->texture_heights[i] : 0;
+        if (!in->texture_pixels || !in->texture_pixels[i] || w <= 0 || h <= 0) continue;
+        int mips = 1;
+        chains[(size_t)i] = build_mip_chain(in->texture_pixels[i], w, h, mips);
+        texrefs[(size_t)i].width = w;
+        texrefs[(size_t)i].height = h;
+        texrefs[(size_t)i].mips = mips;
+    }
+    std::vector<HeightField> hfs(in->heightfields, in->heightfields + std::max(in->num_heightfields, 0));
+    bool has_glass = false;
+    for (int i = 0; i < in->num_materials; i++) has_glass |= in->materials[i].transmission > 0.0f;
+    const double t1 = now_ms();
+
+    // ---- arena layout -------------------------------------------------
+    Arena ar;
+    auto add_vec = [&](const auto& v) -> size_t {
+        return v.empty() ? (size_t)-1 : ar.add(v.data(), v.size() * sizeof(v[0]));
+    };
+    auto add_raw = [&](const void* p, int n, size_t elem) -> size_t {
+        return (p && n > 0) ? ar.add(p, (size_t)n * elem) : (size_t)-1;
+    };
+    const size_t o_obj = add_raw(in->objects, in->num_objects, sizeof(Object));
+    const size_t o_sphb = add_vec(sph_bvh);
+    const size_t o_str = add_raw(in->sweep_strands, in->num_sweep_strands, sizeof(SweepStrand));
+    const size_t o_spt = add_raw(in->sweep_points, in->num_sweep_points, sizeof(SweepPoint));
+    const size_t o_strb = add_vec(strand_bvh);
+    const size_t o_tri = add_raw(in->triangles, in->num_triangles, sizeof(Triangle));
+    const size_t o_trv = add_vec(tri_verts);
+    const size_t o_meshb = add_vec(mesh_bvh);
+    const size_t o_hf = add_vec(hfs);
+    const size_t o_hfb = add_vec(hf_bvh);
+    const size_t o_se = add_raw(in->superellipsoids, in->num_superellipsoids, sizeof(Superellipsoid));
+    const size_t o_seb = add_vec(se_bvh);
+    const size_t o_lat = add_raw(in->lathes, in->num_lathes, sizeof(Lathe));
+    const size_t o_lpt = add_raw(in->lathe_points, in->num_lathe_points, sizeof(LathePoint));
+    const size_t o_latb = add_vec(lathe_bvh);
+    const size_t o_pri = add_raw(in->prisms, in->num_prisms, sizeof(Prism));
+    const size_t o_ppt = add_raw(in->prism_points, in->num_prism_points, sizeof(PrismPoint));
+    const size_t o_prib = add_vec(prism_bvh);
+    const size_t o_csg = add_raw(in->csg_nodes, in->num_csg_nodes, sizeof(CSGNode));
+    const size_t o_pla = add_raw(in->planes, in->num_planes, sizeof(Plane));
+    const size_t o_mat = add_raw(in->materials, in->num_materials, sizeof(Material));
+    const size_t o_lig = add_raw(in->lights, in->num_lights, sizeof(Light));
+    const size_t o_med = add_raw(in->media, in->num_media, sizeof(Medium));
+    const size_t o_qn = add_vec(qb.nodes);
+    const size_t o_qt = add_vec(qb.tris);
+    std::vector<size_t> o_chain(chains.size(), (size_t)-1);
+    for (size_t i = 0; i < chains.size(); i++) o_chain[i] = add_vec(chains[i]);
+    std::vector<size_t> o_img(hfs.size(), (size_t)-1);
+    for (size_t i = 0; i < hfs.size(); i++)
+        if (hfs[i].image && hfs[i].img_w > 0 && hfs[i].img_h > 0)
+            o_img[i] = ar.add(hfs[i].image, (size_t)hfs[i].img_w * hfs[i].img_h);
+    const size_t o_tex = texrefs.empty() ? (size_t)-1 : ar.add(nullptr, texrefs.size() * sizeof(TextureRef));
+    const size_t o_tally = ar.add(nullptr, 8 * sizeof(unsigned long long));
+    ar.size = (ar.size + 255) & ~(size_t)255;
+
+    cudaError_t e = cudaMalloc(&s->arena, ar.size);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); delete s; return -1; }
+    s->arena_bytes = ar.size;
+    char* base = (char*)s->arena;
+    auto dptr = [&](size_t off) -> void* { return off == (size_t)-1 ? nullptr : (void*)(base + off); };
+
+    // Patch device pointers into the host copies that reference other arrays.
+    for (size_t i = 0; i < texrefs.size(); i++) texrefs[i].pixels = (const unsigned char*)dptr(o_chain[i]);
+    for (size_t i = 0; i < hfs.size(); i++) hfs[i].image = (const unsigned char*)dptr(o_img[i]);
+    for (auto& it : ar.items) {
+        if (it.off == o_tex) it.src = texrefs.data();
+        if (it.off == o_hf) it.src = hfs.data();
+    }
+
+    // One pinned staging buffer, one copy.
+    void* stage = nullptr;
+    e = cudaMallocHost(&stage, ar.size);
+    if (e != cudaSuccess) { cudaFree(s->arena); set_error(cudaGetErrorString(e)); delete s; return -1; }
+    std::memset(stage, 0, ar.size);
+    for (const auto& it : ar.items)
+        if (it.src) std::memcpy((char*)stage + it.off, it.src, it.bytes);
+    e = cudaMemcpy(s->arena, stage, ar.size, cudaMemcpyHostToDevice);
+    cudaFreeHost(stage);
+    if (e != cudaSuccess) { cudaFree(s->arena); set_error(cudaGetErrorString(e)); delete s; return -1; }
+    const double t2 = now_ms();
+
+    dev::DevScene& v = s->view;
+    std::memset(&v, 0, sizeof(v));
+    v.cam = in->camera;
+    v.objects = (const Object*)dptr(o_obj); v.num_objects = in->num_objects; v.sphere_bvh = (const dev::BvhNode*)dptr(o_sphb);
+    v.strands = (const SweepStrand*)dptr(o_str); v.sweep_points = (const SweepPoint*)dptr(o_spt);
+    v.num_strands = in->num_sweep_strands; v.strand_bvh = (const dev::BvhNode*)dptr(o_strb);
+    v.tris = (const Triangle*)dptr(o_tri); v.tri_verts = (const float4*)dptr(o_trv); v.num_tris = in->num_triangles;
+    v.mesh_bvh = (const dev::BvhNode*)dptr(o_meshb);
+    v.hfs = (const HeightField*)dptr(o_hf); v.num_hfs = in->num_heightfields; v.hf_bvh = (const dev::BvhNode*)dptr(o_hfb);
+    v.ses = (const Superellipsoid*)dptr(o_se); v.num_ses = in->num_superellipsoids; v.se_bvh = (const dev::BvhNode*)dptr(o_seb);
+    v.lathes = (const Lathe*)dptr(o_lat); v.lathe_points = (const LathePoint*)dptr(o_lpt); v.num_lathes = in->num_lathes;
+    v.lathe_bvh = (const dev::BvhNode*)dptr(o_latb);
+    v.prisms = (const Prism*)dptr(o_pri); v.prism_points = (const PrismPoint*)dptr(o_ppt); v.num_prisms = in->num_prisms;
+    v.prism_bvh = (const dev::BvhNode*)dptr(o_prib);
+    v.csg_nodes = (const CSGNode*)dptr(o_csg);
+    v.csg_root = (in->csg_nodes && in->num_csg_nodes > 0 && in->csg_root >= 0 && in->csg_root < in->num_csg_nodes)
+                     ? in->csg_root : -1;
+    v.planes = (const Plane*)dptr(o_pla); v.num_planes = in->num_planes;
+    v.materials = (const Material*)dptr(o_mat); v.num_materials = in->num_materials;
+    v.textures = (const TextureRef*)dptr(o_tex); v.num_textures = in->num_textures;
+    v.lights = (const Light*)dptr(o_lig); v.num_lights = in->num_lights;
+    v.media = (const Medium*)dptr(o_med); v.num_media = in->num_media;
+    v.caustics = in->caustics;
+    v.mesh_qbvh = (const dev::QNode4*)dptr(o_qn);
+    v.qtri = (const float4*)dptr(o_qt);
+    v.num_qnodes = (int)qb.nodes.size();
+    v.has_glass = has_glass ? 1 : 0;
+    s->d_tally = (unsigned long long*)dptr(o_tally);
+    s->build_ms = t1 - t0;
+    s->upload_ms = t2 - t1;
+
+    if (in->photons > 0 && in->num_lights > 0) {
+        const double tp = now_ms();
+        if (build_photon_map_device(*s, in->photons, in->photon_cell > 0.0f ? in->photon_cell : 0.25f) != 0) {
+            scene_release(s);
+            return -1;
+        }
+        s->photon_ms = now_ms() - tp;
+    }
+    *out = s;
+    return 0;
+}
+
+void scene_release(DeviceScene* s) {
+    if (!s) return;
+    wave_release(*s);
+    for (void* p : s->extra) cudaFree(p);
+    cudaFree(s->arena);
+    delete s;
+}
+
+}  // namespace sheen
