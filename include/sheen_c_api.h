@@ -186,6 +186,12 @@ int sheen_scene_render_host(SheenDeviceScene scene, int width, int height,
 int sheen_scene_primary_hits(SheenDeviceScene scene, int width, int height, int aa_samples,
                              int* obj_id_host, int* mat_id_host, float* t_host);
 
+/* Host-side structural check of the wavefront form's triangle BVH (4-wide,
+ * 8-bit child boxes) for a scene: every triangle in exactly one leaf, every
+ * decoded child box containing all triangles below it.  Returns the tree
+ * depth, or a negative code on a violation.  No device work. */
+int sheen_selfcheck_bvh4(const SheenScene* scene);
+
 /* Owned host scenes: the .sheen loader and the synthetic generators return
  * one.  sheen_owned_view points into storage owned by the handle. */
 typedef struct SheenOwnedScene_* SheenOwnedScene;

@@ -72,7 +72,7 @@ int render_device(sheen::DeviceScene& s, int W, int H, int aa, sheen::Region rg,
     if (s.form == SHEEN_FORM_PLAIN)
         e = sheen::launch_plain(s, W, H, aa, rg, out, stream, (flags & SHEEN_RENDER_COUNT_RAYS) != 0);
     else
-        e = sheen::launch_wavefront(s, W, H, aa, rg, out, stream);
+        e = sheen::launch_wavefront(s, W, H, aa, rg, out, stream, (flags & SHEEN_RENDER_COUNT_RAYS) != 0);
     if (e != cudaSuccess) return fail_cuda(e);
     if (want_stats) {
         cudaEventRecord(ev1, stream);

@@ -1,0 +1,374 @@
+// bvh4.cpp -- triangle BVH of the wavefront form: binned SAH, collapsed to
+// 4-wide nodes whose child boxes are stored as 8-bit integers in a per-node
+// frame, rounded outward so that the decoded box always contains the
+// original one.
+//
+// Node (dev::QNode4, 64 bytes, four 128-bit loads):
+//   origin_exp.xyz  frame origin (the node's box minimum)
+//   origin_exp.w    bits 0-7 / 8-15 / 16-23: biased exponents ex, ey, ez of
+//                   the per-axis scale 2^(e-127); bits 24-31: child count
+//   child[i]        inner child: node index; leaf: 0x80000000 |
+//                   (first triangle << 3) | (count - 1), count <= 8
+//   qbox.x..w       byte i of each word: child i's qlo.x, qhi.x, qlo.y, qhi.y
+//   qz.x, qz.y      byte i: child i's qlo.z, qhi.z
+// A child box decodes as lo = fmaf(qlo, 2^e, origin), hi = fmaf(qhi, 2^e,
+// origin).  The builder computes the same fmaf in float and moves each
+// integer outward until the decoded box contains the exact child box.
+//
+// Triangles are stored in leaf order as three float4: {v0, original index},
+// {e1 = v1 - v0, 0}, {e2 = v2 - v0, 0}; e1/e2 are the same float
+// subtractions the reference's Moller-Trumbore performs per test
+// (primitives/triangle.h:9-10), so the test's results are unchanged.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "engine.h"
+
+namespace sheen {
+
+namespace {
+
+struct Box {
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+    float hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    void grow(const Box& b) {
+        for (int k = 0; k < 3; k++) { lo[k] = std::min(lo[k], b.lo[k]); hi[k] = std::max(hi[k], b.hi[k]); }
+    }
+    void grow(const float p[3]) {
+        for (int k = 0; k < 3; k++) { lo[k] = std::min(lo[k], p[k]); hi[k] = std::max(hi[k], p[k]); }
+    }
+    float area() const {
+        float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+        if (dx < 0.0f) return 0.0f;
+        return 2.0f * (dx * dy + dy * dz + dz * dx);
+    }
+};
+
+struct BNode {
+    Box box;
+    int left = -1, right = -1;   // inner
+    int first = 0, count = 0;    // leaf when count > 0
+};
+
+constexpr int kBins = 16;
+constexpr int kMaxLeaf = 8;
+
+struct SahBuilder {
+    std::vector<Box> tri_box;
+    std::vector<float> cen;   // 3 per triangle
+    std::vector<int> idx;
+
+    // Builds the subtree of idx[first, first+n) into `out`; returns its root.
+    int build(int first, int n, int depth, std::vector<BNode>& out) {
+        const int me = (int)out.size();
+        out.emplace_back();
+        Box b, cb;
+        for (int i = first; i < first + n; i++) {
+            b.grow(tri_box[(size_t)idx[(size_t)i]]);
+            cb.grow(&cen[3 * (size_t)idx[(size_t)i]]);
+        }
+        out[(size_t)me].box = b;
+        if (n <= 2) { out[(size_t)me].first = first; out[(size_t)me].count = n; return me; }
+        // Binned SAH over the centroid box.
+        float best_cost = FLT_MAX;
+        int best_axis = -1, best_split = -1;
+        for (int axis = 0; axis < 3; axis++) {
+            const float ext = cb.hi[axis] - cb.lo[axis];
+            if (!(ext > 0.0f)) continue;
+            Box bins[kBins];
+            int cnt[kBins] = {0};
+            const float k = (float)kBins / ext;
+            for (int i = first; i < first + n; i++) {
+                const int t = idx[(size_t)i];
+                int bi = (int)((cen[3 * (size_t)t + axis] - cb.lo[axis]) * k);
+                bi = std::min(std::max(bi, 0), kBins - 1);
+                cnt[bi]++;
+                bins[bi].grow(tri_box[(size_t)t]);
+            }
+            float right_area[kBins];
+            int right_cnt[kBins];
+            Box acc;
+            int c = 0;
+            for (int i = kBins - 1; i > 0; i--) {
+                acc.grow(bins[i]);
+                c += cnt[i];
+                right_area[i] = acc.area();
+                right_cnt[i] = c;
+            }
+            Box lacc;
+            int lc = 0;
+            for (int i = 0; i < kBins - 1; i++) {
+                lacc.grow(bins[i]);
+                lc += cnt[i];
+                if (lc == 0 || right_cnt[i + 1] == 0) continue;
+                const float cost = lacc.area() * (float)lc + right_area[i + 1] * (float)right_cnt[i + 1];
+                if (cost < best_cost) { best_cost = cost; best_axis = axis; best_split = i; }
+            }
+        }
+        const float leaf_cost = b.area() * (float)n;
+        const float parent_area = b.area();
+        // cost model: traversal 1 (scaled by the parent area), intersection 1 per triangle
+        if (best_axis < 0 || (n <= kMaxLeaf && leaf_cost <= parent_area + best_cost)) {
+            if (n <= kMaxLeaf) { out[(size_t)me].first = first; out[(size_t)me].count = n; return me; }
+        }
+        int mid;
+        if (best_axis >= 0) {
+            const int axis = best_axis;
+            const float k = (float)kBins / (cb.hi[axis] - cb.lo[axis]);
+            const float lo = cb.lo[axis];
+            auto it = std::partition(idx.begin() + first, idx.begin() + first + n, [&](int t) {
+                int bi = (int)((cen[3 * (size_t)t + axis] - lo) * k);
+                bi = std::min(std::max(bi, 0), kBins - 1);
+                return bi <= best_split;
+            });
+            mid = (int)(it - idx.begin());
+        } else {
+            mid = first + n / 2;   // all centroids coincide: split the list
+        }
+        if (mid == first || mid == first + n) mid = first + n / 2;
+        int l, r;
+        if (depth < 5 && n > 50000) {
+            std::vector<BNode> right_nodes;
+            int rroot = 0;
+            std::thread worker([&] { rroot = build(mid, first + n - mid, depth + 1, right_nodes); });
+            l = build(first, mid - first, depth + 1, out);
+            worker.join();
+            const int off = (int)out.size();
+            for (BNode rn : right_nodes) {
+                if (rn.count == 0) { rn.left += off; rn.right += off; }
+                out.push_back(rn);
+            }
+            r = rroot + off;
+        } else {
+            l = build(first, mid - first, depth + 1, out);
+            r = build(mid, first + n - mid, depth + 1, out);
+        }
+        out[(size_t)me].left = l;
+        out[(size_t)me].right = r;
+        return me;
+    }
+};
+
+// Per-axis quantisation of a child interval [a, b] inside a frame starting
+// at `origin` with scale 2^(e-127): outward rounding checked with the
+// device's own decode (fmaf).
+void quantize_axis(float origin, float scale, float a, float b, uint8_t& qlo, uint8_t& qhi) {
+    double fl = std::floor(((double)a - origin) / scale);
+    double fh = std::ceil(((double)b - origin) / scale);
+    int lo = (int)std::max(0.0, std::min(255.0, fl));
+    int hi = (int)std::max(0.0, std::min(255.0, fh));
+    while (lo > 0 && std::fmaf((float)lo, scale, origin) > a) lo--;
+    while (hi < 255 && std::fmaf((float)hi, scale, origin) < b) hi++;
+    qlo = (uint8_t)lo;
+    qhi = (uint8_t)hi;
+}
+
+}  // namespace
+
+void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out) {
+    out.nodes.clear();
+    out.tris.clear();
+    out.max_depth = 0;
+    const int n = (int)subset.size();
+    if (n <= 0) return;
+    SahBuilder sb;
+    sb.tri_box.resize((size_t)n);
+    sb.cen.resize(3 * (size_t)n);
+    sb.idx.resize((size_t)n);
+    for (int i = 0; i < n; i++) {
+        const Triangle& t = tris[subset[(size_t)i]];
+        const float v[3][3] = {{t.v0.x, t.v0.y, t.v0.z}, {t.v1.x, t.v1.y, t.v1.z}, {t.v2.x, t.v2.y, t.v2.z}};
+        Box b;
+        for (int k = 0; k < 3; k++) b.grow(v[k]);
+        sb.tri_box[(size_t)i] = b;
+        for (int k = 0; k < 3; k++) sb.cen[3 * (size_t)i + k] = 0.5f * (b.lo[k] + b.hi[k]);
+        sb.idx[(size_t)i] = i;
+    }
+    std::vector<BNode> bn;
+    bn.reserve((size_t)n);
+    const int root = sb.build(0, n, 0, bn);
+
+    // Leaf triangles in leaf order.
+    out.tris.resize(3 * (size_t)n);
+    for (int i = 0; i < n; i++) {
+        const int orig = subset[(size_t)sb.idx[(size_t)i]];
+        const Triangle& t = tris[orig];
+        float fi;
+        std::memcpy(&fi, &orig, 4);
+        out.tris[3 * (size_t)i] = make_float4(t.v0.x, t.v0.y, t.v0.z, fi);
+        out.tris[3 * (size_t)i + 1] = make_float4(t.v1.x - t.v0.x, t.v1.y - t.v0.y, t.v1.z - t.v0.z, 0.0f);
+        out.tris[3 * (size_t)i + 2] = make_float4(t.v2.x - t.v0.x, t.v2.y - t.v0.y, t.v2.z - t.v0.z, 0.0f);
+    }
+
+    // Collapse to 4-wide nodes, breadth first from the root.
+    struct Pending { int bnode; int slot; };
+    std::vector<Pending> queue;
+    std::vector<int> ndepth;
+    int cur_depth = 0;
+    auto emit = [&](int b) {
+        const int id = (int)out.nodes.size();
+        ndepth.push_back(cur_depth + 1);
+        out.max_depth = std::max(out.max_depth, cur_depth + 1);
+        out.nodes.emplace_back();
+        std::memset(&out.nodes.back(), 0, sizeof(dev::QNode4));
+        queue.push_back({b, id});
+        return id;
+    };
+    if (bn[(size_t)root].count > 0) {
+        // A single leaf: wrap it in one node with one child.
+        const int id = emit(root);
+        queue.clear();
+        dev::QNode4& q = out.nodes[(size_t)id];
+        (void)q;
+        queue.push_back({-1 - root, id});
+    } else {
+        emit(root);
+    }
+    for (size_t qi = 0; qi < queue.size(); qi++) {
+        const int b = queue[qi].bnode;
+        const int id = queue[qi].slot;
+        cur_depth = ndepth[(size_t)id];
+        std::vector<int> kids;
+        if (b < 0) {
+            kids.push_back(-1 - b);
+        } else {
+            kids = {bn[(size_t)b].left, bn[(size_t)b].right};
+            while (kids.size() < 4) {
+                int pick = -1;
+                float best = -1.0f;
+                for (size_t k = 0; k < kids.size(); k++) {
+                    const BNode& c = bn[(size_t)kids[k]];
+                    if (c.count == 0 && c.box.area() > best) { best = c.box.area(); pick = (int)k; }
+                }
+                if (pick < 0) break;
+                const BNode c = bn[(size_t)kids[(size_t)pick]];
+                kids[(size_t)pick] = c.left;
+                kids.push_back(c.right);
+            }
+        }
+        Box nb;
+        for (int k : kids) nb.grow(bn[(size_t)k].box);
+        float origin[3], scale[3];
+        int ebits[3];
+        for (int a = 0; a < 3; a++) {
+            origin[a] = nb.lo[a];
+            const double ext = (double)nb.hi[a] - (double)nb.lo[a];
+            int e = ext > 0.0 ? (int)std::ceil(std::log2(ext / 254.0)) : -20;
+            e = std::max(-100, std::min(100, e));
+            // make sure the whole extent fits below q = 255 after outward rounding
+            while (std::fmaf(255.0f, std::ldexp(1.0f, e), origin[a]) < nb.hi[a] && e < 100) e++;
+            scale[a] = std::ldexp(1.0f, e);
+            ebits[a] = e + 127;
+        }
+        uint32_t packed = (uint32_t)ebits[0] | ((uint32_t)ebits[1] << 8) | ((uint32_t)ebits[2] << 16) |
+                          ((uint32_t)kids.size() << 24);
+        float pw;
+        std::memcpy(&pw, &packed, 4);
+        uint8_t q[6][4] = {{0}};
+        uint32_t child[4] = {0, 0, 0, 0};
+        for (size_t k = 0; k < kids.size(); k++) {
+            const BNode& c = bn[(size_t)kids[k]];
+            for (int a = 0; a < 3; a++)
+                quantize_axis(origin[a], scale[a], c.box.lo[a], c.box.hi[a], q[2 * a][k], q[2 * a + 1][k]);
+            if (c.count > 0) {
+                child[k] = 0x80000000u | ((uint32_t)c.first << 3) | (uint32_t)(c.count - 1);
+            } else {
+                child[k] = (uint32_t)emit(kids[k]);
+            }
+        }
+        dev::QNode4& node = out.nodes[(size_t)id];
+        node.origin_exp = make_float4(origin[0], origin[1], origin[2], pw);
+        node.child = make_uint4(child[0], child[1], child[2], child[3]);
+        auto word = [&](int row) {
+            return (uint32_t)q[row][0] | ((uint32_t)q[row][1] << 8) | ((uint32_t)q[row][2] << 16) |
+                   ((uint32_t)q[row][3] << 24);
+        };
+        node.qbox = make_uint4(word(0), word(1), word(2), word(3));
+        node.qz = make_uint2(word(4), word(5));
+        node.pad = make_uint2(0, 0);
+    }
+    out.leaf_size_max = kMaxLeaf;
+}
+
+// Structural check of a BVH4 (host only): every triangle slot is referenced
+// by exactly one leaf, every decoded child box contains the boxes of all
+// triangles below it, and the depth fits the traversal stack.  Returns 0 or
+// a negative code; `depth` gets the tree depth.
+int check_qbvh4(const QBvh& q, int& depth) {
+    depth = 0;
+    const size_t ntri = q.tris.size() / 3;
+    if (q.nodes.empty()) return ntri == 0 ? 0 : -1;
+    std::vector<int> seen(ntri, 0);
+    struct Item { uint32_t e; int d; Box bound; };
+    std::vector<Item> st;
+    Box root_bound;
+    for (int k = 0; k < 3; k++) { root_bound.lo[k] = -FLT_MAX; root_bound.hi[k] = FLT_MAX; }
+    st.push_back({0u, 1, root_bound});
+    while (!st.empty()) {
+        Item it = st.back();
+        st.pop_back();
+        depth = std::max(depth, it.d);
+        if (it.e & 0x80000000u) {
+            const uint32_t first = (it.e & 0x7fffffffu) >> 3, count = (it.e & 7u) + 1;
+            for (uint32_t k = 0; k < count; k++) {
+                const size_t slot = first + k;
+                if (slot >= ntri) return -2;
+                seen[slot]++;
+                const float4 a = q.tris[3 * slot], b = q.tris[3 * slot + 1], c = q.tris[3 * slot + 2];
+                const float v[3][3] = {{a.x, a.y, a.z}, {a.x + b.x, a.y + b.y, a.z + b.z}, {a.x + c.x, a.y + c.y, a.z + c.z}};
+                for (int p = 0; p < 3; p++)
+                    for (int ax = 0; ax < 3; ax++) {
+                        // v1 = v0 + e1 may round by an ulp: allow it
+                        const float tol = 1e-6f * (std::fabs(v[p][ax]) + 1.0f);
+                        if (v[p][ax] < it.bound.lo[ax] - tol || v[p][ax] > it.bound.hi[ax] + tol) return -3;
+                    }
+            }
+            continue;
+        }
+        if (it.e >= q.nodes.size()) return -4;
+        const dev::QNode4& n = q.nodes[it.e];
+        uint32_t packed;
+        std::memcpy(&packed, &n.origin_exp.w, 4);
+        const int count = (int)(packed >> 24);
+        if (count < 1 || count > 4) return -5;
+        const float org[3] = {n.origin_exp.x, n.origin_exp.y, n.origin_exp.z};
+        float s[3];
+        for (int a = 0; a < 3; a++) {
+            uint32_t bits = ((packed >> (8 * a)) & 0xffu) << 23;
+            std::memcpy(&s[a], &bits, 4);
+        }
+        const uint32_t words[6] = {n.qbox.x, n.qbox.y, n.qbox.z, n.qbox.w, n.qz.x, n.qz.y};
+        const uint32_t ch[4] = {n.child.x, n.child.y, n.child.z, n.child.w};
+        for (int i = 0; i < count; i++) {
+            Box b;
+            for (int a = 0; a < 3; a++) {
+                b.lo[a] = std::fmaf((float)((words[2 * a] >> (8 * i)) & 0xffu), s[a], org[a]);
+                b.hi[a] = std::fmaf((float)((words[2 * a + 1] >> (8 * i)) & 0xffu), s[a], org[a]);
+            }
+            st.push_back({ch[i], it.d + 1, b});
+        }
+    }
+    for (int v : seen)
+        if (v != 1) return -6;
+    return 0;
+}
+
+}  // namespace sheen
+
+// Host-side self check of the wavefront form's triangle BVH for a scene:
+// builds it and runs check_qbvh4.  Returns the tree depth (>= 0) or a
+// negative error code.  No device work.
+extern "C" int sheen_selfcheck_bvh4(const SheenScene* scene) {
+    if (!scene || scene->num_triangles <= 0) return -1;
+    std::vector<int> all((size_t)scene->num_triangles);
+    for (int i = 0; i < scene->num_triangles; i++) all[(size_t)i] = i;
+    sheen::QBvh q;
+    sheen::build_qbvh4(scene->triangles, all, q);
+    int depth = 0;
+    const int rc = sheen::check_qbvh4(q, depth);
+    return rc < 0 ? rc : depth;
+}

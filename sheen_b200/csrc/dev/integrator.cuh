@@ -1,7 +1,13 @@
 // integrator.cuh -- the per-sample integrator of render_kernel.cu:487-809,
-// written once over a query policy T (T::closest, T::opaque,
-// T::strand_depth) so that the plain megakernel (reference-order BVHs) and
-// the BVH4 megakernel share every line of shading.
+// written once over a query policy T so that the plain megakernel
+// (reference-order BVHs) and the BVH4 megakernel share every line of
+// shading.  T provides:
+//   closest(S, r, hit, c)                 scene_intersect (raycast.h:14-70)
+//   shadow(S, r, mask_aware, sh, c)       scene_intersect_opaque plus the
+//                                         glass test of its hit: kClear,
+//                                         kBlocked or kPass (sh = hit t, point)
+//   occluded(S, r, c)                     scene_intersect_opaque's boolean
+//   strand_depth(S, r, c)                 strand_bvh_tau (bvh.h:928-960)
 #pragma once
 #include "shade.cuh"
 #include "trace_ref.cuh"
@@ -23,13 +29,11 @@ template <class T, bool COUNT>
 __device__ __forceinline__ bool shadow_blocked(const DevScene& S, Ray r, RayTally& rt, Counters& c) {
     for (int pass = 0; pass < 3; pass++) {
         rt.shadow++;
-        Hit sh;
-        if (!T::opaque(S, r, sh, c)) return false;
-        if (transmission_at(S, S.materials[sh.mat], sh.uv) > 0.5f) {
-            r.o = sh.p + r.d * 0.002f;
-            continue;
-        }
-        return true;
+        ShadowHit sh;
+        const int q = T::shadow(S, r, true, sh, c);
+        if (q == kClear) return false;
+        if (q == kBlocked) return true;
+        r.o = sh.p + r.d * 0.002f;
     }
     return false;
 }
@@ -108,9 +112,8 @@ __device__ float3 media_march(const DevScene& S, const Ray& ray, float t_surf, u
                 }
                 Ray sr;
                 sr.o = p; sr.d = ld; sr.tmin = 0.002f; sr.tmax = ldist;
-                Hit sh;
                 rt.shadow++;
-                if (T::opaque(S, sr, sh, c)) continue;
+                if (T::occluded(S, sr, c)) continue;
                 rad += lr;
             }
             float3 sc = f3(md.sigma_s) * rad * 0.07957747f;
@@ -166,10 +169,11 @@ __device__ float3 beams(const DevScene& S, const Ray& ray, bool hit, float t_hit
             sr.o = p; sr.d = ldir; sr.tmin = 0.002f; sr.tmax = remain;
             bool blocked = false;
             for (int pass = 0; pass < 3; pass++) {
-                Hit sh;
+                ShadowHit sh;
                 rt.shadow++;
-                if (!T::opaque(S, sr, sh, c)) { blocked = false; break; }
-                if (S.materials[sh.mat].transmission > 0.5f) {
+                const int q = T::shadow(S, sr, false, sh, c);
+                if (q == kClear) { blocked = false; break; }
+                if (q == kPass) {
                     remain -= sh.t + 0.002f;
                     if (remain <= 0.0f) { blocked = false; break; }
                     sr.o = sh.p + ldir * 0.002f;

@@ -45,6 +45,15 @@ struct __align__(16) QNode4 {
     uint2 pad;
 };
 
+// One BVH4 over a set of triangles: nodes and 3 float4 per triangle slot in
+// leaf order ({v0, original index}, {e1, 0}, {e2, 0}).
+struct QMesh {
+    const QNode4* nodes;
+    const float4* tris;
+    int num_nodes;
+    int num_tris;
+};
+
 struct DevScene {
     CameraData cam;
 
@@ -64,10 +73,13 @@ struct DevScene {
     PhotonMapView pmap;
     float caustics;
 
-    // Wavefront form: triangles re-ordered into BVH4 leaf order.
-    const QNode4* mesh_qbvh;       // root at 0 (null when the scene has no triangles)
-    const float4* qtri;            // 3 float4 per triangle slot: v0 | e1 | e2, w of the first = original index
-    int num_qnodes;
+    // Wavefront form: BVH4 meshes (root at node 0; nodes == null when empty).
+    //   q_all     every triangle (closest-hit queries)
+    //   q_block   triangles whose material can never pass a shadow ray
+    //             (transmission <= 0.5): any-hit shadow queries
+    //   q_pass    the others (transmission > 0.5, possibly through a mask):
+    //             closest-hit shadow queries, usually a small set
+    QMesh q_all, q_block, q_pass;
     int has_glass;                 // any material with transmission > 0
 };
 

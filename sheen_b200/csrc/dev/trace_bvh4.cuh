@@ -1,0 +1,261 @@
+// trace_bvh4.cuh -- triangle queries of the wavefront form over the 4-wide
+// BVH with 8-bit child boxes (bvh4.cpp), plus the query policy FastTracer.
+//
+// Closest hit: nearest-child-first traversal with culling against the
+// closest hit found so far; stack entries carry their entry distance and are
+// dropped when popped behind the current hit.  Any hit: the same walk,
+// returning at the first accepted triangle.  The triangle test is the
+// reference's Moller-Trumbore (primitives/triangle.h:8-36) on the stored
+// v0/e1/e2, so a triangle answers exactly as in the plain form; only the
+// order of visits differs, which changes the result only for exact ties.
+//
+// Child-box test: each child interval is decoded as t = fmaf(q, s * 1/d,
+// (origin - o) * 1/d) per plane (one FMA), and the entry/exit distances are
+// widened by 2^-20 relative before the range test, more than the rounding of
+// the folded arithmetic, so a box is never culled where its triangles hit.
+#pragma once
+#include "trace_ref.cuh"
+
+namespace sheen {
+namespace dev {
+
+constexpr int kQStack = 48;
+
+struct QRay {
+    float3 o, d;
+    float ox, oy, oz;      // origin
+    float ix, iy, iz;      // 1 / direction, zero components nudged to +-1e-30
+    float tmin;
+};
+
+__device__ __forceinline__ float safe_inv(float d) {
+    return 1.0f / (fabsf(d) > 1e-30f ? d : copysignf(1e-30f, d));
+}
+
+__device__ __forceinline__ QRay make_qray(const Ray& r) {
+    QRay q;
+    q.o = r.o; q.d = r.d;
+    q.ox = r.o.x; q.oy = r.o.y; q.oz = r.o.z;
+    q.ix = safe_inv(r.d.x); q.iy = safe_inv(r.d.y); q.iz = safe_inv(r.d.z);
+    q.tmin = r.tmin;
+    return q;
+}
+
+__device__ __forceinline__ uint32_t byte_of(uint32_t w, int i) { return (w >> (8 * i)) & 0xffu; }
+
+// Tests the up-to-4 children of `node`; returns a bit mask of hit children
+// and their entry distances.
+__device__ __forceinline__ int qnode_children(const QNode4* __restrict__ nodes, int id, const QRay& r, float tfar,
+                                              float tn[4], uint4& child) {
+    const float4 oe = __ldg(&nodes[id].origin_exp);
+    child = __ldg(&nodes[id].child);
+    const uint4 qb = __ldg(&nodes[id].qbox);
+    const uint2 qz = __ldg(&nodes[id].qz);
+    const uint32_t packed = __float_as_uint(oe.w);
+    const int count = (int)(packed >> 24);
+    const float sx = __uint_as_float((packed & 0xffu) << 23);
+    const float sy = __uint_as_float(((packed >> 8) & 0xffu) << 23);
+    const float sz = __uint_as_float(((packed >> 16) & 0xffu) << 23);
+    // t(q) = q * (s / d) + (origin - o) / d
+    const float ax = sx * r.ix, bx = (oe.x - r.ox) * r.ix;
+    const float ay = sy * r.iy, by = (oe.y - r.oy) * r.iy;
+    const float az = sz * r.iz, bz = (oe.z - r.oz) * r.iz;
+    int mask = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        if (i >= count) break;
+        const float x0 = fmaf((float)byte_of(qb.x, i), ax, bx), x1 = fmaf((float)byte_of(qb.y, i), ax, bx);
+        const float y0 = fmaf((float)byte_of(qb.z, i), ay, by), y1 = fmaf((float)byte_of(qb.w, i), ay, by);
+        const float z0 = fmaf((float)byte_of(qz.x, i), az, bz), z1 = fmaf((float)byte_of(qz.y, i), az, bz);
+        const float tnear = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), r.tmin));
+        const float texit = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tfar));
+        // widen by 2^-20 relative (texit grows, tnear shrinks)
+        const float lo = tnear - fabsf(tnear) * 9.5367431640625e-7f;
+        const float hi = texit + fabsf(texit) * 9.5367431640625e-7f;
+        tn[i] = lo;
+        if (lo <= hi) mask |= 1 << i;
+    }
+    return mask;
+}
+
+// Moller-Trumbore on stored {v0, e1, e2} (primitives/triangle.h:8-36).
+__device__ __forceinline__ bool qtri_test(const QRay& r, float4 a, float4 b, float4 c, float tmin, float tmax,
+                                          float& t, float& u, float& v) {
+    const float3 e1 = f3(b.x, b.y, b.z), e2 = f3(c.x, c.y, c.z);
+    const float3 pv = cross(r.d, e2);
+    const float det = dot(e1, pv);
+    if (fabsf(det) < 1e-8f) return false;
+    const float inv = 1.0f / det;
+    const float3 tv = r.o - f3(a.x, a.y, a.z);
+    u = dot(tv, pv) * inv;
+    if (u < 0.0f || u > 1.0f) return false;
+    const float3 qv = cross(tv, e1);
+    v = dot(r.d, qv) * inv;
+    if (v < 0.0f || u + v > 1.0f) return false;
+    t = dot(e2, qv) * inv;
+    return !(t < tmin || t > tmax);
+}
+
+// Closest (ANY = false) or any (ANY = true) triangle hit with t in
+// [r.tmin, tmax] and strictly below `t_best` (in/out).  Returns the original
+// triangle index or -1.
+template <bool ANY, bool COUNT>
+__device__ __forceinline__ int qmesh_trace(const QMesh& m, const QRay& r, float tmax, float& t_best, float& bu,
+                                           float& bv, Counters& c) {
+    if (!m.nodes) return -1;
+    uint32_t stack_e[kQStack];
+    float stack_t[kQStack];
+    int sp = 0;
+    uint32_t entry = 0;   // root (inner)
+    int best = -1;
+    while (true) {
+        if (!(entry & 0x80000000u)) {
+            float tn[4];
+            uint4 ch;
+            if (COUNT) c.nodes++;
+            const int mask = qnode_children(m.nodes, (int)entry, r, t_best, tn, ch);
+            const uint32_t cid[4] = {ch.x, ch.y, ch.z, ch.w};
+            // Order hit children near to far: keys = distance bits with the slot
+            // in the low 2 bits (entry distances are >= tmin > 0, so their
+            // bit patterns order like the values).
+            uint32_t key[4];
+            int n = 0;
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                if (mask & (1 << i)) key[n++] = (__float_as_uint(fmaxf(tn[i], 0.0f)) & ~3u) | (uint32_t)i;
+            if (n == 0) goto pop;
+#define CSWAP(a, b) if (key[a] > key[b]) { uint32_t t_ = key[a]; key[a] = key[b]; key[b] = t_; }
+            if (n == 2) { CSWAP(0, 1) }
+            else if (n == 3) { CSWAP(0, 1) CSWAP(1, 2) CSWAP(0, 1) }
+            else if (n == 4) { CSWAP(0, 1) CSWAP(2, 3) CSWAP(0, 2) CSWAP(1, 3) CSWAP(1, 2) }
+#undef CSWAP
+            for (int k = n - 1; k >= 1; k--) {
+                if (sp < kQStack) {
+                    stack_e[sp] = cid[key[k] & 3u];
+                    stack_t[sp] = tn[key[k] & 3u];
+                    sp++;
+                }
+            }
+            entry = cid[key[0] & 3u];
+            continue;
+        } else {
+            const int first = (int)((entry & 0x7fffffffu) >> 3);
+            const int count = (int)(entry & 7u) + 1;
+            for (int k = 0; k < count; k++) {
+                const int slot = first + k;
+                const float4 a = __ldg(&m.tris[3 * slot]);
+                const float4 b = __ldg(&m.tris[3 * slot + 1]);
+                const float4 cc = __ldg(&m.tris[3 * slot + 2]);
+                if (COUNT) c.prims++;
+                float t, u, v;
+                if (qtri_test(r, a, b, cc, r.tmin, tmax, t, u, v) && t < t_best) {
+                    t_best = t; bu = u; bv = v;
+                    best = __float_as_int(a.w);
+                    if (ANY) return best;
+                }
+            }
+        }
+    pop:
+        while (true) {
+            if (sp == 0) return best;
+            --sp;
+            if (stack_t[sp] <= t_best) { entry = stack_e[sp]; break; }
+        }
+    }
+}
+
+// Closest mesh hit over q_all as a hit record (mesh_ref's result).
+template <bool COUNT>
+__device__ __forceinline__ bool mesh_q(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    if (!S.q_all.nodes) return false;
+    const QRay q = make_qray(r);
+    float t = r.tmax, u = 0.0f, v = 0.0f;
+    const int tri = qmesh_trace<false, COUNT>(S.q_all, q, r.tmax, t, u, v, c);
+    if (tri < 0) return false;
+    tri_finish(r, S.tris[tri], t, u, v, h);
+    h.obj = -(tri + 1);
+    return true;
+}
+
+// Mesh category of a shadow query (render_kernel.cu:248-267 over
+// raycast.h:87): the category's closest hit decides.  With passable
+// triangles present, the closest passable hit t_p is found first; any
+// blocking hit before it (or anywhere when there is none) makes the closest
+// hit blocking; otherwise the passable hit is classified by its material
+// (mask-aware when asked).  Returns kClear when the mesh has no hit at all.
+template <bool COUNT>
+__device__ __forceinline__ int mesh_shadow_q(const DevScene& S, const Ray& r, bool mask_aware, ShadowHit& sh,
+                                             Counters& c) {
+    if (!S.q_all.nodes) return kClear;
+    const QRay q = make_qray(r);
+    if (!S.q_pass.nodes) {
+        // No triangle can pass (every material's transmission <= 0.5, and a
+        // property map only scales it down): any hit blocks.
+        float t = r.tmax, u, v;
+        return qmesh_trace<true, COUNT>(S.q_all, q, r.tmax, t, u, v, c) >= 0 ? kBlocked : kClear;
+    }
+    float tp = r.tmax, up = 0.0f, vp = 0.0f;
+    const int pass_tri = qmesh_trace<false, COUNT>(S.q_pass, q, r.tmax, tp, up, vp, c);
+    if (S.q_block.nodes) {
+        float tb = tp, ub, vb;   // strictly closer than the passable hit (or than t_max)
+        if (qmesh_trace<true, COUNT>(S.q_block, q, r.tmax, tb, ub, vb, c) >= 0) return kBlocked;
+    }
+    if (pass_tri < 0) return kClear;
+    Hit h;
+    tri_finish(r, S.tris[pass_tri], tp, up, vp, h);
+    return classify_shadow_hit(S, h, mask_aware, sh);
+}
+
+// Any hit in the opaque categories (render_kernel.cu:413-422, media rays).
+template <bool COUNT>
+__device__ __forceinline__ bool mesh_any_q(const DevScene& S, const Ray& r, Counters& c) {
+    if (!S.q_all.nodes) return false;
+    const QRay q = make_qray(r);
+    float t = r.tmax, u, v;
+    return qmesh_trace<true, COUNT>(S.q_all, q, r.tmax, t, u, v, c) >= 0;
+}
+
+// Query policy of the wavefront form: triangles through the BVH4s, every
+// other category through the plain form's code (same category order).
+template <bool COUNT>
+struct FastTracer {
+    __device__ __forceinline__ static bool closest(const DevScene& S, const Ray& r, Hit& rec, Counters& c) {
+        float best = r.tmax;
+        bool hit = false;
+        Hit t;
+        if (spheres_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if (strands_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if (mesh_q<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if (hfs_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if (ses_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if (lathes_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if (prisms_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if (S.csg_root >= 0 && csg_test(S, r, t) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if (planes_scan(S, r, t) && t.t < best) { best = t.t; rec = t; hit = true; }
+        return hit;
+    }
+    __device__ __forceinline__ static int shadow(const DevScene& S, const Ray& r, bool mask_aware, ShadowHit& sh,
+                                                 Counters& c) {
+        Hit h;
+        if (spheres_ref<COUNT>(S, r, h, c)) return classify_shadow_hit(S, h, mask_aware, sh);
+        const int m = mesh_shadow_q<COUNT>(S, r, mask_aware, sh, c);
+        if (m != kClear) return m;
+        if (hfs_ref<COUNT>(S, r, h, c) || ses_ref<COUNT>(S, r, h, c) || lathes_ref<COUNT>(S, r, h, c) ||
+            prisms_ref<COUNT>(S, r, h, c) || (S.csg_root >= 0 && csg_test(S, r, h)) || planes_scan(S, r, h))
+            return classify_shadow_hit(S, h, mask_aware, sh);
+        return kClear;
+    }
+    __device__ __forceinline__ static bool occluded(const DevScene& S, const Ray& r, Counters& c) {
+        Hit h;
+        if (spheres_ref<COUNT>(S, r, h, c)) return true;
+        if (mesh_any_q<COUNT>(S, r, c)) return true;
+        return hfs_ref<COUNT>(S, r, h, c) || ses_ref<COUNT>(S, r, h, c) || lathes_ref<COUNT>(S, r, h, c) ||
+               prisms_ref<COUNT>(S, r, h, c) || (S.csg_root >= 0 && csg_test(S, r, h)) || planes_scan(S, r, h);
+    }
+    __device__ __forceinline__ static float strand_depth(const DevScene& S, const Ray& r, Counters& c) {
+        return strands_tau_ref<COUNT>(S, r, c);
+    }
+};
+
+}  // namespace dev
+}  // namespace sheen

@@ -217,13 +217,58 @@ __device__ __noinline__ float strands_tau_ref(const DevScene& S, const Ray& r, C
     return tau;
 }
 
+// Result of the shadow (opaque-set) query.
+enum : int { kClear = 0, kBlocked = 1, kPass = 2 };
+struct ShadowHit {
+    float t;
+    float3 p;
+};
+
+// Glass test of a shadow hit: transmission above 0.5, read through the
+// material's property map when mask_aware (render_kernel.cu:261-262), from
+// the material alone otherwise (the beam's test, render_kernel.cu:637).
+__device__ __forceinline__ int classify_shadow_hit(const DevScene& S, const Hit& h, bool mask_aware, ShadowHit& sh) {
+    const Material& m = S.materials[h.mat];
+    float tr;
+    if (mask_aware) {
+        tr = 0.0f;
+        if (m.transmission > 0.0f) {
+            tr = m.transmission;
+            if (m.mask_id >= 0 && m.mask_id < S.num_textures) {
+                // transmission_at without the shade.cuh dependency: R of the map at level 0
+                const TextureRef& t = S.textures[m.mask_id];
+                float u = h.uv.x - floorf(h.uv.x), v = 1.0f - (h.uv.y - floorf(h.uv.y));
+                float fx = u * (float)(t.width - 1), fy = v * (float)(t.height - 1);
+                int x0 = (int)fx, y0 = (int)fy, x1 = (x0 + 1) % t.width, y1 = (y0 + 1) % t.height;
+                float tx = fx - (float)x0, ty = fy - (float)y0;
+                auto R = [&](int x, int y) { return t.pixels[(size_t)(y * t.width + x) * 3] / 255.0f; };
+                float a = R(x0, y0) * (1.0f - tx) + R(x1, y0) * tx;
+                float b = R(x0, y1) * (1.0f - tx) + R(x1, y1) * tx;
+                tr *= a * (1.0f - ty) + b * ty;
+            }
+        }
+    } else {
+        tr = m.transmission;
+    }
+    sh.t = h.t;
+    sh.p = h.p;
+    return tr > 0.5f ? kPass : kBlocked;
+}
+
 // The plain form's query policy for the shared integrator.
 template <bool COUNT>
 struct RefTracer {
     __device__ __forceinline__ static bool closest(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
         return closest_ref<COUNT>(S, r, h, c);
     }
-    __device__ __forceinline__ static bool opaque(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    __device__ __forceinline__ static int shadow(const DevScene& S, const Ray& r, bool mask_aware, ShadowHit& sh,
+                                                 Counters& c) {
+        Hit h;
+        if (!opaque_ref<COUNT>(S, r, h, c)) return kClear;
+        return classify_shadow_hit(S, h, mask_aware, sh);
+    }
+    __device__ __forceinline__ static bool occluded(const DevScene& S, const Ray& r, Counters& c) {
+        Hit h;
         return opaque_ref<COUNT>(S, r, h, c);
     }
     __device__ __forceinline__ static float strand_depth(const DevScene& S, const Ray& r, Counters& c) {

@@ -37,8 +37,11 @@ struct QBvh {
     std::vector<dev::QNode4> nodes;
     std::vector<float4> tris;      // 3 float4 per triangle slot in leaf order
     int leaf_size_max = 0;
+    int max_depth = 0;            // inner-node levels (the traversal stack holds 3 per level)
 };
-void build_qbvh4(const Triangle* tris, int n, QBvh& out);
+// Builds over the triangles listed in `subset` (indices into `tris`; the
+// stored triangle records keep those original indices).
+void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out);
 
 // Result/accounting of one render call.
 struct RenderTally {
@@ -83,10 +86,12 @@ cudaError_t launch_primary_hits_bvh4(const DeviceScene& s, int W, int H, int ns,
 // Megakernel over the BVH4 mesh traversal (wavefront form's queries, one
 // thread per pixel); used by the wavefront form for scenes outside its
 // queue pipeline and as a measurement point.
-cudaError_t launch_mega_bvh4(const DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream);
+cudaError_t launch_mega_bvh4(const DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
+                             bool count_nodes);
 
 // Wavefront form.
-cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream);
+cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
+                             bool count_nodes);
 void wave_release(DeviceScene& s);
 
 // Photon pass on the device (emission + hash-grid build), called by

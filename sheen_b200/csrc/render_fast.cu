@@ -1,0 +1,88 @@
+// render_fast.cu -- the BVH4 megakernel: one thread per pixel running the
+// shared integrator over FastTracer (BVH4 closest hit with culling, split
+// any-hit shadow queries).  The wavefront form uses it for frames its queue
+// pipeline does not cover, and it is a measurement point of its own.
+#include "dev/integrator.cuh"
+#include "dev/trace_bvh4.cuh"
+#include "engine.h"
+
+namespace sheen {
+namespace dev {
+
+__device__ __forceinline__ void warp_add_fast(unsigned long long* dst, unsigned long long v) {
+    const unsigned mask = __activemask();
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(mask, v, o);
+    if ((threadIdx.x + threadIdx.y * blockDim.x) % 32 == 0) atomicAdd(dst, v);
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(128) mega_bvh4_kernel(DevScene S, float4* __restrict__ out, int W, int H, int aa,
+                                                        int x0, int y0, int x1, int y1, unsigned long long* tally) {
+    const int x = x0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int y = y0 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    RayTally rt;
+    Counters c;
+    if (x < x1 && y < y1) {
+        const int ns = aa < 1 ? 1 : (aa > 64 ? 64 : aa);
+        float3 acc = f3(0.0f, 0.0f, 0.0f);
+        for (int s = 0; s < ns; s++) acc += render_sample<FastTracer<COUNT>, COUNT>(S, x, y, s, ns, W, H, rt, c);
+        const float inv = 1.0f / float(ns);
+        out[(size_t)y * W + x] = make_float4(acc.x * inv, acc.y * inv, acc.z * inv, 1.0f);
+    }
+    if (tally) {
+        warp_add_fast(&tally[0], rt.primary);
+        warp_add_fast(&tally[1], rt.shadow);
+        warp_add_fast(&tally[2], rt.secondary);
+        if (COUNT) {
+            warp_add_fast(&tally[3], c.nodes);
+            warp_add_fast(&tally[4], c.prims);
+        }
+    }
+}
+
+__global__ void primary_hits_bvh4_kernel(DevScene S, int W, int H, int ns, int* obj, int* mat, float* tt) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    Counters c;
+    for (int s = 0; s < ns; s++) {
+        float pix;
+        const Ray r = camera_ray(S.cam, x, y, s, ns, W, H, pix);
+        Hit h;
+        const size_t k = ((size_t)y * W + x) * ns + s;
+        if (FastTracer<false>::closest(S, r, h, c)) { obj[k] = h.obj; mat[k] = h.mat; tt[k] = h.t; }
+        else { obj[k] = (int)0x80000000; mat[k] = (int)0x80000000; tt[k] = -1.0f; }
+    }
+}
+
+}  // namespace dev
+
+cudaError_t launch_mega_bvh4(const DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
+                             bool count_nodes) {
+    const dim3 block(16, 8);
+    const dim3 grid((rg.x1 - rg.x0 + 15) / 16, (rg.y1 - rg.y0 + 7) / 8);
+    if (count_nodes)
+        dev::mega_bvh4_kernel<true><<<grid, block, 0, stream>>>(s.view, out, W, H, aa, rg.x0, rg.y0, rg.x1, rg.y1,
+                                                                s.d_tally);
+    else
+        dev::mega_bvh4_kernel<false><<<grid, block, 0, stream>>>(s.view, out, W, H, aa, rg.x0, rg.y0, rg.x1, rg.y1,
+                                                                 s.d_tally);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_primary_hits_bvh4(const DeviceScene& s, int W, int H, int ns, int* obj, int* mat, float* t,
+                                     cudaStream_t stream) {
+    const dim3 block(16, 8);
+    const dim3 grid((W + 15) / 16, (H + 7) / 8);
+    dev::primary_hits_bvh4_kernel<<<grid, block, 0, stream>>>(s.view, W, H, ns, obj, mat, t);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
+                             bool count_nodes) {
+    return launch_mega_bvh4(s, W, H, aa, rg, out, stream, count_nodes);
+}
+
+void wave_release(DeviceScene&) {}
+
+}  // namespace sheen

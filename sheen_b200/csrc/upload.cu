@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "engine.h"
@@ -189,8 +190,30 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     }
     build_median_bvh(lo, hi, prims, false, prism_bvh);
 
-    QBvh qb;
-    if (form == SHEEN_FORM_WAVEFRONT && in->num_triangles > 0) build_qbvh4(in->triangles, in->num_triangles, qb);
+    // Wavefront form: BVH4 over all triangles, and -- when some triangles can
+    // pass a shadow ray (transmission > 0.5, render_kernel.cu:261-262) -- one
+    // over the blocking triangles and one over the passable ones.
+    QBvh q_all, q_block, q_pass;
+    if (form == SHEEN_FORM_WAVEFRONT && in->num_triangles > 0) {
+        std::vector<int> all, block, pass;
+        for (int i = 0; i < in->num_triangles; i++) {
+            all.push_back(i);
+            const int m = in->triangles[i].material_id;
+            const bool passable = m >= 0 && m < in->num_materials && in->materials[m].transmission > 0.5f;
+            (passable ? pass : block).push_back(i);
+        }
+        std::thread t1([&] { if (!pass.empty()) build_qbvh4(in->triangles, block, q_block); });
+        std::thread t2([&] { if (!pass.empty()) build_qbvh4(in->triangles, pass, q_pass); });
+        build_qbvh4(in->triangles, all, q_all);
+        t1.join();
+        t2.join();
+        // The traversal stack keeps at most 3 entries per level below the root.
+        if (3 * std::max(q_all.max_depth, std::max(q_block.max_depth, q_pass.max_depth)) + 1 > 48) {
+            set_error("triangle BVH too deep for the traversal stack");
+            delete s;
+            return -1;
+        }
+    }
 
     // Textures with mips; TextureRef pixel pointers are patched after the
     // arena address is known.
@@ -243,8 +266,12 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     const size_t o_mat = add_raw(in->materials, in->num_materials, sizeof(Material));
     const size_t o_lig = add_raw(in->lights, in->num_lights, sizeof(Light));
     const size_t o_med = add_raw(in->media, in->num_media, sizeof(Medium));
-    const size_t o_qn = add_vec(qb.nodes);
-    const size_t o_qt = add_vec(qb.tris);
+    const size_t o_qn = add_vec(q_all.nodes);
+    const size_t o_qt = add_vec(q_all.tris);
+    const size_t o_qbn = add_vec(q_block.nodes);
+    const size_t o_qbt = add_vec(q_block.tris);
+    const size_t o_qpn = add_vec(q_pass.nodes);
+    const size_t o_qpt = add_vec(q_pass.tris);
     std::vector<size_t> o_chain(chains.size(), (size_t)-1);
     for (size_t i = 0; i < chains.size(); i++) o_chain[i] = add_vec(chains[i]);
     std::vector<size_t> o_img(hfs.size(), (size_t)-1);
@@ -304,9 +331,17 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     v.lights = (const Light*)dptr(o_lig); v.num_lights = in->num_lights;
     v.media = (const Medium*)dptr(o_med); v.num_media = in->num_media;
     v.caustics = in->caustics;
-    v.mesh_qbvh = (const dev::QNode4*)dptr(o_qn);
-    v.qtri = (const float4*)dptr(o_qt);
-    v.num_qnodes = (int)qb.nodes.size();
+    auto qmesh = [&](const QBvh& q, size_t on, size_t ot) {
+        dev::QMesh m;
+        m.nodes = (const dev::QNode4*)dptr(on);
+        m.tris = (const float4*)dptr(ot);
+        m.num_nodes = (int)q.nodes.size();
+        m.num_tris = (int)(q.tris.size() / 3);
+        return m;
+    };
+    v.q_all = qmesh(q_all, o_qn, o_qt);
+    v.q_block = qmesh(q_block, o_qbn, o_qbt);
+    v.q_pass = qmesh(q_pass, o_qpn, o_qpt);
     v.has_glass = has_glass ? 1 : 0;
     s->d_tally = (unsigned long long*)dptr(o_tally);
     s->build_ms = t1 - t0;

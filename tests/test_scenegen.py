@@ -40,3 +40,15 @@ def test_sizes():
     assert v.num_sweep_strands == 32 and v.num_heightfields == 1 and v.csg_root >= 0
     s = sb.generate_scene(3, 1, 0, 4000000)
     assert s.view.photons == 4000000 and abs(s.view.photon_cell - 0.2) < 1e-7
+
+
+def test_bvh4_structure():
+    """The wavefront form's BVH4: every triangle in one leaf, decoded 8-bit
+    child boxes contain everything below them, depth within the stack."""
+    L = sb.lib()
+    L.sheen_selfcheck_bvh4.argtypes = [ctypes.c_void_p]
+    L.sheen_selfcheck_bvh4.restype = ctypes.c_int
+    for detail in (3, 6):
+        s = sb.generate_scene(1, 3, detail)
+        d = L.sheen_selfcheck_bvh4(s.view_ptr)
+        assert 1 <= d <= 15, d
