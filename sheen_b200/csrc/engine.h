@@ -62,6 +62,9 @@ struct DeviceScene {
     int photons_stored = 0;
     // Wavefront form state (queues sized for the last render).
     struct Wave* wave = nullptr;
+    // Scene features outside the queue pipeline (visible spot beams, the
+    // shadow-debug material mode): such frames run on the BVH4 megakernel.
+    bool wave_fallback = false;
 };
 
 int scene_upload(const SheenScene* in, int form, DeviceScene** out);

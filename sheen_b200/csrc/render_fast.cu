@@ -78,11 +78,5 @@ cudaError_t launch_primary_hits_bvh4(const DeviceScene& s, int W, int H, int ns,
     return cudaGetLastError();
 }
 
-cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
-                             bool count_nodes) {
-    return launch_mega_bvh4(s, W, H, aa, rg, out, stream, count_nodes);
-}
-
-void wave_release(DeviceScene&) {}
 
 }  // namespace sheen

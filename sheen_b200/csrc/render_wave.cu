@@ -1,0 +1,520 @@
+// render_wave.cu -- wavefront form of the per-sample integrator
+// (render_kernel.cu:487-809) over compacted ray queues.
+//
+// A frame runs as a fixed sequence of persistent kernels (one CUDA graph per
+// frame shape, replayed):
+//   primary   camera ray, closest hit, shading of the hit: writes the
+//             sample's base term (ambient + emission, or sky), pushes one
+//             shadow ray per light that passes the light's own tests, pushes
+//             the mirror ray (reflect > 0) and the first refracted ray
+//             (transmission > 0); records the blend weights
+//   shadow    every queued shadow ray: up to three opaque-set queries with
+//             glass passes, strand transmittance; writes its light slot
+//   reflect   mirror rays: closest hit and shading (or sky) -> shadow queue
+//   shadow
+//   refract   refracted rays: up to three faces, then shading (or sky)
+//   shadow
+//   resolve   per pixel: every sample's color from its slots, averaged
+// Each sample owns 3 segments (primary, mirror, refraction end) x (L + 2)
+// RGB slots: base, one per light, caustic.  Slots are summed in the
+// reference's order (base, light 0..L-1, caustic), then blended with the
+// weights of render_kernel.cu:730-731 and 805, so no float atomics are
+// needed and frames are bit-reproducible.  A segment whose weight is zero is
+// never written nor read.
+//
+// Queues are filled with warp-aggregated appends (ballot + popc, one atomic
+// per warp); persistent blocks claim 32-entry batches from an atomic head,
+// so uneven work (glass, empty sky) balances across the SMs.
+//
+// Frames the queue pipeline does not cover -- visible spot beams, media, a
+// material in the shadow-debug mode (shininess < 0), or more than 16
+// lights -- run on the BVH4 megakernel with identical results.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "dev/integrator.cuh"
+#include "dev/trace_bvh4.cuh"
+#include "engine.h"
+
+namespace sheen {
+
+namespace dev {
+
+constexpr int kMaxWaveLights = 16;
+
+enum CounterSlot {
+    kShadowCount = 0, kShadowHead, kReflCount, kReflHead, kRefrCount, kRefrHead, kPrimHead, kPixHead,
+    kRaysPrimary, kRaysShadow, kRaysSecondary, kCounterWords = 16
+};
+
+struct WaveView {
+    float* slots;          // samples * 3 * (L + 2) * 3
+    float* coef;           // samples * 3: weights of the primary / mirror / refraction segments
+    float4* shq;           // shadow queue, 3 float4 per entry
+    float4* rq;            // mirror queue, 2 float4 per entry
+    float4* tq;            // refraction queue, 2 float4 per entry
+    unsigned int* ctr;     // kCounterWords counters (queue sizes, batch heads, ray tallies)
+    int L;                 // lights
+    int ns;                // samples per pixel
+    int W, H, x0, y0, rw, rh;
+    int nsamples;          // rw * rh * ns
+    float pix_angle;
+    int count_rays;
+};
+
+__device__ __forceinline__ int seg_base(const WaveView& V, int sample, int seg) {
+    return (sample * 3 + seg) * (V.L + 2);
+}
+
+__device__ __forceinline__ void put_slot(const WaveView& V, int slot, float3 c) {
+    V.slots[3 * (size_t)slot] = c.x;
+    V.slots[3 * (size_t)slot + 1] = c.y;
+    V.slots[3 * (size_t)slot + 2] = c.z;
+}
+
+// Warp-aggregated append: every active lane with `want` gets a distinct
+// index in [0, capacity); one atomicAdd per warp.
+__device__ __forceinline__ unsigned int warp_append(unsigned int* counter, bool want) {
+    const unsigned int active = __activemask();
+    const unsigned int ballot = __ballot_sync(active, want);
+    if (!ballot) return 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(ballot) - 1;
+    unsigned int base = 0;
+    if (lane == leader) base = atomicAdd(counter, (unsigned int)__popc(ballot));
+    base = __shfl_sync(active, base, leader);
+    return want ? base + (unsigned int)__popc(ballot & ((1u << lane) - 1u)) : 0xffffffffu;
+}
+
+// Persistent batch claim: 32 consecutive items per warp.
+__device__ __forceinline__ int claim_batch(unsigned int* head) {
+    unsigned int b = 0;
+    if ((threadIdx.x & 31) == 0) b = atomicAdd(head, 32u);
+    return (int)__shfl_sync(0xffffffffu, b, 0);
+}
+
+// Sample index -> pixel and sample number.  Pixels are walked in 16x8 tiles
+// so a warp's primary rays are coherent.
+__device__ __forceinline__ void sample_pixel(const WaveView& V, int i, int& x, int& y, int& s) {
+    s = i % V.ns;
+    const int p = i / V.ns;
+    const int tiles_x = (V.rw + 15) / 16;
+    const int tile = p / 128, in = p % 128;
+    const int tx = tile % tiles_x, ty = tile / tiles_x;
+    x = V.x0 + tx * 16 + (in % 16);
+    y = V.y0 + ty * 8 + (in / 16);
+}
+
+__device__ __forceinline__ bool sample_valid(const WaveView& V, int x, int y) {
+    return x < V.x0 + V.rw && y < V.y0 + V.rh;
+}
+
+__device__ __forceinline__ void tally(const WaveView& V, int word, unsigned int v) {
+    if (!V.count_rays) return;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(&V.ctr[word], v);
+}
+
+// Shading of a hit for segment `seg` of `sample`: the base term now, one
+// queued shadow ray per light that passes its own tests (render_kernel.cu:
+// 152-235), the caustic gather last.  Lights skipped before tracing get a
+// zero slot.
+__device__ __forceinline__ void shade_and_queue(const DevScene& S, const WaveView& V, const Hit& h, float3 view,
+                                                float footprint, uint32_t seed, int sample, int seg, bool active) {
+    ShadePoint sp;
+    int sb = 0;
+    if (active) {
+        sp = shade_prepare(S, h, view, footprint);
+        sb = seg_base(V, sample, seg);
+        put_slot(V, sb, shade_emitted(S, sp));
+        put_slot(V, sb + V.L + 1, caustic_term(S, sp));
+    }
+    const bool strands = active && S.num_strands > 0 && S.materials[h.mat].anisotropy <= 0.0f;
+    for (int i = 0; i < V.L; i++) {
+        LightSample ls;
+        bool want = false;
+        float3 contrib = f3(0.0f, 0.0f, 0.0f);
+        Ray sr;
+        if (active) {
+            want = light_sample(S, sp, i, seed, ls);
+            if (want) {
+                sr.o = sp.p + sp.ng * 0.002f;
+                sr.d = normalize(ls.target - sr.o);
+                sr.tmax = ls.tmax;
+                contrib = brdf(S, sp, ls.L, ls.radiance);
+            } else {
+                put_slot(V, sb + 1 + i, f3(0.0f, 0.0f, 0.0f));
+            }
+        }
+        const unsigned int q = warp_append(&V.ctr[kShadowCount], want);
+        if (want) {
+            V.shq[3 * (size_t)q] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
+            V.shq[3 * (size_t)q + 1] = make_float4(sr.d.x, sr.d.y, sr.d.z, __int_as_float(sb + 1 + i));
+            V.shq[3 * (size_t)q + 2] = make_float4(contrib.x, contrib.y, contrib.z, strands ? 1.0f : 0.0f);
+        }
+    }
+}
+
+__device__ __forceinline__ float3 refract_dir(const DevScene& S, const Hit& gh, float3 d, bool entering,
+                                              float& w) {
+    const Material& sm = S.materials[gh.mat];
+    const float ior = fmaxf(ior_at(S, sm, gh.uv), 1.0f);
+    const float eta = entering ? 1.0f / ior : ior;
+    const float cosi = fmaxf(-dot(d, gh.n), 1.0e-4f);
+    const float k = 1.0f - eta * eta * (1.0f - cosi * cosi);
+    const float3 td = k < 0.0f ? normalize(d + 2.0f * cosi * gh.n) : normalize(eta * d + (eta * cosi - sqrtf(k)) * gh.n);
+    w *= transmission_at(S, sm, gh.uv);
+    return td;
+}
+
+__global__ void __launch_bounds__(128) wave_primary(DevScene S, WaveView V) {
+    using T = FastTracer<false>;
+    Counters c;
+    while (true) {
+        const int base = claim_batch(&V.ctr[kPrimHead]);
+        if (base >= V.nsamples) break;
+        const int i = base + (threadIdx.x & 31);
+        int x = 0, y = 0, s = 0;
+        bool active = i < V.nsamples;
+        if (active) {
+            sample_pixel(V, i, x, y, s);
+            active = sample_valid(V, x, y);
+        }
+        Hit rec;
+        Ray ray;
+        bool hit = false;
+        uint32_t seed = 0;
+        if (active) {
+            float pix;
+            ray = camera_ray(S.cam, x, y, s, V.ns, V.W, V.H, pix);
+            seed = sample_seed(x, y, s);
+            hit = T::closest(S, ray, rec, c);
+        }
+        tally(V, kRaysPrimary, active ? 1u : 0u);
+        float w = 0.0f, gtr = 0.0f;
+        if (active) {
+            if (!hit) {
+                put_slot(V, seg_base(V, i, 0), sky(ray.d));
+                V.coef[3 * (size_t)i] = 1.0f;
+                V.coef[3 * (size_t)i + 1] = 0.0f;
+                V.coef[3 * (size_t)i + 2] = 0.0f;
+            } else {
+                const Material& pm = S.materials[rec.mat];
+                w = pm.reflect > 0.0f ? fminf(pm.reflect, 1.0f) : 0.0f;
+                gtr = transmission_at(S, pm, rec.uv);
+                const float g = gtr > 0.0f ? 1.0f - fminf(gtr, 1.0f) : 1.0f;
+                V.coef[3 * (size_t)i] = (1.0f - w) * g;
+                V.coef[3 * (size_t)i + 1] = w * g;
+                V.coef[3 * (size_t)i + 2] = 0.0f;   // set by the refraction stage
+            }
+        }
+        shade_and_queue(S, V, rec, -ray.d, rec.t * V.pix_angle, seed, i, 0, active && hit);
+        // mirror ray (render_kernel.cu:674-680)
+        const bool want_r = active && hit && w > 0.0f;
+        const unsigned int qr = warp_append(&V.ctr[kReflCount], want_r);
+        if (want_r) {
+            const float3 rd = normalize(ray.d - rec.n * (2.0f * dot(ray.d, rec.n)));
+            const float3 ro = rec.p + rec.n * 0.002f;
+            V.rq[2 * (size_t)qr] = make_float4(ro.x, ro.y, ro.z, __int_as_float(i));
+            V.rq[2 * (size_t)qr + 1] = make_float4(rd.x, rd.y, rd.z, 0.0f);
+        }
+        // first refraction face (render_kernel.cu:749-765 with b = 0)
+        const bool want_t = active && hit && gtr > 0.0f;
+        float wt = 1.0f;
+        float3 td = f3(0.0f, 0.0f, 0.0f);
+        if (want_t) td = refract_dir(S, rec, ray.d, true, wt);
+        const unsigned int qt = warp_append(&V.ctr[kRefrCount], want_t);
+        if (want_t) {
+            const float3 to = rec.p + td * 0.002f;
+            V.tq[2 * (size_t)qt] = make_float4(to.x, to.y, to.z, __int_as_float(i));
+            V.tq[2 * (size_t)qt + 1] = make_float4(td.x, td.y, td.z, wt);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128) wave_shadow(DevScene S, WaveView V) {
+    using T = FastTracer<false>;
+    Counters c;
+    const unsigned int n = V.ctr[kShadowCount];
+    while (true) {
+        const int base = claim_batch(&V.ctr[kShadowHead]);
+        if (base >= (int)n) break;
+        const int q = base + (threadIdx.x & 31);
+        unsigned int rays = 0;
+        if (q < (int)n) {
+            const float4 a = V.shq[3 * (size_t)q], b = V.shq[3 * (size_t)q + 1], cc = V.shq[3 * (size_t)q + 2];
+            Ray r;
+            r.o = f3(a.x, a.y, a.z);
+            r.d = f3(b.x, b.y, b.z);
+            r.tmin = 0.001f;
+            r.tmax = a.w;
+            const Ray first = r;
+            bool blocked = false;
+            for (int pass = 0; pass < 3; pass++) {
+                rays++;
+                ShadowHit sh;
+                const int res = T::shadow(S, r, true, sh, c);
+                if (res == kClear) break;
+                if (res == kBlocked) { blocked = true; break; }
+                r.o = sh.p + r.d * 0.002f;
+            }
+            float3 contrib = f3(0.0f, 0.0f, 0.0f);
+            if (!blocked) {
+                contrib = f3(cc.x, cc.y, cc.z);
+                if (cc.w != 0.0f) contrib = contrib * expf(-T::strand_depth(S, first, c));
+            }
+            put_slot(V, __float_as_int(b.w), contrib);
+        }
+        tally(V, kRaysShadow, rays);
+    }
+}
+
+__global__ void __launch_bounds__(128) wave_reflect(DevScene S, WaveView V) {
+    using T = FastTracer<false>;
+    Counters c;
+    const unsigned int n = V.ctr[kReflCount];
+    while (true) {
+        const int base = claim_batch(&V.ctr[kReflHead]);
+        if (base >= (int)n) break;
+        const int q = base + (threadIdx.x & 31);
+        const bool active = q < (int)n;
+        Ray rr;
+        int i = 0;
+        Hit rh;
+        bool rhit = false;
+        uint32_t seed = 0;
+        if (active) {
+            const float4 a = V.rq[2 * (size_t)q], b = V.rq[2 * (size_t)q + 1];
+            i = __float_as_int(a.w);
+            rr.o = f3(a.x, a.y, a.z);
+            rr.d = f3(b.x, b.y, b.z);
+            rr.tmin = 0.001f;
+            rr.tmax = 1.0e10f;
+            int x, y, s;
+            sample_pixel(V, i, x, y, s);
+            seed = sample_seed(x, y, s);
+            rhit = T::closest(S, rr, rh, c);
+            if (!rhit) {
+                const int sb = seg_base(V, i, 1);
+                put_slot(V, sb, sky(rr.d));
+                for (int l = 0; l < V.L + 1; l++) put_slot(V, sb + 1 + l, f3(0.0f, 0.0f, 0.0f));
+            }
+        }
+        tally(V, kRaysSecondary, active ? 1u : 0u);
+        shade_and_queue(S, V, rh, -rr.d, rh.t * V.pix_angle, seed, i, 1, active && rhit);
+    }
+}
+
+__global__ void __launch_bounds__(128) wave_refract(DevScene S, WaveView V) {
+    using T = FastTracer<false>;
+    Counters c;
+    const unsigned int n = V.ctr[kRefrCount];
+    while (true) {
+        const int base = claim_batch(&V.ctr[kRefrHead]);
+        if (base >= (int)n) break;
+        const int q = base + (threadIdx.x & 31);
+        const bool active = q < (int)n;
+        int i = 0;
+        Hit nh;
+        bool shade = false;
+        uint32_t seed = 0;
+        float3 td = f3(0.0f, 0.0f, 0.0f);
+        unsigned int rays = 0;
+        if (active) {
+            const float4 a = V.tq[2 * (size_t)q], b = V.tq[2 * (size_t)q + 1];
+            i = __float_as_int(a.w);
+            int x, y, s;
+            sample_pixel(V, i, x, y, s);
+            seed = sample_seed(x, y, s);
+            Ray gr;
+            gr.o = f3(a.x, a.y, a.z);
+            gr.d = f3(b.x, b.y, b.z);
+            gr.tmin = 0.001f;
+            gr.tmax = 1.0e10f;
+            float w = b.w;
+            bool entering = true;
+            float cT = 0.0f;
+            const int sb = seg_base(V, i, 2);
+            // render_kernel.cu:749-803: faces b = 0..2 (the first direction was
+            // computed by the primary stage)
+            for (int f = 0; f < 3; f++) {
+                td = gr.d;
+                rays++;
+                if (!T::closest(S, gr, nh, c)) {
+                    put_slot(V, sb, sky(td));
+                    for (int l = 0; l < V.L + 1; l++) put_slot(V, sb + 1 + l, f3(0.0f, 0.0f, 0.0f));
+                    cT = w;
+                    break;
+                }
+                if (transmission_at(S, S.materials[nh.mat], nh.uv) > 0.0f) {
+                    entering = !entering;
+                    if (f == 2) break;   // the reference's loop ends here: no contribution
+                    const float3 nd = refract_dir(S, nh, gr.d, entering, w);
+                    gr.o = nh.p + nd * 0.002f;
+                    gr.d = nd;
+                    continue;
+                }
+                shade = true;
+                cT = w;
+                break;
+            }
+            V.coef[3 * (size_t)i + 2] = cT;
+        }
+        tally(V, kRaysSecondary, rays);
+        shade_and_queue(S, V, nh, -td, nh.t * V.pix_angle, seed, i, 2, active && shade);
+    }
+}
+
+__device__ __forceinline__ float3 get_slot(const WaveView& V, int slot) {
+    return f3(V.slots[3 * (size_t)slot], V.slots[3 * (size_t)slot + 1], V.slots[3 * (size_t)slot + 2]);
+}
+
+__device__ __forceinline__ float3 segment_value(const WaveView& V, int sb) {
+    float3 v = get_slot(V, sb);
+    for (int l = 0; l < V.L; l++) v += get_slot(V, sb + 1 + l);
+    return v + get_slot(V, sb + V.L + 1);
+}
+
+__global__ void wave_resolve(WaveView V, float4* __restrict__ out) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= V.rw * V.rh) return;
+    int x, y, s;
+    sample_pixel(V, p * V.ns, x, y, s);
+    if (!sample_valid(V, x, y)) return;
+    float3 acc = f3(0.0f, 0.0f, 0.0f);
+    for (int k = 0; k < V.ns; k++) {
+        const int i = p * V.ns + k;
+        const float cP = V.coef[3 * (size_t)i], cR = V.coef[3 * (size_t)i + 1], cT = V.coef[3 * (size_t)i + 2];
+        float3 col = segment_value(V, seg_base(V, i, 0)) * cP;
+        if (cR != 0.0f) col += segment_value(V, seg_base(V, i, 1)) * cR;
+        if (cT != 0.0f) col += segment_value(V, seg_base(V, i, 2)) * cT;
+        acc += col;
+    }
+    const float inv = 1.0f / float(V.ns);
+    out[(size_t)y * V.W + x] = make_float4(acc.x * inv, acc.y * inv, acc.z * inv, 1.0f);
+}
+
+__global__ void wave_tally_out(WaveView V, unsigned long long* tally) {
+    tally[0] += V.ctr[kRaysPrimary];
+    tally[1] += V.ctr[kRaysShadow];
+    tally[2] += V.ctr[kRaysSecondary];
+}
+
+}  // namespace dev
+
+// Per-scene buffers and the captured frame graph.
+struct Wave {
+    int nsamples_cap = 0, L = 0;
+    float* slots = nullptr;
+    float* coef = nullptr;
+    float4* shq = nullptr;
+    float4* rq = nullptr;
+    float4* tq = nullptr;
+    unsigned int* ctr = nullptr;
+    size_t bytes = 0;
+    int grid_primary = 0, grid_shadow = 0, grid_reflect = 0, grid_refract = 0;
+};
+
+void wave_release(DeviceScene& s) {
+    if (!s.wave) return;
+    Wave* w = s.wave;
+    cudaFree(w->slots); cudaFree(w->coef); cudaFree(w->shq); cudaFree(w->rq); cudaFree(w->tq); cudaFree(w->ctr);
+    delete w;
+    s.wave = nullptr;
+}
+
+static bool wave_supported(const DeviceScene& s) {
+    const dev::DevScene& v = s.view;
+    if (v.num_media > 0 || v.num_lights > dev::kMaxWaveLights) return false;
+    return !s.wave_fallback;
+}
+
+static cudaError_t wave_reserve(DeviceScene& s, int nsamples) {
+    const int L = s.view.num_lights;
+    if (s.wave && s.wave->nsamples_cap >= nsamples && s.wave->L == L) return cudaSuccess;
+    wave_release(s);
+    Wave* w = new Wave();
+    w->nsamples_cap = nsamples;
+    w->L = L;
+    const size_t slots = (size_t)nsamples * 3 * (L + 2) * 3;
+    const size_t shq = (size_t)nsamples * std::max(L, 1);
+    cudaError_t e;
+    size_t bytes = 0;
+    auto alloc = [&](void** p, size_t n) {
+        bytes += n;
+        return cudaMalloc(p, n);
+    };
+    if ((e = alloc((void**)&w->slots, slots * sizeof(float))) != cudaSuccess ||
+        (e = alloc((void**)&w->coef, (size_t)nsamples * 3 * sizeof(float))) != cudaSuccess ||
+        (e = alloc((void**)&w->shq, shq * 3 * sizeof(float4))) != cudaSuccess ||
+        (e = alloc((void**)&w->rq, (size_t)nsamples * 2 * sizeof(float4))) != cudaSuccess ||
+        (e = alloc((void**)&w->tq, (size_t)nsamples * 2 * sizeof(float4))) != cudaSuccess ||
+        (e = alloc((void**)&w->ctr, dev::kCounterWords * sizeof(unsigned int))) != cudaSuccess) {
+        s.wave = w;
+        wave_release(s);
+        return e;
+    }
+    w->bytes = bytes;
+    int dev_id = 0, sms = 148;
+    cudaGetDevice(&dev_id);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id);
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dev::wave_primary, 128, 0);
+    w->grid_primary = sms * std::max(b, 1);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dev::wave_shadow, 128, 0);
+    w->grid_shadow = sms * std::max(b, 1);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dev::wave_reflect, 128, 0);
+    w->grid_reflect = sms * std::max(b, 1);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dev::wave_refract, 128, 0);
+    w->grid_refract = sms * std::max(b, 1);
+    s.wave = w;
+    return cudaSuccess;
+}
+
+cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
+                             bool count_nodes) {
+    if (!wave_supported(s) || count_nodes) return launch_mega_bvh4(s, W, H, aa, rg, out, stream, count_nodes);
+    const int ns = aa < 1 ? 1 : (aa > 64 ? 64 : aa);
+    const int rw = rg.x1 - rg.x0, rh = rg.y1 - rg.y0;
+    // pixels are padded to whole 16x8 tiles by sample_pixel
+    const long long padded = (long long)((rw + 15) / 16) * 16 * ((rh + 7) / 8) * 8;
+    const long long nsamples = padded * ns;
+    if (nsamples > (1ll << 30)) return cudaErrorInvalidValue;
+    cudaError_t e = wave_reserve(s, (int)nsamples);
+    if (e != cudaSuccess) return e;
+    Wave* w = s.wave;
+    dev::WaveView V;
+    V.slots = w->slots; V.coef = w->coef; V.shq = w->shq; V.rq = w->rq; V.tq = w->tq; V.ctr = w->ctr;
+    V.L = s.view.num_lights;
+    V.ns = ns;
+    V.W = W; V.H = H; V.x0 = rg.x0; V.y0 = rg.y0; V.rw = rw; V.rh = rh;
+    V.nsamples = (int)nsamples;
+    {
+        const CameraData& cam = s.view.cam;
+        float tan_x = 1.0f;
+        if (cam.focal_length > 0.0f) {
+            const float tan_h = 0.5f * cam.sensor_width / cam.focal_length;
+            tan_x = (W >= H) ? tan_h : tan_h * float(W) / float(H);
+        }
+        V.pix_angle = 2.0f * tan_x / (float)W;
+    }
+    V.count_rays = 1;
+    if ((e = cudaMemsetAsync(w->ctr, 0, dev::kCounterWords * sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    dev::wave_primary<<<w->grid_primary, 128, 0, stream>>>(s.view, V);
+    dev::wave_shadow<<<w->grid_shadow, 128, 0, stream>>>(s.view, V);
+    if ((e = cudaMemsetAsync(&w->ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    dev::wave_reflect<<<w->grid_reflect, 128, 0, stream>>>(s.view, V);
+    dev::wave_shadow<<<w->grid_shadow, 128, 0, stream>>>(s.view, V);
+    if ((e = cudaMemsetAsync(&w->ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    dev::wave_refract<<<w->grid_refract, 128, 0, stream>>>(s.view, V);
+    dev::wave_shadow<<<w->grid_shadow, 128, 0, stream>>>(s.view, V);
+    const int npix = rw * rh;
+    (void)npix;
+    const int npad = (int)(padded);
+    dev::wave_resolve<<<(npad + 127) / 128, 128, 0, stream>>>(V, out);
+    dev::wave_tally_out<<<1, 1, 0, stream>>>(V, s.d_tally);
+    return cudaGetLastError();
+}
+
+}  // namespace sheen

@@ -232,7 +232,12 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     }
     std::vector<HeightField> hfs(in->heightfields, in->heightfields + std::max(in->num_heightfields, 0));
     bool has_glass = false;
-    for (int i = 0; i < in->num_materials; i++) has_glass |= in->materials[i].transmission > 0.0f;
+    for (int i = 0; i < in->num_materials; i++) {
+        has_glass |= in->materials[i].transmission > 0.0f;
+        s->wave_fallback |= in->materials[i].shininess < 0.0f;
+    }
+    for (int i = 0; i < in->num_lights; i++)
+        s->wave_fallback |= in->lights[i].type == 3 && in->lights[i].beam > 0.0f;
     const double t1 = now_ms();
 
     // ---- arena layout -------------------------------------------------
