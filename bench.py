@@ -233,7 +233,9 @@ def run_ours(args):
 
 def launches_per_frame(form):
     import sheen_b200 as sb
-    return 1 if form == sb.FORM_PLAIN else int(os.environ.get("SHEEN_WAVE_LAUNCHES", "1"))
+    # plain: one megakernel; wavefront: primary, 3 x shadow, mirror,
+    # refraction, resolve, tally (one CUDA graph launch)
+    return 1 if form == sb.FORM_PLAIN else 8
 
 
 def band_rays(ds, stream, out):

@@ -215,45 +215,59 @@ __device__ __forceinline__ bool mesh_any_q(const DevScene& S, const Ray& r, Coun
     return qmesh_trace<true, COUNT>(S.q_all, q, r.tmax, t, u, v, c) >= 0;
 }
 
+// Scene categories a kernel variant compiles in (a scene outside a
+// variant's set runs the full variant).
+enum : int {
+    kCatSpheres = 1, kCatStrands = 2, kCatMesh = 4, kCatHF = 8, kCatSE = 16, kCatLathe = 32, kCatPrism = 64,
+    kCatCSG = 128, kCatPlanes = 256,
+    kCatAll = 511,
+    kCatSimple = kCatSpheres | kCatMesh | kCatPlanes
+};
+
 // Query policy of the wavefront form: triangles through the BVH4s, every
 // other category through the plain form's code (same category order).
-template <bool COUNT>
+template <bool COUNT, int F = kCatAll>
 struct FastTracer {
     __device__ __forceinline__ static bool closest(const DevScene& S, const Ray& r, Hit& rec, Counters& c) {
         float best = r.tmax;
         bool hit = false;
         Hit t;
-        if (spheres_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if (strands_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if (mesh_q<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if (hfs_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if (ses_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if (lathes_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if (prisms_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if (S.csg_root >= 0 && csg_test(S, r, t) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if (planes_scan(S, r, t) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatSpheres) && spheres_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatStrands) && strands_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatMesh) && mesh_q<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatHF) && hfs_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatSE) && ses_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatLathe) && lathes_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatPrism) && prisms_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatCSG) && S.csg_root >= 0 && csg_test(S, r, t) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatPlanes) && planes_scan(S, r, t) && t.t < best) { best = t.t; rec = t; hit = true; }
         return hit;
     }
     __device__ __forceinline__ static int shadow(const DevScene& S, const Ray& r, bool mask_aware, ShadowHit& sh,
                                                  Counters& c) {
         Hit h;
-        if (spheres_ref<COUNT>(S, r, h, c)) return classify_shadow_hit(S, h, mask_aware, sh);
-        const int m = mesh_shadow_q<COUNT>(S, r, mask_aware, sh, c);
-        if (m != kClear) return m;
-        if (hfs_ref<COUNT>(S, r, h, c) || ses_ref<COUNT>(S, r, h, c) || lathes_ref<COUNT>(S, r, h, c) ||
-            prisms_ref<COUNT>(S, r, h, c) || (S.csg_root >= 0 && csg_test(S, r, h)) || planes_scan(S, r, h))
+        if ((F & kCatSpheres) && spheres_ref<COUNT>(S, r, h, c)) return classify_shadow_hit(S, h, mask_aware, sh);
+        if (F & kCatMesh) {
+            const int m = mesh_shadow_q<COUNT>(S, r, mask_aware, sh, c);
+            if (m != kClear) return m;
+        }
+        if (((F & kCatHF) && hfs_ref<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_ref<COUNT>(S, r, h, c)) ||
+            ((F & kCatLathe) && lathes_ref<COUNT>(S, r, h, c)) || ((F & kCatPrism) && prisms_ref<COUNT>(S, r, h, c)) ||
+            ((F & kCatCSG) && S.csg_root >= 0 && csg_test(S, r, h)) || ((F & kCatPlanes) && planes_scan(S, r, h)))
             return classify_shadow_hit(S, h, mask_aware, sh);
         return kClear;
     }
     __device__ __forceinline__ static bool occluded(const DevScene& S, const Ray& r, Counters& c) {
         Hit h;
-        if (spheres_ref<COUNT>(S, r, h, c)) return true;
-        if (mesh_any_q<COUNT>(S, r, c)) return true;
-        return hfs_ref<COUNT>(S, r, h, c) || ses_ref<COUNT>(S, r, h, c) || lathes_ref<COUNT>(S, r, h, c) ||
-               prisms_ref<COUNT>(S, r, h, c) || (S.csg_root >= 0 && csg_test(S, r, h)) || planes_scan(S, r, h);
+        if ((F & kCatSpheres) && spheres_ref<COUNT>(S, r, h, c)) return true;
+        if ((F & kCatMesh) && mesh_any_q<COUNT>(S, r, c)) return true;
+        return ((F & kCatHF) && hfs_ref<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_ref<COUNT>(S, r, h, c)) ||
+               ((F & kCatLathe) && lathes_ref<COUNT>(S, r, h, c)) ||
+               ((F & kCatPrism) && prisms_ref<COUNT>(S, r, h, c)) ||
+               ((F & kCatCSG) && S.csg_root >= 0 && csg_test(S, r, h)) || ((F & kCatPlanes) && planes_scan(S, r, h));
     }
     __device__ __forceinline__ static float strand_depth(const DevScene& S, const Ray& r, Counters& c) {
-        return strands_tau_ref<COUNT>(S, r, c);
+        return (F & kCatStrands) ? strands_tau_ref<COUNT>(S, r, c) : 0.0f;
     }
 };
 

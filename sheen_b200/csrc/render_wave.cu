@@ -168,8 +168,9 @@ __device__ __forceinline__ float3 refract_dir(const DevScene& S, const Hit& gh, 
     return td;
 }
 
+template <int F>
 __global__ void __launch_bounds__(128) wave_primary(DevScene S, WaveView V) {
-    using T = FastTracer<false>;
+    using T = FastTracer<false, F>;
     Counters c;
     while (true) {
         const int base = claim_batch(&V.ctr[kPrimHead]);
@@ -233,8 +234,9 @@ __global__ void __launch_bounds__(128) wave_primary(DevScene S, WaveView V) {
     }
 }
 
+template <int F>
 __global__ void __launch_bounds__(128) wave_shadow(DevScene S, WaveView V) {
-    using T = FastTracer<false>;
+    using T = FastTracer<false, F>;
     Counters c;
     const unsigned int n = V.ctr[kShadowCount];
     while (true) {
@@ -270,8 +272,9 @@ __global__ void __launch_bounds__(128) wave_shadow(DevScene S, WaveView V) {
     }
 }
 
+template <int F>
 __global__ void __launch_bounds__(128) wave_reflect(DevScene S, WaveView V) {
-    using T = FastTracer<false>;
+    using T = FastTracer<false, F>;
     Counters c;
     const unsigned int n = V.ctr[kReflCount];
     while (true) {
@@ -306,8 +309,9 @@ __global__ void __launch_bounds__(128) wave_reflect(DevScene S, WaveView V) {
     }
 }
 
+template <int F>
 __global__ void __launch_bounds__(128) wave_refract(DevScene S, WaveView V) {
-    using T = FastTracer<false>;
+    using T = FastTracer<false, F>;
     Counters c;
     const unsigned int n = V.ctr[kRefrCount];
     while (true) {
@@ -377,8 +381,10 @@ __device__ __forceinline__ float3 segment_value(const WaveView& V, int sb) {
 }
 
 __global__ void wave_resolve(WaveView V, float4* __restrict__ out) {
+    // p walks the padded 16x8-tile order of sample_pixel; padding pixels
+    // fall outside the region and are skipped below.
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= V.rw * V.rh) return;
+    if (p >= V.nsamples / V.ns) return;
     int x, y, s;
     sample_pixel(V, p * V.ns, x, y, s);
     if (!sample_valid(V, x, y)) return;
@@ -413,12 +419,59 @@ struct Wave {
     float4* tq = nullptr;
     unsigned int* ctr = nullptr;
     size_t bytes = 0;
-    int grid_primary = 0, grid_shadow = 0, grid_reflect = 0, grid_refract = 0;
+    int sms = 148;
+    // The frame's launch sequence captured once per frame shape and replayed.
+    cudaStream_t capture_stream = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    struct Key {
+        int W, H, aa, x0, y0, x1, y1;
+        const void* out;
+        bool operator==(const Key& o) const {
+            return W == o.W && H == o.H && aa == o.aa && x0 == o.x0 && y0 == o.y0 && x1 == o.x1 && y1 == o.y1 &&
+                   out == o.out;
+        }
+    } key{};
 };
+
+// Persistent grid: as many 128-thread blocks as fit on every SM.
+template <class K>
+static int persistent_grid(K kernel, int sms) {
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, 128, 0);
+    return sms * std::max(b, 1);
+}
+
+// The queue pipeline of one frame for category set F.
+template <int F>
+static cudaError_t run_pipeline(DeviceScene& s, const dev::WaveView& V, int npad, float4* out, cudaStream_t stream) {
+    Wave* w = s.wave;
+    static int g_primary = 0, g_shadow = 0, g_reflect = 0, g_refract = 0;
+    if (!g_primary) {
+        g_primary = persistent_grid(dev::wave_primary<F>, w->sms);
+        g_shadow = persistent_grid(dev::wave_shadow<F>, w->sms);
+        g_reflect = persistent_grid(dev::wave_reflect<F>, w->sms);
+        g_refract = persistent_grid(dev::wave_refract<F>, w->sms);
+    }
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(w->ctr, 0, dev::kCounterWords * sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    dev::wave_primary<F><<<g_primary, 128, 0, stream>>>(s.view, V);
+    dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
+    if ((e = cudaMemsetAsync(&w->ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    dev::wave_reflect<F><<<g_reflect, 128, 0, stream>>>(s.view, V);
+    dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
+    if ((e = cudaMemsetAsync(&w->ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    dev::wave_refract<F><<<g_refract, 128, 0, stream>>>(s.view, V);
+    dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
+    dev::wave_resolve<<<(npad + 127) / 128, 128, 0, stream>>>(V, out);
+    dev::wave_tally_out<<<1, 1, 0, stream>>>(V, s.d_tally);
+    return cudaGetLastError();
+}
 
 void wave_release(DeviceScene& s) {
     if (!s.wave) return;
     Wave* w = s.wave;
+    if (w->exec) cudaGraphExecDestroy(w->exec);
+    if (w->capture_stream) cudaStreamDestroy(w->capture_stream);
     cudaFree(w->slots); cudaFree(w->coef); cudaFree(w->shq); cudaFree(w->rq); cudaFree(w->tq); cudaFree(w->ctr);
     delete w;
     s.wave = nullptr;
@@ -459,15 +512,7 @@ static cudaError_t wave_reserve(DeviceScene& s, int nsamples) {
     int dev_id = 0, sms = 148;
     cudaGetDevice(&dev_id);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id);
-    int b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dev::wave_primary, 128, 0);
-    w->grid_primary = sms * std::max(b, 1);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dev::wave_shadow, 128, 0);
-    w->grid_shadow = sms * std::max(b, 1);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dev::wave_reflect, 128, 0);
-    w->grid_reflect = sms * std::max(b, 1);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dev::wave_refract, 128, 0);
-    w->grid_refract = sms * std::max(b, 1);
+    w->sms = sms;
     s.wave = w;
     return cudaSuccess;
 }
@@ -500,21 +545,30 @@ cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, fl
         V.pix_angle = 2.0f * tan_x / (float)W;
     }
     V.count_rays = 1;
-    if ((e = cudaMemsetAsync(w->ctr, 0, dev::kCounterWords * sizeof(unsigned int), stream)) != cudaSuccess) return e;
-    dev::wave_primary<<<w->grid_primary, 128, 0, stream>>>(s.view, V);
-    dev::wave_shadow<<<w->grid_shadow, 128, 0, stream>>>(s.view, V);
-    if ((e = cudaMemsetAsync(&w->ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
-    dev::wave_reflect<<<w->grid_reflect, 128, 0, stream>>>(s.view, V);
-    dev::wave_shadow<<<w->grid_shadow, 128, 0, stream>>>(s.view, V);
-    if ((e = cudaMemsetAsync(&w->ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
-    dev::wave_refract<<<w->grid_refract, 128, 0, stream>>>(s.view, V);
-    dev::wave_shadow<<<w->grid_shadow, 128, 0, stream>>>(s.view, V);
-    const int npix = rw * rh;
-    (void)npix;
-    const int npad = (int)(padded);
-    dev::wave_resolve<<<(npad + 127) / 128, 128, 0, stream>>>(V, out);
-    dev::wave_tally_out<<<1, 1, 0, stream>>>(V, s.d_tally);
-    return cudaGetLastError();
+    const dev::DevScene& sv = s.view;
+    const bool simple = sv.num_strands == 0 && sv.num_hfs == 0 && sv.num_ses == 0 && sv.num_lathes == 0 &&
+                        sv.num_prisms == 0 && sv.csg_root < 0;
+    // Replay the captured frame when the shape and output match; otherwise
+    // capture the sequence on the scene's own stream and instantiate it.
+    const Wave::Key key{W, H, aa, rg.x0, rg.y0, rg.x1, rg.y1, out};
+    if (!w->exec || !(w->key == key)) {
+        if (w->exec) { cudaGraphExecDestroy(w->exec); w->exec = nullptr; }
+        if (!w->capture_stream &&
+            (e = cudaStreamCreateWithFlags(&w->capture_stream, cudaStreamNonBlocking)) != cudaSuccess)
+            return e;
+        if ((e = cudaStreamBeginCapture(w->capture_stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+        cudaError_t le = simple ? run_pipeline<dev::kCatSimple>(s, V, (int)padded, out, w->capture_stream)
+                                : run_pipeline<dev::kCatAll>(s, V, (int)padded, out, w->capture_stream);
+        cudaGraph_t graph = nullptr;
+        e = cudaStreamEndCapture(w->capture_stream, &graph);
+        if (le != cudaSuccess) { if (graph) cudaGraphDestroy(graph); return le; }
+        if (e != cudaSuccess) return e;
+        e = cudaGraphInstantiate(&w->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) { w->exec = nullptr; return e; }
+        w->key = key;
+    }
+    return cudaGraphLaunch(w->exec, stream);
 }
 
 }  // namespace sheen
