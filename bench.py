@@ -150,7 +150,10 @@ def run_ours(args):
     # counting frame: rays per frame and the traversal counters
     st = ds.render_device(W, H, SPP, out.data_ptr(), stream, count_rays=True)
     rays = st["total_rays"]
-    nodes, prims = st["node_visits"], st["prim_tests"]
+    # box/primitive test counts: one instrumented frame of the same traversal
+    stn = ds.render_device(W, H, SPP, out.data_ptr(), stream, count_nodes=True)
+    nodes, prims = stn["node_visits"], stn["prim_tests"]
+    assert stn["total_rays"] == rays or form == sb.FORM_WAVEFRONT
 
     for _ in range(args.warmup):
         ds.render_device(W, H, SPP, out.data_ptr(), stream)

@@ -123,7 +123,9 @@ enum {
 
 /* Render flags. */
 enum {
-    SHEEN_RENDER_COUNT_RAYS = 1   /* fill SheenRenderStats ray and node counters */
+    SHEEN_RENDER_COUNT_RAYS = 1,  /* fill SheenRenderStats ray counters */
+    SHEEN_RENDER_COUNT_NODES = 2  /* also count box and primitive tests (instrumented
+                                     megakernel of the form's traversal; slower) */
 };
 
 typedef struct SheenRenderStats {

@@ -30,6 +30,11 @@ LIB_PATH = os.path.join(_HERE, "libsheen_c_api.so")
 FORM_PLAIN = 0
 FORM_WAVEFRONT = 1
 RENDER_COUNT_RAYS = 1
+RENDER_COUNT_NODES = 2
+
+
+def _flags(count_rays, count_nodes):
+    return (RENDER_COUNT_RAYS if count_rays else 0) | (RENDER_COUNT_NODES if count_nodes else 0)
 
 _lib = None
 
@@ -169,19 +174,20 @@ class DeviceScene:
     def device_bytes(self) -> int:
         return int(lib().sheen_scene_device_bytes(self.handle))
 
-    def render_host(self, width, height, aa, count_rays=False):
+    def render_host(self, width, height, aa, count_rays=False, count_nodes=False):
         out = np.empty((height, width, 4), np.float32)
         st = RenderStats()
         _check(lib().sheen_scene_render_host(self.handle, width, height, aa, out.ctypes.data,
-                                             RENDER_COUNT_RAYS if count_rays else 0, ctypes.byref(st)))
+                                             _flags(count_rays, count_nodes), ctypes.byref(st)))
         return out, st.as_dict()
 
-    def render_device(self, width, height, aa, out_ptr: int, stream: int = 0, count_rays=False, stats=False):
-        """Render into a device buffer (width*height float4).  With count_rays
-        or stats the call synchronises and returns the stats dict."""
-        st = RenderStats() if (stats or count_rays) else None
+    def render_device(self, width, height, aa, out_ptr: int, stream: int = 0, count_rays=False, stats=False,
+                      count_nodes=False):
+        """Render into a device buffer (width*height float4).  With count_rays,
+        count_nodes or stats the call synchronises and returns the stats."""
+        st = RenderStats() if (stats or count_rays or count_nodes) else None
         _check(lib().sheen_scene_render_device(self.handle, width, height, aa, out_ptr, stream,
-                                               RENDER_COUNT_RAYS if count_rays else 0,
+                                               _flags(count_rays, count_nodes),
                                                ctypes.byref(st) if st is not None else None))
         return st.as_dict() if st is not None else None
 
@@ -191,7 +197,7 @@ class DeviceScene:
         device buffer at out_ptr (whole image, width*height float4)."""
         st = RenderStats() if (stats or count_rays) else None
         _check(lib().sheen_scene_render_region(self.handle, width, height, aa, x0, y0, x1, y1, out_ptr, stream,
-                                               RENDER_COUNT_RAYS if count_rays else 0,
+                                               _flags(count_rays, False),
                                                ctypes.byref(st) if st is not None else None))
         return st.as_dict() if st is not None else None
 

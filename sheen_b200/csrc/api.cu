@@ -57,7 +57,7 @@ int render_device(sheen::DeviceScene& s, int W, int H, int aa, sheen::Region rg,
         sheen::set_error("bad render region");
         return -1;
     }
-    const bool want_stats = stats != nullptr || (flags & SHEEN_RENDER_COUNT_RAYS);
+    const bool want_stats = stats != nullptr || (flags & (SHEEN_RENDER_COUNT_RAYS | SHEEN_RENDER_COUNT_NODES));
     cudaError_t e;
     if (want_stats) {
         e = cudaMemsetAsync(s.d_tally, 0, 8 * sizeof(unsigned long long), stream);
@@ -70,9 +70,9 @@ int render_device(sheen::DeviceScene& s, int W, int H, int aa, sheen::Region rg,
         cudaEventRecord(ev0, stream);
     }
     if (s.form == SHEEN_FORM_PLAIN)
-        e = sheen::launch_plain(s, W, H, aa, rg, out, stream, (flags & SHEEN_RENDER_COUNT_RAYS) != 0);
+        e = sheen::launch_plain(s, W, H, aa, rg, out, stream, (flags & SHEEN_RENDER_COUNT_NODES) != 0);
     else
-        e = sheen::launch_wavefront(s, W, H, aa, rg, out, stream, (flags & SHEEN_RENDER_COUNT_RAYS) != 0);
+        e = sheen::launch_wavefront(s, W, H, aa, rg, out, stream, (flags & SHEEN_RENDER_COUNT_NODES) != 0);
     if (e != cudaSuccess) return fail_cuda(e);
     if (want_stats) {
         cudaEventRecord(ev1, stream);

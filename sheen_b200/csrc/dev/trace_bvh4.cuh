@@ -103,8 +103,11 @@ template <bool ANY, bool COUNT>
 __device__ __forceinline__ int qmesh_trace(const QMesh& m, const QRay& r, float tmax, float& t_best, float& bu,
                                            float& bv, Counters& c) {
     if (!m.nodes) return -1;
+    // Any-hit walks need no visiting order: their stack holds entries only.
+    // Closest-hit walks visit children near to far and keep each pushed
+    // entry's distance so that entries behind the current hit are dropped.
     uint32_t stack_e[kQStack];
-    float stack_t[kQStack];
+    float stack_t[ANY ? 1 : kQStack];
     int sp = 0;
     uint32_t entry = 0;   // root (inner)
     int best = -1;
@@ -115,29 +118,41 @@ __device__ __forceinline__ int qmesh_trace(const QMesh& m, const QRay& r, float 
             if (COUNT) c.nodes++;
             const int mask = qnode_children(m.nodes, (int)entry, r, t_best, tn, ch);
             const uint32_t cid[4] = {ch.x, ch.y, ch.z, ch.w};
-            // Order hit children near to far: keys = distance bits with the slot
-            // in the low 2 bits (entry distances are >= tmin > 0, so their
-            // bit patterns order like the values).
-            uint32_t key[4];
-            int n = 0;
+            if (mask == 0) goto pop;
+            if constexpr (ANY) {
+                int first = -1;
 #pragma unroll
-            for (int i = 0; i < 4; i++)
-                if (mask & (1 << i)) key[n++] = (__float_as_uint(fmaxf(tn[i], 0.0f)) & ~3u) | (uint32_t)i;
-            if (n == 0) goto pop;
-#define CSWAP(a, b) if (key[a] > key[b]) { uint32_t t_ = key[a]; key[a] = key[b]; key[b] = t_; }
-            if (n == 2) { CSWAP(0, 1) }
-            else if (n == 3) { CSWAP(0, 1) CSWAP(1, 2) CSWAP(0, 1) }
-            else if (n == 4) { CSWAP(0, 1) CSWAP(2, 3) CSWAP(0, 2) CSWAP(1, 3) CSWAP(1, 2) }
-#undef CSWAP
-            for (int k = n - 1; k >= 1; k--) {
-                if (sp < kQStack) {
-                    stack_e[sp] = cid[key[k] & 3u];
-                    stack_t[sp] = tn[key[k] & 3u];
-                    sp++;
+                for (int i = 0; i < 4; i++) {
+                    if (!(mask & (1 << i))) continue;
+                    if (first < 0) first = i;
+                    else if (sp < kQStack) stack_e[sp++] = cid[i];
                 }
+                entry = cid[first];
+                continue;
+            } else {
+                // keys = distance bits with the slot in the low 2 bits (entry
+                // distances are >= 0 here, so their bit patterns order like
+                // the values)
+                uint32_t key[4];
+                int n = 0;
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+                    if (mask & (1 << i)) key[n++] = (__float_as_uint(fmaxf(tn[i], 0.0f)) & ~3u) | (uint32_t)i;
+#define CSWAP(a, b) if (key[a] > key[b]) { uint32_t t_ = key[a]; key[a] = key[b]; key[b] = t_; }
+                if (n == 2) { CSWAP(0, 1) }
+                else if (n == 3) { CSWAP(0, 1) CSWAP(1, 2) CSWAP(0, 1) }
+                else if (n == 4) { CSWAP(0, 1) CSWAP(2, 3) CSWAP(0, 2) CSWAP(1, 3) CSWAP(1, 2) }
+#undef CSWAP
+                for (int k = n - 1; k >= 1; k--) {
+                    if (sp < kQStack) {
+                        stack_e[sp] = cid[key[k] & 3u];
+                        stack_t[sp] = tn[key[k] & 3u];
+                        sp++;
+                    }
+                }
+                entry = cid[key[0] & 3u];
+                continue;
             }
-            entry = cid[key[0] & 3u];
-            continue;
         } else {
             const int first = (int)((entry & 0x7fffffffu) >> 3);
             const int count = (int)(entry & 7u) + 1;
@@ -156,10 +171,15 @@ __device__ __forceinline__ int qmesh_trace(const QMesh& m, const QRay& r, float 
             }
         }
     pop:
-        while (true) {
+        if constexpr (ANY) {
             if (sp == 0) return best;
-            --sp;
-            if (stack_t[sp] <= t_best) { entry = stack_e[sp]; break; }
+            entry = stack_e[--sp];
+        } else {
+            while (true) {
+                if (sp == 0) return best;
+                --sp;
+                if (stack_t[sp] <= t_best) { entry = stack_e[sp]; break; }
+            }
         }
     }
 }
