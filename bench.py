@@ -226,6 +226,8 @@ def run_ours(args):
     }
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(ds, scene, stream, out)
+    if rank == 0 and not args.no_ref_gpu:
+        line["reference_gpu"] = reference_gpu(scene, rays)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ds.close()
@@ -263,6 +265,35 @@ def cpu_baseline(ds, scene, stream, out, steps=1):
     return {"value": round(rays * steps / dt / 1e6, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
             "sample": f"rows {CPU_BAND[0]}-{CPU_BAND[1]} of the 1920x1080 4 spp frame ({rays} rays), "
                       f"{steps} pass(es), {dt:.1f} s"}
+
+
+def reference_gpu(scene, rays, steps=3):
+    """The reference's own CUDA kernel (render_kernel.cu compiled unchanged for
+    sm_100a, oracle/_ref/libsheen_ref_gpu.so) on the same frame, same GPU."""
+    import ctypes
+    path = os.path.join(ROOT, "oracle", "_ref", "libsheen_ref_gpu.so")
+    if not os.path.exists(path):
+        return {"value": None, "unavailable": "oracle/_ref/libsheen_ref_gpu.so not built"}
+    L = ctypes.CDLL(path)
+    L.sheen_refgpu_scene_create.argtypes = [ctypes.c_void_p]
+    L.sheen_refgpu_scene_create.restype = ctypes.c_void_p
+    L.sheen_refgpu_render.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                      ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    L.sheen_refgpu_render.restype = ctypes.c_int
+    L.sheen_refgpu_scene_destroy.argtypes = [ctypes.c_void_p]
+    h = L.sheen_refgpu_scene_create(scene.view_ptr)
+    if not h:
+        return {"value": None, "unavailable": "reference scene upload failed"}
+    ms = ctypes.c_float(0.0)
+    L.sheen_refgpu_render(h, W, H, SPP, None, 1, ctypes.byref(ms))          # warm-up
+    rc = L.sheen_refgpu_render(h, W, H, SPP, None, steps, ctypes.byref(ms))
+    L.sheen_refgpu_scene_destroy(h)
+    if rc != 0:
+        return {"value": None, "unavailable": "reference kernel launch failed"}
+    frame_ms = ms.value / steps
+    return {"value": round(rays / (frame_ms / 1e3) / 1e6, 2), "unit": "Mrays/s", "ms_per_frame": round(frame_ms, 2),
+            "kernel": "reference render_kernel (render_kernel.cu:438-814) built for sm_100a, 16x16 blocks, "
+                      "16 KB stack limit", "rays": "this renderer's count for the frame (same queries)"}
 
 
 def run_reference(args):
@@ -322,6 +353,7 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--photons", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

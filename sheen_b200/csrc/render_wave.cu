@@ -196,7 +196,11 @@ __global__ void __launch_bounds__(128) wave_primary(DevScene S, WaveView V) {
         float w = 0.0f, gtr = 0.0f;
         if (active) {
             if (!hit) {
-                put_slot(V, seg_base(V, i, 0), sky(ray.d));
+                // sky: the segment's light and caustic slots are summed by the
+                // resolve too, so they are cleared here
+                const int sb = seg_base(V, i, 0);
+                put_slot(V, sb, sky(ray.d));
+                for (int l = 0; l < V.L + 1; l++) put_slot(V, sb + 1 + l, f3(0.0f, 0.0f, 0.0f));
                 V.coef[3 * (size_t)i] = 1.0f;
                 V.coef[3 * (size_t)i + 1] = 0.0f;
                 V.coef[3 * (size_t)i + 2] = 0.0f;

@@ -113,6 +113,18 @@ def test_deterministic_and_resident(form):
     ds.close()
 
 
+def test_reused_buffers_do_not_leak_between_frames():
+    """A resident wavefront scene reuses its queues and slots across frames;
+    a frame must not read anything a previous frame of another shape left."""
+    s = sb.generate_scene(0, 4)
+    ds = sb.DeviceScene(s, sb.FORM_WAVEFRONT)
+    ds.render_host(96, 72, 4)                 # fills the buffers
+    a, _ = ds.render_host(64, 48, 1)          # smaller frame on the same buffers
+    ds.close()
+    b, _ = sb.render_rgba(s, 64, 48, 1, sb.FORM_WAVEFRONT)   # fresh buffers
+    assert np.array_equal(a, b)
+
+
 def test_forms_agree_on_rays_and_pixels():
     case = next(c for c in CASES if c["name"] == "mesh_l3")
     s = load_case(case)
