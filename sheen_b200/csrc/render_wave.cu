@@ -32,6 +32,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "dev/integrator.cuh"
 #include "dev/trace_bvh4.cuh"
@@ -575,4 +576,163 @@ cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, fl
     return cudaGraphLaunch(w->exec, stream);
 }
 
+// ---------------------------------------------------------------------
+// Allocation-free rendering of a small region (sheen_scene_render_region_noalloc).
+//
+// Some callers cannot let the library allocate GPU memory while they draw:
+// a host that records its frame into a CUDA graph (cudaMalloc is not allowed
+// while a stream is being captured), a real-time loop that reserves all of
+// its device memory at start-up and treats any later allocation as a fault,
+// or an embedding application whose memory manager must own every byte.
+// The regular entry points allocate the wavefront queues on first use and a
+// frame-sized output on the host path, so they cannot be used there.  This
+// variant runs the same wavefront kernels with their scratch (per-sample
+// light slots, blend weights, the three ray queues and their counters)
+// placed in one fixed array in the library's device globals instead.
+//
+// Limits: at most kNoAllocMaxSamples samples per call (the region's pixels
+// rounded up to whole 16x8 tiles, times the samples per pixel -- e.g. a
+// 128x128 tile at 1 spp or 64x64 at 4 spp) and scenes with at most
+// kNoAllocMaxLights lights.  The array (about 13 MB) is held on every GPU
+// that loads the library until the process exits.  Every call uses the same
+// array: calls that can overlap on the GPU (different streams, or threads
+// issuing concurrently) race and must be serialised by the caller, e.g. by
+// issuing them on one stream.
+// ---------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocMaxSamples = 16384;
+constexpr int kNoAllocMaxLights = 8;
+constexpr size_t kNoAllocSlotFloats = (size_t)kNoAllocMaxSamples * 3 * (kNoAllocMaxLights + 2) * 3;
+constexpr size_t kNoAllocCoefFloats = (size_t)kNoAllocMaxSamples * 3;
+constexpr size_t kNoAllocShadowEntries = (size_t)kNoAllocMaxSamples * kNoAllocMaxLights;
+constexpr size_t kNoAllocOffSlots = 0;
+constexpr size_t kNoAllocOffCoef = kNoAllocOffSlots + kNoAllocSlotFloats * sizeof(float);
+constexpr size_t kNoAllocOffShq = (kNoAllocOffCoef + kNoAllocCoefFloats * sizeof(float) + 255) & ~(size_t)255;
+constexpr size_t kNoAllocOffRq = kNoAllocOffShq + kNoAllocShadowEntries * 3 * sizeof(float4);
+constexpr size_t kNoAllocOffTq = kNoAllocOffRq + (size_t)kNoAllocMaxSamples * 2 * sizeof(float4);
+constexpr size_t kNoAllocOffCtr = kNoAllocOffTq + (size_t)kNoAllocMaxSamples * 2 * sizeof(float4);
+constexpr size_t kNoAllocBytes = kNoAllocOffCtr + dev::kCounterWords * sizeof(unsigned int);
+
+// The scratch itself.  Host code must not use this name as an address (on
+// the host it names a stand-in, not device memory); noalloc_scratch() below
+// resolves the device address.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+
+// Device address of the scratch array on the current device, looked up once
+// per device (the first call on a device does this; it must not be inside a
+// stream capture).
+cudaError_t noalloc_scratch(unsigned char** out) {
+    int dev_id = 0;
+    cudaError_t e = cudaGetDevice(&dev_id);
+    if (e != cudaSuccess) return e;
+    if (dev_id < 0 || dev_id >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev_id]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[dev_id] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_ptr[dev_id];
+    return cudaSuccess;
+}
+
+template <int F>
+cudaError_t noalloc_pipeline(const DeviceScene& s, const dev::WaveView& V, int npad, float4* out,
+                             cudaStream_t stream) {
+    static int g_sms = 0, g_primary = 0, g_shadow = 0, g_reflect = 0, g_refract = 0;
+    if (!g_primary) {
+        int dev_id = 0;
+        cudaGetDevice(&dev_id);
+        cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev_id);
+        g_primary = persistent_grid(dev::wave_primary<F>, g_sms);
+        g_shadow = persistent_grid(dev::wave_shadow<F>, g_sms);
+        g_reflect = persistent_grid(dev::wave_reflect<F>, g_sms);
+        g_refract = persistent_grid(dev::wave_refract<F>, g_sms);
+    }
+    cudaError_t e;
+    // The queue counters are the only scratch that must start at zero.
+    if ((e = cudaMemsetAsync(V.ctr, 0, dev::kCounterWords * sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    dev::wave_primary<F><<<g_primary, 128, 0, stream>>>(s.view, V);
+    dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
+    if ((e = cudaMemsetAsync(&V.ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    dev::wave_reflect<F><<<g_reflect, 128, 0, stream>>>(s.view, V);
+    dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
+    if ((e = cudaMemsetAsync(&V.ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    dev::wave_refract<F><<<g_refract, 128, 0, stream>>>(s.view, V);
+    dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
+    dev::wave_resolve<<<(npad + 127) / 128, 128, 0, stream>>>(V, out);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
 }  // namespace sheen
+
+extern "C" int sheen_scene_render_region_noalloc(SheenDeviceScene h, int W, int H, int aa, int x0, int y0, int x1,
+                                                 int y1, float* out_rgba_device, void* stream) {
+    using namespace sheen;
+    auto* s = reinterpret_cast<DeviceScene*>(h);
+    if (!s) { set_error("null scene handle"); return -1; }
+    if (W <= 0 || H <= 0 || aa < 1 || aa > 64 || !out_rgba_device) { set_error("bad render params"); return -1; }
+    if (x0 < 0 || y0 < 0 || x1 > W || y1 > H || x0 >= x1 || y0 >= y1) { set_error("bad render region"); return -1; }
+    if (s->form != SHEEN_FORM_WAVEFRONT) {
+        set_error("allocation-free rendering needs a scene created with SHEEN_FORM_WAVEFRONT");
+        return -1;
+    }
+    const int rw = x1 - x0, rh = y1 - y0;
+    const long long padded = (long long)((rw + 15) / 16) * 16 * ((rh + 7) / 8) * 8;
+    const long long nsamples = padded * aa;
+    if (nsamples > kNoAllocMaxSamples) {
+        set_error("region too large for allocation-free rendering: at most 16384 samples per call "
+                  "(pixels rounded up to whole 16x8 tiles, times samples per pixel)");
+        return -1;
+    }
+    if (s->view.num_lights > kNoAllocMaxLights) {
+        set_error("allocation-free rendering supports at most 8 lights");
+        return -1;
+    }
+    const cudaStream_t st = (cudaStream_t)stream;
+    float4* out = reinterpret_cast<float4*>(out_rgba_device);
+    cudaError_t e;
+    if (!wave_supported(*s)) {
+        // Beams, media and the shadow-debug mode run on the BVH4 megakernel,
+        // which needs no scratch at all.
+        e = launch_mega_bvh4(*s, W, H, aa, Region{x0, y0, x1, y1}, out, st, false);
+        if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return -1; }
+        return 0;
+    }
+    unsigned char* base = nullptr;
+    if ((e = noalloc_scratch(&base)) != cudaSuccess) { set_error(cudaGetErrorString(e)); return -1; }
+    dev::WaveView V;
+    V.slots = reinterpret_cast<float*>(base + kNoAllocOffSlots);
+    V.coef = reinterpret_cast<float*>(base + kNoAllocOffCoef);
+    V.shq = reinterpret_cast<float4*>(base + kNoAllocOffShq);
+    V.rq = reinterpret_cast<float4*>(base + kNoAllocOffRq);
+    V.tq = reinterpret_cast<float4*>(base + kNoAllocOffTq);
+    V.ctr = reinterpret_cast<unsigned int*>(base + kNoAllocOffCtr);
+    V.L = s->view.num_lights;
+    V.ns = aa;
+    V.W = W; V.H = H; V.x0 = x0; V.y0 = y0; V.rw = rw; V.rh = rh;
+    V.nsamples = (int)nsamples;
+    const CameraData& cam = s->view.cam;
+    float tan_x = 1.0f;
+    if (cam.focal_length > 0.0f) {
+        const float tan_h = 0.5f * cam.sensor_width / cam.focal_length;
+        tan_x = (W >= H) ? tan_h : tan_h * float(W) / float(H);
+    }
+    V.pix_angle = 2.0f * tan_x / (float)W;
+    V.count_rays = 0;
+    const dev::DevScene& sv = s->view;
+    const bool simple = sv.num_strands == 0 && sv.num_hfs == 0 && sv.num_ses == 0 && sv.num_lathes == 0 &&
+                        sv.num_prisms == 0 && sv.csg_root < 0;
+    e = simple ? noalloc_pipeline<dev::kCatSimple>(*s, V, (int)padded, out, st)
+               : noalloc_pipeline<dev::kCatAll>(*s, V, (int)padded, out, st);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return -1; }
+    return 0;
+}
