@@ -40,7 +40,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 W, H, SPP = 1920, 1080, 4
-CPU_BAND = (480, 512)      # pixel rows of the CPU samples (two 16-row blocks)
+CPU_BAND = (480, 512)      # pixel rows of the CPU samples (two 16-row blocks of the 1080-row frame)
 
 
 def peaks():
@@ -127,9 +127,29 @@ def barrier(world):
         dist.barrier()
 
 
+WORKLOADS = {
+    0: "spheres: 64 seeded spheres + ground plane + 1 point light, reflect 0.3, 640x480, 1 spp",
+    1: "mesh: displaced icosphere L8 (1,310,720 tris) + 16 displaced 50k-tri tori, 1920x1080, 4 spp, "
+       "4 point lights, reflect 0.2, 4 glass tori ior 1.5",
+    2: "analytic: 258 superellipsoids, 64 Bezier lathes, 64 Bezier prisms, 32 Catmull-Rom sweeps, "
+       "fBm heightfield, depth-3 CSG tree; 1920x1080, 4 spp",
+    3: "caustics: glass sphere + glass lathe over a diffuse plane, 1 spot light, 4M photons (hash grid, "
+       "cell 0.2), 1920x1080, 16 spp",
+}
+
+
 def make_scene(args):
+    """The workload's scene; sets the frame size and spp from the generator."""
     import sheen_b200 as sb
-    return sb.generate_scene(args.config, args.seed, args.detail, args.photons)
+    global W, H, SPP
+    photons = args.photons if args.photons > 0 else (4000000 if args.config == 3 else 0)
+    scene = sb.generate_scene(args.config, args.seed, args.detail if args.config == 1 else 0, photons)
+    st = scene.settings
+    W, H, SPP = st["width"], st["height"], st["aa"]
+    global CPU_BAND
+    y0 = (H // 2) // 16 * 16
+    CPU_BAND = (y0, min(H, y0 + 32))
+    return scene
 
 
 def run_ours(args):
@@ -203,8 +223,7 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(frame_ms, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generator)",
-        "config": {"workload": "mesh: displaced icosphere L8 (1,310,720 tris) + 16 displaced 50k-tri tori, "
-                               "1920x1080, 4 spp, 4 point lights, reflect 0.2, 4 glass tori ior 1.5",
+        "config": {"workload": WORKLOADS.get(args.config, f"config {args.config}"),
                    "triangles": scene.view.num_triangles, "width": W, "height": H, "spp": SPP,
                    "form": args.form, "parallelism": f"replicas{world}",
                    "l2": "256 MB buffer written between timed frames; scene arrays exceed L2",
@@ -333,7 +352,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generator)",
-        "config": {"workload": "mesh: displaced icosphere L8 + 16 tori, 1920x1080, 4 spp (row band sample)",
+        "config": {"workload": WORKLOADS.get(args.config, "") + " (row band sample)",
                    "rays_per_step": rays},
         "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
                          "sample": sample},

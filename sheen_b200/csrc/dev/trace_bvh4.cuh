@@ -41,7 +41,15 @@ __device__ __forceinline__ QRay make_qray(const Ray& r) {
     return q;
 }
 
-__device__ __forceinline__ uint32_t byte_of(uint32_t w, int i) { return (w >> (8 * i)) & 0xffu; }
+// Byte i of w as a float: one byte permute builds the float 2^23 + byte
+// (exponent bits 0x4B in the top byte), one add removes 2^23.  Exact for
+// every byte value.
+__device__ __forceinline__ float byte_as_float(uint32_t w, int i) {
+    // selector nibbles pick result bytes (low to high): byte i of w, then
+    // zero, zero, 0x4B from the second operand (bytes 4..7 = 00 00 00 4B)
+    const uint32_t sel = (uint32_t)i | 0x7440u;
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, sel)) - 8388608.0f;
+}
 
 // Tests the up-to-4 children of `node`; returns a bit mask of hit children
 // and their entry distances.
@@ -64,9 +72,9 @@ __device__ __forceinline__ int qnode_children(const QNode4* __restrict__ nodes, 
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         if (i >= count) break;
-        const float x0 = fmaf((float)byte_of(qb.x, i), ax, bx), x1 = fmaf((float)byte_of(qb.y, i), ax, bx);
-        const float y0 = fmaf((float)byte_of(qb.z, i), ay, by), y1 = fmaf((float)byte_of(qb.w, i), ay, by);
-        const float z0 = fmaf((float)byte_of(qz.x, i), az, bz), z1 = fmaf((float)byte_of(qz.y, i), az, bz);
+        const float x0 = fmaf(byte_as_float(qb.x, i), ax, bx), x1 = fmaf(byte_as_float(qb.y, i), ax, bx);
+        const float y0 = fmaf(byte_as_float(qb.z, i), ay, by), y1 = fmaf(byte_as_float(qb.w, i), ay, by);
+        const float z0 = fmaf(byte_as_float(qz.x, i), az, bz), z1 = fmaf(byte_as_float(qz.y, i), az, bz);
         const float tnear = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), r.tmin));
         const float texit = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tfar));
         // widen by 2^-20 relative (texit grows, tnear shrinks)
