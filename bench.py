@@ -360,6 +360,131 @@ def run_reference(args):
     }), flush=True)
 
 
+SERVE_WORKLOAD = ("serving: Poisson request stream at 20/s, each request a scene of the spheres / mesh / "
+                  "analytic / caustics generators (4 seeds each, resident on the device), resolution from "
+                  "{256^2, 512^2, 1280x720, 1920x1080, 2048^2}, spp from {1, 4, 16, 64}")
+
+
+def _serving_scene(config, seed):
+    import sheen_b200 as sb
+    photons = 4000000 if config == 3 else 0
+    return sb.generate_scene(config, seed, 8 if config == 1 else 0, photons)
+
+
+def run_serving(args):
+    """The request loop under the serving stream: requests are submitted at
+    their arrival times from a seeded Poisson stream and the server admits,
+    overlaps and completes them; every request's image lands in a host
+    buffer.  value = all rays of all requests / (last completion - first
+    arrival); p50/p99 of per-request latency (arrival -> image in host
+    memory).  The serial plain-form baseline renders a prefix of the same
+    stream one request at a time through a plain-form server."""
+    rank = int(os.environ.get("RANK", "0"))
+    import torch
+
+    import sheen_b200 as sb
+    from sheen_b200 import serve
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    sb.init(local, 100)
+    stream = serve.request_stream(args.requests, args.rate, seed=args.seed)
+    keys = sorted({(r["config"], r["seed"]) for r in stream})
+    t0 = time.perf_counter()
+    host_scenes = {k: _serving_scene(*k) for k in keys}
+    gen_s = time.perf_counter() - t0
+    srv = serve.Server(sb.FORM_WAVEFRONT, max_inflight=args.inflight)
+    t0 = time.perf_counter()
+    sid = {k: srv.add_scene(host_scenes[k]) for k in keys}
+    add_s = time.perf_counter() - t0
+    # warm-up: one small request per scene (kernels loaded, pool primed)
+    for k in keys:
+        srv.submit(sid[k], 256, 256, 1).wait()
+    for _ in range(max(0, args.warmup - 1)):
+        srv.submit(sid[keys[0]], 512, 512, 4).wait()
+    base = srv.stats()
+
+    reqs = [None] * len(stream)
+    infos = [None] * len(stream)
+
+    def collect():
+        for i in range(len(stream)):
+            while reqs[i] is None:
+                time.sleep(0.0005)
+            _, infos[i] = reqs[i].wait()
+            reqs[i].image = None          # the image was delivered; drop it
+
+    th = threading.Thread(target=collect)
+    th.start()
+    with ClockSampler(local) as clk:
+        t_start = time.perf_counter()
+        for i, r in enumerate(stream):
+            delay = t_start + r["t"] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            reqs[i] = srv.submit(sid[(r["config"], r["seed"])], r["width"], r["height"], r["spp"])
+        th.join()
+        wall_s = time.perf_counter() - t_start
+    st = srv.stats()
+    rays = sum(i["rays"] for i in infos)
+    lat = np.array([i["latency_ms"] for i in infos])
+    value = rays / wall_s / 1e6
+
+    # serial plain-form baseline on a prefix of the stream
+    k = min(args.serial_sample, len(stream))
+    psrv = serve.Server(sb.FORM_PLAIN, max_inflight=1)
+    pkeys = sorted({(r["config"], r["seed"]) for r in stream[:k]})
+    psid = {kk: psrv.add_scene(host_scenes[kk]) for kk in pkeys}
+    psrv.submit(psid[pkeys[0]], 256, 256, 1).wait()
+    t0 = time.perf_counter()
+    prays = 0
+    for r in stream[:k]:
+        _, info = psrv.submit(psid[(r["config"], r["seed"])], r["width"], r["height"], r["spp"]).wait()
+        prays += info["rays"]
+    plain_s = time.perf_counter() - t0
+    psrv.close()
+    # the chosen form serially on the same prefix (what overlap adds)
+    t0 = time.perf_counter()
+    wrays = 0
+    for r in stream[:k]:
+        _, info = srv.submit(sid[(r["config"], r["seed"])], r["width"], r["height"], r["spp"]).wait()
+        wrays += info["rays"]
+    wave_serial_s = time.perf_counter() - t0
+    srv.close()
+    clocks = clk.summary()
+    if rank != 0:
+        return
+    n = len(stream)
+    line = {
+        "metric": "Mrays/s (serving)", "value": round(value, 2), "unit": "Mrays/s", "n_gpus": 1,
+        "steps": n, "warmup": args.warmup, "ms_per_step": round(wall_s * 1e3 / n, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generators, seeded request stream)",
+        "config": {"workload": SERVE_WORKLOAD, "requests": n, "rate_per_s": args.rate, "scenes": len(keys),
+                   "max_inflight": args.inflight, "form": "wavefront",
+                   "l2": "inputs (2.1M-triangle scenes, 4M-photon maps) exceed L2; no flush between requests",
+                   "scene_generate_s": round(gen_s, 2), "scene_add_s": round(add_s, 2),
+                   "scene_bytes": st["scene_bytes"], "hbm_budget": st["hbm_budget"],
+                   "hbm_peak": st["hbm_peak"], "inflight_peak": st["inflight_peak"]},
+        "latency_ms": {"p50": round(float(np.percentile(lat, 50, method="inverted_cdf")), 2),
+                       "p99": round(float(np.percentile(lat, 99, method="inverted_cdf")), 2),
+                       "mean": round(float(lat.mean()), 2), "max": round(float(lat.max()), 2),
+                       "queue_mean": round(float(np.mean([i["queue_ms"] for i in infos])), 2),
+                       "run_mean": round(float(np.mean([i["run_ms"] for i in infos])), 2)},
+        "serial_plain": {"value": round(prays / plain_s / 1e6, 2), "unit": "Mrays/s",
+                         "sample": f"first {k} requests of the stream, one at a time, plain form, "
+                                   f"scenes resident ({prays} rays, {plain_s:.1f} s)"},
+        "serial_wavefront": {"value": round(wrays / wave_serial_s / 1e6, 2), "unit": "Mrays/s",
+                             "sample": f"same {k} requests one at a time through the wavefront server"},
+        "e2e": {"value": round(value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(sum(r["width"] * r["height"] * 16 for r in stream) / n),
+                "call": "sheen_server_submit / sheen_server_wait, images into host buffers"},
+        "gpu_launches": int(sum(i["tiles"] for i in infos) * 8),
+        "clocks": clocks,
+        "server_stats": {kk: st[kk] for kk in ("completed", "failed", "p50_ms", "p99_ms", "busy_ms")},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -373,11 +498,17 @@ def main():
     ap.add_argument("--photons", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--requests", type=int, default=512, help="serving config: requests in the stream")
+    ap.add_argument("--rate", type=float, default=20.0, help="serving config: arrivals per second")
+    ap.add_argument("--inflight", type=int, default=4, help="serving config: requests on the GPU at once")
+    ap.add_argument("--serial-sample", type=int, default=24, help="serving config: serial baseline prefix")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == 4:
+        run_serving(args)
     else:
         run_ours(args)
 

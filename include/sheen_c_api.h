@@ -256,6 +256,85 @@ int sheen_generate_scene(int config, unsigned int seed, int detail, int photons,
 /* 8-bit sRGB PNG writer used by sheen_render_scene (png_color.h:11-20 conversion). */
 int sheen_write_png_srgb(const char* path, const float* rgba, int width, int height);
 
+/* ------------------------------------------------------------------ */
+/* Request loop (continuous batching).  No counterpart in the reference, */
+/* whose C-ABI renders one frame per call and rebuilds and re-uploads   */
+/* the scene every time (api/sheen_c_api.cu:187-361).                   */
+/* ------------------------------------------------------------------ */
+
+/* A server owns resident scenes and renders requests against them.  Each
+ * request (scene, width, height, spp, caller's host buffer) is queued on
+ * submit and admitted onto the GPU when one of max_inflight slots (one CUDA
+ * stream each) is free and its device footprint -- wavefront queues for one
+ * band of rows plus the band's output -- fits in the HBM budget beside the
+ * resident scenes; requests that arrive while others run overlap with them
+ * on the device.  A request behind one that does not fit may be admitted
+ * first, until the blocked one has been passed 16 times.  Images do not
+ * depend on what else runs: a request's result is the same alone and in a
+ * mix.  All functions are thread-safe. */
+typedef struct SheenServer_* SheenServer;
+
+typedef struct SheenServerConfig {
+    int form;                        /* SHEEN_FORM_WAVEFRONT or SHEEN_FORM_PLAIN for the server's scenes */
+    int max_inflight;                /* requests on the GPU at once (1..64); <= 0: 4 */
+    unsigned long long hbm_budget;   /* device bytes for scenes + in-flight requests; 0: 90% of free memory */
+    long long tile_samples;          /* samples per band of rows; <= 0: 4194304 */
+} SheenServerConfig;
+
+enum {
+    SHEEN_REQ_PENDING = 0,   /* queued, not admitted */
+    SHEEN_REQ_RUNNING = 1,   /* admitted, on the GPU */
+    SHEEN_REQ_DONE = 2,      /* image in the caller's buffer */
+    SHEEN_REQ_FAILED = 3     /* see SheenRequestInfo.error */
+};
+
+typedef struct SheenRequestInfo {
+    int status;
+    int scene_id, width, height, aa_samples;
+    int tiles;                       /* bands of rows the request was rendered in */
+    unsigned long long rays;         /* primary + shadow + secondary rays traced */
+    unsigned long long hbm_bytes;    /* device footprint while in flight */
+    double queue_ms;                 /* submit -> admitted */
+    double run_ms;                   /* admitted -> image in the caller's buffer */
+    double latency_ms;               /* submit -> image in the caller's buffer */
+    char error[128];
+} SheenRequestInfo;
+
+typedef struct SheenServerStats {
+    unsigned long long submitted, completed, failed;
+    unsigned long long rays;         /* over completed requests */
+    double p50_ms, p99_ms, mean_ms, max_ms;   /* latency of completed requests (nearest rank) */
+    double busy_ms;                  /* first submit -> last completion */
+    unsigned long long hbm_budget, hbm_used, hbm_peak, scene_bytes;
+    int inflight_peak, inflight, pending;
+} SheenServerStats;
+
+/* cfg may be NULL (defaults).  The server uses the current CUDA device. */
+int  sheen_server_create(const SheenServerConfig* cfg, SheenServer* out);
+/* Cancels pending requests (status FAILED), waits for in-flight ones, frees
+ * every scene and buffer of the server. */
+void sheen_server_destroy(SheenServer server);
+/* Builds and uploads a scene (host BVH build included) and keeps it resident;
+ * fails when it does not fit in the budget. */
+int  sheen_server_add_scene(SheenServer server, const SheenScene* scene, int* scene_id);
+/* Frees the scene once no queued or running request uses it; new submits
+ * naming it fail at once. */
+int  sheen_server_remove_scene(SheenServer server, int scene_id);
+/* Queues a request.  out_rgba_host: width*height float4, written when the
+ * request completes (RGBA, linear, as sheen_render_scene_rgba writes it); it
+ * must stay valid until then.  Fails at once on bad parameters, an unknown
+ * scene, or a footprint that could never fit. */
+int  sheen_server_submit(SheenServer server, int scene_id, int width, int height, int aa_samples,
+                         float* out_rgba_host, unsigned long long* request_id);
+/* Status of a request (SHEEN_REQ_*), or -1 for an unknown id. */
+int  sheen_server_poll(SheenServer server, unsigned long long request_id);
+/* Waits up to timeout_ms (< 0: no limit).  Returns 1 when the request has
+ * finished (info filled, the id is released), 0 on timeout (info filled with
+ * the current state), -1 for an unknown id.  info may be NULL. */
+int  sheen_server_wait(SheenServer server, unsigned long long request_id, double timeout_ms,
+                       SheenRequestInfo* info);
+int  sheen_server_stats(SheenServer server, SheenServerStats* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -77,8 +77,9 @@ struct Region {
 };
 
 // Plain form: one thread per pixel.  Asynchronous on `stream`.
+// Ray tallies go to `tally` (8 device counters) or, when null, the scene's own.
 cudaError_t launch_plain(const DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
-                         bool count_nodes);
+                         bool count_nodes, unsigned long long* tally = nullptr);
 
 // Primary closest hits (object id, material id, t) per pixel sample.
 cudaError_t launch_primary_hits_plain(const DeviceScene& s, int W, int H, int ns, int* obj, int* mat, float* t,
@@ -90,12 +91,25 @@ cudaError_t launch_primary_hits_bvh4(const DeviceScene& s, int W, int H, int ns,
 // thread per pixel); used by the wavefront form for scenes outside its
 // queue pipeline and as a measurement point.
 cudaError_t launch_mega_bvh4(const DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
-                             bool count_nodes);
+                             bool count_nodes, unsigned long long* tally = nullptr);
 
 // Wavefront form.
 cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
                              bool count_nodes);
 void wave_release(DeviceScene& s);
+
+// Wavefront form on caller-owned scratch (the request loop: one block per
+// in-flight request).  Renders a region with the queue kernels launched
+// directly on `stream` (no graph, no synchronisation), its queues carved from
+// [scratch, scratch + scratch_bytes) (256-byte aligned, at least
+// wave_scratch_bytes(lights, padded region samples)).  Scenes outside the
+// queue pipeline (wave_pipeline_used false) run on the BVH4 megakernel and
+// need no scratch.  Ray tallies are added to `tally` (device counters
+// 0..2) when not null.
+cudaError_t launch_wavefront_scratch(DeviceScene& s, void* scratch, size_t scratch_bytes, int W, int H, int aa,
+                                     Region rg, float4* out, cudaStream_t stream, unsigned long long* tally);
+size_t wave_scratch_bytes(int L, long long nsamples);
+bool wave_pipeline_used(const DeviceScene& s);
 
 // Photon pass on the device (emission + hash-grid build), called by
 // scene_upload when the scene asks for photons.

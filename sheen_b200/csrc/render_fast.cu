@@ -58,15 +58,17 @@ __global__ void primary_hits_bvh4_kernel(DevScene S, int W, int H, int ns, int* 
 }  // namespace dev
 
 cudaError_t launch_mega_bvh4(const DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
-                             bool count_nodes) {
+                             bool count_nodes,
+                             unsigned long long* tally) {
+    if (!tally) tally = s.d_tally;
     const dim3 block(16, 8);
     const dim3 grid((rg.x1 - rg.x0 + 15) / 16, (rg.y1 - rg.y0 + 7) / 8);
     if (count_nodes)
         dev::mega_bvh4_kernel<true><<<grid, block, 0, stream>>>(s.view, out, W, H, aa, rg.x0, rg.y0, rg.x1, rg.y1,
-                                                                s.d_tally);
+                                                                tally);
     else
         dev::mega_bvh4_kernel<false><<<grid, block, 0, stream>>>(s.view, out, W, H, aa, rg.x0, rg.y0, rg.x1, rg.y1,
-                                                                 s.d_tally);
+                                                                 tally);
     return cudaGetLastError();
 }
 

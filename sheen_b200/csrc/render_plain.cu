@@ -75,13 +75,15 @@ cudaError_t launch_primary_hits_plain(const DeviceScene& s, int W, int H, int ns
 }
 
 cudaError_t launch_plain(const DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
-                         bool count_nodes) {
+                         bool count_nodes,
+                         unsigned long long* tally) {
+    if (!tally) tally = s.d_tally;
     const dim3 block(16, 8);
     const dim3 grid((rg.x1 - rg.x0 + 15) / 16, (rg.y1 - rg.y0 + 7) / 8);
     if (count_nodes)
-        dev::plain_kernel<true><<<grid, block, 0, stream>>>(s.view, out, W, H, aa, rg.x0, rg.y0, rg.x1, rg.y1, s.d_tally);
+        dev::plain_kernel<true><<<grid, block, 0, stream>>>(s.view, out, W, H, aa, rg.x0, rg.y0, rg.x1, rg.y1, tally);
     else
-        dev::plain_kernel<false><<<grid, block, 0, stream>>>(s.view, out, W, H, aa, rg.x0, rg.y0, rg.x1, rg.y1, s.d_tally);
+        dev::plain_kernel<false><<<grid, block, 0, stream>>>(s.view, out, W, H, aa, rg.x0, rg.y0, rg.x1, rg.y1, tally);
     return cudaGetLastError();
 }
 

@@ -414,15 +414,20 @@ __global__ void wave_tally_out(WaveView V, unsigned long long* tally) {
 
 }  // namespace dev
 
-// Per-scene buffers and the captured frame graph.
+// Queue and slot buffers of the wavefront form, carved from one device block,
+// plus the frame graph.  A resident scene owns one for its own frames; the
+// request loop carves one per in-flight request from memory it allocates, so
+// concurrent requests on one scene never share scratch.
 struct Wave {
-    int nsamples_cap = 0, L = 0;
+    long long nsamples_cap = 0;
+    int L = 0;
     float* slots = nullptr;
     float* coef = nullptr;
     float4* shq = nullptr;
     float4* rq = nullptr;
     float4* tq = nullptr;
     unsigned int* ctr = nullptr;
+    void* block = nullptr;   // owned by this struct when it came from wave_reserve_into
     size_t bytes = 0;
     int sms = 148;
     // The frame's launch sequence captured once per frame shape and replayed.
@@ -438,6 +443,48 @@ struct Wave {
     } key{};
 };
 
+static size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+size_t wave_scratch_bytes(int L, long long nsamples) {
+    const size_t n = (size_t)nsamples;
+    return align256(n * 3 * (L + 2) * 3 * sizeof(float)) + align256(n * 3 * sizeof(float)) +
+           align256(n * std::max(L, 1) * 3 * sizeof(float4)) + 2 * align256(n * 2 * sizeof(float4)) +
+           align256(dev::kCounterWords * sizeof(unsigned int));
+}
+
+// Points w's arrays into [base, base + bytes) for `nsamples` samples and L
+// lights (base 256-byte aligned).  False when the block is too small.
+static bool wave_carve(Wave& w, void* base, size_t bytes, int L, long long nsamples) {
+    if (wave_scratch_bytes(L, nsamples) > bytes) return false;
+    const size_t n = (size_t)nsamples;
+    char* p = static_cast<char*>(base);
+    auto take = [&p](size_t b) {
+        char* q = p;
+        p += align256(b);
+        return q;
+    };
+    w.slots = reinterpret_cast<float*>(take(n * 3 * (L + 2) * 3 * sizeof(float)));
+    w.coef = reinterpret_cast<float*>(take(n * 3 * sizeof(float)));
+    w.shq = reinterpret_cast<float4*>(take(n * std::max(L, 1) * 3 * sizeof(float4)));
+    w.rq = reinterpret_cast<float4*>(take(n * 2 * sizeof(float4)));
+    w.tq = reinterpret_cast<float4*>(take(n * 2 * sizeof(float4)));
+    w.ctr = reinterpret_cast<unsigned int*>(take(dev::kCounterWords * sizeof(unsigned int)));
+    w.nsamples_cap = nsamples;
+    w.L = L;
+    return true;
+}
+
+static int device_sms() {
+    static int sms = 0;
+    if (!sms) {
+        int dev_id = 0, n = 148;
+        cudaGetDevice(&dev_id);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev_id);
+        sms = n;
+    }
+    return sms;
+}
+
 // Persistent grid: as many 128-thread blocks as fit on every SM.
 template <class K>
 static int persistent_grid(K kernel, int sms) {
@@ -448,37 +495,41 @@ static int persistent_grid(K kernel, int sms) {
 
 // The queue pipeline of one frame for category set F.
 template <int F>
-static cudaError_t run_pipeline(DeviceScene& s, const dev::WaveView& V, int npad, float4* out, cudaStream_t stream) {
-    Wave* w = s.wave;
+static cudaError_t run_pipeline(const DeviceScene& s, const dev::WaveView& V, int npad, float4* out,
+                                cudaStream_t stream, unsigned long long* tally) {
     static int g_primary = 0, g_shadow = 0, g_reflect = 0, g_refract = 0;
     if (!g_primary) {
-        g_primary = persistent_grid(dev::wave_primary<F>, w->sms);
-        g_shadow = persistent_grid(dev::wave_shadow<F>, w->sms);
-        g_reflect = persistent_grid(dev::wave_reflect<F>, w->sms);
-        g_refract = persistent_grid(dev::wave_refract<F>, w->sms);
+        const int sms = device_sms();
+        g_primary = persistent_grid(dev::wave_primary<F>, sms);
+        g_shadow = persistent_grid(dev::wave_shadow<F>, sms);
+        g_reflect = persistent_grid(dev::wave_reflect<F>, sms);
+        g_refract = persistent_grid(dev::wave_refract<F>, sms);
     }
     cudaError_t e;
-    if ((e = cudaMemsetAsync(w->ctr, 0, dev::kCounterWords * sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(V.ctr, 0, dev::kCounterWords * sizeof(unsigned int), stream)) != cudaSuccess) return e;
     dev::wave_primary<F><<<g_primary, 128, 0, stream>>>(s.view, V);
     dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
-    if ((e = cudaMemsetAsync(&w->ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(&V.ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
     dev::wave_reflect<F><<<g_reflect, 128, 0, stream>>>(s.view, V);
     dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
-    if ((e = cudaMemsetAsync(&w->ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(&V.ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
     dev::wave_refract<F><<<g_refract, 128, 0, stream>>>(s.view, V);
     dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
     dev::wave_resolve<<<(npad + 127) / 128, 128, 0, stream>>>(V, out);
-    dev::wave_tally_out<<<1, 1, 0, stream>>>(V, s.d_tally);
+    if (tally) dev::wave_tally_out<<<1, 1, 0, stream>>>(V, tally);
     return cudaGetLastError();
 }
 
-void wave_release(DeviceScene& s) {
-    if (!s.wave) return;
-    Wave* w = s.wave;
+static void wave_free(Wave* w) {
+    if (!w) return;
     if (w->exec) cudaGraphExecDestroy(w->exec);
     if (w->capture_stream) cudaStreamDestroy(w->capture_stream);
-    cudaFree(w->slots); cudaFree(w->coef); cudaFree(w->shq); cudaFree(w->rq); cudaFree(w->tq); cudaFree(w->ctr);
+    cudaFree(w->block);
     delete w;
+}
+
+void wave_release(DeviceScene& s) {
+    wave_free(s.wave);
     s.wave = nullptr;
 }
 
@@ -488,71 +539,76 @@ static bool wave_supported(const DeviceScene& s) {
     return !s.wave_fallback;
 }
 
-static cudaError_t wave_reserve(DeviceScene& s, int nsamples) {
-    const int L = s.view.num_lights;
-    if (s.wave && s.wave->nsamples_cap >= nsamples && s.wave->L == L) return cudaSuccess;
-    wave_release(s);
-    Wave* w = new Wave();
-    w->nsamples_cap = nsamples;
-    w->L = L;
-    const size_t slots = (size_t)nsamples * 3 * (L + 2) * 3;
-    const size_t shq = (size_t)nsamples * std::max(L, 1);
-    cudaError_t e;
-    size_t bytes = 0;
-    auto alloc = [&](void** p, size_t n) {
-        bytes += n;
-        return cudaMalloc(p, n);
-    };
-    if ((e = alloc((void**)&w->slots, slots * sizeof(float))) != cudaSuccess ||
-        (e = alloc((void**)&w->coef, (size_t)nsamples * 3 * sizeof(float))) != cudaSuccess ||
-        (e = alloc((void**)&w->shq, shq * 3 * sizeof(float4))) != cudaSuccess ||
-        (e = alloc((void**)&w->rq, (size_t)nsamples * 2 * sizeof(float4))) != cudaSuccess ||
-        (e = alloc((void**)&w->tq, (size_t)nsamples * 2 * sizeof(float4))) != cudaSuccess ||
-        (e = alloc((void**)&w->ctr, dev::kCounterWords * sizeof(unsigned int))) != cudaSuccess) {
-        s.wave = w;
-        wave_release(s);
+// Makes the scene's own scratch hold at least `nsamples` samples for L
+// lights: re-carves the block when it is large enough, else reallocates.
+// A re-carve moves the arrays, so the captured frame graph is dropped.
+static cudaError_t wave_reserve_into(Wave*& w, int L, long long nsamples) {
+    if (w && w->nsamples_cap >= nsamples && w->L == L) return cudaSuccess;
+    if (w && wave_scratch_bytes(L, nsamples) <= w->bytes) {
+        if (w->exec) { cudaGraphExecDestroy(w->exec); w->exec = nullptr; }
+        wave_carve(*w, w->block, w->bytes, L, nsamples);
+        return cudaSuccess;
+    }
+    wave_free(w);
+    w = new Wave();
+    const size_t bytes = wave_scratch_bytes(L, nsamples);
+    cudaError_t e = cudaMalloc(&w->block, bytes);
+    if (e != cudaSuccess) {
+        delete w;
+        w = nullptr;
         return e;
     }
     w->bytes = bytes;
-    int dev_id = 0, sms = 148;
-    cudaGetDevice(&dev_id);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id);
-    w->sms = sms;
-    s.wave = w;
+    w->sms = device_sms();
+    wave_carve(*w, w->block, bytes, L, nsamples);
     return cudaSuccess;
+}
+
+static long long region_padded(Region rg) {
+    const int rw = rg.x1 - rg.x0, rh = rg.y1 - rg.y0;
+    return (long long)((rw + 15) / 16) * 16 * ((rh + 7) / 8) * 8;
+}
+
+static int clamp_spp(int aa) { return aa < 1 ? 1 : (aa > 64 ? 64 : aa); }
+
+// Queue view of one frame region; the region's pixels are walked in whole
+// 16x8 tiles (sample_pixel), so its sample count is padded to them.
+static dev::WaveView make_view(const DeviceScene& s, const Wave& w, int W, int H, int ns, Region rg) {
+    dev::WaveView V;
+    V.slots = w.slots; V.coef = w.coef; V.shq = w.shq; V.rq = w.rq; V.tq = w.tq; V.ctr = w.ctr;
+    V.L = s.view.num_lights;
+    V.ns = ns;
+    V.W = W; V.H = H; V.x0 = rg.x0; V.y0 = rg.y0; V.rw = rg.x1 - rg.x0; V.rh = rg.y1 - rg.y0;
+    V.nsamples = (int)(region_padded(rg) * ns);
+    const CameraData& cam = s.view.cam;
+    float tan_x = 1.0f;
+    if (cam.focal_length > 0.0f) {
+        const float tan_h = 0.5f * cam.sensor_width / cam.focal_length;
+        tan_x = (W >= H) ? tan_h : tan_h * float(W) / float(H);
+    }
+    V.pix_angle = 2.0f * tan_x / (float)W;
+    V.count_rays = 1;
+    return V;
+}
+
+static bool simple_scene(const DeviceScene& s) {
+    const dev::DevScene& sv = s.view;
+    return sv.num_strands == 0 && sv.num_hfs == 0 && sv.num_ses == 0 && sv.num_lathes == 0 && sv.num_prisms == 0 &&
+           sv.csg_root < 0;
 }
 
 cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
                              bool count_nodes) {
     if (!wave_supported(s) || count_nodes) return launch_mega_bvh4(s, W, H, aa, rg, out, stream, count_nodes);
-    const int ns = aa < 1 ? 1 : (aa > 64 ? 64 : aa);
-    const int rw = rg.x1 - rg.x0, rh = rg.y1 - rg.y0;
-    // pixels are padded to whole 16x8 tiles by sample_pixel
-    const long long padded = (long long)((rw + 15) / 16) * 16 * ((rh + 7) / 8) * 8;
-    const long long nsamples = padded * ns;
+    const int ns = clamp_spp(aa);
+    const long long nsamples = region_padded(rg) * ns;
     if (nsamples > (1ll << 30)) return cudaErrorInvalidValue;
-    cudaError_t e = wave_reserve(s, (int)nsamples);
+    cudaError_t e = wave_reserve_into(s.wave, s.view.num_lights, nsamples);
     if (e != cudaSuccess) return e;
     Wave* w = s.wave;
-    dev::WaveView V;
-    V.slots = w->slots; V.coef = w->coef; V.shq = w->shq; V.rq = w->rq; V.tq = w->tq; V.ctr = w->ctr;
-    V.L = s.view.num_lights;
-    V.ns = ns;
-    V.W = W; V.H = H; V.x0 = rg.x0; V.y0 = rg.y0; V.rw = rw; V.rh = rh;
-    V.nsamples = (int)nsamples;
-    {
-        const CameraData& cam = s.view.cam;
-        float tan_x = 1.0f;
-        if (cam.focal_length > 0.0f) {
-            const float tan_h = 0.5f * cam.sensor_width / cam.focal_length;
-            tan_x = (W >= H) ? tan_h : tan_h * float(W) / float(H);
-        }
-        V.pix_angle = 2.0f * tan_x / (float)W;
-    }
-    V.count_rays = 1;
-    const dev::DevScene& sv = s.view;
-    const bool simple = sv.num_strands == 0 && sv.num_hfs == 0 && sv.num_ses == 0 && sv.num_lathes == 0 &&
-                        sv.num_prisms == 0 && sv.csg_root < 0;
+    const dev::WaveView V = make_view(s, *w, W, H, ns, rg);
+    const int npad = (int)region_padded(rg);
+    const bool simple = simple_scene(s);
     // Replay the captured frame when the shape and output match; otherwise
     // capture the sequence on the scene's own stream and instantiate it.
     const Wave::Key key{W, H, aa, rg.x0, rg.y0, rg.x1, rg.y1, out};
@@ -562,8 +618,8 @@ cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, fl
             (e = cudaStreamCreateWithFlags(&w->capture_stream, cudaStreamNonBlocking)) != cudaSuccess)
             return e;
         if ((e = cudaStreamBeginCapture(w->capture_stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
-        cudaError_t le = simple ? run_pipeline<dev::kCatSimple>(s, V, (int)padded, out, w->capture_stream)
-                                : run_pipeline<dev::kCatAll>(s, V, (int)padded, out, w->capture_stream);
+        cudaError_t le = simple ? run_pipeline<dev::kCatSimple>(s, V, npad, out, w->capture_stream, s.d_tally)
+                                : run_pipeline<dev::kCatAll>(s, V, npad, out, w->capture_stream, s.d_tally);
         cudaGraph_t graph = nullptr;
         e = cudaStreamEndCapture(w->capture_stream, &graph);
         if (le != cudaSuccess) { if (graph) cudaGraphDestroy(graph); return le; }
@@ -574,6 +630,22 @@ cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, fl
         w->key = key;
     }
     return cudaGraphLaunch(w->exec, stream);
+}
+
+bool wave_pipeline_used(const DeviceScene& s) { return wave_supported(s); }
+
+cudaError_t launch_wavefront_scratch(DeviceScene& s, void* scratch, size_t scratch_bytes, int W, int H, int aa,
+                                     Region rg, float4* out, cudaStream_t stream, unsigned long long* tally) {
+    if (!wave_supported(s)) return launch_mega_bvh4(s, W, H, aa, rg, out, stream, false, tally);
+    const int ns = clamp_spp(aa);
+    const long long nsamples = region_padded(rg) * ns;
+    if (nsamples > (1ll << 30)) return cudaErrorInvalidValue;
+    Wave w;
+    if (!wave_carve(w, scratch, scratch_bytes, s.view.num_lights, nsamples)) return cudaErrorInvalidValue;
+    const dev::WaveView V = make_view(s, w, W, H, ns, rg);
+    const int npad = (int)region_padded(rg);
+    return simple_scene(s) ? run_pipeline<dev::kCatSimple>(s, V, npad, out, stream, tally)
+                           : run_pipeline<dev::kCatAll>(s, V, npad, out, stream, tally);
 }
 
 // ---------------------------------------------------------------------
