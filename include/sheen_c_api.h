@@ -217,6 +217,20 @@ int sheen_scene_primary_hits(SheenDeviceScene scene, int width, int height, int 
  * depth, or a negative code on a violation.  No device work. */
 int sheen_selfcheck_bvh4(const SheenScene* scene);
 
+/* Launch parameters of the wavefront form, by name (process-wide; frames
+ * captured under older values are re-captured).  No counterpart in the
+ * reference (its launch shape is fixed at 16x16 threads per block,
+ * api/sheen_c_api.cu:309-312).  Keys and ranges:
+ *   "wave.shadow_kernel"         0: every warp takes 32 shadow rays and
+ *                                   finishes them together; 1 (default):
+ *                                   lanes take new rays as theirs finish
+ *   "wave.refill_min"            1..32 (default 8): idle lanes that make a
+ *                                   warp take new rays (shadow_kernel 1)
+ *   "wave.shadow_blocks_per_sm"  0..16 (default 0 = as many as fit)
+ * Every setting gives the same image; only the speed differs.  0 / -1. */
+int sheen_tune_set(const char* key, int value);
+int sheen_tune_get(const char* key, int* value);
+
 /* Owned host scenes: the .sheen loader and the synthetic generators return
  * one.  sheen_owned_view points into storage owned by the handle. */
 typedef struct SheenOwnedScene_* SheenOwnedScene;

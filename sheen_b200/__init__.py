@@ -269,6 +269,26 @@ def generate_scene(config: int, seed: int = 1, detail: int = 0, photons: int = 0
     return OwnedScene(h.value)
 
 
+def tune_set(key: str, value: int) -> None:
+    """Set a launch parameter of the wavefront form (see sheen_tune_set)."""
+    L = lib()
+    L.sheen_tune_set.argtypes = [ctypes.c_char_p, ctypes.c_int]
+    L.sheen_tune_set.restype = ctypes.c_int
+    _check(L.sheen_tune_set(key.encode(), int(value)))
+
+
+def tune_get(key: str) -> int:
+    L = lib()
+    L.sheen_tune_get.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]
+    L.sheen_tune_get.restype = ctypes.c_int
+    v = ctypes.c_int()
+    _check(L.sheen_tune_get(key.encode(), ctypes.byref(v)))
+    return v.value
+
+
+TUNE_KEYS = ("wave.shadow_kernel", "wave.refill_min", "wave.shadow_blocks_per_sm")
+
+
 def write_png(path: str, rgba: np.ndarray) -> None:
     rgba = np.ascontiguousarray(rgba, np.float32)
     _check(lib().sheen_write_png_srgb(path.encode(), rgba.ctypes.data, rgba.shape[1], rgba.shape[0]))

@@ -285,6 +285,25 @@ struct FastTracer {
             return classify_shadow_hit(S, h, mask_aware, sh);
         return kClear;
     }
+    // The shadow query split around its mesh category, for callers that walk
+    // the mesh themselves: the sphere category (-1 when it has no hit, else
+    // its classification) and the categories after the mesh (kClear when
+    // none has a hit).  shadow() == pre, else mesh, else post.
+    __device__ __forceinline__ static int shadow_pre_mesh(const DevScene& S, const Ray& r, bool mask_aware,
+                                                          ShadowHit& sh, Counters& c) {
+        Hit h;
+        if ((F & kCatSpheres) && spheres_ref<COUNT>(S, r, h, c)) return classify_shadow_hit(S, h, mask_aware, sh);
+        return -1;
+    }
+    __device__ __forceinline__ static int shadow_post_mesh(const DevScene& S, const Ray& r, bool mask_aware,
+                                                           ShadowHit& sh, Counters& c) {
+        Hit h;
+        if (((F & kCatHF) && hfs_ref<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_ref<COUNT>(S, r, h, c)) ||
+            ((F & kCatLathe) && lathes_ref<COUNT>(S, r, h, c)) || ((F & kCatPrism) && prisms_ref<COUNT>(S, r, h, c)) ||
+            ((F & kCatCSG) && S.csg_root >= 0 && csg_test(S, r, h)) || ((F & kCatPlanes) && planes_scan(S, r, h)))
+            return classify_shadow_hit(S, h, mask_aware, sh);
+        return kClear;
+    }
     __device__ __forceinline__ static bool occluded(const DevScene& S, const Ray& r, Counters& c) {
         Hit h;
         if ((F & kCatSpheres) && spheres_ref<COUNT>(S, r, h, c)) return true;

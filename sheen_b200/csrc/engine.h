@@ -111,6 +111,17 @@ cudaError_t launch_wavefront_scratch(DeviceScene& s, void* scratch, size_t scrat
 size_t wave_scratch_bytes(int L, long long nsamples);
 bool wave_pipeline_used(const DeviceScene& s);
 
+// Launch parameters of the wavefront form (tuning.cpp).
+struct Tuning {
+    int shadow_kernel = 1;          // 0: 32-ray batches per warp; 1: per-lane refill
+    int refill_min = 8;             // idle lanes that trigger a refill (shadow_kernel 1)
+    int shadow_blocks_per_sm = 0;   // 128-thread blocks per SM for the shadow stage; 0: occupancy limit
+};
+Tuning tuning();
+int tuning_generation();
+int tuning_set(const char* name, int value);
+int tuning_get(const char* name, int* value);
+
 // Photon pass on the device (emission + hash-grid build), called by
 // scene_upload when the scene asks for photons.
 int build_photon_map_device(DeviceScene& s, int per_light, float cell);

@@ -277,6 +277,229 @@ __global__ void __launch_bounds__(128) wave_shadow(DevScene S, WaveView V) {
     }
 }
 
+// Shadow stage with per-lane refill.  Same queries and results as
+// wave_shadow, scheduled differently: every lane carries one shadow ray
+// through a small state machine (sphere category -> closest walk over the
+// passable triangles -> any-hit walk over the blocking ones -> the later
+// categories -> next glass pass), and the warp steps all lanes' mesh walks
+// together: inner nodes until every busy lane sits on a leaf, then one leaf
+// each.  A lane whose ray is finished goes idle; once `refill_min` lanes are
+// idle the warp claims that many new rays from the queue in one atomic, so
+// long rays no longer hold 31 finished lanes hostage.  The mesh walks are
+// qmesh_trace's, step for step (same child order, same stack, same tests),
+// so every ray's result is the one wave_shadow computes.
+template <int F>
+__global__ void __launch_bounds__(128, 5) wave_shadow_refill(DevScene S, WaveView V, int refill_min) {
+    using T = FastTracer<false, F>;
+    constexpr unsigned int kFull = 0xffffffffu;
+    constexpr uint32_t kLeafBit = 0x80000000u;
+    // lane states: idle, walking the passable triangles (closest hit),
+    // walking the blocking triangles (any hit), or waiting at the transition
+    // site (a fresh ray, or a walk that has ended)
+    enum { kIdle = 0, kWalkPass, kWalkBlock, kFresh, kEndPass, kEndBlock };
+    Counters c;
+    const unsigned int n = V.ctr[kShadowCount];
+    const int lane = threadIdx.x & 31;
+
+    // the lane's ray: q holds its current origin and direction
+    QRay q{};
+    float3 o_first = f3(0.0f, 0.0f, 0.0f), cc = o_first;
+    float tmax = 0.0f;
+    int slot = 0, pass = 0;
+    bool strands = false;
+    int state = kIdle;
+    bool block_after_pass = false;
+    int pass_tri = -1;
+    float tp = 0.0f, up = 0.0f, vp = 0.0f;
+    unsigned int rays = 0;
+    // the lane's mesh walk
+    const QNode4* wn = nullptr;
+    const float4* wt = nullptr;
+    uint32_t entry = 0;
+    int sp = 0, wbest = -1;
+    float t_best = 0.0f, wu = 0.0f, wv = 0.0f;
+    uint32_t stack_e[kQStack];
+    float stack_t[kQStack];
+
+    bool exhausted = false;
+    for (;;) {
+        // ---- refill idle lanes ------------------------------------------
+        const unsigned int idle = __ballot_sync(kFull, state == kIdle);
+        if (!exhausted && (idle == kFull || __popc(idle) >= refill_min)) {
+            const unsigned int k = (unsigned int)__popc(idle);
+            unsigned int b = 0;
+            if (lane == 0) b = atomicAdd(&V.ctr[kShadowHead], k);
+            b = __shfl_sync(kFull, b, 0);
+            if (b + k >= n) exhausted = true;
+            if (state == kIdle) {
+                const unsigned int item = b + (unsigned int)__popc(idle & ((1u << lane) - 1u));
+                if (item < n) {
+                    const float4 a = V.shq[3 * (size_t)item], bb = V.shq[3 * (size_t)item + 1],
+                                 c4 = V.shq[3 * (size_t)item + 2];
+                    q.o = f3(a.x, a.y, a.z);
+                    q.d = f3(bb.x, bb.y, bb.z);
+                    o_first = q.o;
+                    tmax = a.w;
+                    slot = __float_as_int(bb.w);
+                    cc = f3(c4.x, c4.y, c4.z);
+                    strands = c4.w != 0.0f;
+                    pass = 0;
+                    state = kFresh;
+                }
+            }
+        }
+        // ---- transition site: start a pass, or settle an ended walk ---------
+        if (state >= kFresh) {
+            int res;
+            ShadowHit sh{};
+            Ray r;
+            r.o = q.o; r.d = q.d; r.tmin = 0.001f; r.tmax = tmax;
+            if (state == kFresh) {
+                res = -2;   // start a pass
+            } else if (state == kEndPass && S.q_block.nodes) {
+                // closest passable hit found; now any blocking hit strictly before it
+                pass_tri = wbest; tp = t_best; up = wu; vp = wv;
+                state = kWalkBlock; block_after_pass = true;
+                wn = S.q_block.nodes; wt = S.q_block.tris;
+                entry = 0; sp = 0; wbest = -1; t_best = tp;
+                res = -3;   // keep walking
+            } else {
+                if (state == kEndPass) { pass_tri = wbest; tp = t_best; up = wu; vp = wv; }
+                res = (state == kEndBlock && wbest >= 0) ? kBlocked : kClear;
+                if (res == kClear && (state == kEndPass || block_after_pass) && pass_tri >= 0) {
+                    Hit h;
+                    tri_finish(r, S.tris[pass_tri], tp, up, vp, h);
+                    res = classify_shadow_hit(S, h, true, sh);
+                }
+                if (res == kClear) res = T::shadow_post_mesh(S, r, true, sh, c);
+            }
+            // settle: pass results and pass starts until the lane walks a
+            // mesh or its ray is finished
+            while (res != -3) {
+                if (res == -2) {
+                    rays++;
+                    r.o = q.o;
+                    res = T::shadow_pre_mesh(S, r, true, sh, c);
+                    if (res >= 0) continue;
+                    if ((F & kCatMesh) && S.q_all.nodes) {
+                        q = make_qray(r);
+                        pass_tri = -1;
+                        entry = 0; sp = 0; wbest = -1; t_best = tmax;
+                        if (S.q_pass.nodes) {
+                            state = kWalkPass;
+                            wn = S.q_pass.nodes; wt = S.q_pass.tris;
+                        } else {
+                            state = kWalkBlock; block_after_pass = false;
+                            wn = S.q_all.nodes; wt = S.q_all.tris;
+                        }
+                        break;
+                    }
+                    res = T::shadow_post_mesh(S, r, true, sh, c);
+                    continue;
+                }
+                if (res == kPass && ++pass < 3) {   // through the glass: next pass
+                    q.o = sh.p + q.d * 0.002f;
+                    res = -2;
+                    continue;
+                }
+                // finished: blocked, clear, or three glass passes (lit)
+                float3 contrib = f3(0.0f, 0.0f, 0.0f);
+                if (res != kBlocked) {
+                    contrib = cc;
+                    if (strands) {
+                        Ray first;
+                        first.o = o_first; first.d = q.d; first.tmin = 0.001f; first.tmax = tmax;
+                        contrib = contrib * expf(-T::strand_depth(S, first, c));
+                    }
+                }
+                put_slot(V, slot, contrib);
+                state = kIdle;
+                break;
+            }
+        }
+        if (!__any_sync(kFull, state != kIdle)) {
+            if (exhausted) break;
+            continue;
+        }
+        // ---- inner nodes until every walking lane sits on a leaf ------------
+        while (true) {
+            const bool inner = (state == kWalkPass || state == kWalkBlock) && !(entry & kLeafBit);
+            if (!__any_sync(kFull, inner)) break;
+            if (!inner) continue;
+            float tn[4];
+            uint4 ch;
+            const int mask = qnode_children(wn, (int)entry, q, t_best, tn, ch);
+            const uint32_t cid[4] = {ch.x, ch.y, ch.z, ch.w};
+            if (mask != 0) {
+                if (state == kWalkBlock) {
+                    int first = -1;
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        if (!(mask & (1 << i))) continue;
+                        if (first < 0) first = i;
+                        else if (sp < kQStack) stack_e[sp++] = cid[i];
+                    }
+                    entry = cid[first];
+                } else {
+                    uint32_t key[4];
+                    int m = 0;
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+                        if (mask & (1 << i)) key[m++] = (__float_as_uint(fmaxf(tn[i], 0.0f)) & ~3u) | (uint32_t)i;
+#define CSWAP(a, b) if (key[a] > key[b]) { uint32_t t_ = key[a]; key[a] = key[b]; key[b] = t_; }
+                    if (m == 2) { CSWAP(0, 1) }
+                    else if (m == 3) { CSWAP(0, 1) CSWAP(1, 2) CSWAP(0, 1) }
+                    else if (m == 4) { CSWAP(0, 1) CSWAP(2, 3) CSWAP(0, 2) CSWAP(1, 3) CSWAP(1, 2) }
+#undef CSWAP
+                    for (int k = m - 1; k >= 1; k--) {
+                        if (sp < kQStack) {
+                            stack_e[sp] = cid[key[k] & 3u];
+                            stack_t[sp] = tn[key[k] & 3u];
+                            sp++;
+                        }
+                    }
+                    entry = cid[key[0] & 3u];
+                }
+                continue;
+            }
+            // no child hit: pop (closest walks skip entries behind the hit)
+            bool ended = true;
+            while (sp > 0) {
+                --sp;
+                if (state == kWalkBlock || stack_t[sp] <= t_best) { entry = stack_e[sp]; ended = false; break; }
+            }
+            if (ended) state = state == kWalkPass ? kEndPass : kEndBlock;
+        }
+        // ---- one leaf per walking lane --------------------------------------
+        if (state == kWalkPass || state == kWalkBlock) {
+            const int first = (int)((entry & 0x7fffffffu) >> 3);
+            const int count = (int)(entry & 7u) + 1;
+            bool ended = false;
+            for (int k = 0; k < count; k++) {
+                const int s = first + k;
+                const float4 a = __ldg(&wt[3 * s]);
+                const float4 b = __ldg(&wt[3 * s + 1]);
+                const float4 c4 = __ldg(&wt[3 * s + 2]);
+                float t, u, v;
+                if (qtri_test(q, a, b, c4, q.tmin, tmax, t, u, v) && t < t_best) {
+                    t_best = t; wu = u; wv = v;
+                    wbest = __float_as_int(a.w);
+                    if (state == kWalkBlock) { ended = true; break; }
+                }
+            }
+            if (!ended) {
+                ended = true;
+                while (sp > 0) {
+                    --sp;
+                    if (state == kWalkBlock || stack_t[sp] <= t_best) { entry = stack_e[sp]; ended = false; break; }
+                }
+            }
+            if (ended) state = state == kWalkPass ? kEndPass : kEndBlock;
+        }
+    }
+    tally(V, kRaysShadow, rays);
+}
+
 template <int F>
 __global__ void __launch_bounds__(128) wave_reflect(DevScene S, WaveView V) {
     using T = FastTracer<false, F>;
@@ -436,9 +659,10 @@ struct Wave {
     struct Key {
         int W, H, aa, x0, y0, x1, y1;
         const void* out;
+        int tuning;   // tuning generation the graph was captured under
         bool operator==(const Key& o) const {
             return W == o.W && H == o.H && aa == o.aa && x0 == o.x0 && y0 == o.y0 && x1 == o.x1 && y1 == o.y1 &&
-                   out == o.out;
+                   out == o.out && tuning == o.tuning;
         }
     } key{};
 };
@@ -493,28 +717,44 @@ static int persistent_grid(K kernel, int sms) {
     return sms * std::max(b, 1);
 }
 
+// Grid of the shadow stage: the tuned blocks per SM, capped by occupancy.
+template <class K>
+static int shadow_grid(K kernel, int sms, int per_sm) {
+    const int full = persistent_grid(kernel, sms);
+    return per_sm > 0 ? std::min(full, sms * per_sm) : full;
+}
+
 // The queue pipeline of one frame for category set F.
 template <int F>
 static cudaError_t run_pipeline(const DeviceScene& s, const dev::WaveView& V, int npad, float4* out,
                                 cudaStream_t stream, unsigned long long* tally) {
-    static int g_primary = 0, g_shadow = 0, g_reflect = 0, g_refract = 0;
+    static int g_primary = 0, g_reflect = 0, g_refract = 0;
+    const int sms = device_sms();
     if (!g_primary) {
-        const int sms = device_sms();
         g_primary = persistent_grid(dev::wave_primary<F>, sms);
-        g_shadow = persistent_grid(dev::wave_shadow<F>, sms);
         g_reflect = persistent_grid(dev::wave_reflect<F>, sms);
         g_refract = persistent_grid(dev::wave_refract<F>, sms);
     }
+    const Tuning tu = tuning();
+    const bool refill = tu.shadow_kernel == 1;
+    const int g_shadow = refill ? shadow_grid(dev::wave_shadow_refill<F>, sms, tu.shadow_blocks_per_sm)
+                                : shadow_grid(dev::wave_shadow<F>, sms, tu.shadow_blocks_per_sm);
+    auto shadow = [&]() {
+        if (refill)
+            dev::wave_shadow_refill<F><<<g_shadow, 128, 0, stream>>>(s.view, V, tu.refill_min);
+        else
+            dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
+    };
     cudaError_t e;
     if ((e = cudaMemsetAsync(V.ctr, 0, dev::kCounterWords * sizeof(unsigned int), stream)) != cudaSuccess) return e;
     dev::wave_primary<F><<<g_primary, 128, 0, stream>>>(s.view, V);
-    dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
+    shadow();
     if ((e = cudaMemsetAsync(&V.ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
     dev::wave_reflect<F><<<g_reflect, 128, 0, stream>>>(s.view, V);
-    dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
+    shadow();
     if ((e = cudaMemsetAsync(&V.ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
     dev::wave_refract<F><<<g_refract, 128, 0, stream>>>(s.view, V);
-    dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
+    shadow();
     dev::wave_resolve<<<(npad + 127) / 128, 128, 0, stream>>>(V, out);
     if (tally) dev::wave_tally_out<<<1, 1, 0, stream>>>(V, tally);
     return cudaGetLastError();
@@ -611,7 +851,7 @@ cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, fl
     const bool simple = simple_scene(s);
     // Replay the captured frame when the shape and output match; otherwise
     // capture the sequence on the scene's own stream and instantiate it.
-    const Wave::Key key{W, H, aa, rg.x0, rg.y0, rg.x1, rg.y1, out};
+    const Wave::Key key{W, H, aa, rg.x0, rg.y0, rg.x1, rg.y1, out, tuning_generation()};
     if (!w->exec || !(w->key == key)) {
         if (w->exec) { cudaGraphExecDestroy(w->exec); w->exec = nullptr; }
         if (!w->capture_stream &&
