@@ -43,6 +43,26 @@ W, H, SPP = 1920, 1080, 4
 CPU_BAND = (480, 512)      # pixel rows of the CPU samples (two 16-row blocks of the 1080-row frame)
 
 
+class quiet_stdout:
+    """Sends file descriptor 1 to /dev/null for the duration: the reference's
+    shading code prints one debug line per caustic gather (render_kernel.cu:
+    291-294), millions per frame on the caustics workload, on the host path
+    and through the device printf buffer alike."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -228,7 +248,8 @@ def run_ours(args):
                    "form": args.form, "parallelism": f"replicas{world}",
                    "l2": "256 MB buffer written between timed frames; scene arrays exceed L2",
                    "rays_per_frame": rays, "box_tests_per_frame": nodes, "prim_tests_per_frame": prims,
-                   "scene_create_s": round(create_s, 3), "device_bytes": ds.device_bytes},
+                   "scene_create_s": round(create_s, 3), "device_bytes": ds.device_bytes,
+                   "tuning": {k: sb.tune_get(k) for k in sb.TUNE_KEYS}},
         "e2e": {"value": round(e2e, 2), "unit": "Mrays/s",
                 "h2d_bytes_per_step": int(st2["device_bytes"]),
                 "d2h_bytes_per_step": W * H * 16,
@@ -275,12 +296,14 @@ def cpu_baseline(ds, scene, stream, out, steps=1):
                 "sample": "unavailable: oracle/_ref not built"}
     ref = RefHost()
     threads = ref.lib.sheen_ref_max_threads()
-    h = ref.scene(scene.view_ptr, threads)
+    with quiet_stdout():
+        h = ref.scene(scene.view_ptr, threads)
     rays = band_rays(ds, stream, out)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        ref.render(h, W, H, SPP, threads, CPU_BAND[0] // 16, CPU_BAND[1] // 16)
-    dt = time.perf_counter() - t0
+    with quiet_stdout():
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            ref.render(h, W, H, SPP, threads, CPU_BAND[0] // 16, CPU_BAND[1] // 16)
+        dt = time.perf_counter() - t0
     return {"value": round(rays * steps / dt / 1e6, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
             "sample": f"rows {CPU_BAND[0]}-{CPU_BAND[1]} of the 1920x1080 4 spp frame ({rays} rays), "
                       f"{steps} pass(es), {dt:.1f} s"}
@@ -300,19 +323,25 @@ def reference_gpu(scene, rays, steps=3):
                                       ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     L.sheen_refgpu_render.restype = ctypes.c_int
     L.sheen_refgpu_scene_destroy.argtypes = [ctypes.c_void_p]
-    h = L.sheen_refgpu_scene_create(scene.view_ptr)
-    if not h:
-        return {"value": None, "unavailable": "reference scene upload failed"}
-    ms = ctypes.c_float(0.0)
-    L.sheen_refgpu_render(h, W, H, SPP, None, 1, ctypes.byref(ms))          # warm-up
-    rc = L.sheen_refgpu_render(h, W, H, SPP, None, steps, ctypes.byref(ms))
-    L.sheen_refgpu_scene_destroy(h)
+    with quiet_stdout():
+        h = L.sheen_refgpu_scene_create(scene.view_ptr)
+        if not h:
+            return {"value": None, "unavailable": "reference scene upload failed"}
+        ms = ctypes.c_float(0.0)
+        L.sheen_refgpu_render(h, W, H, SPP, None, 1, ctypes.byref(ms))          # warm-up
+        rc = L.sheen_refgpu_render(h, W, H, SPP, None, steps, ctypes.byref(ms))
+        L.sheen_refgpu_scene_destroy(h)
     if rc != 0:
         return {"value": None, "unavailable": "reference kernel launch failed"}
     frame_ms = ms.value / steps
-    return {"value": round(rays / (frame_ms / 1e3) / 1e6, 2), "unit": "Mrays/s", "ms_per_frame": round(frame_ms, 2),
+    line = {"value": round(rays / (frame_ms / 1e3) / 1e6, 2), "unit": "Mrays/s", "ms_per_frame": round(frame_ms, 2),
             "kernel": "reference render_kernel (render_kernel.cu:438-814) built for sm_100a, 16x16 blocks, "
                       "16 KB stack limit", "rays": "this renderer's count for the frame (same queries)"}
+    v = scene.view
+    if v.photons > 0 and v.caustics > 0:
+        line["note"] = ("the reference kernel printf()s one debug line per caustic gather "
+                        "(render_kernel.cu:291-294); timed as shipped")
+    return line
 
 
 def run_reference(args):
@@ -330,7 +359,8 @@ def run_reference(args):
     scene = make_scene(args)
     ref = RefHost()
     threads = ref.lib.sheen_ref_max_threads()
-    h = ref.scene(scene.view_ptr, threads)
+    with quiet_stdout():
+        h = ref.scene(scene.view_ptr, threads)
     # ray count of the band: this renderer's counters (bookkeeping only; the
     # timed work below is the reference's code alone)
     ds = sb.DeviceScene(scene, sb.FORM_PLAIN)
@@ -338,12 +368,13 @@ def run_reference(args):
     rays = band_rays(ds, torch.cuda.current_stream().cuda_stream, out)
     ds.close()
     by0, by1 = CPU_BAND[0] // 16, CPU_BAND[1] // 16
-    for _ in range(args.warmup):
-        ref.render(h, W, H, SPP, threads, by0, by0 + 1)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        ref.render(h, W, H, SPP, threads, by0, by1)
-    dt = time.perf_counter() - t0
+    with quiet_stdout():
+        for _ in range(args.warmup):
+            ref.render(h, W, H, SPP, threads, by0, by0 + 1)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ref.render(h, W, H, SPP, threads, by0, by1)
+        dt = time.perf_counter() - t0
     value = rays * args.steps / dt / 1e6
     sample = (f"rows {CPU_BAND[0]}-{CPU_BAND[1]} of the 1920x1080 4 spp frame per step ({rays} rays), "
               f"host-compiled reference render_kernel, {threads} threads")
@@ -498,6 +529,8 @@ def main():
     ap.add_argument("--photons", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
+                    help="launch parameter of the wavefront form (sheen_tune_set), repeatable")
     ap.add_argument("--requests", type=int, default=512, help="serving config: requests in the stream")
     ap.add_argument("--rate", type=float, default=20.0, help="serving config: arrivals per second")
     ap.add_argument("--inflight", type=int, default=4, help="serving config: requests on the GPU at once")
@@ -505,6 +538,11 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
+    if args.tune:
+        import sheen_b200 as sb
+        for kv in args.tune:
+            k, v = kv.split("=", 1)
+            sb.tune_set(k, int(v))
     if args.impl == "reference":
         run_reference(args)
     elif args.config == 4:
