@@ -231,6 +231,22 @@ int sheen_selfcheck_bvh4(const SheenScene* scene);
 int sheen_tune_set(const char* key, int value);
 int sheen_tune_get(const char* key, int* value);
 
+typedef struct SheenTuneResult {
+    int shadow_kernel, refill_min, shadow_blocks_per_sm;   /* the setting kept */
+    int candidates;                                        /* settings timed */
+    double best_ms;                                        /* frame time with it */
+    double default_ms;                                     /* frame time with the setting in force before */
+} SheenTuneResult;
+
+/* Autotuner: times candidate launch parameters (both shadow-stage variants,
+ * refill thresholds 4/8/16/24, shadow blocks per SM) on a resident
+ * SHEEN_FORM_WAVEFRONT scene for one frame shape -- per candidate one
+ * warm-up frame, then `reps` frames timed with CUDA events -- and keeps the
+ * fastest (process-wide, as sheen_tune_set).  Renders into a device buffer it
+ * allocates and frees; synchronous.  0 / -1. */
+int sheen_autotune(SheenDeviceScene scene, int width, int height, int aa_samples, int reps,
+                   SheenTuneResult* out);
+
 /* Owned host scenes: the .sheen loader and the synthetic generators return
  * one.  sheen_owned_view points into storage owned by the handle. */
 typedef struct SheenOwnedScene_* SheenOwnedScene;

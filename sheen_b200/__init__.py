@@ -289,6 +289,47 @@ def tune_get(key: str) -> int:
 TUNE_KEYS = ("wave.shadow_kernel", "wave.refill_min", "wave.shadow_blocks_per_sm")
 
 
+class TuneResult(ctypes.Structure):
+    _fields_ = [("shadow_kernel", ctypes.c_int), ("refill_min", ctypes.c_int),
+                ("shadow_blocks_per_sm", ctypes.c_int), ("candidates", ctypes.c_int),
+                ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double)]
+
+
+def autotune(scene: "DeviceScene", width: int, height: int, aa: int, reps: int = 3, cache: str | None = None,
+             key: str | None = None) -> dict:
+    """Pick the fastest launch parameters for a wavefront scene and frame
+    shape (sheen_autotune) and keep them in force.  With `cache` (a JSON
+    file), a setting found earlier under the same key is applied without
+    timing, and new results are added to the file.  The default key is the
+    scene's device footprint and the frame shape."""
+    import json
+    key = key or f"sm_100a|bytes={scene.device_bytes}|{width}x{height}x{aa}"
+    table = {}
+    if cache and os.path.exists(cache):
+        with open(cache) as f:
+            table = json.load(f)
+        if key in table:
+            for k in TUNE_KEYS:
+                tune_set(k, table[key][k])
+            return dict(table[key], cached=True)
+    L = lib()
+    L.sheen_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                 ctypes.POINTER(TuneResult)]
+    L.sheen_autotune.restype = ctypes.c_int
+    r = TuneResult()
+    _check(L.sheen_autotune(scene.handle, width, height, aa, reps, ctypes.byref(r)))
+    res = {"wave.shadow_kernel": r.shadow_kernel, "wave.refill_min": r.refill_min,
+           "wave.shadow_blocks_per_sm": r.shadow_blocks_per_sm, "candidates": r.candidates,
+           "best_ms": r.best_ms, "default_ms": r.default_ms}
+    if cache:
+        table[key] = res
+        tmp = cache + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(table, f, indent=1, sort_keys=True)
+        os.replace(tmp, cache)
+    return dict(res, cached=False)
+
+
 def write_png(path: str, rgba: np.ndarray) -> None:
     rgba = np.ascontiguousarray(rgba, np.float32)
     _check(lib().sheen_write_png_srgb(path.encode(), rgba.ctypes.data, rgba.shape[1], rgba.shape[0]))

@@ -7,6 +7,7 @@
 #include <atomic>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "engine.h"
 
@@ -70,3 +71,78 @@ int tuning_get(const char* name, int* value) {
 
 extern "C" int sheen_tune_set(const char* key, int value) { return sheen::tuning_set(key, value); }
 extern "C" int sheen_tune_get(const char* key, int* value) { return sheen::tuning_get(key, value); }
+
+// ---------------------------------------------------------------------
+// Autotuner: times the candidate settings on the caller's scene and frame
+// shape, keeps the fastest.
+// ---------------------------------------------------------------------
+namespace sheen {
+namespace {
+
+struct Candidate {
+    int shadow_kernel, refill_min, shadow_blocks_per_sm;
+};
+
+void apply(const Candidate& c) {
+    tuning_set("wave.shadow_kernel", c.shadow_kernel);
+    tuning_set("wave.refill_min", c.refill_min);
+    tuning_set("wave.shadow_blocks_per_sm", c.shadow_blocks_per_sm);
+}
+
+}  // namespace
+}  // namespace sheen
+
+extern "C" int sheen_autotune(SheenDeviceScene h, int W, int H, int aa, int reps, SheenTuneResult* out) {
+    using namespace sheen;
+    auto* s = reinterpret_cast<DeviceScene*>(h);
+    if (!s || !out) { set_error("null scene or result"); return -1; }
+    if (W <= 0 || H <= 0 || aa < 1 || aa > 64) { set_error("bad render params"); return -1; }
+    if (s->form != SHEEN_FORM_WAVEFRONT) { set_error("autotuning applies to SHEEN_FORM_WAVEFRONT scenes"); return -1; }
+    if (reps < 1) reps = 3;
+    const Tuning t0 = tuning();
+    std::vector<Candidate> cands;
+    cands.push_back({t0.shadow_kernel, t0.refill_min, t0.shadow_blocks_per_sm});
+    cands.push_back({0, t0.refill_min, 0});
+    for (int r : {4, 8, 16, 24})
+        for (int b : {0, 4}) cands.push_back({1, r, b});
+    float4* buf = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMalloc(&buf, (size_t)W * H * sizeof(float4));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    double best = 1e30, first = 0.0;
+    int best_i = 0;
+    const Region rg{0, 0, W, H};
+    for (size_t i = 0; i < cands.size() && e == cudaSuccess; i++) {
+        apply(cands[i]);
+        if ((e = launch_wavefront(*s, W, H, aa, rg, buf, st, false)) != cudaSuccess) break;   // warm-up + capture
+        cudaEventRecord(e0, st);
+        for (int k = 0; k < reps && e == cudaSuccess; k++) e = launch_wavefront(*s, W, H, aa, rg, buf, st, false);
+        cudaEventRecord(e1, st);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double per = ms / reps;
+        if (i == 0) first = per;
+        if (per < best) { best = per; best_i = (int)i; }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (st) cudaStreamDestroy(st);
+    cudaFree(buf);
+    if (e != cudaSuccess) {
+        apply({t0.shadow_kernel, t0.refill_min, t0.shadow_blocks_per_sm});
+        set_error(cudaGetErrorString(e));
+        return -1;
+    }
+    apply(cands[best_i]);
+    out->shadow_kernel = cands[best_i].shadow_kernel;
+    out->refill_min = cands[best_i].refill_min;
+    out->shadow_blocks_per_sm = cands[best_i].shadow_blocks_per_sm;
+    out->candidates = (int)cands.size();
+    out->best_ms = best;
+    out->default_ms = first;
+    return 0;
+}

@@ -4,6 +4,9 @@ Every setting must give the same image: the shadow-stage variants only
 schedule the same queries differently (32-ray batches per warp, or lanes
 that take new rays as theirs finish), so images are compared bit for bit.
 """
+import ctypes
+import json
+
 import numpy as np
 import pytest
 
@@ -55,5 +58,50 @@ def test_shadow_variants_give_identical_images(config, seed, detail, photons, sp
         img, st = ds.render_host(W, H, spp, count_rays=True)
         assert np.array_equal(img, ref), (refill, per_sm, float(np.abs(img - ref).max()))
         assert st["total_rays"] == st0["total_rays"]
+    ds.close()
+    scene.close()
+
+
+def test_autotune_rejects_bad_calls():
+    L = sb.lib()
+    L.sheen_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                 ctypes.POINTER(sb.TuneResult)]
+    L.sheen_autotune.restype = ctypes.c_int
+    r = sb.TuneResult()
+    assert L.sheen_autotune(None, 64, 64, 1, 1, ctypes.byref(r)) == -1
+    assert sb.last_error() == "null scene or result"
+
+
+def test_autotune_cache_hit_applies_without_timing(tmp_path, restore_tuning):
+    class FakeScene:          # a cache hit never touches the scene
+        device_bytes = 123
+        handle = None
+    cache = tmp_path / "tune.json"
+    key = "k1"
+    cache.write_text(json.dumps({key: {"wave.shadow_kernel": 0, "wave.refill_min": 16,
+                                       "wave.shadow_blocks_per_sm": 2, "best_ms": 1.0}}))
+    res = sb.autotune(FakeScene(), 64, 64, 1, cache=str(cache), key=key)
+    assert res["cached"] is True
+    assert sb.tune_get("wave.shadow_kernel") == 0
+    assert sb.tune_get("wave.refill_min") == 16
+    assert sb.tune_get("wave.shadow_blocks_per_sm") == 2
+
+
+@pytest.mark.gpu
+def test_autotune_keeps_a_setting_no_slower_than_default(tmp_path, restore_tuning):
+    sb.init(0, 100)
+    scene = sb.generate_scene(1, 8, 4)
+    ds = sb.DeviceScene(scene, sb.FORM_WAVEFRONT)
+    ref, _ = ds.render_host(320, 180, 4)
+    cache = str(tmp_path / "tune.json")
+    res = sb.autotune(ds, 320, 180, 4, reps=2, cache=cache)
+    assert res["cached"] is False and res["candidates"] >= 2
+    assert res["best_ms"] <= res["default_ms"]
+    for k in sb.TUNE_KEYS:
+        assert sb.tune_get(k) == res[k]
+    img, _ = ds.render_host(320, 180, 4)
+    assert np.array_equal(img, ref)
+    again = sb.autotune(ds, 320, 180, 4, cache=cache)
+    assert again["cached"] is True
     ds.close()
     scene.close()
