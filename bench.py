@@ -166,6 +166,10 @@ def make_scene(args):
     scene = sb.generate_scene(args.config, args.seed, args.detail if args.config == 1 else 0, photons)
     st = scene.settings
     W, H, SPP = st["width"], st["height"], st["aa"]
+    # smaller frames of the same scene (profiling captures)
+    W = args.width or W
+    H = args.height or H
+    SPP = args.spp or SPP
     global CPU_BAND
     y0 = (H // 2) // 16 * 16
     CPU_BAND = (y0, min(H, y0 + 32))
@@ -305,7 +309,7 @@ def cpu_baseline(ds, scene, stream, out, steps=1):
             ref.render(h, W, H, SPP, threads, CPU_BAND[0] // 16, CPU_BAND[1] // 16)
         dt = time.perf_counter() - t0
     return {"value": round(rays * steps / dt / 1e6, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
-            "sample": f"rows {CPU_BAND[0]}-{CPU_BAND[1]} of the 1920x1080 4 spp frame ({rays} rays), "
+            "sample": f"rows {CPU_BAND[0]}-{CPU_BAND[1]} of the {W}x{H} {SPP} spp frame ({rays} rays), "
                       f"{steps} pass(es), {dt:.1f} s"}
 
 
@@ -376,7 +380,7 @@ def run_reference(args):
             ref.render(h, W, H, SPP, threads, by0, by1)
         dt = time.perf_counter() - t0
     value = rays * args.steps / dt / 1e6
-    sample = (f"rows {CPU_BAND[0]}-{CPU_BAND[1]} of the 1920x1080 4 spp frame per step ({rays} rays), "
+    sample = (f"rows {CPU_BAND[0]}-{CPU_BAND[1]} of the {W}x{H} {SPP} spp frame per step ({rays} rays), "
               f"host-compiled reference render_kernel, {threads} threads")
     print(json.dumps({
         "impl": "reference", "metric": "Mrays/s", "value": round(value, 3), "unit": "Mrays/s", "n_gpus": 1,
@@ -529,6 +533,9 @@ def main():
     ap.add_argument("--photons", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--width", type=int, default=0, help="override the workload's frame width")
+    ap.add_argument("--height", type=int, default=0, help="override the workload's frame height")
+    ap.add_argument("--spp", type=int, default=0, help="override the workload's samples per pixel")
     ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
                     help="launch parameter of the wavefront form (sheen_tune_set), repeatable")
     ap.add_argument("--requests", type=int, default=512, help="serving config: requests in the stream")

@@ -243,6 +243,167 @@ __device__ __forceinline__ bool mesh_any_q(const DevScene& S, const Ray& r, Coun
     return qmesh_trace<true, COUNT>(S.q_all, q, r.tmax, t, u, v, c) >= 0;
 }
 
+// ---- non-triangle categories: culled, near-first walks ------------------
+//
+// The plain form walks the median BVHs of the other categories in the
+// reference's order and tests every primitive whose leaf box the ray
+// touches (bvh.h:605-922).  The wavefront form walks the same trees but
+// visits the nearer child first and skips every box whose entry distance
+// lies beyond the closest hit found so far.  A box is only ever visited when
+// the reference's own slab test accepts it, so the primitives tested are a
+// subset of the reference's, and the closest hit is the same unless two
+// primitives hit at exactly the same distance.  Entry distances are widened
+// by 2^-20 relative before the comparison, more than the rounding of the
+// slab arithmetic.
+
+// The reference slab test (box_hit_ref) that also returns the entry
+// distance (largest of the three entry planes).
+__device__ __forceinline__ bool box_enter_ref(const Ray& r, float4 a, float4 b, float& tnear) {
+    float ix = 1.0f / r.d.x;
+    float tminX = (a.x - r.o.x) * ix, tmaxX = (b.x - r.o.x) * ix;
+    if (tminX > tmaxX) { float t = tminX; tminX = tmaxX; tmaxX = t; }
+    float iy = 1.0f / r.d.y;
+    float tminY = (a.y - r.o.y) * iy, tmaxY = (b.y - r.o.y) * iy;
+    if (tminY > tmaxY) { float t = tminY; tminY = tmaxY; tmaxY = t; }
+    if (tminX > tmaxY || tminY > tmaxX) return false;
+    if (tminY > tminX) tminX = tminY;
+    if (tmaxY < tmaxX) tmaxX = tmaxY;
+    float iz = 1.0f / r.d.z;
+    float tminZ = (a.z - r.o.z) * iz, tmaxZ = (b.z - r.o.z) * iz;
+    if (tminZ > tmaxZ) { float t = tminZ; tminZ = tmaxZ; tmaxZ = t; }
+    if (tminX > tmaxZ || tminZ > tmaxX) return false;
+    if (tminZ > tminX) tminX = tminZ;
+    tnear = tminX - fabsf(tminX) * 9.5367431640625e-7f;
+    return (tmaxX >= r.tmin) && (tminX <= r.tmax);
+}
+
+// `leaf(prim)` tests one primitive and lowers `best` on a closer hit.
+template <bool COUNT, class Leaf>
+__device__ __forceinline__ void dfs_cull(const BvhNode* __restrict__ nodes, const Ray& r, const float& best,
+                                         Counters& c, Leaf leaf) {
+    int stack[kRefStack];
+    float stack_t[kRefStack];
+    int sp = 0;
+    {
+        const float4 a = __ldg(&nodes[0].a), b = __ldg(&nodes[0].b);
+        float tn;
+        if (COUNT) c.nodes++;
+        if (!box_enter_ref(r, a, b, tn)) return;
+        stack[0] = 0;
+        stack_t[0] = tn;
+        sp = 1;
+    }
+    while (sp > 0) {
+        --sp;
+        if (stack_t[sp] > best) continue;       // NaN entry distances are kept
+        const int id = stack[sp];
+        const float4 a = __ldg(&nodes[id].a), b = __ldg(&nodes[id].b);
+        const int left = __float_as_int(a.w), right = __float_as_int(b.w);
+        if (left < 0) {
+            if (COUNT) c.prims++;
+            leaf(~left);
+            continue;
+        }
+        const float4 la = __ldg(&nodes[left].a), lb = __ldg(&nodes[left].b);
+        const float4 ra = __ldg(&nodes[right].a), rb = __ldg(&nodes[right].b);
+        float tl = 0.0f, tr = 0.0f;
+        if (COUNT) c.nodes += 2;
+        const bool hl = box_enter_ref(r, la, lb, tl) && !(tl > best);
+        const bool hr = box_enter_ref(r, ra, rb, tr) && !(tr > best);
+        if (sp > kRefStack - 2) continue;       // cannot happen for the trees built here
+        if (hl && hr) {
+            const bool l_first = !(tr < tl);
+            stack[sp] = l_first ? right : left; stack_t[sp] = l_first ? tr : tl; sp++;
+            stack[sp] = l_first ? left : right; stack_t[sp] = l_first ? tl : tr; sp++;
+        } else if (hl) {
+            stack[sp] = left; stack_t[sp] = tl; sp++;
+        } else if (hr) {
+            stack[sp] = right; stack_t[sp] = tr; sp++;
+        }
+    }
+}
+
+template <bool COUNT>
+__device__ __forceinline__ bool spheres_cull(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    if (S.num_objects == 0 || !S.sphere_bvh) return false;
+    bool any = false;
+    float best = r.tmax;
+    dfs_cull<COUNT>(S.sphere_bvh, r, best, c, [&](int i) {
+        const Object o = S.objects[i];
+        Hit tmp;
+        if (o.type == 0 && sphere_test(r, f3(o.param1), o.param2, tmp) && tmp.t < best) {
+            h = tmp; h.mat = o.material_id; h.obj = i; best = tmp.t; any = true;
+        }
+    });
+    return any;
+}
+
+template <bool COUNT>
+__device__ __forceinline__ bool strands_cull(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    if (S.num_strands == 0) return false;
+    bool any = false;
+    float best = r.tmax;
+    dfs_cull<COUNT>(S.strand_bvh, r, best, c, [&](int i) {
+        Hit tmp;
+        if (strand_test(r, S.strands[i], S.sweep_points, tmp) && tmp.t < best) {
+            h = tmp; h.obj = -(i + 1); best = tmp.t; any = true;
+        }
+    });
+    return any;
+}
+
+template <bool COUNT>
+__device__ __forceinline__ bool hfs_cull(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    if (S.num_hfs == 0) return false;
+    bool any = false;
+    float best = r.tmax;
+    dfs_cull<COUNT>(S.hf_bvh, r, best, c, [&](int i) {
+        Hit tmp;
+        if (hf_test(r, S.hfs[i], tmp) && tmp.t < best) { h = tmp; h.obj = -(i + 1); best = tmp.t; any = true; }
+    });
+    return any;
+}
+
+template <bool COUNT>
+__device__ __forceinline__ bool ses_cull(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    if (S.num_ses == 0) return false;
+    bool any = false;
+    float best = r.tmax;
+    dfs_cull<COUNT>(S.se_bvh, r, best, c, [&](int i) {
+        Hit tmp;
+        if (se_test(r, S.ses[i], tmp) && tmp.t < best) { h = tmp; h.obj = -(i + 1); best = tmp.t; any = true; }
+    });
+    return any;
+}
+
+template <bool COUNT>
+__device__ __forceinline__ bool lathes_cull(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    if (S.num_lathes == 0) return false;
+    bool any = false;
+    float best = r.tmax;
+    dfs_cull<COUNT>(S.lathe_bvh, r, best, c, [&](int i) {
+        Hit tmp;
+        if (lathe_test(r, S.lathes[i], S.lathe_points, tmp) && tmp.t < best) {
+            h = tmp; h.obj = -(i + 1); best = tmp.t; any = true;
+        }
+    });
+    return any;
+}
+
+template <bool COUNT>
+__device__ __forceinline__ bool prisms_cull(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    if (S.num_prisms == 0) return false;
+    bool any = false;
+    float best = r.tmax;
+    dfs_cull<COUNT>(S.prism_bvh, r, best, c, [&](int i) {
+        Hit tmp;
+        if (prism_test(r, S.prisms[i], S.prism_points, tmp) && tmp.t < best) {
+            h = tmp; h.obj = -(i + 1); best = tmp.t; any = true;
+        }
+    });
+    return any;
+}
+
 // Scene categories a kernel variant compiles in (a scene outside a
 // variant's set runs the full variant).
 enum : int {
@@ -260,13 +421,13 @@ struct FastTracer {
         float best = r.tmax;
         bool hit = false;
         Hit t;
-        if ((F & kCatSpheres) && spheres_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if ((F & kCatStrands) && strands_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatSpheres) && spheres_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatStrands) && strands_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
         if ((F & kCatMesh) && mesh_q<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if ((F & kCatHF) && hfs_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if ((F & kCatSE) && ses_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if ((F & kCatLathe) && lathes_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if ((F & kCatPrism) && prisms_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatHF) && hfs_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatSE) && ses_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatLathe) && lathes_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatPrism) && prisms_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
         if ((F & kCatCSG) && S.csg_root >= 0 && csg_test(S, r, t) && t.t < best) { best = t.t; rec = t; hit = true; }
         if ((F & kCatPlanes) && planes_scan(S, r, t) && t.t < best) { best = t.t; rec = t; hit = true; }
         return hit;
@@ -274,13 +435,13 @@ struct FastTracer {
     __device__ __forceinline__ static int shadow(const DevScene& S, const Ray& r, bool mask_aware, ShadowHit& sh,
                                                  Counters& c) {
         Hit h;
-        if ((F & kCatSpheres) && spheres_ref<COUNT>(S, r, h, c)) return classify_shadow_hit(S, h, mask_aware, sh);
+        if ((F & kCatSpheres) && spheres_cull<COUNT>(S, r, h, c)) return classify_shadow_hit(S, h, mask_aware, sh);
         if (F & kCatMesh) {
             const int m = mesh_shadow_q<COUNT>(S, r, mask_aware, sh, c);
             if (m != kClear) return m;
         }
-        if (((F & kCatHF) && hfs_ref<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_ref<COUNT>(S, r, h, c)) ||
-            ((F & kCatLathe) && lathes_ref<COUNT>(S, r, h, c)) || ((F & kCatPrism) && prisms_ref<COUNT>(S, r, h, c)) ||
+        if (((F & kCatHF) && hfs_cull<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_cull<COUNT>(S, r, h, c)) ||
+            ((F & kCatLathe) && lathes_cull<COUNT>(S, r, h, c)) || ((F & kCatPrism) && prisms_cull<COUNT>(S, r, h, c)) ||
             ((F & kCatCSG) && S.csg_root >= 0 && csg_test(S, r, h)) || ((F & kCatPlanes) && planes_scan(S, r, h)))
             return classify_shadow_hit(S, h, mask_aware, sh);
         return kClear;
@@ -292,25 +453,25 @@ struct FastTracer {
     __device__ __forceinline__ static int shadow_pre_mesh(const DevScene& S, const Ray& r, bool mask_aware,
                                                           ShadowHit& sh, Counters& c) {
         Hit h;
-        if ((F & kCatSpheres) && spheres_ref<COUNT>(S, r, h, c)) return classify_shadow_hit(S, h, mask_aware, sh);
+        if ((F & kCatSpheres) && spheres_cull<COUNT>(S, r, h, c)) return classify_shadow_hit(S, h, mask_aware, sh);
         return -1;
     }
     __device__ __forceinline__ static int shadow_post_mesh(const DevScene& S, const Ray& r, bool mask_aware,
                                                            ShadowHit& sh, Counters& c) {
         Hit h;
-        if (((F & kCatHF) && hfs_ref<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_ref<COUNT>(S, r, h, c)) ||
-            ((F & kCatLathe) && lathes_ref<COUNT>(S, r, h, c)) || ((F & kCatPrism) && prisms_ref<COUNT>(S, r, h, c)) ||
+        if (((F & kCatHF) && hfs_cull<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_cull<COUNT>(S, r, h, c)) ||
+            ((F & kCatLathe) && lathes_cull<COUNT>(S, r, h, c)) || ((F & kCatPrism) && prisms_cull<COUNT>(S, r, h, c)) ||
             ((F & kCatCSG) && S.csg_root >= 0 && csg_test(S, r, h)) || ((F & kCatPlanes) && planes_scan(S, r, h)))
             return classify_shadow_hit(S, h, mask_aware, sh);
         return kClear;
     }
     __device__ __forceinline__ static bool occluded(const DevScene& S, const Ray& r, Counters& c) {
         Hit h;
-        if ((F & kCatSpheres) && spheres_ref<COUNT>(S, r, h, c)) return true;
+        if ((F & kCatSpheres) && spheres_cull<COUNT>(S, r, h, c)) return true;
         if ((F & kCatMesh) && mesh_any_q<COUNT>(S, r, c)) return true;
-        return ((F & kCatHF) && hfs_ref<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_ref<COUNT>(S, r, h, c)) ||
-               ((F & kCatLathe) && lathes_ref<COUNT>(S, r, h, c)) ||
-               ((F & kCatPrism) && prisms_ref<COUNT>(S, r, h, c)) ||
+        return ((F & kCatHF) && hfs_cull<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_cull<COUNT>(S, r, h, c)) ||
+               ((F & kCatLathe) && lathes_cull<COUNT>(S, r, h, c)) ||
+               ((F & kCatPrism) && prisms_cull<COUNT>(S, r, h, c)) ||
                ((F & kCatCSG) && S.csg_root >= 0 && csg_test(S, r, h)) || ((F & kCatPlanes) && planes_scan(S, r, h));
     }
     __device__ __forceinline__ static float strand_depth(const DevScene& S, const Ray& r, Counters& c) {
