@@ -255,9 +255,10 @@ def run_ours(args):
                    "scene_create_s": round(create_s, 3), "device_bytes": ds.device_bytes,
                    "tuning": {k: sb.tune_get(k) for k in sb.TUNE_KEYS}},
         "e2e": {"value": round(e2e, 2), "unit": "Mrays/s",
-                "h2d_bytes_per_step": int(st2["device_bytes"]),
+                "h2d_bytes_per_step": int(st2["upload_bytes"]),
                 "d2h_bytes_per_step": W * H * 16,
-                "call": "sheen_render_scene_rgba (host BVH build + upload + render + readback)"},
+                "call": "sheen_render_scene_rgba (upload + BVH build + render + readback)",
+                "scene_build_ms": round(st2["build_ms"], 1), "scene_upload_ms": round(st2["upload_ms"], 1)},
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": round(achieved_gbs / pk["hbm_gbs"], 4), "traffic": None,
                      "peak_source": pk["src"],

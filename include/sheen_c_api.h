@@ -135,11 +135,13 @@ typedef struct SheenRenderStats {
     unsigned long long total_rays;
     unsigned long long node_visits;      /* box tests issued (counting builds only) */
     unsigned long long prim_tests;       /* primitive tests issued (counting builds only) */
-    double build_ms;                     /* host BVH build */
+    double build_ms;                     /* BVH builds: host, plus the wavefront form's
+                                            triangle BVH4s on the device */
     double upload_ms;                    /* host -> device copies */
     double photon_ms;                    /* photon emission + map build */
     double render_ms;                    /* device time of the render launches */
     unsigned long long device_bytes;     /* resident scene footprint */
+    unsigned long long upload_bytes;     /* bytes copied host -> device for the scene */
 } SheenRenderStats;
 
 /* Render into a caller-owned HOST buffer of width*height float4 (RGBA, linear,
@@ -217,6 +219,16 @@ int sheen_scene_primary_hits(SheenDeviceScene scene, int width, int height, int 
  * depth, or a negative code on a violation.  No device work. */
 int sheen_selfcheck_bvh4(const SheenScene* scene);
 
+/* Builds the wavefront form's three triangle BVH4s (all / blocking /
+ * passable triangles) of a scene with the host builder and with the device
+ * builder and compares them byte for byte.  No counterpart in the reference
+ * (its BVH is built on the host, Scene::build_bvh, scene.h:410-481).
+ * Returns 0 when identical; 1 + 10*set (node count), 2 + 10*set (node
+ * bytes), 3 + 10*set (triangle records) or 4 (depth) for the first
+ * difference, set 0 = all, 1 = blocking, 2 = passable; -1 on error.
+ * times_ms (may be NULL) receives {host build ms, device build ms}. */
+int sheen_bvh4_compare_builders(const SheenScene* scene, double* times_ms);
+
 /* Launch parameters of the wavefront form, by name (process-wide; frames
  * captured under older values are re-captured).  No counterpart in the
  * reference (its launch shape is fixed at 16x16 threads per block,
@@ -227,6 +239,10 @@ int sheen_selfcheck_bvh4(const SheenScene* scene);
  *   "wave.refill_min"            1..32 (default 8): idle lanes that make a
  *                                   warp take new rays (shadow_kernel 1)
  *   "wave.shadow_blocks_per_sm"  0..16 (default 0 = as many as fit)
+ *   "build.device"               1 (default): the wavefront form's triangle
+ *                                   BVH4s are built on the GPU; 0: on the
+ *                                   host.  Both builders give byte-identical
+ *                                   trees; read at sheen_scene_create.
  * Every setting gives the same image; only the speed differs.  0 / -1. */
 int sheen_tune_set(const char* key, int value);
 int sheen_tune_get(const char* key, int* value);

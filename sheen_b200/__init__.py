@@ -45,7 +45,7 @@ class RenderStats(ctypes.Structure):
                 ("node_visits", ctypes.c_ulonglong), ("prim_tests", ctypes.c_ulonglong),
                 ("build_ms", ctypes.c_double), ("upload_ms", ctypes.c_double),
                 ("photon_ms", ctypes.c_double), ("render_ms", ctypes.c_double),
-                ("device_bytes", ctypes.c_ulonglong)]
+                ("device_bytes", ctypes.c_ulonglong), ("upload_bytes", ctypes.c_ulonglong)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -47,6 +47,7 @@ void fill_stats(const sheen::DeviceScene& s, const unsigned long long* t, double
     st->photon_ms = s.photon_ms;
     st->render_ms = render_ms;
     st->device_bytes = s.arena_bytes + s.extra_bytes;
+    st->upload_bytes = s.arena_bytes;
 }
 
 // Launch one frame of `s` into device buffer `out`; optionally count rays

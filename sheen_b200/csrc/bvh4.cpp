@@ -19,6 +19,11 @@
 // {e1 = v1 - v0, 0}, {e2 = v2 - v0, 0}; e1/e2 are the same float
 // subtractions the reference's Moller-Trumbore performs per test
 // (primitives/triangle.h:9-10), so the test's results are unchanged.
+//
+// The arithmetic of every decision (bins, SAH costs, frame exponents,
+// quantisation) is in bvh4_rules.h, shared with the device builder
+// (bvh4_gpu.cu); partitions are stable.  The two builders therefore produce
+// byte-identical trees, which the tests check.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -26,6 +31,7 @@
 #include <thread>
 #include <vector>
 
+#include "bvh4_rules.h"
 #include "engine.h"
 
 namespace sheen {
@@ -41,11 +47,7 @@ struct Box {
     void grow(const float p[3]) {
         for (int k = 0; k < 3; k++) { lo[k] = std::min(lo[k], p[k]); hi[k] = std::max(hi[k], p[k]); }
     }
-    float area() const {
-        float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
-        if (dx < 0.0f) return 0.0f;
-        return 2.0f * (dx * dy + dy * dz + dz * dx);
-    }
+    float area() const { return bvhr::area(lo[0], lo[1], lo[2], hi[0], hi[1], hi[2]); }
 };
 
 struct BNode {
@@ -54,8 +56,8 @@ struct BNode {
     int first = 0, count = 0;    // leaf when count > 0
 };
 
-constexpr int kBins = 16;
-constexpr int kMaxLeaf = 8;
+constexpr int kBins = bvhr::kBins;
+constexpr int kMaxLeaf = bvhr::kMaxLeaf;
 
 struct SahBuilder {
     std::vector<Box> tri_box;
@@ -81,11 +83,10 @@ struct SahBuilder {
             if (!(ext > 0.0f)) continue;
             Box bins[kBins];
             int cnt[kBins] = {0};
-            const float k = (float)kBins / ext;
+            const float k = bvhr::bin_scale(ext);
             for (int i = first; i < first + n; i++) {
                 const int t = idx[(size_t)i];
-                int bi = (int)((cen[3 * (size_t)t + axis] - cb.lo[axis]) * k);
-                bi = std::min(std::max(bi, 0), kBins - 1);
+                const int bi = bvhr::bin_of(cen[3 * (size_t)t + axis], cb.lo[axis], k);
                 cnt[bi]++;
                 bins[bi].grow(tri_box[(size_t)t]);
             }
@@ -105,25 +106,23 @@ struct SahBuilder {
                 lacc.grow(bins[i]);
                 lc += cnt[i];
                 if (lc == 0 || right_cnt[i + 1] == 0) continue;
-                const float cost = lacc.area() * (float)lc + right_area[i + 1] * (float)right_cnt[i + 1];
+                const float cost = bvhr::split_cost(lacc.area(), lc, right_area[i + 1], right_cnt[i + 1]);
                 if (cost < best_cost) { best_cost = cost; best_axis = axis; best_split = i; }
             }
         }
-        const float leaf_cost = b.area() * (float)n;
+        const float leaf_cost = bvhr::mul(b.area(), (float)n);
         const float parent_area = b.area();
         // cost model: traversal 1 (scaled by the parent area), intersection 1 per triangle
-        if (best_axis < 0 || (n <= kMaxLeaf && leaf_cost <= parent_area + best_cost)) {
+        if (best_axis < 0 || (n <= kMaxLeaf && leaf_cost <= bvhr::add(parent_area, best_cost))) {
             if (n <= kMaxLeaf) { out[(size_t)me].first = first; out[(size_t)me].count = n; return me; }
         }
         int mid;
         if (best_axis >= 0) {
             const int axis = best_axis;
-            const float k = (float)kBins / (cb.hi[axis] - cb.lo[axis]);
+            const float k = bvhr::bin_scale(cb.hi[axis] - cb.lo[axis]);
             const float lo = cb.lo[axis];
-            auto it = std::partition(idx.begin() + first, idx.begin() + first + n, [&](int t) {
-                int bi = (int)((cen[3 * (size_t)t + axis] - lo) * k);
-                bi = std::min(std::max(bi, 0), kBins - 1);
-                return bi <= best_split;
+            auto it = std::stable_partition(idx.begin() + first, idx.begin() + first + n, [&](int t) {
+                return bvhr::bin_of(cen[3 * (size_t)t + axis], lo, k) <= best_split;
             });
             mid = (int)(it - idx.begin());
         } else {
@@ -153,20 +152,6 @@ struct SahBuilder {
     }
 };
 
-// Per-axis quantisation of a child interval [a, b] inside a frame starting
-// at `origin` with scale 2^(e-127): outward rounding checked with the
-// device's own decode (fmaf).
-void quantize_axis(float origin, float scale, float a, float b, uint8_t& qlo, uint8_t& qhi) {
-    double fl = std::floor(((double)a - origin) / scale);
-    double fh = std::ceil(((double)b - origin) / scale);
-    int lo = (int)std::max(0.0, std::min(255.0, fl));
-    int hi = (int)std::max(0.0, std::min(255.0, fh));
-    while (lo > 0 && std::fmaf((float)lo, scale, origin) > a) lo--;
-    while (hi < 255 && std::fmaf((float)hi, scale, origin) < b) hi++;
-    qlo = (uint8_t)lo;
-    qhi = (uint8_t)hi;
-}
-
 }  // namespace
 
 void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out) {
@@ -184,8 +169,9 @@ void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out
         const float v[3][3] = {{t.v0.x, t.v0.y, t.v0.z}, {t.v1.x, t.v1.y, t.v1.z}, {t.v2.x, t.v2.y, t.v2.z}};
         Box b;
         for (int k = 0; k < 3; k++) b.grow(v[k]);
+        for (int k = 0; k < 3; k++) { b.lo[k] = bvhr::canon(b.lo[k]); b.hi[k] = bvhr::canon(b.hi[k]); }
         sb.tri_box[(size_t)i] = b;
-        for (int k = 0; k < 3; k++) sb.cen[3 * (size_t)i + k] = 0.5f * (b.lo[k] + b.hi[k]);
+        for (int k = 0; k < 3; k++) sb.cen[3 * (size_t)i + k] = bvhr::centroid(b.lo[k], b.hi[k]);
         sb.idx[(size_t)i] = i;
     }
     std::vector<BNode> bn;
@@ -256,11 +242,7 @@ void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out
         int ebits[3];
         for (int a = 0; a < 3; a++) {
             origin[a] = nb.lo[a];
-            const double ext = (double)nb.hi[a] - (double)nb.lo[a];
-            int e = ext > 0.0 ? (int)std::ceil(std::log2(ext / 254.0)) : -20;
-            e = std::max(-100, std::min(100, e));
-            // make sure the whole extent fits below q = 255 after outward rounding
-            while (std::fmaf(255.0f, std::ldexp(1.0f, e), origin[a]) < nb.hi[a] && e < 100) e++;
+            const int e = bvhr::frame_exponent(nb.lo[a], nb.hi[a]);
             scale[a] = std::ldexp(1.0f, e);
             ebits[a] = e + 127;
         }
@@ -273,7 +255,7 @@ void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out
         for (size_t k = 0; k < kids.size(); k++) {
             const BNode& c = bn[(size_t)kids[k]];
             for (int a = 0; a < 3; a++)
-                quantize_axis(origin[a], scale[a], c.box.lo[a], c.box.hi[a], q[2 * a][k], q[2 * a + 1][k]);
+                bvhr::quantize_axis(origin[a], scale[a], c.box.lo[a], c.box.hi[a], q[2 * a][k], q[2 * a + 1][k]);
             if (c.count > 0) {
                 child[k] = 0x80000000u | ((uint32_t)c.first << 3) | (uint32_t)(c.count - 1);
             } else {

@@ -1,0 +1,1129 @@
+// bvh4_gpu.cu -- the wavefront form's triangle BVH4, built on the device.
+//
+// Same algorithm and the same arithmetic (bvh4_rules.h) as the host builder
+// (bvh4.cpp), so both produce byte-identical node and triangle arrays:
+//   1. triangle boxes of the subset, root box and root centroid box;
+//   2. large nodes (more than kSmall triangles), one tree level per pass:
+//      binned SAH (16 bins per axis over the centroid box) counted in
+//      shared memory per 4096-triangle chunk and merged with atomics,
+//      split chosen by one warp per node, stable partition by a scan over
+//      the chunks in order;
+//   3. small nodes: one block builds the whole subtree in shared memory,
+//      continuing with the smaller child and stacking the larger;
+//   4. collapse to 4-wide nodes breadth first, one level per pass (the
+//      host's greedy rule: open the inner child of largest area until there
+//      are four), child boxes quantised outward in the node's frame, and the
+//      triangles written in leaf order.
+// Node numbering of the intermediate binary tree differs from the host's;
+// the collapse walks the tree structure only, so the output does not.
+// Min/max reductions run as integer atomics on an order-preserving encoding
+// of the floats; they are exact, so reduction order does not matter.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cfloat>
+#include <climits>
+#include <cstring>
+#include <vector>
+
+#include "bvh4_rules.h"
+#include "engine.h"
+
+namespace sheen {
+namespace bvhg {
+
+using namespace bvhr;
+
+constexpr int kSmall = 1024;                      // subtree size built by one block
+constexpr int kSmallThreads = 128;
+constexpr int kSmallPer = kSmall / kSmallThreads;
+constexpr int kChunk = 4096;                      // triangles per block in the large passes
+constexpr int kChunkThreads = 256;
+constexpr int kChunkPer = kChunk / kChunkThreads;
+constexpr int kBinWords = 13;                     // count, box lo/hi, centroid lo/hi
+constexpr int kNodeBins = 3 * kBins * kBinWords;
+constexpr int kCandidates = 3 * (kBins - 1);
+constexpr int kMaxLargeLevels = 4096;
+
+__device__ __forceinline__ int ford(float f) {
+    const int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float funord(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+// Initial value of word w of a bin (count 0, empty boxes).
+__device__ __forceinline__ int bin_init(int w) {
+    const int k = w % kBinWords;
+    if (k == 0) return 0;
+    const bool is_lo = (k >= 1 && k <= 3) || (k >= 7 && k <= 9);
+    return ford(is_lo ? FLT_MAX : -FLT_MAX);
+}
+
+// Binary node of the build.
+struct __align__(16) BNode {
+    float lo[3], hi[3];     // box of the triangle boxes
+    float clo[3], chi[3];   // box of the triangle centroids
+    int first, count;       // triangle range in idx
+    int left, right;        // children, -1 for a leaf
+};
+static_assert(sizeof(BNode) == 64, "BNode is 64 bytes");
+
+__device__ __forceinline__ void add_to_bin(int* B, const float l[3], const float h[3], const float c[3]) {
+    atomicAdd(B, 1);
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        atomicMin(B + 1 + q, ford(l[q]));
+        atomicMax(B + 4 + q, ford(h[q]));
+        atomicMin(B + 7 + q, ford(c[q]));
+        atomicMax(B + 10 + q, ford(c[q]));
+    }
+}
+
+// Union of bins [b0, b1] of one axis into box/centroid box; returns the count.
+__device__ __forceinline__ int bin_union(const int* A, int b0, int b1, float lo[3], float hi[3], float clo[3],
+                                         float chi[3]) {
+    int n = 0;
+    for (int q = 0; q < 3; q++) { lo[q] = FLT_MAX; hi[q] = -FLT_MAX; clo[q] = FLT_MAX; chi[q] = -FLT_MAX; }
+    for (int i = b0; i <= b1; i++) {
+        const int* b = A + i * kBinWords;
+        n += b[0];
+        for (int q = 0; q < 3; q++) {
+            lo[q] = fminf(lo[q], funord(b[1 + q]));
+            hi[q] = fmaxf(hi[q], funord(b[4 + q]));
+            clo[q] = fminf(clo[q], funord(b[7 + q]));
+            chi[q] = fmaxf(chi[q], funord(b[10 + q]));
+        }
+    }
+    return n;
+}
+
+// SAH cost of candidate `cand` (axis cand / 15, split after bin cand % 15);
+// false when the host loop skips it (flat axis, or an empty side).
+__device__ __forceinline__ bool eval_candidate(const int* bins, const float clo[3], const float chi[3], int cand,
+                                               float& cost) {
+    const int a = cand / (kBins - 1), s = cand % (kBins - 1);
+    const float ext = sub(chi[a], clo[a]);
+    if (!(ext > 0.0f)) return false;
+    const int* A = bins + a * kBins * kBinWords;
+    float llo[3], lhi[3], lclo[3], lchi[3], rlo[3], rhi[3], rclo[3], rchi[3];
+    const int lc = bin_union(A, 0, s, llo, lhi, lclo, lchi);
+    const int rc = bin_union(A, s + 1, kBins - 1, rlo, rhi, rclo, rchi);
+    if (lc == 0 || rc == 0) return false;
+    cost = split_cost(area(llo[0], llo[1], llo[2], lhi[0], lhi[1], lhi[2]), lc,
+                      area(rlo[0], rlo[1], rlo[2], rhi[0], rhi[1], rhi[2]), rc);
+    return true;
+}
+
+// Best candidate over one warp: lowest cost, ties to the lowest index (the
+// host's strict "<" in candidate order).  Every lane gets the result; the
+// index is INT_MAX when no candidate qualifies.
+__device__ __forceinline__ void warp_best(const int* bins, const float clo[3], const float chi[3], float& best_cost,
+                                          int& best) {
+    const int lane = threadIdx.x & 31;
+    best_cost = FLT_MAX;
+    best = INT_MAX;
+    for (int cand = lane; cand < kCandidates; cand += 32) {
+        float cost;
+        if (eval_candidate(bins, clo, chi, cand, cost) && cost < best_cost) { best_cost = cost; best = cand; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const float oc = __shfl_xor_sync(0xffffffffu, best_cost, o);
+        const int ob = __shfl_xor_sync(0xffffffffu, best, o);
+        if (oc < best_cost || (oc == best_cost && ob < best)) { best_cost = oc; best = ob; }
+    }
+}
+
+// ---- 1. triangle boxes ----------------------------------------------------
+
+__global__ void k_init_ord(int* ord, int n12) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n12) {
+        const int k = i % 12;
+        ord[i] = ford((k < 3 || (k >= 6 && k < 9)) ? FLT_MAX : -FLT_MAX);
+    }
+}
+
+// ord layout per record: lo[3], hi[3], clo[3], chi[3]
+__global__ void __launch_bounds__(256) k_prep(const Triangle* __restrict__ tris, const int* __restrict__ subset, int n,
+                                              float4* __restrict__ plo, float4* __restrict__ phi,
+                                              int* __restrict__ idx, int* __restrict__ root_ord) {
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    float clo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, chi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Triangle& t = tris[subset ? subset[i] : i];
+        const float v0[3] = {t.v0.x, t.v0.y, t.v0.z}, v1[3] = {t.v1.x, t.v1.y, t.v1.z},
+                    v2[3] = {t.v2.x, t.v2.y, t.v2.z};
+        float bl[3], bh[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            bl[k] = canon(fminf(fminf(fminf(FLT_MAX, v0[k]), v1[k]), v2[k]));
+            bh[k] = canon(fmaxf(fmaxf(fmaxf(-FLT_MAX, v0[k]), v1[k]), v2[k]));
+            const float c = centroid(bl[k], bh[k]);
+            lo[k] = fminf(lo[k], bl[k]); hi[k] = fmaxf(hi[k], bh[k]);
+            clo[k] = fminf(clo[k], c); chi[k] = fmaxf(chi[k], c);
+        }
+        plo[i] = make_float4(bl[0], bl[1], bl[2], 0.0f);
+        phi[i] = make_float4(bh[0], bh[1], bh[2], 0.0f);
+        idx[i] = i;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+            hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+            clo[k] = fminf(clo[k], __shfl_xor_sync(0xffffffffu, clo[k], o));
+            chi[k] = fmaxf(chi[k], __shfl_xor_sync(0xffffffffu, chi[k], o));
+        }
+    if ((threadIdx.x & 31) == 0) {
+        for (int k = 0; k < 3; k++) {
+            atomicMin(&root_ord[k], ford(lo[k]));
+            atomicMax(&root_ord[3 + k], ford(hi[k]));
+            atomicMin(&root_ord[6 + k], ford(clo[k]));
+            atomicMax(&root_ord[9 + k], ford(chi[k]));
+        }
+    }
+}
+
+__global__ void k_root(const int* __restrict__ root_ord, int n, BNode* __restrict__ nodes) {
+    if (threadIdx.x != 0) return;
+    BNode r;
+    for (int k = 0; k < 3; k++) {
+        r.lo[k] = funord(root_ord[k]);
+        r.hi[k] = funord(root_ord[3 + k]);
+        r.clo[k] = funord(root_ord[6 + k]);
+        r.chi[k] = funord(root_ord[9 + k]);
+    }
+    r.first = 0;
+    r.count = n;
+    r.left = r.right = -1;
+    nodes[0] = r;
+}
+
+// ---- 2. large nodes --------------------------------------------------------
+
+// Node slot of chunk c: the last j with chunk_base[j] <= c.
+__device__ __forceinline__ int chunk_node(const int* __restrict__ chunk_base, int m, int c) {
+    int lo = 0, hi = m - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (chunk_base[mid] <= c) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void k_init_bins(int* __restrict__ bins, int words) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < words) bins[i] = bin_init(i % kNodeBins);
+}
+
+__global__ void __launch_bounds__(kChunkThreads) k_bin_large(const int* __restrict__ work, const int* __restrict__ chunk_base,
+                                                             int m, const BNode* __restrict__ nodes,
+                                                             const float4* __restrict__ plo, const float4* __restrict__ phi,
+                                                             const int* __restrict__ idx, int* __restrict__ gbins) {
+    __shared__ int sb[kNodeBins];
+    const int c = blockIdx.x;
+    const int j = chunk_node(chunk_base, m, c);
+    const BNode nd = nodes[work[j]];
+    const int start = nd.first + (c - chunk_base[j]) * kChunk;
+    const int end = min(start + kChunk, nd.first + nd.count);
+    for (int w = threadIdx.x; w < kNodeBins; w += kChunkThreads) sb[w] = bin_init(w);
+    __syncthreads();
+    float ext[3], kk[3];
+    for (int a = 0; a < 3; a++) {
+        ext[a] = sub(nd.chi[a], nd.clo[a]);
+        kk[a] = ext[a] > 0.0f ? bin_scale(ext[a]) : 0.0f;
+    }
+    for (int pos = start + threadIdx.x; pos < end; pos += kChunkThreads) {
+        const int p = idx[pos];
+        const float4 L = plo[p], H = phi[p];
+        const float l[3] = {L.x, L.y, L.z}, h[3] = {H.x, H.y, H.z};
+        const float cc[3] = {centroid(l[0], h[0]), centroid(l[1], h[1]), centroid(l[2], h[2])};
+        for (int a = 0; a < 3; a++) {
+            if (!(ext[a] > 0.0f)) continue;
+            const int b = bin_of(cc[a], nd.clo[a], kk[a]);
+            add_to_bin(sb + (a * kBins + b) * kBinWords, l, h, cc);
+        }
+    }
+    __syncthreads();
+    int* G = gbins + (size_t)j * kNodeBins;
+    for (int w = threadIdx.x; w < kNodeBins; w += kChunkThreads) {
+        const int v = sb[w];
+        const int k = w % kBinWords;
+        if (k == 0) {
+            if (v) atomicAdd(&G[w], v);
+        } else if (v != bin_init(w)) {
+            const bool is_lo = (k >= 1 && k <= 3) || (k >= 7 && k <= 9);
+            if (is_lo) atomicMin(&G[w], v);
+            else atomicMax(&G[w], v);
+        }
+    }
+}
+
+// split[j] = {axis or -1 (list split in half), bin, left count, 0}
+__global__ void __launch_bounds__(32) k_split_large(const int* __restrict__ work, int m, int next_id,
+                                                    BNode* __restrict__ nodes, const int* __restrict__ gbins,
+                                                    int4* __restrict__ split, int2* __restrict__ child_fc) {
+    const int j = blockIdx.x;
+    const int id = work[j];
+    const BNode nd = nodes[id];
+    const int* B = gbins + (size_t)j * kNodeBins;
+    float best_cost;
+    int best;
+    warp_best(B, nd.clo, nd.chi, best_cost, best);
+    if (threadIdx.x != 0) return;
+    const int n = nd.count;                  // > kSmall > kMaxLeaf: never a leaf
+    const int left_id = next_id + 2 * j, right_id = left_id + 1;
+    BNode L, R;
+    int nleft;
+    if (best != INT_MAX) {
+        const int a = best / (kBins - 1), s = best % (kBins - 1);
+        const int* A = B + a * kBins * kBinWords;
+        nleft = bin_union(A, 0, s, L.lo, L.hi, L.clo, L.chi);
+        bin_union(A, s + 1, kBins - 1, R.lo, R.hi, R.clo, R.chi);
+        split[j] = make_int4(a, s, nleft, 0);
+    } else {
+        nleft = n / 2;                          // bounds filled in by k_list_split_bounds
+        for (int q = 0; q < 3; q++) {
+            L.lo[q] = R.lo[q] = FLT_MAX; L.hi[q] = R.hi[q] = -FLT_MAX;
+            L.clo[q] = R.clo[q] = FLT_MAX; L.chi[q] = R.chi[q] = -FLT_MAX;
+        }
+        split[j] = make_int4(-1, 0, nleft, 0);
+    }
+    L.first = nd.first; L.count = nleft; L.left = L.right = -1;
+    R.first = nd.first + nleft; R.count = n - nleft; R.left = R.right = -1;
+    nodes[left_id] = L;
+    nodes[right_id] = R;
+    nodes[id].left = left_id;
+    nodes[id].right = right_id;
+    child_fc[2 * j] = make_int2(L.first, L.count);
+    child_fc[2 * j + 1] = make_int2(R.first, R.count);
+}
+
+__device__ __forceinline__ bool goes_left_large(const BNode& nd, int4 sp, float k_axis, int pos, int p,
+                                                const float4* __restrict__ plo, const float4* __restrict__ phi) {
+    if (sp.x < 0) return pos - nd.first < sp.z;
+    const float4 L = plo[p], H = phi[p];
+    const float lo = sp.x == 0 ? L.x : (sp.x == 1 ? L.y : L.z);
+    const float hi = sp.x == 0 ? H.x : (sp.x == 1 ? H.y : H.z);
+    return bin_of(centroid(lo, hi), nd.clo[sp.x], k_axis) <= sp.y;
+}
+
+__device__ __forceinline__ float split_scale(const BNode& nd, int4 sp) {
+    return sp.x >= 0 ? bin_scale(sub(nd.chi[sp.x], nd.clo[sp.x])) : 0.0f;
+}
+
+// Bounds of the two halves of a list split (every centroid equal): rare.
+__global__ void __launch_bounds__(kChunkThreads) k_list_split_bounds(const int* __restrict__ work, const int* __restrict__ chunk_base,
+                                                                     int m, const BNode* __restrict__ nodes,
+                                                                     const int4* __restrict__ split,
+                                                                     const float4* __restrict__ plo,
+                                                                     const float4* __restrict__ phi,
+                                                                     const int* __restrict__ idx, int* __restrict__ child_ord) {
+    const int c = blockIdx.x;
+    const int j = chunk_node(chunk_base, m, c);
+    const int4 sp = split[j];
+    if (sp.x >= 0) return;
+    const BNode nd = nodes[work[j]];
+    const int start = nd.first + (c - chunk_base[j]) * kChunk;
+    const int end = min(start + kChunk, nd.first + nd.count);
+    for (int pos = start + threadIdx.x; pos < end; pos += kChunkThreads) {
+        const int p = idx[pos];
+        const float4 L = plo[p], H = phi[p];
+        const float l[3] = {L.x, L.y, L.z}, h[3] = {H.x, H.y, H.z};
+        int* o = child_ord + (size_t)(2 * j + (pos - nd.first < sp.z ? 0 : 1)) * 12;
+        for (int q = 0; q < 3; q++) {
+            const float cc = centroid(l[q], h[q]);
+            atomicMin(&o[q], ford(l[q]));
+            atomicMax(&o[3 + q], ford(h[q]));
+            atomicMin(&o[6 + q], ford(cc));
+            atomicMax(&o[9 + q], ford(cc));
+        }
+    }
+}
+
+__global__ void k_list_split_write(int m, int next_id, const int4* __restrict__ split, const int* __restrict__ child_ord,
+                                   BNode* __restrict__ nodes) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;   // child slot 0 .. 2m-1
+    if (i >= 2 * m || split[i / 2].x >= 0) return;
+    BNode& c = nodes[next_id + i];
+    const int* o = child_ord + (size_t)i * 12;
+    for (int q = 0; q < 3; q++) {
+        c.lo[q] = funord(o[q]);
+        c.hi[q] = funord(o[3 + q]);
+        c.clo[q] = funord(o[6 + q]);
+        c.chi[q] = funord(o[9 + q]);
+    }
+}
+
+__global__ void __launch_bounds__(kChunkThreads) k_part_count(const int* __restrict__ work, const int* __restrict__ chunk_base,
+                                                              int m, const BNode* __restrict__ nodes,
+                                                              const int4* __restrict__ split,
+                                                              const float4* __restrict__ plo,
+                                                              const float4* __restrict__ phi,
+                                                              const int* __restrict__ idx, int* __restrict__ chunk_left) {
+    typedef cub::BlockReduce<int, kChunkThreads> Reduce;
+    __shared__ typename Reduce::TempStorage tmp;
+    const int c = blockIdx.x;
+    const int j = chunk_node(chunk_base, m, c);
+    const BNode nd = nodes[work[j]];
+    const int4 sp = split[j];
+    const float k_axis = split_scale(nd, sp);
+    const int start = nd.first + (c - chunk_base[j]) * kChunk;
+    const int end = min(start + kChunk, nd.first + nd.count);
+    int cnt = 0;
+    for (int pos = start + threadIdx.x; pos < end; pos += kChunkThreads)
+        cnt += goes_left_large(nd, sp, k_axis, pos, idx[pos], plo, phi) ? 1 : 0;
+    const int total = Reduce(tmp).Sum(cnt);
+    if (threadIdx.x == 0) chunk_left[c] = total;
+}
+
+// Stable scatter of each chunk into its node's left / right ranges of tmp.
+__global__ void __launch_bounds__(kChunkThreads) k_part_scatter(const int* __restrict__ work, const int* __restrict__ chunk_base,
+                                                                int m, const BNode* __restrict__ nodes,
+                                                                const int4* __restrict__ split,
+                                                                const float4* __restrict__ plo,
+                                                                const float4* __restrict__ phi,
+                                                                const int* __restrict__ idx,
+                                                                const int* __restrict__ chunk_off, int* __restrict__ tmp,
+                                                                int* __restrict__ err) {
+    typedef cub::BlockScan<int, kChunkThreads> Scan;
+    __shared__ typename Scan::TempStorage scan_tmp;
+    const int c = blockIdx.x;
+    const int j = chunk_node(chunk_base, m, c);
+    const BNode nd = nodes[work[j]];
+    const int4 sp = split[j];
+    const float k_axis = split_scale(nd, sp);
+    const int start = nd.first + (c - chunk_base[j]) * kChunk;
+    const int end = min(start + kChunk, nd.first + nd.count);
+    const int left_before = chunk_off[c] - chunk_off[chunk_base[j]];
+    const int right_before = (start - nd.first) - left_before;
+    int p[kChunkPer];
+    bool f[kChunkPer];
+    int cnt = 0;
+    const int t0 = start + threadIdx.x * kChunkPer;
+#pragma unroll
+    for (int e = 0; e < kChunkPer; e++) {
+        const int pos = t0 + e;
+        f[e] = false;
+        p[e] = 0;
+        if (pos < end) {
+            p[e] = idx[pos];
+            f[e] = goes_left_large(nd, sp, k_axis, pos, p[e], plo, phi);
+            cnt += f[e] ? 1 : 0;
+        }
+    }
+    int lpos;
+    Scan(scan_tmp).ExclusiveSum(cnt, lpos);
+    int rpos = min(threadIdx.x * kChunkPer, end - start) - lpos;
+    lpos += nd.first + left_before;
+    rpos += nd.first + sp.z + right_before;
+    // Both sides stay inside the node (the bins and this pass classify with
+    // the same function); a position outside it is recorded, not written.
+    const int lend = nd.first + sp.z, rend = nd.first + nd.count;
+#pragma unroll
+    for (int e = 0; e < kChunkPer; e++) {
+        if (t0 + e >= end) break;
+        if (f[e]) {
+            if (lpos < lend) tmp[lpos++] = p[e];
+            else *err = 2;
+        } else {
+            if (rpos >= lend && rpos < rend) tmp[rpos++] = p[e];
+            else *err = 2;
+        }
+    }
+}
+
+__global__ void k_copy_back(const int* __restrict__ work, const int* __restrict__ chunk_base, int m,
+                            const BNode* __restrict__ nodes, const int* __restrict__ tmp, int* __restrict__ idx) {
+    const int c = blockIdx.x;
+    const int j = chunk_node(chunk_base, m, c);
+    const BNode nd = nodes[work[j]];
+    const int start = nd.first + (c - chunk_base[j]) * kChunk;
+    const int end = min(start + kChunk, nd.first + nd.count);
+    for (int pos = start + threadIdx.x; pos < end; pos += blockDim.x) idx[pos] = tmp[pos];
+}
+
+// ---- 3. small subtrees -----------------------------------------------------
+
+struct SmallFrame {
+    int first, count, id, pad;
+    float lo[3], hi[3], clo[3], chi[3];
+};
+
+constexpr int kSmallStack = 24;
+
+__global__ void __launch_bounds__(kSmallThreads) k_small(const int* __restrict__ list, const int* __restrict__ id_base,
+                                                         const float4* __restrict__ plo, const float4* __restrict__ phi,
+                                                         int* __restrict__ idx, BNode* __restrict__ nodes,
+                                                         int* __restrict__ err) {
+    __shared__ float s_box[6][kSmall];
+    __shared__ int s_pid[kSmall];
+    __shared__ unsigned short s_perm[kSmall];
+    __shared__ unsigned short s_tmp[kSmall];
+    __shared__ int s_bins[kNodeBins];
+    __shared__ int s_cb[24];
+    __shared__ SmallFrame s_stack[kSmallStack];
+    __shared__ SmallFrame s_cur;
+    __shared__ int s_sp, s_next, s_done, s_best, s_leaf;
+    typedef cub::BlockScan<int, kSmallThreads> Scan;
+    __shared__ typename Scan::TempStorage s_scan;
+
+    const int tid = threadIdx.x;
+    const int root = list[blockIdx.x];
+    const int gfirst = nodes[root].first, n0 = nodes[root].count;
+    for (int k = tid; k < n0; k += kSmallThreads) {
+        const int p = idx[gfirst + k];
+        const float4 l = plo[p], h = phi[p];
+        s_box[0][k] = l.x; s_box[1][k] = l.y; s_box[2][k] = l.z;
+        s_box[3][k] = h.x; s_box[4][k] = h.y; s_box[5][k] = h.z;
+        s_pid[k] = p;
+        s_perm[k] = (unsigned short)k;
+    }
+    if (tid == 0) {
+        const BNode r = nodes[root];
+        s_cur.first = 0; s_cur.count = n0; s_cur.id = root; s_cur.pad = 0;
+        for (int q = 0; q < 3; q++) {
+            s_cur.lo[q] = r.lo[q]; s_cur.hi[q] = r.hi[q]; s_cur.clo[q] = r.clo[q]; s_cur.chi[q] = r.chi[q];
+        }
+        s_sp = 0;
+        s_next = id_base[blockIdx.x];
+        s_done = 0;
+    }
+    __syncthreads();
+    while (true) {
+        const SmallFrame cur = s_cur;
+        __syncthreads();   // every thread has its copy before thread 0 may replace s_cur
+        const int n = cur.count;
+        bool leaf = n <= 2;
+        if (!leaf) {
+            for (int w = tid; w < kNodeBins; w += kSmallThreads) s_bins[w] = bin_init(w);
+            __syncthreads();
+            float ext[3], kk[3];
+            for (int a = 0; a < 3; a++) {
+                ext[a] = sub(cur.chi[a], cur.clo[a]);
+                kk[a] = ext[a] > 0.0f ? bin_scale(ext[a]) : 0.0f;
+            }
+            for (int k = tid; k < n; k += kSmallThreads) {
+                const int s = s_perm[cur.first + k];
+                const float l[3] = {s_box[0][s], s_box[1][s], s_box[2][s]};
+                const float h[3] = {s_box[3][s], s_box[4][s], s_box[5][s]};
+                const float cc[3] = {centroid(l[0], h[0]), centroid(l[1], h[1]), centroid(l[2], h[2])};
+                for (int a = 0; a < 3; a++) {
+                    if (!(ext[a] > 0.0f)) continue;
+                    add_to_bin(s_bins + (a * kBins + bin_of(cc[a], cur.clo[a], kk[a])) * kBinWords, l, h, cc);
+                }
+            }
+            __syncthreads();
+            if (tid < 32) {
+                float bc;
+                int bi;
+                warp_best(s_bins, cur.clo, cur.chi, bc, bi);
+                if (tid == 0) {
+                    const int best = bi == INT_MAX ? -1 : bi;
+                    const float pa = area(cur.lo[0], cur.lo[1], cur.lo[2], cur.hi[0], cur.hi[1], cur.hi[2]);
+                    const float leaf_cost = mul(pa, (float)n);
+                    int lf = 0;
+                    if (best < 0 || (n <= kMaxLeaf && leaf_cost <= add(pa, bc))) {
+                        if (n <= kMaxLeaf) lf = 1;
+                    }
+                    s_best = best;
+                    s_leaf = lf;
+                }
+            }
+            __syncthreads();
+            leaf = s_leaf != 0;
+        }
+        if (leaf) {
+            if (tid == 0) {
+                BNode o;
+                for (int q = 0; q < 3; q++) {
+                    o.lo[q] = cur.lo[q]; o.hi[q] = cur.hi[q]; o.clo[q] = cur.clo[q]; o.chi[q] = cur.chi[q];
+                }
+                o.first = gfirst + cur.first;
+                o.count = n;
+                o.left = o.right = -1;
+                nodes[cur.id] = o;
+                if (s_sp == 0) s_done = 1;
+                else s_cur = s_stack[--s_sp];
+            }
+            __syncthreads();
+            if (s_done) break;
+            continue;
+        }
+        // Stable partition of s_perm[cur.first, cur.first + n).
+        const int best = s_best;
+        const int axis = best >= 0 ? best / (kBins - 1) : -1;
+        const int sbin = best >= 0 ? best % (kBins - 1) : 0;
+        const float k_axis = axis >= 0 ? bin_scale(sub(cur.chi[axis], cur.clo[axis])) : 0.0f;
+        bool f[kSmallPer];
+        int cnt = 0;
+#pragma unroll
+        for (int e = 0; e < kSmallPer; e++) {
+            const int k = tid * kSmallPer + e;
+            f[e] = false;
+            if (k < n) {
+                if (axis >= 0) {
+                    const int s = s_perm[cur.first + k];
+                    f[e] = bin_of(centroid(s_box[axis][s], s_box[3 + axis][s]), cur.clo[axis], k_axis) <= sbin;
+                } else {
+                    f[e] = k < n / 2;
+                }
+                cnt += f[e] ? 1 : 0;
+            }
+        }
+        int lpos, nleft;
+        Scan(s_scan).ExclusiveSum(cnt, lpos, nleft);
+        int rpos = min(tid * kSmallPer, n) - lpos;
+#pragma unroll
+        for (int e = 0; e < kSmallPer; e++) {
+            const int k = tid * kSmallPer + e;
+            if (k >= n) break;
+            const unsigned short v = s_perm[cur.first + k];
+            if (f[e]) s_tmp[cur.first + lpos++] = v;
+            else s_tmp[cur.first + nleft + rpos++] = v;
+        }
+        __syncthreads();
+        for (int k = tid; k < n; k += kSmallThreads) s_perm[cur.first + k] = s_tmp[cur.first + k];
+        int mid = cur.first + (axis >= 0 ? nleft : n / 2);
+        bool forced = false;
+        if (mid == cur.first || mid == cur.first + n) { mid = cur.first + n / 2; forced = true; }
+        const bool from_bins = axis >= 0 && !forced;
+        if (!from_bins) {
+            if (tid < 24) s_cb[tid] = ford(((tid % 12) < 3 || ((tid % 12) >= 6 && (tid % 12) < 9)) ? FLT_MAX : -FLT_MAX);
+            __syncthreads();
+            for (int k = tid; k < n; k += kSmallThreads) {
+                const int s = s_perm[cur.first + k];
+                int* o = s_cb + (cur.first + k < mid ? 0 : 12);
+                for (int q = 0; q < 3; q++) {
+                    const float lq = s_box[q][s], hq = s_box[3 + q][s], cq = centroid(lq, hq);
+                    atomicMin(&o[q], ford(lq));
+                    atomicMax(&o[3 + q], ford(hq));
+                    atomicMin(&o[6 + q], ford(cq));
+                    atomicMax(&o[9 + q], ford(cq));
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            SmallFrame L, R;
+            L.first = cur.first; L.count = mid - cur.first; L.pad = 0;
+            R.first = mid; R.count = cur.first + n - mid; R.pad = 0;
+            if (from_bins) {
+                const int* A = s_bins + axis * kBins * kBinWords;
+                bin_union(A, 0, sbin, L.lo, L.hi, L.clo, L.chi);
+                bin_union(A, sbin + 1, kBins - 1, R.lo, R.hi, R.clo, R.chi);
+            } else {
+                for (int q = 0; q < 3; q++) {
+                    L.lo[q] = funord(s_cb[q]); L.hi[q] = funord(s_cb[3 + q]);
+                    L.clo[q] = funord(s_cb[6 + q]); L.chi[q] = funord(s_cb[9 + q]);
+                    R.lo[q] = funord(s_cb[12 + q]); R.hi[q] = funord(s_cb[15 + q]);
+                    R.clo[q] = funord(s_cb[18 + q]); R.chi[q] = funord(s_cb[21 + q]);
+                }
+            }
+            L.id = s_next;
+            R.id = s_next + 1;
+            s_next += 2;
+            BNode o;
+            for (int q = 0; q < 3; q++) {
+                o.lo[q] = cur.lo[q]; o.hi[q] = cur.hi[q]; o.clo[q] = cur.clo[q]; o.chi[q] = cur.chi[q];
+            }
+            o.first = gfirst + cur.first;
+            o.count = n;
+            o.left = L.id;
+            o.right = R.id;
+            nodes[cur.id] = o;
+            if (s_sp >= kSmallStack) {
+                *err = 1;
+                s_done = 1;
+            } else if (R.count >= L.count) {
+                s_stack[s_sp++] = R;
+                s_cur = L;
+            } else {
+                s_stack[s_sp++] = L;
+                s_cur = R;
+            }
+        }
+        __syncthreads();
+        if (s_done) break;
+    }
+    __syncthreads();
+    for (int k = tid; k < n0; k += kSmallThreads) idx[gfirst + k] = s_pid[s_perm[k]];
+}
+
+// ---- 4. collapse to BVH4 ---------------------------------------------------
+
+__device__ __forceinline__ float node_area(const BNode& c) {
+    return area(c.lo[0], c.lo[1], c.lo[2], c.hi[0], c.hi[1], c.hi[2]);
+}
+
+__global__ void k_collapse_count(const int* __restrict__ level, int m, const BNode* __restrict__ nodes,
+                                 int4* __restrict__ kids, int* __restrict__ nkids, int* __restrict__ ninner) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m) return;
+    const int b = level[j];
+    int k[4] = {-1, -1, -1, -1};
+    int nk;
+    const BNode nb = nodes[b];
+    if (nb.left < 0) {
+        k[0] = b;   // a leaf root: one node with one leaf child
+        nk = 1;
+    } else {
+        k[0] = nb.left;
+        k[1] = nb.right;
+        nk = 2;
+        while (nk < 4) {
+            int pick = -1;
+            float best = -1.0f;
+            for (int q = 0; q < nk; q++) {
+                const BNode& c = nodes[k[q]];
+                if (c.left >= 0) {
+                    const float ar = node_area(c);
+                    if (ar > best) { best = ar; pick = q; }
+                }
+            }
+            if (pick < 0) break;
+            const int opened = k[pick];
+            k[pick] = nodes[opened].left;
+            k[nk++] = nodes[opened].right;
+        }
+    }
+    int inner = 0;
+    for (int q = 0; q < nk; q++) inner += nodes[k[q]].left >= 0 ? 1 : 0;
+    kids[j] = make_int4(k[0], k[1], k[2], k[3]);
+    nkids[j] = nk;
+    ninner[j] = inner;
+}
+
+__global__ void k_collapse_emit(const int* __restrict__ level, int m, int base, const int4* __restrict__ kids,
+                                const int* __restrict__ nkids, const int* __restrict__ off,
+                                const BNode* __restrict__ nodes, dev::QNode4* __restrict__ out,
+                                int* __restrict__ next_level) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= m) return;
+    const int4 kv = kids[j];
+    const int k[4] = {kv.x, kv.y, kv.z, kv.w};
+    const int nk = nkids[j];
+    float nlo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, nhi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int q = 0; q < nk; q++) {
+        const BNode& c = nodes[k[q]];
+        for (int a = 0; a < 3; a++) { nlo[a] = fminf(nlo[a], c.lo[a]); nhi[a] = fmaxf(nhi[a], c.hi[a]); }
+    }
+    float scale[3];
+    uint32_t packed = (uint32_t)nk << 24;
+    for (int a = 0; a < 3; a++) {
+        const int e = frame_exponent(nlo[a], nhi[a]);
+        scale[a] = ldexpf(1.0f, e);
+        packed |= (uint32_t)(e + 127) << (8 * a);
+    }
+    uint8_t q6[6][4];
+    for (int r = 0; r < 6; r++)
+        for (int c = 0; c < 4; c++) q6[r][c] = 0;
+    uint32_t child[4] = {0, 0, 0, 0};
+    int r = 0;
+    for (int q = 0; q < nk; q++) {
+        const BNode& c = nodes[k[q]];
+        for (int a = 0; a < 3; a++) quantize_axis(nlo[a], scale[a], c.lo[a], c.hi[a], q6[2 * a][q], q6[2 * a + 1][q]);
+        if (c.left < 0) {
+            child[q] = 0x80000000u | ((uint32_t)c.first << 3) | (uint32_t)(c.count - 1);
+        } else {
+            child[q] = (uint32_t)(base + m + off[j] + r);
+            next_level[off[j] + r] = k[q];
+            r++;
+        }
+    }
+    auto word = [&](int row) {
+        return (uint32_t)q6[row][0] | ((uint32_t)q6[row][1] << 8) | ((uint32_t)q6[row][2] << 16) |
+               ((uint32_t)q6[row][3] << 24);
+    };
+    dev::QNode4 o;
+    o.origin_exp = make_float4(nlo[0], nlo[1], nlo[2], __uint_as_float(packed));
+    o.child = make_uint4(child[0], child[1], child[2], child[3]);
+    o.qbox = make_uint4(word(0), word(1), word(2), word(3));
+    o.qz = make_uint2(word(4), word(5));
+    o.pad = make_uint2(0, 0);
+    out[base + j] = o;
+}
+
+__global__ void k_emit_tris(const Triangle* __restrict__ tris, const int* __restrict__ subset,
+                            const int* __restrict__ idx, int n, float4* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int s = idx[i];
+    const int orig = subset ? subset[s] : s;
+    const Triangle& t = tris[orig];
+    out[3 * (size_t)i] = make_float4(t.v0.x, t.v0.y, t.v0.z, __int_as_float(orig));
+    out[3 * (size_t)i + 1] = make_float4(sub(t.v1.x, t.v0.x), sub(t.v1.y, t.v0.y), sub(t.v1.z, t.v0.z), 0.0f);
+    out[3 * (size_t)i + 2] = make_float4(sub(t.v2.x, t.v0.x), sub(t.v2.y, t.v0.y), sub(t.v2.z, t.v0.z), 0.0f);
+}
+
+// ---- subsets: triangles that can / cannot pass a shadow ray ----------------
+
+__global__ void k_pass_flags(const Triangle* __restrict__ tris, int n, const Material* __restrict__ mats, int nm,
+                             int* __restrict__ iota, unsigned char* __restrict__ pass, unsigned char* __restrict__ block) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int m = tris[i].material_id;
+    const bool p = m >= 0 && m < nm && mats[m].transmission > 0.5f;
+    iota[i] = i;
+    pass[i] = p ? 1 : 0;
+    block[i] = p ? 0 : 1;
+}
+
+// Carves 256-byte aligned arrays from one block.
+struct Carver {
+    char* p;
+    size_t used = 0;
+    template <class T>
+    T* take(size_t count) {
+        T* r = reinterpret_cast<T*>(p + used);
+        used += (count * sizeof(T) + 255) & ~(size_t)255;
+        return r;
+    }
+};
+
+}  // namespace bvhg
+
+// Device-built BVH4 over triangles tris[subset[i]] (subset null: all n).
+// Allocates out.nodes (exact size) and out.tris (3 float4 per triangle);
+// everything else is temporary.  Synchronises `stream` once per tree level.
+cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, DevQBvh& out, cudaStream_t stream) {
+    using namespace bvhg;
+    out = DevQBvh{};
+    if (n <= 0) return cudaSuccess;
+    if (n > (1 << 27)) return cudaErrorInvalidValue;   // leaf words hold first < 2^28
+    const size_t N = (size_t)n;
+    const int max_work = n / kSmall + 2;
+    const int max_chunks = n / kChunk + max_work + 2;
+    size_t cub_a = 0, cub_b = 0;
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, cub_a, (int*)nullptr, (int*)nullptr, max_chunks);
+    if (e != cudaSuccess) return e;
+    e = cub::DeviceScan::ExclusiveSum(nullptr, cub_b, (int*)nullptr, (int*)nullptr, n);
+    if (e != cudaSuccess) return e;
+    const size_t cub_bytes = std::max(cub_a, cub_b);
+
+    // Temporary block: sized by a dry carve.
+    struct Ptrs {
+        float4 *plo, *phi;
+        int *idx, *tmp;
+        BNode* nodes;
+        dev::QNode4* qtmp;
+        int4* kids;
+        int *nk, *ninner, *off, *lvl_a, *lvl_b;
+        int *gbins, *work, *chunk_base, *chunk_left, *chunk_off, *child_ord, *root_ord, *err;
+        int4* split;
+        int2* child_fc;
+        void* cub;
+    } P;
+    auto carve = [&](Carver& c) {
+        P.plo = c.take<float4>(N);
+        P.phi = c.take<float4>(N);
+        P.idx = c.take<int>(N);
+        P.tmp = c.take<int>(N);
+        P.nodes = c.take<BNode>(2 * N);
+        P.qtmp = c.take<dev::QNode4>(N);
+        P.kids = c.take<int4>(N);
+        P.nk = c.take<int>(N);
+        P.ninner = c.take<int>(N);
+        P.off = c.take<int>(N);
+        P.lvl_a = c.take<int>(N);
+        P.lvl_b = c.take<int>(N);
+        P.gbins = c.take<int>((size_t)max_work * kNodeBins);
+        P.work = c.take<int>((size_t)max_work);
+        P.chunk_base = c.take<int>((size_t)max_work + 1);
+        P.chunk_left = c.take<int>((size_t)max_chunks);
+        P.chunk_off = c.take<int>((size_t)max_chunks);
+        P.child_ord = c.take<int>((size_t)2 * max_work * 12);
+        P.root_ord = c.take<int>(12);
+        P.err = c.take<int>(1);
+        P.split = c.take<int4>((size_t)max_work);
+        P.child_fc = c.take<int2>((size_t)2 * max_work);
+        P.cub = c.take<char>(cub_bytes);
+    };
+    Carver dry{nullptr};
+    carve(dry);
+    void* block = nullptr;
+    if ((e = cudaMalloc(&block, dry.used)) != cudaSuccess) return e;
+    Carver real{static_cast<char*>(block)};
+    carve(real);
+    int* small_buf = nullptr;
+    dev::QNode4* nodes_out = nullptr;
+    float4* tris_out = nullptr;
+    int num_q = 0, depth = 0;
+#define CK(x) do { if ((e = (x)) != cudaSuccess) goto done; } while (0)
+    {
+        // 1. boxes and root
+        CK(cudaMemsetAsync(P.err, 0, sizeof(int), stream));
+        k_init_ord<<<1, 32, 0, stream>>>(P.root_ord, 12);
+        const int prep_blocks = (int)std::min<size_t>((N + 255) / 256, 148 * 8);
+        k_prep<<<prep_blocks, 256, 0, stream>>>(tris, subset, n, P.plo, P.phi, P.idx, P.root_ord);
+        k_root<<<1, 32, 0, stream>>>(P.root_ord, n, P.nodes);
+        CK(cudaGetLastError());
+
+        // 2. large nodes, one level per pass
+        std::vector<int> work, work_count, small_ids, small_count;
+        if (n > kSmall) { work.push_back(0); work_count.push_back(n); }
+        else { small_ids.push_back(0); small_count.push_back(n); }
+        int next_id = 1;
+        std::vector<int> chunk_base;
+        std::vector<int4> split_h;
+        std::vector<int2> fc_h;
+        int levels = 0;
+        while (!work.empty()) {
+            if (++levels > kMaxLargeLevels) { e = cudaErrorInvalidValue; goto done; }
+            const int m = (int)work.size();
+            chunk_base.assign((size_t)m + 1, 0);
+            for (int j = 0; j < m; j++) chunk_base[(size_t)j + 1] = chunk_base[(size_t)j] + (work_count[(size_t)j] + kChunk - 1) / kChunk;
+            const int chunks = chunk_base[(size_t)m];
+            CK(cudaMemcpyAsync(P.work, work.data(), (size_t)m * sizeof(int), cudaMemcpyHostToDevice, stream));
+            CK(cudaMemcpyAsync(P.chunk_base, chunk_base.data(), ((size_t)m + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
+            const int words = m * kNodeBins;
+            k_init_bins<<<(words + 255) / 256, 256, 0, stream>>>(P.gbins, words);
+            k_bin_large<<<chunks, kChunkThreads, 0, stream>>>(P.work, P.chunk_base, m, P.nodes, P.plo, P.phi, P.idx, P.gbins);
+            k_split_large<<<m, 32, 0, stream>>>(P.work, m, next_id, P.nodes, P.gbins, P.split, P.child_fc);
+            k_init_ord<<<(2 * m * 12 + 255) / 256, 256, 0, stream>>>(P.child_ord, 2 * m * 12);
+            k_list_split_bounds<<<chunks, kChunkThreads, 0, stream>>>(P.work, P.chunk_base, m, P.nodes, P.split, P.plo,
+                                                                      P.phi, P.idx, P.child_ord);
+            k_list_split_write<<<(2 * m + 127) / 128, 128, 0, stream>>>(m, next_id, P.split, P.child_ord, P.nodes);
+            k_part_count<<<chunks, kChunkThreads, 0, stream>>>(P.work, P.chunk_base, m, P.nodes, P.split, P.plo, P.phi,
+                                                              P.idx, P.chunk_left);
+            size_t cb = cub_bytes;
+            CK(cub::DeviceScan::ExclusiveSum(P.cub, cb, P.chunk_left, P.chunk_off, chunks, stream));
+            k_part_scatter<<<chunks, kChunkThreads, 0, stream>>>(P.work, P.chunk_base, m, P.nodes, P.split, P.plo,
+                                                                P.phi, P.idx, P.chunk_off, P.tmp, P.err);
+            k_copy_back<<<chunks, kChunkThreads, 0, stream>>>(P.work, P.chunk_base, m, P.nodes, P.tmp, P.idx);
+            CK(cudaGetLastError());
+            fc_h.resize((size_t)2 * m);
+            CK(cudaMemcpyAsync(fc_h.data(), P.child_fc, (size_t)2 * m * sizeof(int2), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            std::vector<int> nwork, ncount;
+            for (int i = 0; i < 2 * m; i++) {
+                const int id = next_id + i, cnt = fc_h[(size_t)i].y;
+                if (cnt > kSmall) { nwork.push_back(id); ncount.push_back(cnt); }
+                else { small_ids.push_back(id); small_count.push_back(cnt); }
+            }
+            next_id += 2 * m;
+            work.swap(nwork);
+            work_count.swap(ncount);
+        }
+
+        // 3. small subtrees
+        const int ns = (int)small_ids.size();
+        std::vector<int> small_h((size_t)2 * ns);
+        int id = next_id;
+        for (int b = 0; b < ns; b++) {
+            small_h[(size_t)b] = small_ids[(size_t)b];
+            small_h[(size_t)ns + b] = id;
+            id += std::max(0, 2 * small_count[(size_t)b] - 2);
+        }
+        if ((size_t)id > 2 * N) { e = cudaErrorInvalidValue; goto done; }
+        CK(cudaMalloc(&small_buf, (size_t)2 * ns * sizeof(int)));
+        CK(cudaMemcpyAsync(small_buf, small_h.data(), (size_t)2 * ns * sizeof(int), cudaMemcpyHostToDevice, stream));
+        k_small<<<ns, kSmallThreads, 0, stream>>>(small_buf, small_buf + ns, P.plo, P.phi, P.idx, P.nodes, P.err);
+        CK(cudaGetLastError());
+
+        // 4. collapse, breadth first
+        CK(cudaMemsetAsync(P.lvl_a, 0, sizeof(int), stream));   // level 0: the root, binary node 0
+        int m = 1, base = 0;
+        int* cur = P.lvl_a;
+        int* nxt = P.lvl_b;
+        while (m > 0) {
+            depth++;
+            k_collapse_count<<<(m + 127) / 128, 128, 0, stream>>>(cur, m, P.nodes, P.kids, P.nk, P.ninner);
+            size_t cb = cub_bytes;
+            CK(cub::DeviceScan::ExclusiveSum(P.cub, cb, P.ninner, P.off, m, stream));
+            k_collapse_emit<<<(m + 127) / 128, 128, 0, stream>>>(cur, m, base, P.kids, P.nk, P.off, P.nodes, P.qtmp, nxt);
+            CK(cudaGetLastError());
+            int last[2] = {0, 0};
+            CK(cudaMemcpyAsync(&last[0], P.off + (m - 1), sizeof(int), cudaMemcpyDeviceToHost, stream));
+            CK(cudaMemcpyAsync(&last[1], P.ninner + (m - 1), sizeof(int), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            base += m;
+            m = last[0] + last[1];
+            std::swap(cur, nxt);
+            if (base + m > n) { e = cudaErrorInvalidValue; goto done; }
+        }
+        num_q = base;
+        int err_h = 0;
+        CK(cudaMemcpyAsync(&err_h, P.err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        if (err_h) { e = cudaErrorInvalidValue; goto done; }
+
+        // outputs
+        CK(cudaMalloc(&nodes_out, (size_t)num_q * sizeof(dev::QNode4)));
+        CK(cudaMalloc(&tris_out, 3 * N * sizeof(float4)));
+        CK(cudaMemcpyAsync(nodes_out, P.qtmp, (size_t)num_q * sizeof(dev::QNode4), cudaMemcpyDeviceToDevice, stream));
+        k_emit_tris<<<(n + 255) / 256, 256, 0, stream>>>(tris, subset, P.idx, n, tris_out);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(stream));
+    }
+done:
+#undef CK
+    cudaFree(small_buf);
+    cudaFree(block);
+    if (e != cudaSuccess) {
+        cudaFree(nodes_out);
+        cudaFree(tris_out);
+        return e;
+    }
+    out.nodes = nodes_out;
+    out.tris = tris_out;
+    out.num_nodes = num_q;
+    out.num_tris = n;
+    out.max_depth = depth;
+    return cudaSuccess;
+}
+
+// The wavefront form's three triangle BVH4s of a resident scene (triangles
+// and materials already in the arena), built on the device.  The subsets
+// are the host's: passable = material transmission > 0.5 (in range), in
+// index order.  Allocations go to s.extra.
+cudaError_t build_wave_meshes_device(DeviceScene& s, cudaStream_t stream) {
+    dev::DevScene& v = s.view;
+    const int n = v.num_tris;
+    if (n <= 0) return cudaSuccess;
+    cudaError_t e;
+    DevQBvh all, blk, pas;
+    if ((e = build_qbvh4_device(v.tris, nullptr, n, all, stream)) != cudaSuccess) return e;
+    auto keep = [&](const DevQBvh& q) {
+        s.extra.push_back(q.nodes);
+        s.extra.push_back(q.tris);
+        s.extra_bytes += (size_t)q.num_nodes * sizeof(dev::QNode4) + (size_t)q.num_tris * 3 * sizeof(float4);
+    };
+    keep(all);
+    int* iota = nullptr;
+    int* sel = nullptr;
+    unsigned char* flags = nullptr;
+    void* cub_tmp = nullptr;
+    int* num_sel = nullptr;
+    int npass = 0, nblock = 0;
+    size_t cb = 0;
+#define CK(x) do { if ((e = (x)) != cudaSuccess) goto done; } while (0)
+    CK(cudaMalloc(&iota, (size_t)n * sizeof(int)));
+    CK(cudaMalloc(&sel, (size_t)2 * n * sizeof(int)));
+    CK(cudaMalloc(&flags, (size_t)2 * n));
+    CK(cudaMalloc(&num_sel, 2 * sizeof(int)));
+    bvhg::k_pass_flags<<<(n + 255) / 256, 256, 0, stream>>>(v.tris, n, v.materials, v.num_materials, iota, flags,
+                                                             flags + n);
+    CK(cudaGetLastError());
+    CK(cub::DeviceSelect::Flagged(nullptr, cb, iota, flags, sel, num_sel, n, stream));
+    CK(cudaMalloc(&cub_tmp, cb));
+    CK(cub::DeviceSelect::Flagged(cub_tmp, cb, iota, flags, sel + n, num_sel, n, stream));          // passable
+    CK(cub::DeviceSelect::Flagged(cub_tmp, cb, iota, flags + n, sel, num_sel + 1, n, stream));      // blocking
+    {
+        int h[2] = {0, 0};
+        CK(cudaMemcpyAsync(h, num_sel, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        npass = h[0];
+        nblock = h[1];
+    }
+    if (npass > 0) {
+        if (nblock > 0) {
+            CK(build_qbvh4_device(v.tris, sel, nblock, blk, stream));
+            keep(blk);
+        }
+        CK(build_qbvh4_device(v.tris, sel + n, npass, pas, stream));
+        keep(pas);
+    }
+done:
+#undef CK
+    cudaFree(iota);
+    cudaFree(sel);
+    cudaFree(flags);
+    cudaFree(cub_tmp);
+    cudaFree(num_sel);
+    if (e != cudaSuccess) return e;
+    auto qmesh = [](const DevQBvh& q) {
+        dev::QMesh m;
+        m.nodes = q.nodes;
+        m.tris = q.tris;
+        m.num_nodes = q.num_nodes;
+        m.num_tris = q.num_tris;
+        return m;
+    };
+    v.q_all = qmesh(all);
+    v.q_block = qmesh(blk);
+    v.q_pass = qmesh(pas);
+    s.wave_depth = std::max(all.max_depth, std::max(blk.max_depth, pas.max_depth));
+    return cudaSuccess;
+}
+
+}  // namespace sheen
+
+// Both builders on one scene, compared byte for byte (a parity check of the
+// device builder; no rendering).  Returns 0 when the three BVH4s (all /
+// blocking / passable triangles) are identical, 1 + 10*set for a differing
+// node count, 2 + 10*set for differing node bytes, 3 + 10*set for differing
+// triangle records, 4 + 10*set for a differing depth (set 0 all, 1
+// blocking, 2 passable), -1 on error.  times_ms (may be NULL) receives the
+// host and the device build times.
+extern "C" int sheen_bvh4_compare_builders(const SheenScene* scene, double* times_ms) {
+    using namespace sheen;
+    if (!scene || scene->num_triangles <= 0 || !scene->triangles) { set_error("scene has no triangles"); return -1; }
+    const int n = scene->num_triangles;
+    std::vector<int> all, block, pass;
+    for (int i = 0; i < n; i++) {
+        all.push_back(i);
+        const int m = scene->triangles[i].material_id;
+        const bool passable = m >= 0 && m < scene->num_materials && scene->materials[m].transmission > 0.5f;
+        (passable ? pass : block).push_back(i);
+    }
+    const double h0 = now_ms();
+    QBvh hq[3];
+    build_qbvh4(scene->triangles, all, hq[0]);
+    if (!pass.empty()) {
+        build_qbvh4(scene->triangles, block, hq[1]);
+        build_qbvh4(scene->triangles, pass, hq[2]);
+    }
+    const double host_ms = now_ms() - h0;
+
+    DeviceScene ds;
+    Triangle* dt = nullptr;
+    Material* dm = nullptr;
+    int rc = 0;
+    cudaError_t e = cudaMalloc(&dt, (size_t)n * sizeof(Triangle));
+    if (e == cudaSuccess) e = cudaMalloc(&dm, (size_t)std::max(scene->num_materials, 1) * sizeof(Material));
+    if (e == cudaSuccess) e = cudaMemcpy(dt, scene->triangles, (size_t)n * sizeof(Triangle), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && scene->num_materials > 0)
+        e = cudaMemcpy(dm, scene->materials, (size_t)scene->num_materials * sizeof(Material), cudaMemcpyHostToDevice);
+    double dev_ms = 0.0;
+    if (e == cudaSuccess) {
+        ds.form = SHEEN_FORM_WAVEFRONT;
+        ds.view.tris = dt;
+        ds.view.num_tris = n;
+        ds.view.materials = dm;
+        ds.view.num_materials = scene->num_materials;
+        e = cudaDeviceSynchronize();
+        const double d0 = now_ms();
+        if (e == cudaSuccess) e = build_wave_meshes_device(ds, 0);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        dev_ms = now_ms() - d0;
+    }
+    const dev::QMesh dq[3] = {ds.view.q_all, ds.view.q_block, ds.view.q_pass};
+    for (int k = 0; k < 3 && e == cudaSuccess && rc == 0; k++) {
+        const QBvh& h = hq[k];
+        if ((size_t)dq[k].num_nodes != h.nodes.size() || (size_t)dq[k].num_tris * 3 != h.tris.size()) {
+            rc = 1 + 10 * k;
+            break;
+        }
+        if (h.nodes.empty()) continue;
+        std::vector<dev::QNode4> nodes(h.nodes.size());
+        std::vector<float4> tris(h.tris.size());
+        e = cudaMemcpy(nodes.data(), dq[k].nodes, nodes.size() * sizeof(dev::QNode4), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(tris.data(), dq[k].tris, tris.size() * sizeof(float4), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) break;
+        if (std::memcmp(nodes.data(), h.nodes.data(), nodes.size() * sizeof(dev::QNode4)) != 0) rc = 2 + 10 * k;
+        else if (std::memcmp(tris.data(), h.tris.data(), tris.size() * sizeof(float4)) != 0) rc = 3 + 10 * k;
+    }
+    if (e == cudaSuccess && rc == 0) {
+        const int hd = std::max(hq[0].max_depth, std::max(hq[1].max_depth, hq[2].max_depth));
+        if (hd != ds.wave_depth) rc = 4;
+    }
+    for (void* p : ds.extra) cudaFree(p);
+    cudaFree(dt);
+    cudaFree(dm);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return -1; }
+    if (times_ms) { times_ms[0] = host_ms; times_ms[1] = dev_ms; }
+    return rc;
+}

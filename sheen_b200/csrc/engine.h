@@ -43,6 +43,18 @@ struct QBvh {
 // stored triangle records keep those original indices).
 void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out);
 
+// The same BVH4 built on the device (bvh4_gpu.cu), byte-identical to
+// build_qbvh4's.  nodes/tris are device allocations owned by the caller.
+struct DevQBvh {
+    dev::QNode4* nodes = nullptr;
+    float4* tris = nullptr;
+    int num_nodes = 0;
+    int num_tris = 0;
+    int max_depth = 0;
+};
+cudaError_t build_qbvh4_device(const Triangle* tris_dev, const int* subset_dev, int n, DevQBvh& out,
+                               cudaStream_t stream);
+
 // Result/accounting of one render call.
 struct RenderTally {
     unsigned long long primary = 0, shadow = 0, secondary = 0, nodes = 0, prims = 0;
@@ -65,7 +77,13 @@ struct DeviceScene {
     // Scene features outside the queue pipeline (visible spot beams, the
     // shadow-debug material mode): such frames run on the BVH4 megakernel.
     bool wave_fallback = false;
+    int wave_depth = 0;                    // levels of the deepest triangle BVH4
 };
+
+// The wavefront form's three triangle BVH4s (all / blocking / passable) of
+// a scene whose triangles and materials are already resident, built on the
+// device; allocations are added to s.extra.
+cudaError_t build_wave_meshes_device(DeviceScene& s, cudaStream_t stream);
 
 int scene_upload(const SheenScene* in, int form, DeviceScene** out);
 void scene_release(DeviceScene* s);
@@ -116,6 +134,7 @@ struct Tuning {
     int shadow_kernel = 1;          // 0: 32-ray batches per warp; 1: per-lane refill
     int refill_min = 8;             // idle lanes that trigger a refill (shadow_kernel 1)
     int shadow_blocks_per_sm = 0;   // 128-thread blocks per SM for the shadow stage; 0: occupancy limit
+    int build_device = 1;           // wavefront triangle BVH4s: 1 built on the device, 0 on the host
 };
 Tuning tuning();
 int tuning_generation();

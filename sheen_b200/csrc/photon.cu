@@ -16,11 +16,15 @@
 #include <cub/cub.cuh>
 
 #include "dev/integrator.cuh"
+#include "dev/trace_bvh4.cuh"
 #include "engine.h"
 
 namespace sheen {
 namespace dev {
 
+// T: the scene's query policy (the plain form's reference-order walks, or
+// the wavefront form's BVH4s: same closest hits except exact ties).
+template <class T>
 __global__ void photon_emit_kernel(DevScene S, int per_light, int total, float4* pos, float4* nrm, float4* flux,
                                    int* valid) {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -60,7 +64,7 @@ __global__ void photon_emit_kernel(DevScene S, int per_light, int total, float4*
     Counters c;
     for (int b = 0; b < 4; b++) {
         Hit h;
-        if (!closest_ref<false>(S, ray, h, c)) return;
+        if (!T::closest(S, ray, h, c)) return;
         const Material& m = S.materials[h.mat];
         if (m.transmission > 0.5f) {
             const float3 n = h.n;
@@ -138,7 +142,12 @@ int build_photon_map_device(DeviceScene& s, int per_light, float cell) {
     CK(cudaMalloc(&flux, (size_t)total * sizeof(float4)));
     CK(cudaMalloc(&valid, (size_t)total * sizeof(int)));
     CK(cudaMalloc(&rank, (size_t)total * sizeof(int)));
-    dev::photon_emit_kernel<<<(total + 127) / 128, 128>>>(s.view, per_light, total, pos, nrm, flux, valid);
+    if (s.form == SHEEN_FORM_PLAIN)
+        dev::photon_emit_kernel<dev::RefTracer<false>><<<(total + 127) / 128, 128>>>(s.view, per_light, total, pos, nrm,
+                                                                                   flux, valid);
+    else
+        dev::photon_emit_kernel<dev::FastTracer<false>><<<(total + 127) / 128, 128>>>(s.view, per_light, total, pos,
+                                                                                    nrm, flux, valid);
     CK(cudaGetLastError());
     {
         size_t b1 = 0, b2 = 0;

@@ -28,6 +28,7 @@ const Key kKeys[] = {
     {"wave.shadow_kernel", &Tuning::shadow_kernel, 0, 1},
     {"wave.refill_min", &Tuning::refill_min, 1, 32},
     {"wave.shadow_blocks_per_sm", &Tuning::shadow_blocks_per_sm, 0, 16},
+    {"build.device", &Tuning::build_device, 0, 1},
 };
 
 }  // namespace

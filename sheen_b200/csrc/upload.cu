@@ -118,11 +118,18 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     }
     build_median_bvh(lo, hi, prims, true, strand_bvh);
 
+    // Triangles: the plain form walks a median BVH over 48-byte position
+    // records; the wavefront form walks only its BVH4s (built below, on the
+    // device by default) and needs neither.
     lo.clear(); hi.clear(); prims.clear();
-    std::vector<float4> tri_verts((size_t)in->num_triangles * 3);
-    lo.reserve((size_t)in->num_triangles * 3);
-    hi.reserve((size_t)in->num_triangles * 3);
-    for (int i = 0; i < in->num_triangles; i++) {   // bvh.h:235-242
+    const bool plain_mesh = form == SHEEN_FORM_PLAIN;
+    const bool device_build = form == SHEEN_FORM_WAVEFRONT && tuning().build_device != 0;
+    std::vector<float4> tri_verts(plain_mesh ? (size_t)in->num_triangles * 3 : 0);
+    if (plain_mesh) {
+        lo.reserve((size_t)in->num_triangles * 3);
+        hi.reserve((size_t)in->num_triangles * 3);
+    }
+    for (int i = 0; plain_mesh && i < in->num_triangles; i++) {   // bvh.h:235-242
         const Triangle& t = in->triangles[i];
         float a[3] = {fminf(t.v0.x, fminf(t.v1.x, t.v2.x)), fminf(t.v0.y, fminf(t.v1.y, t.v2.y)),
                       fminf(t.v0.z, fminf(t.v1.z, t.v2.z))};
@@ -134,7 +141,7 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
         tri_verts[3 * (size_t)i + 1] = make_float4(t.v1.x, t.v1.y, t.v1.z, 0.0f);
         tri_verts[3 * (size_t)i + 2] = make_float4(t.v2.x, t.v2.y, t.v2.z, 0.0f);
     }
-    build_median_bvh(lo, hi, prims, false, mesh_bvh);
+    if (plain_mesh) build_median_bvh(lo, hi, prims, false, mesh_bvh);
 
     lo.clear(); hi.clear(); prims.clear();
     for (int i = 0; i < in->num_heightfields; i++) {   // bvh.h:304-309
@@ -194,7 +201,7 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     // pass a shadow ray (transmission > 0.5, render_kernel.cu:261-262) -- one
     // over the blocking triangles and one over the passable ones.
     QBvh q_all, q_block, q_pass;
-    if (form == SHEEN_FORM_WAVEFRONT && in->num_triangles > 0) {
+    if (form == SHEEN_FORM_WAVEFRONT && !device_build && in->num_triangles > 0) {
         std::vector<int> all, block, pass;
         for (int i = 0; i < in->num_triangles; i++) {
             all.push_back(i);
@@ -319,7 +326,8 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     v.objects = (const Object*)dptr(o_obj); v.num_objects = in->num_objects; v.sphere_bvh = (const dev::BvhNode*)dptr(o_sphb);
     v.strands = (const SweepStrand*)dptr(o_str); v.sweep_points = (const SweepPoint*)dptr(o_spt);
     v.num_strands = in->num_sweep_strands; v.strand_bvh = (const dev::BvhNode*)dptr(o_strb);
-    v.tris = (const Triangle*)dptr(o_tri); v.tri_verts = (const float4*)dptr(o_trv); v.num_tris = in->num_triangles;
+    v.tris = (const Triangle*)dptr(o_tri); v.tri_verts = (const float4*)dptr(o_trv);
+    v.num_tris = std::max(in->num_triangles, 0);
     v.mesh_bvh = (const dev::BvhNode*)dptr(o_meshb);
     v.hfs = (const HeightField*)dptr(o_hf); v.num_hfs = in->num_heightfields; v.hf_bvh = (const dev::BvhNode*)dptr(o_hfb);
     v.ses = (const Superellipsoid*)dptr(o_se); v.num_ses = in->num_superellipsoids; v.se_bvh = (const dev::BvhNode*)dptr(o_seb);
@@ -349,8 +357,26 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     v.q_pass = qmesh(q_pass, o_qpn, o_qpt);
     v.has_glass = has_glass ? 1 : 0;
     s->d_tally = (unsigned long long*)dptr(o_tally);
+    s->wave_depth = std::max(q_all.max_depth, std::max(q_block.max_depth, q_pass.max_depth));
     s->build_ms = t1 - t0;
     s->upload_ms = t2 - t1;
+    if (device_build && v.num_tris > 0) {
+        const double tb = now_ms();
+        e = build_wave_meshes_device(*s, 0);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+        if (e != cudaSuccess) {
+            set_error(cudaGetErrorString(e));
+            scene_release(s);
+            return -1;
+        }
+        // The traversal stack keeps at most 3 entries per level below the root.
+        if (3 * s->wave_depth + 1 > 48) {
+            set_error("triangle BVH too deep for the traversal stack");
+            scene_release(s);
+            return -1;
+        }
+        s->build_ms += now_ms() - tb;
+    }
 
     if (in->photons > 0 && in->num_lights > 0) {
         const double tp = now_ms();
