@@ -112,6 +112,8 @@ void sheen_cleanup(void) {
         g_scenes.clear();
     }
     cudaDeviceSynchronize();
+    sheen::release_upload_rings();
+    sheen::release_pools();
     cudaDeviceReset();
 }
 
@@ -175,14 +177,14 @@ int sheen_scene_render_host(SheenDeviceScene h, int W, int H, int aa, float* out
     if (!s) { sheen::set_error("null scene handle"); return -1; }
     if (W <= 0 || H <= 0 || aa < 1 || aa > 64 || !out_host) { sheen::set_error("bad render params"); return -1; }
     float4* d = nullptr;
-    cudaError_t e = cudaMalloc(&d, (size_t)W * H * sizeof(float4));
+    cudaError_t e = sheen::dmalloc(&d, (size_t)W * H * sizeof(float4));
     if (e != cudaSuccess) return fail_cuda(e);
     int rc = render_device(*s, W, H, aa, sheen::Region{0, 0, W, H}, d, 0, flags, stats);
     if (rc == 0) {
         e = cudaMemcpy(out_host, d, (size_t)W * H * sizeof(float4), cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) rc = fail_cuda(e);
     }
-    cudaFree(d);
+    sheen::dfree(d);
     return rc;
 }
 
@@ -194,18 +196,18 @@ int sheen_scene_primary_hits(SheenDeviceScene h, int W, int H, int aa, int* obj,
     const size_t n = (size_t)W * H * ns;
     int *dobj = nullptr, *dmat = nullptr;
     float* dt = nullptr;
-    cudaError_t e = cudaMalloc(&dobj, n * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&dmat, n * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&dt, n * sizeof(float));
+    cudaError_t e = sheen::dmalloc(&dobj, n * sizeof(int));
+    if (e == cudaSuccess) e = sheen::dmalloc(&dmat, n * sizeof(int));
+    if (e == cudaSuccess) e = sheen::dmalloc(&dt, n * sizeof(float));
     if (e == cudaSuccess)
         e = s->form == SHEEN_FORM_PLAIN ? sheen::launch_primary_hits_plain(*s, W, H, ns, dobj, dmat, dt, 0)
                                         : sheen::launch_primary_hits_bvh4(*s, W, H, ns, dobj, dmat, dt, 0);
     if (e == cudaSuccess) e = cudaMemcpy(obj, dobj, n * sizeof(int), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(mat, dmat, n * sizeof(int), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(t, dt, n * sizeof(float), cudaMemcpyDeviceToHost);
-    cudaFree(dobj);
-    cudaFree(dmat);
-    cudaFree(dt);
+    sheen::dfree(dobj);
+    sheen::dfree(dmat);
+    sheen::dfree(dt);
     return e == cudaSuccess ? 0 : fail_cuda(e);
 }
 

@@ -24,6 +24,7 @@
 #include <cfloat>
 #include <climits>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "bvh4_rules.h"
@@ -42,7 +43,6 @@ constexpr int kChunkThreads = 256;
 constexpr int kChunkPer = kChunk / kChunkThreads;
 constexpr int kBinWords = 13;                     // count, box lo/hi, centroid lo/hi
 constexpr int kNodeBins = 3 * kBins * kBinWords;
-constexpr int kCandidates = 3 * (kBins - 1);
 constexpr int kMaxLargeLevels = 4096;
 
 __device__ __forceinline__ int ford(float f) {
@@ -97,39 +97,71 @@ __device__ __forceinline__ int bin_union(const int* A, int b0, int b1, float lo[
     return n;
 }
 
-// SAH cost of candidate `cand` (axis cand / 15, split after bin cand % 15);
-// false when the host loop skips it (flat axis, or an empty side).
-__device__ __forceinline__ bool eval_candidate(const int* bins, const float clo[3], const float chi[3], int cand,
-                                               float& cost) {
-    const int a = cand / (kBins - 1), s = cand % (kBins - 1);
-    const float ext = sub(chi[a], clo[a]);
-    if (!(ext > 0.0f)) return false;
-    const int* A = bins + a * kBins * kBinWords;
-    float llo[3], lhi[3], lclo[3], lchi[3], rlo[3], rhi[3], rclo[3], rchi[3];
-    const int lc = bin_union(A, 0, s, llo, lhi, lclo, lchi);
-    const int rc = bin_union(A, s + 1, kBins - 1, rlo, rhi, rclo, rchi);
-    if (lc == 0 || rc == 0) return false;
-    cost = split_cost(area(llo[0], llo[1], llo[2], lhi[0], lhi[1], lhi[2]), lc,
-                      area(rlo[0], rlo[1], rlo[2], rhi[0], rhi[1], rhi[2]), rc);
-    return true;
-}
-
-// Best candidate over one warp: lowest cost, ties to the lowest index (the
-// host's strict "<" in candidate order).  Every lane gets the result; the
-// index is INT_MAX when no candidate qualifies.
+// Best split over the bins of a node, computed by one warp: for each axis,
+// lanes 0..15 hold one bin each, shuffle scans give every lane the union of
+// the bins up to it (left side) and from it on (right side), lane s prices
+// the split after bin s.  The result is candidate axis * 15 + split with the
+// lowest cost, ties to the lowest index (the host's strict "<" in candidate
+// order), or INT_MAX when no split qualifies (flat axes or an empty side).
+// Every lane gets the result.  Min/max unions are exact and the counts are
+// integers, so the scan order does not change any value.
 __device__ __forceinline__ void warp_best(const int* bins, const float clo[3], const float chi[3], float& best_cost,
                                           int& best) {
+    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     best_cost = FLT_MAX;
     best = INT_MAX;
-    for (int cand = lane; cand < kCandidates; cand += 32) {
-        float cost;
-        if (eval_candidate(bins, clo, chi, cand, cost) && cost < best_cost) { best_cost = cost; best = cand; }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        const float oc = __shfl_xor_sync(0xffffffffu, best_cost, o);
-        const int ob = __shfl_xor_sync(0xffffffffu, best, o);
-        if (oc < best_cost || (oc == best_cost && ob < best)) { best_cost = oc; best = ob; }
+    for (int a = 0; a < 3; a++) {
+        const float ext = sub(chi[a], clo[a]);
+        if (!(ext > 0.0f)) continue;
+        const int* A = bins + a * kBins * kBinWords;
+        int lc = 0;
+        float l0[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, l1[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+        if (lane < kBins) {
+            const int* b = A + lane * kBinWords;
+            lc = b[0];
+            for (int q = 0; q < 3; q++) { l0[q] = funord(b[1 + q]); l1[q] = funord(b[4 + q]); }
+        }
+        int rc = lc;
+        float r0[3] = {l0[0], l0[1], l0[2]}, r1[3] = {l1[0], l1[1], l1[2]};
+        for (int o = 1; o < kBins; o <<= 1) {
+            const int cu = __shfl_up_sync(full, lc, o), cd = __shfl_down_sync(full, rc, o);
+            float u0[3], u1[3], d0[3], d1[3];
+            for (int q = 0; q < 3; q++) {
+                u0[q] = __shfl_up_sync(full, l0[q], o);
+                u1[q] = __shfl_up_sync(full, l1[q], o);
+                d0[q] = __shfl_down_sync(full, r0[q], o);
+                d1[q] = __shfl_down_sync(full, r1[q], o);
+            }
+            if (lane >= o) {
+                lc += cu;
+                for (int q = 0; q < 3; q++) { l0[q] = fminf(l0[q], u0[q]); l1[q] = fmaxf(l1[q], u1[q]); }
+            }
+            if (lane + o < kBins) {
+                rc += cd;
+                for (int q = 0; q < 3; q++) { r0[q] = fminf(r0[q], d0[q]); r1[q] = fmaxf(r1[q], d1[q]); }
+            }
+        }
+        // right side of the split after bin s = suffix starting at s + 1
+        const int nrc = __shfl_down_sync(full, rc, 1);
+        float n0[3], n1[3];
+        for (int q = 0; q < 3; q++) {
+            n0[q] = __shfl_down_sync(full, r0[q], 1);
+            n1[q] = __shfl_down_sync(full, r1[q], 1);
+        }
+        float cost = FLT_MAX;
+        int cand = INT_MAX;
+        if (lane < kBins - 1 && lc > 0 && nrc > 0) {
+            const float c = split_cost(area(l0[0], l0[1], l0[2], l1[0], l1[1], l1[2]), lc,
+                                       area(n0[0], n0[1], n0[2], n1[0], n1[1], n1[2]), nrc);
+            if (c < FLT_MAX) { cost = c; cand = a * (kBins - 1) + lane; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const float oc = __shfl_xor_sync(full, cost, o);
+            const int ob = __shfl_xor_sync(full, cand, o);
+            if (oc < cost || (oc == cost && ob < cand)) { cost = oc; cand = ob; }
+        }
+        if (cost < best_cost) { best_cost = cost; best = cand; }   // earlier axes win ties
     }
 }
 
@@ -843,7 +875,7 @@ cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, D
     Carver dry{nullptr};
     carve(dry);
     void* block = nullptr;
-    if ((e = cudaMalloc(&block, dry.used)) != cudaSuccess) return e;
+    if ((e = dmalloc_async(&block, dry.used, stream)) != cudaSuccess) return e;
     Carver real{static_cast<char*>(block)};
     carve(real);
     int* small_buf = nullptr;
@@ -917,7 +949,7 @@ cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, D
             id += std::max(0, 2 * small_count[(size_t)b] - 2);
         }
         if ((size_t)id > 2 * N) { e = cudaErrorInvalidValue; goto done; }
-        CK(cudaMalloc(&small_buf, (size_t)2 * ns * sizeof(int)));
+        CK(dmalloc_async(&small_buf, (size_t)2 * ns * sizeof(int), stream));
         CK(cudaMemcpyAsync(small_buf, small_h.data(), (size_t)2 * ns * sizeof(int), cudaMemcpyHostToDevice, stream));
         k_small<<<ns, kSmallThreads, 0, stream>>>(small_buf, small_buf + ns, P.plo, P.phi, P.idx, P.nodes, P.err);
         CK(cudaGetLastError());
@@ -950,8 +982,8 @@ cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, D
         if (err_h) { e = cudaErrorInvalidValue; goto done; }
 
         // outputs
-        CK(cudaMalloc(&nodes_out, (size_t)num_q * sizeof(dev::QNode4)));
-        CK(cudaMalloc(&tris_out, 3 * N * sizeof(float4)));
+        CK(dmalloc_async(&nodes_out, (size_t)num_q * sizeof(dev::QNode4), stream));
+        CK(dmalloc_async(&tris_out, 3 * N * sizeof(float4), stream));
         CK(cudaMemcpyAsync(nodes_out, P.qtmp, (size_t)num_q * sizeof(dev::QNode4), cudaMemcpyDeviceToDevice, stream));
         k_emit_tris<<<(n + 255) / 256, 256, 0, stream>>>(tris, subset, P.idx, n, tris_out);
         CK(cudaGetLastError());
@@ -959,11 +991,11 @@ cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, D
     }
 done:
 #undef CK
-    cudaFree(small_buf);
-    cudaFree(block);
+    dfree_async(small_buf, stream);
+    dfree_async(block, stream);
     if (e != cudaSuccess) {
-        cudaFree(nodes_out);
-        cudaFree(tris_out);
+        dfree_async(nodes_out, stream);
+        dfree_async(tris_out, stream);
         return e;
     }
     out.nodes = nodes_out;
@@ -977,20 +1009,15 @@ done:
 // The wavefront form's three triangle BVH4s of a resident scene (triangles
 // and materials already in the arena), built on the device.  The subsets
 // are the host's: passable = material transmission > 0.5 (in range), in
-// index order.  Allocations go to s.extra.
+// index order.  The tree over all triangles and the two subset trees are
+// built at the same time from two host threads on two streams.  Allocations
+// go to s.extra.
 cudaError_t build_wave_meshes_device(DeviceScene& s, cudaStream_t stream) {
     dev::DevScene& v = s.view;
     const int n = v.num_tris;
     if (n <= 0) return cudaSuccess;
-    cudaError_t e;
+    cudaError_t e = cudaSuccess;
     DevQBvh all, blk, pas;
-    if ((e = build_qbvh4_device(v.tris, nullptr, n, all, stream)) != cudaSuccess) return e;
-    auto keep = [&](const DevQBvh& q) {
-        s.extra.push_back(q.nodes);
-        s.extra.push_back(q.tris);
-        s.extra_bytes += (size_t)q.num_nodes * sizeof(dev::QNode4) + (size_t)q.num_tris * 3 * sizeof(float4);
-    };
-    keep(all);
     int* iota = nullptr;
     int* sel = nullptr;
     unsigned char* flags = nullptr;
@@ -998,16 +1025,19 @@ cudaError_t build_wave_meshes_device(DeviceScene& s, cudaStream_t stream) {
     int* num_sel = nullptr;
     int npass = 0, nblock = 0;
     size_t cb = 0;
+    cudaStream_t st2 = nullptr;
+    cudaError_t e_all = cudaSuccess, e_sub = cudaSuccess;
 #define CK(x) do { if ((e = (x)) != cudaSuccess) goto done; } while (0)
-    CK(cudaMalloc(&iota, (size_t)n * sizeof(int)));
-    CK(cudaMalloc(&sel, (size_t)2 * n * sizeof(int)));
-    CK(cudaMalloc(&flags, (size_t)2 * n));
-    CK(cudaMalloc(&num_sel, 2 * sizeof(int)));
+    CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+    CK(dmalloc_async(&iota, (size_t)n * sizeof(int), stream));
+    CK(dmalloc_async(&sel, (size_t)2 * n * sizeof(int), stream));
+    CK(dmalloc_async(&flags, (size_t)2 * n, stream));
+    CK(dmalloc_async(&num_sel, 2 * sizeof(int), stream));
     bvhg::k_pass_flags<<<(n + 255) / 256, 256, 0, stream>>>(v.tris, n, v.materials, v.num_materials, iota, flags,
                                                              flags + n);
     CK(cudaGetLastError());
     CK(cub::DeviceSelect::Flagged(nullptr, cb, iota, flags, sel, num_sel, n, stream));
-    CK(cudaMalloc(&cub_tmp, cb));
+    CK(dmalloc_async(&cub_tmp, cb, stream));
     CK(cub::DeviceSelect::Flagged(cub_tmp, cb, iota, flags, sel + n, num_sel, n, stream));          // passable
     CK(cub::DeviceSelect::Flagged(cub_tmp, cb, iota, flags + n, sel, num_sel + 1, n, stream));      // blocking
     {
@@ -1017,21 +1047,40 @@ cudaError_t build_wave_meshes_device(DeviceScene& s, cudaStream_t stream) {
         npass = h[0];
         nblock = h[1];
     }
-    if (npass > 0) {
-        if (nblock > 0) {
-            CK(build_qbvh4_device(v.tris, sel, nblock, blk, stream));
-            keep(blk);
+    {
+        int dev_id = 0;
+        CK(cudaGetDevice(&dev_id));
+        auto subset_trees = [&] {
+            cudaSetDevice(dev_id);
+            if (npass > 0 && nblock > 0) e_sub = build_qbvh4_device(v.tris, sel, nblock, blk, st2);
+            if (npass > 0 && e_sub == cudaSuccess) e_sub = build_qbvh4_device(v.tris, sel + n, npass, pas, st2);
+        };
+        if (tuning().build_concurrent) {
+            std::thread subsets(subset_trees);
+            e_all = build_qbvh4_device(v.tris, nullptr, n, all, stream);
+            subsets.join();
+        } else {
+            e_all = build_qbvh4_device(v.tris, nullptr, n, all, stream);
+            subset_trees();
         }
-        CK(build_qbvh4_device(v.tris, sel + n, npass, pas, stream));
-        keep(pas);
+        e = e_all != cudaSuccess ? e_all : e_sub;
     }
 done:
 #undef CK
-    cudaFree(iota);
-    cudaFree(sel);
-    cudaFree(flags);
-    cudaFree(cub_tmp);
-    cudaFree(num_sel);
+    dfree_async(iota, stream);
+    dfree_async(sel, stream);
+    dfree_async(flags, stream);
+    dfree_async(cub_tmp, stream);
+    dfree_async(num_sel, stream);
+    if (st2) cudaStreamDestroy(st2);
+    auto keep = [&](const DevQBvh& q) {
+        if (q.nodes) s.extra.push_back(q.nodes);
+        if (q.tris) s.extra.push_back(q.tris);
+        s.extra_bytes += (size_t)q.num_nodes * sizeof(dev::QNode4) + (size_t)q.num_tris * 3 * sizeof(float4);
+    };
+    keep(all);
+    keep(blk);
+    keep(pas);
     if (e != cudaSuccess) return e;
     auto qmesh = [](const DevQBvh& q) {
         dev::QMesh m;
@@ -1081,8 +1130,8 @@ extern "C" int sheen_bvh4_compare_builders(const SheenScene* scene, double* time
     Triangle* dt = nullptr;
     Material* dm = nullptr;
     int rc = 0;
-    cudaError_t e = cudaMalloc(&dt, (size_t)n * sizeof(Triangle));
-    if (e == cudaSuccess) e = cudaMalloc(&dm, (size_t)std::max(scene->num_materials, 1) * sizeof(Material));
+    cudaError_t e = dmalloc(&dt, (size_t)n * sizeof(Triangle));
+    if (e == cudaSuccess) e = dmalloc(&dm, (size_t)std::max(scene->num_materials, 1) * sizeof(Material));
     if (e == cudaSuccess) e = cudaMemcpy(dt, scene->triangles, (size_t)n * sizeof(Triangle), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && scene->num_materials > 0)
         e = cudaMemcpy(dm, scene->materials, (size_t)scene->num_materials * sizeof(Material), cudaMemcpyHostToDevice);
@@ -1120,9 +1169,9 @@ extern "C" int sheen_bvh4_compare_builders(const SheenScene* scene, double* time
         const int hd = std::max(hq[0].max_depth, std::max(hq[1].max_depth, hq[2].max_depth));
         if (hd != ds.wave_depth) rc = 4;
     }
-    for (void* p : ds.extra) cudaFree(p);
-    cudaFree(dt);
-    cudaFree(dm);
+    for (void* p : ds.extra) dfree(p);
+    dfree(dt);
+    dfree(dm);
     if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return -1; }
     if (times_ms) { times_ms[0] = host_ms; times_ms[1] = dev_ms; }
     return rc;

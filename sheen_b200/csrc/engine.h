@@ -86,6 +86,7 @@ struct DeviceScene {
 cudaError_t build_wave_meshes_device(DeviceScene& s, cudaStream_t stream);
 
 int scene_upload(const SheenScene* in, int form, DeviceScene** out);
+void release_upload_rings();
 void scene_release(DeviceScene* s);
 
 // Pixel rectangle [x0, x1) x [y0, y1) of a W x H image; the output buffer
@@ -135,6 +136,8 @@ struct Tuning {
     int refill_min = 8;             // idle lanes that trigger a refill (shadow_kernel 1)
     int shadow_blocks_per_sm = 0;   // 128-thread blocks per SM for the shadow stage; 0: occupancy limit
     int build_device = 1;           // wavefront triangle BVH4s: 1 built on the device, 0 on the host
+    int build_concurrent = 1;       // device build: the subset trees beside the full tree (2 host threads)
+    int pool_keep_mb = 16384;       // freed device memory the library's pool keeps for reuse
 };
 Tuning tuning();
 int tuning_generation();
@@ -146,5 +149,23 @@ int tuning_get(const char* name, int* value);
 int build_photon_map_device(DeviceScene& s, int per_light, float cell);
 
 double now_ms();
+
+// Device memory of the library (mem.cpp): a stream-ordered pool per device
+// that keeps freed blocks mapped for reuse.  dmalloc's block is usable on
+// every stream when it returns; dfree waits for the device (as cudaFree
+// does) before returning the block.  The _async forms are ordered on
+// `stream` only.
+cudaError_t dmalloc(void** ptr, size_t bytes);
+cudaError_t dmalloc_async(void** ptr, size_t bytes, cudaStream_t stream);
+void dfree(void* ptr);
+void dfree_async(void* ptr, cudaStream_t stream);
+void release_pools();
+void trim_pool();
+template <class T>
+cudaError_t dmalloc(T** ptr, size_t bytes) { return dmalloc(reinterpret_cast<void**>(ptr), bytes); }
+template <class T>
+cudaError_t dmalloc_async(T** ptr, size_t bytes, cudaStream_t stream) {
+    return dmalloc_async(reinterpret_cast<void**>(ptr), bytes, stream);
+}
 
 }  // namespace sheen

@@ -137,11 +137,11 @@ int build_photon_map_device(DeviceScene& s, int per_light, float cell) {
     size_t cub_bytes = 0;
     cudaError_t e = cudaSuccess;
 #define CK(x) do { e = (x); if (e != cudaSuccess) goto fail; } while (0)
-    CK(cudaMalloc(&pos, (size_t)total * sizeof(float4)));
-    CK(cudaMalloc(&nrm, (size_t)total * sizeof(float4)));
-    CK(cudaMalloc(&flux, (size_t)total * sizeof(float4)));
-    CK(cudaMalloc(&valid, (size_t)total * sizeof(int)));
-    CK(cudaMalloc(&rank, (size_t)total * sizeof(int)));
+    CK(dmalloc(&pos, (size_t)total * sizeof(float4)));
+    CK(dmalloc(&nrm, (size_t)total * sizeof(float4)));
+    CK(dmalloc(&flux, (size_t)total * sizeof(float4)));
+    CK(dmalloc(&valid, (size_t)total * sizeof(int)));
+    CK(dmalloc(&rank, (size_t)total * sizeof(int)));
     if (s.form == SHEEN_FORM_PLAIN)
         dev::photon_emit_kernel<dev::RefTracer<false>><<<(total + 127) / 128, 128>>>(s.view, per_light, total, pos, nrm,
                                                                                    flux, valid);
@@ -154,7 +154,7 @@ int build_photon_map_device(DeviceScene& s, int per_light, float cell) {
         CK(cub::DeviceScan::ExclusiveSum(nullptr, b1, valid, rank, total));
         CK(cub::DeviceRadixSort::SortPairs(nullptr, b2, keys, keys_sorted, src, order, cap, 0, 18));
         cub_bytes = b1 > b2 ? b1 : b2;
-        CK(cudaMalloc(&cub_tmp, cub_bytes));
+        CK(dmalloc(&cub_tmp, cub_bytes));
         CK(cub::DeviceScan::ExclusiveSum(cub_tmp, b1, valid, rank, total));
         int last_rank = 0, last_valid = 0;
         CK(cudaMemcpy(&last_rank, rank + total - 1, sizeof(int), cudaMemcpyDeviceToHost));
@@ -163,10 +163,10 @@ int build_photon_map_device(DeviceScene& s, int per_light, float cell) {
         if (n > cap) n = cap;
         s.photons_stored = n;
         if (n == 0) goto done;
-        CK(cudaMalloc(&keys, (size_t)n * sizeof(int)));
-        CK(cudaMalloc(&src, (size_t)n * sizeof(int)));
-        CK(cudaMalloc(&keys_sorted, (size_t)n * sizeof(int)));
-        CK(cudaMalloc(&order, (size_t)n * sizeof(int)));
+        CK(dmalloc(&keys, (size_t)n * sizeof(int)));
+        CK(dmalloc(&src, (size_t)n * sizeof(int)));
+        CK(dmalloc(&keys_sorted, (size_t)n * sizeof(int)));
+        CK(dmalloc(&order, (size_t)n * sizeof(int)));
         dev::photon_compact_kernel<<<(total + 127) / 128, 128>>>(total, valid, rank, n, cell, num_cells, pos, keys, src);
         CK(cudaGetLastError());
         size_t b3 = cub_bytes;
@@ -175,15 +175,15 @@ int build_photon_map_device(DeviceScene& s, int per_light, float cell) {
         // Resident map: sorted photons + cell_count + cell_start.
         float4 *mpos = nullptr, *mnrm = nullptr, *mflux = nullptr;
         int *cstart = nullptr, *ccount = nullptr;
-        CK(cudaMalloc(&mpos, (size_t)n * sizeof(float4)));
+        CK(dmalloc(&mpos, (size_t)n * sizeof(float4)));
         s.extra.push_back(mpos);
-        CK(cudaMalloc(&mnrm, (size_t)n * sizeof(float4)));
+        CK(dmalloc(&mnrm, (size_t)n * sizeof(float4)));
         s.extra.push_back(mnrm);
-        CK(cudaMalloc(&mflux, (size_t)n * sizeof(float4)));
+        CK(dmalloc(&mflux, (size_t)n * sizeof(float4)));
         s.extra.push_back(mflux);
-        CK(cudaMalloc(&ccount, (size_t)num_cells * sizeof(int)));
+        CK(dmalloc(&ccount, (size_t)num_cells * sizeof(int)));
         s.extra.push_back(ccount);
-        CK(cudaMalloc(&cstart, (size_t)(num_cells + 1) * sizeof(int)));
+        CK(dmalloc(&cstart, (size_t)(num_cells + 1) * sizeof(int)));
         s.extra.push_back(cstart);
         s.extra_bytes = (size_t)n * 3 * sizeof(float4) + (size_t)(2 * num_cells + 1) * sizeof(int);
         CK(cudaMemset(ccount, 0, (size_t)num_cells * sizeof(int)));
@@ -192,9 +192,9 @@ int build_photon_map_device(DeviceScene& s, int per_light, float cell) {
         size_t b4 = 0;
         CK(cub::DeviceScan::ExclusiveSum(nullptr, b4, ccount, cstart, num_cells));
         if (b4 > cub_bytes) {
-            cudaFree(cub_tmp);
+            dfree(cub_tmp);
             cub_tmp = nullptr;
-            CK(cudaMalloc(&cub_tmp, b4));
+            CK(dmalloc(&cub_tmp, b4));
             cub_bytes = b4;
         }
         CK(cub::DeviceScan::ExclusiveSum(cub_tmp, b4, ccount, cstart, num_cells));
@@ -211,13 +211,13 @@ int build_photon_map_device(DeviceScene& s, int per_light, float cell) {
         s.view.pmap.cell_size = cell;
     }
 done:
-    cudaFree(pos); cudaFree(nrm); cudaFree(flux); cudaFree(valid); cudaFree(rank);
-    cudaFree(keys); cudaFree(src); cudaFree(keys_sorted); cudaFree(order); cudaFree(cub_tmp); cudaFree(counter);
+    dfree(pos); dfree(nrm); dfree(flux); dfree(valid); dfree(rank);
+    dfree(keys); dfree(src); dfree(keys_sorted); dfree(order); dfree(cub_tmp); dfree(counter);
     return 0;
 fail:
     set_error(cudaGetErrorString(e));
-    cudaFree(pos); cudaFree(nrm); cudaFree(flux); cudaFree(valid); cudaFree(rank);
-    cudaFree(keys); cudaFree(src); cudaFree(keys_sorted); cudaFree(order); cudaFree(cub_tmp); cudaFree(counter);
+    dfree(pos); dfree(nrm); dfree(flux); dfree(valid); dfree(rank);
+    dfree(keys); dfree(src); dfree(keys_sorted); dfree(order); dfree(cub_tmp); dfree(counter);
     return -1;
 #undef CK
 }

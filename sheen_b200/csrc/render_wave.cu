@@ -764,7 +764,7 @@ static void wave_free(Wave* w) {
     if (!w) return;
     if (w->exec) cudaGraphExecDestroy(w->exec);
     if (w->capture_stream) cudaStreamDestroy(w->capture_stream);
-    cudaFree(w->block);
+    dfree(w->block);
     delete w;
 }
 
@@ -792,7 +792,7 @@ static cudaError_t wave_reserve_into(Wave*& w, int L, long long nsamples) {
     wave_free(w);
     w = new Wave();
     const size_t bytes = wave_scratch_bytes(L, nsamples);
-    cudaError_t e = cudaMalloc(&w->block, bytes);
+    cudaError_t e = dmalloc(&w->block, bytes);
     if (e != cudaSuccess) {
         delete w;
         w = nullptr;

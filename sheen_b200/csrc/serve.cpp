@@ -383,6 +383,7 @@ extern "C" int sheen_server_create(const SheenServerConfig* cfg, SheenServer* ou
     sv->form = c.form;
     sv->tile_samples = c.tile_samples > 0 ? c.tile_samples : kDefaultTileSamples;
     size_t free_b = 0, total_b = 0;
+    trim_pool();   // blocks the library keeps for reuse count as free
     cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
     if (e != cudaSuccess) {
         delete sv;

@@ -29,6 +29,8 @@ const Key kKeys[] = {
     {"wave.refill_min", &Tuning::refill_min, 1, 32},
     {"wave.shadow_blocks_per_sm", &Tuning::shadow_blocks_per_sm, 0, 16},
     {"build.device", &Tuning::build_device, 0, 1},
+    {"build.concurrent", &Tuning::build_concurrent, 0, 1},
+    {"mem.pool_keep_mb", &Tuning::pool_keep_mb, 0, 1 << 20},
 };
 
 }  // namespace
@@ -109,7 +111,7 @@ extern "C" int sheen_autotune(SheenDeviceScene h, int W, int H, int aa, int reps
     float4* buf = nullptr;
     cudaStream_t st = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    cudaError_t e = cudaMalloc(&buf, (size_t)W * H * sizeof(float4));
+    cudaError_t e = dmalloc(&buf, (size_t)W * H * sizeof(float4));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
@@ -132,7 +134,7 @@ extern "C" int sheen_autotune(SheenDeviceScene h, int W, int H, int aa, int reps
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (st) cudaStreamDestroy(st);
-    cudaFree(buf);
+    dfree(buf);
     if (e != cudaSuccess) {
         apply({t0.shadow_kernel, t0.refill_min, t0.shadow_blocks_per_sm});
         set_error(cudaGetErrorString(e));

@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -56,7 +57,7 @@ std::vector<uint8_t> build_mip_chain(const uint8_t* px, int w, int h, int& mips)
 }
 
 // Arena layout builder: records (host source, size) pairs at 256-byte
-// aligned offsets, then copies everything with one staging buffer.
+// aligned offsets; upload_items copies them.
 struct Arena {
     struct Item { const void* src; size_t bytes; size_t off; };
     std::vector<Item> items;
@@ -68,6 +69,93 @@ struct Arena {
         return size - bytes;
     }
 };
+
+// Host -> device copies through a pinned ring kept for the life of the
+// process (per device): kUpWorkers threads each own two kUpSlot-byte pinned
+// slots and a stream; a worker copies its chunk into a free slot (waiting on
+// the slot's event) and queues the slot's H2D copy, so host copies and DMA
+// overlap and several host cores share the memcpy.  Allocating and freeing
+// pinned memory per call costs far more than the copy itself.
+constexpr int kUpWorkers = 8;
+constexpr size_t kUpSlot = 4u << 20;
+constexpr int kUpMaxDevices = 64;
+
+struct UploadRing {
+    void* slot[2 * kUpWorkers] = {nullptr};
+    cudaEvent_t ev[2 * kUpWorkers] = {nullptr};
+    cudaStream_t st[kUpWorkers] = {nullptr};
+    bool ready = false;
+};
+std::mutex g_up_mu;
+UploadRing g_up[kUpMaxDevices];
+
+cudaError_t ring_init(UploadRing& r) {
+    if (r.ready) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 2 * kUpWorkers && e == cudaSuccess; i++) {
+        e = cudaMallocHost(&r.slot[i], kUpSlot);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r.ev[i], cudaEventDisableTiming);
+    }
+    for (int w = 0; w < kUpWorkers && e == cudaSuccess; w++) e = cudaStreamCreateWithFlags(&r.st[w], cudaStreamNonBlocking);
+    if (e == cudaSuccess) r.ready = true;
+    return e;
+}
+
+struct Copy { void* dst; const void* src; size_t bytes; };
+
+// Copies every item (src null: zero fill) and waits for completion.
+cudaError_t upload_items(const std::vector<Copy>& items) {
+    int dev_id = 0;
+    cudaError_t e = cudaGetDevice(&dev_id);
+    if (e != cudaSuccess) return e;
+    if (dev_id < 0 || dev_id >= kUpMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_up_mu);
+    UploadRing& r = g_up[dev_id];
+    if ((e = ring_init(r)) != cudaSuccess) return e;
+    struct Chunk { char* dst; const char* src; size_t bytes; };
+    std::vector<Chunk> chunks;
+    for (const Copy& c : items) {
+        if (!c.bytes) continue;
+        if (!c.src) {
+            if ((e = cudaMemsetAsync(c.dst, 0, c.bytes, r.st[0])) != cudaSuccess) return e;
+            continue;
+        }
+        for (size_t off = 0; off < c.bytes; off += kUpSlot)
+            chunks.push_back({static_cast<char*>(c.dst) + off, static_cast<const char*>(c.src) + off,
+                              std::min(kUpSlot, c.bytes - off)});
+    }
+    const int workers = (int)std::min<size_t>(kUpWorkers, std::max<size_t>(chunks.size(), 1));
+    std::vector<cudaError_t> err((size_t)workers, cudaSuccess);
+    auto work = [&](int w) {
+        cudaSetDevice(dev_id);
+        int k = 0;
+        for (size_t c = (size_t)w; c < chunks.size(); c += (size_t)workers, k++) {
+            const int sl = 2 * w + (k & 1);
+            cudaError_t we = cudaEventSynchronize(r.ev[sl]);
+            if (we == cudaSuccess) {
+                std::memcpy(r.slot[sl], chunks[c].src, chunks[c].bytes);
+                we = cudaMemcpyAsync(chunks[c].dst, r.slot[sl], chunks[c].bytes, cudaMemcpyHostToDevice, r.st[w]);
+            }
+            if (we == cudaSuccess) we = cudaEventRecord(r.ev[sl], r.st[w]);
+            if (we != cudaSuccess) { err[(size_t)w] = we; return; }
+        }
+    };
+    if (workers == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> th;
+        for (int w = 1; w < workers; w++) th.emplace_back(work, w);
+        work(0);
+        for (auto& t : th) t.join();
+    }
+    for (int w = 0; w < kUpWorkers; w++) {
+        const cudaError_t se = cudaStreamSynchronize(r.st[w]);
+        if (e == cudaSuccess) e = se;
+    }
+    for (cudaError_t we : err)
+        if (e == cudaSuccess) e = we;
+    return e;
+}
 
 template <class T>
 void push_box(std::vector<float>& lo, std::vector<float>& hi, const T a[3], const T b[3]) {
@@ -294,7 +382,7 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     const size_t o_tally = ar.add(nullptr, 8 * sizeof(unsigned long long));
     ar.size = (ar.size + 255) & ~(size_t)255;
 
-    cudaError_t e = cudaMalloc(&s->arena, ar.size);
+    cudaError_t e = dmalloc(&s->arena, ar.size);
     if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); delete s; return -1; }
     s->arena_bytes = ar.size;
     char* base = (char*)s->arena;
@@ -308,16 +396,11 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
         if (it.off == o_hf) it.src = hfs.data();
     }
 
-    // One pinned staging buffer, one copy.
-    void* stage = nullptr;
-    e = cudaMallocHost(&stage, ar.size);
-    if (e != cudaSuccess) { cudaFree(s->arena); set_error(cudaGetErrorString(e)); delete s; return -1; }
-    std::memset(stage, 0, ar.size);
-    for (const auto& it : ar.items)
-        if (it.src) std::memcpy((char*)stage + it.off, it.src, it.bytes);
-    e = cudaMemcpy(s->arena, stage, ar.size, cudaMemcpyHostToDevice);
-    cudaFreeHost(stage);
-    if (e != cudaSuccess) { cudaFree(s->arena); set_error(cudaGetErrorString(e)); delete s; return -1; }
+    // Every array straight from its host source through the pinned ring.
+    std::vector<Copy> copies;
+    for (const auto& it : ar.items) copies.push_back({base + it.off, it.src, it.bytes});
+    e = upload_items(copies);
+    if (e != cudaSuccess) { dfree(s->arena); set_error(cudaGetErrorString(e)); delete s; return -1; }
     const double t2 = now_ms();
 
     dev::DevScene& v = s->view;
@@ -390,11 +473,27 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     return 0;
 }
 
+// Frees the pinned upload rings (sheen_cleanup, before the device reset).
+void release_upload_rings() {
+    std::lock_guard<std::mutex> lk(g_up_mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (int d = 0; d < kUpMaxDevices; d++) {
+        UploadRing& r = g_up[d];
+        if (!r.ready) continue;
+        cudaSetDevice(d);
+        for (int i = 0; i < 2 * kUpWorkers; i++) { cudaFreeHost(r.slot[i]); cudaEventDestroy(r.ev[i]); }
+        for (int w = 0; w < kUpWorkers; w++) cudaStreamDestroy(r.st[w]);
+        r = UploadRing();
+    }
+    cudaSetDevice(cur);
+}
+
 void scene_release(DeviceScene* s) {
     if (!s) return;
     wave_release(*s);
-    for (void* p : s->extra) cudaFree(p);
-    cudaFree(s->arena);
+    for (void* p : s->extra) dfree(p);
+    dfree(s->arena);
     delete s;
 }
 
