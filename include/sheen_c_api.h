@@ -239,6 +239,13 @@ int sheen_bvh4_compare_builders(const SheenScene* scene, double* times_ms);
  *   "wave.refill_min"            1..32 (default 8): idle lanes that make a
  *                                   warp take new rays (shadow_kernel 1)
  *   "wave.shadow_blocks_per_sm"  0..16 (default 0 = as many as fit)
+ *   "wave.shadow_stack"          0 (default): traversal stack of the refill
+ *                                   shadow stage in local memory; 1: node
+ *                                   entries in shared memory (24 KB/block)
+ *   "build.concurrent"           1 (default): the subset BVH4s are built
+ *                                   beside the full one (two host threads)
+ *   "mem.pool_keep_mb"           0..1048576 (default 16384): freed device
+ *                                   memory the library keeps for reuse
  *   "build.device"               1 (default): the wavefront form's triangle
  *                                   BVH4s are built on the GPU; 0: on the
  *                                   host.  Both builders give byte-identical
@@ -252,10 +259,12 @@ typedef struct SheenTuneResult {
     int candidates;                                        /* settings timed */
     double best_ms;                                        /* frame time with it */
     double default_ms;                                     /* frame time with the setting in force before */
+    int shadow_stack;                                      /* the setting kept: wave.shadow_stack */
 } SheenTuneResult;
 
 /* Autotuner: times candidate launch parameters (both shadow-stage variants,
- * refill thresholds 4/8/16/24, shadow blocks per SM) on a resident
+ * refill thresholds 4/8/16/24, shadow blocks per SM, traversal stack in
+ * local or shared memory) on a resident
  * SHEEN_FORM_WAVEFRONT scene for one frame shape -- per candidate one
  * warm-up frame, then `reps` frames timed with CUDA events -- and keeps the
  * fastest (process-wide, as sheen_tune_set).  Renders into a device buffer it

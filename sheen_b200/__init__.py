@@ -286,13 +286,13 @@ def tune_get(key: str) -> int:
     return v.value
 
 
-TUNE_KEYS = ("wave.shadow_kernel", "wave.refill_min", "wave.shadow_blocks_per_sm")
+TUNE_KEYS = ("wave.shadow_kernel", "wave.refill_min", "wave.shadow_blocks_per_sm", "wave.shadow_stack")
 
 
 class TuneResult(ctypes.Structure):
     _fields_ = [("shadow_kernel", ctypes.c_int), ("refill_min", ctypes.c_int),
                 ("shadow_blocks_per_sm", ctypes.c_int), ("candidates", ctypes.c_int),
-                ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double)]
+                ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double), ("shadow_stack", ctypes.c_int)]
 
 
 def autotune(scene: "DeviceScene", width: int, height: int, aa: int, reps: int = 3, cache: str | None = None,
@@ -310,7 +310,8 @@ def autotune(scene: "DeviceScene", width: int, height: int, aa: int, reps: int =
             table = json.load(f)
         if key in table:
             for k in TUNE_KEYS:
-                tune_set(k, table[key][k])
+                if k in table[key]:
+                    tune_set(k, table[key][k])
             return dict(table[key], cached=True)
     L = lib()
     L.sheen_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -319,7 +320,8 @@ def autotune(scene: "DeviceScene", width: int, height: int, aa: int, reps: int =
     r = TuneResult()
     _check(L.sheen_autotune(scene.handle, width, height, aa, reps, ctypes.byref(r)))
     res = {"wave.shadow_kernel": r.shadow_kernel, "wave.refill_min": r.refill_min,
-           "wave.shadow_blocks_per_sm": r.shadow_blocks_per_sm, "candidates": r.candidates,
+           "wave.shadow_blocks_per_sm": r.shadow_blocks_per_sm, "wave.shadow_stack": r.shadow_stack,
+           "candidates": r.candidates,
            "best_ms": r.best_ms, "default_ms": r.default_ms}
     if cache:
         table[key] = res

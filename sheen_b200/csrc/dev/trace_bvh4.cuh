@@ -26,6 +26,7 @@ struct QRay {
     float ox, oy, oz;      // origin
     float ix, iy, iz;      // 1 / direction, zero components nudged to +-1e-30
     float tmin;
+    uint32_t octant;       // bit k set when inverse direction component k is negative
 };
 
 __device__ __forceinline__ float safe_inv(float d) {
@@ -38,6 +39,7 @@ __device__ __forceinline__ QRay make_qray(const Ray& r) {
     q.ox = r.o.x; q.oy = r.o.y; q.oz = r.o.z;
     q.ix = safe_inv(r.d.x); q.iy = safe_inv(r.d.y); q.iz = safe_inv(r.d.z);
     q.tmin = r.tmin;
+    q.octant = (q.ix < 0.0f ? 1u : 0u) | (q.iy < 0.0f ? 2u : 0u) | (q.iz < 0.0f ? 4u : 0u);
     return q;
 }
 
@@ -53,6 +55,14 @@ __device__ __forceinline__ float byte_as_float(uint32_t w, int i) {
 
 // Tests the up-to-4 children of `node`; returns a bit mask of hit children
 // and their entry distances.
+//
+// With a = s / d >= 0 the decoded plane distance fmaf(q, a, b) grows with q
+// (fmaf is monotone in q), so the low byte gives the entry plane and the
+// high byte the exit plane; with a < 0 the other way round.  The ray's
+// octant picks the entry and exit words once per node, which gives exactly
+// the min / max of the two plane distances without computing both orders.
+// All four slots are evaluated and the unused ones masked off by the child
+// count, so lanes on nodes with different counts do not diverge.
 __device__ __forceinline__ int qnode_children(const QNode4* __restrict__ nodes, int id, const QRay& r, float tfar,
                                               float tn[4], uint4& child) {
     const float4 oe = __ldg(&nodes[id].origin_exp);
@@ -68,20 +78,22 @@ __device__ __forceinline__ int qnode_children(const QNode4* __restrict__ nodes, 
     const float ax = sx * r.ix, bx = (oe.x - r.ox) * r.ix;
     const float ay = sy * r.iy, by = (oe.y - r.oy) * r.iy;
     const float az = sz * r.iz, bz = (oe.z - r.oz) * r.iz;
+    const uint32_t xn = (r.octant & 1u) ? qb.y : qb.x, xf = (r.octant & 1u) ? qb.x : qb.y;
+    const uint32_t yn = (r.octant & 2u) ? qb.w : qb.z, yf = (r.octant & 2u) ? qb.z : qb.w;
+    const uint32_t zn = (r.octant & 4u) ? qz.y : qz.x, zf = (r.octant & 4u) ? qz.x : qz.y;
     int mask = 0;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        if (i >= count) break;
-        const float x0 = fmaf(byte_as_float(qb.x, i), ax, bx), x1 = fmaf(byte_as_float(qb.y, i), ax, bx);
-        const float y0 = fmaf(byte_as_float(qb.z, i), ay, by), y1 = fmaf(byte_as_float(qb.w, i), ay, by);
-        const float z0 = fmaf(byte_as_float(qz.x, i), az, bz), z1 = fmaf(byte_as_float(qz.y, i), az, bz);
-        const float tnear = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), r.tmin));
-        const float texit = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tfar));
+        const float x0 = fmaf(byte_as_float(xn, i), ax, bx), x1 = fmaf(byte_as_float(xf, i), ax, bx);
+        const float y0 = fmaf(byte_as_float(yn, i), ay, by), y1 = fmaf(byte_as_float(yf, i), ay, by);
+        const float z0 = fmaf(byte_as_float(zn, i), az, bz), z1 = fmaf(byte_as_float(zf, i), az, bz);
+        const float tnear = fmaxf(fmaxf(x0, y0), fmaxf(z0, r.tmin));
+        const float texit = fminf(fminf(x1, y1), fminf(z1, tfar));
         // widen by 2^-20 relative (texit grows, tnear shrinks)
         const float lo = tnear - fabsf(tnear) * 9.5367431640625e-7f;
         const float hi = texit + fabsf(texit) * 9.5367431640625e-7f;
         tn[i] = lo;
-        if (lo <= hi) mask |= 1 << i;
+        if (lo <= hi && i < count) mask |= 1 << i;
     }
     return mask;
 }

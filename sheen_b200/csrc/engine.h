@@ -135,6 +135,7 @@ struct Tuning {
     int shadow_kernel = 1;          // 0: 32-ray batches per warp; 1: per-lane refill
     int refill_min = 8;             // idle lanes that trigger a refill (shadow_kernel 1)
     int shadow_blocks_per_sm = 0;   // 128-thread blocks per SM for the shadow stage; 0: occupancy limit
+    int shadow_stack = 0;           // refill shadow stage: traversal stack nodes in 0 local / 1 shared memory
     int build_device = 1;           // wavefront triangle BVH4s: 1 built on the device, 0 on the host
     int build_concurrent = 1;       // device build: the subset trees beside the full tree (2 host threads)
     int pool_keep_mb = 16384;       // freed device memory the library's pool keeps for reuse

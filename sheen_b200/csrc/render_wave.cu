@@ -170,7 +170,7 @@ __device__ __forceinline__ float3 refract_dir(const DevScene& S, const Hit& gh, 
 }
 
 template <int F>
-__global__ void __launch_bounds__(128) wave_primary(DevScene S, WaveView V) {
+__global__ void __launch_bounds__(128, 8) wave_primary(DevScene S, WaveView V) {
     using T = FastTracer<false, F>;
     Counters c;
     while (true) {
@@ -288,8 +288,15 @@ __global__ void __launch_bounds__(128) wave_shadow(DevScene S, WaveView V) {
 // long rays no longer hold 31 finished lanes hostage.  The mesh walks are
 // qmesh_trace's, step for step (same child order, same stack, same tests),
 // so every ray's result is the one wave_shadow computes.
-template <int F>
-__global__ void __launch_bounds__(128, 5) wave_shadow_refill(DevScene S, WaveView V, int refill_min) {
+//
+// SMEM_STACK places the node half of the traversal stack in shared memory
+// (slot-major, [slot][thread]: the lanes of a warp touch 32 consecutive
+// words, one per bank, whatever their stack depths) instead of per-thread
+// local memory, whose scattered stores fill L1 with 32-byte sectors carrying
+// 4 useful bytes; the entry distances (closest-hit walks of the passable set
+// only) stay in local memory.  24 KB per 128-thread block.
+template <int F, bool SMEM_STACK>
+__global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S, WaveView V, int refill_min) {
     using T = FastTracer<false, F>;
     constexpr unsigned int kFull = 0xffffffffu;
     constexpr uint32_t kLeafBit = 0x80000000u;
@@ -318,8 +325,13 @@ __global__ void __launch_bounds__(128, 5) wave_shadow_refill(DevScene S, WaveVie
     uint32_t entry = 0;
     int sp = 0, wbest = -1;
     float t_best = 0.0f, wu = 0.0f, wv = 0.0f;
-    uint32_t stack_e[kQStack];
+    uint32_t stack_e_local[SMEM_STACK ? 1 : kQStack];
+    __shared__ uint32_t stack_e_shared[SMEM_STACK ? kQStack : 1][SMEM_STACK ? 128 : 1];
     float stack_t[kQStack];
+    auto stack_e = [&](int i) -> uint32_t& {
+        if constexpr (SMEM_STACK) return stack_e_shared[i][threadIdx.x];
+        else return stack_e_local[i];
+    };
 
     bool exhausted = false;
     for (;;) {
@@ -437,7 +449,7 @@ __global__ void __launch_bounds__(128, 5) wave_shadow_refill(DevScene S, WaveVie
                     for (int i = 0; i < 4; i++) {
                         if (!(mask & (1 << i))) continue;
                         if (first < 0) first = i;
-                        else if (sp < kQStack) stack_e[sp++] = cid[i];
+                        else if (sp < kQStack) stack_e(sp++) = cid[i];
                     }
                     entry = cid[first];
                 } else {
@@ -453,7 +465,7 @@ __global__ void __launch_bounds__(128, 5) wave_shadow_refill(DevScene S, WaveVie
 #undef CSWAP
                     for (int k = m - 1; k >= 1; k--) {
                         if (sp < kQStack) {
-                            stack_e[sp] = cid[key[k] & 3u];
+                            stack_e(sp) = cid[key[k] & 3u];
                             stack_t[sp] = tn[key[k] & 3u];
                             sp++;
                         }
@@ -466,7 +478,7 @@ __global__ void __launch_bounds__(128, 5) wave_shadow_refill(DevScene S, WaveVie
             bool ended = true;
             while (sp > 0) {
                 --sp;
-                if (state == kWalkBlock || stack_t[sp] <= t_best) { entry = stack_e[sp]; ended = false; break; }
+                if (state == kWalkBlock || stack_t[sp] <= t_best) { entry = stack_e(sp); ended = false; break; }
             }
             if (ended) state = state == kWalkPass ? kEndPass : kEndBlock;
         }
@@ -491,7 +503,7 @@ __global__ void __launch_bounds__(128, 5) wave_shadow_refill(DevScene S, WaveVie
                 ended = true;
                 while (sp > 0) {
                     --sp;
-                    if (state == kWalkBlock || stack_t[sp] <= t_best) { entry = stack_e[sp]; ended = false; break; }
+                    if (state == kWalkBlock || stack_t[sp] <= t_best) { entry = stack_e(sp); ended = false; break; }
                 }
             }
             if (ended) state = state == kWalkPass ? kEndPass : kEndBlock;
@@ -501,7 +513,7 @@ __global__ void __launch_bounds__(128, 5) wave_shadow_refill(DevScene S, WaveVie
 }
 
 template <int F>
-__global__ void __launch_bounds__(128) wave_reflect(DevScene S, WaveView V) {
+__global__ void __launch_bounds__(128, 8) wave_reflect(DevScene S, WaveView V) {
     using T = FastTracer<false, F>;
     Counters c;
     const unsigned int n = V.ctr[kReflCount];
@@ -538,7 +550,7 @@ __global__ void __launch_bounds__(128) wave_reflect(DevScene S, WaveView V) {
 }
 
 template <int F>
-__global__ void __launch_bounds__(128) wave_refract(DevScene S, WaveView V) {
+__global__ void __launch_bounds__(128, 8) wave_refract(DevScene S, WaveView V) {
     using T = FastTracer<false, F>;
     Counters c;
     const unsigned int n = V.ctr[kRefrCount];
@@ -737,13 +749,17 @@ static cudaError_t run_pipeline(const DeviceScene& s, const dev::WaveView& V, in
     }
     const Tuning tu = tuning();
     const bool refill = tu.shadow_kernel == 1;
-    const int g_shadow = refill ? shadow_grid(dev::wave_shadow_refill<F>, sms, tu.shadow_blocks_per_sm)
-                                : shadow_grid(dev::wave_shadow<F>, sms, tu.shadow_blocks_per_sm);
+    const bool smem = tu.shadow_stack == 1;
+    const int g_shadow = !refill ? shadow_grid(dev::wave_shadow<F>, sms, tu.shadow_blocks_per_sm)
+                         : smem  ? shadow_grid(dev::wave_shadow_refill<F, true>, sms, tu.shadow_blocks_per_sm)
+                                 : shadow_grid(dev::wave_shadow_refill<F, false>, sms, tu.shadow_blocks_per_sm);
     auto shadow = [&]() {
-        if (refill)
-            dev::wave_shadow_refill<F><<<g_shadow, 128, 0, stream>>>(s.view, V, tu.refill_min);
-        else
+        if (!refill)
             dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
+        else if (smem)
+            dev::wave_shadow_refill<F, true><<<g_shadow, 128, 0, stream>>>(s.view, V, tu.refill_min);
+        else
+            dev::wave_shadow_refill<F, false><<<g_shadow, 128, 0, stream>>>(s.view, V, tu.refill_min);
     };
     cudaError_t e;
     if ((e = cudaMemsetAsync(V.ctr, 0, dev::kCounterWords * sizeof(unsigned int), stream)) != cudaSuccess) return e;

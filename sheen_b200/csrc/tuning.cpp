@@ -28,6 +28,7 @@ const Key kKeys[] = {
     {"wave.shadow_kernel", &Tuning::shadow_kernel, 0, 1},
     {"wave.refill_min", &Tuning::refill_min, 1, 32},
     {"wave.shadow_blocks_per_sm", &Tuning::shadow_blocks_per_sm, 0, 16},
+    {"wave.shadow_stack", &Tuning::shadow_stack, 0, 1},
     {"build.device", &Tuning::build_device, 0, 1},
     {"build.concurrent", &Tuning::build_concurrent, 0, 1},
     {"mem.pool_keep_mb", &Tuning::pool_keep_mb, 0, 1 << 20},
@@ -83,13 +84,14 @@ namespace sheen {
 namespace {
 
 struct Candidate {
-    int shadow_kernel, refill_min, shadow_blocks_per_sm;
+    int shadow_kernel, refill_min, shadow_blocks_per_sm, shadow_stack;
 };
 
 void apply(const Candidate& c) {
     tuning_set("wave.shadow_kernel", c.shadow_kernel);
     tuning_set("wave.refill_min", c.refill_min);
     tuning_set("wave.shadow_blocks_per_sm", c.shadow_blocks_per_sm);
+    tuning_set("wave.shadow_stack", c.shadow_stack);
 }
 
 }  // namespace
@@ -104,10 +106,11 @@ extern "C" int sheen_autotune(SheenDeviceScene h, int W, int H, int aa, int reps
     if (reps < 1) reps = 3;
     const Tuning t0 = tuning();
     std::vector<Candidate> cands;
-    cands.push_back({t0.shadow_kernel, t0.refill_min, t0.shadow_blocks_per_sm});
-    cands.push_back({0, t0.refill_min, 0});
-    for (int r : {4, 8, 16, 24})
-        for (int b : {0, 4}) cands.push_back({1, r, b});
+    cands.push_back({t0.shadow_kernel, t0.refill_min, t0.shadow_blocks_per_sm, t0.shadow_stack});
+    cands.push_back({0, t0.refill_min, 0, 0});
+    for (int st : {0, 1})
+        for (int r : {4, 8, 16, 24})
+            for (int b : {0, 4}) cands.push_back({1, r, b, st});
     float4* buf = nullptr;
     cudaStream_t st = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -136,7 +139,7 @@ extern "C" int sheen_autotune(SheenDeviceScene h, int W, int H, int aa, int reps
     if (st) cudaStreamDestroy(st);
     dfree(buf);
     if (e != cudaSuccess) {
-        apply({t0.shadow_kernel, t0.refill_min, t0.shadow_blocks_per_sm});
+        apply({t0.shadow_kernel, t0.refill_min, t0.shadow_blocks_per_sm, t0.shadow_stack});
         set_error(cudaGetErrorString(e));
         return -1;
     }
@@ -144,6 +147,7 @@ extern "C" int sheen_autotune(SheenDeviceScene h, int W, int H, int aa, int reps
     out->shadow_kernel = cands[best_i].shadow_kernel;
     out->refill_min = cands[best_i].refill_min;
     out->shadow_blocks_per_sm = cands[best_i].shadow_blocks_per_sm;
+    out->shadow_stack = cands[best_i].shadow_stack;
     out->candidates = (int)cands.size();
     out->best_ms = best;
     out->default_ms = first;
