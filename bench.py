@@ -40,7 +40,12 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 W, H, SPP = 1920, 1080, 4
-CPU_BAND = (480, 512)      # pixel rows of the CPU samples (two 16-row blocks of the 1080-row frame)
+CPU_BAND = (480, 512)
+# DRAM bytes (read + write) per shadow ray of the shadow stage, from the
+# one-pass ncu capture of the full-size mesh frame (profiles/
+# wave_shadow_refill_mesh_1920x1080_4spp_dram.md); the roofline's traffic
+# per launch is this times the launch's shadow rays.
+SHADOW_DRAM_BYTES_PER_RAY = 5159825152 / 38552584      # pixel rows of the CPU samples (two 16-row blocks of the 1080-row frame)
 
 
 class quiet_stdout:
@@ -233,15 +238,51 @@ def run_ours(args):
     e2e = rays * e2e_steps * world / e2e_s / 1e6
 
     pk = peaks()
-    # algorithmic bytes: 32 B ray in + 16 B hit out per
-    # ray, B_node per box test, B_prim per primitive test
-    b_node, b_prim = (32, 48) if form == sb.FORM_PLAIN else (64, 48)
-    bytes_alg = rays * 48 + nodes * b_node + prims * b_prim
-    achieved_gbs = bytes_alg / (frame_ms / 1e3) / 1e9
-    fp32_flops = nodes * 14 + prims * 35
     fp32_peak = 148 * 128 * 2 * pk["sm_max_mhz"] * 1e6
-    clocks = clk.summary()
+    # Algorithmic bytes and FP32 work: 32 B ray in +
+    # 16 B hit out per ray, the node record per node visited, 48 B per
+    # triangle tested; 14 FP32 ops per box test (a BVH4 node visit tests 4
+    # boxes; the plain form counts single boxes), 35 per triangle test.
+    b_node, boxes_per_visit = (32, 1) if form == sb.FORM_PLAIN else (64, 4)
+    bytes_alg = rays * 48 + nodes * b_node + prims * 48
+    fp32_flops = nodes * boxes_per_visit * 14 + prims * 35
+    frame_roof = {"achieved_gbs": round(bytes_alg / (frame_ms / 1e3) / 1e9, 1),
+                  "frac": round(bytes_alg / (frame_ms / 1e3) / 1e9 / pk["hbm_gbs"], 4),
+                  "algorithmic_bytes": int(bytes_alg), "fp32_flops": int(fp32_flops),
+                  "fp32_tflops": round(fp32_flops / (frame_ms / 1e3) / 1e12, 2)}
 
+    # Dominant kernel.  Wavefront: the shadow stage (3 launches a frame),
+    # timed with CUDA events at the stage boundaries of directly launched
+    # frames (L2 flushed before each); its node / triangle tests are the
+    # counting megakernel's shadow-query counters (same walks).  Plain: the
+    # single megakernel launch, timed above.
+    stages = None
+    if form == sb.FORM_WAVEFRONT:
+        profs = []
+        for i in range(max(3, args.steps // 2)):
+            flush.fill_(float(i))
+            profs.append(ds.profile_stages(W, H, SPP, out.data_ptr(), stream))
+        med = lambda key: float(np.median([p[key] if not isinstance(p[key], list) else sum(p[key]) for p in profs]))
+        stages = {k: round(med(k), 3) for k in ("primary_ms", "shadow_ms", "reflect_ms", "refract_ms", "resolve_ms",
+                                                 "total_ms")}
+        stages["shadow_launch_ms"] = [round(float(np.median([p["shadow_ms"][j] for p in profs])), 3) for j in range(3)]
+        stages["shadow_rays"] = list(profs[0]["shadow_rays"])
+        stages["share_shadow"] = round(stages["shadow_ms"] / stages["total_ms"], 3)
+        k_name, k_launches = "wave_shadow_refill (shadow stage)", 3
+        k_ms = stages["shadow_ms"]
+        k_rays, k_nodes, k_prims = stn["shadow_rays"], stn["shadow_node_visits"], stn["shadow_prim_tests"]
+    else:
+        k_name, k_launches, k_ms = "plain_kernel", 1, frame_ms
+        k_rays, k_nodes, k_prims = rays, nodes, prims
+    k_bytes = k_rays * 48 + k_nodes * b_node + k_prims * 48
+    k_flops = k_nodes * boxes_per_visit * 14 + k_prims * 35
+    k_gbs = k_bytes / (k_ms / 1e3) / 1e9
+    k_tflops = k_flops / (k_ms / 1e3) / 1e12
+    hbm_bound = k_bytes / (pk["hbm_gbs"] * 1e9) >= k_flops / fp32_peak
+    traffic = None
+    if form == sb.FORM_WAVEFRONT and (W, H, SPP) == (1920, 1080, 4) and args.config == 1:
+        traffic = int(SHADOW_DRAM_BYTES_PER_RAY * k_rays / k_launches) if SHADOW_DRAM_BYTES_PER_RAY else None
+    clocks = clk.summary()
     line = {
         "metric": "Mrays/s", "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(frame_ms, 3),
@@ -259,13 +300,15 @@ def run_ours(args):
                 "d2h_bytes_per_step": W * H * 16,
                 "call": "sheen_render_scene_rgba (upload + BVH build + render + readback)",
                 "scene_build_ms": round(st2["build_ms"], 1), "scene_upload_ms": round(st2["upload_ms"], 1)},
-        "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
-                     "frac": round(achieved_gbs / pk["hbm_gbs"], 4), "traffic": None,
-                     "peak_source": pk["src"],
-                     "algorithmic_bytes_per_frame": int(bytes_alg),
-                     "fp32": {"flops_per_frame": int(fp32_flops),
-                              "achieved_tflops": round(fp32_flops / (frame_ms / 1e3) / 1e12, 2),
-                              "peak_tflops_nominal": round(fp32_peak / 1e12, 1)}},
+        "roofline": {"bound": "hbm" if hbm_bound else "fp32", "achieved": round(k_gbs, 1), "peak": pk["hbm_gbs"],
+                     "unit": "GB/s", "frac": round(k_gbs / pk["hbm_gbs"], 4), "traffic": traffic,
+                     "peak_source": pk["src"], "kernel": k_name, "launches_per_frame": k_launches,
+                     "avg_launch_ms": round(k_ms / k_launches, 3),
+                     "algorithmic_bytes_per_launch": int(k_bytes / k_launches),
+                     "fp32": {"achieved_tflops": round(k_tflops, 2), "peak_tflops_nominal": round(fp32_peak / 1e12, 1),
+                              "frac": round(k_tflops * 1e12 / fp32_peak, 4)},
+                     "frame": frame_roof},
+        "stages": stages,
         "gpu_launches": args.steps * launches_per_frame(form),
         "clocks": clocks,
     }

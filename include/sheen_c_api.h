@@ -142,6 +142,9 @@ typedef struct SheenRenderStats {
     double render_ms;                    /* device time of the render launches */
     unsigned long long device_bytes;     /* resident scene footprint */
     unsigned long long upload_bytes;     /* bytes copied host -> device for the scene */
+    unsigned long long shadow_node_visits; /* part of node_visits spent on glass-aware shadow
+                                              queries (the wavefront shadow stage) */
+    unsigned long long shadow_prim_tests;  /* part of prim_tests spent on them */
 } SheenRenderStats;
 
 /* Render into a caller-owned HOST buffer of width*height float4 (RGBA, linear,
@@ -228,6 +231,23 @@ int sheen_selfcheck_bvh4(const SheenScene* scene);
  * difference, set 0 = all, 1 = blocking, 2 = passable; -1 on error.
  * times_ms (may be NULL) receives {host build ms, device build ms}. */
 int sheen_bvh4_compare_builders(const SheenScene* scene, double* times_ms);
+
+/* Stage profile of one wavefront frame (sheen_scene_profile_stages): device
+ * times of the queue kernels, measured with CUDA events at the stage
+ * boundaries of a frame launched directly (not from the captured graph), and
+ * the rays each kernel issued.  No counterpart in the reference (one
+ * megakernel, render_kernel.cu:438-814). */
+typedef struct SheenStageProfile {
+    double primary_ms, shadow_ms[3], reflect_ms, refract_ms, resolve_ms, total_ms;
+    unsigned long long primary_rays, shadow_rays[3], reflect_rays, refract_rays;
+} SheenStageProfile;
+
+/* One full frame of a SHEEN_FORM_WAVEFRONT scene into a DEVICE buffer
+ * (width*height float4) with the stage profile above; synchronous.  Scenes
+ * whose frames run on the megakernel (beams, media, shadow-debug materials,
+ * more than 16 lights) have no stages: -1. */
+int sheen_scene_profile_stages(SheenDeviceScene scene, int width, int height, int aa_samples,
+                               float* out_rgba_device, void* stream, SheenStageProfile* out);
 
 /* Launch parameters of the wavefront form, by name (process-wide; frames
  * captured under older values are re-captured).  No counterpart in the

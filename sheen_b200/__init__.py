@@ -45,10 +45,25 @@ class RenderStats(ctypes.Structure):
                 ("node_visits", ctypes.c_ulonglong), ("prim_tests", ctypes.c_ulonglong),
                 ("build_ms", ctypes.c_double), ("upload_ms", ctypes.c_double),
                 ("photon_ms", ctypes.c_double), ("render_ms", ctypes.c_double),
-                ("device_bytes", ctypes.c_ulonglong), ("upload_bytes", ctypes.c_ulonglong)]
+                ("device_bytes", ctypes.c_ulonglong), ("upload_bytes", ctypes.c_ulonglong),
+                ("shadow_node_visits", ctypes.c_ulonglong), ("shadow_prim_tests", ctypes.c_ulonglong)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class StageProfile(ctypes.Structure):
+    _fields_ = [("primary_ms", ctypes.c_double), ("shadow_ms", ctypes.c_double * 3), ("reflect_ms", ctypes.c_double),
+                ("refract_ms", ctypes.c_double), ("resolve_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+                ("primary_rays", ctypes.c_ulonglong), ("shadow_rays", ctypes.c_ulonglong * 3),
+                ("reflect_rays", ctypes.c_ulonglong), ("refract_rays", ctypes.c_ulonglong)]
+
+    def as_dict(self):
+        d = {}
+        for k, _ in self._fields_:
+            v = getattr(self, k)
+            d[k] = list(v) if not isinstance(v, (int, float)) else v
+        return d
 
 
 class SceneSettings(ctypes.Structure):
@@ -101,6 +116,8 @@ def lib():
     L.sheen_generate_scene.argtypes = [I, U, I, I, ctypes.POINTER(P)]
     L.sheen_generate_scene.restype = I
     L.sheen_scene_primary_hits.argtypes = [P, I, I, I, P, P, P]
+    L.sheen_scene_profile_stages.argtypes = [P, I, I, I, P, P, ctypes.POINTER(StageProfile)]
+    L.sheen_scene_profile_stages.restype = I
     L.sheen_scene_primary_hits.restype = I
     L.sheen_write_png_srgb.argtypes = [ctypes.c_char_p, P, I, I]
     L.sheen_write_png_srgb.restype = I
@@ -200,6 +217,13 @@ class DeviceScene:
                                                _flags(count_rays, False),
                                                ctypes.byref(st) if st is not None else None))
         return st.as_dict() if st is not None else None
+
+    def profile_stages(self, width, height, aa, out_ptr: int, stream: int = 0) -> dict:
+        """One wavefront frame into the device buffer at out_ptr with per-stage
+        device times (CUDA events) and per-kernel ray counts."""
+        p = StageProfile()
+        _check(lib().sheen_scene_profile_stages(self.handle, width, height, aa, out_ptr, stream, ctypes.byref(p)))
+        return p.as_dict()
 
     def primary_hits(self, width, height, aa):
         """Per-sample primary closest hits: object id, material id, t."""

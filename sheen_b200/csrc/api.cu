@@ -40,6 +40,8 @@ void fill_stats(const sheen::DeviceScene& s, const unsigned long long* t, double
         st->secondary_rays = t[2];
         st->node_visits = t[3];
         st->prim_tests = t[4];
+        st->shadow_node_visits = t[5];
+        st->shadow_prim_tests = t[6];
         st->total_rays = t[0] + t[1] + t[2];
     }
     st->build_ms = s.build_ms;
@@ -186,6 +188,23 @@ int sheen_scene_render_host(SheenDeviceScene h, int W, int H, int aa, float* out
     }
     sheen::dfree(d);
     return rc;
+}
+
+int sheen_scene_profile_stages(SheenDeviceScene h, int W, int H, int aa, float* out_device, void* stream,
+                               SheenStageProfile* prof) {
+    auto* s = reinterpret_cast<sheen::DeviceScene*>(h);
+    if (!s || !prof) { sheen::set_error("null scene handle or profile"); return -1; }
+    if (W <= 0 || H <= 0 || aa < 1 || aa > 64 || !out_device) { sheen::set_error("bad render params"); return -1; }
+    if (s->form != SHEEN_FORM_WAVEFRONT) { sheen::set_error("stage profiles apply to SHEEN_FORM_WAVEFRONT scenes"); return -1; }
+    std::memset(prof, 0, sizeof(*prof));
+    const cudaError_t e = sheen::profile_wavefront(*s, W, H, aa, reinterpret_cast<float4*>(out_device),
+                                                   (cudaStream_t)stream, prof);
+    if (e == cudaErrorNotSupported) {
+        sheen::set_error("this scene's frames run on the megakernel: no queue stages");
+        return -1;
+    }
+    if (e != cudaSuccess) return fail_cuda(e);
+    return 0;
 }
 
 int sheen_scene_primary_hits(SheenDeviceScene h, int W, int H, int aa, int* obj, int* mat, float* t) {

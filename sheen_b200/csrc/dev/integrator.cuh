@@ -30,7 +30,12 @@ __device__ __forceinline__ bool shadow_blocked(const DevScene& S, Ray r, RayTall
     for (int pass = 0; pass < 3; pass++) {
         rt.shadow++;
         ShadowHit sh;
+        const unsigned long long n0 = c.nodes, p0 = c.prims;
         const int q = T::shadow(S, r, true, sh, c);
+        if (COUNT) {
+            c.shadow_nodes += c.nodes - n0;
+            c.shadow_prims += c.prims - p0;
+        }
         if (q == kClear) return false;
         if (q == kBlocked) return true;
         r.o = sh.p + r.d * 0.002f;

@@ -16,6 +16,9 @@ namespace dev {
 
 struct Counters {
     unsigned long long nodes = 0, prims = 0;
+    // the part of nodes / prims spent on the glass-aware shadow queries of
+    // the lighting loop (the wavefront form's shadow stage)
+    unsigned long long shadow_nodes = 0, shadow_prims = 0;
 };
 
 constexpr int kRefStack = 64;

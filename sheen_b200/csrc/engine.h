@@ -129,6 +129,8 @@ cudaError_t launch_wavefront_scratch(DeviceScene& s, void* scratch, size_t scrat
                                      Region rg, float4* out, cudaStream_t stream, unsigned long long* tally);
 size_t wave_scratch_bytes(int L, long long nsamples);
 bool wave_pipeline_used(const DeviceScene& s);
+cudaError_t profile_wavefront(DeviceScene& s, int W, int H, int aa, float4* out, cudaStream_t stream,
+                              SheenStageProfile* prof);
 
 // Launch parameters of the wavefront form (tuning.cpp).
 struct Tuning {

@@ -36,6 +36,8 @@ __global__ void __launch_bounds__(128) mega_bvh4_kernel(DevScene S, float4* __re
         if (COUNT) {
             warp_add_fast(&tally[3], c.nodes);
             warp_add_fast(&tally[4], c.prims);
+            warp_add_fast(&tally[5], c.shadow_nodes);
+            warp_add_fast(&tally[6], c.shadow_prims);
         }
     }
 }

@@ -42,6 +42,8 @@ __global__ void __launch_bounds__(128) plain_kernel(DevScene S, float4* __restri
         if (COUNT) {
             warp_add(&tally[3], c.nodes);
             warp_add(&tally[4], c.prims);
+            warp_add(&tally[5], c.shadow_nodes);
+            warp_add(&tally[6], c.shadow_prims);
         }
     }
 }

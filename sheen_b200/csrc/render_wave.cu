@@ -641,6 +641,13 @@ __global__ void wave_resolve(WaveView V, float4* __restrict__ out) {
     out[(size_t)y * V.W + x] = make_float4(acc.x * inv, acc.y * inv, acc.z * inv, 1.0f);
 }
 
+// Copies the three ray counters into snap[3*k .. 3*k+2] (stage profiling).
+__global__ void wave_snapshot(WaveView V, unsigned int* snap, int k) {
+    snap[3 * k] = V.ctr[kRaysPrimary];
+    snap[3 * k + 1] = V.ctr[kRaysShadow];
+    snap[3 * k + 2] = V.ctr[kRaysSecondary];
+}
+
 __global__ void wave_tally_out(WaveView V, unsigned long long* tally) {
     tally[0] += V.ctr[kRaysPrimary];
     tally[1] += V.ctr[kRaysShadow];
@@ -736,10 +743,15 @@ static int shadow_grid(K kernel, int sms, int per_sm) {
     return per_sm > 0 ? std::min(full, sms * per_sm) : full;
 }
 
-// The queue pipeline of one frame for category set F.
+// The queue pipeline of one frame for category set F.  Stage profiling
+// (not inside a graph): `ev` gets 8 events recorded at the stage
+// boundaries (before primary, after primary, shadow, reflect, shadow,
+// refract, shadow, resolve) and `snap` the ray counters after each of the
+// 7 kernels (3 words each).
 template <int F>
 static cudaError_t run_pipeline(const DeviceScene& s, const dev::WaveView& V, int npad, float4* out,
-                                cudaStream_t stream, unsigned long long* tally) {
+                                cudaStream_t stream, unsigned long long* tally, cudaEvent_t* ev = nullptr,
+                                unsigned int* snap = nullptr) {
     static int g_primary = 0, g_reflect = 0, g_refract = 0;
     const int sms = device_sms();
     if (!g_primary) {
@@ -761,17 +773,31 @@ static cudaError_t run_pipeline(const DeviceScene& s, const dev::WaveView& V, in
         else
             dev::wave_shadow_refill<F, false><<<g_shadow, 128, 0, stream>>>(s.view, V, tu.refill_min);
     };
+    int mark = 0;
+    auto stage_end = [&]() {
+        if (snap) dev::wave_snapshot<<<1, 1, 0, stream>>>(V, snap, mark);
+        if (ev) cudaEventRecord(ev[mark + 1], stream);
+        mark++;
+    };
     cudaError_t e;
     if ((e = cudaMemsetAsync(V.ctr, 0, dev::kCounterWords * sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    if (ev) cudaEventRecord(ev[0], stream);
     dev::wave_primary<F><<<g_primary, 128, 0, stream>>>(s.view, V);
+    stage_end();
     shadow();
+    stage_end();
     if ((e = cudaMemsetAsync(&V.ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
     dev::wave_reflect<F><<<g_reflect, 128, 0, stream>>>(s.view, V);
+    stage_end();
     shadow();
+    stage_end();
     if ((e = cudaMemsetAsync(&V.ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
     dev::wave_refract<F><<<g_refract, 128, 0, stream>>>(s.view, V);
+    stage_end();
     shadow();
+    stage_end();
     dev::wave_resolve<<<(npad + 127) / 128, 128, 0, stream>>>(V, out);
+    if (ev) cudaEventRecord(ev[7], stream);
     if (tally) dev::wave_tally_out<<<1, 1, 0, stream>>>(V, tally);
     return cudaGetLastError();
 }
@@ -889,6 +915,63 @@ cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, fl
 }
 
 bool wave_pipeline_used(const DeviceScene& s) { return wave_supported(s); }
+
+// One frame of the queue pipeline launched directly (no graph) with events
+// at the stage boundaries and the ray counters read after every kernel.
+cudaError_t profile_wavefront(DeviceScene& s, int W, int H, int aa, float4* out, cudaStream_t stream,
+                              SheenStageProfile* prof) {
+    if (!wave_supported(s)) return cudaErrorNotSupported;
+    const int ns = clamp_spp(aa);
+    const Region rg{0, 0, W, H};
+    const long long nsamples = region_padded(rg) * ns;
+    if (nsamples > (1ll << 30)) return cudaErrorInvalidValue;
+    cudaError_t e = wave_reserve_into(s.wave, s.view.num_lights, nsamples);
+    if (e != cudaSuccess) return e;
+    const dev::WaveView V = make_view(s, *s.wave, W, H, ns, rg);
+    const int npad = (int)region_padded(rg);
+    cudaEvent_t ev[8] = {nullptr};
+    unsigned int* snap = nullptr;
+    for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&ev[i]);
+    if (e == cudaSuccess) e = dmalloc(&snap, 21 * sizeof(unsigned int));
+    if (e == cudaSuccess)
+        e = simple_scene(s) ? run_pipeline<dev::kCatSimple>(s, V, npad, out, stream, nullptr, ev, snap)
+                            : run_pipeline<dev::kCatAll>(s, V, npad, out, stream, nullptr, ev, snap);
+    unsigned int h[21] = {0};
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) e = cudaMemcpy(h, snap, sizeof(h), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) {
+        float ms[7];
+        for (int i = 0; i < 7; i++) cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
+        // stages in launch order: primary, shadow, reflect, shadow, refract, shadow, resolve
+        prof->primary_ms = ms[0];
+        prof->shadow_ms[0] = ms[1];
+        prof->reflect_ms = ms[2];
+        prof->shadow_ms[1] = ms[3];
+        prof->refract_ms = ms[4];
+        prof->shadow_ms[2] = ms[5];
+        prof->resolve_ms = ms[6];
+        float total = 0.0f;
+        cudaEventElapsedTime(&total, ev[0], ev[7]);
+        prof->total_ms = total;
+        // rays issued by each kernel: differences of the counter snapshots
+        unsigned int prev[3] = {0, 0, 0};
+        unsigned long long rays[7];
+        for (int k = 0; k < 7; k++) {
+            rays[k] = 0;
+            for (int j = 0; j < 3; j++) { rays[k] += h[3 * k + j] - prev[j]; prev[j] = h[3 * k + j]; }
+        }
+        prof->primary_rays = rays[0];
+        prof->shadow_rays[0] = rays[1];
+        prof->reflect_rays = rays[2];
+        prof->shadow_rays[1] = rays[3];
+        prof->refract_rays = rays[4];
+        prof->shadow_rays[2] = rays[5];
+    }
+    for (int i = 0; i < 8; i++)
+        if (ev[i]) cudaEventDestroy(ev[i]);
+    dfree(snap);
+    return e;
+}
 
 cudaError_t launch_wavefront_scratch(DeviceScene& s, void* scratch, size_t scratch_bytes, int W, int H, int aa,
                                      Region rg, float4* out, cudaStream_t stream, unsigned long long* tally) {
