@@ -204,8 +204,18 @@ def run_ours(args):
     nodes, prims = stn["node_visits"], stn["prim_tests"]
     assert stn["total_rays"] == rays or form == sb.FORM_WAVEFRONT
 
+    # --tiles N: each frame as N uneven screen tiles in one batch (one pass
+    # of the queue kernels over all tiles) instead of the captured frame graph
+    tiles = uneven_tiles(W, H, args.tiles, 7) if args.tiles > 0 else None
+
+    def frame():
+        if tiles is None:
+            ds.render_device(W, H, SPP, out.data_ptr(), stream)
+        else:
+            sb.render_batch([(ds, W, H, SPP, t, out.data_ptr()) for t in tiles], stream)
+
     for _ in range(args.warmup):
-        ds.render_device(W, H, SPP, out.data_ptr(), stream)
+        frame()
     torch.cuda.synchronize()
 
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -216,7 +226,7 @@ def run_ours(args):
         for i in range(args.steps):
             flush.fill_(float(i))                      # evict L2 between frames (outside the events)
             starts[i].record()
-            ds.render_device(W, H, SPP, out.data_ptr(), stream)
+            frame()
             ends[i].record()
         torch.cuda.synchronize()
     barrier(world)
@@ -291,6 +301,8 @@ def run_ours(args):
         "config": {"workload": WORKLOADS.get(args.config, f"config {args.config}"),
                    "triangles": scene.view.num_triangles, "width": W, "height": H, "spp": SPP,
                    "form": args.form, "parallelism": f"replicas{world}",
+                   "frame": (f"{args.tiles} uneven tiles in one batched pass" if args.tiles > 0
+                             else "whole frame, captured CUDA graph"),
                    "l2": "256 MB buffer written between timed frames; scene arrays exceed L2",
                    "rays_per_frame": rays, "box_tests_per_frame": nodes, "prim_tests_per_frame": prims,
                    "scene_create_s": round(create_s, 3), "device_bytes": ds.device_bytes,
@@ -322,6 +334,20 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def uneven_tiles(W, H, n, seed):
+    """n rectangles of uneven size covering a W x H frame: rows of uneven
+    height, each cut into tiles of uneven width."""
+    rng = np.random.default_rng(seed)
+    rows = max(1, int(np.sqrt(n)))
+    cols = [n // rows + (1 if r < n % rows else 0) for r in range(rows)]
+    ys = [0] + np.sort(rng.choice(np.arange(1, H), rows - 1, replace=False)).tolist() + [H]
+    tiles = []
+    for r in range(rows):
+        xs = [0] + np.sort(rng.choice(np.arange(1, W), cols[r] - 1, replace=False)).tolist() + [W]
+        tiles += [(xs[c], ys[r], xs[c + 1], ys[r + 1]) for c in range(cols[r])]
+    return tiles
 
 
 def launches_per_frame(form):
@@ -580,6 +606,8 @@ def main():
     ap.add_argument("--width", type=int, default=0, help="override the workload's frame width")
     ap.add_argument("--height", type=int, default=0, help="override the workload's frame height")
     ap.add_argument("--spp", type=int, default=0, help="override the workload's samples per pixel")
+    ap.add_argument("--tiles", type=int, default=0,
+                    help="render each frame as this many uneven screen tiles in one batched pass (wavefront form)")
     ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
                     help="launch parameter of the wavefront form (sheen_tune_set), repeatable")
     ap.add_argument("--requests", type=int, default=512, help="serving config: requests in the stream")

@@ -232,6 +232,31 @@ int sheen_selfcheck_bvh4(const SheenScene* scene);
  * times_ms (may be NULL) receives {host build ms, device build ms}. */
 int sheen_bvh4_compare_builders(const SheenScene* scene, double* times_ms);
 
+/* One job of sheen_render_batch: the pixel rectangle [x0, x1) x [y0, y1) of
+ * a width x height frame of `scene` (x1 <= x0 or y1 <= y0: the whole frame)
+ * at aa_samples per pixel, written into the DEVICE image out_rgba_device
+ * (width*height float4; pixels outside the rectangle are left unchanged). */
+typedef struct SheenBatchJob {
+    SheenDeviceScene scene;
+    int width, height, aa_samples;
+    int x0, y0, x1, y1;
+    float* out_rgba_device;
+} SheenBatchJob;
+
+/* Renders every job in one pass of the wavefront queue kernels (one pass per
+ * kernel variant: scenes of triangles, spheres and planes only, and the
+ * rest, so that batching never changes a pixel): each stage is
+ * one persistent launch over the samples of all jobs (tiles of one frame,
+ * several frames, several scenes, of uneven cost), claimed dynamically by
+ * the blocks from shared queues.  Each job's pixels are exactly those of
+ * rendering it alone.  Jobs on SHEEN_FORM_PLAIN scenes, or whose frames run
+ * on the megakernel (beams, media, shadow-debug materials, more than 16
+ * lights), are rendered one by one on the same stream first.  Asynchronous on
+ * `stream` unless stats is non-NULL (then it synchronises and fills the ray
+ * counts and render_ms).  No counterpart in the reference (one frame per
+ * launch, render_kernel.cu:438-814).  0 / -1. */
+int sheen_render_batch(const SheenBatchJob* jobs, int num_jobs, void* stream, SheenRenderStats* stats);
+
 /* Stage profile of one wavefront frame (sheen_scene_profile_stages): device
  * times of the queue kernels, measured with CUDA events at the stage
  * boundaries of a frame launched directly (not from the captured graph), and

@@ -52,6 +52,12 @@ class RenderStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchJob(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_void_p), ("width", ctypes.c_int), ("height", ctypes.c_int),
+                ("aa_samples", ctypes.c_int), ("x0", ctypes.c_int), ("y0", ctypes.c_int), ("x1", ctypes.c_int),
+                ("y1", ctypes.c_int), ("out_rgba_device", ctypes.c_void_p)]
+
+
 class StageProfile(ctypes.Structure):
     _fields_ = [("primary_ms", ctypes.c_double), ("shadow_ms", ctypes.c_double * 3), ("reflect_ms", ctypes.c_double),
                 ("refract_ms", ctypes.c_double), ("resolve_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
@@ -117,6 +123,8 @@ def lib():
     L.sheen_generate_scene.restype = I
     L.sheen_scene_primary_hits.argtypes = [P, I, I, I, P, P, P]
     L.sheen_scene_profile_stages.argtypes = [P, I, I, I, P, P, ctypes.POINTER(StageProfile)]
+    L.sheen_render_batch.argtypes = [ctypes.POINTER(BatchJob), I, P, ctypes.POINTER(RenderStats)]
+    L.sheen_render_batch.restype = I
     L.sheen_scene_profile_stages.restype = I
     L.sheen_scene_primary_hits.restype = I
     L.sheen_write_png_srgb.argtypes = [ctypes.c_char_p, P, I, I]
@@ -291,6 +299,22 @@ def generate_scene(config: int, seed: int = 1, detail: int = 0, photons: int = 0
     h = ctypes.c_void_p()
     _check(lib().sheen_generate_scene(config, seed, detail, photons, ctypes.byref(h)))
     return OwnedScene(h.value)
+
+
+def render_batch(jobs, stream: int = 0, stats: bool = False):
+    """Render many jobs in one pass of the wavefront queue kernels
+    (sheen_render_batch).  Each job is (scene, width, height, aa, region,
+    out_ptr): a DeviceScene, the frame size, samples per pixel, a pixel
+    rectangle (x0, y0, x1, y1) or None for the whole frame, and the address
+    of a device buffer of width*height float4.  Returns the ray counts when
+    stats is true (then it synchronises)."""
+    arr = (BatchJob * max(len(jobs), 1))()
+    for k, (scene, w, h, aa, region, out_ptr) in enumerate(jobs):
+        x0, y0, x1, y1 = region if region is not None else (0, 0, 0, 0)
+        arr[k] = BatchJob(scene.handle, w, h, aa, x0, y0, x1, y1, out_ptr)
+    st = RenderStats() if stats else None
+    _check(lib().sheen_render_batch(arr, len(jobs), stream, ctypes.byref(st) if st is not None else None))
+    return st.as_dict() if st is not None else None
 
 
 def tune_set(key: str, value: int) -> None:

@@ -190,6 +190,75 @@ int sheen_scene_render_host(SheenDeviceScene h, int W, int H, int aa, float* out
     return rc;
 }
 
+int sheen_render_batch(const SheenBatchJob* jobs, int num_jobs, void* stream, SheenRenderStats* stats) {
+    if (num_jobs < 0 || (num_jobs > 0 && !jobs)) { sheen::set_error("bad job list"); return -1; }
+    const cudaStream_t st = (cudaStream_t)stream;
+    std::vector<sheen::BatchItem> batch;
+    std::vector<std::pair<sheen::DeviceScene*, int>> single;   // (scene, job index)
+    for (int j = 0; j < num_jobs; j++) {
+        const SheenBatchJob& b = jobs[j];
+        auto* s = reinterpret_cast<sheen::DeviceScene*>(b.scene);
+        if (!s) { sheen::set_error("null scene handle in batch"); return -1; }
+        if (b.width <= 0 || b.height <= 0 || b.aa_samples < 1 || b.aa_samples > 64 || !b.out_rgba_device) {
+            sheen::set_error("bad render params in batch");
+            return -1;
+        }
+        sheen::Region rg{b.x0, b.y0, b.x1, b.y1};
+        if (rg.x1 <= rg.x0 || rg.y1 <= rg.y0) rg = sheen::Region{0, 0, b.width, b.height};
+        if (rg.x0 < 0 || rg.y0 < 0 || rg.x1 > b.width || rg.y1 > b.height) {
+            sheen::set_error("bad render region in batch");
+            return -1;
+        }
+        if (s->form == SHEEN_FORM_WAVEFRONT && sheen::wave_pipeline_used(*s))
+            batch.push_back({s, b.width, b.height, b.aa_samples, rg, reinterpret_cast<float4*>(b.out_rgba_device)});
+        else
+            single.push_back({s, j});
+    }
+    unsigned long long* d_tally = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (stats) {
+        e = sheen::dmalloc(&d_tally, 8 * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMemsetAsync(d_tally, 0, 8 * sizeof(unsigned long long), st);
+        if (e == cudaSuccess) e = cudaEventCreate(&ev0);
+        if (e == cudaSuccess) e = cudaEventCreate(&ev1);
+        if (e == cudaSuccess) e = cudaEventRecord(ev0, st);
+    }
+    for (size_t k = 0; k < single.size() && e == cudaSuccess; k++) {
+        const SheenBatchJob& b = jobs[single[k].second];
+        sheen::DeviceScene& s = *single[k].first;
+        sheen::Region rg{b.x0, b.y0, b.x1, b.y1};
+        if (rg.x1 <= rg.x0 || rg.y1 <= rg.y0) rg = sheen::Region{0, 0, b.width, b.height};
+        float4* out = reinterpret_cast<float4*>(b.out_rgba_device);
+        if (s.form == SHEEN_FORM_PLAIN)
+            e = sheen::launch_plain(s, b.width, b.height, b.aa_samples, rg, out, st, false, d_tally);
+        else
+            e = sheen::launch_mega_bvh4(s, b.width, b.height, b.aa_samples, rg, out, st, false, d_tally);
+    }
+    if (e == cudaSuccess) e = sheen::launch_wavefront_batch(batch, st, d_tally);
+    if (e == cudaSuccess && stats) {
+        e = cudaEventRecord(ev1, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        unsigned long long t[8] = {0};
+        if (e == cudaSuccess) e = cudaMemcpy(t, d_tally, sizeof(t), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, ev0, ev1);
+            std::memset(stats, 0, sizeof(*stats));
+            stats->primary_rays = t[0];
+            stats->shadow_rays = t[1];
+            stats->secondary_rays = t[2];
+            stats->total_rays = t[0] + t[1] + t[2];
+            stats->render_ms = ms;
+        }
+    }
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (d_tally) sheen::dfree(d_tally);
+    if (e != cudaSuccess) return fail_cuda(e);
+    return 0;
+}
+
 int sheen_scene_profile_stages(SheenDeviceScene h, int W, int H, int aa, float* out_device, void* stream,
                                SheenStageProfile* prof) {
     auto* s = reinterpret_cast<sheen::DeviceScene*>(h);

@@ -129,6 +129,20 @@ cudaError_t launch_wavefront_scratch(DeviceScene& s, void* scratch, size_t scrat
                                      Region rg, float4* out, cudaStream_t stream, unsigned long long* tally);
 size_t wave_scratch_bytes(int L, long long nsamples);
 bool wave_pipeline_used(const DeviceScene& s);
+
+// One job of a multi-job wavefront launch: region rg of a W x H frame of
+// scene s at aa samples per pixel into the device image `out` (W*H float4).
+struct BatchItem {
+    DeviceScene* s;
+    int W, H, aa;
+    Region rg;
+    float4* out;
+};
+// Every job in one pass of the queue kernels (scenes must be wavefront-form
+// scenes whose frames run on the queue pipeline).  Ray tallies are added to
+// `tally` (device counters 0..2) when not null.
+cudaError_t launch_wavefront_batch(const std::vector<BatchItem>& items, cudaStream_t stream,
+                                   unsigned long long* tally);
 cudaError_t profile_wavefront(DeviceScene& s, int W, int H, int aa, float4* out, cudaStream_t stream,
                               SheenStageProfile* prof);
 

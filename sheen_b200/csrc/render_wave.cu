@@ -32,7 +32,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "dev/integrator.cuh"
 #include "dev/trace_bvh4.cuh"
@@ -62,7 +64,42 @@ struct WaveView {
     int nsamples;          // rw * rh * ns
     float pix_angle;
     int count_rays;
+    // Multi-job launches (the MULTI kernels): the job table.  nsamples is
+    // then the total over all jobs, npix the total of their padded pixels,
+    // and the queues and counters above are shared; every per-frame field
+    // is per job, in jobs[j].V, whose slots and coef point at the job's own
+    // part and whose sample indices are local to the job.
+    const struct JobDesc* jobs;
+    int num_jobs;
+    int npix;
 };
+
+// One region of one frame of one scene in a multi-job launch.
+struct JobDesc {
+    DevScene S;        // the job's scene
+    WaveView V;        // its frame, slots and weights (job-local sample indices)
+    float4* out;       // its image (V.W * V.H float4)
+    int sample_base;   // its first sample in the launch's global sample order
+    int pix_base;      // its first padded pixel in the launch's global pixel order
+};
+
+// Job of a global sample (pix = false) or padded pixel (pix = true) index:
+// the last job whose base is at or below it.
+__device__ __forceinline__ int job_of(const JobDesc* __restrict__ jobs, int n, int i, bool pix) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int b = pix ? jobs[mid].pix_base : jobs[mid].sample_base;
+        if (b <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Shadow queue entries carry their job and the strand flag in one word.
+__device__ __forceinline__ float shadow_tag(int job, bool strands) {
+    return __int_as_float((job << 1) | (strands ? 1 : 0));
+}
 
 __device__ __forceinline__ int seg_base(const WaveView& V, int sample, int seg) {
     return (sample * 3 + seg) * (V.L + 2);
@@ -122,7 +159,8 @@ __device__ __forceinline__ void tally(const WaveView& V, int word, unsigned int 
 // 152-235), the caustic gather last.  Lights skipped before tracing get a
 // zero slot.
 __device__ __forceinline__ void shade_and_queue(const DevScene& S, const WaveView& V, const Hit& h, float3 view,
-                                                float footprint, uint32_t seed, int sample, int seg, bool active) {
+                                                float footprint, uint32_t seed, int sample, int seg, bool active,
+                                                int job) {
     ShadePoint sp;
     int sb = 0;
     if (active) {
@@ -152,7 +190,7 @@ __device__ __forceinline__ void shade_and_queue(const DevScene& S, const WaveVie
         if (want) {
             V.shq[3 * (size_t)q] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
             V.shq[3 * (size_t)q + 1] = make_float4(sr.d.x, sr.d.y, sr.d.z, __int_as_float(sb + 1 + i));
-            V.shq[3 * (size_t)q + 2] = make_float4(contrib.x, contrib.y, contrib.z, strands ? 1.0f : 0.0f);
+            V.shq[3 * (size_t)q + 2] = make_float4(contrib.x, contrib.y, contrib.z, shadow_tag(job, strands));
         }
     }
 }
@@ -169,111 +207,143 @@ __device__ __forceinline__ float3 refract_dir(const DevScene& S, const Hit& gh, 
     return td;
 }
 
+// One primary sample: local index i of the frame V (gi: its global index in
+// a multi-job launch, which the secondary queues carry).
 template <int F>
-__global__ void __launch_bounds__(128, 8) wave_primary(DevScene S, WaveView V) {
+__device__ __forceinline__ void primary_item(const DevScene& S, const WaveView& V, int i, int gi, bool active,
+                                             int job, Counters& c) {
     using T = FastTracer<false, F>;
+    int x = 0, y = 0, s = 0;
+    if (active) {
+        sample_pixel(V, i, x, y, s);
+        active = sample_valid(V, x, y);
+    }
+    Hit rec;
+    Ray ray;
+    bool hit = false;
+    uint32_t seed = 0;
+    if (active) {
+        float pix;
+        ray = camera_ray(S.cam, x, y, s, V.ns, V.W, V.H, pix);
+        seed = sample_seed(x, y, s);
+        hit = T::closest(S, ray, rec, c);
+    }
+    tally(V, kRaysPrimary, active ? 1u : 0u);
+    float w = 0.0f, gtr = 0.0f;
+    if (active) {
+        if (!hit) {
+            // sky: the segment's light and caustic slots are summed by the
+            // resolve too, so they are cleared here
+            const int sb = seg_base(V, i, 0);
+            put_slot(V, sb, sky(ray.d));
+            for (int l = 0; l < V.L + 1; l++) put_slot(V, sb + 1 + l, f3(0.0f, 0.0f, 0.0f));
+            V.coef[3 * (size_t)i] = 1.0f;
+            V.coef[3 * (size_t)i + 1] = 0.0f;
+            V.coef[3 * (size_t)i + 2] = 0.0f;
+        } else {
+            const Material& pm = S.materials[rec.mat];
+            w = pm.reflect > 0.0f ? fminf(pm.reflect, 1.0f) : 0.0f;
+            gtr = transmission_at(S, pm, rec.uv);
+            const float g = gtr > 0.0f ? 1.0f - fminf(gtr, 1.0f) : 1.0f;
+            V.coef[3 * (size_t)i] = (1.0f - w) * g;
+            V.coef[3 * (size_t)i + 1] = w * g;
+            V.coef[3 * (size_t)i + 2] = 0.0f;   // set by the refraction stage
+        }
+    }
+    shade_and_queue(S, V, rec, -ray.d, rec.t * V.pix_angle, seed, i, 0, active && hit, job);
+    // mirror ray (render_kernel.cu:674-680)
+    const bool want_r = active && hit && w > 0.0f;
+    const unsigned int qr = warp_append(&V.ctr[kReflCount], want_r);
+    if (want_r) {
+        const float3 rd = normalize(ray.d - rec.n * (2.0f * dot(ray.d, rec.n)));
+        const float3 ro = rec.p + rec.n * 0.002f;
+        V.rq[2 * (size_t)qr] = make_float4(ro.x, ro.y, ro.z, __int_as_float(gi));
+        V.rq[2 * (size_t)qr + 1] = make_float4(rd.x, rd.y, rd.z, 0.0f);
+    }
+    // first refraction face (render_kernel.cu:749-765 with b = 0)
+    const bool want_t = active && hit && gtr > 0.0f;
+    float wt = 1.0f;
+    float3 td = f3(0.0f, 0.0f, 0.0f);
+    if (want_t) td = refract_dir(S, rec, ray.d, true, wt);
+    const unsigned int qt = warp_append(&V.ctr[kRefrCount], want_t);
+    if (want_t) {
+        const float3 to = rec.p + td * 0.002f;
+        V.tq[2 * (size_t)qt] = make_float4(to.x, to.y, to.z, __int_as_float(gi));
+        V.tq[2 * (size_t)qt + 1] = make_float4(td.x, td.y, td.z, wt);
+    }
+}
+
+// MULTI: samples of every job in the launch's table (V0.jobs), one claim
+// counter over their global order; otherwise the single frame S0 / V0.
+template <int F, bool MULTI>
+__global__ void __launch_bounds__(128, 8) wave_primary(DevScene S0, WaveView V0) {
     Counters c;
     while (true) {
-        const int base = claim_batch(&V.ctr[kPrimHead]);
-        if (base >= V.nsamples) break;
-        const int i = base + (threadIdx.x & 31);
-        int x = 0, y = 0, s = 0;
-        bool active = i < V.nsamples;
-        if (active) {
-            sample_pixel(V, i, x, y, s);
-            active = sample_valid(V, x, y);
-        }
-        Hit rec;
-        Ray ray;
-        bool hit = false;
-        uint32_t seed = 0;
-        if (active) {
-            float pix;
-            ray = camera_ray(S.cam, x, y, s, V.ns, V.W, V.H, pix);
-            seed = sample_seed(x, y, s);
-            hit = T::closest(S, ray, rec, c);
-        }
-        tally(V, kRaysPrimary, active ? 1u : 0u);
-        float w = 0.0f, gtr = 0.0f;
-        if (active) {
-            if (!hit) {
-                // sky: the segment's light and caustic slots are summed by the
-                // resolve too, so they are cleared here
-                const int sb = seg_base(V, i, 0);
-                put_slot(V, sb, sky(ray.d));
-                for (int l = 0; l < V.L + 1; l++) put_slot(V, sb + 1 + l, f3(0.0f, 0.0f, 0.0f));
-                V.coef[3 * (size_t)i] = 1.0f;
-                V.coef[3 * (size_t)i + 1] = 0.0f;
-                V.coef[3 * (size_t)i + 2] = 0.0f;
-            } else {
-                const Material& pm = S.materials[rec.mat];
-                w = pm.reflect > 0.0f ? fminf(pm.reflect, 1.0f) : 0.0f;
-                gtr = transmission_at(S, pm, rec.uv);
-                const float g = gtr > 0.0f ? 1.0f - fminf(gtr, 1.0f) : 1.0f;
-                V.coef[3 * (size_t)i] = (1.0f - w) * g;
-                V.coef[3 * (size_t)i + 1] = w * g;
-                V.coef[3 * (size_t)i + 2] = 0.0f;   // set by the refraction stage
-            }
-        }
-        shade_and_queue(S, V, rec, -ray.d, rec.t * V.pix_angle, seed, i, 0, active && hit);
-        // mirror ray (render_kernel.cu:674-680)
-        const bool want_r = active && hit && w > 0.0f;
-        const unsigned int qr = warp_append(&V.ctr[kReflCount], want_r);
-        if (want_r) {
-            const float3 rd = normalize(ray.d - rec.n * (2.0f * dot(ray.d, rec.n)));
-            const float3 ro = rec.p + rec.n * 0.002f;
-            V.rq[2 * (size_t)qr] = make_float4(ro.x, ro.y, ro.z, __int_as_float(i));
-            V.rq[2 * (size_t)qr + 1] = make_float4(rd.x, rd.y, rd.z, 0.0f);
-        }
-        // first refraction face (render_kernel.cu:749-765 with b = 0)
-        const bool want_t = active && hit && gtr > 0.0f;
-        float wt = 1.0f;
-        float3 td = f3(0.0f, 0.0f, 0.0f);
-        if (want_t) td = refract_dir(S, rec, ray.d, true, wt);
-        const unsigned int qt = warp_append(&V.ctr[kRefrCount], want_t);
-        if (want_t) {
-            const float3 to = rec.p + td * 0.002f;
-            V.tq[2 * (size_t)qt] = make_float4(to.x, to.y, to.z, __int_as_float(i));
-            V.tq[2 * (size_t)qt + 1] = make_float4(td.x, td.y, td.z, wt);
+        const int base = claim_batch(&V0.ctr[kPrimHead]);
+        if (base >= V0.nsamples) break;
+        const int gi = base + (threadIdx.x & 31);
+        const bool active = gi < V0.nsamples;
+        if constexpr (MULTI) {
+            const int j = job_of(V0.jobs, V0.num_jobs, active ? gi : V0.nsamples - 1, false);
+            const JobDesc& J = V0.jobs[j];
+            primary_item<F>(J.S, J.V, gi - J.sample_base, gi, active, j, c);
+        } else {
+            primary_item<F>(S0, V0, gi, gi, active, 0, c);
         }
     }
 }
 
+// One queued shadow ray (entry a, b, cc) of frame S / V: up to three
+// opaque-set queries with glass passes, strand transmittance; writes its
+// light slot.  Returns the queries issued.
 template <int F>
-__global__ void __launch_bounds__(128) wave_shadow(DevScene S, WaveView V) {
+__device__ __forceinline__ unsigned int shadow_item(const DevScene& S, const WaveView& V, float4 a, float4 b, float4 cc,
+                                                    Counters& c) {
     using T = FastTracer<false, F>;
+    unsigned int rays = 0;
+    Ray r;
+    r.o = f3(a.x, a.y, a.z);
+    r.d = f3(b.x, b.y, b.z);
+    r.tmin = 0.001f;
+    r.tmax = a.w;
+    const Ray first = r;
+    bool blocked = false;
+    for (int pass = 0; pass < 3; pass++) {
+        rays++;
+        ShadowHit sh;
+        const int res = T::shadow(S, r, true, sh, c);
+        if (res == kClear) break;
+        if (res == kBlocked) { blocked = true; break; }
+        r.o = sh.p + r.d * 0.002f;
+    }
+    float3 contrib = f3(0.0f, 0.0f, 0.0f);
+    if (!blocked) {
+        contrib = f3(cc.x, cc.y, cc.z);
+        if (__float_as_int(cc.w) & 1) contrib = contrib * expf(-T::strand_depth(S, first, c));
+    }
+    put_slot(V, __float_as_int(b.w), contrib);
+    return rays;
+}
+
+template <int F, bool MULTI>
+__global__ void __launch_bounds__(128) wave_shadow(DevScene S0, WaveView V0) {
     Counters c;
-    const unsigned int n = V.ctr[kShadowCount];
+    const unsigned int n = V0.ctr[kShadowCount];
     while (true) {
-        const int base = claim_batch(&V.ctr[kShadowHead]);
+        const int base = claim_batch(&V0.ctr[kShadowHead]);
         if (base >= (int)n) break;
         const int q = base + (threadIdx.x & 31);
         unsigned int rays = 0;
         if (q < (int)n) {
-            const float4 a = V.shq[3 * (size_t)q], b = V.shq[3 * (size_t)q + 1], cc = V.shq[3 * (size_t)q + 2];
-            Ray r;
-            r.o = f3(a.x, a.y, a.z);
-            r.d = f3(b.x, b.y, b.z);
-            r.tmin = 0.001f;
-            r.tmax = a.w;
-            const Ray first = r;
-            bool blocked = false;
-            for (int pass = 0; pass < 3; pass++) {
-                rays++;
-                ShadowHit sh;
-                const int res = T::shadow(S, r, true, sh, c);
-                if (res == kClear) break;
-                if (res == kBlocked) { blocked = true; break; }
-                r.o = sh.p + r.d * 0.002f;
+            const float4 a = V0.shq[3 * (size_t)q], b = V0.shq[3 * (size_t)q + 1], cc = V0.shq[3 * (size_t)q + 2];
+            if constexpr (MULTI) {
+                const JobDesc& J = V0.jobs[__float_as_int(cc.w) >> 1];
+                rays = shadow_item<F>(J.S, J.V, a, b, cc, c);
+            } else {
+                rays = shadow_item<F>(S0, V0, a, b, cc, c);
             }
-            float3 contrib = f3(0.0f, 0.0f, 0.0f);
-            if (!blocked) {
-                contrib = f3(cc.x, cc.y, cc.z);
-                if (cc.w != 0.0f) contrib = contrib * expf(-T::strand_depth(S, first, c));
-            }
-            put_slot(V, __float_as_int(b.w), contrib);
         }
-        tally(V, kRaysShadow, rays);
+        tally(V0, kRaysShadow, rays);
     }
 }
 
@@ -295,8 +365,8 @@ __global__ void __launch_bounds__(128) wave_shadow(DevScene S, WaveView V) {
 // local memory, whose scattered stores fill L1 with 32-byte sectors carrying
 // 4 useful bytes; the entry distances (closest-hit walks of the passable set
 // only) stay in local memory.  24 KB per 128-thread block.
-template <int F, bool SMEM_STACK>
-__global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S, WaveView V, int refill_min) {
+template <int F, bool SMEM_STACK, bool MULTI>
+__global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveView V0, int refill_min) {
     using T = FastTracer<false, F>;
     constexpr unsigned int kFull = 0xffffffffu;
     constexpr uint32_t kLeafBit = 0x80000000u;
@@ -305,8 +375,18 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S, WaveVie
     // site (a fresh ray, or a walk that has ended)
     enum { kIdle = 0, kWalkPass, kWalkBlock, kFresh, kEndPass, kEndBlock };
     Counters c;
-    const unsigned int n = V.ctr[kShadowCount];
+    const unsigned int n = V0.ctr[kShadowCount];
     const int lane = threadIdx.x & 31;
+    // the lane's job (MULTI): its scene and frame
+    int job = 0;
+    auto scene = [&]() -> const DevScene& {
+        if constexpr (MULTI) return V0.jobs[job].S;
+        else return S0;
+    };
+    auto view = [&]() -> const WaveView& {
+        if constexpr (MULTI) return V0.jobs[job].V;
+        else return V0;
+    };
 
     // the lane's ray: q holds its current origin and direction
     QRay q{};
@@ -340,21 +420,22 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S, WaveVie
         if (!exhausted && (idle == kFull || __popc(idle) >= refill_min)) {
             const unsigned int k = (unsigned int)__popc(idle);
             unsigned int b = 0;
-            if (lane == 0) b = atomicAdd(&V.ctr[kShadowHead], k);
+            if (lane == 0) b = atomicAdd(&V0.ctr[kShadowHead], k);
             b = __shfl_sync(kFull, b, 0);
             if (b + k >= n) exhausted = true;
             if (state == kIdle) {
                 const unsigned int item = b + (unsigned int)__popc(idle & ((1u << lane) - 1u));
                 if (item < n) {
-                    const float4 a = V.shq[3 * (size_t)item], bb = V.shq[3 * (size_t)item + 1],
-                                 c4 = V.shq[3 * (size_t)item + 2];
+                    const float4 a = V0.shq[3 * (size_t)item], bb = V0.shq[3 * (size_t)item + 1],
+                                 c4 = V0.shq[3 * (size_t)item + 2];
                     q.o = f3(a.x, a.y, a.z);
                     q.d = f3(bb.x, bb.y, bb.z);
                     o_first = q.o;
                     tmax = a.w;
                     slot = __float_as_int(bb.w);
                     cc = f3(c4.x, c4.y, c4.z);
-                    strands = c4.w != 0.0f;
+                    strands = (__float_as_int(c4.w) & 1) != 0;
+                    job = __float_as_int(c4.w) >> 1;
                     pass = 0;
                     state = kFresh;
                 }
@@ -368,11 +449,11 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S, WaveVie
             r.o = q.o; r.d = q.d; r.tmin = 0.001f; r.tmax = tmax;
             if (state == kFresh) {
                 res = -2;   // start a pass
-            } else if (state == kEndPass && S.q_block.nodes) {
+            } else if (state == kEndPass && scene().q_block.nodes) {
                 // closest passable hit found; now any blocking hit strictly before it
                 pass_tri = wbest; tp = t_best; up = wu; vp = wv;
                 state = kWalkBlock; block_after_pass = true;
-                wn = S.q_block.nodes; wt = S.q_block.tris;
+                wn = scene().q_block.nodes; wt = scene().q_block.tris;
                 entry = 0; sp = 0; wbest = -1; t_best = tp;
                 res = -3;   // keep walking
             } else {
@@ -380,10 +461,10 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S, WaveVie
                 res = (state == kEndBlock && wbest >= 0) ? kBlocked : kClear;
                 if (res == kClear && (state == kEndPass || block_after_pass) && pass_tri >= 0) {
                     Hit h;
-                    tri_finish(r, S.tris[pass_tri], tp, up, vp, h);
-                    res = classify_shadow_hit(S, h, true, sh);
+                    tri_finish(r, scene().tris[pass_tri], tp, up, vp, h);
+                    res = classify_shadow_hit(scene(), h, true, sh);
                 }
-                if (res == kClear) res = T::shadow_post_mesh(S, r, true, sh, c);
+                if (res == kClear) res = T::shadow_post_mesh(scene(), r, true, sh, c);
             }
             // settle: pass results and pass starts until the lane walks a
             // mesh or its ray is finished
@@ -391,22 +472,22 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S, WaveVie
                 if (res == -2) {
                     rays++;
                     r.o = q.o;
-                    res = T::shadow_pre_mesh(S, r, true, sh, c);
+                    res = T::shadow_pre_mesh(scene(), r, true, sh, c);
                     if (res >= 0) continue;
-                    if ((F & kCatMesh) && S.q_all.nodes) {
+                    if ((F & kCatMesh) && scene().q_all.nodes) {
                         q = make_qray(r);
                         pass_tri = -1;
                         entry = 0; sp = 0; wbest = -1; t_best = tmax;
-                        if (S.q_pass.nodes) {
+                        if (scene().q_pass.nodes) {
                             state = kWalkPass;
-                            wn = S.q_pass.nodes; wt = S.q_pass.tris;
+                            wn = scene().q_pass.nodes; wt = scene().q_pass.tris;
                         } else {
                             state = kWalkBlock; block_after_pass = false;
-                            wn = S.q_all.nodes; wt = S.q_all.tris;
+                            wn = scene().q_all.nodes; wt = scene().q_all.tris;
                         }
                         break;
                     }
-                    res = T::shadow_post_mesh(S, r, true, sh, c);
+                    res = T::shadow_post_mesh(scene(), r, true, sh, c);
                     continue;
                 }
                 if (res == kPass && ++pass < 3) {   // through the glass: next pass
@@ -421,10 +502,10 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S, WaveVie
                     if (strands) {
                         Ray first;
                         first.o = o_first; first.d = q.d; first.tmin = 0.001f; first.tmax = tmax;
-                        contrib = contrib * expf(-T::strand_depth(S, first, c));
+                        contrib = contrib * expf(-T::strand_depth(scene(), first, c));
                     }
                 }
-                put_slot(V, slot, contrib);
+                put_slot(view(), slot, contrib);
                 state = kIdle;
                 break;
             }
@@ -509,104 +590,131 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S, WaveVie
             if (ended) state = state == kWalkPass ? kEndPass : kEndBlock;
         }
     }
-    tally(V, kRaysShadow, rays);
+    tally(V0, kRaysShadow, rays);
 }
 
+// One mirror ray (entry a, b; i = its job-local sample) of frame S / V.
 template <int F>
-__global__ void __launch_bounds__(128, 8) wave_reflect(DevScene S, WaveView V) {
+__device__ __forceinline__ void reflect_item(const DevScene& S, const WaveView& V, float4 a, float4 b, int i,
+                                             bool active, int job, Counters& c) {
     using T = FastTracer<false, F>;
+    Ray rr;
+    Hit rh;
+    bool rhit = false;
+    uint32_t seed = 0;
+    if (active) {
+        rr.o = f3(a.x, a.y, a.z);
+        rr.d = f3(b.x, b.y, b.z);
+        rr.tmin = 0.001f;
+        rr.tmax = 1.0e10f;
+        int x, y, s;
+        sample_pixel(V, i, x, y, s);
+        seed = sample_seed(x, y, s);
+        rhit = T::closest(S, rr, rh, c);
+        if (!rhit) {
+            const int sb = seg_base(V, i, 1);
+            put_slot(V, sb, sky(rr.d));
+            for (int l = 0; l < V.L + 1; l++) put_slot(V, sb + 1 + l, f3(0.0f, 0.0f, 0.0f));
+        }
+    }
+    tally(V, kRaysSecondary, active ? 1u : 0u);
+    shade_and_queue(S, V, rh, -rr.d, rh.t * V.pix_angle, seed, i, 1, active && rhit, job);
+}
+
+template <int F, bool MULTI>
+__global__ void __launch_bounds__(128, 8) wave_reflect(DevScene S0, WaveView V0) {
     Counters c;
-    const unsigned int n = V.ctr[kReflCount];
+    const unsigned int n = V0.ctr[kReflCount];
     while (true) {
-        const int base = claim_batch(&V.ctr[kReflHead]);
+        const int base = claim_batch(&V0.ctr[kReflHead]);
         if (base >= (int)n) break;
         const int q = base + (threadIdx.x & 31);
         const bool active = q < (int)n;
-        Ray rr;
-        int i = 0;
-        Hit rh;
-        bool rhit = false;
-        uint32_t seed = 0;
-        if (active) {
-            const float4 a = V.rq[2 * (size_t)q], b = V.rq[2 * (size_t)q + 1];
-            i = __float_as_int(a.w);
-            rr.o = f3(a.x, a.y, a.z);
-            rr.d = f3(b.x, b.y, b.z);
-            rr.tmin = 0.001f;
-            rr.tmax = 1.0e10f;
-            int x, y, s;
-            sample_pixel(V, i, x, y, s);
-            seed = sample_seed(x, y, s);
-            rhit = T::closest(S, rr, rh, c);
-            if (!rhit) {
-                const int sb = seg_base(V, i, 1);
-                put_slot(V, sb, sky(rr.d));
-                for (int l = 0; l < V.L + 1; l++) put_slot(V, sb + 1 + l, f3(0.0f, 0.0f, 0.0f));
-            }
+        float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b = a;
+        if (active) { a = V0.rq[2 * (size_t)q]; b = V0.rq[2 * (size_t)q + 1]; }
+        const int gi = __float_as_int(a.w);
+        if constexpr (MULTI) {
+            const int j = job_of(V0.jobs, V0.num_jobs, gi, false);
+            const JobDesc& J = V0.jobs[j];
+            reflect_item<F>(J.S, J.V, a, b, gi - J.sample_base, active, j, c);
+        } else {
+            reflect_item<F>(S0, V0, a, b, gi, active, 0, c);
         }
-        tally(V, kRaysSecondary, active ? 1u : 0u);
-        shade_and_queue(S, V, rh, -rr.d, rh.t * V.pix_angle, seed, i, 1, active && rhit);
     }
 }
 
+// One refracted ray (entry a, b; i = its job-local sample) of frame S / V:
+// up to three faces, then shading (or sky).
 template <int F>
-__global__ void __launch_bounds__(128, 8) wave_refract(DevScene S, WaveView V) {
+__device__ __forceinline__ void refract_item(const DevScene& S, const WaveView& V, float4 a, float4 b, int i,
+                                             bool active, int job, Counters& c) {
     using T = FastTracer<false, F>;
-    Counters c;
-    const unsigned int n = V.ctr[kRefrCount];
-    while (true) {
-        const int base = claim_batch(&V.ctr[kRefrHead]);
-        if (base >= (int)n) break;
-        const int q = base + (threadIdx.x & 31);
-        const bool active = q < (int)n;
-        int i = 0;
-        Hit nh;
-        bool shade = false;
-        uint32_t seed = 0;
-        float3 td = f3(0.0f, 0.0f, 0.0f);
-        unsigned int rays = 0;
-        if (active) {
-            const float4 a = V.tq[2 * (size_t)q], b = V.tq[2 * (size_t)q + 1];
-            i = __float_as_int(a.w);
-            int x, y, s;
-            sample_pixel(V, i, x, y, s);
-            seed = sample_seed(x, y, s);
-            Ray gr;
-            gr.o = f3(a.x, a.y, a.z);
-            gr.d = f3(b.x, b.y, b.z);
-            gr.tmin = 0.001f;
-            gr.tmax = 1.0e10f;
-            float w = b.w;
-            bool entering = true;
-            float cT = 0.0f;
-            const int sb = seg_base(V, i, 2);
-            // render_kernel.cu:749-803: faces b = 0..2 (the first direction was
-            // computed by the primary stage)
-            for (int f = 0; f < 3; f++) {
-                td = gr.d;
-                rays++;
-                if (!T::closest(S, gr, nh, c)) {
-                    put_slot(V, sb, sky(td));
-                    for (int l = 0; l < V.L + 1; l++) put_slot(V, sb + 1 + l, f3(0.0f, 0.0f, 0.0f));
-                    cT = w;
-                    break;
-                }
-                if (transmission_at(S, S.materials[nh.mat], nh.uv) > 0.0f) {
-                    entering = !entering;
-                    if (f == 2) break;   // the reference's loop ends here: no contribution
-                    const float3 nd = refract_dir(S, nh, gr.d, entering, w);
-                    gr.o = nh.p + nd * 0.002f;
-                    gr.d = nd;
-                    continue;
-                }
-                shade = true;
+    Hit nh;
+    bool shade = false;
+    uint32_t seed = 0;
+    float3 td = f3(0.0f, 0.0f, 0.0f);
+    unsigned int rays = 0;
+    if (active) {
+        int x, y, s;
+        sample_pixel(V, i, x, y, s);
+        seed = sample_seed(x, y, s);
+        Ray gr;
+        gr.o = f3(a.x, a.y, a.z);
+        gr.d = f3(b.x, b.y, b.z);
+        gr.tmin = 0.001f;
+        gr.tmax = 1.0e10f;
+        float w = b.w;
+        bool entering = true;
+        float cT = 0.0f;
+        const int sb = seg_base(V, i, 2);
+        // render_kernel.cu:749-803: faces b = 0..2 (the first direction was
+        // computed by the primary stage)
+        for (int f = 0; f < 3; f++) {
+            td = gr.d;
+            rays++;
+            if (!T::closest(S, gr, nh, c)) {
+                put_slot(V, sb, sky(td));
+                for (int l = 0; l < V.L + 1; l++) put_slot(V, sb + 1 + l, f3(0.0f, 0.0f, 0.0f));
                 cT = w;
                 break;
             }
-            V.coef[3 * (size_t)i + 2] = cT;
+            if (transmission_at(S, S.materials[nh.mat], nh.uv) > 0.0f) {
+                entering = !entering;
+                if (f == 2) break;   // the reference's loop ends here: no contribution
+                const float3 nd = refract_dir(S, nh, gr.d, entering, w);
+                gr.o = nh.p + nd * 0.002f;
+                gr.d = nd;
+                continue;
+            }
+            shade = true;
+            cT = w;
+            break;
         }
-        tally(V, kRaysSecondary, rays);
-        shade_and_queue(S, V, nh, -td, nh.t * V.pix_angle, seed, i, 2, active && shade);
+        V.coef[3 * (size_t)i + 2] = cT;
+    }
+    tally(V, kRaysSecondary, rays);
+    shade_and_queue(S, V, nh, -td, nh.t * V.pix_angle, seed, i, 2, active && shade, job);
+}
+
+template <int F, bool MULTI>
+__global__ void __launch_bounds__(128, 8) wave_refract(DevScene S0, WaveView V0) {
+    Counters c;
+    const unsigned int n = V0.ctr[kRefrCount];
+    while (true) {
+        const int base = claim_batch(&V0.ctr[kRefrHead]);
+        if (base >= (int)n) break;
+        const int q = base + (threadIdx.x & 31);
+        const bool active = q < (int)n;
+        float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b = a;
+        if (active) { a = V0.tq[2 * (size_t)q]; b = V0.tq[2 * (size_t)q + 1]; }
+        const int gi = __float_as_int(a.w);
+        if constexpr (MULTI) {
+            const int j = job_of(V0.jobs, V0.num_jobs, gi, false);
+            const JobDesc& J = V0.jobs[j];
+            refract_item<F>(J.S, J.V, a, b, gi - J.sample_base, active, j, c);
+        } else {
+            refract_item<F>(S0, V0, a, b, gi, active, 0, c);
+        }
     }
 }
 
@@ -620,11 +728,10 @@ __device__ __forceinline__ float3 segment_value(const WaveView& V, int sb) {
     return v + get_slot(V, sb + V.L + 1);
 }
 
-__global__ void wave_resolve(WaveView V, float4* __restrict__ out) {
-    // p walks the padded 16x8-tile order of sample_pixel; padding pixels
-    // fall outside the region and are skipped below.
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= V.nsamples / V.ns) return;
+// Pixel p (padded tile order of sample_pixel) of frame V: every sample's
+// color from its slots, averaged.  Padding pixels fall outside the region
+// and are skipped.
+__device__ __forceinline__ void resolve_item(const WaveView& V, float4* __restrict__ out, int p) {
     int x, y, s;
     sample_pixel(V, p * V.ns, x, y, s);
     if (!sample_valid(V, x, y)) return;
@@ -639,6 +746,19 @@ __global__ void wave_resolve(WaveView V, float4* __restrict__ out) {
     }
     const float inv = 1.0f / float(V.ns);
     out[(size_t)y * V.W + x] = make_float4(acc.x * inv, acc.y * inv, acc.z * inv, 1.0f);
+}
+
+template <bool MULTI>
+__global__ void wave_resolve(WaveView V0, float4* __restrict__ out0) {
+    const int gp = blockIdx.x * blockDim.x + threadIdx.x;
+    if constexpr (MULTI) {
+        if (gp >= V0.npix) return;
+        const JobDesc& J = V0.jobs[job_of(V0.jobs, V0.num_jobs, gp, true)];
+        resolve_item(J.V, J.out, gp - J.pix_base);
+    } else {
+        if (gp >= V0.nsamples / V0.ns) return;
+        resolve_item(V0, out0, gp);
+    }
 }
 
 // Copies the three ray counters into snap[3*k .. 3*k+2] (stage profiling).
@@ -743,35 +863,36 @@ static int shadow_grid(K kernel, int sms, int per_sm) {
     return per_sm > 0 ? std::min(full, sms * per_sm) : full;
 }
 
-// The queue pipeline of one frame for category set F.  Stage profiling
-// (not inside a graph): `ev` gets 8 events recorded at the stage
-// boundaries (before primary, after primary, shadow, reflect, shadow,
-// refract, shadow, resolve) and `snap` the ray counters after each of the
-// 7 kernels (3 words each).
-template <int F>
-static cudaError_t run_pipeline(const DeviceScene& s, const dev::WaveView& V, int npad, float4* out,
+// The queue pipeline for category set F: one frame (S0 / V), or with MULTI
+// every job of V.jobs (S0 unused; npad is then the total padded pixels).
+// Stage profiling (not inside a graph): `ev` gets 8 events recorded at the
+// stage boundaries (before primary, after primary, shadow, reflect, shadow,
+// refract, shadow, resolve) and `snap` the ray counters after each of the 7
+// kernels (3 words each).
+template <int F, bool MULTI = false>
+static cudaError_t run_pipeline(const dev::DevScene& S0, const dev::WaveView& V, int npad, float4* out,
                                 cudaStream_t stream, unsigned long long* tally, cudaEvent_t* ev = nullptr,
                                 unsigned int* snap = nullptr) {
     static int g_primary = 0, g_reflect = 0, g_refract = 0;
     const int sms = device_sms();
     if (!g_primary) {
-        g_primary = persistent_grid(dev::wave_primary<F>, sms);
-        g_reflect = persistent_grid(dev::wave_reflect<F>, sms);
-        g_refract = persistent_grid(dev::wave_refract<F>, sms);
+        g_primary = persistent_grid(dev::wave_primary<F, MULTI>, sms);
+        g_reflect = persistent_grid(dev::wave_reflect<F, MULTI>, sms);
+        g_refract = persistent_grid(dev::wave_refract<F, MULTI>, sms);
     }
     const Tuning tu = tuning();
     const bool refill = tu.shadow_kernel == 1;
     const bool smem = tu.shadow_stack == 1;
-    const int g_shadow = !refill ? shadow_grid(dev::wave_shadow<F>, sms, tu.shadow_blocks_per_sm)
-                         : smem  ? shadow_grid(dev::wave_shadow_refill<F, true>, sms, tu.shadow_blocks_per_sm)
-                                 : shadow_grid(dev::wave_shadow_refill<F, false>, sms, tu.shadow_blocks_per_sm);
+    const int g_shadow = !refill ? shadow_grid(dev::wave_shadow<F, MULTI>, sms, tu.shadow_blocks_per_sm)
+                         : smem  ? shadow_grid(dev::wave_shadow_refill<F, true, MULTI>, sms, tu.shadow_blocks_per_sm)
+                                 : shadow_grid(dev::wave_shadow_refill<F, false, MULTI>, sms, tu.shadow_blocks_per_sm);
     auto shadow = [&]() {
         if (!refill)
-            dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
+            dev::wave_shadow<F, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V);
         else if (smem)
-            dev::wave_shadow_refill<F, true><<<g_shadow, 128, 0, stream>>>(s.view, V, tu.refill_min);
+            dev::wave_shadow_refill<F, true, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V, tu.refill_min);
         else
-            dev::wave_shadow_refill<F, false><<<g_shadow, 128, 0, stream>>>(s.view, V, tu.refill_min);
+            dev::wave_shadow_refill<F, false, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V, tu.refill_min);
     };
     int mark = 0;
     auto stage_end = [&]() {
@@ -782,21 +903,21 @@ static cudaError_t run_pipeline(const DeviceScene& s, const dev::WaveView& V, in
     cudaError_t e;
     if ((e = cudaMemsetAsync(V.ctr, 0, dev::kCounterWords * sizeof(unsigned int), stream)) != cudaSuccess) return e;
     if (ev) cudaEventRecord(ev[0], stream);
-    dev::wave_primary<F><<<g_primary, 128, 0, stream>>>(s.view, V);
+    dev::wave_primary<F, MULTI><<<g_primary, 128, 0, stream>>>(S0, V);
     stage_end();
     shadow();
     stage_end();
     if ((e = cudaMemsetAsync(&V.ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
-    dev::wave_reflect<F><<<g_reflect, 128, 0, stream>>>(s.view, V);
+    dev::wave_reflect<F, MULTI><<<g_reflect, 128, 0, stream>>>(S0, V);
     stage_end();
     shadow();
     stage_end();
     if ((e = cudaMemsetAsync(&V.ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
-    dev::wave_refract<F><<<g_refract, 128, 0, stream>>>(s.view, V);
+    dev::wave_refract<F, MULTI><<<g_refract, 128, 0, stream>>>(S0, V);
     stage_end();
     shadow();
     stage_end();
-    dev::wave_resolve<<<(npad + 127) / 128, 128, 0, stream>>>(V, out);
+    if (npad > 0) dev::wave_resolve<MULTI><<<(npad + 127) / 128, 128, 0, stream>>>(V, out);
     if (ev) cudaEventRecord(ev[7], stream);
     if (tally) dev::wave_tally_out<<<1, 1, 0, stream>>>(V, tally);
     return cudaGetLastError();
@@ -870,6 +991,9 @@ static dev::WaveView make_view(const DeviceScene& s, const Wave& w, int W, int H
     }
     V.pix_angle = 2.0f * tan_x / (float)W;
     V.count_rays = 1;
+    V.jobs = nullptr;
+    V.num_jobs = 0;
+    V.npix = 0;
     return V;
 }
 
@@ -900,8 +1024,8 @@ cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, fl
             (e = cudaStreamCreateWithFlags(&w->capture_stream, cudaStreamNonBlocking)) != cudaSuccess)
             return e;
         if ((e = cudaStreamBeginCapture(w->capture_stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
-        cudaError_t le = simple ? run_pipeline<dev::kCatSimple>(s, V, npad, out, w->capture_stream, s.d_tally)
-                                : run_pipeline<dev::kCatAll>(s, V, npad, out, w->capture_stream, s.d_tally);
+        cudaError_t le = simple ? run_pipeline<dev::kCatSimple>(s.view, V, npad, out, w->capture_stream, s.d_tally)
+                                : run_pipeline<dev::kCatAll>(s.view, V, npad, out, w->capture_stream, s.d_tally);
         cudaGraph_t graph = nullptr;
         e = cudaStreamEndCapture(w->capture_stream, &graph);
         if (le != cudaSuccess) { if (graph) cudaGraphDestroy(graph); return le; }
@@ -915,6 +1039,101 @@ cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, fl
 }
 
 bool wave_pipeline_used(const DeviceScene& s) { return wave_supported(s); }
+
+// Many frames, regions and scenes in one pass of the queue kernels: every
+// stage is one persistent launch over the samples of all jobs, whose work
+// the blocks claim from the same counters, so cheap jobs (sky, a small
+// tile) and expensive ones (glass, a dense mesh) share the SMs.  Each job
+// gets its own part of the slot and weight arrays (its light count decides
+// its slot stride); the ray queues are shared and their entries carry the
+// job.  Jobs run under the kernel variant their scene would use alone
+// (scenes of triangles, spheres and planes only, or every category), one
+// pass per variant, so every sample computes bit for bit what a single-frame
+// render computes: the compiler rounds the two variants' shading arithmetic
+// differently.  Scratch comes from the library's pool, ordered on `stream`.
+template <int F>
+static cudaError_t batch_pass(const std::vector<BatchItem>& items, cudaStream_t stream, unsigned long long* tally) {
+    const int n = (int)items.size();
+    if (n == 0) return cudaSuccess;
+    long long total_samples = 0, total_pix = 0, slot_floats = 0, shadow_entries = 0;
+    for (const BatchItem& it : items) {
+        const long long npad = region_padded(it.rg), ns = clamp_spp(it.aa);
+        const int L = it.s->view.num_lights;
+        total_samples += npad * ns;
+        total_pix += npad;
+        slot_floats += npad * ns * 3 * (L + 2) * 3;
+        shadow_entries += npad * ns * std::max(L, 1);
+    }
+    if (total_samples > (1ll << 30) || slot_floats > (1ll << 40)) return cudaErrorInvalidValue;
+    const size_t b_jobs = align256((size_t)n * sizeof(dev::JobDesc));
+    const size_t b_slots = align256((size_t)slot_floats * sizeof(float));
+    const size_t b_coef = align256((size_t)total_samples * 3 * sizeof(float));
+    const size_t b_shq = align256((size_t)shadow_entries * 3 * sizeof(float4));
+    const size_t b_rq = align256((size_t)total_samples * 2 * sizeof(float4));
+    const size_t b_ctr = align256(dev::kCounterWords * sizeof(unsigned int));
+    char* block = nullptr;
+    cudaError_t e = dmalloc_async(&block, b_jobs + b_slots + b_coef + b_shq + 2 * b_rq + b_ctr, stream);
+    if (e != cudaSuccess) return e;
+    dev::JobDesc* d_jobs = reinterpret_cast<dev::JobDesc*>(block);
+    float* slots = reinterpret_cast<float*>(block + b_jobs);
+    float* coef = reinterpret_cast<float*>(block + b_jobs + b_slots);
+    float4* shq = reinterpret_cast<float4*>(block + b_jobs + b_slots + b_coef);
+    float4* rq = reinterpret_cast<float4*>(block + b_jobs + b_slots + b_coef + b_shq);
+    float4* tq = reinterpret_cast<float4*>(block + b_jobs + b_slots + b_coef + b_shq + b_rq);
+    unsigned int* ctr = reinterpret_cast<unsigned int*>(block + b_jobs + b_slots + b_coef + b_shq + 2 * b_rq);
+    std::vector<dev::JobDesc> jobs((size_t)n);
+    long long sample_off = 0, pix_off = 0, slot_off = 0;
+    for (int j = 0; j < n; j++) {
+        const BatchItem& it = items[(size_t)j];
+        const int ns = clamp_spp(it.aa);
+        Wave w;
+        w.slots = slots + slot_off;
+        w.coef = coef + 3 * sample_off;
+        w.shq = shq;
+        w.rq = rq;
+        w.tq = tq;
+        w.ctr = ctr;
+        dev::JobDesc& J = jobs[(size_t)j];
+        std::memset(&J, 0, sizeof(J));
+        J.S = it.s->view;
+        J.V = make_view(*it.s, w, it.W, it.H, ns, it.rg);
+        J.out = it.out;
+        J.sample_base = (int)sample_off;
+        J.pix_base = (int)pix_off;
+        const long long npad = region_padded(it.rg);
+        sample_off += npad * ns;
+        pix_off += npad;
+        slot_off += npad * ns * 3 * (it.s->view.num_lights + 2) * 3;
+    }
+    e = cudaMemcpyAsync(d_jobs, jobs.data(), (size_t)n * sizeof(dev::JobDesc), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) {
+        dev::WaveView V0 = jobs[0].V;
+        V0.slots = slots;
+        V0.coef = coef;
+        V0.nsamples = (int)total_samples;
+        V0.npix = (int)total_pix;
+        V0.jobs = d_jobs;
+        V0.num_jobs = n;
+        V0.count_rays = 1;
+        e = run_pipeline<F, true>(items[0].s->view, V0, (int)total_pix, nullptr, stream, tally);
+    }
+    // the copy above reads `jobs` before returning (pageable host memory);
+    // the block returns to the pool once the stream has finished with it
+    dfree_async(block, stream);
+    return e;
+}
+
+cudaError_t launch_wavefront_batch(const std::vector<BatchItem>& items, cudaStream_t stream,
+                                   unsigned long long* tally) {
+    std::vector<BatchItem> simple, full;
+    for (const BatchItem& it : items) {
+        if (!it.s || it.s->form != SHEEN_FORM_WAVEFRONT || !wave_supported(*it.s)) return cudaErrorInvalidValue;
+        (simple_scene(*it.s) ? simple : full).push_back(it);
+    }
+    cudaError_t e = batch_pass<dev::kCatSimple>(simple, stream, tally);
+    if (e == cudaSuccess) e = batch_pass<dev::kCatAll>(full, stream, tally);
+    return e;
+}
 
 // One frame of the queue pipeline launched directly (no graph) with events
 // at the stage boundaries and the ray counters read after every kernel.
@@ -934,8 +1153,8 @@ cudaError_t profile_wavefront(DeviceScene& s, int W, int H, int aa, float4* out,
     for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&ev[i]);
     if (e == cudaSuccess) e = dmalloc(&snap, 21 * sizeof(unsigned int));
     if (e == cudaSuccess)
-        e = simple_scene(s) ? run_pipeline<dev::kCatSimple>(s, V, npad, out, stream, nullptr, ev, snap)
-                            : run_pipeline<dev::kCatAll>(s, V, npad, out, stream, nullptr, ev, snap);
+        e = simple_scene(s) ? run_pipeline<dev::kCatSimple>(s.view, V, npad, out, stream, nullptr, ev, snap)
+                            : run_pipeline<dev::kCatAll>(s.view, V, npad, out, stream, nullptr, ev, snap);
     unsigned int h[21] = {0};
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e == cudaSuccess) e = cudaMemcpy(h, snap, sizeof(h), cudaMemcpyDeviceToHost);
@@ -983,8 +1202,8 @@ cudaError_t launch_wavefront_scratch(DeviceScene& s, void* scratch, size_t scrat
     if (!wave_carve(w, scratch, scratch_bytes, s.view.num_lights, nsamples)) return cudaErrorInvalidValue;
     const dev::WaveView V = make_view(s, w, W, H, ns, rg);
     const int npad = (int)region_padded(rg);
-    return simple_scene(s) ? run_pipeline<dev::kCatSimple>(s, V, npad, out, stream, tally)
-                           : run_pipeline<dev::kCatAll>(s, V, npad, out, stream, tally);
+    return simple_scene(s) ? run_pipeline<dev::kCatSimple>(s.view, V, npad, out, stream, tally)
+                           : run_pipeline<dev::kCatAll>(s.view, V, npad, out, stream, tally);
 }
 
 // ---------------------------------------------------------------------
@@ -1061,23 +1280,23 @@ cudaError_t noalloc_pipeline(const DeviceScene& s, const dev::WaveView& V, int n
         int dev_id = 0;
         cudaGetDevice(&dev_id);
         cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev_id);
-        g_primary = persistent_grid(dev::wave_primary<F>, g_sms);
-        g_shadow = persistent_grid(dev::wave_shadow<F>, g_sms);
-        g_reflect = persistent_grid(dev::wave_reflect<F>, g_sms);
-        g_refract = persistent_grid(dev::wave_refract<F>, g_sms);
+        g_primary = persistent_grid(dev::wave_primary<F, false>, g_sms);
+        g_shadow = persistent_grid(dev::wave_shadow<F, false>, g_sms);
+        g_reflect = persistent_grid(dev::wave_reflect<F, false>, g_sms);
+        g_refract = persistent_grid(dev::wave_refract<F, false>, g_sms);
     }
     cudaError_t e;
     // The queue counters are the only scratch that must start at zero.
     if ((e = cudaMemsetAsync(V.ctr, 0, dev::kCounterWords * sizeof(unsigned int), stream)) != cudaSuccess) return e;
-    dev::wave_primary<F><<<g_primary, 128, 0, stream>>>(s.view, V);
-    dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
+    dev::wave_primary<F, false><<<g_primary, 128, 0, stream>>>(s.view, V);
+    dev::wave_shadow<F, false><<<g_shadow, 128, 0, stream>>>(s.view, V);
     if ((e = cudaMemsetAsync(&V.ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
-    dev::wave_reflect<F><<<g_reflect, 128, 0, stream>>>(s.view, V);
-    dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
+    dev::wave_reflect<F, false><<<g_reflect, 128, 0, stream>>>(s.view, V);
+    dev::wave_shadow<F, false><<<g_shadow, 128, 0, stream>>>(s.view, V);
     if ((e = cudaMemsetAsync(&V.ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
-    dev::wave_refract<F><<<g_refract, 128, 0, stream>>>(s.view, V);
-    dev::wave_shadow<F><<<g_shadow, 128, 0, stream>>>(s.view, V);
-    dev::wave_resolve<<<(npad + 127) / 128, 128, 0, stream>>>(V, out);
+    dev::wave_refract<F, false><<<g_refract, 128, 0, stream>>>(s.view, V);
+    dev::wave_shadow<F, false><<<g_shadow, 128, 0, stream>>>(s.view, V);
+    dev::wave_resolve<false><<<(npad + 127) / 128, 128, 0, stream>>>(V, out);
     return cudaGetLastError();
 }
 
