@@ -216,6 +216,15 @@ int sheen_scene_render_host(SheenDeviceScene scene, int width, int height,
 int sheen_scene_primary_hits(SheenDeviceScene scene, int width, int height, int aa_samples,
                              int* obj_id_host, int* mat_id_host, float* t_host);
 
+/* Closest hits of arbitrary rays through a resident scene's own traversal.
+ * rays_host: n records of 8 floats {origin.xyz, t_min, direction.xyz, t_max}
+ * (the direction is used as given); per ray, in HOST arrays: object_id and
+ * material_id as scene_intersect sets them (integrator/raycast.h:14-70;
+ * 0x80000000 on a miss) and t (-1 on a miss).  No counterpart in the
+ * reference (its queries are internal to render_kernel).  0 / -1. */
+int sheen_scene_trace(SheenDeviceScene scene, const float* rays_host, int n, int* obj_id_host, int* mat_id_host,
+                      float* t_host);
+
 /* Host-side structural check of the wavefront form's triangle BVH (4-wide,
  * 8-bit child boxes) for a scene: every triangle in exactly one leaf, every
  * decoded child box containing all triangles below it.  Returns the tree
@@ -244,8 +253,9 @@ typedef struct SheenBatchJob {
 } SheenBatchJob;
 
 /* Renders every job in one pass of the wavefront queue kernels (one pass per
- * kernel variant: scenes of triangles, spheres and planes only, and the
- * rest, so that batching never changes a pixel): each stage is
+ * kernel variant: scenes of triangles, spheres and planes only or of every
+ * category, with the Moller-Trumbore or the watertight triangle test, so
+ * that batching never changes which code renders a job): each stage is
  * one persistent launch over the samples of all jobs (tiles of one frame,
  * several frames, several scenes, of uneven cost), claimed dynamically by
  * the blocks from shared queues.  Each job's pixels are exactly those of
@@ -291,11 +301,19 @@ int sheen_scene_profile_stages(SheenDeviceScene scene, int width, int height, in
  *                                   beside the full one (two host threads)
  *   "mem.pool_keep_mb"           0..1048576 (default 16384): freed device
  *                                   memory the library keeps for reuse
+ *   "trace.watertight"           0 (default): the wavefront form tests
+ *                                   triangles with the reference's
+ *                                   Moller-Trumbore; 1: a watertight
+ *                                   edge-function test (no ray passes
+ *                                   between triangles sharing an edge or
+ *                                   a vertex; hits may differ from the
+ *                                   reference's on edges).  Read at
+ *                                   sheen_scene_create.
  *   "build.device"               1 (default): the wavefront form's triangle
  *                                   BVH4s are built on the GPU; 0: on the
  *                                   host.  Both builders give byte-identical
  *                                   trees; read at sheen_scene_create.
- * Every setting gives the same image; only the speed differs.  0 / -1. */
+ * Every other setting gives the same image; only the speed differs.  0 / -1. */
 int sheen_tune_set(const char* key, int value);
 int sheen_tune_get(const char* key, int* value);
 

@@ -124,6 +124,8 @@ def lib():
     L.sheen_scene_primary_hits.argtypes = [P, I, I, I, P, P, P]
     L.sheen_scene_profile_stages.argtypes = [P, I, I, I, P, P, ctypes.POINTER(StageProfile)]
     L.sheen_render_batch.argtypes = [ctypes.POINTER(BatchJob), I, P, ctypes.POINTER(RenderStats)]
+    L.sheen_scene_trace.argtypes = [P, P, I, P, P, P]
+    L.sheen_scene_trace.restype = I
     L.sheen_render_batch.restype = I
     L.sheen_scene_profile_stages.restype = I
     L.sheen_scene_primary_hits.restype = I
@@ -232,6 +234,18 @@ class DeviceScene:
         p = StageProfile()
         _check(lib().sheen_scene_profile_stages(self.handle, width, height, aa, out_ptr, stream, ctypes.byref(p)))
         return p.as_dict()
+
+    def trace(self, rays: np.ndarray):
+        """Closest hits of arbitrary rays (n x 8 float32: origin, t_min,
+        direction, t_max): object ids, material ids, t (-1 on a miss)."""
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = len(rays)
+        obj = np.empty(n, np.int32)
+        mat = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        _check(lib().sheen_scene_trace(self.handle, rays.ctypes.data, n, obj.ctypes.data, mat.ctypes.data,
+                                       t.ctypes.data))
+        return obj, mat, t
 
     def primary_hits(self, width, height, aa):
         """Per-sample primary closest hits: object id, material id, t."""

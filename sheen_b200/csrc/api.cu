@@ -276,6 +276,32 @@ int sheen_scene_profile_stages(SheenDeviceScene h, int W, int H, int aa, float* 
     return 0;
 }
 
+int sheen_scene_trace(SheenDeviceScene h, const float* rays_host, int n, int* obj, int* mat, float* t) {
+    auto* s = reinterpret_cast<sheen::DeviceScene*>(h);
+    if (!s) { sheen::set_error("null scene handle"); return -1; }
+    if (n < 0 || (n > 0 && (!rays_host || !obj || !mat || !t))) { sheen::set_error("bad ray query"); return -1; }
+    if (n == 0) return 0;
+    float4* drays = nullptr;
+    int *dobj = nullptr, *dmat = nullptr;
+    float* dt = nullptr;
+    const size_t N = (size_t)n;
+    cudaError_t e = sheen::dmalloc(&drays, N * 2 * sizeof(float4));
+    if (e == cudaSuccess) e = sheen::dmalloc(&dobj, N * sizeof(int));
+    if (e == cudaSuccess) e = sheen::dmalloc(&dmat, N * sizeof(int));
+    if (e == cudaSuccess) e = sheen::dmalloc(&dt, N * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpy(drays, rays_host, N * 2 * sizeof(float4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = sheen::launch_trace_rays(*s, drays, n, dobj, dmat, dt, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(obj, dobj, N * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(mat, dmat, N * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(t, dt, N * sizeof(float), cudaMemcpyDeviceToHost);
+    sheen::dfree(drays);
+    sheen::dfree(dobj);
+    sheen::dfree(dmat);
+    sheen::dfree(dt);
+    if (e != cudaSuccess) return fail_cuda(e);
+    return 0;
+}
+
 int sheen_scene_primary_hits(SheenDeviceScene h, int W, int H, int aa, int* obj, int* mat, float* t) {
     auto* s = reinterpret_cast<sheen::DeviceScene*>(h);
     if (!s) { sheen::set_error("null scene handle"); return -1; }

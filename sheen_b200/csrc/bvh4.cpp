@@ -16,9 +16,10 @@
 // integer outward until the decoded box contains the exact child box.
 //
 // Triangles are stored in leaf order as three float4: {v0, original index},
-// {e1 = v1 - v0, 0}, {e2 = v2 - v0, 0}; e1/e2 are the same float
-// subtractions the reference's Moller-Trumbore performs per test
-// (primitives/triangle.h:9-10), so the test's results are unchanged.
+// then {e1 = v1 - v0, 0}, {e2 = v2 - v0, 0} for the Moller-Trumbore test
+// (the same float subtractions the reference performs per test,
+// primitives/triangle.h:9-10, so its results are unchanged), or {v1, 0},
+// {v2, 0} for the watertight test, which needs the vertices themselves.
 //
 // The arithmetic of every decision (bins, SAH costs, frame exponents,
 // quantisation) is in bvh4_rules.h, shared with the device builder
@@ -154,10 +155,11 @@ struct SahBuilder {
 
 }  // namespace
 
-void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out) {
+void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out, bool vertices) {
     out.nodes.clear();
     out.tris.clear();
     out.max_depth = 0;
+    out.vertices = vertices;
     const int n = (int)subset.size();
     if (n <= 0) return;
     SahBuilder sb;
@@ -186,8 +188,13 @@ void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out
         float fi;
         std::memcpy(&fi, &orig, 4);
         out.tris[3 * (size_t)i] = make_float4(t.v0.x, t.v0.y, t.v0.z, fi);
-        out.tris[3 * (size_t)i + 1] = make_float4(t.v1.x - t.v0.x, t.v1.y - t.v0.y, t.v1.z - t.v0.z, 0.0f);
-        out.tris[3 * (size_t)i + 2] = make_float4(t.v2.x - t.v0.x, t.v2.y - t.v0.y, t.v2.z - t.v0.z, 0.0f);
+        if (vertices) {
+            out.tris[3 * (size_t)i + 1] = make_float4(t.v1.x, t.v1.y, t.v1.z, 0.0f);
+            out.tris[3 * (size_t)i + 2] = make_float4(t.v2.x, t.v2.y, t.v2.z, 0.0f);
+        } else {
+            out.tris[3 * (size_t)i + 1] = make_float4(t.v1.x - t.v0.x, t.v1.y - t.v0.y, t.v1.z - t.v0.z, 0.0f);
+            out.tris[3 * (size_t)i + 2] = make_float4(t.v2.x - t.v0.x, t.v2.y - t.v0.y, t.v2.z - t.v0.z, 0.0f);
+        }
     }
 
     // Collapse to 4-wide nodes, breadth first from the root.
@@ -301,11 +308,14 @@ int check_qbvh4(const QBvh& q, int& depth) {
                 if (slot >= ntri) return -2;
                 seen[slot]++;
                 const float4 a = q.tris[3 * slot], b = q.tris[3 * slot + 1], c = q.tris[3 * slot + 2];
-                const float v[3][3] = {{a.x, a.y, a.z}, {a.x + b.x, a.y + b.y, a.z + b.z}, {a.x + c.x, a.y + c.y, a.z + c.z}};
+                float v[3][3] = {{a.x, a.y, a.z}, {b.x, b.y, b.z}, {c.x, c.y, c.z}};
+                if (!q.vertices)
+                    for (int p = 1; p < 3; p++)
+                        for (int ax = 0; ax < 3; ax++) v[p][ax] += v[0][ax];
                 for (int p = 0; p < 3; p++)
                     for (int ax = 0; ax < 3; ax++) {
-                        // v1 = v0 + e1 may round by an ulp: allow it
-                        const float tol = 1e-6f * (std::fabs(v[p][ax]) + 1.0f);
+                        // v0 + (v1 - v0) may round by an ulp: allow it for edge records
+                        const float tol = q.vertices ? 0.0f : 1e-6f * (std::fabs(v[p][ax]) + 1.0f);
                         if (v[p][ax] < it.bound.lo[ax] - tol || v[p][ax] > it.bound.hi[ax] + tol) return -3;
                     }
             }

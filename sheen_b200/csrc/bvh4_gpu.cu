@@ -778,15 +778,20 @@ __global__ void k_collapse_emit(const int* __restrict__ level, int m, int base, 
 }
 
 __global__ void k_emit_tris(const Triangle* __restrict__ tris, const int* __restrict__ subset,
-                            const int* __restrict__ idx, int n, float4* __restrict__ out) {
+                            const int* __restrict__ idx, int n, float4* __restrict__ out, bool vertices) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int s = idx[i];
     const int orig = subset ? subset[s] : s;
     const Triangle& t = tris[orig];
     out[3 * (size_t)i] = make_float4(t.v0.x, t.v0.y, t.v0.z, __int_as_float(orig));
-    out[3 * (size_t)i + 1] = make_float4(sub(t.v1.x, t.v0.x), sub(t.v1.y, t.v0.y), sub(t.v1.z, t.v0.z), 0.0f);
-    out[3 * (size_t)i + 2] = make_float4(sub(t.v2.x, t.v0.x), sub(t.v2.y, t.v0.y), sub(t.v2.z, t.v0.z), 0.0f);
+    if (vertices) {
+        out[3 * (size_t)i + 1] = make_float4(t.v1.x, t.v1.y, t.v1.z, 0.0f);
+        out[3 * (size_t)i + 2] = make_float4(t.v2.x, t.v2.y, t.v2.z, 0.0f);
+    } else {
+        out[3 * (size_t)i + 1] = make_float4(sub(t.v1.x, t.v0.x), sub(t.v1.y, t.v0.y), sub(t.v1.z, t.v0.z), 0.0f);
+        out[3 * (size_t)i + 2] = make_float4(sub(t.v2.x, t.v0.x), sub(t.v2.y, t.v0.y), sub(t.v2.z, t.v0.z), 0.0f);
+    }
 }
 
 // ---- subsets: triangles that can / cannot pass a shadow ray ----------------
@@ -819,7 +824,8 @@ struct Carver {
 // Device-built BVH4 over triangles tris[subset[i]] (subset null: all n).
 // Allocates out.nodes (exact size) and out.tris (3 float4 per triangle);
 // everything else is temporary.  Synchronises `stream` once per tree level.
-cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, DevQBvh& out, cudaStream_t stream) {
+cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, DevQBvh& out, cudaStream_t stream,
+                               bool vertices) {
     using namespace bvhg;
     out = DevQBvh{};
     if (n <= 0) return cudaSuccess;
@@ -985,7 +991,7 @@ cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, D
         CK(dmalloc_async(&nodes_out, (size_t)num_q * sizeof(dev::QNode4), stream));
         CK(dmalloc_async(&tris_out, 3 * N * sizeof(float4), stream));
         CK(cudaMemcpyAsync(nodes_out, P.qtmp, (size_t)num_q * sizeof(dev::QNode4), cudaMemcpyDeviceToDevice, stream));
-        k_emit_tris<<<(n + 255) / 256, 256, 0, stream>>>(tris, subset, P.idx, n, tris_out);
+        k_emit_tris<<<(n + 255) / 256, 256, 0, stream>>>(tris, subset, P.idx, n, tris_out, vertices);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(stream));
     }
@@ -1027,6 +1033,7 @@ cudaError_t build_wave_meshes_device(DeviceScene& s, cudaStream_t stream) {
     size_t cb = 0;
     cudaStream_t st2 = nullptr;
     cudaError_t e_all = cudaSuccess, e_sub = cudaSuccess;
+    const bool wt = tuning().watertight != 0;
 #define CK(x) do { if ((e = (x)) != cudaSuccess) goto done; } while (0)
     CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
     CK(dmalloc_async(&iota, (size_t)n * sizeof(int), stream));
@@ -1052,15 +1059,15 @@ cudaError_t build_wave_meshes_device(DeviceScene& s, cudaStream_t stream) {
         CK(cudaGetDevice(&dev_id));
         auto subset_trees = [&] {
             cudaSetDevice(dev_id);
-            if (npass > 0 && nblock > 0) e_sub = build_qbvh4_device(v.tris, sel, nblock, blk, st2);
-            if (npass > 0 && e_sub == cudaSuccess) e_sub = build_qbvh4_device(v.tris, sel + n, npass, pas, st2);
+            if (npass > 0 && nblock > 0) e_sub = build_qbvh4_device(v.tris, sel, nblock, blk, st2, wt);
+            if (npass > 0 && e_sub == cudaSuccess) e_sub = build_qbvh4_device(v.tris, sel + n, npass, pas, st2, wt);
         };
         if (tuning().build_concurrent) {
             std::thread subsets(subset_trees);
-            e_all = build_qbvh4_device(v.tris, nullptr, n, all, stream);
+            e_all = build_qbvh4_device(v.tris, nullptr, n, all, stream, wt);
             subsets.join();
         } else {
-            e_all = build_qbvh4_device(v.tris, nullptr, n, all, stream);
+            e_all = build_qbvh4_device(v.tris, nullptr, n, all, stream, wt);
             subset_trees();
         }
         e = e_all != cudaSuccess ? e_all : e_sub;
@@ -1082,12 +1089,13 @@ done:
     keep(blk);
     keep(pas);
     if (e != cudaSuccess) return e;
-    auto qmesh = [](const DevQBvh& q) {
+    auto qmesh = [wt](const DevQBvh& q) {
         dev::QMesh m;
         m.nodes = q.nodes;
         m.tris = q.tris;
         m.num_nodes = q.num_nodes;
         m.num_tris = q.num_tris;
+        m.watertight = wt ? 1 : 0;
         return m;
     };
     v.q_all = qmesh(all);
@@ -1119,10 +1127,11 @@ extern "C" int sheen_bvh4_compare_builders(const SheenScene* scene, double* time
     }
     const double h0 = now_ms();
     QBvh hq[3];
-    build_qbvh4(scene->triangles, all, hq[0]);
+    const bool wt = tuning().watertight != 0;   // both builders use the record layout in force
+    build_qbvh4(scene->triangles, all, hq[0], wt);
     if (!pass.empty()) {
-        build_qbvh4(scene->triangles, block, hq[1]);
-        build_qbvh4(scene->triangles, pass, hq[2]);
+        build_qbvh4(scene->triangles, block, hq[1], wt);
+        build_qbvh4(scene->triangles, pass, hq[2], wt);
     }
     const double host_ms = now_ms() - h0;
 

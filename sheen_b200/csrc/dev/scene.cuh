@@ -46,12 +46,16 @@ struct __align__(16) QNode4 {
 };
 
 // One BVH4 over a set of triangles: nodes and 3 float4 per triangle slot in
-// leaf order ({v0, original index}, {e1, 0}, {e2, 0}).
+// leaf order.  watertight selects the triangle test and the record layout:
+// 0 the reference's Moller-Trumbore on {v0, original index}, {e1, 0},
+// {e2, 0}; 1 the watertight edge-function test on {v0, index}, {v1, 0},
+// {v2, 0}.
 struct QMesh {
     const QNode4* nodes;
     const float4* tris;
     int num_nodes;
     int num_tris;
+    int watertight;
 };
 
 struct DevScene {

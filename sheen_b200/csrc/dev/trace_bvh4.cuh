@@ -112,8 +112,8 @@ __device__ __forceinline__ int qnode_children(const QNode4* __restrict__ nodes, 
 }
 
 // Moller-Trumbore on stored {v0, e1, e2} (primitives/triangle.h:8-36).
-__device__ __forceinline__ bool qtri_test(const QRay& r, float4 a, float4 b, float4 c, float tmin, float tmax,
-                                          float& t, float& u, float& v) {
+__device__ __forceinline__ bool qtri_test_mt(const QRay& r, float4 a, float4 b, float4 c, float tmin, float tmax,
+                                             float& t, float& u, float& v) {
     const float3 e1 = f3(b.x, b.y, b.z), e2 = f3(c.x, c.y, c.z);
     const float3 pv = cross(r.d, e2);
     const float det = dot(e1, pv);
@@ -129,10 +129,70 @@ __device__ __forceinline__ bool qtri_test(const QRay& r, float4 a, float4 b, flo
     return !(t < tmin || t > tmax);
 }
 
+__device__ __forceinline__ float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+// Watertight ray / triangle test (Woop, Benthin and Wald, "Watertight
+// Ray/Triangle Intersection", JCGT 2013, restated).  The ray is sheared so
+// that its direction becomes +z; the three 2D edge functions of the sheared
+// triangle then decide the hit, each computed from the vertices alone, so
+// two triangles sharing an edge evaluate that edge with the same operands
+// and a ray through the edge (or a shared vertex) cannot pass between them.
+// An edge function that rounds to exactly 0 is recomputed in double (the
+// paper's fallback).  Same outputs as the Moller-Trumbore test: t and the
+// weights u of v1, v of v2.
+__device__ __forceinline__ bool qtri_test_wt(const QRay& r, float4 a, float4 b, float4 c, float tmin, float tmax,
+                                             float& t, float& u, float& v) {
+    const float ax = fabsf(r.d.x), ay = fabsf(r.d.y), az = fabsf(r.d.z);
+    const int kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    const float dz = comp(r.d, kz);
+    if (dz < 0.0f) { const int k = kx; kx = ky; ky = k; }   // keep the winding
+    const float sx = comp(r.d, kx) / dz, sy = comp(r.d, ky) / dz, sz = 1.0f / dz;
+    const float3 A = f3(a.x, a.y, a.z) - r.o, B = f3(b.x, b.y, b.z) - r.o, C = f3(c.x, c.y, c.z) - r.o;
+    const float Ax = comp(A, kx) - sx * comp(A, kz), Ay = comp(A, ky) - sy * comp(A, kz);
+    const float Bx = comp(B, kx) - sx * comp(B, kz), By = comp(B, ky) - sy * comp(B, kz);
+    const float Cx = comp(C, kx) - sx * comp(C, kz), Cy = comp(C, ky) - sy * comp(C, kz);
+    // Products rounded separately (no fused multiply-add): a neighbour
+    // evaluates the shared edge with the operands swapped, and only then is
+    // its value exactly the negation of this one.
+    float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+    float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+    float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+        V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+        W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    const float det = U + V + W;
+    if (det == 0.0f) return false;
+    const float T = U * (sz * comp(A, kz)) + V * (sz * comp(B, kz)) + W * (sz * comp(C, kz));
+    const float inv = 1.0f / det;
+    t = T * inv;
+    if (t < tmin || t > tmax) return false;
+    u = V * inv;
+    v = W * inv;
+    return true;
+}
+
+// Triangle test selection: TRI 1 Moller-Trumbore, 2 watertight, 0 by the
+// mesh's own flag at run time.  The hot queue kernels are compiled per test
+// (TRI 1 or 2): the watertight code inlined beside the default one, even
+// untaken, costs the default scenes 3% of their frame time.
+template <int TRI>
+__device__ __forceinline__ bool qtri_test(const QRay& r, float4 a, float4 b, float4 c, float tmin, float tmax,
+                                          float& t, float& u, float& v, int watertight) {
+    if constexpr (TRI == 1) return qtri_test_mt(r, a, b, c, tmin, tmax, t, u, v);
+    else if constexpr (TRI == 2) return qtri_test_wt(r, a, b, c, tmin, tmax, t, u, v);
+    else return watertight ? qtri_test_wt(r, a, b, c, tmin, tmax, t, u, v)
+                           : qtri_test_mt(r, a, b, c, tmin, tmax, t, u, v);
+}
+
 // Closest (ANY = false) or any (ANY = true) triangle hit with t in
 // [r.tmin, tmax] and strictly below `t_best` (in/out).  Returns the original
 // triangle index or -1.
-template <bool ANY, bool COUNT>
+template <bool ANY, bool COUNT, int TRI>
 __device__ __forceinline__ int qmesh_trace(const QMesh& m, const QRay& r, float tmax, float& t_best, float& bu,
                                            float& bv, Counters& c) {
     if (!m.nodes) return -1;
@@ -196,7 +256,7 @@ __device__ __forceinline__ int qmesh_trace(const QMesh& m, const QRay& r, float 
                 const float4 cc = __ldg(&m.tris[3 * slot + 2]);
                 if (COUNT) c.prims++;
                 float t, u, v;
-                if (qtri_test(r, a, b, cc, r.tmin, tmax, t, u, v) && t < t_best) {
+                if (qtri_test<TRI>(r, a, b, cc, r.tmin, tmax, t, u, v, m.watertight) && t < t_best) {
                     t_best = t; bu = u; bv = v;
                     best = __float_as_int(a.w);
                     if (ANY) return best;
@@ -218,12 +278,12 @@ __device__ __forceinline__ int qmesh_trace(const QMesh& m, const QRay& r, float 
 }
 
 // Closest mesh hit over q_all as a hit record (mesh_ref's result).
-template <bool COUNT>
+template <bool COUNT, int TRI>
 __device__ __forceinline__ bool mesh_q(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
     if (!S.q_all.nodes) return false;
     const QRay q = make_qray(r);
     float t = r.tmax, u = 0.0f, v = 0.0f;
-    const int tri = qmesh_trace<false, COUNT>(S.q_all, q, r.tmax, t, u, v, c);
+    const int tri = qmesh_trace<false, COUNT, TRI>(S.q_all, q, r.tmax, t, u, v, c);
     if (tri < 0) return false;
     tri_finish(r, S.tris[tri], t, u, v, h);
     h.obj = -(tri + 1);
@@ -236,7 +296,7 @@ __device__ __forceinline__ bool mesh_q(const DevScene& S, const Ray& r, Hit& h, 
 // blocking hit before it (or anywhere when there is none) makes the closest
 // hit blocking; otherwise the passable hit is classified by its material
 // (mask-aware when asked).  Returns kClear when the mesh has no hit at all.
-template <bool COUNT>
+template <bool COUNT, int TRI>
 __device__ __forceinline__ int mesh_shadow_q(const DevScene& S, const Ray& r, bool mask_aware, ShadowHit& sh,
                                              Counters& c) {
     if (!S.q_all.nodes) return kClear;
@@ -245,13 +305,13 @@ __device__ __forceinline__ int mesh_shadow_q(const DevScene& S, const Ray& r, bo
         // No triangle can pass (every material's transmission <= 0.5, and a
         // property map only scales it down): any hit blocks.
         float t = r.tmax, u, v;
-        return qmesh_trace<true, COUNT>(S.q_all, q, r.tmax, t, u, v, c) >= 0 ? kBlocked : kClear;
+        return qmesh_trace<true, COUNT, TRI>(S.q_all, q, r.tmax, t, u, v, c) >= 0 ? kBlocked : kClear;
     }
     float tp = r.tmax, up = 0.0f, vp = 0.0f;
-    const int pass_tri = qmesh_trace<false, COUNT>(S.q_pass, q, r.tmax, tp, up, vp, c);
+    const int pass_tri = qmesh_trace<false, COUNT, TRI>(S.q_pass, q, r.tmax, tp, up, vp, c);
     if (S.q_block.nodes) {
         float tb = tp, ub, vb;   // strictly closer than the passable hit (or than t_max)
-        if (qmesh_trace<true, COUNT>(S.q_block, q, r.tmax, tb, ub, vb, c) >= 0) return kBlocked;
+        if (qmesh_trace<true, COUNT, TRI>(S.q_block, q, r.tmax, tb, ub, vb, c) >= 0) return kBlocked;
     }
     if (pass_tri < 0) return kClear;
     Hit h;
@@ -260,12 +320,12 @@ __device__ __forceinline__ int mesh_shadow_q(const DevScene& S, const Ray& r, bo
 }
 
 // Any hit in the opaque categories (render_kernel.cu:413-422, media rays).
-template <bool COUNT>
+template <bool COUNT, int TRI>
 __device__ __forceinline__ bool mesh_any_q(const DevScene& S, const Ray& r, Counters& c) {
     if (!S.q_all.nodes) return false;
     const QRay q = make_qray(r);
     float t = r.tmax, u, v;
-    return qmesh_trace<true, COUNT>(S.q_all, q, r.tmax, t, u, v, c) >= 0;
+    return qmesh_trace<true, COUNT, TRI>(S.q_all, q, r.tmax, t, u, v, c) >= 0;
 }
 
 // ---- non-triangle categories: culled, near-first walks ------------------
@@ -435,11 +495,16 @@ enum : int {
     kCatSpheres = 1, kCatStrands = 2, kCatMesh = 4, kCatHF = 8, kCatSE = 16, kCatLathe = 32, kCatPrism = 64,
     kCatCSG = 128, kCatPlanes = 256,
     kCatAll = 511,
-    kCatSimple = kCatSpheres | kCatMesh | kCatPlanes
+    kCatSimple = kCatSpheres | kCatMesh | kCatPlanes,
+    // triangle test compiled in (neither bit: chosen per mesh at run time)
+    kTriMT = 512, kTriWT = 1024
 };
 
 // Query policy of the wavefront form: triangles through the BVH4s, every
 // other category through the plain form's code (same category order).
+template <int F>
+constexpr int tri_of() { return (F & kTriWT) ? 2 : ((F & kTriMT) ? 1 : 0); }
+
 template <bool COUNT, int F = kCatAll>
 struct FastTracer {
     __device__ __forceinline__ static bool closest(const DevScene& S, const Ray& r, Hit& rec, Counters& c) {
@@ -448,7 +513,7 @@ struct FastTracer {
         Hit t;
         if ((F & kCatSpheres) && spheres_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
         if ((F & kCatStrands) && strands_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if ((F & kCatMesh) && mesh_q<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatMesh) && mesh_q<COUNT, tri_of<F>()>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
         if ((F & kCatHF) && hfs_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
         if ((F & kCatSE) && ses_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
         if ((F & kCatLathe) && lathes_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
@@ -462,7 +527,7 @@ struct FastTracer {
         Hit h;
         if ((F & kCatSpheres) && spheres_cull<COUNT>(S, r, h, c)) return classify_shadow_hit(S, h, mask_aware, sh);
         if (F & kCatMesh) {
-            const int m = mesh_shadow_q<COUNT>(S, r, mask_aware, sh, c);
+            const int m = mesh_shadow_q<COUNT, tri_of<F>()>(S, r, mask_aware, sh, c);
             if (m != kClear) return m;
         }
         if (((F & kCatHF) && hfs_cull<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_cull<COUNT>(S, r, h, c)) ||
@@ -493,7 +558,7 @@ struct FastTracer {
     __device__ __forceinline__ static bool occluded(const DevScene& S, const Ray& r, Counters& c) {
         Hit h;
         if ((F & kCatSpheres) && spheres_cull<COUNT>(S, r, h, c)) return true;
-        if ((F & kCatMesh) && mesh_any_q<COUNT>(S, r, c)) return true;
+        if ((F & kCatMesh) && mesh_any_q<COUNT, tri_of<F>()>(S, r, c)) return true;
         return ((F & kCatHF) && hfs_cull<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_cull<COUNT>(S, r, h, c)) ||
                ((F & kCatLathe) && lathes_cull<COUNT>(S, r, h, c)) ||
                ((F & kCatPrism) && prisms_cull<COUNT>(S, r, h, c)) ||

@@ -38,10 +38,12 @@ struct QBvh {
     std::vector<float4> tris;      // 3 float4 per triangle slot in leaf order
     int leaf_size_max = 0;
     int max_depth = 0;            // inner-node levels (the traversal stack holds 3 per level)
+    bool vertices = false;        // triangle records hold v1, v2 (watertight test) instead of e1, e2
 };
 // Builds over the triangles listed in `subset` (indices into `tris`; the
-// stored triangle records keep those original indices).
-void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out);
+// stored triangle records keep those original indices).  `vertices`
+// selects the record layout of the watertight triangle test.
+void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out, bool vertices = false);
 
 // The same BVH4 built on the device (bvh4_gpu.cu), byte-identical to
 // build_qbvh4's.  nodes/tris are device allocations owned by the caller.
@@ -53,7 +55,7 @@ struct DevQBvh {
     int max_depth = 0;
 };
 cudaError_t build_qbvh4_device(const Triangle* tris_dev, const int* subset_dev, int n, DevQBvh& out,
-                               cudaStream_t stream);
+                               cudaStream_t stream, bool vertices = false);
 
 // Result/accounting of one render call.
 struct RenderTally {
@@ -103,6 +105,9 @@ cudaError_t launch_plain(const DeviceScene& s, int W, int H, int aa, Region rg, 
 // Primary closest hits (object id, material id, t) per pixel sample.
 cudaError_t launch_primary_hits_plain(const DeviceScene& s, int W, int H, int ns, int* obj, int* mat, float* t,
                                       cudaStream_t stream);
+// Closest hits of arbitrary rays through the scene form's own traversal.
+cudaError_t launch_trace_rays(const DeviceScene& s, const float4* rays, int n, int* obj, int* mat, float* t,
+                              cudaStream_t stream);
 cudaError_t launch_primary_hits_bvh4(const DeviceScene& s, int W, int H, int ns, int* obj, int* mat, float* t,
                                      cudaStream_t stream);
 
@@ -155,6 +160,7 @@ struct Tuning {
     int build_device = 1;           // wavefront triangle BVH4s: 1 built on the device, 0 on the host
     int build_concurrent = 1;       // device build: the subset trees beside the full tree (2 host threads)
     int pool_keep_mb = 16384;       // freed device memory the library's pool keeps for reuse
+    int watertight = 0;             // wavefront triangle test: 0 Moller-Trumbore (the reference's), 1 watertight
 };
 Tuning tuning();
 int tuning_generation();

@@ -57,7 +57,35 @@ __global__ void primary_hits_bvh4_kernel(DevScene S, int W, int H, int ns, int* 
     }
 }
 
+// Closest hits of arbitrary rays (sheen_scene_trace): rays[2i] = {origin,
+// tmin}, rays[2i+1] = {direction, tmax}; T is the scene form's query policy.
+template <class T>
+__global__ void trace_rays_kernel(DevScene S, const float4* __restrict__ rays, int n, int* obj, int* mat, float* tt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = rays[2 * (size_t)i], b = rays[2 * (size_t)i + 1];
+    Ray r;
+    r.o = f3(a.x, a.y, a.z);
+    r.tmin = a.w;
+    r.d = f3(b.x, b.y, b.z);
+    r.tmax = b.w;
+    Hit h;
+    Counters c;
+    if (T::closest(S, r, h, c)) { obj[i] = h.obj; mat[i] = h.mat; tt[i] = h.t; }
+    else { obj[i] = (int)0x80000000; mat[i] = (int)0x80000000; tt[i] = -1.0f; }
+}
+
 }  // namespace dev
+
+cudaError_t launch_trace_rays(const DeviceScene& s, const float4* rays, int n, int* obj, int* mat, float* t,
+                              cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    if (s.form == SHEEN_FORM_PLAIN)
+        dev::trace_rays_kernel<dev::RefTracer<false>><<<(n + 127) / 128, 128, 0, stream>>>(s.view, rays, n, obj, mat, t);
+    else
+        dev::trace_rays_kernel<dev::FastTracer<false>><<<(n + 127) / 128, 128, 0, stream>>>(s.view, rays, n, obj, mat, t);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_mega_bvh4(const DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
                              bool count_nodes,

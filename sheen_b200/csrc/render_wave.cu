@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "dev/integrator.cuh"
@@ -574,7 +575,8 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveVi
                 const float4 b = __ldg(&wt[3 * s + 1]);
                 const float4 c4 = __ldg(&wt[3 * s + 2]);
                 float t, u, v;
-                if (qtri_test(q, a, b, c4, q.tmin, tmax, t, u, v) && t < t_best) {
+                if (qtri_test<tri_of<F>()>(q, a, b, c4, q.tmin, tmax, t, u, v, scene().q_all.watertight) &&
+                    t < t_best) {
                     t_best = t; wu = u; wv = v;
                     wbest = __float_as_int(a.w);
                     if (state == kWalkBlock) { ended = true; break; }
@@ -997,6 +999,24 @@ static dev::WaveView make_view(const DeviceScene& s, const Wave& w, int W, int H
     return V;
 }
 
+// Calls fn(std::integral_constant<int, F>) with the queue kernels' template
+// argument for a scene: its category set (triangles + spheres + planes only,
+// or every category) and its triangle test (Moller-Trumbore or watertight).
+template <class Fn>
+static cudaError_t dispatch_variant(bool simple, bool watertight, Fn&& fn) {
+    using dev::kCatAll;
+    using dev::kCatSimple;
+    using dev::kTriMT;
+    using dev::kTriWT;
+    if (simple)
+        return watertight ? fn(std::integral_constant<int, kCatSimple | kTriWT>{})
+                          : fn(std::integral_constant<int, kCatSimple | kTriMT>{});
+    return watertight ? fn(std::integral_constant<int, kCatAll | kTriWT>{})
+                      : fn(std::integral_constant<int, kCatAll | kTriMT>{});
+}
+
+static bool watertight_scene(const DeviceScene& s) { return s.view.q_all.watertight != 0; }
+
 static bool simple_scene(const DeviceScene& s) {
     const dev::DevScene& sv = s.view;
     return sv.num_strands == 0 && sv.num_hfs == 0 && sv.num_ses == 0 && sv.num_lathes == 0 && sv.num_prisms == 0 &&
@@ -1024,8 +1044,9 @@ cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, fl
             (e = cudaStreamCreateWithFlags(&w->capture_stream, cudaStreamNonBlocking)) != cudaSuccess)
             return e;
         if ((e = cudaStreamBeginCapture(w->capture_stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
-        cudaError_t le = simple ? run_pipeline<dev::kCatSimple>(s.view, V, npad, out, w->capture_stream, s.d_tally)
-                                : run_pipeline<dev::kCatAll>(s.view, V, npad, out, w->capture_stream, s.d_tally);
+        cudaError_t le = dispatch_variant(simple, watertight_scene(s), [&](auto f) {
+            return run_pipeline<decltype(f)::value>(s.view, V, npad, out, w->capture_stream, s.d_tally);
+        });
         cudaGraph_t graph = nullptr;
         e = cudaStreamEndCapture(w->capture_stream, &graph);
         if (le != cudaSuccess) { if (graph) cudaGraphDestroy(graph); return le; }
@@ -1125,13 +1146,18 @@ static cudaError_t batch_pass(const std::vector<BatchItem>& items, cudaStream_t 
 
 cudaError_t launch_wavefront_batch(const std::vector<BatchItem>& items, cudaStream_t stream,
                                    unsigned long long* tally) {
-    std::vector<BatchItem> simple, full;
+    // one pass per kernel variant: category set x triangle test
+    std::vector<BatchItem> groups[4];
     for (const BatchItem& it : items) {
         if (!it.s || it.s->form != SHEEN_FORM_WAVEFRONT || !wave_supported(*it.s)) return cudaErrorInvalidValue;
-        (simple_scene(*it.s) ? simple : full).push_back(it);
+        groups[(simple_scene(*it.s) ? 0 : 2) + (watertight_scene(*it.s) ? 1 : 0)].push_back(it);
     }
-    cudaError_t e = batch_pass<dev::kCatSimple>(simple, stream, tally);
-    if (e == cudaSuccess) e = batch_pass<dev::kCatAll>(full, stream, tally);
+    cudaError_t e = cudaSuccess;
+    for (int g = 0; g < 4 && e == cudaSuccess; g++)
+        if (!groups[g].empty())
+            e = dispatch_variant(g < 2, (g & 1) != 0, [&](auto f) {
+                return batch_pass<decltype(f)::value>(groups[g], stream, tally);
+            });
     return e;
 }
 
@@ -1153,8 +1179,9 @@ cudaError_t profile_wavefront(DeviceScene& s, int W, int H, int aa, float4* out,
     for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&ev[i]);
     if (e == cudaSuccess) e = dmalloc(&snap, 21 * sizeof(unsigned int));
     if (e == cudaSuccess)
-        e = simple_scene(s) ? run_pipeline<dev::kCatSimple>(s.view, V, npad, out, stream, nullptr, ev, snap)
-                            : run_pipeline<dev::kCatAll>(s.view, V, npad, out, stream, nullptr, ev, snap);
+        e = dispatch_variant(simple_scene(s), watertight_scene(s), [&](auto f) {
+            return run_pipeline<decltype(f)::value>(s.view, V, npad, out, stream, nullptr, ev, snap);
+        });
     unsigned int h[21] = {0};
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e == cudaSuccess) e = cudaMemcpy(h, snap, sizeof(h), cudaMemcpyDeviceToHost);
@@ -1202,8 +1229,9 @@ cudaError_t launch_wavefront_scratch(DeviceScene& s, void* scratch, size_t scrat
     if (!wave_carve(w, scratch, scratch_bytes, s.view.num_lights, nsamples)) return cudaErrorInvalidValue;
     const dev::WaveView V = make_view(s, w, W, H, ns, rg);
     const int npad = (int)region_padded(rg);
-    return simple_scene(s) ? run_pipeline<dev::kCatSimple>(s.view, V, npad, out, stream, tally)
-                           : run_pipeline<dev::kCatAll>(s.view, V, npad, out, stream, tally);
+    return dispatch_variant(simple_scene(s), watertight_scene(s), [&](auto f) {
+        return run_pipeline<decltype(f)::value>(s.view, V, npad, out, stream, tally);
+    });
 }
 
 // ---------------------------------------------------------------------

@@ -32,6 +32,7 @@ const Key kKeys[] = {
     {"build.device", &Tuning::build_device, 0, 1},
     {"build.concurrent", &Tuning::build_concurrent, 0, 1},
     {"mem.pool_keep_mb", &Tuning::pool_keep_mb, 0, 1 << 20},
+    {"trace.watertight", &Tuning::watertight, 0, 1},
 };
 
 }  // namespace

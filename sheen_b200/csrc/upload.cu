@@ -297,9 +297,10 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
             const bool passable = m >= 0 && m < in->num_materials && in->materials[m].transmission > 0.5f;
             (passable ? pass : block).push_back(i);
         }
-        std::thread t1([&] { if (!pass.empty()) build_qbvh4(in->triangles, block, q_block); });
-        std::thread t2([&] { if (!pass.empty()) build_qbvh4(in->triangles, pass, q_pass); });
-        build_qbvh4(in->triangles, all, q_all);
+        const bool wt = tuning().watertight != 0;
+        std::thread t1([&] { if (!pass.empty()) build_qbvh4(in->triangles, block, q_block, wt); });
+        std::thread t2([&] { if (!pass.empty()) build_qbvh4(in->triangles, pass, q_pass, wt); });
+        build_qbvh4(in->triangles, all, q_all, wt);
         t1.join();
         t2.join();
         // The traversal stack keeps at most 3 entries per level below the root.
@@ -433,6 +434,7 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
         m.tris = (const float4*)dptr(ot);
         m.num_nodes = (int)q.nodes.size();
         m.num_tris = (int)(q.tris.size() / 3);
+        m.watertight = q.vertices ? 1 : 0;
         return m;
     };
     v.q_all = qmesh(q_all, o_qn, o_qt);

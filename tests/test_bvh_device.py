@@ -78,6 +78,18 @@ def test_triangle_soups_identical(n):
 
 
 @pytest.mark.gpu
+def test_vertex_records_identical():
+    """The watertight test's record layout ({v0}, {v1}, {v2}) from both builders."""
+    _init()
+    sb.tune_set("trace.watertight", 1)
+    try:
+        rc, _ = _compare(sb.generate_scene(1, 3, 5))
+    finally:
+        sb.tune_set("trace.watertight", 0)
+    assert rc == 0, (rc, sb.last_error())
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("n", [40, 3000])
 def test_coincident_centroids_identical(n):
     """Every centroid equal: no SAH candidate qualifies, the list is split in
