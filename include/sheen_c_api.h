@@ -313,7 +313,13 @@ int sheen_scene_profile_stages(SheenDeviceScene scene, int width, int height, in
  *                                   BVH4s are built on the GPU; 0: on the
  *                                   host.  Both builders give byte-identical
  *                                   trees; read at sheen_scene_create.
- * Every other setting gives the same image; only the speed differs.  0 / -1. */
+ *   "camera.centered"            0 (default): the reference's sample
+ *                                   positions, jittered even at 1 spp
+ *                                   (sampling/aa.h:45-58); 1: no jitter --
+ *                                   the pixel centre at 1 spp, cell centres
+ *                                   otherwise.  Read at sheen_scene_create.
+ * Every other setting gives the same image (watertight and centered change
+ * it on purpose); only the speed differs.  0 / -1. */
 int sheen_tune_set(const char* key, int value);
 int sheen_tune_get(const char* key, int* value);
 

@@ -88,6 +88,22 @@ static void aa_offset(int s, int n, int x, int y, real* ox, real* oy) {
     *oy = ((real)(s / side) + aa_rand(seed ^ 0x9e3779b9u)) * inv;
 }
 
+/* Extension (no reference counterpart): sample positions without jitter --
+ * the pixel centre at 1 spp, the centres of the same cells otherwise. */
+static void aa_offset_centered(int s, int n, real* ox, real* oy) {
+    if (n <= 1) { *ox = R(0.5); *oy = R(0.5); return; }
+    if (n <= 4) {
+        *ox = (s == 0 || s == 2) ? R(0.25) : R(0.75);
+        *oy = s < 2 ? R(0.25) : R(0.75);
+        return;
+    }
+    int side = 2;
+    while (side * side < n) side++;
+    real inv = R(1) / (real)side;
+    *ox = ((real)(s % side) + R(0.5)) * inv;
+    *oy = ((real)(s / side) + R(0.5)) * inv;
+}
+
 /* ------------------------------------------------------------------ */
 /* scene                                                               */
 /* ------------------------------------------------------------------ */
@@ -104,7 +120,13 @@ struct OracleScene {
     /* photon map (render_kernel.h:47-53) */
     sheen_float3* ph_pos; sheen_float3* ph_dir; sheen_float3* ph_nrm; sheen_float3* ph_flux;
     int nph; int* cell_start; int* cell_count; int num_cells; real cell;
+    int centered;                       /* samples without jitter (extension) */
 };
+
+static void sample_pos(const OracleScene* S, int s, int n, int x, int y, real* ox, real* oy) {
+    if (S->centered) aa_offset_centered(s, n, ox, oy);
+    else aa_offset(s, n, x, y, ox, oy);
+}
 
 /* ------------------------------------------------------------------ */
 /* bvh.h:578-600 -- slab test exactly as the reference writes it        */
@@ -1346,7 +1368,7 @@ static void render_pixel(const OracleScene* S, int x, int y, int W, int H, int a
     V acc = v3(0, 0, 0);
     for (int s = 0; s < ns; s++) {
         real ox, oy;
-        aa_offset(s, ns, x, y, &ox, &oy);
+        sample_pos(S, s, ns, x, y, &ox, &oy);
         real u = ((real)x + ox) / (real)W * 2 - 1;
         real v = 1 - ((real)y + oy) / (real)H * 2;
         uint32_t seed = aa_hash((uint32_t)x * 73856093u ^ (uint32_t)y * 19349663u ^ (uint32_t)s * 83492791u);
@@ -1688,6 +1710,10 @@ void oracle_scene_destroy(OracleScene* S) {
 
 int oracle_scene_photon_count(const OracleScene* S) { return S ? S->nph : 0; }
 
+void oracle_scene_set_centered(OracleScene* S, int centered) {
+    if (S) S->centered = centered;
+}
+
 int oracle_render(const OracleScene* S, int W, int H, int aa, float* out, int y0, int y1, int nthreads) {
     if (!S || W <= 0 || H <= 0 || !out) return -1;
     if (y1 <= 0 || y1 > H) y1 = H;
@@ -1715,7 +1741,7 @@ int oracle_primary_hits(const OracleScene* S, int W, int H, int aa, int* cat, in
         for (int x = 0; x < W; x++)
             for (int s = 0; s < ns; s++) {
                 real ox, oy;
-                aa_offset(s, ns, x, y, &ox, &oy);
+                sample_pos(S, s, ns, x, y, &ox, &oy);
                 real u = ((real)x + ox) / (real)W * 2 - 1, v = 1 - ((real)y + oy) / (real)H * 2;
                 real tan_h = 1, tan_x = 1, tan_y = 1;
                 if (cam->focal_length > 0) {

@@ -36,6 +36,8 @@ typedef struct OracleScene OracleScene;
 OracleScene* oracle_scene_create(const SheenScene* scene);
 void oracle_scene_destroy(OracleScene* s);
 int oracle_scene_photon_count(const OracleScene* s);
+/* Extension: camera samples without jitter (the library's "camera.centered"). */
+void oracle_scene_set_centered(OracleScene* s, int centered);
 
 /* RGBA (width*height*4 floats) for pixel rows [y0, y1) (y1 <= 0: all rows). */
 int oracle_render(const OracleScene* s, int width, int height, int aa,

@@ -197,9 +197,10 @@ __device__ float3 beams(const DevScene& S, const Ray& ray, bool hit, float t_hit
 }
 
 // Camera ray of sample (s of ns) in pixel (x, y): render_kernel.cu:491-521.
+// centered: no jitter (sample_offset_centered), an extension.
 __device__ __forceinline__ Ray camera_ray(const CameraData& cam, int x, int y, int s, int ns, int W, int H,
-                                          float& pix_angle) {
-    float2 off = sample_offset(s, ns, x, y);
+                                          float& pix_angle, int centered) {
+    float2 off = centered ? sample_offset_centered(s, ns) : sample_offset(s, ns, x, y);
     float u = (float(x) + off.x) / float(W) * 2.0f - 1.0f;
     float v = 1.0f - (float(y) + off.y) / float(H) * 2.0f;
     float tan_h = 1.0f, tan_x = 1.0f, tan_y = 1.0f;
@@ -227,7 +228,7 @@ template <class T, bool COUNT>
 __device__ float3 render_sample(const DevScene& S, int x, int y, int s, int ns, int W, int H,
                                 RayTally& rt, Counters& c) {
     float pix;
-    const Ray ray = camera_ray(S.cam, x, y, s, ns, W, H, pix);
+    const Ray ray = camera_ray(S.cam, x, y, s, ns, W, H, pix, S.aa_centered);
     const uint32_t seed = sample_seed(x, y, s);
     Hit rec;
     rt.primary++;

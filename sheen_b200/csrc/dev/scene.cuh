@@ -85,6 +85,7 @@ struct DevScene {
     //             closest-hit shadow queries, usually a small set
     QMesh q_all, q_block, q_pass;
     int has_glass;                 // any material with transmission > 0
+    int aa_centered;               // camera samples without jitter (extension; 0: the reference's jitter)
 };
 
 struct Ray {

@@ -65,5 +65,16 @@ __device__ __forceinline__ float2 sample_offset(int s, int n, int x, int y) {
     return make_float2((float(s % side) + jx) * inv, (float(s / side) + jy) * inv);
 }
 
+// Sample positions without jitter (a scene created with "camera.centered"):
+// the pixel centre at 1 spp, otherwise the centres of the same cells.
+__device__ __forceinline__ float2 sample_offset_centered(int s, int n) {
+    if (n <= 1) return make_float2(0.5f, 0.5f);
+    if (n <= 4) return make_float2((s == 0 || s == 2) ? 0.25f : 0.75f, (s < 2) ? 0.25f : 0.75f);
+    int side = 2;
+    while (side * side < n) side++;
+    const float inv = 1.0f / (float)side;
+    return make_float2((float(s % side) + 0.5f) * inv, (float(s / side) + 0.5f) * inv);
+}
+
 }  // namespace dev
 }  // namespace sheen

@@ -161,6 +161,7 @@ struct Tuning {
     int build_concurrent = 1;       // device build: the subset trees beside the full tree (2 host threads)
     int pool_keep_mb = 16384;       // freed device memory the library's pool keeps for reuse
     int watertight = 0;             // wavefront triangle test: 0 Moller-Trumbore (the reference's), 1 watertight
+    int aa_centered = 0;            // camera samples: 0 the reference's jitter, 1 cell centres
 };
 Tuning tuning();
 int tuning_generation();

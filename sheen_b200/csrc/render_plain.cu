@@ -58,7 +58,7 @@ __global__ void primary_hits_kernel(DevScene S, int W, int H, int ns, int* obj, 
     Counters c;
     for (int s = 0; s < ns; s++) {
         float pix;
-        const Ray r = camera_ray(S.cam, x, y, s, ns, W, H, pix);
+        const Ray r = camera_ray(S.cam, x, y, s, ns, W, H, pix, S.aa_centered);
         Hit h;
         const size_t k = ((size_t)y * W + x) * ns + s;
         if (T::closest(S, r, h, c)) { obj[k] = h.obj; mat[k] = h.mat; tt[k] = h.t; }

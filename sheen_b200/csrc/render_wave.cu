@@ -225,7 +225,7 @@ __device__ __forceinline__ void primary_item(const DevScene& S, const WaveView& 
     uint32_t seed = 0;
     if (active) {
         float pix;
-        ray = camera_ray(S.cam, x, y, s, V.ns, V.W, V.H, pix);
+        ray = camera_ray(S.cam, x, y, s, V.ns, V.W, V.H, pix, S.aa_centered);
         seed = sample_seed(x, y, s);
         hit = T::closest(S, ray, rec, c);
     }

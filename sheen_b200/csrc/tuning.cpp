@@ -33,6 +33,7 @@ const Key kKeys[] = {
     {"build.concurrent", &Tuning::build_concurrent, 0, 1},
     {"mem.pool_keep_mb", &Tuning::pool_keep_mb, 0, 1 << 20},
     {"trace.watertight", &Tuning::watertight, 0, 1},
+    {"camera.centered", &Tuning::aa_centered, 0, 1},
 };
 
 }  // namespace

@@ -43,14 +43,30 @@ class Oracle:
         L.oracle_primary_hits.restype = I
         L.oracle_trace.argtypes = [P, I, P, P, P, P, I]
         L.oracle_trace.restype = I
+        L.oracle_scene_set_centered.argtypes = [P, I]
+        L.oracle_scene_set_centered.restype = None
 
-    def scene(self, view_ptr: int):
-        return _Handle(self.lib, self.lib.oracle_scene_create(view_ptr), self.lib.oracle_scene_destroy)
+    def scene(self, view_ptr: int, centered: bool = False):
+        h = _Handle(self.lib, self.lib.oracle_scene_create(view_ptr), self.lib.oracle_scene_destroy)
+        if centered:
+            self.lib.oracle_scene_set_centered(h.ptr, 1)
+        return h
 
     def render(self, h, W, H, aa, y0=0, y1=0, threads=0):
         out = np.zeros((H, W, 4), np.float32)
         assert self.lib.oracle_render(h.ptr, W, H, aa, out.ctypes.data, y0, y1, threads) == 0
         return out
+
+    def trace(self, h, rays, threads=0):
+        """Closest hits of rays given as (n, 6) doubles (origin, direction)."""
+        rays = np.ascontiguousarray(rays, dtype=np.float64).reshape(-1, 6)
+        n = len(rays)
+        cat = np.zeros(n, np.int32)
+        prim = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float64)
+        assert self.lib.oracle_trace(h.ptr, n, rays.ctypes.data, cat.ctypes.data, prim.ctypes.data, t.ctypes.data,
+                                     threads) == 0
+        return cat, prim, t
 
     def primary_hits(self, h, W, H, aa, threads=0):
         ns = max(1, min(aa, 64))
