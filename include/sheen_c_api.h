@@ -318,8 +318,14 @@ int sheen_scene_profile_stages(SheenDeviceScene scene, int width, int height, in
  *                                   (sampling/aa.h:45-58); 1: no jitter --
  *                                   the pixel centre at 1 spp, cell centres
  *                                   otherwise.  Read at sheen_scene_create.
- * Every other setting gives the same image (watertight and centered change
- * it on purpose); only the speed differs.  0 / -1. */
+ *   "trace.se_polish"            0 (default): a superellipsoid entry lies on
+ *                                   the sample where the reference's 32-step
+ *                                   march finds it (superellipsoid.h:100-
+ *                                   112); 1: refined in FP64 (safeguarded
+ *                                   Newton) onto the surface.  Read at
+ *                                   sheen_scene_create.
+ * Every other setting gives the same image (watertight, centered and
+ * se_polish change it on purpose); only the speed differs.  0 / -1. */
 int sheen_tune_set(const char* key, int value);
 int sheen_tune_get(const char* key, int* value);
 

@@ -369,7 +369,7 @@ __device__ __forceinline__ void se_chord(const Ray& r, const Superellipsoid& s, 
 // found by sampling is not refined (its bisection interval is empty), so
 // the entry lies on a sample.
 __device__ __forceinline__ bool se_span(const Ray& r, const Superellipsoid& s, float t0, float t1,
-                                        float& te, float& tx) {
+                                        float& te, float& tx, float* te_prev = nullptr) {
     float tA, tB;
     se_chord(r, s, tA, tB);
     if (tB < t0 || tA > t1 || tB < tA) return false;
@@ -380,6 +380,7 @@ __device__ __forceinline__ bool se_span(const Ray& r, const Superellipsoid& s, f
     bool inside = se_value(s, r.o + tp * r.d) <= 1.0f;
     bool found_in = inside, found_out = false;
     te = inside ? t0 : -1e30f;
+    if (te_prev) *te_prev = te;   // the last sample outside before the entry (te itself: no bracket)
     tx = -1e30f;
     for (int i = 1; i <= 32 && !found_out; i++) {
         float t = fminf(t0 + step * (float)i, t1);
@@ -394,27 +395,60 @@ __device__ __forceinline__ bool se_span(const Ray& r, const Superellipsoid& s, f
             found_out = true;
             break;
         }
-        tp = t;
         if (!inside && F <= 1.0f) {
             te = fmaxf(t, t0);   // bisection over [t, t] in the reference
+            if (te_prev) *te_prev = tp;
             found_in = true;
             inside = true;
         }
+        tp = t;
     }
     if (!found_in) return false;
     if (!found_out) tx = t1;
     return te <= tx;
 }
 
+// Extension (a scene created with "trace.se_polish"; the reference has
+// none): the entry that the sampling above leaves on a sample is refined in
+// FP64 -- safeguarded Newton on G(t) = F(o + t d) - 1 inside the bracket
+// [last outside sample, first inside sample], bisection whenever a Newton
+// step leaves the bracket -- so the hit lies on the surface instead of up
+// to one sample step (1/32 of the chord) inside it.
+static __device__ __noinline__ float se_polish_entry(const Ray& r, const Superellipsoid& s, float t_out, float t_in) {
+    const double ox = (double)r.o.x - s.center.x, oy = (double)r.o.y - s.center.y, oz = (double)r.o.z - s.center.z;
+    const double dx = r.d.x, dy = r.d.y, dz = r.d.z;
+    const double ia = 1.0 / s.a, ib = 1.0 / s.b, ic = 1.0 / s.c, n = s.n;
+    auto G = [&](double t, double& dG) {
+        const double qx = (ox + t * dx) * ia, qy = (oy + t * dy) * ib, qz = (oz + t * dz) * ic;
+        const double ax = fabs(qx), ay = fabs(qy), az = fabs(qz);
+        const double px = pow(ax, n - 1.0), py = pow(ay, n - 1.0), pz = pow(az, n - 1.0);
+        dG = n * (px * copysign(1.0, qx) * dx * ia + py * copysign(1.0, qy) * dy * ib + pz * copysign(1.0, qz) * dz * ic);
+        return px * ax + py * ay + pz * az - 1.0;
+    };
+    double lo = t_out, hi = t_in, x = t_in, dG = 0.0;
+    double g = G(x, dG);
+    for (int k = 0; k < 60 && hi - lo > 1e-13 * fmax(fabs(hi), 1.0); k++) {
+        double xn = (dG != 0.0) ? x - g / dG : 0.5 * (lo + hi);
+        if (!(xn > lo && xn < hi)) xn = 0.5 * (lo + hi);
+        x = xn;
+        g = G(x, dG);
+        if (g > 0.0) lo = x;
+        else hi = x;
+        if (g == 0.0) break;
+    }
+    return (float)hi;
+}
+
 // primitives/superellipsoid.h:123-161
-__device__ __forceinline__ bool se_test(const Ray& r, const Superellipsoid& s, Hit& h) {
+__device__ __forceinline__ bool se_test(const Ray& r, const Superellipsoid& s, Hit& h, int polish = 0) {
     float t0, t1;
     se_chord(r, s, t0, t1);
     if (t1 < r.tmin || t0 > r.tmax || t1 < t0) return false;
     t0 = fmaxf(t0, r.tmin);
     t1 = fminf(t1, r.tmax);
-    float te, tx;
-    if (!se_span(r, s, t0, t1, te, tx)) return false;
+    float te, tx, te_prev;
+    if (!se_span(r, s, t0, t1, te, tx, &te_prev)) return false;
+    if (polish && te_prev < te) te = se_polish_entry(r, s, te_prev, te);
     h.t = te;
     h.p = r.o + te * r.d;
     h.n = normalize(se_gradient(s, h.p));

@@ -86,6 +86,7 @@ struct DevScene {
     QMesh q_all, q_block, q_pass;
     int has_glass;                 // any material with transmission > 0
     int aa_centered;               // camera samples without jitter (extension; 0: the reference's jitter)
+    int se_polish;                 // FP64 Newton polish of superellipsoid entries (extension; 0: off)
 };
 
 struct Ray {

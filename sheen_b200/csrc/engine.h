@@ -162,6 +162,7 @@ struct Tuning {
     int pool_keep_mb = 16384;       // freed device memory the library's pool keeps for reuse
     int watertight = 0;             // wavefront triangle test: 0 Moller-Trumbore (the reference's), 1 watertight
     int aa_centered = 0;            // camera samples: 0 the reference's jitter, 1 cell centres
+    int se_polish = 0;              // superellipsoid entries: 0 on a sample (reference), 1 FP64 Newton polish
 };
 Tuning tuning();
 int tuning_generation();

@@ -34,6 +34,7 @@ const Key kKeys[] = {
     {"mem.pool_keep_mb", &Tuning::pool_keep_mb, 0, 1 << 20},
     {"trace.watertight", &Tuning::watertight, 0, 1},
     {"camera.centered", &Tuning::aa_centered, 0, 1},
+    {"trace.se_polish", &Tuning::se_polish, 0, 1},
 };
 
 }  // namespace

@@ -70,3 +70,80 @@ def test_centered_camera_matches_oracle(form, aa):
     jit, _ = ds2.render_host(W, H, aa)
     ds2.close()
     assert not np.array_equal(img, jit)
+
+
+# ---- trace.se_polish ---------------------------------------------------------
+#
+# The reference marches 32 samples along the superellipsoid's box chord and
+# keeps the first inside sample as the entry (superellipsoid.h:100-112: the
+# bisection there runs over an empty interval), so a hit can lie up to 1/32
+# of the chord inside the surface.  With trace.se_polish the entry is refined
+# in FP64 onto the surface.  Truth here: the first root of
+# G(t) = |qx|^n + |qy|^n + |qz|^n - 1 along the ray in float64 (dense
+# sampling, then brentq).
+
+from sheen_b200 import contract as C
+
+
+def _se_scene(seed=5, count=24):
+    rng = np.random.default_rng(seed)
+    s = C.SceneArrays()
+    se = np.zeros(count, C.SUPERELLIPSOID)
+    se["center"] = rng.uniform(-8, 8, (count, 3)).astype(np.float32)
+    se["a"], se["b"], se["c"] = (rng.uniform(0.6, 1.6, count).astype(np.float32) for _ in range(3))
+    se["n"] = rng.uniform(1.2, 8.0, count).astype(np.float32)
+    s.superellipsoids = se
+    s.materials = C.default_material()
+    return s, se
+
+
+def _true_entry(o, d, se, t_hint):
+    from scipy.optimize import brentq
+    c = se["center"].astype(np.float64)
+    ax = np.array([se["a"], se["b"], se["c"]], np.float64)
+    n = float(se["n"])
+    G = lambda t: float(np.sum(np.abs((o + t * d - c) / ax) ** n) - 1.0)
+    ts = np.linspace(max(t_hint - 4.0, 1e-3), t_hint + 4.0, 20001)
+    g = np.sum(np.abs((o[None] + ts[:, None] * d[None] - c) / ax) ** n, axis=1) - 1.0
+    k = np.nonzero((g[:-1] > 0) & (g[1:] <= 0))[0]
+    if len(k) == 0:
+        return None
+    return brentq(G, ts[k[0]], ts[k[0] + 1], xtol=1e-15, rtol=1e-15)
+
+
+@pytest.mark.gpu
+def test_se_polish_puts_hits_on_the_surface():
+    sb.init(0, 100)
+    scene, se = _se_scene()
+    rng = np.random.default_rng(9)
+    rays, target = [], []
+    for i in range(len(se)):
+        for _ in range(40):
+            o = rng.uniform(-20, 20, 3)
+            aim = se["center"][i].astype(np.float64) + rng.normal(0, 0.3, 3)
+            d = aim - o
+            d /= np.linalg.norm(d)
+            rays.append(np.r_[o, 1e-3, d, 1e10])
+            target.append(i)
+    rays = np.array(rays, np.float32)
+    errs = {}
+    for polish in (0, 1):
+        ds = _with_tuning("trace.se_polish", polish, lambda: sb.DeviceScene(scene, sb.FORM_WAVEFRONT))
+        obj, mat, t = ds.trace(rays)
+        ds.close()
+        rel = []
+        for k in range(len(rays)):
+            if t[k] <= 0 or obj[k] >= 0:
+                continue
+            i = -obj[k] - 1
+            o = rays[k, :3].astype(np.float64)
+            d = rays[k, 4:7].astype(np.float64)
+            tt = _true_entry(o, d, se[i], float(t[k]))
+            if tt is not None:
+                rel.append(abs(t[k] - tt) / tt)
+        rel = np.array(rel)
+        assert len(rel) > 0.5 * len(rays)
+        errs[polish] = (float(np.median(rel)), float(rel.max()))
+    print(f"hit-t relative error vs the true surface: reference entry (median, max) {errs[0]}, "
+          f"polished {errs[1]}")
+    assert errs[1][1] < 1e-5 and errs[1][1] < errs[0][1] / 100
