@@ -324,8 +324,15 @@ int sheen_scene_profile_stages(SheenDeviceScene scene, int width, int height, in
  *                                   112); 1: refined in FP64 (safeguarded
  *                                   Newton) onto the surface.  Read at
  *                                   sheen_scene_create.
- * Every other setting gives the same image (watertight, centered and
- * se_polish change it on purpose); only the speed differs.  0 / -1. */
+ *   "caustic.knn"                0 (default): the reference's caustic gather
+ *                                   (the first <= 128 photons within
+ *                                   cell / 2, render_kernel.h:68-111);
+ *                                   k = 1..64: the k nearest photons within
+ *                                   r_max = cell / 2, the estimate's radius
+ *                                   the k-th distance.  Read at
+ *                                   sheen_scene_create.
+ * Every other setting gives the same image (watertight, centered, se_polish
+ * and knn change it on purpose); only the speed differs.  0 / -1. */
 int sheen_tune_set(const char* key, int value);
 int sheen_tune_get(const char* key, int* value);
 
@@ -385,6 +392,12 @@ int sheen_generate_scene(int config, unsigned int seed, int detail, int photons,
 
 /* 8-bit sRGB PNG writer used by sheen_render_scene (png_color.h:11-20 conversion). */
 int sheen_write_png_srgb(const char* path, const float* rgba, int width, int height);
+
+/* The conversion's byte steps: out[b - 1] = the smallest non-negative float
+ * whose sRGB byte is >= b, b = 1..255 (255 floats).  sheen_render_scene packs
+ * on the device by searching these, which gives the host conversion's bytes
+ * exactly.  No counterpart in the reference (it converts on the host). */
+void sheen_srgb_thresholds(float* out);
 
 /* ------------------------------------------------------------------ */
 /* Request loop (continuous batching).  No counterpart in the reference, */

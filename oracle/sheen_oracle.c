@@ -121,6 +121,7 @@ struct OracleScene {
     sheen_float3* ph_pos; sheen_float3* ph_dir; sheen_float3* ph_nrm; sheen_float3* ph_flux;
     int nph; int* cell_start; int* cell_count; int num_cells; real cell;
     int centered;                       /* samples without jitter (extension) */
+    int knn;                            /* k-nearest-photon gather (extension; 0: the reference's) */
 };
 
 static void sample_pos(const OracleScene* S, int s, int n, int x, int y, real* ox, real* oy) {
@@ -1120,6 +1121,65 @@ static V photon_gather(const OracleScene* S, V p, V n, real radius, int max_samp
     return acc;
 }
 
+/* Extension (no reference counterpart): the k nearest photons within rmax
+ * facing n, found by a full sort of the candidates' squared distances (the
+ * library uses a heap); the estimate's radius is the k-th distance, or rmax
+ * when fewer are found.  Returns their flux sum, *r2 the radius squared. */
+static int cmp_real(const void* a, const void* b) {
+    const real x = *(const real*)a, y = *(const real*)b;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+static V photon_knn(const OracleScene* S, V p, V n, real rmax, int k, real* r2_out) {
+    V acc = v3(0, 0, 0);
+    *r2_out = rmax * rmax;
+    if (!S->nph || S->num_cells <= 0 || S->cell <= 0 || k <= 0) return acc;
+    real c = S->cell;
+    int x0 = (int)floor((p.x - rmax) / c), x1 = (int)floor((p.x + rmax) / c);
+    int y0 = (int)floor((p.y - rmax) / c), y1 = (int)floor((p.y + rmax) / c);
+    int z0 = (int)floor((p.z - rmax) / c), z1 = (int)floor((p.z + rmax) / c);
+    int cells[27], nc = 0;
+    for (int iz = z0; iz <= z1; iz++)
+        for (int iy = y0; iy <= y1; iy++)
+            for (int ix = x0; ix <= x1; ix++) {
+                int hc = cell_hash(ix, iy, iz, S->num_cells), seen = 0;
+                for (int q = 0; q < nc; q++) if (cells[q] == hc) { seen = 1; break; }
+                if (!seen && nc < 27) cells[nc++] = hc;
+            }
+    real rmax2 = rmax * rmax;
+    int total = 0;
+    for (int q = 0; q < nc; q++) total += S->cell_count[cells[q]];
+    real* d2s = (real*)malloc(sizeof(real) * (size_t)(total > 0 ? total : 1));
+    int m = 0;
+    for (int q = 0; q < nc; q++) {
+        int st = S->cell_start[cells[q]], cnt = S->cell_count[cells[q]];
+        for (int j = 0; j < cnt; j++) {
+            V d = sub(fv(S->ph_pos[st + j]), p);
+            real d2 = dot(d, d);
+            if (d2 > rmax2) continue;
+            if (dot(fv(S->ph_nrm[st + j]), n) < R(0.1)) continue;
+            d2s[m++] = d2;
+        }
+    }
+    real r2 = rmax2;
+    if (m >= k) {
+        qsort(d2s, (size_t)m, sizeof(real), cmp_real);
+        r2 = d2s[k - 1];
+    }
+    free(d2s);
+    *r2_out = r2;
+    for (int q = 0; q < nc; q++) {
+        int st = S->cell_start[cells[q]], cnt = S->cell_count[cells[q]];
+        for (int j = 0; j < cnt; j++) {
+            V d = sub(fv(S->ph_pos[st + j]), p);
+            if (dot(d, d) > r2) continue;
+            if (dot(fv(S->ph_nrm[st + j]), n) < R(0.1)) continue;
+            acc = add(acc, fv(S->ph_flux[st + j]));
+        }
+    }
+    return acc;
+}
+
 static V up_for(V a) { return fabs(a.y) < R(0.9) ? v3(0, 1, 0) : v3(1, 0, 0); }
 
 /* render_kernel.cu:13-24 */
@@ -1273,8 +1333,14 @@ static V lighting(const OracleScene* S, const Hit* rec, V view, real footprint, 
     }
     if (S->nph && S->s.caustics > 0) {
         real r = S->cell * R(0.5);
-        V flux = photon_gather(S, rec->p, rec->n, r, 128);
-        result = add(result, mul(vmul(base, flux), S->s.caustics / (R(9.8696044) * r * r)));
+        if (S->knn > 0) {
+            real r2;
+            V flux = photon_knn(S, rec->p, rec->n, r, S->knn, &r2);
+            result = add(result, mul(vmul(base, flux), S->s.caustics / (R(9.8696044) * r2)));
+        } else {
+            V flux = photon_gather(S, rec->p, rec->n, r, 128);
+            result = add(result, mul(vmul(base, flux), S->s.caustics / (R(9.8696044) * r * r)));
+        }
     }
     return result;
 }
@@ -1712,6 +1778,10 @@ int oracle_scene_photon_count(const OracleScene* S) { return S ? S->nph : 0; }
 
 void oracle_scene_set_centered(OracleScene* S, int centered) {
     if (S) S->centered = centered;
+}
+
+void oracle_scene_set_knn(OracleScene* S, int k) {
+    if (S) S->knn = k;
 }
 
 int oracle_render(const OracleScene* S, int W, int H, int aa, float* out, int y0, int y1, int nthreads) {

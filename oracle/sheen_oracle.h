@@ -38,6 +38,8 @@ void oracle_scene_destroy(OracleScene* s);
 int oracle_scene_photon_count(const OracleScene* s);
 /* Extension: camera samples without jitter (the library's "camera.centered"). */
 void oracle_scene_set_centered(OracleScene* s, int centered);
+/* Extension: k-nearest-photon caustic gather (the library's "caustic.knn"). */
+void oracle_scene_set_knn(OracleScene* s, int k);
 
 /* RGBA (width*height*4 floats) for pixel rows [y0, y1) (y1 <= 0: all rows). */
 int oracle_render(const OracleScene* s, int width, int height, int aa,

@@ -336,12 +336,32 @@ int sheen_render_scene_rgba(const SheenScene* scene, int W, int H, int aa, int f
     return rc;
 }
 
+// The drop-in call: plain form, 8-bit sRGB PNG.  The image is converted on
+// the device (the host conversion's exact bytes) and read back as PNG rows,
+// 3 bytes a pixel instead of the float4 image.
 int sheen_render_scene(const SheenScene* scene, int W, int H, int aa, const char* path) {
     if (check_params(scene, W, H, aa) != 0) return -1;
     if (!path) { sheen::set_error("bad render params"); return -1; }
-    std::vector<float> rgba((size_t)W * H * 4);
-    if (sheen_render_scene_rgba(scene, W, H, aa, SHEEN_FORM_PLAIN, rgba.data(), nullptr) != 0) return -1;
-    return sheen_write_png_srgb(path, rgba.data(), W, H);
+    sheen::DeviceScene* s = nullptr;
+    if (sheen::scene_upload(scene, SHEEN_FORM_PLAIN, &s) != 0) return -1;
+    float4* img = nullptr;
+    unsigned char* rows = nullptr;
+    const size_t row_bytes = (size_t)H * (1 + 3 * (size_t)W);
+    std::vector<unsigned char> host_rows(row_bytes);
+    cudaError_t e = sheen::dmalloc(&img, (size_t)W * H * sizeof(float4));
+    if (e == cudaSuccess) e = sheen::dmalloc(&rows, row_bytes);
+    int rc = e == cudaSuccess ? 0 : fail_cuda(e);
+    if (rc == 0) rc = render_device(*s, W, H, aa, sheen::Region{0, 0, W, H}, img, 0, 0, nullptr);
+    if (rc == 0) {
+        e = sheen::pack_srgb_rows(img, W, H, rows, 0);
+        if (e == cudaSuccess) e = cudaMemcpy(host_rows.data(), rows, row_bytes, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = fail_cuda(e);
+    }
+    sheen::dfree(img);
+    sheen::dfree(rows);
+    sheen::scene_release(s);
+    if (rc != 0) return rc;
+    return sheen::write_png_rows(path, host_rows.data(), W, H);
 }
 
 }  // extern "C"

@@ -87,6 +87,7 @@ struct DevScene {
     int has_glass;                 // any material with transmission > 0
     int aa_centered;               // camera samples without jitter (extension; 0: the reference's jitter)
     int se_polish;                 // FP64 Newton polish of superellipsoid entries (extension; 0: off)
+    int caustic_knn;               // k-nearest-photon gather (extension; 0: the reference's gather)
 };
 
 struct Ray {

@@ -313,9 +313,89 @@ __device__ __forceinline__ float3 photon_gather(const PhotonMapView& m, float3 p
     return acc;
 }
 
+// Extension (a scene created with "caustic.knn" = k, 1..64; the reference
+// gathers the first <= 128 photons within r = cell / 2): the k nearest
+// photons within r_max = cell / 2 facing the normal.  Pass 1 keeps the k
+// smallest squared distances in a max-heap; pass 2 sums the flux of every
+// photon within the k-th distance (ties included).  The radius of the
+// estimate is that distance, or r_max when fewer than k photons are found;
+// the flux goes through the reference's estimate flux / (pi^2 r^2).
+constexpr int kKnnMax = 64;
+__device__ __forceinline__ float3 photon_knn(const PhotonMapView& m, float3 p, float3 n, float rmax, int k,
+                                                 float& r2_used) {
+    float3 acc = f3(0.0f, 0.0f, 0.0f);
+    r2_used = rmax * rmax;
+    if (!m.pos || m.num_cells <= 0 || m.cell_size <= 0.0f || k <= 0) return acc;
+    k = k > kKnnMax ? kKnnMax : k;
+    const int x0 = (int)floorf((p.x - rmax) / m.cell_size), x1 = (int)floorf((p.x + rmax) / m.cell_size);
+    const int y0 = (int)floorf((p.y - rmax) / m.cell_size), y1 = (int)floorf((p.y + rmax) / m.cell_size);
+    const int z0 = (int)floorf((p.z - rmax) / m.cell_size), z1 = (int)floorf((p.z + rmax) / m.cell_size);
+    int cells[27], nc = 0;
+    for (int iz = z0; iz <= z1; iz++)
+        for (int iy = y0; iy <= y1; iy++)
+            for (int ix = x0; ix <= x1; ix++) {
+                const int c = photon_cell(ix, iy, iz, m.num_cells);
+                bool seen = false;
+                for (int q = 0; q < nc; q++) seen |= (cells[q] == c);
+                if (!seen && nc < 27) cells[nc++] = c;
+            }
+    float heap[kKnnMax];
+    int hn = 0;
+    const float rmax2 = rmax * rmax;
+    for (int q = 0; q < nc; q++) {
+        const int st = m.cell_start[cells[q]], cnt = m.cell_count[cells[q]];
+        for (int j = 0; j < cnt; j++) {
+            const float4 pp = __ldg(&m.pos[st + j]);
+            const float3 d = f3(pp.x, pp.y, pp.z) - p;
+            const float d2 = dot(d, d);
+            if (d2 > rmax2) continue;
+            const float4 pn = __ldg(&m.nrm[st + j]);
+            if (dot(f3(pn.x, pn.y, pn.z), n) < 0.1f) continue;
+            if (hn < k) {   // push, sift up
+                int i = hn++;
+                while (i > 0 && heap[(i - 1) / 2] < d2) { heap[i] = heap[(i - 1) / 2]; i = (i - 1) / 2; }
+                heap[i] = d2;
+            } else if (d2 < heap[0]) {   // replace the largest, sift down
+                int i = 0;
+                while (true) {
+                    const int l = 2 * i + 1, r = l + 1;
+                    int big = i;
+                    float vb = d2;
+                    if (l < hn && heap[l] > vb) { big = l; vb = heap[l]; }
+                    if (r < hn && heap[r] > vb) { big = r; vb = heap[r]; }
+                    if (big == i) break;
+                    heap[i] = heap[big];
+                    i = big;
+                }
+                heap[i] = d2;
+            }
+        }
+    }
+    const float r2 = hn < k ? rmax2 : heap[0];
+    r2_used = r2;
+    for (int q = 0; q < nc; q++) {
+        const int st = m.cell_start[cells[q]], cnt = m.cell_count[cells[q]];
+        for (int j = 0; j < cnt; j++) {
+            const float4 pp = __ldg(&m.pos[st + j]);
+            const float3 d = f3(pp.x, pp.y, pp.z) - p;
+            if (dot(d, d) > r2) continue;
+            const float4 pn = __ldg(&m.nrm[st + j]);
+            if (dot(f3(pn.x, pn.y, pn.z), n) < 0.1f) continue;
+            const float4 pf = __ldg(&m.flux[st + j]);
+            acc += f3(pf.x, pf.y, pf.z);
+        }
+    }
+    return acc;
+}
+
 __device__ __forceinline__ float3 caustic_term(const DevScene& S, const ShadePoint& sp) {
     if (!S.pmap.pos || S.caustics <= 0.0f) return f3(0.0f, 0.0f, 0.0f);
     const float r = S.pmap.cell_size * 0.5f;
+    if (S.caustic_knn > 0) {
+        float r2 = r * r;
+        const float3 flux = photon_knn(S.pmap, sp.p, sp.ng, r, S.caustic_knn, r2);
+        return sp.base * flux * (S.caustics / (9.8696044f * r2));
+    }
     float3 flux = photon_gather(S.pmap, sp.p, sp.ng, r, 128);
     return sp.base * flux * (S.caustics / (9.8696044f * r * r));
 }

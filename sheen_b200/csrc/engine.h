@@ -163,6 +163,7 @@ struct Tuning {
     int watertight = 0;             // wavefront triangle test: 0 Moller-Trumbore (the reference's), 1 watertight
     int aa_centered = 0;            // camera samples: 0 the reference's jitter, 1 cell centres
     int se_polish = 0;              // superellipsoid entries: 0 on a sample (reference), 1 FP64 Newton polish
+    int caustic_knn = 0;            // caustic gather: 0 the reference's, k in 1..64 the k nearest photons
 };
 Tuning tuning();
 int tuning_generation();
@@ -174,6 +175,11 @@ int tuning_get(const char* name, int* value);
 int build_photon_map_device(DeviceScene& s, int per_light, float cell);
 
 double now_ms();
+
+// PNG path (png.cpp, png_pack.cu): the float4 image packed into PNG raw rows
+// (h rows of 1 + 3w bytes) on the device, and a PNG written from such rows.
+cudaError_t pack_srgb_rows(const float4* img, int W, int H, unsigned char* rows, cudaStream_t stream);
+int write_png_rows(const char* path, const unsigned char* rows, int w, int h);
 
 // Device memory of the library (mem.cpp): a stream-ordered pool per device
 // that keeps freed blocks mapped for reuse.  dmalloc's block is usable on

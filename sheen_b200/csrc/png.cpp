@@ -2,7 +2,11 @@
 //
 // Conversion per channel as png_color.h:11-20 (clamp, sRGB curve, +0.5,
 // truncate); the file is a plain RGB8 PNG (IHDR, one zlib IDAT, IEND) with
-// filter 0 rows.
+// filter 0 rows.  The conversion is a non-decreasing step function of the
+// linear value, so it is also given as the 255 thresholds at which the byte
+// steps up (srgb_thresholds): the device packs pixels by searching them
+// (png_pack.cu), which yields exactly the bytes of this host conversion
+// without evaluating pow on the device.
 #include <zlib.h>
 
 #include <cmath>
@@ -27,6 +31,28 @@ static unsigned char srgb_byte(float c) {
     return (unsigned char)(v > 255.0f ? 255.0f : v);
 }
 
+// thr[b - 1] = the smallest non-negative float whose byte is >= b, for
+// b = 1..255 (found by bisection over the ordered bit patterns of [0, 1]).
+const float* srgb_thresholds() {
+    static float thr[255];
+    static bool ready = [] {
+        for (int b = 1; b <= 255; b++) {
+            uint32_t lo = 0, hi = 0x3f800000u;   // srgb_byte(1.0f) == 255 >= b
+            while (lo < hi) {
+                const uint32_t mid = lo + (hi - lo) / 2;
+                float f;
+                std::memcpy(&f, &mid, 4);
+                if (srgb_byte(f) >= b) hi = mid;
+                else lo = mid + 1;
+            }
+            std::memcpy(&thr[b - 1], &lo, 4);
+        }
+        return true;
+    }();
+    (void)ready;
+    return thr;
+}
+
 static void put32(std::vector<unsigned char>& b, uint32_t v) {
     b.push_back((unsigned char)(v >> 24)); b.push_back((unsigned char)(v >> 16));
     b.push_back((unsigned char)(v >> 8)); b.push_back((unsigned char)v);
@@ -42,18 +68,9 @@ static void chunk(std::vector<unsigned char>& out, const char* tag, const unsign
     put32(out, (uint32_t)crc);
 }
 
-}  // namespace sheen
-
-extern "C" int sheen_write_png_srgb(const char* path, const float* rgba, int w, int h) {
-    using namespace sheen;
-    if (!path || !rgba || w <= 0 || h <= 0) { set_error("bad png params"); return -1; }
-    std::vector<unsigned char> raw((size_t)h * (1 + (size_t)w * 3));
-    for (int y = 0; y < h; y++) {
-        unsigned char* row = raw.data() + (size_t)y * (1 + (size_t)w * 3);
-        row[0] = 0;
-        for (int x = 0; x < w; x++)
-            for (int c = 0; c < 3; c++) row[1 + 3 * x + c] = srgb_byte(rgba[4 * ((size_t)y * w + x) + c]);
-    }
+// Writes a PNG from raw filter-0 rows (h rows of 1 + 3w bytes).
+int write_png_rows(const char* path, const unsigned char* rows, int w, int h) {
+    std::vector<unsigned char> raw(rows, rows + (size_t)h * (1 + (size_t)w * 3));
     uLongf zlen = compressBound((uLong)raw.size());
     std::vector<unsigned char> z(zlen);
     if (compress2(z.data(), &zlen, raw.data(), (uLong)raw.size(), 6) != Z_OK) { set_error("png deflate failed"); return -1; }
@@ -71,4 +88,25 @@ extern "C" int sheen_write_png_srgb(const char* path, const float* rgba, int w, 
     std::fclose(f);
     if (wr != out.size()) { set_error("stbi_write_png failed"); return -1; }
     return 0;
+}
+
+}  // namespace sheen
+
+extern "C" void sheen_srgb_thresholds(float* out) {
+    if (!out) return;
+    const float* t = sheen::srgb_thresholds();
+    for (int i = 0; i < 255; i++) out[i] = t[i];
+}
+
+extern "C" int sheen_write_png_srgb(const char* path, const float* rgba, int w, int h) {
+    using namespace sheen;
+    if (!path || !rgba || w <= 0 || h <= 0) { set_error("bad png params"); return -1; }
+    std::vector<unsigned char> raw((size_t)h * (1 + (size_t)w * 3));
+    for (int y = 0; y < h; y++) {
+        unsigned char* row = raw.data() + (size_t)y * (1 + (size_t)w * 3);
+        row[0] = 0;
+        for (int x = 0; x < w; x++)
+            for (int c = 0; c < 3; c++) row[1 + 3 * x + c] = srgb_byte(rgba[4 * ((size_t)y * w + x) + c]);
+    }
+    return write_png_rows(path, raw.data(), w, h);
 }

@@ -35,6 +35,7 @@ const Key kKeys[] = {
     {"trace.watertight", &Tuning::watertight, 0, 1},
     {"camera.centered", &Tuning::aa_centered, 0, 1},
     {"trace.se_polish", &Tuning::se_polish, 0, 1},
+    {"caustic.knn", &Tuning::caustic_knn, 0, 64},
 };
 
 }  // namespace

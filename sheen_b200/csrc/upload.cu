@@ -443,6 +443,7 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     v.has_glass = has_glass ? 1 : 0;
     v.aa_centered = tuning().aa_centered;
     v.se_polish = tuning().se_polish;
+    v.caustic_knn = tuning().caustic_knn;
     s->d_tally = (unsigned long long*)dptr(o_tally);
     s->wave_depth = std::max(q_all.max_depth, std::max(q_block.max_depth, q_pass.max_depth));
     s->build_ms = t1 - t0;

@@ -45,11 +45,15 @@ class Oracle:
         L.oracle_trace.restype = I
         L.oracle_scene_set_centered.argtypes = [P, I]
         L.oracle_scene_set_centered.restype = None
+        L.oracle_scene_set_knn.argtypes = [P, I]
+        L.oracle_scene_set_knn.restype = None
 
-    def scene(self, view_ptr: int, centered: bool = False):
+    def scene(self, view_ptr: int, centered: bool = False, knn: int = 0):
         h = _Handle(self.lib, self.lib.oracle_scene_create(view_ptr), self.lib.oracle_scene_destroy)
         if centered:
             self.lib.oracle_scene_set_centered(h.ptr, 1)
+        if knn:
+            self.lib.oracle_scene_set_knn(h.ptr, knn)
         return h
 
     def render(self, h, W, H, aa, y0=0, y1=0, threads=0):

@@ -151,3 +151,55 @@ def test_png_writer(tmp_path):
     c = 0.4
     want = int((1.055 * c ** (1 / 2.4) - 0.055) * 255 + 0.5)
     assert abs(int(row[1, 0]) - want) <= 1
+
+
+def _png_rows(path):
+    """RGB8 pixels of a PNG written by this library (one IDAT, filter 0)."""
+    import struct
+    import zlib
+    b = open(path, "rb").read()
+    assert b[:8] == b"\x89PNG\r\n\x1a\n"
+    pos, idat, w, h = 8, b"", 0, 0
+    while pos < len(b):
+        n = struct.unpack(">I", b[pos:pos + 4])[0]
+        tag = b[pos + 4:pos + 8]
+        data = b[pos + 8:pos + 8 + n]
+        if tag == b"IHDR":
+            w, h = struct.unpack(">II", data[:8])
+        elif tag == b"IDAT":
+            idat += data
+        pos += 12 + n
+    raw = np.frombuffer(zlib.decompress(idat), np.uint8).reshape(h, 1 + 3 * w)
+    assert (raw[:, 0] == 0).all()
+    return raw[:, 1:].reshape(h, w, 3)
+
+
+def test_srgb_thresholds_are_the_host_conversion_steps(tmp_path):
+    """At every threshold the host conversion steps up by one byte value, so
+    counting thresholds reproduces it (the device packs that way)."""
+    L = sheen_b200.lib()
+    thr = np.zeros(255, np.float32)
+    L.sheen_srgb_thresholds.argtypes = [ctypes.c_void_p]
+    L.sheen_srgb_thresholds.restype = None
+    L.sheen_srgb_thresholds(thr.ctypes.data)
+    assert (np.diff(thr) > 0).all() and thr[-1] <= 1.0 and thr[0] > 0.0
+    below = np.nextafter(thr, np.float32(-1.0))
+    rng = np.random.default_rng(2)
+    extra = np.r_[rng.random(5000).astype(np.float32), [0.0, -1.0, 1.0, 2.0, np.inf, np.nan, 1e-30]]
+    vals = np.r_[thr, below, extra].astype(np.float32)
+    n = len(vals)
+    img = np.zeros((1, n, 4), np.float32)
+    img[0, :, 0] = vals
+    img[0, :, 1] = vals[::-1]
+    img[0, :, 2] = vals
+    p = str(tmp_path / "steps.png")
+    L.sheen_write_png_srgb.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    assert L.sheen_write_png_srgb(p.encode(), img.ctypes.data, n, 1) == 0
+    got = _png_rows(p)[0]
+    def by_table(v):
+        v = np.where(np.isnan(v) | (v <= 0), -1.0, v)
+        return np.where(v > 0, np.searchsorted(thr, v, side="right"), 0).astype(np.uint8)
+    assert np.array_equal(got[:, 0], by_table(vals))
+    assert np.array_equal(got[:, 1], by_table(vals[::-1]))
+    assert np.array_equal(got[:255, 0], np.arange(1, 256, dtype=np.uint8))   # each threshold: its byte
+    assert np.array_equal(got[255:510, 0], np.arange(0, 255, dtype=np.uint8))  # one ulp below: the byte before

@@ -147,3 +147,35 @@ def test_se_polish_puts_hits_on_the_surface():
     print(f"hit-t relative error vs the true surface: reference entry (median, max) {errs[0]}, "
           f"polished {errs[1]}")
     assert errs[1][1] < 1e-5 and errs[1][1] < errs[0][1] / 100
+
+
+# ---- caustic.knn -------------------------------------------------------------
+#
+# The caustics workload's extension: the k = 64 nearest photons within
+# r_max = cell / 2 (0.1) instead of the reference's first <= 128 photons
+# found.  The library (max-heap of distances) and the oracle (full sort of
+# the candidates) are separate implementations of the same estimate; both
+# build their photon maps from the same seeded emission.
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", [sb.FORM_PLAIN, sb.FORM_WAVEFRONT], ids=["plain", "wavefront"])
+def test_knn_caustic_gather_matches_oracle(form):
+    """200,000 photons: dense enough that 64 neighbours usually lie inside
+    r_max (at 20,000 the two estimates coincide almost everywhere).  Bar, as
+    for the other photon-map comparisons: mean absolute error and PSNR."""
+    sb.init(0, 100)
+    scene = sb.generate_scene(3, 2, 0, 200000)
+    W, H, aa = 160, 120, 1
+    ds = _with_tuning("caustic.knn", 64, lambda: sb.DeviceScene(scene, form))
+    img, _ = ds.render_host(W, H, aa)
+    ds.close()
+    o = Oracle()
+    ref = o.render(o.scene(scene.view_ptr, knn=64), W, H, aa)
+    e = image_error(img, ref)
+    print(f"knn 64 vs oracle: {e}")
+    assert e["mean_abs"] <= 2e-3 and e["psnr"] >= 40.0, e
+    ds2 = sb.DeviceScene(scene, form)
+    base, _ = ds2.render_host(W, H, aa)
+    ds2.close()
+    assert image_error(img, base)["mean_abs"] > 1e-3      # a different estimate where caustics fall

@@ -166,9 +166,16 @@ def test_full_size_workload_properties():
 
 
 def test_c_api_png(tmp_path):
+    """The drop-in PNG call packs sRGB on the device; its pixels are exactly
+    the host conversion (png_color.h:11-20) of the same render."""
+    from test_abi import _png_rows
     s = sb.generate_scene(0, 1)
     p = tmp_path / "spheres.png"
     sb.render_scene(s, 160, 120, 1, str(p))
     assert p.read_bytes()[:8] == b"\x89PNG\r\n\x1a\n"
+    img, _ = sb.render_rgba(s, 160, 120, 1, sb.FORM_PLAIN)
+    q = tmp_path / "host.png"
+    sb.write_png(str(q), img)
+    assert np.array_equal(_png_rows(str(p)), _png_rows(str(q)))
     with pytest.raises(RuntimeError, match="bad render params"):
         sb.render_scene(s, 160, 120, 0, str(p))
