@@ -105,15 +105,17 @@ __device__ __forceinline__ int bin_union(const int* A, int b0, int b1, float lo[
 // order), or INT_MAX when no split qualifies (flat axes or an empty side).
 // Every lane gets the result.  Min/max unions are exact and the counts are
 // integers, so the scan order does not change any value.
-__device__ __forceinline__ void warp_best(const int* bins, const float clo[3], const float chi[3], float& best_cost,
-                                          int& best) {
+// One axis of warp_best: the lowest-cost split of axis a (ties to the lower
+// split), or FLT_MAX / INT_MAX.
+__device__ __forceinline__ void axis_best(const int* bins, const float clo[3], const float chi[3], int a,
+                                          float& best_cost, int& best) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     best_cost = FLT_MAX;
     best = INT_MAX;
-    for (int a = 0; a < 3; a++) {
+    {
         const float ext = sub(chi[a], clo[a]);
-        if (!(ext > 0.0f)) continue;
+        if (!(ext > 0.0f)) return;
         const int* A = bins + a * kBins * kBinWords;
         int lc = 0;
         float l0[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, l1[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
@@ -161,7 +163,20 @@ __device__ __forceinline__ void warp_best(const int* bins, const float clo[3], c
             const int ob = __shfl_xor_sync(full, cand, o);
             if (oc < cost || (oc == cost && ob < cand)) { cost = oc; cand = ob; }
         }
-        if (cost < best_cost) { best_cost = cost; best = cand; }   // earlier axes win ties
+        best_cost = cost;
+        best = cand;
+    }
+}
+
+__device__ __forceinline__ void warp_best(const int* bins, const float clo[3], const float chi[3], float& best_cost,
+                                          int& best) {
+    best_cost = FLT_MAX;
+    best = INT_MAX;
+    for (int a = 0; a < 3; a++) {
+        float c;
+        int b;
+        axis_best(bins, clo, chi, a, c, b);
+        if (c < best_cost) { best_cost = c; best = b; }   // earlier axes win ties
     }
 }
 
@@ -498,6 +513,8 @@ __global__ void __launch_bounds__(kSmallThreads) k_small(const int* __restrict__
     __shared__ SmallFrame s_stack[kSmallStack];
     __shared__ SmallFrame s_cur;
     __shared__ int s_sp, s_next, s_done, s_best, s_leaf;
+    __shared__ float s_axis_cost[3];
+    __shared__ int s_axis_cand[3];
     typedef cub::BlockScan<int, kSmallThreads> Scan;
     __shared__ typename Scan::TempStorage s_scan;
 
@@ -547,11 +564,22 @@ __global__ void __launch_bounds__(kSmallThreads) k_small(const int* __restrict__
                 }
             }
             __syncthreads();
-            if (tid < 32) {
-                float bc;
-                int bi;
-                warp_best(s_bins, cur.clo, cur.chi, bc, bi);
+            // one warp per axis, then thread 0 takes the lowest cost (ties
+            // to the lower axis, as warp_best)
+            const int warp = tid >> 5;
+            if (warp < 3) {
+                float c;
+                int b;
+                axis_best(s_bins, cur.clo, cur.chi, warp, c, b);
+                if ((tid & 31) == 0) { s_axis_cost[warp] = c; s_axis_cand[warp] = b; }
+            }
+            __syncthreads();
+            {
                 if (tid == 0) {
+                    float bc = FLT_MAX;
+                    int bi = INT_MAX;
+                    for (int a = 0; a < 3; a++)
+                        if (s_axis_cost[a] < bc) { bc = s_axis_cost[a]; bi = s_axis_cand[a]; }
                     const int best = bi == INT_MAX ? -1 : bi;
                     const float pa = area(cur.lo[0], cur.lo[1], cur.lo[2], cur.hi[0], cur.hi[1], cur.hi[2]);
                     const float leaf_cost = mul(pa, (float)n);
@@ -957,6 +985,16 @@ cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, D
         if ((size_t)id > 2 * N) { e = cudaErrorInvalidValue; goto done; }
         CK(dmalloc_async(&small_buf, (size_t)2 * ns * sizeof(int), stream));
         CK(cudaMemcpyAsync(small_buf, small_h.data(), (size_t)2 * ns * sizeof(int), cudaMemcpyHostToDevice, stream));
+        {
+            // 37.6 KB of static shared memory a block: ask for the largest
+            // shared-memory carveout so that six blocks fit on an SM
+            static const bool carveout = [] {
+                cudaFuncSetAttribute(k_small, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     cudaSharedmemCarveoutMaxShared);
+                return true;
+            }();
+            (void)carveout;
+        }
         k_small<<<ns, kSmallThreads, 0, stream>>>(small_buf, small_buf + ns, P.plo, P.phi, P.idx, P.nodes, P.err);
         CK(cudaGetLastError());
 
