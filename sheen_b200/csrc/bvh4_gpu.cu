@@ -105,18 +105,16 @@ __device__ __forceinline__ int bin_union(const int* A, int b0, int b1, float lo[
 // order), or INT_MAX when no split qualifies (flat axes or an empty side).
 // Every lane gets the result.  Min/max unions are exact and the counts are
 // integers, so the scan order does not change any value.
-// One axis of warp_best: the lowest-cost split of axis a (ties to the lower
-// split), or FLT_MAX / INT_MAX.
-__device__ __forceinline__ void axis_best(const int* bins, const float clo[3], const float chi[3], int a,
-                                          float& best_cost, int& best) {
+// One axis of warp_best, from that axis's 16 bins A: the lowest-cost split
+// (ties to the lower split) as candidate a * 15 + split, or FLT_MAX /
+// INT_MAX.  ext is the axis's centroid extent.
+__device__ __forceinline__ void axis_best_bins(const int* A, float ext, int a, float& best_cost, int& best) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     best_cost = FLT_MAX;
     best = INT_MAX;
     {
-        const float ext = sub(chi[a], clo[a]);
         if (!(ext > 0.0f)) return;
-        const int* A = bins + a * kBins * kBinWords;
         int lc = 0;
         float l0[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, l1[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
         if (lane < kBins) {
@@ -166,6 +164,11 @@ __device__ __forceinline__ void axis_best(const int* bins, const float clo[3], c
         best_cost = cost;
         best = cand;
     }
+}
+
+__device__ __forceinline__ void axis_best(const int* bins, const float clo[3], const float chi[3], int a,
+                                          float& best_cost, int& best) {
+    axis_best_bins(bins + a * kBins * kBinWords, sub(chi[a], clo[a]), a, best_cost, best);
 }
 
 __device__ __forceinline__ void warp_best(const int* bins, const float clo[3], const float chi[3], float& best_cost,
@@ -493,26 +496,158 @@ __global__ void k_copy_back(const int* __restrict__ work, const int* __restrict_
 
 // ---- 3. small subtrees -----------------------------------------------------
 
+// ---- subtrees of at most 32 triangles: one warp each ----------------------
+//
+// One triangle per lane; every sub-node's box and centroid box are warp
+// min / max reductions over its triangles (exactly the unions of its bins),
+// bins live in a per-warp array of one axis, partitions are ballots.  The
+// decisions are the block path's, on the same values.
+
+constexpr int kTiny = 32;
+constexpr int kTinyCap = 128;     // tiny subtree roots listed per block (packed words)
+constexpr int kTinyStack = 8;     // smaller child first: depth <= log2(32) + 1
+constexpr int kAxisWords = kBins * kBinWords;
+
+struct TinyFrame {
+    unsigned short first, count;  // range in the block's permutation
+    int id;                       // binary node id
+};
+
+__device__ __forceinline__ float warp_min(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Builds the subtree of `root` (count <= 32) with the calling warp.  perm:
+// the block's permutation of local triangle slots; box: their boxes
+// (6 x kSmall); bins: this warp's kAxisWords ints; stack: this warp's
+// kTinyStack frames; next_id: the block's id counter.
+__device__ void build_tiny(TinyFrame root, unsigned short* __restrict__ perm, const float (*box)[kSmall], int gfirst,
+                           int* __restrict__ bins, TinyFrame* __restrict__ stack, int* next_id,
+                           BNode* __restrict__ nodes, int* __restrict__ err) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int sp = 0;
+    TinyFrame cur = root;
+    while (true) {
+        const int m = cur.count, first = cur.first;
+        const bool act = lane < m;
+        const int s = act ? perm[first + lane] : 0;
+        float l[3], h[3], c[3];
+        for (int q = 0; q < 3; q++) {
+            l[q] = act ? box[q][s] : FLT_MAX;
+            h[q] = act ? box[3 + q][s] : -FLT_MAX;
+            c[q] = act ? centroid(l[q], h[q]) : FLT_MAX;
+        }
+        float lo[3], hi[3], clo[3], chi[3];
+        for (int q = 0; q < 3; q++) {
+            lo[q] = warp_min(l[q]);
+            hi[q] = warp_max(h[q]);
+            clo[q] = warp_min(c[q]);
+            chi[q] = warp_max(act ? c[q] : -FLT_MAX);
+        }
+        bool leaf = m <= 2;
+        int best = -1;
+        if (!leaf) {
+            float bc = FLT_MAX;
+            int bi = INT_MAX;
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const float ext = sub(chi[a], clo[a]);
+                if (!(ext > 0.0f)) continue;
+                for (int w = lane; w < kAxisWords; w += 32) bins[w] = bin_init(w);
+                __syncwarp();
+                if (act) add_to_bin(bins + bin_of(c[a], clo[a], bin_scale(ext)) * kBinWords, l, h, c);
+                __syncwarp();
+                float cost;
+                int cand;
+                axis_best_bins(bins, ext, a, cost, cand);
+                if (cost < bc) { bc = cost; bi = cand; }   // earlier axes win ties
+                __syncwarp();
+            }
+            best = bi == INT_MAX ? -1 : bi;
+            const float pa = area(lo[0], lo[1], lo[2], hi[0], hi[1], hi[2]);
+            const float leaf_cost = mul(pa, (float)m);
+            if (best < 0 || (m <= kMaxLeaf && leaf_cost <= add(pa, bc))) leaf = m <= kMaxLeaf;
+        }
+        BNode o;
+        for (int q = 0; q < 3; q++) { o.lo[q] = lo[q]; o.hi[q] = hi[q]; o.clo[q] = clo[q]; o.chi[q] = chi[q]; }
+        o.first = gfirst + first;
+        o.count = m;
+        if (leaf) {
+            o.left = o.right = -1;
+            if (lane == 0) nodes[cur.id] = o;
+            if (sp == 0) break;
+            cur = stack[--sp];
+            continue;
+        }
+        // stable partition by ballot
+        const int axis = best >= 0 ? best / (kBins - 1) : -1;
+        const int sbin = best >= 0 ? best % (kBins - 1) : 0;
+        const float ca = axis == 0 ? c[0] : (axis == 1 ? c[1] : c[2]);
+        const float la = axis == 0 ? clo[0] : (axis == 1 ? clo[1] : clo[2]);
+        const float ha = axis == 0 ? chi[0] : (axis == 1 ? chi[1] : chi[2]);
+        bool f = false;
+        if (act) f = axis >= 0 ? bin_of(ca, la, bin_scale(sub(ha, la))) <= sbin : lane < m / 2;
+        const unsigned left_mask = __ballot_sync(full, act && f);
+        const int nleft = __popc(left_mask);
+        const int before = __popc(left_mask & ((1u << lane) - 1u));
+        __syncwarp();
+        if (act) perm[first + (f ? before : nleft + (lane - before))] = (unsigned short)s;
+        __syncwarp();
+        int mid = first + (axis >= 0 ? nleft : m / 2);
+        if (mid == first || mid == first + m) mid = first + m / 2;
+        int base = 0;
+        if (lane == 0) base = atomicAdd(next_id, 2);
+        base = __shfl_sync(full, base, 0);
+        o.left = base;
+        o.right = base + 1;
+        if (lane == 0) nodes[cur.id] = o;
+        TinyFrame L, R;
+        L.first = (unsigned short)first; L.count = (unsigned short)(mid - first); L.id = base;
+        R.first = (unsigned short)mid; R.count = (unsigned short)(first + m - mid); R.id = base + 1;
+        if (sp >= kTinyStack) {
+            if (lane == 0) *err = 3;
+            break;
+        }
+        if (R.count >= L.count) { stack[sp++] = R; cur = L; }
+        else { stack[sp++] = L; cur = R; }
+    }
+    __syncwarp();
+}
+
 struct SmallFrame {
     int first, count, id, pad;
     float lo[3], hi[3], clo[3], chi[3];
 };
 
-constexpr int kSmallStack = 24;
+// Smaller child first: a frame is pushed only when descending into a child
+// of at most half its parent's count, so the stack holds at most
+// log2(kSmall) = 10 frames.
+constexpr int kSmallStack = 16;
 
-__global__ void __launch_bounds__(kSmallThreads) k_small(const int* __restrict__ list, const int* __restrict__ id_base,
+// List word of a tiny subtree root: first (10 bits) | count - 1 (5 bits) |
+// node id - the block's first id (11 bits; 2047 for the block's root).
+static_assert(kSmall <= 1024 && kTiny <= 32 && 2 * kSmall - 2 < 2047, "tiny list word");
+
+__global__ void __launch_bounds__(kSmallThreads, 6) k_small(const int* __restrict__ list, const int* __restrict__ id_base,
                                                          const float4* __restrict__ plo, const float4* __restrict__ phi,
                                                          int* __restrict__ idx, BNode* __restrict__ nodes,
                                                          int* __restrict__ err) {
     __shared__ float s_box[6][kSmall];
     __shared__ int s_pid[kSmall];
     __shared__ unsigned short s_perm[kSmall];
-    __shared__ unsigned short s_tmp[kSmall];
+    __shared__ __align__(16) unsigned short s_tmp[kSmall];
     __shared__ int s_bins[kNodeBins];
     __shared__ int s_cb[24];
-    __shared__ SmallFrame s_stack[kSmallStack];
+    __shared__ __align__(16) SmallFrame s_stack[kSmallStack];
     __shared__ SmallFrame s_cur;
-    __shared__ int s_sp, s_next, s_done, s_best, s_leaf;
+    __shared__ unsigned s_tiny[kTinyCap];
+    __shared__ int s_sp, s_next, s_done, s_best, s_leaf, s_ntiny;
     __shared__ float s_axis_cost[3];
     __shared__ int s_axis_cand[3];
     typedef cub::BlockScan<int, kSmallThreads> Scan;
@@ -538,12 +673,28 @@ __global__ void __launch_bounds__(kSmallThreads) k_small(const int* __restrict__
         s_sp = 0;
         s_next = id_base[blockIdx.x];
         s_done = 0;
+        s_ntiny = 0;
     }
     __syncthreads();
     while (true) {
         const SmallFrame cur = s_cur;
-        __syncthreads();   // every thread has its copy before thread 0 may replace s_cur
+        const int ntiny = s_ntiny;
+        __syncthreads();   // every thread has its copies before thread 0 may replace them
         const int n = cur.count;
+        if (n <= kTiny && ntiny < kTinyCap) {
+            // left to one warp after the block phase (a full list falls back
+            // to the block path below)
+            if (tid == 0) {
+                const unsigned rel = cur.id == root ? 2047u : (unsigned)(cur.id - id_base[blockIdx.x]);
+                s_tiny[ntiny] = (unsigned)cur.first | (unsigned)(n - 1) << 10 | rel << 15;
+                s_ntiny = ntiny + 1;
+                if (s_sp == 0) s_done = 1;
+                else s_cur = s_stack[--s_sp];
+            }
+            __syncthreads();
+            if (s_done) break;
+            continue;
+        }
         bool leaf = n <= 2;
         if (!leaf) {
             for (int w = tid; w < kNodeBins; w += kSmallThreads) s_bins[w] = bin_init(w);
@@ -706,6 +857,28 @@ __global__ void __launch_bounds__(kSmallThreads) k_small(const int* __restrict__
         }
         __syncthreads();
         if (s_done) break;
+    }
+    __syncthreads();
+    {
+        // Subtrees of at most kTiny triangles, one warp each.  The block
+        // phase's bins (three warps) and partition buffer (the fourth) hold
+        // the warps' bins, its frame stack their stacks.
+        static_assert(3 * kAxisWords <= kNodeBins && kAxisWords * 4 <= (int)sizeof(s_tmp), "tiny bins fit");
+        static_assert(4 * kTinyStack * sizeof(TinyFrame) <= sizeof(s_stack), "tiny stacks fit");
+        static_assert(kSmallThreads == 128, "four warps");
+        const int warp = tid >> 5;
+        int* wbins = warp < 3 ? s_bins + warp * kAxisWords : reinterpret_cast<int*>(s_tmp);
+        TinyFrame* wstack = reinterpret_cast<TinyFrame*>(s_stack) + warp * kTinyStack;
+        const int nt = s_ntiny, id0 = id_base[blockIdx.x];
+        for (int t = warp; t < nt; t += kSmallThreads / 32) {
+            const unsigned w = s_tiny[t];
+            TinyFrame f;
+            f.first = (unsigned short)(w & 1023u);
+            f.count = (unsigned short)(((w >> 10) & 31u) + 1u);
+            const unsigned rel = w >> 15;
+            f.id = rel == 2047u ? root : id0 + (int)rel;
+            build_tiny(f, s_perm, s_box, gfirst, wbins, wstack, &s_next, nodes, err);
+        }
     }
     __syncthreads();
     for (int k = tid; k < n0; k += kSmallThreads) idx[gfirst + k] = s_pid[s_perm[k]];
