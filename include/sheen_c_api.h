@@ -231,6 +231,17 @@ int sheen_scene_trace(SheenDeviceScene scene, const float* rays_host, int n, int
  * depth, or a negative code on a violation.  No device work. */
 int sheen_selfcheck_bvh4(const SheenScene* scene);
 
+/* Host-side check of the blocking triangles' BVH4 (material transmission
+ * <= 0.5), which the wavefront form derives from the tree over all
+ * triangles instead of building it: drops the passable triangles from the
+ * leaves, splices out nodes left with one child and refits every box.
+ * Checks that the tree over all equals the plainly built one byte for byte,
+ * that both trees are structurally valid with every child box exactly the
+ * quantised union of the triangles below it, and that the derived tree
+ * holds each blocking triangle once.  Returns the derived tree's depth (0
+ * when nothing blocks) or a negative code.  No device work. */
+int sheen_selfcheck_bvh4_kept(const SheenScene* scene);
+
 /* Builds the wavefront form's three triangle BVH4s (all / blocking /
  * passable triangles) of a scene with the host builder and with the device
  * builder and compares them byte for byte.  No counterpart in the reference

@@ -21,6 +21,12 @@
 // primitives/triangle.h:9-10, so its results are unchanged), or {v1, 0},
 // {v2, 0} for the watertight test, which needs the vertices themselves.
 //
+// The tree over a subset of the triangles (the blocking ones) can be derived
+// from the tree over all of them instead of built (build_qbvh4_with_kept):
+// leaves lose the other triangles, nodes left with one child are spliced
+// out, boxes are refitted.  Where the subset is most of the triangles its
+// derived tree is nearly the built one, at a fraction of the build's cost.
+//
 // The arithmetic of every decision (bins, SAH costs, frame exponents,
 // quantisation) is in bvh4_rules.h, shared with the device builder
 // (bvh4_gpu.cu); partitions are stable.  The two builders therefore produce
@@ -153,16 +159,10 @@ struct SahBuilder {
     }
 };
 
-}  // namespace
-
-void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out, bool vertices) {
-    out.nodes.clear();
-    out.tris.clear();
-    out.max_depth = 0;
-    out.vertices = vertices;
+// Binned SAH tree over tris[subset[i]]: box and centroid of every
+// triangle, then the recursive build.  Returns the root of `bn`.
+int sah_build(const Triangle* tris, const std::vector<int>& subset, SahBuilder& sb, std::vector<BNode>& bn) {
     const int n = (int)subset.size();
-    if (n <= 0) return;
-    SahBuilder sb;
     sb.tri_box.resize((size_t)n);
     sb.cen.resize(3 * (size_t)n);
     sb.idx.resize((size_t)n);
@@ -176,28 +176,35 @@ void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out
         for (int k = 0; k < 3; k++) sb.cen[3 * (size_t)i + k] = bvhr::centroid(b.lo[k], b.hi[k]);
         sb.idx[(size_t)i] = i;
     }
-    std::vector<BNode> bn;
     bn.reserve((size_t)n);
-    const int root = sb.build(0, n, 0, bn);
+    return sb.build(0, n, 0, bn);
+}
 
-    // Leaf triangles in leaf order.
-    out.tris.resize(3 * (size_t)n);
-    for (int i = 0; i < n; i++) {
-        const int orig = subset[(size_t)sb.idx[(size_t)i]];
+// Triangle records of `out` in leaf order; order[i] is the original index of
+// leaf slot i.
+void emit_tris(const Triangle* tris, const std::vector<int>& order, QBvh& out, bool vertices) {
+    const size_t n = order.size();
+    out.tris.resize(3 * n);
+    for (size_t i = 0; i < n; i++) {
+        const int orig = order[i];
         const Triangle& t = tris[orig];
         float fi;
         std::memcpy(&fi, &orig, 4);
-        out.tris[3 * (size_t)i] = make_float4(t.v0.x, t.v0.y, t.v0.z, fi);
+        out.tris[3 * i] = make_float4(t.v0.x, t.v0.y, t.v0.z, fi);
         if (vertices) {
-            out.tris[3 * (size_t)i + 1] = make_float4(t.v1.x, t.v1.y, t.v1.z, 0.0f);
-            out.tris[3 * (size_t)i + 2] = make_float4(t.v2.x, t.v2.y, t.v2.z, 0.0f);
+            out.tris[3 * i + 1] = make_float4(t.v1.x, t.v1.y, t.v1.z, 0.0f);
+            out.tris[3 * i + 2] = make_float4(t.v2.x, t.v2.y, t.v2.z, 0.0f);
         } else {
-            out.tris[3 * (size_t)i + 1] = make_float4(t.v1.x - t.v0.x, t.v1.y - t.v0.y, t.v1.z - t.v0.z, 0.0f);
-            out.tris[3 * (size_t)i + 2] = make_float4(t.v2.x - t.v0.x, t.v2.y - t.v0.y, t.v2.z - t.v0.z, 0.0f);
+            out.tris[3 * i + 1] = make_float4(t.v1.x - t.v0.x, t.v1.y - t.v0.y, t.v1.z - t.v0.z, 0.0f);
+            out.tris[3 * i + 2] = make_float4(t.v2.x - t.v0.x, t.v2.y - t.v0.y, t.v2.z - t.v0.z, 0.0f);
         }
     }
+}
 
-    // Collapse to 4-wide nodes, breadth first from the root.
+// Collapses the binary tree bn (root `root`; a leaf has count > 0) into
+// 4-wide nodes, breadth first from the root, each inner node opening its
+// largest-area inner child until it has four children.
+void collapse(const std::vector<BNode>& bn, int root, QBvh& out) {
     struct Pending { int bnode; int slot; };
     std::vector<Pending> queue;
     std::vector<int> ndepth;
@@ -215,8 +222,6 @@ void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out
         // A single leaf: wrap it in one node with one child.
         const int id = emit(root);
         queue.clear();
-        dev::QNode4& q = out.nodes[(size_t)id];
-        (void)q;
         queue.push_back({-1 - root, id});
     } else {
         emit(root);
@@ -281,6 +286,89 @@ void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out
         node.pad = make_uint2(0, 0);
     }
     out.leaf_size_max = kMaxLeaf;
+}
+
+// The binary tree bn restricted to the leaf slots `kept` marks (pre: its
+// prefix counts, so kept slot i moves to pre[i]): a leaf keeps its kept
+// triangles (none: the leaf goes), an inner node with one child left is
+// replaced by that child, and every box is the union of the kept triangle
+// boxes below it.  Returns the new root in `out`, or -1 when nothing is kept.
+int prune(const std::vector<BNode>& bn, int i, const std::vector<int>& pre, const std::vector<unsigned char>& kept,
+          const SahBuilder& sb, std::vector<BNode>& out) {
+    const BNode& b = bn[(size_t)i];
+    if (b.count > 0) {
+        const int kc = pre[(size_t)(b.first + b.count)] - pre[(size_t)b.first];
+        if (kc == 0) return -1;
+        BNode o;
+        o.first = pre[(size_t)b.first];
+        o.count = kc;
+        for (int p = b.first; p < b.first + b.count; p++)
+            if (kept[(size_t)p]) o.box.grow(sb.tri_box[(size_t)sb.idx[(size_t)p]]);
+        out.push_back(o);
+        return (int)out.size() - 1;
+    }
+    const int l = prune(bn, b.left, pre, kept, sb, out);
+    const int r = prune(bn, b.right, pre, kept, sb, out);
+    if (l < 0) return r;
+    if (r < 0) return l;
+    BNode o;
+    o.left = l;
+    o.right = r;
+    o.box = out[(size_t)l].box;
+    o.box.grow(out[(size_t)r].box);
+    out.push_back(o);
+    return (int)out.size() - 1;
+}
+
+void reset(QBvh& q, bool vertices) {
+    q.nodes.clear();
+    q.tris.clear();
+    q.max_depth = 0;
+    q.vertices = vertices;
+}
+
+}  // namespace
+
+void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out, bool vertices) {
+    reset(out, vertices);
+    const int n = (int)subset.size();
+    if (n <= 0) return;
+    SahBuilder sb;
+    std::vector<BNode> bn;
+    const int root = sah_build(tris, subset, sb, bn);
+    std::vector<int> order((size_t)n);
+    for (int i = 0; i < n; i++) order[(size_t)i] = subset[(size_t)sb.idx[(size_t)i]];
+    emit_tris(tris, order, out, vertices);
+    collapse(bn, root, out);
+}
+
+void build_qbvh4_with_kept(const Triangle* tris, int n, const std::vector<unsigned char>& keep, QBvh& all,
+                           QBvh& kept_out, bool vertices) {
+    reset(all, vertices);
+    reset(kept_out, vertices);
+    if (n <= 0) return;
+    std::vector<int> subset((size_t)n);
+    for (int i = 0; i < n; i++) subset[(size_t)i] = i;
+    SahBuilder sb;
+    std::vector<BNode> bn;
+    const int root = sah_build(tris, subset, sb, bn);
+    std::vector<int> order((size_t)n), kept_order;
+    std::vector<unsigned char> kept((size_t)n);
+    std::vector<int> pre((size_t)n + 1, 0);
+    for (int i = 0; i < n; i++) {
+        order[(size_t)i] = sb.idx[(size_t)i];
+        kept[(size_t)i] = keep[(size_t)order[(size_t)i]] ? 1 : 0;
+        pre[(size_t)i + 1] = pre[(size_t)i] + kept[(size_t)i];
+        if (kept[(size_t)i]) kept_order.push_back(order[(size_t)i]);
+    }
+    emit_tris(tris, order, all, vertices);
+    collapse(bn, root, all);
+    if (kept_order.empty()) return;
+    std::vector<BNode> pn;
+    pn.reserve(bn.size());
+    const int proot = prune(bn, root, pre, kept, sb, pn);
+    emit_tris(tris, kept_order, kept_out, vertices);
+    collapse(pn, proot, kept_out);
 }
 
 // Structural check of a BVH4 (host only): every triangle slot is referenced
@@ -349,6 +437,61 @@ int check_qbvh4(const QBvh& q, int& depth) {
     return 0;
 }
 
+// Tightness of a BVH4 against the triangles it was built from: every child
+// box is exactly the outward quantisation, in its node's frame, of the union
+// of the (canonical) boxes of the original triangles below it, and every
+// frame is the one the builder derives from the union of its children.
+// Returns 0 or a negative code.
+namespace {
+int tight_box(const QBvh& q, const Triangle* tris, uint32_t e, Box& out) {
+    out = Box();
+    if (e & 0x80000000u) {
+        const uint32_t first = (e & 0x7fffffffu) >> 3, count = (e & 7u) + 1;
+        for (uint32_t k = 0; k < count; k++) {
+            int orig;
+            std::memcpy(&orig, &q.tris[3 * (size_t)(first + k)].w, 4);
+            const Triangle& t = tris[orig];
+            const float v[3][3] = {{t.v0.x, t.v0.y, t.v0.z}, {t.v1.x, t.v1.y, t.v1.z}, {t.v2.x, t.v2.y, t.v2.z}};
+            Box b;
+            for (int p = 0; p < 3; p++) b.grow(v[p]);
+            for (int a = 0; a < 3; a++) { b.lo[a] = bvhr::canon(b.lo[a]); b.hi[a] = bvhr::canon(b.hi[a]); }
+            out.grow(b);
+        }
+        return 0;
+    }
+    const dev::QNode4& n = q.nodes[e];
+    uint32_t packed;
+    std::memcpy(&packed, &n.origin_exp.w, 4);
+    const int count = (int)(packed >> 24);
+    const uint32_t ch[4] = {n.child.x, n.child.y, n.child.z, n.child.w};
+    const uint32_t words[6] = {n.qbox.x, n.qbox.y, n.qbox.z, n.qbox.w, n.qz.x, n.qz.y};
+    Box kb[4];
+    for (int i = 0; i < count; i++) {
+        const int rc = tight_box(q, tris, ch[i], kb[i]);
+        if (rc) return rc;
+        out.grow(kb[i]);
+    }
+    for (int a = 0; a < 3; a++) {
+        if (n.origin_exp.x != out.lo[0] || n.origin_exp.y != out.lo[1] || n.origin_exp.z != out.lo[2]) return -11;
+        const int ex = bvhr::frame_exponent(out.lo[a], out.hi[a]);
+        if ((int)((packed >> (8 * a)) & 0xffu) != ex + 127) return -12;
+        const float scale = std::ldexp(1.0f, ex);
+        for (int i = 0; i < count; i++) {
+            uint8_t ql, qh;
+            bvhr::quantize_axis(out.lo[a], scale, kb[i].lo[a], kb[i].hi[a], ql, qh);
+            if (((words[2 * a] >> (8 * i)) & 0xffu) != ql || ((words[2 * a + 1] >> (8 * i)) & 0xffu) != qh) return -13;
+        }
+    }
+    return 0;
+}
+}  // namespace
+
+int check_qbvh4_tight(const QBvh& q, const Triangle* tris) {
+    if (q.nodes.empty()) return 0;
+    Box b;
+    return tight_box(q, tris, 0u, b);
+}
+
 }  // namespace sheen
 
 // Host-side self check of the wavefront form's triangle BVH for a scene:
@@ -363,4 +506,49 @@ extern "C" int sheen_selfcheck_bvh4(const SheenScene* scene) {
     int depth = 0;
     const int rc = sheen::check_qbvh4(q, depth);
     return rc < 0 ? rc : depth;
+}
+
+// Host-side self check of the blocking triangles' BVH4 derived from the tree
+// over all triangles (build_qbvh4_with_kept, blocking = material
+// transmission <= 0.5): the tree over all equals build_qbvh4's byte for byte,
+// both trees pass check_qbvh4 and check_qbvh4_tight, and the derived tree
+// holds each blocking triangle exactly once.  Returns the derived tree's
+// depth (0 when nothing blocks) or a negative code.  No device work.
+extern "C" int sheen_selfcheck_bvh4_kept(const SheenScene* scene) {
+    using namespace sheen;
+    if (!scene || scene->num_triangles <= 0) return -1;
+    const int n = scene->num_triangles;
+    std::vector<int> all((size_t)n);
+    std::vector<unsigned char> blocking((size_t)n);
+    int nblock = 0;
+    for (int i = 0; i < n; i++) {
+        all[(size_t)i] = i;
+        const int m = scene->triangles[i].material_id;
+        const bool passable = m >= 0 && m < scene->num_materials && scene->materials[m].transmission > 0.5f;
+        blocking[(size_t)i] = passable ? 0 : 1;
+        nblock += passable ? 0 : 1;
+    }
+    QBvh built, q_all, q_kept;
+    build_qbvh4(scene->triangles, all, built);
+    build_qbvh4_with_kept(scene->triangles, n, blocking, q_all, q_kept);
+    if (built.nodes.size() != q_all.nodes.size() || built.tris.size() != q_all.tris.size() ||
+        std::memcmp(built.nodes.data(), q_all.nodes.data(), built.nodes.size() * sizeof(dev::QNode4)) != 0 ||
+        std::memcmp(built.tris.data(), q_all.tris.data(), built.tris.size() * sizeof(float4)) != 0)
+        return -20;
+    int d_all = 0, d_kept = 0;
+    int rc = check_qbvh4(q_all, d_all);
+    if (rc < 0) return rc;
+    if ((rc = check_qbvh4_tight(q_all, scene->triangles)) < 0) return rc;
+    if ((int)(q_kept.tris.size() / 3) != nblock) return -21;
+    if (nblock == 0) return q_kept.nodes.empty() ? 0 : -22;
+    if ((rc = check_qbvh4(q_kept, d_kept)) < 0) return rc - 30;
+    if ((rc = check_qbvh4_tight(q_kept, scene->triangles)) < 0) return rc - 30;
+    std::vector<int> seen((size_t)n, 0);
+    for (size_t k = 0; k < q_kept.tris.size() / 3; k++) {
+        int orig;
+        std::memcpy(&orig, &q_kept.tris[3 * k].w, 4);
+        if (orig < 0 || orig >= n || !blocking[(size_t)orig] || seen[(size_t)orig]++) return -23;
+    }
+    if (d_kept > d_all) return -24;
+    return d_kept;
 }

@@ -79,6 +79,64 @@ __device__ __forceinline__ void add_to_bin(int* B, const float l[3], const float
     }
 }
 
+// Adds each active lane's triangle (box l, h, centroid c) to bin b[a] of
+// every axis a with axis_on[a] (bins of axis a start at A + a * kBins *
+// kBinWords).  On an axis where all active lanes of the warp share one bin
+// the warp reduces first and one lane adds the result: mesh order puts runs
+// of neighbouring triangles into the same bin, where one atomic per lane on
+// the same words serialises.  Integer min / max of the ordered keys give the
+// same words as the per-lane atomics.  Called by all 32 lanes with the same
+// axis_on.
+__device__ __forceinline__ void add_to_bins_warp(int* A, const int b[3], bool act, const bool axis_on[3],
+                                                 const float l[3], const float h[3], const float c[3]) {
+    const unsigned full = 0xffffffffu;
+    const unsigned active = __ballot_sync(full, act);
+    if (!active) return;
+    const int src = __ffs(active) - 1;
+    bool uni[3];
+    bool any_uni = false;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const int b0 = __shfl_sync(full, b[a], src);
+        uni[a] = axis_on[a] && __all_sync(full, !act || b[a] == b0);
+        any_uni |= uni[a];
+        if (axis_on[a] && !uni[a] && act) add_to_bin(A + (a * kBins + b[a]) * kBinWords, l, h, c);
+    }
+    if (!any_uni) return;
+    int k[12];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        k[q] = act ? ford(l[q]) : INT_MAX;
+        k[3 + q] = act ? ford(h[q]) : INT_MIN;
+        k[6 + q] = act ? ford(c[q]) : INT_MAX;
+        k[9 + q] = act ? ford(c[q]) : INT_MIN;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int q = 0; q < 12; q++) {
+            const int v = __shfl_xor_sync(full, k[q], o);
+            k[q] = (q < 3 || (q >= 6 && q < 9)) ? min(k[q], v) : max(k[q], v);
+        }
+    }
+    if ((threadIdx.x & 31) == src) {
+        const int cnt = __popc(active);
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            if (!uni[a]) continue;
+            int* B = A + (a * kBins + b[a]) * kBinWords;
+            atomicAdd(B, cnt);
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                atomicMin(B + 1 + q, k[q]);
+                atomicMax(B + 4 + q, k[3 + q]);
+                atomicMin(B + 7 + q, k[6 + q]);
+                atomicMax(B + 10 + q, k[9 + q]);
+            }
+        }
+    }
+}
+
 // Union of bins [b0, b1] of one axis into box/centroid box; returns the count.
 __device__ __forceinline__ int bin_union(const int* A, int b0, int b1, float lo[3], float hi[3], float clo[3],
                                          float chi[3]) {
@@ -279,21 +337,29 @@ __global__ void __launch_bounds__(kChunkThreads) k_bin_large(const int* __restri
     const int end = min(start + kChunk, nd.first + nd.count);
     for (int w = threadIdx.x; w < kNodeBins; w += kChunkThreads) sb[w] = bin_init(w);
     __syncthreads();
-    float ext[3], kk[3];
+    float kk[3];
+    bool on[3];
+#pragma unroll
     for (int a = 0; a < 3; a++) {
-        ext[a] = sub(nd.chi[a], nd.clo[a]);
-        kk[a] = ext[a] > 0.0f ? bin_scale(ext[a]) : 0.0f;
+        const float ext = sub(nd.chi[a], nd.clo[a]);
+        on[a] = ext > 0.0f;
+        kk[a] = on[a] ? bin_scale(ext) : 0.0f;
     }
-    for (int pos = start + threadIdx.x; pos < end; pos += kChunkThreads) {
-        const int p = idx[pos];
-        const float4 L = plo[p], H = phi[p];
-        const float l[3] = {L.x, L.y, L.z}, h[3] = {H.x, H.y, H.z};
-        const float cc[3] = {centroid(l[0], h[0]), centroid(l[1], h[1]), centroid(l[2], h[2])};
-        for (int a = 0; a < 3; a++) {
-            if (!(ext[a] > 0.0f)) continue;
-            const int b = bin_of(cc[a], nd.clo[a], kk[a]);
-            add_to_bin(sb + (a * kBins + b) * kBinWords, l, h, cc);
+    for (int base = start; base < end; base += kChunkThreads) {   // uniform trip count per warp
+        const int pos = base + threadIdx.x;
+        const bool act = pos < end;
+        float l[3] = {0.0f, 0.0f, 0.0f}, h[3] = {0.0f, 0.0f, 0.0f};
+        if (act) {
+            const int p = idx[pos];
+            const float4 L = plo[p], H = phi[p];
+            l[0] = L.x; l[1] = L.y; l[2] = L.z;
+            h[0] = H.x; h[1] = H.y; h[2] = H.z;
         }
+        const float cc[3] = {centroid(l[0], h[0]), centroid(l[1], h[1]), centroid(l[2], h[2])};
+        int b[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) b[a] = on[a] ? bin_of(cc[a], nd.clo[a], kk[a]) : 0;
+        add_to_bins_warp(sb, b, act, on, l, h, cc);
     }
     __syncthreads();
     int* G = gbins + (size_t)j * kNodeBins;
@@ -699,20 +765,25 @@ __global__ void __launch_bounds__(kSmallThreads, 6) k_small(const int* __restric
         if (!leaf) {
             for (int w = tid; w < kNodeBins; w += kSmallThreads) s_bins[w] = bin_init(w);
             __syncthreads();
-            float ext[3], kk[3];
+            float kk[3];
+            bool on[3];
+#pragma unroll
             for (int a = 0; a < 3; a++) {
-                ext[a] = sub(cur.chi[a], cur.clo[a]);
-                kk[a] = ext[a] > 0.0f ? bin_scale(ext[a]) : 0.0f;
+                const float ext = sub(cur.chi[a], cur.clo[a]);
+                on[a] = ext > 0.0f;
+                kk[a] = on[a] ? bin_scale(ext) : 0.0f;
             }
-            for (int k = tid; k < n; k += kSmallThreads) {
-                const int s = s_perm[cur.first + k];
+            for (int k0 = 0; k0 < n; k0 += kSmallThreads) {   // uniform trip count per warp
+                const int k = k0 + tid;
+                const bool act = k < n;
+                const int s = act ? s_perm[cur.first + k] : 0;
                 const float l[3] = {s_box[0][s], s_box[1][s], s_box[2][s]};
                 const float h[3] = {s_box[3][s], s_box[4][s], s_box[5][s]};
                 const float cc[3] = {centroid(l[0], h[0]), centroid(l[1], h[1]), centroid(l[2], h[2])};
-                for (int a = 0; a < 3; a++) {
-                    if (!(ext[a] > 0.0f)) continue;
-                    add_to_bin(s_bins + (a * kBins + bin_of(cc[a], cur.clo[a], kk[a])) * kBinWords, l, h, cc);
-                }
+                int b[3];
+#pragma unroll
+                for (int a = 0; a < 3; a++) b[a] = on[a] ? bin_of(cc[a], cur.clo[a], kk[a]) : 0;
+                add_to_bins_warp(s_bins, b, act, on, l, h, cc);
             }
             __syncthreads();
             // one warp per axis, then thread 0 takes the lowest cost (ties
@@ -882,6 +953,15 @@ __global__ void __launch_bounds__(kSmallThreads, 6) k_small(const int* __restric
     }
     __syncthreads();
     for (int k = tid; k < n0; k += kSmallThreads) idx[gfirst + k] = s_pid[s_perm[k]];
+    // Ids reserved for this subtree but not used (a tree with leaves of
+    // several triangles has fewer than 2 n0 - 1 nodes) are marked empty
+    // (count 0), so that passes over every id see only real nodes.
+    const int id_end = id_base[blockIdx.x] + max(0, 2 * n0 - 2);
+    for (int k = s_next + tid; k < id_end; k += kSmallThreads) {
+        nodes[k].count = 0;
+        nodes[k].first = 0;
+        nodes[k].left = nodes[k].right = -1;
+    }
 }
 
 // ---- 4. collapse to BVH4 ---------------------------------------------------
@@ -1008,6 +1088,119 @@ __global__ void k_pass_flags(const Triangle* __restrict__ tris, int n, const Mat
     block[i] = p ? 0 : 1;
 }
 
+// ---- 6. the tree over a kept subset, derived from the built one -----------
+//
+// The binary tree over all triangles restricted to those with keep[t]: a
+// leaf keeps its kept triangles (none: it goes), an inner node left with one
+// child is replaced by that child, boxes are refitted to the kept triangles
+// bottom up, and the result is collapsed like a built tree.  Kept leaf slot
+// p moves to pre[p] (the exclusive prefix count of kept slots).
+
+// kp[p] = 1 when leaf slot p is kept (p < n); kp[n] = 0 so that the scan
+// yields the total in pre[n].
+__global__ void k_keep_pos(const int* __restrict__ idx, int n, const unsigned char* __restrict__ keep,
+                           int* __restrict__ kp) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) kp[p] = keep[idx[p]] ? 1 : 0;
+    else if (p == n) kp[p] = 0;
+}
+
+// Kept count kc of every node (0 for ids marked empty), parent links, and
+// the refit counters cleared.
+__global__ void k_prune_count(const BNode* __restrict__ nodes, int nb, const int* __restrict__ pre,
+                              int* __restrict__ kc, int* __restrict__ parent, int* __restrict__ visit) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nb) return;
+    const BNode& b = nodes[i];
+    const int cnt = b.count;
+    kc[i] = cnt > 0 ? pre[b.first + cnt] - pre[b.first] : 0;
+    visit[i] = 0;
+    if (cnt > 0 && b.left >= 0) {
+        parent[b.left] = i;
+        parent[b.right] = i;
+    }
+    if (i == 0) parent[0] = -1;
+}
+
+// Bottom-up refit: every kept leaf writes its box, then climbs; at a parent
+// with both children kept the first arrival stops and the second unites the
+// two boxes (min / max are exact, so the order of arrival does not matter).
+__global__ void k_prune_refit(const BNode* __restrict__ nodes, int nb, const int* __restrict__ kc,
+                              const int* __restrict__ pre, const int* __restrict__ parent, const int* __restrict__ idx,
+                              const unsigned char* __restrict__ keep, const float4* __restrict__ plo,
+                              const float4* __restrict__ phi, BNode* __restrict__ Q, int* __restrict__ visit) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nb) return;
+    const BNode b = nodes[i];
+    if (!(b.count > 0 && b.left < 0 && kc[i] > 0)) return;
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int p = b.first; p < b.first + b.count; p++) {
+        const int t = idx[p];
+        if (!keep[t]) continue;
+        const float4 l = plo[t], h = phi[t];
+        lo[0] = fminf(lo[0], l.x); lo[1] = fminf(lo[1], l.y); lo[2] = fminf(lo[2], l.z);
+        hi[0] = fmaxf(hi[0], h.x); hi[1] = fmaxf(hi[1], h.y); hi[2] = fmaxf(hi[2], h.z);
+    }
+    BNode& o = Q[i];
+    for (int q = 0; q < 3; q++) { o.lo[q] = lo[q]; o.hi[q] = hi[q]; }
+    o.first = pre[b.first];
+    o.count = kc[i];
+    o.left = o.right = -1;
+    int j = i;
+    while (true) {
+        const int p = parent[j];
+        if (p < 0) break;
+        const int sib = nodes[p].left == j ? nodes[p].right : nodes[p].left;
+        if (kc[sib] > 0) {
+            __threadfence();
+            if (atomicAdd(&visit[p], 1) == 0) return;   // the sibling's climb continues
+            __threadfence();
+            const float* sl = Q[sib].lo;
+            const float* sh = Q[sib].hi;
+            for (int q = 0; q < 3; q++) {
+                lo[q] = fminf(lo[q], __ldcg(sl + q));
+                hi[q] = fmaxf(hi[q], __ldcg(sh + q));
+            }
+        }
+        for (int q = 0; q < 3; q++) { Q[p].lo[q] = lo[q]; Q[p].hi[q] = hi[q]; }
+        j = p;
+    }
+}
+
+// The kept node that stands for node x: x itself, or down the chain of
+// nodes with one kept child.
+__device__ __forceinline__ int prune_resolve(const BNode* __restrict__ nodes, const int* __restrict__ kc, int x) {
+    while (true) {
+        const BNode& c = nodes[x];
+        if (c.left < 0) return x;
+        const bool l = kc[c.left] > 0, r = kc[c.right] > 0;
+        if (l && r) return x;
+        x = l ? c.left : c.right;
+    }
+}
+
+// Links of the kept inner nodes (both children kept); thread 0 also puts
+// the kept root into level[0].
+__global__ void k_prune_link(const BNode* __restrict__ nodes, int nb, const int* __restrict__ kc,
+                             const int* __restrict__ pre, BNode* __restrict__ Q, int* __restrict__ level) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nb) return;
+    if (i == 0) level[0] = prune_resolve(nodes, kc, 0);
+    const BNode& b = nodes[i];
+    if (!(b.count > 0 && b.left >= 0 && kc[i] > 0 && kc[b.left] > 0 && kc[b.right] > 0)) return;
+    Q[i].first = pre[b.first];
+    Q[i].count = kc[i];
+    Q[i].left = prune_resolve(nodes, kc, b.left);
+    Q[i].right = prune_resolve(nodes, kc, b.right);
+}
+
+// kept slot list: out[pre[p]] = idx[p] for every kept slot p.
+__global__ void k_prune_compact(const int* __restrict__ idx, int n, const int* __restrict__ kp,
+                                const int* __restrict__ pre, int* __restrict__ out) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n && kp[p]) out[pre[p]] = idx[p];
+}
+
 // Carves 256-byte aligned arrays from one block.
 struct Carver {
     char* p;
@@ -1025,10 +1218,14 @@ struct Carver {
 // Device-built BVH4 over triangles tris[subset[i]] (subset null: all n).
 // Allocates out.nodes (exact size) and out.tris (3 float4 per triangle);
 // everything else is temporary.  Synchronises `stream` once per tree level.
+// With keep (per triangle, subset null) it also derives the BVH4 over the
+// triangles with keep[t] != 0 into *kept_out (build_qbvh4_with_kept's).
 cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, DevQBvh& out, cudaStream_t stream,
-                               bool vertices) {
+                               bool vertices, const unsigned char* keep, DevQBvh* kept_out) {
     using namespace bvhg;
     out = DevQBvh{};
+    if (kept_out) *kept_out = DevQBvh{};
+    if (keep && (subset || !kept_out)) return cudaErrorInvalidValue;
     if (n <= 0) return cudaSuccess;
     if (n > (1 << 27)) return cudaErrorInvalidValue;   // leaf words hold first < 2^28
     const size_t N = (size_t)n;
@@ -1037,7 +1234,7 @@ cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, D
     size_t cub_a = 0, cub_b = 0;
     cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, cub_a, (int*)nullptr, (int*)nullptr, max_chunks);
     if (e != cudaSuccess) return e;
-    e = cub::DeviceScan::ExclusiveSum(nullptr, cub_b, (int*)nullptr, (int*)nullptr, n);
+    e = cub::DeviceScan::ExclusiveSum(nullptr, cub_b, (int*)nullptr, (int*)nullptr, n + 1);
     if (e != cudaSuccess) return e;
     const size_t cub_bytes = std::max(cub_a, cub_b);
 
@@ -1053,6 +1250,8 @@ cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, D
         int4* split;
         int2* child_fc;
         void* cub;
+        int *kp, *pre, *kc, *parent, *visit;   // kept-subset derivation
+        BNode* Q;
     } P;
     auto carve = [&](Carver& c) {
         P.plo = c.take<float4>(N);
@@ -1078,6 +1277,14 @@ cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, D
         P.split = c.take<int4>((size_t)max_work);
         P.child_fc = c.take<int2>((size_t)2 * max_work);
         P.cub = c.take<char>(cub_bytes);
+        if (keep) {
+            P.kp = c.take<int>(N + 1);
+            P.pre = c.take<int>(N + 1);
+            P.kc = c.take<int>(2 * N);
+            P.parent = c.take<int>(2 * N);
+            P.visit = c.take<int>(2 * N);
+            P.Q = c.take<BNode>(2 * N);
+        }
     };
     Carver dry{nullptr};
     carve(dry);
@@ -1088,7 +1295,9 @@ cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, D
     int* small_buf = nullptr;
     dev::QNode4* nodes_out = nullptr;
     float4* tris_out = nullptr;
-    int num_q = 0, depth = 0;
+    dev::QNode4* kept_nodes = nullptr;
+    float4* kept_tris = nullptr;
+    int num_q = 0, depth = 0, num_kq = 0, kdepth = 0, nkept = 0;
 #define CK(x) do { if ((e = (x)) != cudaSuccess) goto done; } while (0)
     {
         // 1. boxes and root
@@ -1171,28 +1380,40 @@ cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, D
         k_small<<<ns, kSmallThreads, 0, stream>>>(small_buf, small_buf + ns, P.plo, P.phi, P.idx, P.nodes, P.err);
         CK(cudaGetLastError());
 
-        // 4. collapse, breadth first
-        CK(cudaMemsetAsync(P.lvl_a, 0, sizeof(int), stream));   // level 0: the root, binary node 0
-        int m = 1, base = 0;
-        int* cur = P.lvl_a;
-        int* nxt = P.lvl_b;
-        while (m > 0) {
-            depth++;
-            k_collapse_count<<<(m + 127) / 128, 128, 0, stream>>>(cur, m, P.nodes, P.kids, P.nk, P.ninner);
-            size_t cb = cub_bytes;
-            CK(cub::DeviceScan::ExclusiveSum(P.cub, cb, P.ninner, P.off, m, stream));
-            k_collapse_emit<<<(m + 127) / 128, 128, 0, stream>>>(cur, m, base, P.kids, P.nk, P.off, P.nodes, P.qtmp, nxt);
-            CK(cudaGetLastError());
-            int last[2] = {0, 0};
-            CK(cudaMemcpyAsync(&last[0], P.off + (m - 1), sizeof(int), cudaMemcpyDeviceToHost, stream));
-            CK(cudaMemcpyAsync(&last[1], P.ninner + (m - 1), sizeof(int), cudaMemcpyDeviceToHost, stream));
-            CK(cudaStreamSynchronize(stream));
-            base += m;
-            m = last[0] + last[1];
-            std::swap(cur, nxt);
-            if (base + m > n) { e = cudaErrorInvalidValue; goto done; }
-        }
-        num_q = base;
+        // 4. collapse, breadth first from the binary node in P.lvl_a[0]: the
+        // 4-wide nodes go to P.qtmp; returns their count and the depth
+        auto collapse = [&](const BNode* tree, int ntris, int& count, int& levels) -> cudaError_t {
+            cudaError_t ce = cudaSuccess;
+            int m = 1, base = 0;
+            int* cur = P.lvl_a;
+            int* nxt = P.lvl_b;
+            levels = 0;
+            while (m > 0) {
+                levels++;
+                k_collapse_count<<<(m + 127) / 128, 128, 0, stream>>>(cur, m, tree, P.kids, P.nk, P.ninner);
+                size_t cb = cub_bytes;
+                if ((ce = cub::DeviceScan::ExclusiveSum(P.cub, cb, P.ninner, P.off, m, stream)) != cudaSuccess) return ce;
+                k_collapse_emit<<<(m + 127) / 128, 128, 0, stream>>>(cur, m, base, P.kids, P.nk, P.off, tree, P.qtmp,
+                                                                     nxt);
+                if ((ce = cudaGetLastError()) != cudaSuccess) return ce;
+                int last[2] = {0, 0};
+                if ((ce = cudaMemcpyAsync(&last[0], P.off + (m - 1), sizeof(int), cudaMemcpyDeviceToHost, stream)) !=
+                    cudaSuccess)
+                    return ce;
+                if ((ce = cudaMemcpyAsync(&last[1], P.ninner + (m - 1), sizeof(int), cudaMemcpyDeviceToHost, stream)) !=
+                    cudaSuccess)
+                    return ce;
+                if ((ce = cudaStreamSynchronize(stream)) != cudaSuccess) return ce;
+                base += m;
+                m = last[0] + last[1];
+                std::swap(cur, nxt);
+                if (base + m > ntris) return cudaErrorInvalidValue;
+            }
+            count = base;
+            return cudaSuccess;
+        };
+        CK(cudaMemsetAsync(P.lvl_a, 0, sizeof(int), stream));   // the root, binary node 0
+        CK(collapse(P.nodes, n, num_q, depth));
         int err_h = 0;
         CK(cudaMemcpyAsync(&err_h, P.err, sizeof(int), cudaMemcpyDeviceToHost, stream));
         CK(cudaStreamSynchronize(stream));
@@ -1204,6 +1425,32 @@ cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, D
         CK(cudaMemcpyAsync(nodes_out, P.qtmp, (size_t)num_q * sizeof(dev::QNode4), cudaMemcpyDeviceToDevice, stream));
         k_emit_tris<<<(n + 255) / 256, 256, 0, stream>>>(tris, subset, P.idx, n, tris_out, vertices);
         CK(cudaGetLastError());
+
+        // 6. the kept subset's tree, derived from this one
+        if (keep) {
+            const int nb = id;   // every id below is a node (or marked empty)
+            k_keep_pos<<<(n + 1 + 255) / 256, 256, 0, stream>>>(P.idx, n, keep, P.kp);
+            size_t cb = cub_bytes;
+            CK(cub::DeviceScan::ExclusiveSum(P.cub, cb, P.kp, P.pre, n + 1, stream));
+            CK(cudaMemcpyAsync(&nkept, P.pre + n, sizeof(int), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            if (nkept > 0) {
+                const int g = (nb + 255) / 256;
+                k_prune_count<<<g, 256, 0, stream>>>(P.nodes, nb, P.pre, P.kc, P.parent, P.visit);
+                k_prune_refit<<<g, 256, 0, stream>>>(P.nodes, nb, P.kc, P.pre, P.parent, P.idx, keep, P.plo, P.phi, P.Q,
+                                                     P.visit);
+                k_prune_link<<<g, 256, 0, stream>>>(P.nodes, nb, P.kc, P.pre, P.Q, P.lvl_a);
+                CK(cudaGetLastError());
+                CK(collapse(P.Q, nkept, num_kq, kdepth));
+                CK(dmalloc_async(&kept_nodes, (size_t)num_kq * sizeof(dev::QNode4), stream));
+                CK(dmalloc_async(&kept_tris, 3 * (size_t)nkept * sizeof(float4), stream));
+                CK(cudaMemcpyAsync(kept_nodes, P.qtmp, (size_t)num_kq * sizeof(dev::QNode4), cudaMemcpyDeviceToDevice,
+                                   stream));
+                k_prune_compact<<<(n + 255) / 256, 256, 0, stream>>>(P.idx, n, P.kp, P.pre, P.tmp);
+                k_emit_tris<<<(nkept + 255) / 256, 256, 0, stream>>>(tris, nullptr, P.tmp, nkept, kept_tris, vertices);
+                CK(cudaGetLastError());
+            }
+        }
         CK(cudaStreamSynchronize(stream));
     }
 done:
@@ -1213,7 +1460,16 @@ done:
     if (e != cudaSuccess) {
         dfree_async(nodes_out, stream);
         dfree_async(tris_out, stream);
+        dfree_async(kept_nodes, stream);
+        dfree_async(kept_tris, stream);
         return e;
+    }
+    if (kept_out && nkept > 0) {
+        kept_out->nodes = kept_nodes;
+        kept_out->tris = kept_tris;
+        kept_out->num_nodes = num_kq;
+        kept_out->num_tris = nkept;
+        kept_out->max_depth = kdepth;
     }
     out.nodes = nodes_out;
     out.tris = tris_out;
@@ -1226,9 +1482,10 @@ done:
 // The wavefront form's three triangle BVH4s of a resident scene (triangles
 // and materials already in the arena), built on the device.  The subsets
 // are the host's: passable = material transmission > 0.5 (in range), in
-// index order.  The tree over all triangles and the two subset trees are
-// built at the same time from two host threads on two streams.  Allocations
-// go to s.extra.
+// index order.  The blocking triangles' tree is derived from the tree over
+// all triangles (build_qbvh4_with_kept); the passable triangles' tree is
+// built at the same time from a second host thread on a second stream.
+// Allocations go to s.extra.
 cudaError_t build_wave_meshes_device(DeviceScene& s, cudaStream_t stream) {
     dev::DevScene& v = s.view;
     const int n = v.num_tris;
@@ -1240,7 +1497,7 @@ cudaError_t build_wave_meshes_device(DeviceScene& s, cudaStream_t stream) {
     unsigned char* flags = nullptr;
     void* cub_tmp = nullptr;
     int* num_sel = nullptr;
-    int npass = 0, nblock = 0;
+    int npass = 0;
     size_t cb = 0;
     cudaStream_t st2 = nullptr;
     cudaError_t e_all = cudaSuccess, e_sub = cudaSuccess;
@@ -1257,28 +1514,24 @@ cudaError_t build_wave_meshes_device(DeviceScene& s, cudaStream_t stream) {
     CK(cub::DeviceSelect::Flagged(nullptr, cb, iota, flags, sel, num_sel, n, stream));
     CK(dmalloc_async(&cub_tmp, cb, stream));
     CK(cub::DeviceSelect::Flagged(cub_tmp, cb, iota, flags, sel + n, num_sel, n, stream));          // passable
-    CK(cub::DeviceSelect::Flagged(cub_tmp, cb, iota, flags + n, sel, num_sel + 1, n, stream));      // blocking
-    {
-        int h[2] = {0, 0};
-        CK(cudaMemcpyAsync(h, num_sel, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
-        CK(cudaStreamSynchronize(stream));
-        npass = h[0];
-        nblock = h[1];
-    }
+    CK(cudaMemcpyAsync(&npass, num_sel, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
     {
         int dev_id = 0;
         CK(cudaGetDevice(&dev_id));
         auto subset_trees = [&] {
             cudaSetDevice(dev_id);
-            if (npass > 0 && nblock > 0) e_sub = build_qbvh4_device(v.tris, sel, nblock, blk, st2, wt);
-            if (npass > 0 && e_sub == cudaSuccess) e_sub = build_qbvh4_device(v.tris, sel + n, npass, pas, st2, wt);
+            if (npass > 0) e_sub = build_qbvh4_device(v.tris, sel + n, npass, pas, st2, wt);
         };
+        // with passable triangles present: the blocking ones' tree from the
+        // tree over all (flags + n: the blocking flags)
+        const unsigned char* keep = npass > 0 ? flags + n : nullptr;
         if (tuning().build_concurrent) {
             std::thread subsets(subset_trees);
-            e_all = build_qbvh4_device(v.tris, nullptr, n, all, stream, wt);
+            e_all = build_qbvh4_device(v.tris, nullptr, n, all, stream, wt, keep, keep ? &blk : nullptr);
             subsets.join();
         } else {
-            e_all = build_qbvh4_device(v.tris, nullptr, n, all, stream, wt);
+            e_all = build_qbvh4_device(v.tris, nullptr, n, all, stream, wt, keep, keep ? &blk : nullptr);
             subset_trees();
         }
         e = e_all != cudaSuccess ? e_all : e_sub;
@@ -1329,20 +1582,23 @@ extern "C" int sheen_bvh4_compare_builders(const SheenScene* scene, double* time
     using namespace sheen;
     if (!scene || scene->num_triangles <= 0 || !scene->triangles) { set_error("scene has no triangles"); return -1; }
     const int n = scene->num_triangles;
-    std::vector<int> all, block, pass;
+    std::vector<int> all, pass;
+    std::vector<unsigned char> blocking((size_t)n);
     for (int i = 0; i < n; i++) {
         all.push_back(i);
         const int m = scene->triangles[i].material_id;
         const bool passable = m >= 0 && m < scene->num_materials && scene->materials[m].transmission > 0.5f;
-        (passable ? pass : block).push_back(i);
+        if (passable) pass.push_back(i);
+        blocking[(size_t)i] = passable ? 0 : 1;
     }
     const double h0 = now_ms();
     QBvh hq[3];
     const bool wt = tuning().watertight != 0;   // both builders use the record layout in force
-    build_qbvh4(scene->triangles, all, hq[0], wt);
     if (!pass.empty()) {
-        build_qbvh4(scene->triangles, block, hq[1], wt);
+        build_qbvh4_with_kept(scene->triangles, n, blocking, hq[0], hq[1], wt);
         build_qbvh4(scene->triangles, pass, hq[2], wt);
+    } else {
+        build_qbvh4(scene->triangles, all, hq[0], wt);
     }
     const double host_ms = now_ms() - h0;
 

@@ -45,6 +45,18 @@ struct QBvh {
 // selects the record layout of the watertight triangle test.
 void build_qbvh4(const Triangle* tris, const std::vector<int>& subset, QBvh& out, bool vertices = false);
 
+// The BVH4 over all n triangles, and the one over the triangles with
+// keep[i] != 0 derived from it instead of built: the binary tree loses the
+// other triangles from its leaves, nodes left with one child are spliced
+// out, boxes are refitted to the kept triangles, and the result is collapsed
+// like a built tree.  kept_out is empty when nothing is kept.
+void build_qbvh4_with_kept(const Triangle* tris, int n, const std::vector<unsigned char>& keep, QBvh& all,
+                           QBvh& kept_out, bool vertices = false);
+
+// Every child box of q is exactly the quantised union of the boxes of the
+// original triangles (tris) below it; 0 or a negative code (host only).
+int check_qbvh4_tight(const QBvh& q, const Triangle* tris);
+
 // The same BVH4 built on the device (bvh4_gpu.cu), byte-identical to
 // build_qbvh4's.  nodes/tris are device allocations owned by the caller.
 struct DevQBvh {
@@ -54,8 +66,11 @@ struct DevQBvh {
     int num_tris = 0;
     int max_depth = 0;
 };
+// With keep_dev (one flag per triangle; subset_dev null) it also derives
+// build_qbvh4_with_kept's tree over the kept triangles into *kept_out.
 cudaError_t build_qbvh4_device(const Triangle* tris_dev, const int* subset_dev, int n, DevQBvh& out,
-                               cudaStream_t stream, bool vertices = false);
+                               cudaStream_t stream, bool vertices = false, const unsigned char* keep_dev = nullptr,
+                               DevQBvh* kept_out = nullptr);
 
 // Result/accounting of one render call.
 struct RenderTally {

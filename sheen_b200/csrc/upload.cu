@@ -287,21 +287,23 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
 
     // Wavefront form: BVH4 over all triangles, and -- when some triangles can
     // pass a shadow ray (transmission > 0.5, render_kernel.cu:261-262) -- one
-    // over the blocking triangles and one over the passable ones.
+    // over the blocking triangles (derived from the first) and one over the
+    // passable ones.
     QBvh q_all, q_block, q_pass;
     if (form == SHEEN_FORM_WAVEFRONT && !device_build && in->num_triangles > 0) {
-        std::vector<int> all, block, pass;
+        std::vector<int> all, pass;
+        std::vector<unsigned char> blocking((size_t)in->num_triangles);
         for (int i = 0; i < in->num_triangles; i++) {
             all.push_back(i);
             const int m = in->triangles[i].material_id;
             const bool passable = m >= 0 && m < in->num_materials && in->materials[m].transmission > 0.5f;
-            (passable ? pass : block).push_back(i);
+            if (passable) pass.push_back(i);
+            blocking[(size_t)i] = passable ? 0 : 1;
         }
         const bool wt = tuning().watertight != 0;
-        std::thread t1([&] { if (!pass.empty()) build_qbvh4(in->triangles, block, q_block, wt); });
         std::thread t2([&] { if (!pass.empty()) build_qbvh4(in->triangles, pass, q_pass, wt); });
-        build_qbvh4(in->triangles, all, q_all, wt);
-        t1.join();
+        if (!pass.empty()) build_qbvh4_with_kept(in->triangles, in->num_triangles, blocking, q_all, q_block, wt);
+        else build_qbvh4(in->triangles, all, q_all, wt);
         t2.join();
         // The traversal stack keeps at most 3 entries per level below the root.
         if (3 * std::max(q_all.max_depth, std::max(q_block.max_depth, q_pass.max_depth)) + 1 > 48) {

@@ -165,3 +165,45 @@ def test_host_builder_edge_cases(name):
     ptr, keep = sb._scene_ptr(scene)
     d = L.sheen_selfcheck_bvh4(ptr)
     assert 1 <= d <= 15, d
+
+
+def _kept_cases():
+    cases = {}
+    for n in (3, 9, 40, 1025, 5000):
+        rng = np.random.default_rng(n + 3)
+        cases[f"soup{n}_glass20"] = _mesh(_soup(n, n), rng.random(n) < 0.2)
+    cases["soup3000_glass90"] = _mesh(_soup(3000, 5), np.random.default_rng(9).random(3000) < 0.9)
+    cases["soup500_all_glass"] = _mesh(_soup(500, 6), np.ones(500, bool))
+    cases["soup500_one_blocking"] = _mesh(_soup(500, 8), np.arange(500) != 17)
+    cases["mesh_workload_detail4"] = sb.generate_scene(1, 3, 4)
+    return cases
+
+
+@pytest.mark.parametrize("name", sorted(_kept_cases()))
+def test_derived_blocking_tree(name):
+    """The blocking triangles' tree derived from the tree over all (leaves
+    lose the passable triangles, one-child nodes are spliced out, boxes
+    refitted): the tree over all is unchanged, the derived one holds every
+    blocking triangle once, and each of its child boxes is exactly the
+    quantised union of the triangles below it (a loose refit fails)."""
+    L = sb.lib()
+    L.sheen_selfcheck_bvh4_kept.argtypes = [ctypes.c_void_p]
+    L.sheen_selfcheck_bvh4_kept.restype = ctypes.c_int
+    scene = _kept_cases()[name]
+    ptr, keep = sb._scene_ptr(scene)
+    d = L.sheen_selfcheck_bvh4_kept(ptr)
+    if name == "soup500_all_glass":
+        assert d == 0
+    else:
+        assert 1 <= d <= 15, d
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["soup3000_glass90", "soup500_all_glass", "soup500_one_blocking", "soup40_glass20"])
+def test_derived_blocking_tree_device_identical(name):
+    """The device's derived blocking tree equals the host's byte for byte,
+    including a mostly-passable mesh, an all-passable one (no blocking tree)
+    and a single blocking triangle."""
+    _init()
+    rc, _ = _compare(_kept_cases()[name])
+    assert rc == 0, (rc, sb.last_error())
