@@ -302,8 +302,13 @@ int sheen_scene_profile_stages(SheenDeviceScene scene, int width, int height, in
  *   "wave.shadow_kernel"         0: every warp takes 32 shadow rays and
  *                                   finishes them together; 1 (default):
  *                                   lanes take new rays as theirs finish
- *   "wave.refill_min"            1..32 (default 8): idle lanes that make a
+ *   "wave.refill_min"            1..32 (default 16): idle lanes that make a
  *                                   warp take new rays (shadow_kernel 1)
+ *   "wave.inner_min"             0..32 (default 10): the refill shadow
+ *                                   stage ends a warp's inner-node phase
+ *                                   once fewer lanes than this still
+ *                                   descend while one waits at a leaf
+ *                                   (0: when none descends)
  *   "wave.shadow_blocks_per_sm"  0..16 (default 0 = as many as fit)
  *   "wave.shadow_stack"          0 (default): traversal stack of the refill
  *                                   shadow stage in local memory; 1: node
@@ -353,11 +358,12 @@ typedef struct SheenTuneResult {
     double best_ms;                                        /* frame time with it */
     double default_ms;                                     /* frame time with the setting in force before */
     int shadow_stack;                                      /* the setting kept: wave.shadow_stack */
+    int inner_min;                                         /* the setting kept: wave.inner_min */
 } SheenTuneResult;
 
 /* Autotuner: times candidate launch parameters (both shadow-stage variants,
- * refill thresholds 4/8/16/24, shadow blocks per SM, traversal stack in
- * local or shared memory) on a resident
+ * refill thresholds 8/16/24, inner-phase thresholds 0/6/10/14, shadow
+ * blocks per SM, traversal stack in local or shared memory) on a resident
  * SHEEN_FORM_WAVEFRONT scene for one frame shape -- per candidate one
  * warm-up frame, then `reps` frames timed with CUDA events -- and keeps the
  * fastest (process-wide, as sheen_tune_set).  Renders into a device buffer it

@@ -348,13 +348,15 @@ def tune_get(key: str) -> int:
     return v.value
 
 
-TUNE_KEYS = ("wave.shadow_kernel", "wave.refill_min", "wave.shadow_blocks_per_sm", "wave.shadow_stack")
+TUNE_KEYS = ("wave.shadow_kernel", "wave.refill_min", "wave.shadow_blocks_per_sm", "wave.shadow_stack",
+             "wave.inner_min")
 
 
 class TuneResult(ctypes.Structure):
     _fields_ = [("shadow_kernel", ctypes.c_int), ("refill_min", ctypes.c_int),
                 ("shadow_blocks_per_sm", ctypes.c_int), ("candidates", ctypes.c_int),
-                ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double), ("shadow_stack", ctypes.c_int)]
+                ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double), ("shadow_stack", ctypes.c_int),
+                ("inner_min", ctypes.c_int)]
 
 
 def autotune(scene: "DeviceScene", width: int, height: int, aa: int, reps: int = 3, cache: str | None = None,
@@ -383,6 +385,7 @@ def autotune(scene: "DeviceScene", width: int, height: int, aa: int, reps: int =
     _check(L.sheen_autotune(scene.handle, width, height, aa, reps, ctypes.byref(r)))
     res = {"wave.shadow_kernel": r.shadow_kernel, "wave.refill_min": r.refill_min,
            "wave.shadow_blocks_per_sm": r.shadow_blocks_per_sm, "wave.shadow_stack": r.shadow_stack,
+           "wave.inner_min": r.inner_min,
            "candidates": r.candidates,
            "best_ms": r.best_ms, "default_ms": r.default_ms}
     if cache:

@@ -356,7 +356,11 @@ __global__ void __launch_bounds__(128) wave_shadow(DevScene S0, WaveView V0) {
 // together: inner nodes until every busy lane sits on a leaf, then one leaf
 // each.  A lane whose ray is finished goes idle; once `refill_min` lanes are
 // idle the warp claims that many new rays from the queue in one atomic, so
-// long rays no longer hold 31 finished lanes hostage.  The mesh walks are
+// long rays no longer hold 31 finished lanes hostage.  With `inner_min` > 0
+// the inner-node phase also ends once fewer than inner_min lanes are still
+// descending while some lane waits at a leaf: the descending lanes carry on
+// in the next round (beside the refilled rays) instead of running the
+// phase's tail with a few lanes.  The mesh walks are
 // qmesh_trace's, step for step (same child order, same stack, same tests),
 // so every ray's result is the one wave_shadow computes.
 //
@@ -367,7 +371,8 @@ __global__ void __launch_bounds__(128) wave_shadow(DevScene S0, WaveView V0) {
 // 4 useful bytes; the entry distances (closest-hit walks of the passable set
 // only) stay in local memory.  24 KB per 128-thread block.
 template <int F, bool SMEM_STACK, bool MULTI>
-__global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveView V0, int refill_min) {
+__global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveView V0, int refill_min,
+                                                             int inner_min) {
     using T = FastTracer<false, F>;
     constexpr unsigned int kFull = 0xffffffffu;
     constexpr uint32_t kLeafBit = 0x80000000u;
@@ -517,8 +522,11 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveVi
         }
         // ---- inner nodes until every walking lane sits on a leaf ------------
         while (true) {
-            const bool inner = (state == kWalkPass || state == kWalkBlock) && !(entry & kLeafBit);
-            if (!__any_sync(kFull, inner)) break;
+            const bool walking = state == kWalkPass || state == kWalkBlock;
+            const bool inner = walking && !(entry & kLeafBit);
+            const unsigned int descending = __ballot_sync(kFull, inner);
+            if (!descending) break;
+            if (__popc(descending) < inner_min && __any_sync(kFull, walking && (entry & kLeafBit))) break;
             if (!inner) continue;
             float tn[4];
             uint4 ch;
@@ -564,8 +572,8 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveVi
             }
             if (ended) state = state == kWalkPass ? kEndPass : kEndBlock;
         }
-        // ---- one leaf per walking lane --------------------------------------
-        if (state == kWalkPass || state == kWalkBlock) {
+        // ---- one leaf per walking lane at a leaf -----------------------------
+        if ((state == kWalkPass || state == kWalkBlock) && (entry & kLeafBit)) {
             const int first = (int)((entry & 0x7fffffffu) >> 3);
             const int count = (int)(entry & 7u) + 1;
             bool ended = false;
@@ -892,9 +900,10 @@ static cudaError_t run_pipeline(const dev::DevScene& S0, const dev::WaveView& V,
         if (!refill)
             dev::wave_shadow<F, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V);
         else if (smem)
-            dev::wave_shadow_refill<F, true, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V, tu.refill_min);
+            dev::wave_shadow_refill<F, true, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V, tu.refill_min, tu.inner_min);
         else
-            dev::wave_shadow_refill<F, false, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V, tu.refill_min);
+            dev::wave_shadow_refill<F, false, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V, tu.refill_min,
+                                                                                  tu.inner_min);
     };
     int mark = 0;
     auto stage_end = [&]() {

@@ -27,6 +27,7 @@ struct Key {
 const Key kKeys[] = {
     {"wave.shadow_kernel", &Tuning::shadow_kernel, 0, 1},
     {"wave.refill_min", &Tuning::refill_min, 1, 32},
+    {"wave.inner_min", &Tuning::inner_min, 0, 32},
     {"wave.shadow_blocks_per_sm", &Tuning::shadow_blocks_per_sm, 0, 16},
     {"wave.shadow_stack", &Tuning::shadow_stack, 0, 1},
     {"build.device", &Tuning::build_device, 0, 1},
@@ -88,7 +89,7 @@ namespace sheen {
 namespace {
 
 struct Candidate {
-    int shadow_kernel, refill_min, shadow_blocks_per_sm, shadow_stack;
+    int shadow_kernel, refill_min, shadow_blocks_per_sm, shadow_stack, inner_min;
 };
 
 void apply(const Candidate& c) {
@@ -96,6 +97,7 @@ void apply(const Candidate& c) {
     tuning_set("wave.refill_min", c.refill_min);
     tuning_set("wave.shadow_blocks_per_sm", c.shadow_blocks_per_sm);
     tuning_set("wave.shadow_stack", c.shadow_stack);
+    tuning_set("wave.inner_min", c.inner_min);
 }
 
 }  // namespace
@@ -110,11 +112,12 @@ extern "C" int sheen_autotune(SheenDeviceScene h, int W, int H, int aa, int reps
     if (reps < 1) reps = 3;
     const Tuning t0 = tuning();
     std::vector<Candidate> cands;
-    cands.push_back({t0.shadow_kernel, t0.refill_min, t0.shadow_blocks_per_sm, t0.shadow_stack});
-    cands.push_back({0, t0.refill_min, 0, 0});
+    cands.push_back({t0.shadow_kernel, t0.refill_min, t0.shadow_blocks_per_sm, t0.shadow_stack, t0.inner_min});
+    cands.push_back({0, t0.refill_min, 0, 0, 0});
     for (int st : {0, 1})
-        for (int r : {4, 8, 16, 24})
-            for (int b : {0, 4}) cands.push_back({1, r, b, st});
+        for (int r : {8, 16, 24})
+            for (int im : {0, 6, 10, 14}) cands.push_back({1, r, 0, st, im});
+    cands.push_back({1, 16, 4, 0, 10});
     float4* buf = nullptr;
     cudaStream_t st = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -143,7 +146,7 @@ extern "C" int sheen_autotune(SheenDeviceScene h, int W, int H, int aa, int reps
     if (st) cudaStreamDestroy(st);
     dfree(buf);
     if (e != cudaSuccess) {
-        apply({t0.shadow_kernel, t0.refill_min, t0.shadow_blocks_per_sm, t0.shadow_stack});
+        apply({t0.shadow_kernel, t0.refill_min, t0.shadow_blocks_per_sm, t0.shadow_stack, t0.inner_min});
         set_error(cudaGetErrorString(e));
         return -1;
     }
@@ -152,6 +155,7 @@ extern "C" int sheen_autotune(SheenDeviceScene h, int W, int H, int aa, int reps
     out->refill_min = cands[best_i].refill_min;
     out->shadow_blocks_per_sm = cands[best_i].shadow_blocks_per_sm;
     out->shadow_stack = cands[best_i].shadow_stack;
+    out->inner_min = cands[best_i].inner_min;
     out->candidates = (int)cands.size();
     out->best_ms = best;
     out->default_ms = first;

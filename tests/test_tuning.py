@@ -12,7 +12,8 @@ import pytest
 
 import sheen_b200 as sb
 
-DEFAULTS = {"wave.shadow_kernel": 1, "wave.refill_min": 8, "wave.shadow_blocks_per_sm": 0, "wave.shadow_stack": 0}
+DEFAULTS = {"wave.shadow_kernel": 1, "wave.refill_min": 16, "wave.shadow_blocks_per_sm": 0, "wave.shadow_stack": 0,
+            "wave.inner_min": 10}
 
 
 @pytest.fixture
@@ -52,12 +53,15 @@ def test_shadow_variants_give_identical_images(config, seed, detail, photons, sp
     ref, st0 = ds.render_host(W, H, spp, count_rays=True)
     assert np.isfinite(ref).all()
     sb.tune_set("wave.shadow_kernel", 1)
-    for refill, per_sm, stack in ((1, 0, 0), (8, 0, 0), (32, 0, 0), (8, 1, 0), (8, 0, 1), (1, 0, 1), (24, 2, 1)):
+    for refill, per_sm, stack, inner in ((1, 0, 0, 0), (8, 0, 0, 0), (32, 0, 0, 0), (8, 1, 0, 0), (8, 0, 1, 0),
+                                         (1, 0, 1, 0), (24, 2, 1, 0), (16, 0, 0, 10), (16, 0, 1, 10), (1, 0, 0, 32),
+                                         (32, 0, 0, 1), (8, 1, 1, 20)):
         sb.tune_set("wave.refill_min", refill)
         sb.tune_set("wave.shadow_blocks_per_sm", per_sm)
         sb.tune_set("wave.shadow_stack", stack)
+        sb.tune_set("wave.inner_min", inner)
         img, st = ds.render_host(W, H, spp, count_rays=True)
-        assert np.array_equal(img, ref), (refill, per_sm, stack, float(np.abs(img - ref).max()))
+        assert np.array_equal(img, ref), (refill, per_sm, stack, inner, float(np.abs(img - ref).max()))
         assert st["total_rays"] == st0["total_rays"]
     ds.close()
     scene.close()
