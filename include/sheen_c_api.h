@@ -325,6 +325,13 @@ int sheen_scene_profile_stages(SheenDeviceScene scene, int width, int height, in
  *                                   a vertex; hits may differ from the
  *                                   reference's on edges).  Read at
  *                                   sheen_scene_create.
+ *   "build.node_cost"            1..64 (default 4): the SAH cost of a node
+ *                                   visit in quarters of a triangle test,
+ *                                   against which the triangle BVH4
+ *                                   builders weigh a leaf of <= 8
+ *                                   triangles (larger: bigger leaves,
+ *                                   fewer nodes).  Read at
+ *                                   sheen_scene_create.
  *   "build.device"               1 (default): the wavefront form's triangle
  *                                   BVH4s are built on the GPU; 0: on the
  *                                   host.  Both builders give byte-identical

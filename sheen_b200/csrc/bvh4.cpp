@@ -67,6 +67,7 @@ constexpr int kBins = bvhr::kBins;
 constexpr int kMaxLeaf = bvhr::kMaxLeaf;
 
 struct SahBuilder {
+    float node_cost = 1.0f;   // a node visit in triangle tests ("build.node_cost")
     std::vector<Box> tri_box;
     std::vector<float> cen;   // 3 per triangle
     std::vector<int> idx;
@@ -117,10 +118,8 @@ struct SahBuilder {
                 if (cost < best_cost) { best_cost = cost; best_axis = axis; best_split = i; }
             }
         }
-        const float leaf_cost = bvhr::mul(b.area(), (float)n);
-        const float parent_area = b.area();
-        // cost model: traversal 1 (scaled by the parent area), intersection 1 per triangle
-        if (best_axis < 0 || (n <= kMaxLeaf && leaf_cost <= bvhr::add(parent_area, best_cost))) {
+        // cost model: a node visit node_cost, a triangle test 1 (both scaled by the area)
+        if (best_axis < 0 || (n <= kMaxLeaf && bvhr::leaf_wins(b.area(), n, best_cost, node_cost))) {
             if (n <= kMaxLeaf) { out[(size_t)me].first = first; out[(size_t)me].count = n; return me; }
         }
         int mid;
@@ -163,6 +162,7 @@ struct SahBuilder {
 // triangle, then the recursive build.  Returns the root of `bn`.
 int sah_build(const Triangle* tris, const std::vector<int>& subset, SahBuilder& sb, std::vector<BNode>& bn) {
     const int n = (int)subset.size();
+    sb.node_cost = bvhr::node_cost_of(tuning().node_cost);
     sb.tri_box.resize((size_t)n);
     sb.cen.resize(3 * (size_t)n);
     sb.idx.resize((size_t)n);

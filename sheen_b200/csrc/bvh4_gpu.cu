@@ -592,7 +592,8 @@ __device__ __forceinline__ float warp_max(float v) {
 // the block's permutation of local triangle slots; box: their boxes
 // (6 x kSmall); bins: this warp's kAxisWords ints; stack: this warp's
 // kTinyStack frames; next_id: the block's id counter.
-__device__ void build_tiny(TinyFrame root, unsigned short* __restrict__ perm, const float (*box)[kSmall], int gfirst,
+__device__ void build_tiny(TinyFrame root, float node_cost, unsigned short* __restrict__ perm,
+                           const float (*box)[kSmall], int gfirst,
                            int* __restrict__ bins, TinyFrame* __restrict__ stack, int* next_id,
                            BNode* __restrict__ nodes, int* __restrict__ err) {
     const unsigned full = 0xffffffffu;
@@ -637,8 +638,7 @@ __device__ void build_tiny(TinyFrame root, unsigned short* __restrict__ perm, co
             }
             best = bi == INT_MAX ? -1 : bi;
             const float pa = area(lo[0], lo[1], lo[2], hi[0], hi[1], hi[2]);
-            const float leaf_cost = mul(pa, (float)m);
-            if (best < 0 || (m <= kMaxLeaf && leaf_cost <= add(pa, bc))) leaf = m <= kMaxLeaf;
+            if (best < 0 || (m <= kMaxLeaf && leaf_wins(pa, m, bc, node_cost))) leaf = m <= kMaxLeaf;
         }
         BNode o;
         for (int q = 0; q < 3; q++) { o.lo[q] = lo[q]; o.hi[q] = hi[q]; o.clo[q] = clo[q]; o.chi[q] = chi[q]; }
@@ -703,7 +703,7 @@ static_assert(kSmall <= 1024 && kTiny <= 32 && 2 * kSmall - 2 < 2047, "tiny list
 __global__ void __launch_bounds__(kSmallThreads, 6) k_small(const int* __restrict__ list, const int* __restrict__ id_base,
                                                          const float4* __restrict__ plo, const float4* __restrict__ phi,
                                                          int* __restrict__ idx, BNode* __restrict__ nodes,
-                                                         int* __restrict__ err) {
+                                                         int* __restrict__ err, float node_cost) {
     __shared__ float s_box[6][kSmall];
     __shared__ int s_pid[kSmall];
     __shared__ unsigned short s_perm[kSmall];
@@ -804,9 +804,8 @@ __global__ void __launch_bounds__(kSmallThreads, 6) k_small(const int* __restric
                         if (s_axis_cost[a] < bc) { bc = s_axis_cost[a]; bi = s_axis_cand[a]; }
                     const int best = bi == INT_MAX ? -1 : bi;
                     const float pa = area(cur.lo[0], cur.lo[1], cur.lo[2], cur.hi[0], cur.hi[1], cur.hi[2]);
-                    const float leaf_cost = mul(pa, (float)n);
                     int lf = 0;
-                    if (best < 0 || (n <= kMaxLeaf && leaf_cost <= add(pa, bc))) {
+                    if (best < 0 || (n <= kMaxLeaf && leaf_wins(pa, n, bc, node_cost))) {
                         if (n <= kMaxLeaf) lf = 1;
                     }
                     s_best = best;
@@ -948,7 +947,7 @@ __global__ void __launch_bounds__(kSmallThreads, 6) k_small(const int* __restric
             f.count = (unsigned short)(((w >> 10) & 31u) + 1u);
             const unsigned rel = w >> 15;
             f.id = rel == 2047u ? root : id0 + (int)rel;
-            build_tiny(f, s_perm, s_box, gfirst, wbins, wstack, &s_next, nodes, err);
+            build_tiny(f, node_cost, s_perm, s_box, gfirst, wbins, wstack, &s_next, nodes, err);
         }
     }
     __syncthreads();
@@ -1377,7 +1376,8 @@ cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, D
             }();
             (void)carveout;
         }
-        k_small<<<ns, kSmallThreads, 0, stream>>>(small_buf, small_buf + ns, P.plo, P.phi, P.idx, P.nodes, P.err);
+        k_small<<<ns, kSmallThreads, 0, stream>>>(small_buf, small_buf + ns, P.plo, P.phi, P.idx, P.nodes, P.err,
+                                                  node_cost_of(tuning().node_cost));
         CK(cudaGetLastError());
 
         // 4. collapse, breadth first from the binary node in P.lvl_a[0]: the

@@ -86,6 +86,18 @@ BVH_HD int bin_of(float c, float lo, float k) {
 
 BVH_HD float bin_scale(float ext) { return div((float)kBins, ext); }
 
+// Leaf or split for a node of n <= kMaxLeaf triangles with box area pa and
+// best split cost best_cost (both sides' area x count): the leaf wins when
+// its n tests cost no more than one node visit (node_cost, in triangle
+// tests, scaled by the area) plus the split's tests.  node_cost 1 is exact
+// (1 * pa == pa).
+BVH_HD bool leaf_wins(float pa, int n, float best_cost, float node_cost) {
+    return mul(pa, (float)n) <= add(mul(node_cost, pa), best_cost);
+}
+
+// node_cost from the "build.node_cost" setting (quarters of a triangle test).
+BVH_HD float node_cost_of(int quarters) { return (float)quarters * 0.25f; }
+
 // Smallest e with 2^e >= v for v > 0 (frexp is exact; log2 is not).
 BVH_HD int ceil_log2(double v) {
     int x = 0;

@@ -171,6 +171,7 @@ struct Tuning {
     int shadow_kernel = 1;          // 0: 32-ray batches per warp; 1: per-lane refill
     int refill_min = 16;            // idle lanes that trigger a refill (shadow_kernel 1)
     int inner_min = 10;             // refill shadow stage: descending lanes below which the node phase ends
+    int node_cost = 4;              // triangle BVH4 build: a node visit's SAH cost, in quarters of a triangle test
     int shadow_blocks_per_sm = 0;   // 128-thread blocks per SM for the shadow stage; 0: occupancy limit
     int shadow_stack = 0;           // refill shadow stage: traversal stack nodes in 0 local / 1 shared memory
     int build_device = 1;           // wavefront triangle BVH4s: 1 built on the device, 0 on the host

@@ -28,6 +28,7 @@ const Key kKeys[] = {
     {"wave.shadow_kernel", &Tuning::shadow_kernel, 0, 1},
     {"wave.refill_min", &Tuning::refill_min, 1, 32},
     {"wave.inner_min", &Tuning::inner_min, 0, 32},
+    {"build.node_cost", &Tuning::node_cost, 1, 64},
     {"wave.shadow_blocks_per_sm", &Tuning::shadow_blocks_per_sm, 0, 16},
     {"wave.shadow_stack", &Tuning::shadow_stack, 0, 1},
     {"build.device", &Tuning::build_device, 0, 1},

@@ -207,3 +207,33 @@ def test_derived_blocking_tree_device_identical(name):
     _init()
     rc, _ = _compare(_kept_cases()[name])
     assert rc == 0, (rc, sb.last_error())
+
+
+@pytest.mark.parametrize("node_cost", [1, 8, 64])
+def test_node_cost_setting_host_trees_valid(node_cost):
+    """build.node_cost (the SAH price of a node visit against a triangle
+    test) changes the leaf sizes; the trees stay valid and tight."""
+    L = sb.lib()
+    L.sheen_selfcheck_bvh4_kept.argtypes = [ctypes.c_void_p]
+    L.sheen_selfcheck_bvh4_kept.restype = ctypes.c_int
+    scene = _kept_cases()["mesh_workload_detail4"]
+    ptr, keep = sb._scene_ptr(scene)
+    sb.tune_set("build.node_cost", node_cost)
+    try:
+        d = L.sheen_selfcheck_bvh4_kept(ptr)
+    finally:
+        sb.tune_set("build.node_cost", 4)
+    assert 1 <= d <= 15, d
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("node_cost", [2, 8])
+def test_node_cost_setting_device_identical(node_cost):
+    """Both builders read build.node_cost and stay byte-identical."""
+    _init()
+    sb.tune_set("build.node_cost", node_cost)
+    try:
+        rc, _ = _compare(sb.generate_scene(1, 3, 6))
+    finally:
+        sb.tune_set("build.node_cost", 4)
+    assert rc == 0, (rc, sb.last_error())
