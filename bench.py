@@ -45,7 +45,7 @@ CPU_BAND = (480, 512)
 # one-pass ncu capture of the full-size mesh frame (profiles/
 # wave_shadow_refill_mesh_1920x1080_4spp_dram.md); the roofline's traffic
 # per launch is this times the launch's shadow rays.
-SHADOW_DRAM_BYTES_PER_RAY = 5159825152 / 38552584      # pixel rows of the CPU samples (two 16-row blocks of the 1080-row frame)
+SHADOW_DRAM_BYTES_PER_RAY = 5061321984 / 38552584
 
 
 class quiet_stdout:
