@@ -183,7 +183,18 @@ int sheen_scene_render_host(SheenDeviceScene h, int W, int H, int aa, float* out
     if (e != cudaSuccess) return fail_cuda(e);
     int rc = render_device(*s, W, H, aa, sheen::Region{0, 0, W, H}, d, 0, flags, stats);
     if (rc == 0) {
-        e = cudaMemcpy(out_host, d, (size_t)W * H * sizeof(float4), cudaMemcpyDeviceToHost);
+        // a pinned destination takes the copy directly; a pageable one of
+        // more than a few MB goes through the pinned ring
+        const size_t bytes = (size_t)W * H * sizeof(float4);
+        cudaPointerAttributes pa{};
+        const bool pinned = cudaPointerGetAttributes(&pa, out_host) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        if (pinned || bytes < ((size_t)8 << 20)) {
+            e = cudaMemcpy(out_host, d, bytes, cudaMemcpyDeviceToHost);
+        } else {
+            e = cudaStreamSynchronize(0);
+            if (e == cudaSuccess) e = sheen::download_to_host(out_host, d, bytes);
+        }
         if (e != cudaSuccess) rc = fail_cuda(e);
     }
     sheen::dfree(d);

@@ -166,6 +166,11 @@ cudaError_t launch_wavefront_batch(const std::vector<BatchItem>& items, cudaStre
 cudaError_t profile_wavefront(DeviceScene& s, int W, int H, int aa, float4* out, cudaStream_t stream,
                               SheenStageProfile* prof);
 
+// Device -> host copy into pageable memory through the library's pinned
+// ring, several host threads sharing the copies (upload.cu).  The source
+// must be complete.
+cudaError_t download_to_host(void* dst, const void* src, size_t bytes);
+
 // Launch parameters of the wavefront form (tuning.cpp).
 struct Tuning {
     int shadow_kernel = 1;          // 0: 32-ray batches per warp; 1: per-lane refill

@@ -803,6 +803,9 @@ struct Wave {
     size_t bytes = 0;
     int sms = 148;
     // The frame's launch sequence captured once per frame shape and replayed.
+    // The first frame of a shape is launched directly (a scene rendered once,
+    // as by the one-call entry points, never pays for a capture); the graph
+    // is captured when the same shape comes again.
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t exec = nullptr;
     struct Key {
@@ -814,6 +817,8 @@ struct Wave {
                    out == o.out && tuning == o.tuning;
         }
     } key{};
+    Key direct{};              // shape of the last frame launched directly
+    bool has_direct = false;
 };
 
 static size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
@@ -1044,9 +1049,17 @@ cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, fl
     const dev::WaveView V = make_view(s, *w, W, H, ns, rg);
     const int npad = (int)region_padded(rg);
     const bool simple = simple_scene(s);
-    // Replay the captured frame when the shape and output match; otherwise
-    // capture the sequence on the scene's own stream and instantiate it.
+    // Replay the captured frame when the shape and output match.  A shape
+    // seen for the first time is launched directly; on its second frame the
+    // sequence is captured on the scene's own stream and instantiated.
     const Wave::Key key{W, H, aa, rg.x0, rg.y0, rg.x1, rg.y1, out, tuning_generation()};
+    if ((!w->exec || !(w->key == key)) && !(w->has_direct && w->direct == key)) {
+        w->direct = key;
+        w->has_direct = true;
+        return dispatch_variant(simple, watertight_scene(s), [&](auto f) {
+            return run_pipeline<decltype(f)::value>(s.view, V, npad, out, stream, s.d_tally);
+        });
+    }
     if (!w->exec || !(w->key == key)) {
         if (w->exec) { cudaGraphExecDestroy(w->exec); w->exec = nullptr; }
         if (!w->capture_stream &&

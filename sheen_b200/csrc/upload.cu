@@ -157,6 +157,68 @@ cudaError_t upload_items(const std::vector<Copy>& items) {
     return e;
 }
 
+}  // namespace
+
+// Device -> host copy into pageable memory through the same pinned ring:
+// each worker queues the copy of its next chunk into one of its two slots
+// while it copies the previous chunk out of the other, so the DMA overlaps
+// the host copies, which several cores share (together with the page faults
+// of a freshly allocated destination).  The source must be complete: the
+// caller has synchronised the stream that wrote it.
+cudaError_t download_to_host(void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return cudaSuccess;
+    int dev_id = 0;
+    cudaError_t e = cudaGetDevice(&dev_id);
+    if (e != cudaSuccess) return e;
+    if (dev_id < 0 || dev_id >= kUpMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_up_mu);
+    UploadRing& r = g_up[dev_id];
+    if ((e = ring_init(r)) != cudaSuccess) return e;
+    const size_t nchunks = (bytes + kUpSlot - 1) / kUpSlot;
+    const int workers = (int)std::min<size_t>(kUpWorkers, nchunks);
+    std::vector<cudaError_t> err((size_t)workers, cudaSuccess);
+    char* d = static_cast<char*>(dst);
+    const char* s = static_cast<const char*>(src);
+    auto len = [&](size_t c) { return std::min(kUpSlot, bytes - c * kUpSlot); };
+    auto work = [&](int w) {
+        cudaSetDevice(dev_id);
+        size_t prev = 0;
+        int prev_sl = -1, k = 0;
+        cudaError_t we = cudaSuccess;
+        for (size_t c = (size_t)w; c < nchunks && we == cudaSuccess; c += (size_t)workers, k++) {
+            const int sl = 2 * w + (k & 1);
+            we = cudaEventSynchronize(r.ev[sl]);
+            if (we == cudaSuccess)
+                we = cudaMemcpyAsync(r.slot[sl], s + c * kUpSlot, len(c), cudaMemcpyDeviceToHost, r.st[w]);
+            if (we == cudaSuccess) we = cudaEventRecord(r.ev[sl], r.st[w]);
+            if (we == cudaSuccess && prev_sl >= 0) {
+                we = cudaEventSynchronize(r.ev[prev_sl]);
+                if (we == cudaSuccess) std::memcpy(d + prev * kUpSlot, r.slot[prev_sl], len(prev));
+            }
+            prev = c;
+            prev_sl = sl;
+        }
+        if (we == cudaSuccess && prev_sl >= 0) {
+            we = cudaEventSynchronize(r.ev[prev_sl]);
+            if (we == cudaSuccess) std::memcpy(d + prev * kUpSlot, r.slot[prev_sl], len(prev));
+        }
+        err[(size_t)w] = we;
+    };
+    if (workers == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> th;
+        for (int w = 1; w < workers; w++) th.emplace_back(work, w);
+        work(0);
+        for (auto& t : th) t.join();
+    }
+    for (cudaError_t we : err)
+        if (e == cudaSuccess) e = we;
+    return e;
+}
+
+namespace {
+
 template <class T>
 void push_box(std::vector<float>& lo, std::vector<float>& hi, const T a[3], const T b[3]) {
     for (int k = 0; k < 3; k++) { lo.push_back(a[k]); hi.push_back(b[k]); }
