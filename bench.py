@@ -240,8 +240,11 @@ def run_ours(args):
     # end to end through the drop-in call: host scene arrays in, host RGBA
     # out, per step: BVH build + scene upload + render + read back
     img = np.empty((H, W, 4), np.float32)
-    e2e_steps = max(1, min(args.steps, 2))
-    sb.render_rgba(scene, W, H, SPP, form)          # warm the allocation paths
+    e2e_steps = max(1, min(args.steps, 3))
+    # warm-up calls: the library's memory pool grows to its working set over
+    # the first one or two calls (measured: 80 ms builds, then 13.5 ms)
+    for _ in range(max(1, args.warmup)):
+        sb.render_rgba(scene, W, H, SPP, form)
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):

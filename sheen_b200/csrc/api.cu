@@ -114,6 +114,7 @@ void sheen_cleanup(void) {
         g_scenes.clear();
     }
     cudaDeviceSynchronize();
+    sheen::release_parked_waves();
     sheen::release_upload_rings();
     sheen::release_pools();
     cudaDeviceReset();

@@ -136,6 +136,8 @@ cudaError_t launch_mega_bvh4(const DeviceScene& s, int W, int H, int aa, Region 
 cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
                              bool count_nodes);
 void wave_release(DeviceScene& s);
+// Frees the queue blocks kept from released scenes (render_wave.cu).
+void release_parked_waves();
 
 // Wavefront form on caller-owned scratch (the request loop: one block per
 // in-flight request).  Renders a region with the queue kernels launched

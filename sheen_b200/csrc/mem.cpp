@@ -75,6 +75,7 @@ static cudaError_t pool_alloc(void** ptr, size_t bytes, cudaStream_t stream, boo
     e = cudaMallocFromPoolAsync(ptr, bytes, p->pool, st);
     if (e == cudaErrorMemoryAllocation) {
         cudaGetLastError();
+        release_parked_waves();
         cudaDeviceSynchronize();
         cudaMemPoolTrimTo(p->pool, 0);
         e = cudaMallocFromPoolAsync(ptr, bytes, p->pool, st);
@@ -96,6 +97,7 @@ void trim_pool() {
     if (cudaGetDevice(&dev) != cudaSuccess) return;
     DevPool* p = nullptr;
     if (pool_of(dev, p) != cudaSuccess) return;
+    release_parked_waves();
     cudaDeviceSynchronize();
     cudaMemPoolTrimTo(p->pool, 0);
 }

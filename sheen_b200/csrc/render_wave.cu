@@ -947,9 +947,63 @@ static void wave_free(Wave* w) {
     delete w;
 }
 
+// A released scene's queue block is kept (one per device, the larger one)
+// for the next scene that fits: the one-call entry points upload, render and
+// release a scene per call, and a 4 GB pool allocation was measured at about
+// 5 ms on a B200 even with the freed block in the pool.  The kept block goes
+// back to the pool at sheen_cleanup, when the pool trims, before an
+// allocation that ran out of memory is retried, and not at all with
+// "mem.pool_keep_mb" 0.
+namespace {
+constexpr int kParkDevices = 64;
+std::mutex g_park_mu;
+Wave* g_parked[kParkDevices] = {};
+}  // namespace
+
+static Wave* take_parked(size_t bytes) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kParkDevices) return nullptr;
+    std::lock_guard<std::mutex> lk(g_park_mu);
+    Wave* w = g_parked[dev];
+    if (!w || w->bytes < bytes) return nullptr;
+    g_parked[dev] = nullptr;
+    return w;
+}
+
+void release_parked_waves() {
+    std::lock_guard<std::mutex> lk(g_park_mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (int d = 0; d < kParkDevices; d++) {
+        if (!g_parked[d]) continue;
+        cudaSetDevice(d);
+        wave_free(g_parked[d]);
+        g_parked[d] = nullptr;
+    }
+    cudaSetDevice(cur);
+}
+
 void wave_release(DeviceScene& s) {
-    wave_free(s.wave);
+    Wave* w = s.wave;
     s.wave = nullptr;
+    if (!w) return;
+    int dev = 0;
+    if (tuning().pool_keep_mb <= 0 || cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kParkDevices) {
+        wave_free(w);
+        return;
+    }
+    cudaDeviceSynchronize();   // as a free: no frame of the released scene may still run
+    if (w->exec) { cudaGraphExecDestroy(w->exec); w->exec = nullptr; }
+    w->key = Wave::Key{};
+    w->has_direct = false;
+    std::lock_guard<std::mutex> lk(g_park_mu);
+    Wave*& slot = g_parked[dev];
+    if (slot && slot->bytes >= w->bytes) {
+        wave_free(w);
+    } else {
+        wave_free(slot);
+        slot = w;
+    }
 }
 
 static bool wave_supported(const DeviceScene& s) {
@@ -968,9 +1022,16 @@ static cudaError_t wave_reserve_into(Wave*& w, int L, long long nsamples) {
         wave_carve(*w, w->block, w->bytes, L, nsamples);
         return cudaSuccess;
     }
+    const size_t bytes = wave_scratch_bytes(L, nsamples);
+    if (!w) {
+        if (Wave* p = take_parked(bytes)) {
+            w = p;
+            wave_carve(*w, w->block, w->bytes, L, nsamples);
+            return cudaSuccess;
+        }
+    }
     wave_free(w);
     w = new Wave();
-    const size_t bytes = wave_scratch_bytes(L, nsamples);
     cudaError_t e = dmalloc(&w->block, bytes);
     if (e != cudaSuccess) {
         delete w;

@@ -52,3 +52,34 @@ def test_pageable_readback_through_ring(W, H):
     ds.close()
     assert np.array_equal(host, dev.cpu().numpy())
     assert np.isfinite(host).all() and host.any()
+
+
+@pytest.mark.gpu
+def test_kept_queue_block_reused_across_scenes():
+    """A released scene's queue block is kept and handed to the next scene
+    that fits (other lights, a smaller frame): images equal those rendered
+    with freshly allocated blocks (mem.pool_keep_mb 0 keeps nothing)."""
+    sb.init(0, 100)
+    a = sb.generate_scene(1, 21, 3)        # 4 lights
+    b = sb.generate_scene(0, 22, 0)        # spheres, other lights
+    shapes = [(a, 320, 200, 2), (b, 256, 128, 1), (a, 160, 100, 4), (b, 320, 200, 2)]
+
+    def run():
+        imgs = []
+        for sc, W, H, spp in shapes:
+            ds = sb.DeviceScene(sc, sb.FORM_WAVEFRONT)
+            img, _ = ds.render_host(W, H, spp)
+            img2, _ = ds.render_host(W, H, spp)   # the captured graph over the same block
+            assert np.array_equal(img, img2)
+            ds.close()
+            imgs.append(img)
+        return imgs
+
+    kept = run()
+    sb.tune_set("mem.pool_keep_mb", 0)
+    try:
+        fresh = run()
+    finally:
+        sb.tune_set("mem.pool_keep_mb", 16384)
+    for k, f in zip(kept, fresh):
+        assert np.array_equal(k, f)
