@@ -960,9 +960,11 @@ std::mutex g_park_mu;
 Wave* g_parked[kParkDevices] = {};
 }  // namespace
 
-static Wave* take_parked(size_t bytes) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kParkDevices) return nullptr;
+// The kept block of device `dev` when it holds at least `bytes` and `dev` is
+// the current device (the block's memory belongs to it).
+static Wave* take_parked(size_t bytes, int dev) {
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || cur != dev || dev < 0 || dev >= kParkDevices) return nullptr;
     std::lock_guard<std::mutex> lk(g_park_mu);
     Wave* w = g_parked[dev];
     if (!w || w->bytes < bytes) return nullptr;
@@ -987,8 +989,12 @@ void wave_release(DeviceScene& s) {
     Wave* w = s.wave;
     s.wave = nullptr;
     if (!w) return;
-    int dev = 0;
-    if (tuning().pool_keep_mb <= 0 || cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kParkDevices) {
+    // kept under the scene's own device, and only when it is the current one
+    // (the pool calls below act on the current device)
+    const int dev = s.device;
+    int cur = -1;
+    if (tuning().pool_keep_mb <= 0 || cudaGetDevice(&cur) != cudaSuccess || cur != dev || dev < 0 ||
+        dev >= kParkDevices) {
         wave_free(w);
         return;
     }
@@ -1015,7 +1021,7 @@ static bool wave_supported(const DeviceScene& s) {
 // Makes the scene's own scratch hold at least `nsamples` samples for L
 // lights: re-carves the block when it is large enough, else reallocates.
 // A re-carve moves the arrays, so the captured frame graph is dropped.
-static cudaError_t wave_reserve_into(Wave*& w, int L, long long nsamples) {
+static cudaError_t wave_reserve_into(Wave*& w, int L, long long nsamples, int dev) {
     if (w && w->nsamples_cap >= nsamples && w->L == L) return cudaSuccess;
     if (w && wave_scratch_bytes(L, nsamples) <= w->bytes) {
         if (w->exec) { cudaGraphExecDestroy(w->exec); w->exec = nullptr; }
@@ -1024,7 +1030,7 @@ static cudaError_t wave_reserve_into(Wave*& w, int L, long long nsamples) {
     }
     const size_t bytes = wave_scratch_bytes(L, nsamples);
     if (!w) {
-        if (Wave* p = take_parked(bytes)) {
+        if (Wave* p = take_parked(bytes, dev)) {
             w = p;
             wave_carve(*w, w->block, w->bytes, L, nsamples);
             return cudaSuccess;
@@ -1104,7 +1110,7 @@ cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, fl
     const int ns = clamp_spp(aa);
     const long long nsamples = region_padded(rg) * ns;
     if (nsamples > (1ll << 30)) return cudaErrorInvalidValue;
-    cudaError_t e = wave_reserve_into(s.wave, s.view.num_lights, nsamples);
+    cudaError_t e = wave_reserve_into(s.wave, s.view.num_lights, nsamples, s.device);
     if (e != cudaSuccess) return e;
     Wave* w = s.wave;
     const dev::WaveView V = make_view(s, *w, W, H, ns, rg);
@@ -1253,7 +1259,7 @@ cudaError_t profile_wavefront(DeviceScene& s, int W, int H, int aa, float4* out,
     const Region rg{0, 0, W, H};
     const long long nsamples = region_padded(rg) * ns;
     if (nsamples > (1ll << 30)) return cudaErrorInvalidValue;
-    cudaError_t e = wave_reserve_into(s.wave, s.view.num_lights, nsamples);
+    cudaError_t e = wave_reserve_into(s.wave, s.view.num_lights, nsamples, s.device);
     if (e != cudaSuccess) return e;
     const dev::WaveView V = make_view(s, *s.wave, W, H, ns, rg);
     const int npad = (int)region_padded(rg);
