@@ -226,10 +226,92 @@ void push_box(std::vector<float>& lo, std::vector<float>& hi, const T a[3], cons
 
 }  // namespace
 
+namespace {
+
+// Index checks of a scene before upload.  The device code trusts every index
+// it reads (as the reference's does: render_kernel.cu:67 reads
+// materials[rec.material_id], integrator/csg.h reads objects / SEs by leaf
+// index), so a scene whose indices leave their arrays is refused here
+// instead of faulting on the GPU.  Returns null or the first problem.
+const char* scene_index_error(const SheenScene* in) {
+    struct Arr { const void* p; int n; const char* what; };
+    const Arr arrays[] = {
+        {in->objects, in->num_objects, "objects"}, {in->sweep_points, in->num_sweep_points, "sweep points"},
+        {in->sweep_strands, in->num_sweep_strands, "sweep strands"}, {in->triangles, in->num_triangles, "triangles"},
+        {in->heightfields, in->num_heightfields, "heightfields"},
+        {in->superellipsoids, in->num_superellipsoids, "superellipsoids"},
+        {in->lathe_points, in->num_lathe_points, "lathe points"}, {in->lathes, in->num_lathes, "lathes"},
+        {in->prism_points, in->num_prism_points, "prism points"}, {in->prisms, in->num_prisms, "prisms"},
+        {in->planes, in->num_planes, "planes"}, {in->lights, in->num_lights, "lights"},
+        {in->media, in->num_media, "media"}};
+    for (const Arr& a : arrays) {
+        if (a.n < 0) return "negative element count";
+        if (a.n > 0 && !a.p) return "null array with a nonzero count";
+    }
+    const int nm = in->num_materials;
+    auto mat_ok = [nm](int m) { return m >= 0 && m < nm; };
+    auto range_ok = [](int off, int cnt, int n) { return off >= 0 && cnt >= 0 && (long long)off + cnt <= n; };
+    for (int i = 0; i < in->num_objects; i++)
+        if (!mat_ok(in->objects[i].material_id)) return "object material_id out of range";
+    for (int i = 0; i < in->num_sweep_strands; i++) {
+        const SweepStrand& st = in->sweep_strands[i];
+        if (!mat_ok(st.material_id)) return "strand material_id out of range";
+        if (!range_ok(st.point_offset, st.point_count, in->num_sweep_points)) return "strand points out of range";
+    }
+    for (int i = 0; i < in->num_heightfields; i++)
+        if (!mat_ok(in->heightfields[i].material_id)) return "heightfield material_id out of range";
+    for (int i = 0; i < in->num_superellipsoids; i++)
+        if (!mat_ok(in->superellipsoids[i].material_id)) return "superellipsoid material_id out of range";
+    for (int i = 0; i < in->num_lathes; i++) {
+        if (!mat_ok(in->lathes[i].material_id)) return "lathe material_id out of range";
+        if (!range_ok(in->lathes[i].point_offset, in->lathes[i].point_count, in->num_lathe_points))
+            return "lathe points out of range";
+    }
+    for (int i = 0; i < in->num_prisms; i++) {
+        if (!mat_ok(in->prisms[i].material_id)) return "prism material_id out of range";
+        if (!range_ok(in->prisms[i].point_offset, in->prisms[i].point_count, in->num_prism_points))
+            return "prism points out of range";
+    }
+    for (int i = 0; i < in->num_planes; i++)
+        if (!mat_ok(in->planes[i].material_id)) return "plane material_id out of range";
+    if (in->csg_nodes && in->num_csg_nodes > 0 && in->csg_root >= 0 && in->csg_root < in->num_csg_nodes) {
+        for (int i = 0; i < in->num_csg_nodes; i++) {
+            const CSGNode& c = in->csg_nodes[i];
+            if (c.leaf_kind == 0) {
+                if (!in->objects || c.leaf_index < 0 || c.leaf_index >= in->num_objects)
+                    return "CSG sphere leaf index out of range";
+                if (!mat_ok(in->objects[c.leaf_index].material_id)) return "CSG leaf material_id out of range";
+            } else if (c.leaf_kind == 1) {
+                if (!in->superellipsoids || c.leaf_index < 0 || c.leaf_index >= in->num_superellipsoids)
+                    return "CSG superellipsoid leaf index out of range";
+            } else if (c.leaf_kind < 0) {
+                if (c.left < -1 || c.left >= in->num_csg_nodes || c.right < -1 || c.right >= in->num_csg_nodes)
+                    return "CSG child index out of range";
+            } else {
+                return "unknown CSG leaf kind";
+            }
+        }
+    }
+    return nullptr;
+}
+
+// Triangles' material ids, checked on the device after upload (reading
+// 2 M ids on the host would touch the whole 112-byte records).
+__global__ void k_check_tri_materials(const Triangle* __restrict__ t, int n, int nm, int* __restrict__ bad) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int m = t[i].material_id;
+        if (m < 0 || m >= nm) { atomicExch(bad, 1); return; }
+    }
+}
+
+}  // namespace
+
 int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     *out = nullptr;
     if (!in) { set_error("null scene"); return -1; }
     if (form != SHEEN_FORM_PLAIN && form != SHEEN_FORM_WAVEFRONT) { set_error("unknown renderer form"); return -1; }
+    if (in->num_materials <= 0 || !in->materials) { set_error("no materials"); return -1; }
+    if (const char* why = scene_index_error(in)) { set_error(why); return -1; }
     DeviceScene* s = new DeviceScene();
     s->form = form;
     cudaGetDevice(&s->device);
@@ -445,6 +527,7 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
             o_img[i] = ar.add(hfs[i].image, (size_t)hfs[i].img_w * hfs[i].img_h);
     const size_t o_tex = texrefs.empty() ? (size_t)-1 : ar.add(nullptr, texrefs.size() * sizeof(TextureRef));
     const size_t o_tally = ar.add(nullptr, 8 * sizeof(unsigned long long));
+    const size_t o_tricheck = ar.add(nullptr, sizeof(int));   // zero-filled; set by k_check_tri_materials
     ar.size = (ar.size + 255) & ~(size_t)255;
 
     cudaError_t e = dmalloc(&s->arena, ar.size);
@@ -465,6 +548,20 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     std::vector<Copy> copies;
     for (const auto& it : ar.items) copies.push_back({base + it.off, it.src, it.bytes});
     e = upload_items(copies);
+    if (e == cudaSuccess && in->num_triangles > 0) {
+        int* bad = reinterpret_cast<int*>(static_cast<char*>(s->arena) + o_tricheck);
+        k_check_tri_materials<<<(int)std::min<long long>((in->num_triangles + 255) / 256, 148 * 8), 256>>>(
+            reinterpret_cast<const Triangle*>(static_cast<char*>(s->arena) + o_tri), in->num_triangles,
+            in->num_materials, bad);
+        int bad_h = 0;
+        e = cudaMemcpy(&bad_h, bad, sizeof(int), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && bad_h) {
+            dfree(s->arena);
+            set_error("triangle material_id out of range");
+            delete s;
+            return -1;
+        }
+    }
     if (e != cudaSuccess) { dfree(s->arena); set_error(cudaGetErrorString(e)); delete s; return -1; }
     const double t2 = now_ms();
 

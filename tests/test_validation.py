@@ -1,0 +1,95 @@
+"""Scenes whose indices leave their arrays are refused at scene creation
+(the device code trusts every index it reads, as the reference's does), so
+a bad scene is an error message instead of a GPU fault.  The host checks
+run before any device call; triangle material ids are checked on the
+device after upload."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import sheen_b200 as sb
+from sheen_b200 import contract as C
+
+
+def _create_error(view):
+    L = sb.lib()
+    L.sheen_scene_create.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    L.sheen_scene_create.restype = ctypes.c_int
+    h = ctypes.c_void_p()
+    rc = L.sheen_scene_create(ctypes.addressof(view), sb.FORM_WAVEFRONT, ctypes.byref(h))
+    return rc, sb.last_error()
+
+
+@pytest.fixture(scope="module")
+def analytic():
+    return sb.generate_scene(2, 1, 0, 0)
+
+
+def _copy(scene):
+    return C.SheenScene.from_buffer_copy(scene.view)
+
+
+def test_csg_leaf_without_its_superellipsoids(analytic):
+    v = _copy(analytic)
+    assert v.csg_root >= 0
+    v.num_superellipsoids = 0
+    v.superellipsoids = None
+    rc, err = _create_error(v)
+    assert rc == -1 and "CSG superellipsoid leaf index out of range" in err
+
+
+def test_csg_child_index_out_of_range(analytic):
+    v = _copy(analytic)
+    # a copy of the node array with the root's left child past the end
+    raw = np.ctypeslib.as_array((ctypes.c_int32 * (8 * v.num_csg_nodes)).from_address(v.csg_nodes)).copy()
+    raw = raw.reshape(v.num_csg_nodes, 8)
+    root = v.csg_root
+    assert raw[root, 1] < 0                       # interior node
+    raw[root, 3] = v.num_csg_nodes + 5
+    buf = np.ascontiguousarray(raw)
+    v.csg_nodes = buf.ctypes.data
+    rc, err = _create_error(v)
+    assert rc == -1 and "CSG child index out of range" in err
+
+
+def test_lathe_points_out_of_range(analytic):
+    v = _copy(analytic)
+    assert v.num_lathes > 0
+    v.num_lathe_points = 1
+    rc, err = _create_error(v)
+    assert rc == -1 and "lathe points out of range" in err
+
+
+def test_material_id_out_of_range(analytic):
+    v = _copy(analytic)
+    v.num_materials = 1          # other primitives use higher ids
+    rc, err = _create_error(v)
+    assert rc == -1 and "material_id out of range" in err
+
+
+def test_null_array_with_count(analytic):
+    v = _copy(analytic)
+    v.prisms = None
+    rc, err = _create_error(v)
+    assert rc == -1 and "null array with a nonzero count" in err
+
+
+@pytest.mark.gpu
+def test_triangle_material_out_of_range_refused_on_device():
+    sb.init(0, 100)
+    s = C.SceneArrays()
+    t = np.zeros(3, C.TRIANGLE)
+    t["v0"] = [[0, 0, 0]] * 3
+    t["v1"] = [[1, 0, 0]] * 3
+    t["v2"] = [[0, 1, 0]] * 3
+    t["material_id"] = [0, 0, 7]
+    s.materials = np.zeros(1, C.MATERIAL)
+    s.materials[0] = C.default_material()[0]
+    s.triangles = t
+    with pytest.raises(RuntimeError, match="triangle material_id out of range"):
+        sb.DeviceScene(s, sb.FORM_WAVEFRONT)
+    t["material_id"] = 0
+    s.triangles = t
+    ds = sb.DeviceScene(s, sb.FORM_WAVEFRONT)     # the same scene with valid ids
+    ds.close()
