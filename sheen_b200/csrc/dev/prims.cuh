@@ -255,6 +255,85 @@ __device__ __forceinline__ bool lathe_test(const Ray& r, const Lathe& l, const L
     return any;
 }
 
+// cone_test's constants of every lathe segment (p0 = (0, y_i, 0), p1 =
+// (0, y_{i+1}, 0)), with cone_test's expressions: seg[2p] = {y0, r0, k, L},
+// seg[2p + 1] = {da.y, 0, 0, valid}; valid 0 for a segment lathe_test
+// skips (both radii <= 0, or L^2 < 1e-12).  The axis has no x / z part, so
+// da = (0, da.y, 0) exactly.
+static __global__ void lathe_segments_kernel(const Lathe* __restrict__ lathes, int nl, const LathePoint* __restrict__ pts,
+                                      float4* __restrict__ seg) {
+    const int l = blockIdx.x;
+    if (l >= nl) return;
+    const Lathe L0 = lathes[l];
+    for (int i = threadIdx.x; i < L0.point_count - 1; i += blockDim.x) {
+        const int p = L0.point_offset + i;
+        const LathePoint a = pts[p], b = pts[p + 1];
+        float4 s0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), s1 = s0;
+        if (!(a.radius <= 0.0f && b.radius <= 0.0f)) {
+            const float3 p0 = f3(0.0f, a.y, 0.0f), p1 = f3(0.0f, b.y, 0.0f);
+            const float3 axis = p1 - p0;
+            const float L2 = dot(axis, axis);
+            if (!(L2 < 1e-12f)) {
+                const float L = sqrtf(L2);
+                const float3 da = axis / L;
+                const float k = (b.radius - a.radius) / L;
+                s0 = make_float4(a.y, a.radius, k, L);
+                s1 = make_float4(da.y, 0.0f, 0.0f, 1.0f);
+            }
+        }
+        seg[2 * (size_t)p] = s0;
+        seg[2 * (size_t)p + 1] = s1;
+    }
+}
+
+// lathe_test with the segment constants precomputed (lathe_segments_kernel):
+// cone_test's steps after its axis, L, da and k, so the same hits and
+// records, without a square root and four divisions per segment.
+__device__ __forceinline__ bool lathe_test_pre(const Ray& r, const Lathe& l, const float4* __restrict__ seg, Hit& h) {
+    if (l.point_count < 2) return false;
+    bool any = false;
+    float best = r.tmax;
+    for (int i = 0; i < l.point_count - 1; i++) {
+        const int p = l.point_offset + i;
+        const float4 s1 = __ldg(&seg[2 * (size_t)p + 1]);
+        if (s1.w == 0.0f) continue;
+        const float4 s0 = __ldg(&seg[2 * (size_t)p]);
+        const float3 p0 = f3(0.0f, s0.x, 0.0f);
+        const float r0 = s0.y, k = s0.z, L = s0.w;
+        const float3 da = f3(0.0f, s1.x, 0.0f);
+        const float3 Q = r.o - p0;
+        const float u = dot(r.d, da), v = dot(Q, da);
+        const float3 Dp = r.d - u * da, Qp = Q - v * da;
+        const float A = dot(Dp, Dp) - k * k * u * u;
+        const float B = 2.0f * (dot(Dp, Qp) - k * r0 * u - k * k * v * u);
+        const float C = dot(Qp, Qp) - k * k * v * v - 2.0f * k * r0 * v - r0 * r0;
+        const float disc = B * B - 4.0f * A * C;
+        if (disc < 0.0f) continue;
+        const float sq = sqrtf(disc);
+        const float i2a = 1.0f / (2.0f * A);
+        const float s1r = (-B - sq) * i2a, s2r = (-B + sq) * i2a;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const float s = j == 0 ? s1r : s2r;
+            if (s < r.tmin || s > r.tmax) continue;
+            const float tp = v + s * u;
+            if (tp < 0.0f || tp > L) continue;
+            if (s < best) {
+                h.t = s;
+                h.n = normalize(Qp + s * Dp);
+                h.tan = da;
+                if (dot(h.n, r.d) > 0.0f) h.n = -h.n;
+                h.p = r.o + s * r.d;
+                best = s;
+                any = true;
+            }
+            break;   // cone_test reports its first root in range
+        }
+    }
+    if (any) { h.mat = l.material_id; h.uv = make_float2(0.0f, 0.0f); }
+    return any;
+}
+
 // primitives/prism.h:18-63: even-odd containment of (x, z) over the closed
 // sub-contours (a contour ends where its first point repeats).
 __device__ __forceinline__ bool prism_contains(float x, float z, const Prism& p, const PrismPoint* all) {

@@ -67,6 +67,11 @@ struct DevScene {
     const HeightField* hfs; int num_hfs; const BvhNode* hf_bvh;
     const Superellipsoid* ses; int num_ses; const BvhNode* se_bvh;
     const Lathe* lathes; const LathePoint* lathe_points; int num_lathes; const BvhNode* lathe_bvh;
+    // Per lathe point p (the segment from p to p + 1): cone_test's profile
+    // constants, {y0, r0, k, L} and {axis y, 0, 0, 1 when the segment is
+    // tested}, computed on the device by lathe_segments_kernel with
+    // cone_test's own expressions.
+    const float4* lathe_seg;
     const Prism* prisms; const PrismPoint* prism_points; int num_prisms; const BvhNode* prism_bvh;
     const CSGNode* csg_nodes; int csg_root;
     const Plane* planes; int num_planes;

@@ -14,6 +14,7 @@
 #include <thread>
 #include <vector>
 
+#include "dev/prims.cuh"
 #include "engine.h"
 
 namespace sheen {
@@ -528,6 +529,9 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     const size_t o_tex = texrefs.empty() ? (size_t)-1 : ar.add(nullptr, texrefs.size() * sizeof(TextureRef));
     const size_t o_tally = ar.add(nullptr, 8 * sizeof(unsigned long long));
     const size_t o_tricheck = ar.add(nullptr, sizeof(int));   // zero-filled; set by k_check_tri_materials
+    const size_t o_lseg = (in->num_lathes > 0 && in->num_lathe_points > 0)
+                              ? ar.add(nullptr, 2 * (size_t)in->num_lathe_points * sizeof(float4))
+                              : (size_t)-1;   // zero-filled; set by lathe_segments_kernel
     ar.size = (ar.size + 255) & ~(size_t)255;
 
     cudaError_t e = dmalloc(&s->arena, ar.size);
@@ -562,6 +566,12 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
             return -1;
         }
     }
+    if (e == cudaSuccess && o_lseg != (size_t)-1) {
+        dev::lathe_segments_kernel<<<in->num_lathes, 64>>>((const Lathe*)(base + o_lat), in->num_lathes,
+                                                          (const LathePoint*)(base + o_lpt),
+                                                          (float4*)(base + o_lseg));
+        e = cudaGetLastError();
+    }
     if (e != cudaSuccess) { dfree(s->arena); set_error(cudaGetErrorString(e)); delete s; return -1; }
     const double t2 = now_ms();
 
@@ -577,6 +587,7 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     v.hfs = (const HeightField*)dptr(o_hf); v.num_hfs = in->num_heightfields; v.hf_bvh = (const dev::BvhNode*)dptr(o_hfb);
     v.ses = (const Superellipsoid*)dptr(o_se); v.num_ses = in->num_superellipsoids; v.se_bvh = (const dev::BvhNode*)dptr(o_seb);
     v.lathes = (const Lathe*)dptr(o_lat); v.lathe_points = (const LathePoint*)dptr(o_lpt); v.num_lathes = in->num_lathes;
+    v.lathe_seg = (const float4*)dptr(o_lseg);
     v.lathe_bvh = (const dev::BvhNode*)dptr(o_latb);
     v.prisms = (const Prism*)dptr(o_pri); v.prism_points = (const PrismPoint*)dptr(o_ppt); v.num_prisms = in->num_prisms;
     v.prism_bvh = (const dev::BvhNode*)dptr(o_prib);
