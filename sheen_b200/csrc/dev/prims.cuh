@@ -4,6 +4,8 @@
 // They are shared by every renderer form: the forms differ in how they find
 // candidate primitives, never in how a primitive answers.
 #pragma once
+#include <cfloat>
+
 #include "scene.cuh"
 #include "vec.cuh"
 
@@ -261,10 +263,25 @@ __device__ __forceinline__ bool lathe_test(const Ray& r, const Lathe& l, const L
 // skips (both radii <= 0, or L^2 < 1e-12).  The axis has no x / z part, so
 // da = (0, da.y, 0) exactly.
 static __global__ void lathe_segments_kernel(const Lathe* __restrict__ lathes, int nl, const LathePoint* __restrict__ pts,
-                                      float4* __restrict__ seg) {
+                                      float4* __restrict__ seg, float4* __restrict__ bound) {
     const int l = blockIdx.x;
     if (l >= nl) return;
     const Lathe L0 = lathes[l];
+    if (threadIdx.x == 0) {
+        // the surface's box about the Y axis (cone_test's hits lie on cones
+        // between consecutive profile points), widened by 1e-4 relative:
+        // far more than the rounding of a hit cone_test accepts
+        float R = 0.0f, ylo = FLT_MAX, yhi = -FLT_MAX;
+        for (int i = 0; i < L0.point_count; i++) {
+            const LathePoint q = pts[L0.point_offset + i];
+            R = fmaxf(R, fabsf(q.radius));
+            ylo = fminf(ylo, q.y);
+            yhi = fmaxf(yhi, q.y);
+        }
+        const float m = 1e-4f * (R + fabsf(ylo) + fabsf(yhi)) + 1e-6f;
+        bound[l] = L0.point_count >= 2 ? make_float4(R + m, ylo - m, yhi + m, 1.0f)
+                                        : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
     for (int i = threadIdx.x; i < L0.point_count - 1; i += blockDim.x) {
         const int p = L0.point_offset + i;
         const LathePoint a = pts[p], b = pts[p + 1];
@@ -289,8 +306,24 @@ static __global__ void lathe_segments_kernel(const Lathe* __restrict__ lathes, i
 // lathe_test with the segment constants precomputed (lathe_segments_kernel):
 // cone_test's steps after its axis, L, da and k, so the same hits and
 // records, without a square root and four divisions per segment.
-__device__ __forceinline__ bool lathe_test_pre(const Ray& r, const Lathe& l, const float4* __restrict__ seg, Hit& h) {
-    if (l.point_count < 2) return false;
+__device__ __forceinline__ bool lathe_test_pre(const Ray& r, const Lathe& l, const float4* __restrict__ seg,
+                                               float4 bound, Hit& h) {
+    if (l.point_count < 2 || bound.w == 0.0f) return false;
+    {
+        // slab test against the surface's box (a NaN from 0 * inf leaves
+        // that slab unconstrained)
+        const float lo[3] = {-bound.x, bound.y, -bound.x}, hi[3] = {bound.x, bound.z, bound.x};
+        const float o[3] = {r.o.x, r.o.y, r.o.z}, d[3] = {r.d.x, r.d.y, r.d.z};
+        float tn = r.tmin, tf = r.tmax;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const float inv = 1.0f / d[a];
+            const float t0 = (lo[a] - o[a]) * inv, t1 = (hi[a] - o[a]) * inv;
+            tn = fmaxf(tn, fminf(t0, t1));
+            tf = fminf(tf, fmaxf(t0, t1));
+        }
+        if (tn > tf * (1.0f + 1e-6f) + 1e-6f) return false;
+    }
     bool any = false;
     float best = r.tmax;
     for (int i = 0; i < l.point_count - 1; i++) {

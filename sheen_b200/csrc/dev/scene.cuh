@@ -72,6 +72,10 @@ struct DevScene {
     // tested}, computed on the device by lathe_segments_kernel with
     // cone_test's own expressions.
     const float4* lathe_seg;
+    // Per lathe: {R, y_lo, y_hi, valid}, a box about the world Y axis that
+    // holds the lathe's surface (|x|, |z| <= R, y in [y_lo, y_hi]) with a
+    // margin of 1e-4 relative; a ray that misses it cannot hit the lathe.
+    const float4* lathe_bound;
     const Prism* prisms; const PrismPoint* prism_points; int num_prisms; const BvhNode* prism_bvh;
     const CSGNode* csg_nodes; int csg_root;
     const Plane* planes; int num_planes;

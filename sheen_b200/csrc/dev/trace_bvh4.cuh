@@ -470,7 +470,7 @@ __device__ __forceinline__ bool lathes_cull(const DevScene& S, const Ray& r, Hit
     float best = r.tmax;
     dfs_cull<COUNT>(S.lathe_bvh, r, best, c, [&](int i) {
         Hit tmp;
-        if (lathe_test_pre(r, S.lathes[i], S.lathe_seg, tmp) && tmp.t < best) {
+        if (lathe_test_pre(r, S.lathes[i], S.lathe_seg, __ldg(&S.lathe_bound[i]), tmp) && tmp.t < best) {
             h = tmp; h.obj = -(i + 1); best = tmp.t; any = true;
         }
     });

@@ -532,6 +532,8 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     const size_t o_lseg = (in->num_lathes > 0 && in->num_lathe_points > 0)
                               ? ar.add(nullptr, 2 * (size_t)in->num_lathe_points * sizeof(float4))
                               : (size_t)-1;   // zero-filled; set by lathe_segments_kernel
+    const size_t o_lbnd = (o_lseg != (size_t)-1) ? ar.add(nullptr, (size_t)in->num_lathes * sizeof(float4))
+                                                 : (size_t)-1;
     ar.size = (ar.size + 255) & ~(size_t)255;
 
     cudaError_t e = dmalloc(&s->arena, ar.size);
@@ -569,7 +571,7 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     if (e == cudaSuccess && o_lseg != (size_t)-1) {
         dev::lathe_segments_kernel<<<in->num_lathes, 64>>>((const Lathe*)(base + o_lat), in->num_lathes,
                                                           (const LathePoint*)(base + o_lpt),
-                                                          (float4*)(base + o_lseg));
+                                                          (float4*)(base + o_lseg), (float4*)(base + o_lbnd));
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) { dfree(s->arena); set_error(cudaGetErrorString(e)); delete s; return -1; }
@@ -588,6 +590,7 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     v.ses = (const Superellipsoid*)dptr(o_se); v.num_ses = in->num_superellipsoids; v.se_bvh = (const dev::BvhNode*)dptr(o_seb);
     v.lathes = (const Lathe*)dptr(o_lat); v.lathe_points = (const LathePoint*)dptr(o_lpt); v.num_lathes = in->num_lathes;
     v.lathe_seg = (const float4*)dptr(o_lseg);
+    v.lathe_bound = (const float4*)dptr(o_lbnd);
     v.lathe_bvh = (const dev::BvhNode*)dptr(o_latb);
     v.prisms = (const Prism*)dptr(o_pri); v.prism_points = (const PrismPoint*)dptr(o_ppt); v.num_prisms = in->num_prisms;
     v.prism_bvh = (const dev::BvhNode*)dptr(o_prib);

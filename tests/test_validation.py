@@ -98,9 +98,10 @@ def test_triangle_material_out_of_range_refused_on_device():
 @pytest.mark.gpu
 def test_lathe_segment_table_hits_equal_plain_form(analytic):
     """The wavefront form tests lathes with the segment constants computed
-    once per scene (lathe_segments_kernel) instead of per ray; on a scene
-    of lathes (and the ground plane) its primary hits equal the plain
-    form's, which runs cone_test itself, bit for bit."""
+    once per scene (lathe_segments_kernel) instead of per ray, after a box
+    test against the surface's own bound about the Y axis; on a scene of
+    lathes (and the ground plane) its primary hits equal the plain form's,
+    which runs cone_test on every segment, bit for bit."""
     sb.init(0, 100)
     v = _copy(analytic)
     for k in ("num_objects", "num_sweep_strands", "num_triangles", "num_heightfields", "num_superellipsoids",
@@ -110,7 +111,7 @@ def test_lathe_segment_table_hits_equal_plain_form(analytic):
     hits = []
     for form in (sb.FORM_PLAIN, sb.FORM_WAVEFRONT):
         ds = sb.DeviceScene(v, form)
-        hits.append(ds.primary_hits(256, 144, 1))
+        hits.append(ds.primary_hits(640, 360, 1))
         ds.close()
     (o0, m0, t0), (o1, m1, t1) = hits
     assert (o0 < 0).sum() > 1000                    # lathe hits present
