@@ -460,6 +460,38 @@ __device__ __forceinline__ float3 se_gradient(const Superellipsoid& s, float3 p)
               s.n * powf(fabsf(qz), s.n - 1.0f) * (qz >= 0.0f ? 1.0f : -1.0f) / s.c);
 }
 
+// Whether F(p) = |qx|^n + |qy|^n + |qz|^n exceeds 1 -- the only use se_span
+// makes of F -- deciding from two bounds before any powf where they can:
+//   F <= 3 max|q_i|^n, so max|q_i| < (1/3)^(1/n) means inside;
+//   F >= 3 (sum|q_i| / 3)^n for n >= 1 (power means) and F >= sum|q_i| for
+//   n < 1 (|x|^n >= |x| on [0, 1]; a |q_i| > 1 is outside anyway), so
+//   sum|q_i| above 3^(1 - 1/n), or 1, means outside.
+// The thresholds carry a 1e-4 relative margin, far above the few-ulp error
+// of powf and the sum, so every decision equals se_value(s, p) > 1; any
+// other point (or a NaN) is evaluated exactly with se_value's arithmetic.
+struct SeSign {
+    float thr_in, thr_out;   // on max|q_i| and on sum|q_i|; -1 / +inf: no shortcut
+    __device__ __forceinline__ explicit SeSign(float n) {
+        if (n >= 0.25f && n <= 1e4f) {
+            thr_in = powf(1.0f / 3.0f, 1.0f / n) * (1.0f - 1e-4f);
+            thr_out = (n >= 1.0f ? powf(3.0f, 1.0f - 1.0f / n) : 1.0f) * (1.0f + 1e-4f);
+        } else {
+            thr_in = -1.0f;
+            thr_out = __int_as_float(0x7f800000);
+        }
+    }
+    __device__ __forceinline__ bool outside(const Superellipsoid& s, float3 p) const {
+        const float qx = (p.x - s.center.x) / s.a, qy = (p.y - s.center.y) / s.b, qz = (p.z - s.center.z) / s.c;
+        const float ax = fabsf(qx), ay = fabsf(qy), az = fabsf(qz);
+        const float sum = ax + ay + az;
+        if (sum == sum) {
+            if (fmaxf(fmaxf(ax, ay), az) < thr_in) return false;
+            if (sum > thr_out) return true;
+        }
+        return powf(ax, s.n) + powf(ay, s.n) + powf(az, s.n) > 1.0f;
+    }
+};
+
 __device__ __forceinline__ void se_chord(const Ray& r, const Superellipsoid& s, float& tA, float& tB) {
     const float3 lo = f3(s.center.x - s.a, s.center.y - s.b, s.center.z - s.c);
     const float3 hi = f3(s.center.x + s.a, s.center.y + s.b, s.center.z + s.c);
@@ -480,6 +512,8 @@ __device__ __forceinline__ void se_chord(const Ray& r, const Superellipsoid& s, 
 // chord, 20 bisection steps for the exit.  As in the reference an entry
 // found by sampling is not refined (its bisection interval is empty), so
 // the entry lies on a sample.
+// SIGN: decide the samples through SeSign (the same decisions, fewer powf).
+template <bool SIGN = false>
 __device__ __forceinline__ bool se_span(const Ray& r, const Superellipsoid& s, float t0, float t1,
                                         float& te, float& tx, float* te_prev = nullptr) {
     float tA, tB;
@@ -487,27 +521,29 @@ __device__ __forceinline__ bool se_span(const Ray& r, const Superellipsoid& s, f
     if (tB < t0 || tA > t1 || tB < tA) return false;
     t0 = fmaxf(t0, tA);
     t1 = fminf(t1, tB);
+    const SeSign sg(SIGN ? s.n : 0.0f);
+    auto out = [&](float3 p) { return SIGN ? sg.outside(s, p) : se_value(s, p) > 1.0f; };
     const float step = (t1 - t0) / 32.0f;
     float tp = t0;
-    bool inside = se_value(s, r.o + tp * r.d) <= 1.0f;
+    bool inside = !out(r.o + tp * r.d);
     bool found_in = inside, found_out = false;
     te = inside ? t0 : -1e30f;
     if (te_prev) *te_prev = te;   // the last sample outside before the entry (te itself: no bracket)
     tx = -1e30f;
     for (int i = 1; i <= 32 && !found_out; i++) {
         float t = fminf(t0 + step * (float)i, t1);
-        float F = se_value(s, r.o + t * r.d);
-        if (inside && F > 1.0f) {
+        const bool o = out(r.o + t * r.d);
+        if (inside && o) {
             float lo = tp, hi = t;
             for (int b = 0; b < 20; b++) {
                 float mid = 0.5f * (lo + hi);
-                if (se_value(s, r.o + mid * r.d) > 1.0f) hi = mid; else lo = mid;
+                if (out(r.o + mid * r.d)) hi = mid; else lo = mid;
             }
             tx = fminf(0.5f * (lo + hi), t1);
             found_out = true;
             break;
         }
-        if (!inside && F <= 1.0f) {
+        if (!inside && !o) {
             te = fmaxf(t, t0);   // bisection over [t, t] in the reference
             if (te_prev) *te_prev = tp;
             found_in = true;
@@ -552,6 +588,7 @@ static __device__ __noinline__ float se_polish_entry(const Ray& r, const Superel
 }
 
 // primitives/superellipsoid.h:123-161
+template <bool SIGN = false>
 __device__ __forceinline__ bool se_test(const Ray& r, const Superellipsoid& s, Hit& h, int polish = 0) {
     float t0, t1;
     se_chord(r, s, t0, t1);
@@ -559,7 +596,7 @@ __device__ __forceinline__ bool se_test(const Ray& r, const Superellipsoid& s, H
     t0 = fmaxf(t0, r.tmin);
     t1 = fminf(t1, r.tmax);
     float te, tx, te_prev;
-    if (!se_span(r, s, t0, t1, te, tx, &te_prev)) return false;
+    if (!se_span<SIGN>(r, s, t0, t1, te, tx, &te_prev)) return false;
     if (polish && te_prev < te) te = se_polish_entry(r, s, te_prev, te);
     h.t = te;
     h.p = r.o + te * r.d;

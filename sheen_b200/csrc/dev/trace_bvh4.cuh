@@ -456,7 +456,7 @@ __device__ __forceinline__ bool ses_cull(const DevScene& S, const Ray& r, Hit& h
     float best = r.tmax;
     dfs_cull<COUNT>(S.se_bvh, r, best, c, [&](int i) {
         Hit tmp;
-        if (se_test(r, S.ses[i], tmp, S.se_polish) && tmp.t < best) {
+        if (se_test<true>(r, S.ses[i], tmp, S.se_polish) && tmp.t < best) {
             h = tmp; h.obj = -(i + 1); best = tmp.t; any = true;
         }
     });

@@ -117,3 +117,26 @@ def test_lathe_segment_table_hits_equal_plain_form(analytic):
     assert (o0 < 0).sum() > 1000                    # lathe hits present
     assert np.array_equal(o0, o1) and np.array_equal(m0, m1)
     assert np.array_equal(t0, t1)
+
+
+@pytest.mark.gpu
+def test_superellipsoid_sign_shortcuts_hits_equal_plain_form(analytic):
+    """The wavefront form decides most superellipsoid samples from two
+    bounds on max|q| and sum|q| (SeSign) instead of three powf; the
+    decisions equal F > 1's, so on a scene of superellipsoids (and the
+    ground plane) its primary hits equal the plain form's bit for bit."""
+    sb.init(0, 100)
+    v = _copy(analytic)
+    for k in ("num_objects", "num_sweep_strands", "num_triangles", "num_heightfields", "num_lathes",
+              "num_prisms"):
+        setattr(v, k, 0)
+    v.csg_root = -1
+    hits = []
+    for form in (sb.FORM_PLAIN, sb.FORM_WAVEFRONT):
+        ds = sb.DeviceScene(v, form)
+        hits.append(ds.primary_hits(640, 360, 1))
+        ds.close()
+    (o0, m0, t0), (o1, m1, t1) = hits
+    assert (o0 < 0).sum() > 1000                    # superellipsoid hits present
+    assert np.array_equal(o0, o1) and np.array_equal(m0, m1)
+    assert np.array_equal(t0, t1)
