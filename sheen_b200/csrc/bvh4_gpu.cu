@@ -137,6 +137,18 @@ __device__ __forceinline__ void add_to_bins_warp(int* A, const int b[3], bool ac
     }
 }
 
+// add_to_bin without the centroid words (1 + 6 atomics): for bins whose
+// centroid bounds nobody reads (the warp-built subtrees, which take each
+// node's bounds from warp reductions; axis_best_bins reads count and box).
+__device__ __forceinline__ void add_to_bin_box(int* B, const float l[3], const float h[3]) {
+    atomicAdd(B, 1);
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        atomicMin(B + 1 + q, ford(l[q]));
+        atomicMax(B + 4 + q, ford(h[q]));
+    }
+}
+
 // Union of bins [b0, b1] of one axis into box/centroid box; returns the count.
 __device__ __forceinline__ int bin_union(const int* A, int b0, int b1, float lo[3], float hi[3], float clo[3],
                                          float chi[3]) {
@@ -628,7 +640,7 @@ __device__ void build_tiny(TinyFrame root, float node_cost, unsigned short* __re
                 if (!(ext > 0.0f)) continue;
                 for (int w = lane; w < kAxisWords; w += 32) bins[w] = bin_init(w);
                 __syncwarp();
-                if (act) add_to_bin(bins + bin_of(c[a], clo[a], bin_scale(ext)) * kBinWords, l, h, c);
+                if (act) add_to_bin_box(bins + bin_of(c[a], clo[a], bin_scale(ext)) * kBinWords, l, h);
                 __syncwarp();
                 float cost;
                 int cand;
