@@ -22,13 +22,20 @@ namespace sheen {
 
 namespace {
 
+// One primitive as the builder moves it: its centroid, box and id side by
+// side, so partitions and box unions read contiguous memory instead of
+// gathering through an id array (the gathers dominated the build).
+struct Item {
+    float c[3];
+    float lo[3];
+    float hi[3];
+    int id;
+};
+
 struct Builder {
-    const float* lo;
-    const float* hi;
-    std::vector<float> cen;   // 3 per primitive id
     bool axis_from_centroids;
 
-    void build(std::vector<int>& idx, int start, int end, int depth, std::vector<HostNode>& nodes) {
+    void build(std::vector<Item>& it, int start, int end, int depth, std::vector<HostNode>& nodes) {
         const int node = (int)nodes.size();
         nodes.push_back(HostNode{});
         float bl[3] = {1e30f, 1e30f, 1e30f}, bh[3] = {-1e30f, -1e30f, -1e30f};
@@ -37,19 +44,19 @@ struct Builder {
             for (int k = 0; k < 3; k++) { bl[k] = 1e10f; bh[k] = -1e10f; cl[k] = 1e10f; ch[k] = -1e10f; }
         }
         for (int i = start; i < end; i++) {
-            const int p = idx[(size_t)i];
+            const Item& p = it[(size_t)i];
             for (int k = 0; k < 3; k++) {
-                bl[k] = fminf(bl[k], lo[3 * (size_t)p + k]);
-                bh[k] = fmaxf(bh[k], hi[3 * (size_t)p + k]);
-                cl[k] = fminf(cl[k], cen[3 * (size_t)p + k]);
-                ch[k] = fmaxf(ch[k], cen[3 * (size_t)p + k]);
+                bl[k] = fminf(bl[k], p.lo[k]);
+                bh[k] = fmaxf(bh[k], p.hi[k]);
+                cl[k] = fminf(cl[k], p.c[k]);
+                ch[k] = fmaxf(ch[k], p.c[k]);
             }
         }
         HostNode& n = nodes[(size_t)node];
         for (int k = 0; k < 3; k++) { n.lo[k] = bl[k]; n.hi[k] = bh[k]; }
         const int count = end - start;
         if (count <= 1) {
-            n.left = n.right = ~idx[(size_t)start];
+            n.left = n.right = ~it[(size_t)start].id;
             return;
         }
         float ext[3];
@@ -58,14 +65,15 @@ struct Builder {
         if (ext[1] > ext[0] && ext[1] > ext[2]) axis = 1;
         if (ext[2] > ext[0] && ext[2] > ext[1]) axis = 2;
         const int mid = start + count / 2;
-        const float* c = cen.data();
-        std::nth_element(idx.begin() + start, idx.begin() + mid, idx.begin() + end,
-                         [c, axis](int a, int b) { return c[3 * (size_t)a + axis] < c[3 * (size_t)b + axis]; });
+        // the comparisons, and so the permutation nth_element makes, are the
+        // ones an id array ordered by the same keys would get
+        std::nth_element(it.begin() + start, it.begin() + mid, it.begin() + end,
+                         [axis](const Item& a, const Item& b) { return a.c[axis] < b.c[axis]; });
         if (depth < 4 && count > 65536) {
             std::vector<HostNode> right_nodes;
-            std::thread worker([&] { build(idx, mid, end, depth + 1, right_nodes); });
+            std::thread worker([&] { build(it, mid, end, depth + 1, right_nodes); });
             const int left = (int)nodes.size();
-            build(idx, start, mid, depth + 1, nodes);
+            build(it, start, mid, depth + 1, nodes);
             worker.join();
             const int right = (int)nodes.size();
             for (HostNode rn : right_nodes) {
@@ -76,9 +84,9 @@ struct Builder {
             nodes[(size_t)node].right = right;
         } else {
             const int left = (int)nodes.size();
-            build(idx, start, mid, depth + 1, nodes);
+            build(it, start, mid, depth + 1, nodes);
             const int right = (int)nodes.size();
-            build(idx, mid, end, depth + 1, nodes);
+            build(it, mid, end, depth + 1, nodes);
             nodes[(size_t)node].left = left;
             nodes[(size_t)node].right = right;
         }
@@ -92,14 +100,20 @@ void build_median_bvh(const std::vector<float>& lo, const std::vector<float>& hi
     out.clear();
     if (prims.empty()) return;
     Builder b;
-    b.lo = lo.data();
-    b.hi = hi.data();
     b.axis_from_centroids = axis_from_centroids;
-    b.cen.resize(lo.size());
-    for (size_t i = 0; i < lo.size(); i++) b.cen[i] = (lo[i] + hi[i]) * 0.5f;
-    std::vector<int> idx = prims;
+    std::vector<Item> it(prims.size());
+    for (size_t i = 0; i < prims.size(); i++) {
+        const size_t p = (size_t)prims[i];
+        Item& m = it[i];
+        for (int k = 0; k < 3; k++) {
+            m.lo[k] = lo[3 * p + k];
+            m.hi[k] = hi[3 * p + k];
+            m.c[k] = (lo[3 * p + k] + hi[3 * p + k]) * 0.5f;
+        }
+        m.id = prims[i];
+    }
     out.reserve(2 * prims.size());
-    b.build(idx, 0, (int)idx.size(), 0, out);
+    b.build(it, 0, (int)it.size(), 0, out);
 }
 
 }  // namespace sheen
