@@ -322,7 +322,7 @@ __device__ __forceinline__ bool lathe_test_pre(const Ray& r, const Lathe& l, con
             tn = fmaxf(tn, fminf(t0, t1));
             tf = fminf(tf, fmaxf(t0, t1));
         }
-        if (tn > tf * (1.0f + 1e-6f) + 1e-6f) return false;
+        if (tn > tf + 1e-5f * (fabsf(tn) + fabsf(tf)) + 1e-6f) return false;
     }
     bool any = false;
     float best = r.tmax;
@@ -365,6 +365,23 @@ __device__ __forceinline__ bool lathe_test_pre(const Ray& r, const Lathe& l, con
     }
     if (any) { h.mat = l.material_id; h.uv = make_float2(0.0f, 0.0f); }
     return any;
+}
+
+// Whether the ray's [tmin, tmax] range can meet the box [lo, hi]: a slab
+// test that accepts up to 1e-5 relative in t beyond the box, far more than
+// the rounding of any hit computed inside it (a NaN from 0 * inf leaves
+// that slab unconstrained).
+__device__ __forceinline__ bool ray_meets_box(const Ray& r, const float lo[3], const float hi[3]) {
+    const float o[3] = {r.o.x, r.o.y, r.o.z}, d[3] = {r.d.x, r.d.y, r.d.z};
+    float tn = r.tmin, tf = r.tmax;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float inv = 1.0f / d[a];
+        const float t0 = (lo[a] - o[a]) * inv, t1 = (hi[a] - o[a]) * inv;
+        tn = fmaxf(tn, fminf(t0, t1));
+        tf = fminf(tf, fmaxf(t0, t1));
+    }
+    return !(tn > tf + 1e-5f * (fabsf(tn) + fabsf(tf)) + 1e-6f);
 }
 
 // primitives/prism.h:18-63: even-odd containment of (x, z) over the closed

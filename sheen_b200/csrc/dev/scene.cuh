@@ -78,6 +78,11 @@ struct DevScene {
     const float4* lathe_bound;
     const Prism* prisms; const PrismPoint* prism_points; int num_prisms; const BvhNode* prism_bvh;
     const CSGNode* csg_nodes; int csg_root;
+    // Box holding every CSG leaf solid (sphere: centre +- radius;
+    // superellipsoid: centre +- (a, b, c)), widened by 1e-4 relative: the
+    // tree's solid lies inside the union of its leaves, so a ray that misses
+    // the box has no CSG hit.  Empty (lo > hi) without a tree.
+    float csg_lo[3], csg_hi[3];
     const Plane* planes; int num_planes;
     const Material* materials; int num_materials;
     const TextureRef* textures; int num_textures;

@@ -520,7 +520,7 @@ struct FastTracer {
         if ((F & kCatSE) && ses_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
         if ((F & kCatLathe) && lathes_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
         if ((F & kCatPrism) && prisms_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if ((F & kCatCSG) && S.csg_root >= 0 && csg_test(S, r, t) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatCSG) && S.csg_root >= 0 && ray_meets_box(r, S.csg_lo, S.csg_hi) && csg_test(S, r, t) && t.t < best) { best = t.t; rec = t; hit = true; }
         if ((F & kCatPlanes) && planes_scan(S, r, t) && t.t < best) { best = t.t; rec = t; hit = true; }
         return hit;
     }
@@ -534,7 +534,7 @@ struct FastTracer {
         }
         if (((F & kCatHF) && hfs_cull<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_cull<COUNT>(S, r, h, c)) ||
             ((F & kCatLathe) && lathes_cull<COUNT>(S, r, h, c)) || ((F & kCatPrism) && prisms_cull<COUNT>(S, r, h, c)) ||
-            ((F & kCatCSG) && S.csg_root >= 0 && csg_test(S, r, h)) || ((F & kCatPlanes) && planes_scan(S, r, h)))
+            ((F & kCatCSG) && S.csg_root >= 0 && ray_meets_box(r, S.csg_lo, S.csg_hi) && csg_test(S, r, h)) || ((F & kCatPlanes) && planes_scan(S, r, h)))
             return classify_shadow_hit(S, h, mask_aware, sh);
         return kClear;
     }
@@ -553,7 +553,7 @@ struct FastTracer {
         Hit h;
         if (((F & kCatHF) && hfs_cull<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_cull<COUNT>(S, r, h, c)) ||
             ((F & kCatLathe) && lathes_cull<COUNT>(S, r, h, c)) || ((F & kCatPrism) && prisms_cull<COUNT>(S, r, h, c)) ||
-            ((F & kCatCSG) && S.csg_root >= 0 && csg_test(S, r, h)) || ((F & kCatPlanes) && planes_scan(S, r, h)))
+            ((F & kCatCSG) && S.csg_root >= 0 && ray_meets_box(r, S.csg_lo, S.csg_hi) && csg_test(S, r, h)) || ((F & kCatPlanes) && planes_scan(S, r, h)))
             return classify_shadow_hit(S, h, mask_aware, sh);
         return kClear;
     }
@@ -564,7 +564,7 @@ struct FastTracer {
         return ((F & kCatHF) && hfs_cull<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_cull<COUNT>(S, r, h, c)) ||
                ((F & kCatLathe) && lathes_cull<COUNT>(S, r, h, c)) ||
                ((F & kCatPrism) && prisms_cull<COUNT>(S, r, h, c)) ||
-               ((F & kCatCSG) && S.csg_root >= 0 && csg_test(S, r, h)) || ((F & kCatPlanes) && planes_scan(S, r, h));
+               ((F & kCatCSG) && S.csg_root >= 0 && ray_meets_box(r, S.csg_lo, S.csg_hi) && csg_test(S, r, h)) || ((F & kCatPlanes) && planes_scan(S, r, h));
     }
     __device__ __forceinline__ static float strand_depth(const DevScene& S, const Ray& r, Counters& c) {
         return (F & kCatStrands) ? strands_tau_ref<COUNT>(S, r, c) : 0.0f;

@@ -597,6 +597,33 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     v.csg_nodes = (const CSGNode*)dptr(o_csg);
     v.csg_root = (in->csg_nodes && in->num_csg_nodes > 0 && in->csg_root >= 0 && in->csg_root < in->num_csg_nodes)
                      ? in->csg_root : -1;
+    {
+        // the CSG leaves' box (the leaf indices were checked at the start)
+        float lo3[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi3[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+        for (int i = 0; v.csg_root >= 0 && i < in->num_csg_nodes; i++) {
+            const CSGNode& c = in->csg_nodes[i];
+            float cen[3], ext[3];
+            if (c.leaf_kind == 0) {
+                const Object& o = in->objects[c.leaf_index];
+                cen[0] = o.param1.x; cen[1] = o.param1.y; cen[2] = o.param1.z;
+                ext[0] = ext[1] = ext[2] = std::fabs(o.param2);
+            } else if (c.leaf_kind == 1) {
+                const Superellipsoid& se = in->superellipsoids[c.leaf_index];
+                cen[0] = se.center.x; cen[1] = se.center.y; cen[2] = se.center.z;
+                ext[0] = std::fabs(se.a); ext[1] = std::fabs(se.b); ext[2] = std::fabs(se.c);
+            } else {
+                continue;
+            }
+            for (int k = 0; k < 3; k++) {
+                lo3[k] = std::min(lo3[k], cen[k] - ext[k]);
+                hi3[k] = std::max(hi3[k], cen[k] + ext[k]);
+            }
+        }
+        float scale = 0.0f;
+        for (int k = 0; k < 3; k++) scale = std::max(scale, std::max(std::fabs(lo3[k]), std::fabs(hi3[k])));
+        const float m = lo3[0] <= hi3[0] ? 1e-4f * scale + 1e-6f : 0.0f;
+        for (int k = 0; k < 3; k++) { v.csg_lo[k] = lo3[k] - m; v.csg_hi[k] = hi3[k] + m; }
+    }
     v.planes = (const Plane*)dptr(o_pla); v.num_planes = in->num_planes;
     v.materials = (const Material*)dptr(o_mat); v.num_materials = in->num_materials;
     v.textures = (const TextureRef*)dptr(o_tex); v.num_textures = in->num_textures;

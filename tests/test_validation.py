@@ -140,3 +140,28 @@ def test_superellipsoid_sign_shortcuts_hits_equal_plain_form(analytic):
     assert (o0 < 0).sum() > 1000                    # superellipsoid hits present
     assert np.array_equal(o0, o1) and np.array_equal(m0, m1)
     assert np.array_equal(t0, t1)
+
+
+@pytest.mark.gpu
+def test_csg_box_hits_equal_plain_form(analytic):
+    """The wavefront form skips the CSG tree for rays that miss the box of
+    its leaf solids; on a scene of spheres, superellipsoids, the CSG tree
+    and the ground plane its primary hits equal the plain form's bit for
+    bit (the plain form evaluates the tree for every ray, as the reference
+    does)."""
+    sb.init(0, 100)
+    v = _copy(analytic)
+    for k in ("num_sweep_strands", "num_triangles", "num_heightfields", "num_lathes", "num_prisms"):
+        setattr(v, k, 0)
+    assert v.csg_root >= 0
+    hits = []
+    for form in (sb.FORM_PLAIN, sb.FORM_WAVEFRONT):
+        ds = sb.DeviceScene(v, form)
+        hits.append(ds.primary_hits(640, 360, 1))
+        img, _ = ds.render_host(160, 90, 1)
+        hits[-1] = hits[-1] + (img,)
+        ds.close()
+    (o0, m0, t0, i0), (o1, m1, t1, i1) = hits
+    assert np.array_equal(o0, o1) and np.array_equal(m0, m1)
+    assert np.array_equal(t0, t1)
+    assert np.abs(i0 - i1).mean() <= 1e-3
