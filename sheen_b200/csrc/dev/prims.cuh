@@ -259,7 +259,7 @@ __device__ __forceinline__ bool lathe_test(const Ray& r, const Lathe& l, const L
 
 // cone_test's constants of every lathe segment (p0 = (0, y_i, 0), p1 =
 // (0, y_{i+1}, 0)), with cone_test's expressions: seg[2p] = {y0, r0, k, L},
-// seg[2p + 1] = {da.y, 0, 0, valid}; valid 0 for a segment lathe_test
+// seg[2p + 1] = {da.y, y1, r1, valid}; valid 0 for a segment lathe_test
 // skips (both radii <= 0, or L^2 < 1e-12).  The axis has no x / z part, so
 // da = (0, da.y, 0) exactly.
 static __global__ void lathe_segments_kernel(const Lathe* __restrict__ lathes, int nl, const LathePoint* __restrict__ pts,
@@ -295,7 +295,7 @@ static __global__ void lathe_segments_kernel(const Lathe* __restrict__ lathes, i
                 const float3 da = axis / L;
                 const float k = (b.radius - a.radius) / L;
                 s0 = make_float4(a.y, a.radius, k, L);
-                s1 = make_float4(da.y, 0.0f, 0.0f, 1.0f);
+                s1 = make_float4(da.y, b.y, b.radius, 1.0f);
             }
         }
         seg[2 * (size_t)p] = s0;
@@ -303,27 +303,52 @@ static __global__ void lathe_segments_kernel(const Lathe* __restrict__ lathes, i
     }
 }
 
+// The ray's terms shared by every lathe test (computed once per ray: the
+// reference's lathe bounds are infinite in x and z, so a ray meets every
+// lathe whose y range it crosses).
+struct LatheRay {
+    float inv[3];            // 1 / d
+    float axz, bxz, cxz;     // squared distance to the Y axis: axz t^2 + 2 bxz t + cxz
+    float tstar;             // its minimum
+    __device__ __forceinline__ explicit LatheRay(const Ray& r) {
+        inv[0] = 1.0f / r.d.x;
+        inv[1] = 1.0f / r.d.y;
+        inv[2] = 1.0f / r.d.z;
+        axz = r.d.x * r.d.x + r.d.z * r.d.z;
+        bxz = r.o.x * r.d.x + r.o.z * r.d.z;
+        cxz = r.o.x * r.o.x + r.o.z * r.o.z;
+        tstar = axz > 0.0f ? -bxz / axz : 0.0f;
+    }
+};
+
 // lathe_test with the segment constants precomputed (lathe_segments_kernel):
 // cone_test's steps after its axis, L, da and k, so the same hits and
 // records, without a square root and four divisions per segment.
-__device__ __forceinline__ bool lathe_test_pre(const Ray& r, const Lathe& l, const float4* __restrict__ seg,
-                                               float4 bound, Hit& h) {
+__device__ __forceinline__ bool lathe_test_pre(const Ray& r, const LatheRay& lr, const Lathe& l,
+                                               const float4* __restrict__ seg, float4 bound, Hit& h) {
     if (l.point_count < 2 || bound.w == 0.0f) return false;
     {
         // slab test against the surface's box (a NaN from 0 * inf leaves
         // that slab unconstrained)
         const float lo[3] = {-bound.x, bound.y, -bound.x}, hi[3] = {bound.x, bound.z, bound.x};
-        const float o[3] = {r.o.x, r.o.y, r.o.z}, d[3] = {r.d.x, r.d.y, r.d.z};
+        const float o[3] = {r.o.x, r.o.y, r.o.z};
         float tn = r.tmin, tf = r.tmax;
 #pragma unroll
         for (int a = 0; a < 3; a++) {
-            const float inv = 1.0f / d[a];
+            const float inv = lr.inv[a];
             const float t0 = (lo[a] - o[a]) * inv, t1 = (hi[a] - o[a]) * inv;
             tn = fmaxf(tn, fminf(t0, t1));
             tf = fminf(tf, fmaxf(t0, t1));
         }
         if (tn > tf + 1e-5f * (fabsf(tn) + fabsf(tf)) + 1e-6f) return false;
     }
+    // The ray's squared distance to the Y axis, q(t) = axz t^2 + 2 bxz t +
+    // cxz, is convex: a segment is skipped when q stays above its largest
+    // radius squared over the ray's t-range inside the segment's y-slab
+    // (1e-4 relative margins in space, 1e-5 relative slack in t and q, far
+    // above the rounding of a hit cone_test accepts, cancellation included).
+    const float idy = lr.inv[1];
+    const float axz = lr.axz, bxz = lr.bxz, cxz = lr.cxz, tstar = lr.tstar;
     bool any = false;
     float best = r.tmax;
     for (int i = 0; i < l.point_count - 1; i++) {
@@ -331,6 +356,27 @@ __device__ __forceinline__ bool lathe_test_pre(const Ray& r, const Lathe& l, con
         const float4 s1 = __ldg(&seg[2 * (size_t)p + 1]);
         if (s1.w == 0.0f) continue;
         const float4 s0 = __ldg(&seg[2 * (size_t)p]);
+        {
+            const float rs = fmaxf(fabsf(s0.y), fabsf(s1.z));
+            const float m = 1e-4f * (fabsf(s0.x) + fabsf(s1.y) + rs) + 1e-6f;
+            const float ylo = fminf(s0.x, s1.y) - m, yhi = fmaxf(s0.x, s1.y) + m;
+            float ta = r.tmin, tb = r.tmax;
+            if (r.d.y != 0.0f) {
+                const float u0 = (ylo - r.o.y) * idy, u1 = (yhi - r.o.y) * idy;
+                ta = fmaxf(ta, fminf(u0, u1));
+                tb = fminf(tb, fmaxf(u0, u1));
+            } else if (r.o.y < ylo || r.o.y > yhi) {
+                continue;
+            }
+            if (ta > tb + 1e-5f * (fabsf(ta) + fabsf(tb)) + 1e-6f) continue;
+            if (ta <= tb) {
+                const float tc = fminf(fmaxf(tstar, ta), tb);
+                const float q = axz * tc * tc + 2.0f * bxz * tc + cxz;
+                const float rr = rs + m;
+                const float tol = 1e-5f * (axz * tc * tc + 2.0f * fabsf(bxz * tc) + cxz) + 1e-4f * rr * rr;
+                if (q > rr * rr + tol) continue;
+            }
+        }
         const float3 p0 = f3(0.0f, s0.x, 0.0f);
         const float r0 = s0.y, k = s0.z, L = s0.w;
         const float3 da = f3(0.0f, s1.x, 0.0f);

@@ -468,9 +468,10 @@ __device__ __forceinline__ bool lathes_cull(const DevScene& S, const Ray& r, Hit
     if (S.num_lathes == 0) return false;
     bool any = false;
     float best = r.tmax;
+    const LatheRay lr(r);
     dfs_cull<COUNT>(S.lathe_bvh, r, best, c, [&](int i) {
         Hit tmp;
-        if (lathe_test_pre(r, S.lathes[i], S.lathe_seg, __ldg(&S.lathe_bound[i]), tmp) && tmp.t < best) {
+        if (lathe_test_pre(r, lr, S.lathes[i], S.lathe_seg, __ldg(&S.lathe_bound[i]), tmp) && tmp.t < best) {
             h = tmp; h.obj = -(i + 1); best = tmp.t; any = true;
         }
     });
