@@ -24,6 +24,7 @@
 #include <cfloat>
 #include <climits>
 #include <cstring>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -1498,6 +1499,25 @@ done:
 // all triangles (build_qbvh4_with_kept); the passable triangles' tree is
 // built at the same time from a second host thread on a second stream.
 // Allocations go to s.extra.
+// The second build stream of a device, created once and kept: memory the
+// pool hands out and takes back on the same stream is reused in stream
+// order, where a fresh stream per call can make the pool map new memory.
+static cudaError_t build_stream2(cudaStream_t* out) {
+    static std::mutex mu;
+    static cudaStream_t streams[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!streams[dev] && (e = cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking)) != cudaSuccess) {
+        streams[dev] = nullptr;
+        return e;
+    }
+    *out = streams[dev];
+    return cudaSuccess;
+}
+
 cudaError_t build_wave_meshes_device(DeviceScene& s, cudaStream_t stream) {
     dev::DevScene& v = s.view;
     const int n = v.num_tris;
@@ -1515,7 +1535,7 @@ cudaError_t build_wave_meshes_device(DeviceScene& s, cudaStream_t stream) {
     cudaError_t e_all = cudaSuccess, e_sub = cudaSuccess;
     const bool wt = tuning().watertight != 0;
 #define CK(x) do { if ((e = (x)) != cudaSuccess) goto done; } while (0)
-    CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+    CK(build_stream2(&st2));
     CK(dmalloc_async(&iota, (size_t)n * sizeof(int), stream));
     CK(dmalloc_async(&sel, (size_t)2 * n * sizeof(int), stream));
     CK(dmalloc_async(&flags, (size_t)2 * n, stream));
@@ -1555,7 +1575,7 @@ done:
     dfree_async(flags, stream);
     dfree_async(cub_tmp, stream);
     dfree_async(num_sel, stream);
-    if (st2) cudaStreamDestroy(st2);
+    if (st2) cudaStreamSynchronize(st2);
     auto keep = [&](const DevQBvh& q) {
         if (q.nodes) s.extra.push_back(q.nodes);
         if (q.tris) s.extra.push_back(q.tris);

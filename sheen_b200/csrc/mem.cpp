@@ -110,6 +110,7 @@ void dfree(void* ptr) {
     if (pool_of(dev, p) != cudaSuccess) return;
     cudaDeviceSynchronize();   // like cudaFree: no kernel may still use the block
     cudaFreeAsync(ptr, p->stream);
+    cudaStreamSynchronize(p->stream);   // the free has happened: any stream may reuse the block
 }
 
 void dfree_async(void* ptr, cudaStream_t stream) {
