@@ -254,7 +254,7 @@ def run_ours(args):
 
     pk = peaks()
     fp32_peak = 148 * 128 * 2 * pk["sm_max_mhz"] * 1e6
-    # Algorithmic bytes and FP32 work (BASELINE.md section 3): 32 B ray in +
+    # Algorithmic bytes and FP32 work: 32 B ray in +
     # 16 B hit out per ray, the node record per node visited, 48 B per
     # triangle tested; 14 FP32 ops per box test (a BVH4 node visit tests 4
     # boxes; the plain form counts single boxes), 35 per triangle test.

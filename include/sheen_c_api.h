@@ -183,22 +183,24 @@ int sheen_scene_render_region(SheenDeviceScene scene, int width, int height, int
  * the reference (its C-ABI only renders whole frames to a PNG).
  *
  * For callers that must not have the library allocate GPU memory during a
- * render: a frame recorded into a CUDA graph (cudaMalloc is not allowed while
- * a stream is being captured), a real-time loop that reserves all of its
- * device memory at start-up, or an application whose memory manager owns
- * every byte.  It renders the pixel rectangle [x0, x1) x [y0, y1) of a
- * width x height image of a SHEEN_FORM_WAVEFRONT scene into the caller's
- * DEVICE buffer (whole image, width*height float4) on `stream`, with the
- * wavefront kernels' scratch in a fixed array in the library's device
- * globals (about 13 MB, held on every GPU that loads the library until
- * exit).  Nothing is allocated and nothing is synchronised.
+ * render: a real-time loop that reserves all of its device memory at
+ * start-up and treats any later allocation as a fault, or an application
+ * whose own memory manager must own every byte on the device.  It renders
+ * the pixel rectangle [x0, x1) x [y0, y1) of a width x height image of a
+ * SHEEN_FORM_WAVEFRONT scene into the caller's DEVICE buffer (whole image,
+ * width*height float4) on `stream`, with the same queue kernels as the
+ * regular entry points and their scratch in a fixed array in the library's
+ * device globals (about 13 MB, held on every GPU that loads the library
+ * until exit).  Nothing is allocated and nothing is synchronised.
  *
  * Limits: at most 16384 samples per call (the rectangle's pixels rounded up
  * to whole 16x8 tiles, times aa_samples -- e.g. 128x128 at 1 spp or 64x64 at
  * 4 spp) and at most 8 lights; larger requests fail with -1 and a message.
- * The first call on each device looks up the array's device address; make
- * that first call outside any stream capture.  Every call shares the array:
- * calls that can overlap on the GPU race, so serialise them (one stream). */
+ * The first call on each device (and the first after sheen_cleanup) looks up
+ * the array's device address; make that call before any stream capture.
+ * Each call clears the queue counters it starts from; the rest of the array
+ * keeps the last call's contents.  Every call shares the array: calls that
+ * can overlap on the GPU race, so serialise them (one stream). */
 int sheen_scene_render_region_noalloc(SheenDeviceScene scene, int width, int height, int aa_samples,
                                       int x0, int y0, int x1, int y1, float* out_rgba_device, void* stream);
 

@@ -956,8 +956,15 @@ static int cat_planes(const OracleScene* S, const Ray* r, Hit* h) {
     return any;
 }
 
+/* Scene queries issued by this thread (every scene_hit / scene_hit_opaque
+ * call): the ray count of the throughput metric -- primary, each glass pass
+ * of a shadow ray, every mirror / refraction segment, beam and medium shadow
+ * rays. */
+static _Thread_local unsigned long long tl_queries;
+
 /* integrator/raycast.h:14-70 -- closest hit over the categories in order */
 static int scene_hit(const OracleScene* S, const Ray* r, Hit* rec) {
+    tl_queries++;
     real best = r->tmax;
     int hit = 0;
     Hit t;
@@ -978,6 +985,7 @@ static int scene_hit(const OracleScene* S, const Ray* r, Hit* rec) {
 /* integrator/raycast.h:74-97 -- QUIRK: the first category with any hit wins
  * (its closest hit), strands excluded */
 static int scene_hit_opaque(const OracleScene* S, const Ray* r, Hit* rec) {
+    tl_queries++;
     if (cat_spheres(S, r, rec)) return 1;
     if (cat_mesh(S, r, rec)) return 1;
     if (cat_hf(S, r, rec)) return 1;
@@ -1798,9 +1806,30 @@ int oracle_render(const OracleScene* S, int W, int H, int aa, float* out, int y0
     return 0;
 }
 
+/* Closest hit of the camera ray of sample s of pixel (x, y) (the camera of
+ * render_kernel.cu:500-521 in the oracle's precision). */
+static int primary_sample(const OracleScene* S, int W, int H, int ns, int x, int y, int s, Hit* h) {
+    const CameraData* cam = &S->s.camera;
+    real ox, oy;
+    sample_pos(S, s, ns, x, y, &ox, &oy);
+    real u = ((real)x + ox) / (real)W * 2 - 1, v = 1 - ((real)y + oy) / (real)H * 2;
+    real tan_h = 1, tan_x = 1, tan_y = 1;
+    if (cam->focal_length > 0) {
+        tan_h = R(0.5) * cam->sensor_width / cam->focal_length;
+        if (W >= H) { tan_x = tan_h; tan_y = tan_h * (real)H / (real)W; }
+        else { tan_y = tan_h; tan_x = tan_h * (real)W / (real)H; }
+    }
+    Ray ray;
+    ray.o = fv(cam->position);
+    ray.d = nrm(add(add(fv(cam->forward), mul(fv(cam->right), u * tan_x + cam->shift_x * tan_h)),
+                    mul(fv(cam->up), v * tan_y + cam->shift_y * tan_h)));
+    ray.tmin = R(0.001);
+    ray.tmax = R(1e10);
+    return scene_hit(S, &ray, h);
+}
+
 int oracle_primary_hits(const OracleScene* S, int W, int H, int aa, int* cat, int* prim, double* tt, int nthreads) {
     if (!S) return -1;
-    const CameraData* cam = &S->s.camera;
     const int ns = aa < 1 ? 1 : (aa > 64 ? 64 : aa);
 #ifdef _OPENMP
     if (nthreads <= 0) nthreads = omp_get_max_threads();
@@ -1810,26 +1839,53 @@ int oracle_primary_hits(const OracleScene* S, int W, int H, int aa, int* cat, in
     for (int y = 0; y < H; y++)
         for (int x = 0; x < W; x++)
             for (int s = 0; s < ns; s++) {
-                real ox, oy;
-                sample_pos(S, s, ns, x, y, &ox, &oy);
-                real u = ((real)x + ox) / (real)W * 2 - 1, v = 1 - ((real)y + oy) / (real)H * 2;
-                real tan_h = 1, tan_x = 1, tan_y = 1;
-                if (cam->focal_length > 0) {
-                    tan_h = R(0.5) * cam->sensor_width / cam->focal_length;
-                    if (W >= H) { tan_x = tan_h; tan_y = tan_h * (real)H / (real)W; }
-                    else { tan_y = tan_h; tan_x = tan_h * (real)W / (real)H; }
-                }
-                Ray ray;
-                ray.o = fv(cam->position);
-                ray.d = nrm(add(add(fv(cam->forward), mul(fv(cam->right), u * tan_x + cam->shift_x * tan_h)),
-                                mul(fv(cam->up), v * tan_y + cam->shift_y * tan_h)));
-                ray.tmin = R(0.001);
-                ray.tmax = R(1e10);
                 Hit h;
                 size_t k = ((size_t)y * W + x) * ns + s;
-                if (scene_hit(S, &ray, &h)) { cat[k] = h.cat; prim[k] = h.prim; tt[k] = (double)h.t; }
+                if (primary_sample(S, W, H, ns, x, y, s, &h)) { cat[k] = h.cat; prim[k] = h.prim; tt[k] = (double)h.t; }
                 else { cat[k] = -1; prim[k] = -1; tt[k] = -1.0; }
             }
+    return 0;
+}
+
+int oracle_primary_hits_px(const OracleScene* S, int W, int H, int aa, int n, const int* pixels, int* cat,
+                           int* prim, double* tt, int nthreads) {
+    if (!S || n < 0 || (n > 0 && !pixels)) return -1;
+    const int ns = aa < 1 ? 1 : (aa > 64 ? 64 : aa);
+    for (int i = 0; i < n; i++)
+        if (pixels[i] < 0 || pixels[i] >= W * H) return -1;
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#endif
+    (void)nthreads;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int i = 0; i < n; i++)
+        for (int s = 0; s < ns; s++) {
+            Hit h;
+            const int x = pixels[i] % W, y = pixels[i] / W;
+            size_t k = (size_t)i * ns + s;
+            if (primary_sample(S, W, H, ns, x, y, s, &h)) { cat[k] = h.cat; prim[k] = h.prim; tt[k] = (double)h.t; }
+            else { cat[k] = -1; prim[k] = -1; tt[k] = -1.0; }
+        }
+    return 0;
+}
+
+int oracle_render_region(const OracleScene* S, int W, int H, int aa, int x0, int y0, int x1, int y1, float* out,
+                         int nthreads, unsigned long long* queries) {
+    if (!S || W <= 0 || H <= 0 || !out || x0 < 0 || y0 < 0 || x1 > W || y1 > H || x0 >= x1 || y0 >= y1) return -1;
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#endif
+    (void)nthreads;
+    unsigned long long total = 0;
+#pragma omp parallel num_threads(nthreads) reduction(+ : total)
+    {
+        const unsigned long long q0 = tl_queries;
+#pragma omp for schedule(dynamic, 1)
+        for (int y = y0; y < y1; y++)
+            for (int x = x0; x < x1; x++) render_pixel(S, x, y, W, H, aa, out + 4 * ((size_t)y * W + x));
+        total += tl_queries - q0;
+    }
+    if (queries) *queries = total;
     return 0;
 }
 

@@ -52,6 +52,19 @@ int oracle_render(const OracleScene* s, int width, int height, int aa,
 int oracle_primary_hits(const OracleScene* s, int width, int height, int aa,
                         int* category, int* prim, double* t, int nthreads);
 
+/* Primary closest hits of the n pixels pixels[i] = y*width + x: n*ns
+ * entries, index i*ns + s, as oracle_primary_hits. */
+int oracle_primary_hits_px(const OracleScene* s, int width, int height, int aa, int n, const int* pixels,
+                           int* category, int* prim, double* t, int nthreads);
+
+/* RGBA of the pixel rectangle [x0, x1) x [y0, y1) into out_rgba (the whole
+ * width*height*4 image; other pixels untouched) and the number of scene
+ * queries the rectangle issued (*queries, may be NULL): primary rays, each
+ * glass pass of a shadow ray, every mirror / refraction segment, beam and
+ * medium shadow rays -- the ray count of the throughput metric. */
+int oracle_render_region(const OracleScene* s, int width, int height, int aa, int x0, int y0, int x1, int y1,
+                         float* out_rgba, int nthreads, unsigned long long* queries);
+
 /* Closest hit of arbitrary rays (origin, direction as 6 doubles per ray,
  * t_min 1e-3, t_max 1e10): category, prim, t. */
 int oracle_trace(const OracleScene* s, int n, const double* rays,

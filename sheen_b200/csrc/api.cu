@@ -116,6 +116,9 @@ void sheen_cleanup(void) {
     cudaDeviceSynchronize();
     sheen::release_parked_waves();
     sheen::release_upload_rings();
+    sheen::release_build_streams();
+    sheen::release_noalloc_scratch();
+    sheen::release_srgb_tables();
     sheen::release_pools();
     cudaDeviceReset();
 }

@@ -1382,12 +1382,10 @@ cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, D
         {
             // 37.6 KB of static shared memory a block: ask for the largest
             // shared-memory carveout so that six blocks fit on an SM
-            static const bool carveout = [] {
-                cudaFuncSetAttribute(k_small, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                     cudaSharedmemCarveoutMaxShared);
-                return true;
-            }();
-            (void)carveout;
+            // (a per-context hint: set on every build, so that it holds on
+            // every device and after sheen_cleanup's device reset)
+            cudaFuncSetAttribute(k_small, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
         }
         k_small<<<ns, kSmallThreads, 0, stream>>>(small_buf, small_buf + ns, P.plo, P.phi, P.idx, P.nodes, P.err,
                                                   node_cost_of(tuning().node_cost));
@@ -1502,9 +1500,27 @@ done:
 // The second build stream of a device, created once and kept: memory the
 // pool hands out and takes back on the same stream is reused in stream
 // order, where a fresh stream per call can make the pool map new memory.
+namespace {
+std::mutex g_build_stream_mu;
+cudaStream_t g_build_streams[64] = {};
+}  // namespace
+
+void release_build_streams() {
+    std::lock_guard<std::mutex> lk(g_build_stream_mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (int d = 0; d < 64; d++) {
+        if (!g_build_streams[d]) continue;
+        cudaSetDevice(d);
+        cudaStreamDestroy(g_build_streams[d]);
+        g_build_streams[d] = nullptr;
+    }
+    cudaSetDevice(cur);
+}
+
 static cudaError_t build_stream2(cudaStream_t* out) {
-    static std::mutex mu;
-    static cudaStream_t streams[64] = {};
+    auto& mu = g_build_stream_mu;
+    auto& streams = g_build_streams;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;

@@ -138,6 +138,13 @@ cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, fl
 void wave_release(DeviceScene& s);
 // Frees the queue blocks kept from released scenes (render_wave.cu).
 void release_parked_waves();
+// Forget the cached device address of the allocation-free entry point's
+// scratch array (sheen_cleanup resets the device, which invalidates it).
+void release_noalloc_scratch();
+// Destroy the device BVH builder's cached second streams (one per device).
+void release_build_streams();
+// Mark the device sRGB threshold tables as not uploaded.
+void release_srgb_tables();
 
 // Wavefront form on caller-owned scratch (the request loop: one block per
 // in-flight request).  Renders a region with the queue kernels launched

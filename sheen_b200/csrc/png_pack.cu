@@ -50,6 +50,13 @@ std::mutex g_mu;
 bool g_ready[kMaxDevices] = {false};
 }  // namespace
 
+// sheen_cleanup resets the device, which clears the constant table: the next
+// pack on each device uploads it again.
+void release_srgb_tables() {
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (auto& r : g_ready) r = false;
+}
+
 cudaError_t pack_srgb_rows(const float4* img, int W, int H, unsigned char* rows, cudaStream_t stream) {
     int dev_id = 0;
     cudaError_t e = cudaGetDevice(&dev_id);

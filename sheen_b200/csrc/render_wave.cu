@@ -821,14 +821,18 @@ struct Wave {
     bool has_direct = false;
 };
 
-static size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+static constexpr size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
-size_t wave_scratch_bytes(int L, long long nsamples) {
-    const size_t n = (size_t)nsamples;
-    return align256(n * 3 * (L + 2) * 3 * sizeof(float)) + align256(n * 3 * sizeof(float)) +
-           align256(n * std::max(L, 1) * 3 * sizeof(float4)) + 2 * align256(n * 2 * sizeof(float4)) +
-           align256(dev::kCounterWords * sizeof(unsigned int));
+// Bytes of the queue and slot arrays for `nsamples` samples and L lights, as
+// wave_carve lays them out (each array 256-byte aligned).
+static constexpr size_t wave_scratch_bytes_for(int L, long long nsamples) {
+    return align256((size_t)nsamples * 3 * (L + 2) * 3 * sizeof(float)) +
+           align256((size_t)nsamples * 3 * sizeof(float)) +
+           align256((size_t)nsamples * (L > 1 ? L : 1) * 3 * sizeof(float4)) +
+           2 * align256((size_t)nsamples * 2 * sizeof(float4)) + align256(dev::kCounterWords * sizeof(unsigned int));
 }
+
+size_t wave_scratch_bytes(int L, long long nsamples) { return wave_scratch_bytes_for(L, nsamples); }
 
 // Points w's arrays into [base, base + bytes) for `nsamples` samples and L
 // lights (base 256-byte aligned).  False when the block is too small.
@@ -852,15 +856,11 @@ static bool wave_carve(Wave& w, void* base, size_t bytes, int L, long long nsamp
     return true;
 }
 
+// SM count of the current device.
 static int device_sms() {
-    static int sms = 0;
-    if (!sms) {
-        int dev_id = 0, n = 148;
-        cudaGetDevice(&dev_id);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev_id);
-        sms = n;
-    }
-    return sms;
+    int dev_id = 0, n = 148;
+    if (cudaGetDevice(&dev_id) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev_id);
+    return n > 0 ? n : 148;
 }
 
 // Persistent grid: as many 128-thread blocks as fit on every SM.
@@ -878,6 +878,38 @@ static int shadow_grid(K kernel, int sms, int per_sm) {
     return per_sm > 0 ? std::min(full, sms * per_sm) : full;
 }
 
+// Persistent grids of the primary, mirror and refraction kernels of one
+// variant, per device: computed on a device's first frame under a lock, so
+// threads that start frames at the same time, or on different GPU models,
+// each see complete grids for their own device.
+struct StageGrids {
+    int sms = 0, primary = 0, reflect = 0, refract = 0;
+};
+constexpr int kGridDevices = 64;
+
+template <int F, bool MULTI>
+static StageGrids stage_grids() {
+    static std::mutex mu;
+    static StageGrids grids[kGridDevices];
+    int d = 0;
+    cudaGetDevice(&d);
+    StageGrids g;
+    if (d >= 0 && d < kGridDevices) {
+        std::lock_guard<std::mutex> lk(mu);
+        g = grids[d];
+    }
+    if (g.primary) return g;
+    g.sms = device_sms();
+    g.primary = persistent_grid(dev::wave_primary<F, MULTI>, g.sms);
+    g.reflect = persistent_grid(dev::wave_reflect<F, MULTI>, g.sms);
+    g.refract = persistent_grid(dev::wave_refract<F, MULTI>, g.sms);
+    if (d >= 0 && d < kGridDevices) {
+        std::lock_guard<std::mutex> lk(mu);
+        grids[d] = g;
+    }
+    return g;
+}
+
 // The queue pipeline for category set F: one frame (S0 / V), or with MULTI
 // every job of V.jobs (S0 unused; npad is then the total padded pixels).
 // Stage profiling (not inside a graph): `ev` gets 8 events recorded at the
@@ -888,13 +920,8 @@ template <int F, bool MULTI = false>
 static cudaError_t run_pipeline(const dev::DevScene& S0, const dev::WaveView& V, int npad, float4* out,
                                 cudaStream_t stream, unsigned long long* tally, cudaEvent_t* ev = nullptr,
                                 unsigned int* snap = nullptr) {
-    static int g_primary = 0, g_reflect = 0, g_refract = 0;
-    const int sms = device_sms();
-    if (!g_primary) {
-        g_primary = persistent_grid(dev::wave_primary<F, MULTI>, sms);
-        g_reflect = persistent_grid(dev::wave_reflect<F, MULTI>, sms);
-        g_refract = persistent_grid(dev::wave_refract<F, MULTI>, sms);
-    }
+    const StageGrids grids = stage_grids<F, MULTI>();
+    const int sms = grids.sms, g_primary = grids.primary, g_reflect = grids.reflect, g_refract = grids.refract;
     const Tuning tu = tuning();
     const bool refill = tu.shadow_kernel == 1;
     const bool smem = tu.shadow_stack == 1;
@@ -1327,39 +1354,31 @@ cudaError_t launch_wavefront_scratch(DeviceScene& s, void* scratch, size_t scrat
 // Allocation-free rendering of a small region (sheen_scene_render_region_noalloc).
 //
 // Some callers cannot let the library allocate GPU memory while they draw:
-// a host that records its frame into a CUDA graph (cudaMalloc is not allowed
-// while a stream is being captured), a real-time loop that reserves all of
-// its device memory at start-up and treats any later allocation as a fault,
-// or an embedding application whose memory manager must own every byte.
-// The regular entry points allocate the wavefront queues on first use and a
-// frame-sized output on the host path, so they cannot be used there.  This
-// variant runs the same wavefront kernels with their scratch (per-sample
+// a real-time loop that reserves all of its device memory at start-up and
+// treats any later allocation as a fault, or an embedding application whose
+// memory manager must own every byte on the device.  The regular entry
+// points allocate the wavefront queues on a scene's first frame (and again
+// when a larger frame comes), so they cannot be used there.  This variant
+// runs the same queue pipeline -- the same kernels, variant and launch
+// parameters as a resident scene's own frames -- with its scratch (per-sample
 // light slots, blend weights, the three ray queues and their counters)
-// placed in one fixed array in the library's device globals instead.
+// carved from one fixed array in the library's device globals instead.
 //
 // Limits: at most kNoAllocMaxSamples samples per call (the region's pixels
 // rounded up to whole 16x8 tiles, times the samples per pixel -- e.g. a
 // 128x128 tile at 1 spp or 64x64 at 4 spp) and scenes with at most
 // kNoAllocMaxLights lights.  The array (about 13 MB) is held on every GPU
 // that loads the library until the process exits.  Every call uses the same
-// array: calls that can overlap on the GPU (different streams, or threads
-// issuing concurrently) race and must be serialised by the caller, e.g. by
-// issuing them on one stream.
+// array and each call clears the queue counters it starts from: calls that
+// can overlap on the GPU (different streams, or threads issuing
+// concurrently) race and must be serialised by the caller, e.g. by issuing
+// them on one stream.
 // ---------------------------------------------------------------------
 namespace {
 
 constexpr int kNoAllocMaxSamples = 16384;
 constexpr int kNoAllocMaxLights = 8;
-constexpr size_t kNoAllocSlotFloats = (size_t)kNoAllocMaxSamples * 3 * (kNoAllocMaxLights + 2) * 3;
-constexpr size_t kNoAllocCoefFloats = (size_t)kNoAllocMaxSamples * 3;
-constexpr size_t kNoAllocShadowEntries = (size_t)kNoAllocMaxSamples * kNoAllocMaxLights;
-constexpr size_t kNoAllocOffSlots = 0;
-constexpr size_t kNoAllocOffCoef = kNoAllocOffSlots + kNoAllocSlotFloats * sizeof(float);
-constexpr size_t kNoAllocOffShq = (kNoAllocOffCoef + kNoAllocCoefFloats * sizeof(float) + 255) & ~(size_t)255;
-constexpr size_t kNoAllocOffRq = kNoAllocOffShq + kNoAllocShadowEntries * 3 * sizeof(float4);
-constexpr size_t kNoAllocOffTq = kNoAllocOffRq + (size_t)kNoAllocMaxSamples * 2 * sizeof(float4);
-constexpr size_t kNoAllocOffCtr = kNoAllocOffTq + (size_t)kNoAllocMaxSamples * 2 * sizeof(float4);
-constexpr size_t kNoAllocBytes = kNoAllocOffCtr + dev::kCounterWords * sizeof(unsigned int);
+constexpr size_t kNoAllocBytes = wave_scratch_bytes_for(kNoAllocMaxLights, kNoAllocMaxSamples);
 
 // The scratch itself.  Host code must not use this name as an address (on
 // the host it names a stand-in, not device memory); noalloc_scratch() below
@@ -1370,9 +1389,9 @@ constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mu;
 unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
 
-// Device address of the scratch array on the current device, looked up once
-// per device (the first call on a device does this; it must not be inside a
-// stream capture).
+// Device address of the scratch array on the current device, looked up with
+// cudaGetSymbolAddress on the first call on each device (and again after
+// sheen_cleanup, which resets the device and forgets the addresses).
 cudaError_t noalloc_scratch(unsigned char** out) {
     int dev_id = 0;
     cudaError_t e = cudaGetDevice(&dev_id);
@@ -1389,35 +1408,12 @@ cudaError_t noalloc_scratch(unsigned char** out) {
     return cudaSuccess;
 }
 
-template <int F>
-cudaError_t noalloc_pipeline(const DeviceScene& s, const dev::WaveView& V, int npad, float4* out,
-                             cudaStream_t stream) {
-    static int g_sms = 0, g_primary = 0, g_shadow = 0, g_reflect = 0, g_refract = 0;
-    if (!g_primary) {
-        int dev_id = 0;
-        cudaGetDevice(&dev_id);
-        cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev_id);
-        g_primary = persistent_grid(dev::wave_primary<F, false>, g_sms);
-        g_shadow = persistent_grid(dev::wave_shadow<F, false>, g_sms);
-        g_reflect = persistent_grid(dev::wave_reflect<F, false>, g_sms);
-        g_refract = persistent_grid(dev::wave_refract<F, false>, g_sms);
-    }
-    cudaError_t e;
-    // The queue counters are the only scratch that must start at zero.
-    if ((e = cudaMemsetAsync(V.ctr, 0, dev::kCounterWords * sizeof(unsigned int), stream)) != cudaSuccess) return e;
-    dev::wave_primary<F, false><<<g_primary, 128, 0, stream>>>(s.view, V);
-    dev::wave_shadow<F, false><<<g_shadow, 128, 0, stream>>>(s.view, V);
-    if ((e = cudaMemsetAsync(&V.ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
-    dev::wave_reflect<F, false><<<g_reflect, 128, 0, stream>>>(s.view, V);
-    dev::wave_shadow<F, false><<<g_shadow, 128, 0, stream>>>(s.view, V);
-    if ((e = cudaMemsetAsync(&V.ctr[dev::kShadowCount], 0, 2 * sizeof(unsigned int), stream)) != cudaSuccess) return e;
-    dev::wave_refract<F, false><<<g_refract, 128, 0, stream>>>(s.view, V);
-    dev::wave_shadow<F, false><<<g_shadow, 128, 0, stream>>>(s.view, V);
-    dev::wave_resolve<false><<<(npad + 127) / 128, 128, 0, stream>>>(V, out);
-    return cudaGetLastError();
-}
-
 }  // namespace
+
+void release_noalloc_scratch() {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    for (auto& p : g_noalloc_ptr) p = nullptr;
+}
 
 }  // namespace sheen
 
@@ -1432,9 +1428,8 @@ extern "C" int sheen_scene_render_region_noalloc(SheenDeviceScene h, int W, int 
         set_error("allocation-free rendering needs a scene created with SHEEN_FORM_WAVEFRONT");
         return -1;
     }
-    const int rw = x1 - x0, rh = y1 - y0;
-    const long long padded = (long long)((rw + 15) / 16) * 16 * ((rh + 7) / 8) * 8;
-    const long long nsamples = padded * aa;
+    const Region rg{x0, y0, x1, y1};
+    const long long nsamples = region_padded(rg) * aa;
     if (nsamples > kNoAllocMaxSamples) {
         set_error("region too large for allocation-free rendering: at most 16384 samples per call "
                   "(pixels rounded up to whole 16x8 tiles, times samples per pixel)");
@@ -1444,42 +1439,14 @@ extern "C" int sheen_scene_render_region_noalloc(SheenDeviceScene h, int W, int 
         set_error("allocation-free rendering supports at most 8 lights");
         return -1;
     }
-    const cudaStream_t st = (cudaStream_t)stream;
-    float4* out = reinterpret_cast<float4*>(out_rgba_device);
-    cudaError_t e;
-    if (!wave_supported(*s)) {
-        // Beams, media and the shadow-debug mode run on the BVH4 megakernel,
-        // which needs no scratch at all.
-        e = launch_mega_bvh4(*s, W, H, aa, Region{x0, y0, x1, y1}, out, st, false);
-        if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return -1; }
-        return 0;
-    }
     unsigned char* base = nullptr;
-    if ((e = noalloc_scratch(&base)) != cudaSuccess) { set_error(cudaGetErrorString(e)); return -1; }
-    dev::WaveView V;
-    V.slots = reinterpret_cast<float*>(base + kNoAllocOffSlots);
-    V.coef = reinterpret_cast<float*>(base + kNoAllocOffCoef);
-    V.shq = reinterpret_cast<float4*>(base + kNoAllocOffShq);
-    V.rq = reinterpret_cast<float4*>(base + kNoAllocOffRq);
-    V.tq = reinterpret_cast<float4*>(base + kNoAllocOffTq);
-    V.ctr = reinterpret_cast<unsigned int*>(base + kNoAllocOffCtr);
-    V.L = s->view.num_lights;
-    V.ns = aa;
-    V.W = W; V.H = H; V.x0 = x0; V.y0 = y0; V.rw = rw; V.rh = rh;
-    V.nsamples = (int)nsamples;
-    const CameraData& cam = s->view.cam;
-    float tan_x = 1.0f;
-    if (cam.focal_length > 0.0f) {
-        const float tan_h = 0.5f * cam.sensor_width / cam.focal_length;
-        tan_x = (W >= H) ? tan_h : tan_h * float(W) / float(H);
-    }
-    V.pix_angle = 2.0f * tan_x / (float)W;
-    V.count_rays = 0;
-    const dev::DevScene& sv = s->view;
-    const bool simple = sv.num_strands == 0 && sv.num_hfs == 0 && sv.num_ses == 0 && sv.num_lathes == 0 &&
-                        sv.num_prisms == 0 && sv.csg_root < 0;
-    e = simple ? noalloc_pipeline<dev::kCatSimple>(*s, V, (int)padded, out, st)
-               : noalloc_pipeline<dev::kCatAll>(*s, V, (int)padded, out, st);
+    cudaError_t e = noalloc_scratch(&base);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return -1; }
+    // Beams, media and the shadow-debug mode run on the BVH4 megakernel,
+    // which needs no scratch; everything else runs the queue pipeline on the
+    // carved array (launch_wavefront_scratch allocates nothing).
+    e = launch_wavefront_scratch(*s, base, kNoAllocBytes, W, H, aa, rg, reinterpret_cast<float4*>(out_rgba_device),
+                                 (cudaStream_t)stream, nullptr);
     if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return -1; }
     return 0;
 }

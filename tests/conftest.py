@@ -8,7 +8,8 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
 
-REFERENCE = "/root/reference"
+# the reference source tree (loader and layout tests read it when present)
+REFERENCE = os.environ.get("SHEEN_REFERENCE", "/root/reference")
 
 
 def pytest_configure(config):

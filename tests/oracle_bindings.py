@@ -47,6 +47,10 @@ class Oracle:
         L.oracle_scene_set_centered.restype = None
         L.oracle_scene_set_knn.argtypes = [P, I]
         L.oracle_scene_set_knn.restype = None
+        L.oracle_primary_hits_px.argtypes = [P, I, I, I, I, P, P, P, P, I]
+        L.oracle_primary_hits_px.restype = I
+        L.oracle_render_region.argtypes = [P, I, I, I, I, I, I, I, P, I, P]
+        L.oracle_render_region.restype = I
 
     def scene(self, view_ptr: int, centered: bool = False, knn: int = 0):
         h = _Handle(self.lib, self.lib.oracle_scene_create(view_ptr), self.lib.oracle_scene_destroy)
@@ -80,6 +84,28 @@ class Oracle:
         assert self.lib.oracle_primary_hits(h.ptr, W, H, aa, cat.ctypes.data, prim.ctypes.data,
                                             t.ctypes.data, threads) == 0
         return cat, prim, t
+
+    def primary_hits_px(self, h, W, H, aa, pixels, threads=0):
+        """Primary hits of the given pixels (flat indices y*W + x): arrays of
+        len(pixels) * ns entries, index i*ns + s."""
+        ns = max(1, min(aa, 64))
+        px = np.ascontiguousarray(pixels, dtype=np.int32)
+        n = len(px)
+        cat = np.zeros(n * ns, np.int32)
+        prim = np.zeros(n * ns, np.int32)
+        t = np.zeros(n * ns, np.float64)
+        assert self.lib.oracle_primary_hits_px(h.ptr, W, H, aa, n, px.ctypes.data, cat.ctypes.data,
+                                               prim.ctypes.data, t.ctypes.data, threads) == 0
+        return cat, prim, t
+
+    def render_region(self, h, W, H, aa, x0, y0, x1, y1, threads=0):
+        """RGBA of a pixel rectangle (whole-image array) and the number of
+        scene queries it issued."""
+        out = np.zeros((H, W, 4), np.float32)
+        q = ctypes.c_ulonglong(0)
+        assert self.lib.oracle_render_region(h.ptr, W, H, aa, x0, y0, x1, y1, out.ctypes.data, threads,
+                                             ctypes.byref(q)) == 0
+        return out, int(q.value)
 
     def photon_count(self, h):
         return self.lib.oracle_scene_photon_count(h.ptr)

@@ -1,6 +1,6 @@
 """Parity of the CUDA renderer forms with the oracle (B200 only).
 
-Bars (restated):
+Bars:
   - per-pixel RGB (linear float4 before sRGB): mean absolute error <= 1e-3
     against the reference's render (committed golden fixtures rendered by
     the reference's own code) and against the oracle, with at most 1% of
