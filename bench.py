@@ -14,6 +14,17 @@ timed region; the path is deterministic, every frame issues the same rays).
   python bench.py [--gpus N] [--steps K] [--warmup W] [--form wavefront|plain]
                   [--impl ours|reference]
 
+Beside the timed value the line carries the metric's other parts:
+  plain     the plain FP32 form (the drop-in) on the same scene, same
+            process, same timing (vs_plain = value / plain value);
+  serving   p50/p99 latency and Mrays/s of a 64-request prefix of the
+            seeded serving stream through the request loop (N = 1 only);
+  e2e       the same frame through the host-array drop-in call (upload,
+            BVH build, render and read-back inside the timed region);
+  cpu_baseline.ray_count_check
+            the device's ray count on an 8x8 region against the oracle's
+            count of the same scene queries.
+
 --gpus N > 1 runs under torchrun: every rank renders its own replica of the
 frame on its own GPU (the path has no data exchange: "replicas only",
 weak scaling), timing is the max over ranks.
@@ -252,6 +263,41 @@ def run_ours(args):
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     e2e = rays * e2e_steps * world / e2e_s / 1e6
 
+    # The metric's denominator: the plain FP32 form (the drop-in) on the same
+    # scene in the same process, timed the same way (CUDA events, L2 flushed
+    # before each frame).
+    plain = None
+    if form == sb.FORM_WAVEFRONT and not args.no_plain:
+        pds = sb.DeviceScene(scene, sb.FORM_PLAIN)
+        prays = pds.render_device(W, H, SPP, out.data_ptr(), stream, count_rays=True)["total_rays"]
+        pds.render_device(W, H, SPP, out.data_ptr(), stream)
+        torch.cuda.synchronize()
+        pk_frames = 3
+        p_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(pk_frames)]
+        barrier(world)
+        for i, (a, b) in enumerate(p_ev):
+            flush.fill_(float(i))
+            a.record()
+            pds.render_device(W, H, SPP, out.data_ptr(), stream)
+            b.record()
+        torch.cuda.synchronize()
+        p_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in p_ev) / pk_frames, world)
+        pds.close()
+        plain = {"value": round(prays * world / (p_ms / 1e3) / 1e6, 2), "unit": "Mrays/s",
+                 "ms_per_step": round(p_ms, 3), "rays_per_frame": prays, "frames": pk_frames,
+                 "form": "plain FP32 (drop-in megakernel, reference traversal order)"}
+
+    # A short serving run: a prefix of the seeded Poisson request stream
+    # (20 requests/s, every workload generator, mixed sizes and spp) through
+    # the request loop, for the metric's p50/p99 latency.
+    serving = None
+    if world == 1 and args.serve_requests > 0:
+        res = serve_stream(args.serve_requests, args.rate, args.inflight, args.seed, 1, 0, local)
+        serving = {"value": round(res["value"], 2), "unit": "Mrays/s", "requests": len(res["stream"]),
+                   "rate_per_s": args.rate, "max_inflight": args.inflight,
+                   "latency_ms": latency_summary(res), "clocks": res["clocks"],
+                   "workload": "first %d requests of the serving stream (%s)" % (len(res["stream"]), SERVE_WORKLOAD)}
+
     pk = peaks()
     fp32_peak = 148 * 128 * 2 * pk["sm_max_mhz"] * 1e6
     # Algorithmic bytes and FP32 work: 32 B ray in +
@@ -329,6 +375,11 @@ def run_ours(args):
         "gpu_launches": args.steps * launches_per_frame(form),
         "clocks": clocks,
     }
+    if plain is not None:
+        line["plain"] = plain
+        line["vs_plain"] = round(value / plain["value"], 3)
+    if serving is not None:
+        line["serving"] = serving
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(ds, scene, stream, out)
     if rank == 0 and not args.no_ref_gpu:
@@ -391,7 +442,27 @@ def cpu_baseline(ds, scene, stream, out, steps=1):
         dt = time.perf_counter() - t0
     return {"value": round(rays * steps / dt / 1e6, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
             "sample": f"rows {CPU_BAND[0]}-{CPU_BAND[1]} of the {W}x{H} {SPP} spp frame ({rays} rays), "
-                      f"{steps} pass(es), {dt:.1f} s"}
+                      f"{steps} pass(es), {dt:.1f} s",
+            "ray_count_check": ray_count_check(ds, scene, stream, out)}
+
+
+def ray_count_check(ds, scene, stream, out):
+    """The ray count cross-check: the renderer's device counters against the
+    oracle's count of the same scene queries (its brute-force C restatement
+    of the path) on an 8x8-pixel region at the centre of the frame."""
+    from oracle_bindings import Oracle
+    x0, y0 = (W // 2) & ~7, (H // 2) & ~7
+    reg = (x0, y0, x0 + 8, y0 + 8)
+    dev = ds.render_region(W, H, SPP, *reg, out.data_ptr(), stream, count_rays=True)["total_rays"]
+    o = Oracle()
+    with quiet_stdout():
+        h = o.scene(scene.view_ptr)
+        t0 = time.perf_counter()
+        _, q = o.render_region(h, W, H, SPP, *reg)
+        dt = time.perf_counter() - t0
+    h.close()
+    return {"region": list(reg), "device_rays": dev, "oracle_rays": q, "equal": dev == q,
+            "oracle_s": round(dt, 2)}
 
 
 def reference_gpu(scene, rays, steps=3):
@@ -456,6 +527,7 @@ def run_reference(args):
     ds = sb.DeviceScene(scene, sb.FORM_PLAIN)
     out = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
     rays = band_rays(ds, torch.cuda.current_stream().cuda_stream, out)
+    count_check = ray_count_check(ds, scene, torch.cuda.current_stream().cuda_stream, out)
     ds.close()
     by0, by1 = CPU_BAND[0] // 16, CPU_BAND[1] // 16
     with quiet_stdout():
@@ -474,7 +546,7 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generator)",
         "config": {"workload": WORKLOADS.get(args.config, "") + " (row band sample)",
-                   "rays_per_step": rays},
+                   "rays_per_step": rays, "ray_count_check": count_check},
         "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -492,37 +564,30 @@ def _serving_scene(config, seed):
     return sb.generate_scene(config, seed, 8 if config == 1 else 0, photons)
 
 
-def run_serving(args):
-    """The request loop under the serving stream: requests are submitted at
-    their arrival times from a seeded Poisson stream and the server admits,
-    overlaps and completes them; every request's image lands in a host
-    buffer.  value = all rays of all requests / (last completion - first
-    arrival); p50/p99 of per-request latency (arrival -> image in host
-    memory).  The serial plain-form baseline renders a prefix of the same
-    stream one request at a time through a plain-form server."""
-    rank = int(os.environ.get("RANK", "0"))
-    import torch
-
+def serve_stream(n_requests, rate, inflight, seed, warmup, serial_k=0, local=0):
+    """The request loop under a seeded Poisson stream: requests are submitted
+    at their arrival times and the server admits, overlaps and completes
+    them; every request's image lands in a host buffer.  Returns value = all
+    rays of all requests / (last completion - first arrival) and the
+    per-request latencies (arrival -> image in host memory).  With serial_k,
+    also the first serial_k requests one at a time through a plain-form
+    server and through the wavefront server (what overlap adds)."""
     import sheen_b200 as sb
     from sheen_b200 import serve
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    sb.init(local, 100)
-    stream = serve.request_stream(args.requests, args.rate, seed=args.seed)
+    stream = serve.request_stream(n_requests, rate, seed=seed)
     keys = sorted({(r["config"], r["seed"]) for r in stream})
     t0 = time.perf_counter()
     host_scenes = {k: _serving_scene(*k) for k in keys}
     gen_s = time.perf_counter() - t0
-    srv = serve.Server(sb.FORM_WAVEFRONT, max_inflight=args.inflight)
+    srv = serve.Server(sb.FORM_WAVEFRONT, max_inflight=inflight)
     t0 = time.perf_counter()
     sid = {k: srv.add_scene(host_scenes[k]) for k in keys}
     add_s = time.perf_counter() - t0
     # warm-up: one small request per scene (kernels loaded, pool primed)
     for k in keys:
         srv.submit(sid[k], 256, 256, 1).wait()
-    for _ in range(max(0, args.warmup - 1)):
+    for _ in range(max(0, warmup - 1)):
         srv.submit(sid[keys[0]], 512, 512, 4).wait()
-    base = srv.stats()
 
     reqs = [None] * len(stream)
     infos = [None] * len(stream)
@@ -548,59 +613,82 @@ def run_serving(args):
     st = srv.stats()
     rays = sum(i["rays"] for i in infos)
     lat = np.array([i["latency_ms"] for i in infos])
-    value = rays / wall_s / 1e6
-
-    # serial plain-form baseline on a prefix of the stream
-    k = min(args.serial_sample, len(stream))
-    psrv = serve.Server(sb.FORM_PLAIN, max_inflight=1)
-    pkeys = sorted({(r["config"], r["seed"]) for r in stream[:k]})
-    psid = {kk: psrv.add_scene(host_scenes[kk]) for kk in pkeys}
-    psrv.submit(psid[pkeys[0]], 256, 256, 1).wait()
-    t0 = time.perf_counter()
-    prays = 0
-    for r in stream[:k]:
-        _, info = psrv.submit(psid[(r["config"], r["seed"])], r["width"], r["height"], r["spp"]).wait()
-        prays += info["rays"]
-    plain_s = time.perf_counter() - t0
-    psrv.close()
-    # the chosen form serially on the same prefix (what overlap adds)
-    t0 = time.perf_counter()
-    wrays = 0
-    for r in stream[:k]:
-        _, info = srv.submit(sid[(r["config"], r["seed"])], r["width"], r["height"], r["spp"]).wait()
-        wrays += info["rays"]
-    wave_serial_s = time.perf_counter() - t0
+    res = {"stream": stream, "infos": infos, "keys": keys, "wall_s": wall_s, "rays": rays,
+           "value": rays / wall_s / 1e6, "lat": lat, "stats": st, "clocks": clk.summary(),
+           "gen_s": gen_s, "add_s": add_s}
+    if serial_k:
+        # serial plain-form baseline on a prefix of the stream
+        k = min(serial_k, len(stream))
+        psrv = serve.Server(sb.FORM_PLAIN, max_inflight=1)
+        pkeys = sorted({(r["config"], r["seed"]) for r in stream[:k]})
+        psid = {kk: psrv.add_scene(host_scenes[kk]) for kk in pkeys}
+        psrv.submit(psid[pkeys[0]], 256, 256, 1).wait()
+        t0 = time.perf_counter()
+        prays = 0
+        for r in stream[:k]:
+            _, info = psrv.submit(psid[(r["config"], r["seed"])], r["width"], r["height"], r["spp"]).wait()
+            prays += info["rays"]
+        plain_s = time.perf_counter() - t0
+        psrv.close()
+        # the chosen form serially on the same prefix (what overlap adds)
+        t0 = time.perf_counter()
+        wrays = 0
+        for r in stream[:k]:
+            _, info = srv.submit(sid[(r["config"], r["seed"])], r["width"], r["height"], r["spp"]).wait()
+            wrays += info["rays"]
+        wave_serial_s = time.perf_counter() - t0
+        res.update(serial_k=k, prays=prays, plain_s=plain_s, wrays=wrays, wave_serial_s=wave_serial_s)
     srv.close()
-    clocks = clk.summary()
+    return res
+
+
+def latency_summary(res):
+    lat, infos = res["lat"], res["infos"]
+    return {"p50": round(float(np.percentile(lat, 50, method="inverted_cdf")), 2),
+            "p99": round(float(np.percentile(lat, 99, method="inverted_cdf")), 2),
+            "mean": round(float(lat.mean()), 2), "max": round(float(lat.max()), 2),
+            "queue_mean": round(float(np.mean([i["queue_ms"] for i in infos])), 2),
+            "run_mean": round(float(np.mean([i["run_ms"] for i in infos])), 2)}
+
+
+def run_serving(args):
+    """The serving workload: the whole seeded stream through the request
+    loop, with the serial plain-form and serial wavefront baselines on a
+    prefix of it."""
+    rank = int(os.environ.get("RANK", "0"))
+    import torch
+
+    import sheen_b200 as sb
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    sb.init(local, 100)
+    res = serve_stream(args.requests, args.rate, args.inflight, args.seed, args.warmup, args.serial_sample, local)
     if rank != 0:
         return
-    n = len(stream)
+    st, stream, infos, n = res["stats"], res["stream"], res["infos"], len(res["stream"])
+    k = res["serial_k"]
     line = {
-        "metric": "Mrays/s (serving)", "value": round(value, 2), "unit": "Mrays/s", "n_gpus": 1,
-        "steps": n, "warmup": args.warmup, "ms_per_step": round(wall_s * 1e3 / n, 3),
+        "metric": "Mrays/s (serving)", "value": round(res["value"], 2), "unit": "Mrays/s", "n_gpus": 1,
+        "steps": n, "warmup": args.warmup, "ms_per_step": round(res["wall_s"] * 1e3 / n, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generators, seeded request stream)",
-        "config": {"workload": SERVE_WORKLOAD, "requests": n, "rate_per_s": args.rate, "scenes": len(keys),
+        "config": {"workload": SERVE_WORKLOAD, "requests": n, "rate_per_s": args.rate, "scenes": len(res["keys"]),
                    "max_inflight": args.inflight, "form": "wavefront",
                    "l2": "inputs (2.1M-triangle scenes, 4M-photon maps) exceed L2; no flush between requests",
-                   "scene_generate_s": round(gen_s, 2), "scene_add_s": round(add_s, 2),
+                   "scene_generate_s": round(res["gen_s"], 2), "scene_add_s": round(res["add_s"], 2),
                    "scene_bytes": st["scene_bytes"], "hbm_budget": st["hbm_budget"],
                    "hbm_peak": st["hbm_peak"], "inflight_peak": st["inflight_peak"]},
-        "latency_ms": {"p50": round(float(np.percentile(lat, 50, method="inverted_cdf")), 2),
-                       "p99": round(float(np.percentile(lat, 99, method="inverted_cdf")), 2),
-                       "mean": round(float(lat.mean()), 2), "max": round(float(lat.max()), 2),
-                       "queue_mean": round(float(np.mean([i["queue_ms"] for i in infos])), 2),
-                       "run_mean": round(float(np.mean([i["run_ms"] for i in infos])), 2)},
-        "serial_plain": {"value": round(prays / plain_s / 1e6, 2), "unit": "Mrays/s",
+        "latency_ms": latency_summary(res),
+        "serial_plain": {"value": round(res["prays"] / res["plain_s"] / 1e6, 2), "unit": "Mrays/s",
                          "sample": f"first {k} requests of the stream, one at a time, plain form, "
-                                   f"scenes resident ({prays} rays, {plain_s:.1f} s)"},
-        "serial_wavefront": {"value": round(wrays / wave_serial_s / 1e6, 2), "unit": "Mrays/s",
+                                   f"scenes resident ({res['prays']} rays, {res['plain_s']:.1f} s)"},
+        "serial_wavefront": {"value": round(res["wrays"] / res["wave_serial_s"] / 1e6, 2), "unit": "Mrays/s",
                              "sample": f"same {k} requests one at a time through the wavefront server"},
-        "e2e": {"value": round(value, 2), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+        "e2e": {"value": round(res["value"], 2), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": int(sum(r["width"] * r["height"] * 16 for r in stream) / n),
                 "call": "sheen_server_submit / sheen_server_wait, images into host buffers"},
         "gpu_launches": int(sum(i["tiles"] for i in infos) * 8),
-        "clocks": clocks,
+        "clocks": res["clocks"],
         "server_stats": {kk: st[kk] for kk in ("completed", "failed", "p50_ms", "p99_ms", "busy_ms")},
     }
     print(json.dumps(line), flush=True)
@@ -630,6 +718,9 @@ def main():
     ap.add_argument("--rate", type=float, default=20.0, help="serving config: arrivals per second")
     ap.add_argument("--inflight", type=int, default=4, help="serving config: requests on the GPU at once")
     ap.add_argument("--serial-sample", type=int, default=24, help="serving config: serial baseline prefix")
+    ap.add_argument("--serve-requests", type=int, default=64,
+                    help="requests of the short serving run in the default bench line (0: skip)")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-form denominator")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -1227,6 +1227,26 @@ struct Carver {
 
 }  // namespace bvhg
 
+namespace {
+std::mutex g_build_stream_mu;
+cudaStream_t g_build_streams[64] = {};
+}  // namespace
+
+namespace {
+bool g_carveout_set[64] = {};
+}  // namespace
+
+// The small-subtree kernel asks for the largest shared-memory carveout.
+static void set_small_carveout() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> lk(g_build_stream_mu);
+    if (g_carveout_set[dev]) return;
+    cudaFuncSetAttribute(bvhg::k_small, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    g_carveout_set[dev] = true;
+}
+
+
 // Device-built BVH4 over triangles tris[subset[i]] (subset null: all n).
 // Allocates out.nodes (exact size) and out.tris (3 float4 per triangle);
 // everything else is temporary.  Synchronises `stream` once per tree level.
@@ -1382,10 +1402,9 @@ cudaError_t build_qbvh4_device(const Triangle* tris, const int* subset, int n, D
         {
             // 37.6 KB of static shared memory a block: ask for the largest
             // shared-memory carveout so that six blocks fit on an SM
-            // (a per-context hint: set on every build, so that it holds on
-            // every device and after sheen_cleanup's device reset)
-            cudaFuncSetAttribute(k_small, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 cudaSharedmemCarveoutMaxShared);
+            // (a per-context hint: set once per device, and again after
+            // sheen_cleanup's device reset)
+            set_small_carveout();
         }
         k_small<<<ns, kSmallThreads, 0, stream>>>(small_buf, small_buf + ns, P.plo, P.phi, P.idx, P.nodes, P.err,
                                                   node_cost_of(tuning().node_cost));
@@ -1500,13 +1519,9 @@ done:
 // The second build stream of a device, created once and kept: memory the
 // pool hands out and takes back on the same stream is reused in stream
 // order, where a fresh stream per call can make the pool map new memory.
-namespace {
-std::mutex g_build_stream_mu;
-cudaStream_t g_build_streams[64] = {};
-}  // namespace
-
 void release_build_streams() {
     std::lock_guard<std::mutex> lk(g_build_stream_mu);
+    for (auto& c : g_carveout_set) c = false;
     int cur = 0;
     cudaGetDevice(&cur);
     for (int d = 0; d < 64; d++) {

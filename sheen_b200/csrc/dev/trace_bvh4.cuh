@@ -499,6 +499,7 @@ enum : int {
     kCatCSG = 128, kCatPlanes = 256,
     kCatAll = 511,
     kCatSimple = kCatSpheres | kCatMesh | kCatPlanes,
+    kCatBasic = kCatSpheres | kCatPlanes,
     // triangle test compiled in (neither bit: chosen per mesh at run time)
     kTriMT = 512, kTriWT = 1024
 };

@@ -195,6 +195,9 @@ struct Tuning {
     int aa_centered = 0;            // camera samples: 0 the reference's jitter, 1 cell centres
     int se_polish = 0;              // superellipsoid entries: 0 on a sample (reference), 1 FP64 Newton polish
     int caustic_knn = 0;            // caustic gather: 0 the reference's, k in 1..64 the k nearest photons
+    int shadow_cache = 0;           // refill shadow stage: 1 tests each warp's last occluder leaf first
+    int mega_samples = 0;           // wavefront frames of at most this many samples (tile-padded pixels x spp)
+                                    // run on the BVH4 megakernel (one launch) instead of the queue stages
 };
 Tuning tuning();
 int tuning_generation();

@@ -15,7 +15,10 @@ __device__ __forceinline__ void warp_add_fast(unsigned long long* dst, unsigned 
     if ((threadIdx.x + threadIdx.y * blockDim.x) % 32 == 0) atomicAdd(dst, v);
 }
 
-template <bool COUNT>
+// F: the scene's category set and triangle test (as the queue kernels'),
+// so a scene of spheres, triangles and planes does not carry the other
+// categories' code and registers.
+template <bool COUNT, int F = kCatAll>
 __global__ void __launch_bounds__(128) mega_bvh4_kernel(DevScene S, float4* __restrict__ out, int W, int H, int aa,
                                                         int x0, int y0, int x1, int y1, unsigned long long* tally) {
     const int x = x0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
@@ -25,7 +28,7 @@ __global__ void __launch_bounds__(128) mega_bvh4_kernel(DevScene S, float4* __re
     if (x < x1 && y < y1) {
         const int ns = aa < 1 ? 1 : (aa > 64 ? 64 : aa);
         float3 acc = f3(0.0f, 0.0f, 0.0f);
-        for (int s = 0; s < ns; s++) acc += render_sample<FastTracer<COUNT>, COUNT>(S, x, y, s, ns, W, H, rt, c);
+        for (int s = 0; s < ns; s++) acc += render_sample<FastTracer<COUNT, F>, COUNT>(S, x, y, s, ns, W, H, rt, c);
         const float inv = 1.0f / float(ns);
         out[(size_t)y * W + x] = make_float4(acc.x * inv, acc.y * inv, acc.z * inv, 1.0f);
     }
@@ -93,12 +96,20 @@ cudaError_t launch_mega_bvh4(const DeviceScene& s, int W, int H, int aa, Region 
     if (!tally) tally = s.d_tally;
     const dim3 block(16, 8);
     const dim3 grid((rg.x1 - rg.x0 + 15) / 16, (rg.y1 - rg.y0 + 7) / 8);
-    if (count_nodes)
-        dev::mega_bvh4_kernel<true><<<grid, block, 0, stream>>>(s.view, out, W, H, aa, rg.x0, rg.y0, rg.x1, rg.y1,
-                                                                tally);
-    else
-        dev::mega_bvh4_kernel<false><<<grid, block, 0, stream>>>(s.view, out, W, H, aa, rg.x0, rg.y0, rg.x1, rg.y1,
-                                                                 tally);
+    const dev::DevScene& v = s.view;
+    const bool simple = v.num_strands == 0 && v.num_hfs == 0 && v.num_ses == 0 && v.num_lathes == 0 &&
+                        v.num_prisms == 0 && v.csg_root < 0;
+    const bool wt = v.q_all.watertight != 0;
+    const bool basic = simple && v.num_tris == 0;
+#define MEGA(C, F) dev::mega_bvh4_kernel<C, F><<<grid, block, 0, stream>>>(v, out, W, H, aa, rg.x0, rg.y0, rg.x1, \
+                                                                          rg.y1, tally)
+    if (count_nodes) MEGA(true, dev::kCatAll);
+    else if (basic) MEGA(false, dev::kCatBasic);
+    else if (simple && !wt) MEGA(false, dev::kCatSimple | dev::kTriMT);
+    else if (simple) MEGA(false, dev::kCatSimple | dev::kTriWT);
+    else if (!wt) MEGA(false, dev::kCatAll | dev::kTriMT);
+    else MEGA(false, dev::kCatAll | dev::kTriWT);
+#undef MEGA
     return cudaGetLastError();
 }
 

@@ -370,9 +370,19 @@ __global__ void __launch_bounds__(128) wave_shadow(DevScene S0, WaveView V0) {
 // local memory, whose scattered stores fill L1 with 32-byte sectors carrying
 // 4 useful bytes; the entry distances (closest-hit walks of the passable set
 // only) stay in local memory.  24 KB per 128-thread block.
+//
+// With `occluder_cache`, each warp remembers the leaf (and the job whose
+// tree it belongs to) where one of its lanes last found a blocking
+// triangle, and a lane starting an any-hit walk of that job's blocking tree
+// tests that leaf's triangles first.  Neighbouring queue entries are
+// neighbouring samples towards the same light, whose occluders are usually
+// the same few triangles.  Any blocking hit before the passable one decides
+// the query, and the cached triangles are in the tree the walk would search
+// (their leaf box holds them), so the result is the walk's: a hit there is
+// one the walk would have found, a miss falls through to the walk.
 template <int F, bool SMEM_STACK, bool MULTI>
 __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveView V0, int refill_min,
-                                                             int inner_min) {
+                                                             int inner_min, int occluder_cache) {
     using T = FastTracer<false, F>;
     constexpr unsigned int kFull = 0xffffffffu;
     constexpr uint32_t kLeafBit = 0x80000000u;
@@ -419,6 +429,34 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveVi
         else return stack_e_local[i];
     };
 
+    __shared__ unsigned long long occ_leaf[4];   // per warp: job << 32 | leaf entry; ~0: none
+    unsigned long long& occ = occ_leaf[threadIdx.x >> 5];
+    if (lane == 0) occ = ~0ull;
+    __syncwarp();
+    // A fresh any-hit walk (wn / wt / t_best set up): the cached leaf first.
+    auto cached_block_hit = [&]() -> bool {
+        if (!occluder_cache) return false;
+        const unsigned long long k = occ;
+        if ((unsigned int)(k >> 32) != (unsigned int)job) return false;
+        const uint32_t le = (uint32_t)k;
+        const int first = (int)((le & 0x7fffffffu) >> 3);
+        const int count = (int)(le & 7u) + 1;
+        for (int i = 0; i < count; i++) {
+            const int s = first + i;
+            const float4 a = __ldg(&wt[3 * s]);
+            const float4 b = __ldg(&wt[3 * s + 1]);
+            const float4 c4 = __ldg(&wt[3 * s + 2]);
+            float t, u, v;
+            if (qtri_test<tri_of<F>()>(q, a, b, c4, q.tmin, tmax, t, u, v, scene().q_all.watertight) &&
+                t < t_best) {
+                t_best = t; wu = u; wv = v;
+                wbest = __float_as_int(a.w);
+                return true;
+            }
+        }
+        return false;
+    };
+
     bool exhausted = false;
     for (;;) {
         // ---- refill idle lanes ------------------------------------------
@@ -461,7 +499,8 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveVi
                 state = kWalkBlock; block_after_pass = true;
                 wn = scene().q_block.nodes; wt = scene().q_block.tris;
                 entry = 0; sp = 0; wbest = -1; t_best = tp;
-                res = -3;   // keep walking
+                if (cached_block_hit()) state = kEndBlock;
+                res = -3;   // keep walking (or settle the cached hit next round)
             } else {
                 if (state == kEndPass) { pass_tri = wbest; tp = t_best; up = wu; vp = wv; }
                 res = (state == kEndBlock && wbest >= 0) ? kBlocked : kClear;
@@ -490,6 +529,7 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveVi
                         } else {
                             state = kWalkBlock; block_after_pass = false;
                             wn = scene().q_all.nodes; wt = scene().q_all.tris;
+                            if (cached_block_hit()) state = kEndBlock;
                         }
                         break;
                     }
@@ -587,7 +627,11 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveVi
                     t < t_best) {
                     t_best = t; wu = u; wv = v;
                     wbest = __float_as_int(a.w);
-                    if (state == kWalkBlock) { ended = true; break; }
+                    if (state == kWalkBlock) {
+                        if (occluder_cache) occ = ((unsigned long long)(unsigned int)job << 32) | entry;
+                        ended = true;
+                        break;
+                    }
                 }
             }
             if (!ended) {
@@ -932,10 +976,11 @@ static cudaError_t run_pipeline(const dev::DevScene& S0, const dev::WaveView& V,
         if (!refill)
             dev::wave_shadow<F, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V);
         else if (smem)
-            dev::wave_shadow_refill<F, true, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V, tu.refill_min, tu.inner_min);
+            dev::wave_shadow_refill<F, true, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V, tu.refill_min, tu.inner_min,
+                                                                                 tu.shadow_cache);
         else
             dev::wave_shadow_refill<F, false, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V, tu.refill_min,
-                                                                                  tu.inner_min);
+                                                                                  tu.inner_min, tu.shadow_cache);
     };
     int mark = 0;
     auto stage_end = [&]() {
@@ -1131,12 +1176,25 @@ static bool simple_scene(const DeviceScene& s) {
            sv.csg_root < 0;
 }
 
+// Small frames run on the BVH4 megakernel: below wave.mega_samples samples
+// (a quarter of that for scenes with triangles, whose megakernel carries the
+// BVH4 walks and falls behind sooner) the fixed cost of the queue stages --
+// eight launches, each a full-GPU persistent grid, and the slot traffic --
+// outweighs the megakernel's divergence.  Same queries and shading; the
+// image agrees with the queue pipeline's to the last bits of the float
+// arithmetic.
+static bool small_frame(const DeviceScene& s, long long nsamples) {
+    const long long m = tuning().mega_samples;
+    return m > 0 && nsamples <= (s.view.num_tris > 0 ? m / 4 : m);
+}
+
 cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
                              bool count_nodes) {
     if (!wave_supported(s) || count_nodes) return launch_mega_bvh4(s, W, H, aa, rg, out, stream, count_nodes);
     const int ns = clamp_spp(aa);
     const long long nsamples = region_padded(rg) * ns;
     if (nsamples > (1ll << 30)) return cudaErrorInvalidValue;
+    if (small_frame(s, nsamples)) return launch_mega_bvh4(s, W, H, aa, rg, out, stream, false);
     cudaError_t e = wave_reserve_into(s.wave, s.view.num_lights, nsamples, s.device);
     if (e != cudaSuccess) return e;
     Wave* w = s.wave;
@@ -1341,6 +1399,7 @@ cudaError_t launch_wavefront_scratch(DeviceScene& s, void* scratch, size_t scrat
     const int ns = clamp_spp(aa);
     const long long nsamples = region_padded(rg) * ns;
     if (nsamples > (1ll << 30)) return cudaErrorInvalidValue;
+    if (small_frame(s, nsamples)) return launch_mega_bvh4(s, W, H, aa, rg, out, stream, false, tally);
     Wave w;
     if (!wave_carve(w, scratch, scratch_bytes, s.view.num_lights, nsamples)) return cudaErrorInvalidValue;
     const dev::WaveView V = make_view(s, w, W, H, ns, rg);

@@ -38,6 +38,8 @@ const Key kKeys[] = {
     {"camera.centered", &Tuning::aa_centered, 0, 1},
     {"trace.se_polish", &Tuning::se_polish, 0, 1},
     {"caustic.knn", &Tuning::caustic_knn, 0, 64},
+    {"wave.mega_samples", &Tuning::mega_samples, 0, 1 << 30},
+    {"wave.shadow_cache", &Tuning::shadow_cache, 0, 1},
 };
 
 }  // namespace
