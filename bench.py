@@ -179,7 +179,8 @@ def make_scene(args):
     import sheen_b200 as sb
     global W, H, SPP
     photons = args.photons if args.photons > 0 else (4000000 if args.config == 3 else 0)
-    scene = sb.generate_scene(args.config, args.seed, args.detail if args.config == 1 else 0, photons)
+    scene = sb.generate_scene(args.config, args.seed, args.detail if args.config == 1 else 0, photons,
+                              extended=args.extended)
     st = scene.settings
     W, H, SPP = st["width"], st["height"], st["aa"]
     # smaller frames of the same scene (profiling captures)
@@ -202,8 +203,38 @@ def run_ours(args):
     sb.init(local, 100)
     form = sb.FORM_WAVEFRONT if args.form == "wavefront" else sb.FORM_PLAIN
     scene = make_scene(args)
+
+    # End to end through the drop-in call: host scene arrays in, host RGBA
+    # out, per step: BVH build + scene upload + render + read back.  Run
+    # before the resident scene below exists: a one-call render next to a
+    # resident scene and its frame queues was measured 5-20 ms slower a call
+    # (the library's memory pool then serves two working sets), which is not
+    # the drop-in caller's situation.
+    # (scenes with extensions: sheen_scene_create_ext + render to a host
+    # buffer + destroy, the extension's public path)
+    img = np.empty((H, W, 4), np.float32)
+    e2e_steps = max(1, min(args.steps, 3))
+
+    def one_call():
+        if not args.extended:
+            return sb.render_rgba(scene, W, H, SPP, form)
+        d = sb.DeviceScene(scene, form, ext=True)
+        out_img, out_st = d.render_host(W, H, SPP)
+        d.close()
+        return out_img, out_st
+
+    # warm-up calls: the library's memory pool grows to its working set over
+    # the first one or two calls (measured: 80 ms builds, then 13.5 ms)
+    for _ in range(max(1, args.warmup)):
+        one_call()
+    barrier(world)
     t0 = time.perf_counter()
-    ds = sb.DeviceScene(scene, form)
+    for _ in range(e2e_steps):
+        img, st2 = one_call()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+
+    t0 = time.perf_counter()
+    ds = sb.DeviceScene(scene, form, ext=args.extended)
     create_s = time.perf_counter() - t0
     out = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # > 126 MB L2
@@ -247,20 +278,6 @@ def run_ours(args):
     ms = max_over_ranks(ms, world)
     frame_ms = ms / args.steps
     value = rays * args.steps * world / (ms / 1e3) / 1e6
-
-    # end to end through the drop-in call: host scene arrays in, host RGBA
-    # out, per step: BVH build + scene upload + render + read back
-    img = np.empty((H, W, 4), np.float32)
-    e2e_steps = max(1, min(args.steps, 3))
-    # warm-up calls: the library's memory pool grows to its working set over
-    # the first one or two calls (measured: 80 ms builds, then 13.5 ms)
-    for _ in range(max(1, args.warmup)):
-        sb.render_rgba(scene, W, H, SPP, form)
-    barrier(world)
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        img, st2 = sb.render_rgba(scene, W, H, SPP, form)
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     e2e = rays * e2e_steps * world / e2e_s / 1e6
 
     # The metric's denominator: the plain FP32 form (the drop-in) on the same
@@ -304,7 +321,11 @@ def run_ours(args):
     # 16 B hit out per ray, the node record per node visited, 48 B per
     # triangle tested; 14 FP32 ops per box test (a BVH4 node visit tests 4
     # boxes; the plain form counts single boxes), 35 per triangle test.
-    b_node, boxes_per_visit = (32, 1) if form == sb.FORM_PLAIN else (64, 4)
+    # the wavefront form's node counter counts 4-wide BVH4 node visits on
+    # triangle scenes and single boxes of the per-class binary trees on the
+    # others (the workloads do not mix triangles with those classes)
+    wide = form == sb.FORM_WAVEFRONT and scene.view.num_triangles > 0
+    b_node, boxes_per_visit = (64, 4) if wide else (32, 1)
     bytes_alg = rays * 48 + nodes * b_node + prims * 48
     fp32_flops = nodes * boxes_per_visit * 14 + prims * 35
     frame_roof = {"achieved_gbs": round(bytes_alg / (frame_ms / 1e3) / 1e9, 1),
@@ -318,7 +339,8 @@ def run_ours(args):
     # counting megakernel's shadow-query counters (same walks).  Plain: the
     # single megakernel launch, timed above.
     stages = None
-    if form == sb.FORM_WAVEFRONT:
+    mega = form == sb.FORM_WAVEFRONT and uses_megakernel(scene, W, H, SPP)
+    if form == sb.FORM_WAVEFRONT and not mega:
         profs = []
         for i in range(max(3, args.steps // 2)):
             flush.fill_(float(i))
@@ -333,7 +355,7 @@ def run_ours(args):
         k_ms = stages["shadow_ms"]
         k_rays, k_nodes, k_prims = stn["shadow_rays"], stn["shadow_node_visits"], stn["shadow_prim_tests"]
     else:
-        k_name, k_launches, k_ms = "plain_kernel", 1, frame_ms
+        k_name, k_launches, k_ms = ("mega_bvh4_kernel (small frame)" if mega else "plain_kernel"), 1, frame_ms
         k_rays, k_nodes, k_prims = rays, nodes, prims
     k_bytes = k_rays * 48 + k_nodes * b_node + k_prims * 48
     k_flops = k_nodes * boxes_per_visit * 14 + k_prims * 35
@@ -353,6 +375,7 @@ def run_ours(args):
                    "triangles": scene.view.num_triangles, "width": W, "height": H, "spp": SPP,
                    "form": args.form, "parallelism": f"replicas{world}",
                    "frame": (f"{args.tiles} uneven tiles in one batched pass" if args.tiles > 0
+                             else "whole frame, one megakernel launch (small frame)" if mega
                              else "whole frame, captured CUDA graph"),
                    "l2": "256 MB buffer written between timed frames; scene arrays exceed L2",
                    "rays_per_frame": rays, "box_tests_per_frame": nodes, "prim_tests_per_frame": prims,
@@ -361,7 +384,9 @@ def run_ours(args):
         "e2e": {"value": round(e2e, 2), "unit": "Mrays/s",
                 "h2d_bytes_per_step": int(st2["upload_bytes"]),
                 "d2h_bytes_per_step": W * H * 16,
-                "call": "sheen_render_scene_rgba (upload + BVH build + render + readback)",
+                "call": ("sheen_scene_create_ext + sheen_scene_render_host + destroy (upload + BVH build + render "
+                         "+ readback)" if args.extended else
+                         "sheen_render_scene_rgba (upload + BVH build + render + readback)"),
                 "scene_build_ms": round(st2["build_ms"], 1), "scene_upload_ms": round(st2["upload_ms"], 1)},
         "roofline": {"bound": "hbm" if hbm_bound else "fp32", "achieved": round(k_gbs, 1), "peak": pk["hbm_gbs"],
                      "unit": "GB/s", "frac": round(k_gbs / pk["hbm_gbs"], 4), "traffic": traffic,
@@ -372,7 +397,7 @@ def run_ours(args):
                               "frac": round(k_tflops * 1e12 / fp32_peak, 4)},
                      "frame": frame_roof},
         "stages": stages,
-        "gpu_launches": args.steps * launches_per_frame(form),
+        "gpu_launches": args.steps * (1 if mega else launches_per_frame(form)),
         "clocks": clocks,
     }
     if plain is not None:
@@ -410,6 +435,17 @@ def uneven_tiles(W, H, n, seed):
         xs = [0] + np.sort(rng.choice(np.arange(1, W), cols[r] - 1, replace=False)).tolist() + [W]
         tiles += [(xs[c], ys[r], xs[c + 1], ys[r + 1]) for c in range(cols[r])]
     return tiles
+
+
+def uses_megakernel(scene, W, H, spp):
+    """The library's small-frame rule (wave.mega_samples): a frame of at most
+    that many samples -- pixels padded to whole 16x8 tiles, times spp; a
+    quarter of it for scenes with triangles -- runs on the BVH4 megakernel."""
+    import sheen_b200 as sb
+    m = sb.tune_get("wave.mega_samples")
+    samples = ((W + 15) // 16 * 16) * ((H + 7) // 8 * 8) * max(1, min(spp, 64))
+    limit = m // 4 if scene.view.num_triangles > 0 else m
+    return m > 0 and samples <= limit
 
 
 def launches_per_frame(form):
@@ -694,6 +730,37 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+CAPTURE_CASES = {
+    # name: (generator config, detail, photons, width, height, spp, form, small-frame switch on)
+    "wave": (1, 8, 0, 640, 360, 4, "wavefront", False),
+    "plain": (1, 8, 0, 640, 360, 4, "plain", False),
+    "mega": (0, 0, 0, 640, 480, 1, "wavefront", True),
+    "photon": (3, 0, 1000000, 320, 180, 1, "wavefront", True),
+}
+
+
+def run_capture(name):
+    """One small frame of a named case, for profiler captures (ncu -k ...):
+    wave / plain: the mesh workload at 640x360 4 spp through the queue stages
+    or the plain form; mega: the spheres workload at 640x480 1 spp (the
+    small-frame megakernel); photon: the caustics workload with 1M photons
+    per light (its scene build runs the photon emission)."""
+    import torch
+
+    import sheen_b200 as sb
+    cfg, detail, photons, w, h, spp, form, mega = CAPTURE_CASES[name]
+    sb.init(0, 100)
+    if not mega:
+        sb.tune_set("wave.mega_samples", 0)
+    ds = sb.DeviceScene(sb.generate_scene(cfg, 1, detail, photons),
+                        sb.FORM_WAVEFRONT if form == "wavefront" else sb.FORM_PLAIN)
+    out = torch.empty((h, w, 4), dtype=torch.float32, device="cuda")
+    ds.render_device(w, h, spp, out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    print(json.dumps({"capture": name, "mean": float(out[..., :3].mean())}))
+    ds.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -721,9 +788,23 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=64,
                     help="requests of the short serving run in the default bench line (0: skip)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form denominator")
+    ap.add_argument("--extended", action="store_true",
+                    help="config 2 with its extension column (exact Bezier lathes and prisms, two-exponent "
+                         "superellipsoids, FP32 height grid, 128 CSG trees); the reference has none of these, "
+                         "so the line carries no reference or host-array legs")
+    ap.add_argument("--capture", choices=sorted(CAPTURE_CASES),
+                    help="render one small frame of a named case and exit (for profiler captures)")
     args = ap.parse_args()
+    if args.capture:
+        run_capture(args.capture)
+        return
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
+    if args.extended:
+        if args.config != 2:
+            ap.error("--extended applies to --config 2")
+        args.no_cpu = args.no_ref_gpu = args.no_plain = True
+        args.serve_requests = 0
     if args.tune:
         import sheen_b200 as sb
         for kv in args.tune:

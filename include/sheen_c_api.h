@@ -160,6 +160,91 @@ int sheen_render_scene_rgba(const SheenScene* scene, int width, int height,
 typedef struct SheenDeviceScene_* SheenDeviceScene;
 int  sheen_scene_create(const SheenScene* scene, int form, SheenDeviceScene* out);
 void sheen_scene_destroy(SheenDeviceScene scene);
+
+/* ------------------------------------------------------------------ */
+/* Scene extensions.  No counterpart in the reference: shapes its       */
+/* renderer does not have (the benchmark workloads' extension columns:  */
+/* exact Bezier surfaces, two-exponent superellipsoids, FP32 height     */
+/* grids, forests of CSG trees with box and cone leaves).  Every field  */
+/* is optional: a zero-filled SheenSceneExt renders exactly what        */
+/* sheen_scene_create renders.                                          */
+/* ------------------------------------------------------------------ */
+
+/* ctrl_count control points starting at ctrl_offset, cubic Bezier spans of
+ * four points each (the layout of the .sheen lathe_bezier / prism_bezier
+ * commands, api/scene_io.cpp:86-102, 791-819); 0 points: no extension. */
+typedef struct SheenBezierRun {
+    int ctrl_offset;
+    int ctrl_count;
+} SheenBezierRun;
+
+/* Solid leaves of extension CSG trees (CSGNode.leaf_kind 2 and 3). */
+typedef struct SheenCsgBox {        /* axis-aligned box */
+    sheen_float3 lo;
+    sheen_float3 hi;
+    int material_id;
+    int _pad0;
+} SheenCsgBox;
+
+typedef struct SheenCsgCone {       /* capped cone (frustum) from p0 (radius r0) to p1 (radius r1) */
+    sheen_float3 p0;
+    float r0;
+    sheen_float3 p1;
+    float r1;
+    int material_id;
+    int _pad0, _pad1, _pad2;
+} SheenCsgCone;
+
+typedef struct SheenHeightGrid {    /* w x h FP32 heights in [0, 1], row-major, rows along z */
+    int offset;                     /* first value in SheenSceneExt.hf_heights; < 0: none */
+    int w, h;
+} SheenHeightGrid;
+
+typedef struct SheenSceneExt {
+    /* Exact cubic-Bezier surfaces, replacing the tessellation the reference
+     * renders (its loader turns Bezier profiles into polylines on the
+     * host).  lathe_bezier[i] (num_lathes entries, or NULL): lathe i's
+     * profile as control points (y, radius), turned about the world Y axis
+     * like the tessellated lathe (whose test ignores Lathe.center).
+     * prism_bezier[i] (num_prisms entries, or NULL): prism i's closed
+     * contour as control points (x, z) about the prism's centre, extruded
+     * over [y_min, y_max].  Control points are (a, b) pairs in bezier_ctrl.
+     * The ray-surface roots (a sextic per lathe span, cubics for prism walls
+     * and cap contours) are isolated in FP64 on the GPU; everything else
+     * stays FP32. */
+    const SheenBezierRun* lathe_bezier;
+    const SheenBezierRun* prism_bezier;
+    const float* bezier_ctrl;
+    int num_bezier_ctrl;               /* pairs */
+    /* Two-exponent superellipsoids: se_n2[i] > 0 (num_superellipsoids
+     * entries, or NULL) gives superellipsoid i the surface
+     * (|x/a|^n + |z/c|^n)^(n2/n) + |y/b|^n2 = 1 (n = Superellipsoid.n: the
+     * east-west exponent, n2 the north-south one; n2 == n is the
+     * reference's single-exponent body), tested with the reference's march
+     * and bisection. */
+    const float* se_n2;
+    /* FP32 height grids: hf_grid[i] (num_heightfields entries, or NULL)
+     * replaces heightfield i's procedural or 8-bit height with a bilinear
+     * FP32 grid spanning its size_x x size_z footprint, scaled by
+     * HeightField.height. */
+    const SheenHeightGrid* hf_grid;
+    const float* hf_heights;
+    int num_hf_heights;
+    /* CSG forest: further tree roots beside SheenScene.csg_root (closest
+     * hit over all trees), and the box / cone leaves their CSGNode records
+     * name with leaf_kind 2 / 3 (leaf_index into these arrays).  A tree
+     * keeps the reference's rules (8 intervals per node). */
+    const int* csg_roots;
+    int num_csg_roots;
+    const SheenCsgBox* csg_boxes;
+    int num_csg_boxes;
+    const SheenCsgCone* csg_cones;
+    int num_csg_cones;
+} SheenSceneExt;
+
+/* sheen_scene_create with extensions (ext may be NULL).  Fails with a
+ * message when an extension array names something out of range. */
+int  sheen_scene_create_ext(const SheenScene* scene, const SheenSceneExt* ext, int form, SheenDeviceScene* out);
 unsigned long long sheen_scene_device_bytes(SheenDeviceScene scene);
 int  sheen_scene_form(SheenDeviceScene scene);
 
@@ -194,8 +279,9 @@ int sheen_scene_render_region(SheenDeviceScene scene, int width, int height, int
  * until exit).  Nothing is allocated and nothing is synchronised.
  *
  * Limits: at most 16384 samples per call (the rectangle's pixels rounded up
- * to whole 16x8 tiles, times aa_samples -- e.g. 128x128 at 1 spp or 64x64 at
- * 4 spp) and at most 8 lights; larger requests fail with -1 and a message.
+ * to whole tiles of 128 pixels, 16x8 unless "wave.tile_w" says otherwise,
+ * times aa_samples -- e.g. 128x128 at 1 spp or 64x64 at 4 spp) and at most
+ * 8 lights; larger requests fail with -1 and a message.
  * The first call on each device (and the first after sheen_cleanup) looks up
  * the array's device address; make that call before any stream capture.
  * Each call clears the queue counters it starts from; the rest of the array
@@ -368,15 +454,20 @@ typedef struct SheenTuneResult {
     double default_ms;                                     /* frame time with the setting in force before */
     int shadow_stack;                                      /* the setting kept: wave.shadow_stack */
     int inner_min;                                         /* the setting kept: wave.inner_min */
+    int tile_w;                                            /* the setting kept: wave.tile_w */
+    int mega_samples;                                      /* the setting kept: wave.mega_samples */
 } SheenTuneResult;
 
-/* Autotuner: times candidate launch parameters (both shadow-stage variants,
- * refill thresholds 8/16/24, inner-phase thresholds 0/6/10/14, shadow
- * blocks per SM, traversal stack in local or shared memory) on a resident
+/* Autotuner: times candidate launch parameters on a resident
  * SHEEN_FORM_WAVEFRONT scene for one frame shape -- per candidate one
  * warm-up frame, then `reps` frames timed with CUDA events -- and keeps the
- * fastest (process-wide, as sheen_tune_set).  Renders into a device buffer it
- * allocates and frees; synchronous.  0 / -1. */
+ * fastest (process-wide, as sheen_tune_set).  First the shadow stage (both
+ * variants, refill thresholds 8/16/24, inner-phase thresholds 0/6/10/14,
+ * shadow blocks per SM, traversal stack in local or shared memory), then,
+ * with the best of those, the pixel tile of the sample order (8x16, 16x8,
+ * 32x4) and the small-frame switch (queue stages or the BVH4 megakernel for
+ * this frame).  Renders into a device buffer it allocates and frees;
+ * synchronous.  0 / -1. */
 int sheen_autotune(SheenDeviceScene scene, int width, int height, int aa_samples, int reps,
                    SheenTuneResult* out);
 
@@ -415,6 +506,21 @@ void sheen_owned_free(SheenOwnedScene scene);
  * the others it is ignored unless > 0 where noted. */
 int sheen_generate_scene(int config, unsigned int seed, int detail, int photons,
                          SheenOwnedScene* out);
+
+/* The workload generators with their extension column (no counterpart in
+ * the reference).  extended != 0, config 2: the same scene with
+ * two-exponent superellipsoids (both exponents 2/e, e uniform in [0.2, 3]),
+ * the lathes' and prisms' Bezier control points as exact surfaces, a
+ * 1024 x 1024 FP32 height grid (heights in [0, 2]) for the heightfield, and
+ * 128 further CSG trees of depth 3 over spheres, boxes and cones.  The
+ * extensions are read with sheen_owned_ext() and passed to
+ * sheen_scene_create_ext(); the SheenScene view alone is the reference's
+ * scene.  Other configs: extended must be 0. */
+int sheen_generate_scene_ext(int config, unsigned int seed, int detail, int photons, int extended,
+                             SheenOwnedScene* out);
+
+/* The extension arrays of an owned scene (zero-filled when it has none). */
+const SheenSceneExt* sheen_owned_ext(SheenOwnedScene scene);
 
 /* 8-bit sRGB PNG writer used by sheen_render_scene (png_color.h:11-20 conversion). */
 int sheen_write_png_srgb(const char* path, const float* rgba, int width, int height);

@@ -122,6 +122,17 @@ struct OracleScene {
     int nph; int* cell_start; int* cell_count; int num_cells; real cell;
     int centered;                       /* samples without jitter (extension) */
     int knn;                            /* k-nearest-photon gather (extension; 0: the reference's) */
+    /* scene extensions (SheenSceneExt); NULL / 0 when absent */
+    float* se_n2;                       /* per superellipsoid: north-south exponent (> 0: two-exponent) */
+    int* hfg;                           /* per heightfield: offset (< 0 none), w, h */
+    float* hf_heights;
+    int* lathe_run;                     /* per lathe: first span, spans */
+    int* prism_run;                     /* per prism */
+    double* spans;                      /* 8 per cubic span: a0 b0 a1 b1 a2 b2 a3 b3 */
+    int nspans;
+    int* csg_roots; int ncsg_roots;
+    SheenCsgBox* csg_boxes; int ncsg_boxes;
+    SheenCsgCone* csg_cones; int ncsg_cones;
 };
 
 static void sample_pos(const OracleScene* S, int s, int n, int x, int y, real* ox, real* oy) {
@@ -520,14 +531,24 @@ static void prism_box(const Prism* p, const PrismPoint* pts, V* lo, V* hi) {
 /* ------------------------------------------------------------------ */
 /* primitives/superellipsoid.h:12-161                                  */
 /* ------------------------------------------------------------------ */
-static real se_f(const Superellipsoid* s, V p) {
+/* n2 > 0 (extension, no counterpart in the reference): the two-exponent
+ * body (|qx|^n + |qz|^n)^(n2/n) + |qy|^n2. */
+static real se_f(const Superellipsoid* s, V p, real n2) {
     real qx = (p.x - s->center.x) / s->a, qy = (p.y - s->center.y) / s->b, qz = (p.z - s->center.z) / s->c;
+    if (n2 > 0) return rpow(rpow(fabs(qx), s->n) + rpow(fabs(qz), s->n), n2 / s->n) + rpow(fabs(qy), n2);
     return rpow(fabs(qx), s->n) + rpow(fabs(qy), s->n) + rpow(fabs(qz), s->n);
 }
 
-static V se_grad(const Superellipsoid* s, V p) {
+static V se_grad(const Superellipsoid* s, V p, real n2) {
     real qx = (p.x - s->center.x) / s->a, qy = (p.y - s->center.y) / s->b, qz = (p.z - s->center.z) / s->c;
     real n = s->n;
+    if (n2 > 0) {
+        real xz = rpow(fabs(qx), n) + rpow(fabs(qz), n);
+        real k = xz > 0 ? n2 * rpow(xz, n2 / n - 1) : 0;
+        return v3(k * rpow(fabs(qx), n - 1) * (qx >= 0 ? 1 : -1) / s->a,
+                  n2 * rpow(fabs(qy), n2 - 1) * (qy >= 0 ? 1 : -1) / s->b,
+                  k * rpow(fabs(qz), n - 1) * (qz >= 0 ? 1 : -1) / s->c);
+    }
     return v3(n * rpow(fabs(qx), n - 1) * (qx >= 0 ? 1 : -1) / s->a,
               n * rpow(fabs(qy), n - 1) * (qy >= 0 ? 1 : -1) / s->b,
               n * rpow(fabs(qz), n - 1) * (qz >= 0 ? 1 : -1) / s->c);
@@ -551,7 +572,7 @@ static int se_clip(const Ray* r, const Superellipsoid* s, real* tA, real* tB) {
 /* superellipsoid.h:41-117.  QUIRK: on an outside->inside crossing the
  * bisection runs on [t, t] (t_prev was already advanced), so the entry point
  * is the sample itself. */
-static int se_intervals(const Ray* r, const Superellipsoid* s, real t0, real t1, real* te, real* tx) {
+static int se_intervals(const Ray* r, const Superellipsoid* s, real t0, real t1, real* te, real* tx, real n2) {
     real tA, tB;
     se_clip(r, s, &tA, &tB);
     if (tB < t0 || tA > t1 || tB < tA) return 0;
@@ -561,18 +582,18 @@ static int se_intervals(const Ray* r, const Superellipsoid* s, real t0, real t1,
     const int NS = 32;
     real step = (t1 - t0) / (real)NS;
     real tp = t0;
-    real Fp = se_f(s, add(r->o, mul(r->d, tp)));
+    real Fp = se_f(s, add(r->o, mul(r->d, tp)), n2);
     int inside = Fp <= EPS, fe = 0, fx = 0;
     *te = R(-1e30); *tx = R(-1e30);
     if (inside) { *te = t0; fe = 1; }
     for (int i = 1; i <= NS && !fx; i++) {
         real t = rfmin(t0 + step * (real)i, t1);
-        real F = se_f(s, add(r->o, mul(r->d, t)));
+        real F = se_f(s, add(r->o, mul(r->d, t)), n2);
         if (inside && F > EPS) {
             real lo = tp, hi = t;
             for (int b = 0; b < 20; b++) {
                 real mid = R(0.5) * (lo + hi);
-                if (se_f(s, add(r->o, mul(r->d, mid))) > EPS) hi = mid; else lo = mid;
+                if (se_f(s, add(r->o, mul(r->d, mid)), n2) > EPS) hi = mid; else lo = mid;
             }
             *tx = R(0.5) * (lo + hi);
             if (*tx > t1) *tx = t1;
@@ -585,7 +606,7 @@ static int se_intervals(const Ray* r, const Superellipsoid* s, real t0, real t1,
             real lo = tp, hi = t;
             for (int b = 0; b < 20; b++) {
                 real mid = R(0.5) * (lo + hi);
-                if (se_f(s, add(r->o, mul(r->d, mid))) <= EPS) hi = mid; else lo = mid;
+                if (se_f(s, add(r->o, mul(r->d, mid)), n2) <= EPS) hi = mid; else lo = mid;
             }
             *te = R(0.5) * (lo + hi);
             if (*te < t0) *te = t0;
@@ -599,17 +620,17 @@ static int se_intervals(const Ray* r, const Superellipsoid* s, real t0, real t1,
     return *te <= *tx;
 }
 
-static int se_hit(const Ray* r, const Superellipsoid* s, Hit* h) {
+static int se_hit(const Ray* r, const Superellipsoid* s, Hit* h, real n2) {
     real t0, t1;
     se_clip(r, s, &t0, &t1);
     if (t1 < r->tmin || t0 > r->tmax || t1 < t0) return 0;
     t0 = rfmax(t0, r->tmin);
     t1 = rfmin(t1, r->tmax);
     real te, tx;
-    if (!se_intervals(r, s, t0, t1, &te, &tx)) return 0;
+    if (!se_intervals(r, s, t0, t1, &te, &tx, n2)) return 0;
     h->t = te;
     h->p = add(r->o, mul(r->d, te));
-    h->n = nrm(se_grad(s, h->p));
+    h->n = nrm(se_grad(s, h->p, n2));
     h->tan = v3(1, 0, 0);
     h->u = h->p.x; h->v = h->p.y;
     if (dot(h->n, r->d) > 0) h->n = neg(h->n);
@@ -648,10 +669,25 @@ static real hf_fbm(real x, real z, real freq, int octaves, int seed) {
     return sum / nrmz;
 }
 
-static real hf_eval(const HeightField* hf, const unsigned char* img, real x, real z) {
+/* grid (extension): gw x gh FP32 heights in [0, 1], bilinear over the
+ * footprint, scaled by height; replaces the procedural / 8-bit height. */
+typedef struct { const float* h; int w, hgt; } Grid;
+
+static real hf_eval(const HeightField* hf, const unsigned char* img, real x, real z, Grid g) {
     real lx = (x - hf->center.x) / hf->size_x + R(0.5);
     real lz = (z - hf->center.z) / hf->size_z + R(0.5);
     if (lx < 0 || lx > 1 || lz < 0 || lz > 1) return 0;
+    if (g.h) {
+        real fu = lx * (real)(g.w - 1), fvv = lz * (real)(g.hgt - 1);
+        int u0 = (int)fu, v0 = (int)fvv;
+        int u1 = u0 < g.w - 1 ? u0 + 1 : u0, v1 = v0 < g.hgt - 1 ? v0 + 1 : v0;
+        real tx = fu - (real)u0, ty = fvv - (real)v0;
+#define GV(u, v) ((real)g.h[(size_t)(v) * g.w + (u)])
+        real hh = GV(u0, v0) * (1 - tx) * (1 - ty) + GV(u1, v0) * tx * (1 - ty) + GV(u0, v1) * (1 - tx) * ty +
+                  GV(u1, v1) * tx * ty;
+#undef GV
+        return hh * hf->height;
+    }
     if (img) {
         if (hf->img_w < 1 || hf->img_h < 1) return 0;
         real fu = lx * (real)(hf->img_w - 1), fvv = lz * (real)(hf->img_h - 1);
@@ -670,7 +706,7 @@ static real hf_eval(const HeightField* hf, const unsigned char* img, real x, rea
     return t * hf->height;
 }
 
-static int hf_hit(const Ray* r, const HeightField* hf, const unsigned char* img, Hit* h) {
+static int hf_hit(const Ray* r, const HeightField* hf, const unsigned char* img, Hit* h, Grid g) {
     V lo = v3(R(hf->center.x) - R(0.5) * hf->size_x, hf->center.y, R(hf->center.z) - R(0.5) * hf->size_z);
     V hi = v3(R(hf->center.x) + R(0.5) * hf->size_x, R(hf->center.y) + hf->height, R(hf->center.z) + R(0.5) * hf->size_z);
     real ix = R(1) / r->d.x, iy = R(1) / r->d.y, iz = R(1) / r->d.z;
@@ -690,7 +726,7 @@ static int hf_hit(const Ray* r, const HeightField* hf, const unsigned char* img,
     int inside = 0;
     for (int i = 0; i < 256; i++) {
         V p = add(r->o, mul(r->d, t));
-        real hg = hf_eval(hf, img, p.x, p.z) + hf->center.y;
+        real hg = hf_eval(hf, img, p.x, p.z, g) + hf->center.y;
         int iyy = p.y <= hg;
         if (iyy != inside) {
             real a = t - step, b = t;
@@ -698,7 +734,7 @@ static int hf_hit(const Ray* r, const HeightField* hf, const unsigned char* img,
             for (int k = 0; k < 10; k++) {
                 real mid = R(0.5) * (a + b);
                 V pm = add(r->o, mul(r->d, mid));
-                real hm = hf_eval(hf, img, pm.x, pm.z) + hf->center.y;
+                real hm = hf_eval(hf, img, pm.x, pm.z, g) + hf->center.y;
                 if ((pm.y <= hm) == iyy) b = mid; else a = mid;
             }
             real tt = R(0.5) * (a + b);
@@ -707,8 +743,8 @@ static int hf_hit(const Ray* r, const HeightField* hf, const unsigned char* img,
                 h->t = tt;
                 h->p = P;
                 real e = rfmax(hf->size_x, hf->size_z) / R(256);
-                real hxp = hf_eval(hf, img, P.x + e, P.z), hxm = hf_eval(hf, img, P.x - e, P.z);
-                real hzp = hf_eval(hf, img, P.x, P.z + e), hzm = hf_eval(hf, img, P.x, P.z - e);
+                real hxp = hf_eval(hf, img, P.x + e, P.z, g), hxm = hf_eval(hf, img, P.x - e, P.z, g);
+                real hzp = hf_eval(hf, img, P.x, P.z + e, g), hzm = hf_eval(hf, img, P.x, P.z - e, g);
                 h->n = nrm(v3(-(hxp - hxm) / (R(2) * e), 1, -(hzp - hzm) / (R(2) * e)));
                 h->tan = v3(1, 0, 0);
                 h->u = P.x; h->v = P.z;
@@ -727,6 +763,285 @@ static int hf_hit(const Ray* r, const HeightField* hf, const unsigned char* img,
 /* ------------------------------------------------------------------ */
 /* integrator/csg.h:22-186 -- interval CSG, 8 intervals per node        */
 /* ------------------------------------------------------------------ */
+/* ------------------------------------------------------------------ */
+/* Extension: exact cubic-Bezier lathes and prisms (no counterpart in the */
+/* reference, which tessellates Bezier profiles on the host,             */
+/* api/scene_io.cpp:86-102, 791-819).  Independent of the library's      */
+/* Bernstein root isolation: each span's polynomial is evaluated directly */
+/* at 4096 points and every sign change bisected to the last bit, in      */
+/* double whatever the build's precision.                                 */
+/* ------------------------------------------------------------------ */
+static double bz(const double* c, double u) {
+    double v = 1.0 - u;
+    return v * v * v * c[0] + 3.0 * v * v * u * c[1] + 3.0 * v * u * u * c[2] + u * u * u * c[3];
+}
+static double bzd(const double* c, double u) {
+    double v = 1.0 - u;
+    return 3.0 * (v * v * (c[1] - c[0]) + 2.0 * v * u * (c[2] - c[1]) + u * u * (c[3] - c[2]));
+}
+static void span_ab(const OracleScene* S, int k, double a[4], double b[4]) {
+    const double* q = S->spans + 8 * (size_t)k;
+    for (int i = 0; i < 4; i++) { a[i] = q[2 * i]; b[i] = q[2 * i + 1]; }
+}
+
+/* Sign-change roots in [0, 1) of f (sampled at n points, bisected). */
+typedef double (*ufun)(const void* ctx, double u);
+static int sampled_roots(ufun f, const void* ctx, int n, double* roots, int max_roots) {
+    int nr = 0;
+    double u0 = 0.0, f0 = f(ctx, 0.0);
+    for (int i = 1; i <= n && nr < max_roots; i++) {
+        double u1 = (double)i / n, f1 = f(ctx, u1);
+        if (f0 == 0.0) { roots[nr++] = u0; }
+        else if ((f0 < 0.0) != (f1 < 0.0) && f1 != 0.0) {
+            double lo = u0, hi = u1, flo = f0;
+            for (int k = 0; k < 80 && hi - lo > 0.0; k++) {
+                double mid = 0.5 * (lo + hi);
+                if (mid <= lo || mid >= hi) break;
+                double fm = f(ctx, mid);
+                if ((fm < 0.0) == (flo < 0.0)) { lo = mid; flo = fm; } else hi = mid;
+            }
+            roots[nr++] = 0.5 * (lo + hi);
+        }
+        u0 = u1; f0 = f1;
+    }
+    return nr;
+}
+
+typedef struct { double Y[4], Rr[4], A, B, C, dy; } LatheCtx;
+static double lathe_f(const void* c, double u) {
+    const LatheCtx* L = (const LatheCtx*)c;
+    double y = bz(L->Y, u), rr = bz(L->Rr, u);
+    return L->A * y * y + L->B * L->dy * y + L->C * L->dy * L->dy - L->dy * L->dy * rr * rr;
+}
+static double cubic_f(const void* c, double u) { return bz((const double*)c, u); }
+
+static int lathe_exact_hit(const OracleScene* S, const Ray* r, int i, Hit* h) {
+    const int first = S->lathe_run[2 * i], cnt = S->lathe_run[2 * i + 1];
+    double ox = r->o.x, oy = r->o.y, oz = r->o.z, dx = r->d.x, dy = r->d.y, dz = r->d.z;
+    double A = dx * dx + dz * dz, B = 2 * (ox * dx + oz * dz), C = ox * ox + oz * oz;
+    int flat = dy * dy <= 1e-24 * (A + dy * dy);
+    double best = r->tmax, bu = 0;
+    int bk = -1;
+    for (int k = first; k < first + cnt; k++) {
+        LatheCtx L;
+        span_ab(S, k, L.Y, L.Rr);
+        for (int j = 0; j < 4; j++) L.Y[j] -= oy;
+        double roots[64];
+        if (!flat) {
+            L.A = A; L.B = B; L.C = C; L.dy = dy;
+            int n = sampled_roots(lathe_f, &L, 4096, roots, 64);
+            for (int j = 0; j < n; j++) {
+                double sv = bz(L.Y, roots[j]) / dy;
+                if (sv >= r->tmin && sv < best) { best = sv; bu = roots[j]; bk = k; }
+            }
+        } else {
+            int n = sampled_roots(cubic_f, L.Y, 4096, roots, 64);
+            for (int j = 0; j < n; j++) {
+                double rad = bz(L.Rr, roots[j]), disc = B * B - 4 * A * (C - rad * rad);
+                if (disc < 0 || A <= 0) continue;
+                double sq = sqrt(disc), s0 = (-B - sq) / (2 * A), s1 = (-B + sq) / (2 * A);
+                if (s0 >= r->tmin && s0 < best) { best = s0; bu = roots[j]; bk = k; }
+                else if (s1 >= r->tmin && s1 < best) { best = s1; bu = roots[j]; bk = k; }
+            }
+        }
+    }
+    if (bk < 0 || best > r->tmax) return 0;
+    double Y[4], Rr[4];
+    span_ab(S, bk, Y, Rr);
+    h->t = (real)best;
+    h->p = add(r->o, mul(r->d, h->t));
+    double yd = bzd(Y, bu), rd = bzd(Rr, bu), rv = bz(Rr, bu);
+    double rho = sqrt((double)h->p.x * h->p.x + (double)h->p.z * h->p.z);
+    double cx = rho > 0 ? h->p.x / rho : 1, cz = rho > 0 ? h->p.z / rho : 0;
+    h->n = nrm(v3((real)(yd * cx), (real)(-rd * (rv < 0 ? -1 : 1)), (real)(yd * cz)));
+    if (dot(h->n, r->d) > 0) h->n = neg(h->n);
+    h->tan = v3(0, 1, 0);
+    h->u = 0; h->v = 0;
+    h->mat = S->lathes[i].material_id;
+    return 1;
+}
+
+static void lathe_exact_box(const OracleScene* S, int i, V* lo, V* hi) {
+    const int first = S->lathe_run[2 * i], cnt = S->lathe_run[2 * i + 1];
+    double R = 0, y0 = 1e300, y1 = -1e300;
+    for (int k = first; k < first + cnt; k++)
+        for (int j = 0; j < 4; j++) {
+            const double* q = S->spans + 8 * (size_t)k + 2 * j;
+            y0 = fmin(y0, q[0]); y1 = fmax(y1, q[0]); R = fmax(R, fabs(q[1]));
+        }
+    *lo = v3((real)-R, (real)y0, (real)-R);
+    *hi = v3((real)R, (real)y1, (real)R);
+    widen(lo, hi);
+}
+
+/* even-odd: crossings of z = pz at x > px, u in [0, 1) per span */
+static int bez_inside(const OracleScene* S, int first, int cnt, double px, double pz) {
+    int inside = 0;
+    for (int k = first; k < first + cnt; k++) {
+        double X[4], Z[4], roots[64];
+        span_ab(S, k, X, Z);
+        for (int j = 0; j < 4; j++) Z[j] -= pz;
+        int n = sampled_roots(cubic_f, Z, 4096, roots, 64);
+        for (int j = 0; j < n; j++)
+            if (roots[j] < 1.0 && bz(X, roots[j]) > px) inside = !inside;
+    }
+    return inside;
+}
+
+typedef struct { double X[4], Z[4], ox, oz, dx, dz; } WallCtx;
+static double wall_f(const void* c, double u) {
+    const WallCtx* w = (const WallCtx*)c;
+    return (bz(w->X, u) - w->ox) * w->dz - (bz(w->Z, u) - w->oz) * w->dx;
+}
+
+static int prism_exact_hit(const OracleScene* S, const Ray* r, int i, Hit* h) {
+    const Prism* p = &S->prisms[i];
+    const int first = S->prism_run[2 * i], cnt = S->prism_run[2 * i + 1];
+    double y0 = (double)p->center.y + p->y_min, y1 = (double)p->center.y + p->y_max;
+    double best = r->tmax, bu = 0, capn = 0;
+    int kind = -1, bk = -1;
+    for (int face = 0; face < 2; face++) {
+        double yf = face == 0 ? y0 : y1;
+        double t = (yf - r->o.y) / r->d.y;
+        if (!(t >= r->tmin && t <= r->tmax) || t >= best) continue;
+        double Px = r->o.x + t * r->d.x, Pz = r->o.z + t * r->d.z;
+        if (!bez_inside(S, first, cnt, Px - p->center.x, Pz - p->center.z)) continue;
+        best = t; kind = 0; capn = face == 0 ? -1 : 1;
+    }
+    WallCtx w;
+    w.ox = (double)r->o.x - p->center.x; w.oz = (double)r->o.z - p->center.z; w.dx = r->d.x; w.dz = r->d.z;
+    double a2 = w.dx * w.dx + w.dz * w.dz;
+    if (a2 > 1e-24 * (a2 + (double)r->d.y * r->d.y)) {
+        for (int k = first; k < first + cnt; k++) {
+            double roots[64];
+            span_ab(S, k, w.X, w.Z);
+            int n = sampled_roots(wall_f, &w, 4096, roots, 64);
+            for (int j = 0; j < n; j++) {
+                double sv = ((bz(w.X, roots[j]) - w.ox) * w.dx + (bz(w.Z, roots[j]) - w.oz) * w.dz) / a2;
+                if (!(sv >= r->tmin && sv < best)) continue;
+                double yy = r->o.y + sv * r->d.y;
+                if (yy < y0 - 1e-6 * fabs(y0) - 1e-7 || yy > y1 + 1e-6 * fabs(y1) + 1e-7) continue;
+                best = sv; kind = 1; bu = roots[j]; bk = k;
+            }
+        }
+    }
+    if (kind < 0) return 0;
+    h->t = (real)best;
+    h->p = add(r->o, mul(r->d, h->t));
+    if (kind == 0) { h->n = v3(0, (real)capn, 0); h->tan = v3(1, 0, 0); }
+    else {
+        double X[4], Z[4];
+        span_ab(S, bk, X, Z);
+        h->n = nrm(v3((real)bzd(Z, bu), 0, (real)-bzd(X, bu)));
+        h->tan = v3(0, 1, 0);
+    }
+    if (dot(h->n, r->d) > 0) h->n = neg(h->n);
+    h->u = 0; h->v = 0;
+    h->mat = p->material_id;
+    return 1;
+}
+
+static void prism_exact_box(const OracleScene* S, int i, V* lo, V* hi) {
+    const Prism* p = &S->prisms[i];
+    const int first = S->prism_run[2 * i], cnt = S->prism_run[2 * i + 1];
+    double x0 = 1e300, x1 = -1e300, z0 = 1e300, z1 = -1e300;
+    for (int k = first; k < first + cnt; k++)
+        for (int j = 0; j < 4; j++) {
+            const double* q = S->spans + 8 * (size_t)k + 2 * j;
+            x0 = fmin(x0, q[0]); x1 = fmax(x1, q[0]); z0 = fmin(z0, q[1]); z1 = fmax(z1, q[1]);
+        }
+    *lo = v3((real)(p->center.x + x0), (real)(p->center.y + p->y_min), (real)(p->center.z + z0));
+    *hi = v3((real)(p->center.x + x1), (real)(p->center.y + p->y_max), (real)(p->center.z + z1));
+    widen(lo, hi);
+}
+
+/* Extension CSG leaves: axis-aligned box and capped cone, one interval each
+ * (both convex), clipped to [t0, t1]. */
+static int box_iv(const Ray* r, const SheenCsgBox* b, real t0, real t1, real* te, real* tx) {
+    real lo[3] = {b->lo.x, b->lo.y, b->lo.z}, hi[3] = {b->hi.x, b->hi.y, b->hi.z};
+    real o[3] = {r->o.x, r->o.y, r->o.z}, d[3] = {r->d.x, r->d.y, r->d.z};
+    real tn = R(-1e300), tf = R(1e300);
+    for (int a = 0; a < 3; a++) {
+        if (d[a] == 0) { if (o[a] < lo[a] || o[a] > hi[a]) return 0; continue; }
+        real ta = (lo[a] - o[a]) / d[a], tb = (hi[a] - o[a]) / d[a];
+        if (ta > tb) { real t = ta; ta = tb; tb = t; }
+        tn = rfmax(tn, ta); tf = rfmin(tf, tb);
+    }
+    if (!(tn <= tf) || tf < t0 || tn > t1) return 0;
+    *te = rfmax(tn, t0); *tx = rfmin(tf, t1);
+    return *te <= *tx;
+}
+
+static int cone_iv(const Ray* r, const SheenCsgCone* c, real t0, real t1, real* te, real* tx) {
+    V p0 = v3(c->p0.x, c->p0.y, c->p0.z), ax = sub(v3(c->p1.x, c->p1.y, c->p1.z), p0);
+    real L = sqrt(dot(ax, ax));
+    if (!(L > 0)) return 0;
+    V a = mul(ax, 1 / L), oc = sub(r->o, p0);
+    real ho = dot(oc, a), hd = dot(r->d, a);
+    real sa, sb;
+    if (hd != 0) { sa = -ho / hd; sb = (L - ho) / hd; if (sa > sb) { real t = sa; sa = sb; sb = t; } }
+    else { if (ho < 0 || ho > L) return 0; sa = R(-1e300); sb = R(1e300); }
+    real k = (c->r1 - c->r0) / L, rb = c->r0 + k * ho, rk = k * hd;
+    real A = dot(r->d, r->d) - hd * hd - rk * rk;
+    real B = 2 * (dot(oc, r->d) - ho * hd - rb * rk);
+    real Cc = dot(oc, oc) - ho * ho - rb * rb;
+    real lo = sa, hi = sb;
+    if (fabs(A) <= 1e-12 * (fabs(B) + fabs(Cc) + 1e-300)) {
+        if (B == 0) { if (Cc > 0) return 0; }
+        else if (B > 0) hi = rfmin(hi, -Cc / B);
+        else lo = rfmax(lo, -Cc / B);
+    } else {
+        real disc = B * B - 4 * A * Cc;
+        if (A > 0) {
+            if (disc < 0) return 0;
+            real sq = sqrt(disc);
+            lo = rfmax(lo, (-B - sq) / (2 * A)); hi = rfmin(hi, (-B + sq) / (2 * A));
+        } else if (disc >= 0) {
+            real sq = sqrt(disc), ra = (-B + sq) / (2 * A), rbb = (-B - sq) / (2 * A);
+            real l1 = lo, h1 = rfmin(hi, ra), l2 = rfmax(lo, rbb), h2 = hi;
+            int ok1 = l1 <= h1, ok2 = l2 <= h2;
+            if (ok1 && ok2) {
+                real m1 = R(0.5) * (rfmax(l1, R(-1e30)) + rfmin(h1, R(1e30)));
+                if (c->r0 + k * (ho + m1 * hd) >= 0) hi = h1; else lo = l2;
+            } else if (ok1) hi = h1;
+            else if (ok2) lo = l2;
+            else return 0;
+        }
+    }
+    if (!(lo <= hi) || hi < t0 || lo > t1) return 0;
+    *te = rfmax(lo, t0); *tx = rfmin(hi, t1);
+    return *te <= *tx;
+}
+
+static V csg_ext_normal(const OracleScene* S, int kind, int leaf, V p) {
+    if (kind == 2) {
+        const SheenCsgBox* b = &S->csg_boxes[leaf];
+        real c[3] = {R(0.5) * (b->lo.x + b->hi.x), R(0.5) * (b->lo.y + b->hi.y), R(0.5) * (b->lo.z + b->hi.z)};
+        real e[3] = {R(0.5) * (b->hi.x - b->lo.x), R(0.5) * (b->hi.y - b->lo.y), R(0.5) * (b->hi.z - b->lo.z)};
+        real q[3] = {p.x - c[0], p.y - c[1], p.z - c[2]};
+        int best = 0; real bd = R(1e300);
+        for (int a = 0; a < 3; a++) {
+            real dd = fabs(e[a] - fabs(q[a])) / rfmax(e[a], R(1e-30));
+            if (dd < bd) { bd = dd; best = a; }
+        }
+        real n[3] = {0, 0, 0};
+        n[best] = q[best] >= 0 ? 1 : -1;
+        return v3(n[0], n[1], n[2]);
+    }
+    const SheenCsgCone* c = &S->csg_cones[leaf];
+    V p0 = v3(c->p0.x, c->p0.y, c->p0.z), ax = sub(v3(c->p1.x, c->p1.y, c->p1.z), p0);
+    real L = sqrt(dot(ax, ax));
+    V a = mul(ax, 1 / L);
+    real hh = dot(sub(p, p0), a);
+    V w = sub(sub(p, p0), mul(a, hh));
+    real k = (c->r1 - c->r0) / L, rad = c->r0 + k * hh, wl = sqrt(dot(w, w));
+    real side = fabs(wl - rad) / rfmax(rfmax(c->r0, c->r1), R(1e-30));
+    real cap0 = fabs(hh) / L, cap1 = fabs(hh - L) / L;
+    if (cap0 < side && cap0 <= cap1) return neg(a);
+    if (cap1 < side) return a;
+    return wl > 0 ? sub(w, mul(a, rad * k)) : a;
+}
+
 typedef struct { real te, tx; int mat, leaf, kind; } Iv;
 
 static void csg_merge(const Iv* A, int nA, const Iv* B, int nB, int op, Iv* out, int* nOut) {
@@ -780,8 +1095,14 @@ static void csg_collect(const OracleScene* S, int node, const Ray* r, real t0, r
             iv.mat = o->material_id;
         } else if (n->leaf_kind == 1) {
             const Superellipsoid* se = &S->ses[n->leaf_index];
-            ok = se_intervals(r, se, t0, t1, &iv.te, &iv.tx);
+            ok = se_intervals(r, se, t0, t1, &iv.te, &iv.tx, S->se_n2 ? S->se_n2[n->leaf_index] : 0);
             iv.mat = se->material_id;
+        } else if (n->leaf_kind == 2 && S->csg_boxes) {
+            ok = box_iv(r, &S->csg_boxes[n->leaf_index], t0, t1, &iv.te, &iv.tx);
+            iv.mat = S->csg_boxes[n->leaf_index].material_id;
+        } else if (n->leaf_kind == 3 && S->csg_cones) {
+            ok = cone_iv(r, &S->csg_cones[n->leaf_index], t0, t1, &iv.te, &iv.tx);
+            iv.mat = S->csg_cones[n->leaf_index].material_id;
         }
         if (ok) { iv.leaf = n->leaf_index; iv.kind = n->leaf_kind; out[(*nOut)++] = iv; }
         return;
@@ -793,11 +1114,11 @@ static void csg_collect(const OracleScene* S, int node, const Ray* r, real t0, r
     csg_merge(A, nA, B, nB, n->op, out, nOut);
 }
 
-static int csg_hit(const OracleScene* S, const Ray* r, Hit* h) {
+static int csg_tree_hit(const OracleScene* S, int root, const Ray* r, Hit* h) {
     Iv iv[8];
     int cnt = 0;
     real t0 = r->tmin, t1 = r->tmax;
-    csg_collect(S, S->s.csg_root, r, t0, t1, iv, &cnt);
+    csg_collect(S, root, r, t0, t1, iv, &cnt);
     real best = R(1e30);
     int bi = -1;
     for (int i = 0; i < cnt; i++)
@@ -812,7 +1133,10 @@ static int csg_hit(const OracleScene* S, const Ray* r, Hit* h) {
         h->n = nrm(sub(h->p, fv(S->objects[iv[bi].leaf].param1)));
         h->tan = v3(0, 0, 0);
     } else if (iv[bi].kind == 1) {
-        h->n = nrm(se_grad(&S->ses[iv[bi].leaf], h->p));
+        h->n = nrm(se_grad(&S->ses[iv[bi].leaf], h->p, S->se_n2 ? S->se_n2[iv[bi].leaf] : 0));
+        h->tan = v3(1, 0, 0);
+    } else if (iv[bi].kind == 2 || iv[bi].kind == 3) {
+        h->n = nrm(csg_ext_normal(S, iv[bi].kind, iv[bi].leaf, h->p));
         h->tan = v3(1, 0, 0);
     } else {
         h->n = v3(0, 1, 0);
@@ -823,6 +1147,18 @@ static int csg_hit(const OracleScene* S, const Ray* r, Hit* h) {
     h->obj = 0;
     h->prim = bi;
     return 1;
+}
+
+/* The CSG category: the scene's tree, then the extension trees in index
+ * order; a later tree replaces the hit only when strictly closer. */
+static int csg_hit(const OracleScene* S, const Ray* r, Hit* h) {
+    int any = 0;
+    if (S->s.csg_root >= 0 && csg_tree_hit(S, S->s.csg_root, r, h)) any = 1;
+    for (int k = 0; k < S->ncsg_roots; k++) {
+        Hit t;
+        if (csg_tree_hit(S, S->csg_roots[k], r, &t) && (!any || t.t < h->t)) { *h = t; any = 1; }
+    }
+    return any;
 }
 
 /* ------------------------------------------------------------------ */
@@ -892,7 +1228,9 @@ static int cat_hf(const OracleScene* S, const Ray* r, Hit* h) {
         V hi = v3(hf->center.x + 0.5f * hf->size_x, hf->center.y + hf->height, hf->center.z + 0.5f * hf->size_z);
         widen(&lo, &hi);
         if (!slab(r, lo, hi)) continue;
-        if (hf_hit(r, hf, S->hf_img[i], &tmp) && tmp.t < best) {
+        Grid g = {NULL, 0, 0};
+        if (S->hfg && S->hfg[3 * i] >= 0) { g.h = S->hf_heights + S->hfg[3 * i]; g.w = S->hfg[3 * i + 1]; g.hgt = S->hfg[3 * i + 2]; }
+        if (hf_hit(r, hf, S->hf_img[i], &tmp, g) && tmp.t < best) {
             *h = tmp; h->mat = hf->material_id; h->obj = -(i + 1); h->cat = CAT_HF; h->prim = i;
             best = tmp.t; any = 1;
         }
@@ -908,7 +1246,7 @@ static int cat_se(const OracleScene* S, const Ray* r, Hit* h) {
         V hi = v3(se->center.x + se->a, se->center.y + se->b, se->center.z + se->c);
         widen(&lo, &hi);
         if (!slab(r, lo, hi)) continue;
-        if (se_hit(r, se, &tmp) && tmp.t < best) {
+        if (se_hit(r, se, &tmp, S->se_n2 ? S->se_n2[i] : 0) && tmp.t < best) {
             *h = tmp; h->mat = se->material_id; h->obj = -(i + 1); h->cat = CAT_SE; h->prim = i;
             best = tmp.t; any = 1;
         }
@@ -920,9 +1258,11 @@ static int cat_lathe(const OracleScene* S, const Ray* r, Hit* h) {
     int any = 0; real best = r->tmax; Hit tmp;
     for (int i = 0; i < S->s.num_lathes; i++) {
         V lo, hi;
-        lathe_box(&S->lathes[i], S->lpts, &lo, &hi);
+        const int exact = S->lathe_run && S->lathe_run[2 * i + 1] > 0;
+        if (exact) lathe_exact_box(S, i, &lo, &hi);
+        else lathe_box(&S->lathes[i], S->lpts, &lo, &hi);
         if (!slab(r, lo, hi)) continue;
-        if (lathe_hit(r, &S->lathes[i], S->lpts, &tmp) && tmp.t < best) {
+        if ((exact ? lathe_exact_hit(S, r, i, &tmp) : lathe_hit(r, &S->lathes[i], S->lpts, &tmp)) && tmp.t < best) {
             *h = tmp; h->obj = -(i + 1); h->cat = CAT_LATHE; h->prim = i;
             best = tmp.t; any = 1;
         }
@@ -934,9 +1274,11 @@ static int cat_prism(const OracleScene* S, const Ray* r, Hit* h) {
     int any = 0; real best = r->tmax; Hit tmp;
     for (int i = 0; i < S->s.num_prisms; i++) {
         V lo, hi;
-        prism_box(&S->prisms[i], S->ppts, &lo, &hi);
+        const int exact = S->prism_run && S->prism_run[2 * i + 1] > 0;
+        if (exact) prism_exact_box(S, i, &lo, &hi);
+        else prism_box(&S->prisms[i], S->ppts, &lo, &hi);
         if (!slab(r, lo, hi)) continue;
-        if (prism_hit(r, &S->prisms[i], S->ppts, &tmp) && tmp.t < best) {
+        if ((exact ? prism_exact_hit(S, r, i, &tmp) : prism_hit(r, &S->prisms[i], S->ppts, &tmp)) && tmp.t < best) {
             *h = tmp; h->obj = -(i + 1); h->cat = CAT_PRISM; h->prim = i;
             best = tmp.t; any = 1;
         }
@@ -976,7 +1318,7 @@ static int scene_hit(const OracleScene* S, const Ray* r, Hit* rec) {
     CAT(cat_se(S, r, &t))
     CAT(cat_lathe(S, r, &t))
     CAT(cat_prism(S, r, &t))
-    if (S->s.csg_root >= 0) { CAT(csg_hit(S, r, &t) && ((t.cat = CAT_CSG), 1)) }
+    if (S->s.csg_root >= 0 || S->ncsg_roots > 0) { CAT(csg_hit(S, r, &t) && ((t.cat = CAT_CSG), 1)) }
     CAT(cat_planes(S, r, &t))
 #undef CAT
     return hit;
@@ -992,7 +1334,7 @@ static int scene_hit_opaque(const OracleScene* S, const Ray* r, Hit* rec) {
     if (cat_se(S, r, rec)) return 1;
     if (cat_lathe(S, r, rec)) return 1;
     if (cat_prism(S, r, rec)) return 1;
-    if (S->s.csg_root >= 0 && csg_hit(S, r, rec)) { rec->cat = CAT_CSG; return 1; }
+    if ((S->s.csg_root >= 0 || S->ncsg_roots > 0) && csg_hit(S, r, rec)) { rec->cat = CAT_CSG; return 1; }
     return cat_planes(S, r, rec);
 }
 
@@ -1731,6 +2073,56 @@ static void build_tex(Tex* t, const unsigned char* px, int w, int h) {
     }
 }
 
+/* Bezier runs -> cubic spans: consecutive spans joined, and prism contours
+ * closed, by straight spans where their ends differ (the limit of the
+ * reference's host polyline). */
+static void add_runs(OracleScene* S, const SheenSceneExt* x, const SheenBezierRun* runs, int n, int close,
+                     int** out_run) {
+    if (!runs || n <= 0) return;
+    *out_run = (int*)calloc((size_t)n * 2, sizeof(int));
+    for (int i = 0; i < n; i++) {
+        const SheenBezierRun* r = &runs[i];
+        if (r->ctrl_count < 4) continue;
+        const float* c = x->bezier_ctrl + 2 * (size_t)r->ctrl_offset;
+        int ns = r->ctrl_count / 4, first = S->nspans;
+        S->spans = (double*)realloc(S->spans, sizeof(double) * 8 * (size_t)(S->nspans + 2 * ns + 1));
+#define PUSH8(a0, b0, a1, b1, a2, b2, a3, b3) do { double v8_[8] = {a0, b0, a1, b1, a2, b2, a3, b3}; \
+        memcpy(S->spans + 8 * (size_t)S->nspans++, v8_, sizeof(v8_)); } while (0)
+#define LINE(pa, pb, qa, qb) PUSH8(pa, pb, pa + (qa - pa) / 3.0, pb + (qb - pb) / 3.0, \
+        pa + 2.0 * (qa - pa) / 3.0, pb + 2.0 * (qb - pb) / 3.0, qa, qb)
+        for (int k = 0; k < ns; k++) {
+            const float* q = c + 8 * k;
+            if (k > 0 && (q[-2] != q[0] || q[-1] != q[1])) LINE((double)q[-2], (double)q[-1], (double)q[0], (double)q[1]);
+            PUSH8(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7]);
+        }
+        const float* last = c + 8 * (ns - 1) + 6;
+        if (close && (last[0] != c[0] || last[1] != c[1])) LINE((double)last[0], (double)last[1], (double)c[0], (double)c[1]);
+#undef LINE
+#undef PUSH8
+        (*out_run)[2 * i] = first;
+        (*out_run)[2 * i + 1] = S->nspans - first;
+    }
+}
+
+OracleScene* oracle_scene_create_ext(const SheenScene* in, const SheenSceneExt* x) {
+    OracleScene* S = oracle_scene_create(in);
+    if (!S || !x) return S;
+    if (x->se_n2 && in->num_superellipsoids > 0) S->se_n2 = (float*)dup(x->se_n2, sizeof(float) * (size_t)in->num_superellipsoids);
+    if (x->hf_grid && in->num_heightfields > 0) {
+        S->hfg = (int*)calloc((size_t)in->num_heightfields * 3, sizeof(int));
+        for (int i = 0; i < in->num_heightfields; i++) {
+            S->hfg[3 * i] = x->hf_grid[i].offset; S->hfg[3 * i + 1] = x->hf_grid[i].w; S->hfg[3 * i + 2] = x->hf_grid[i].h;
+        }
+        if (x->num_hf_heights > 0) S->hf_heights = (float*)dup(x->hf_heights, sizeof(float) * (size_t)x->num_hf_heights);
+    }
+    add_runs(S, x, x->lathe_bezier, in->num_lathes, 0, &S->lathe_run);
+    add_runs(S, x, x->prism_bezier, in->num_prisms, 1, &S->prism_run);
+    if (x->num_csg_roots > 0) { S->csg_roots = (int*)dup(x->csg_roots, sizeof(int) * (size_t)x->num_csg_roots); S->ncsg_roots = x->num_csg_roots; }
+    if (x->num_csg_boxes > 0) { S->csg_boxes = (SheenCsgBox*)dup(x->csg_boxes, sizeof(SheenCsgBox) * (size_t)x->num_csg_boxes); S->ncsg_boxes = x->num_csg_boxes; }
+    if (x->num_csg_cones > 0) { S->csg_cones = (SheenCsgCone*)dup(x->csg_cones, sizeof(SheenCsgCone) * (size_t)x->num_csg_cones); S->ncsg_cones = x->num_csg_cones; }
+    return S;
+}
+
 OracleScene* oracle_scene_create(const SheenScene* in) {
     if (!in) return NULL;
     OracleScene* S = (OracleScene*)calloc(1, sizeof(OracleScene));
@@ -1779,6 +2171,8 @@ void oracle_scene_destroy(OracleScene* S) {
     free(S->tex);
     free(S->ph_pos); free(S->ph_dir); free(S->ph_nrm); free(S->ph_flux);
     free(S->cell_start); free(S->cell_count);
+    free(S->se_n2); free(S->hfg); free(S->hf_heights); free(S->lathe_run); free(S->prism_run); free(S->spans);
+    free(S->csg_roots); free(S->csg_boxes); free(S->csg_cones);
     free(S);
 }
 

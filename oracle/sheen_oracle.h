@@ -34,6 +34,11 @@ typedef struct OracleScene OracleScene;
  * are lights) runs the photon pass with the reference's fixed seed.  Photon
  * slots follow emission order. */
 OracleScene* oracle_scene_create(const SheenScene* scene);
+/* With scene extensions (SheenSceneExt; no counterpart in the reference):
+ * two-exponent superellipsoids, FP32 height grids, exact Bezier lathes and
+ * prisms (found by dense sampling and bisection in double), CSG forests
+ * with box and cone leaves.  ext may be NULL. */
+OracleScene* oracle_scene_create_ext(const SheenScene* scene, const SheenSceneExt* ext);
 void oracle_scene_destroy(OracleScene* s);
 int oracle_scene_photon_count(const OracleScene* s);
 /* Extension: camera samples without jitter (the library's "camera.centered"). */

@@ -121,6 +121,12 @@ def lib():
     L.sheen_owned_free.restype = None
     L.sheen_generate_scene.argtypes = [I, U, I, I, ctypes.POINTER(P)]
     L.sheen_generate_scene.restype = I
+    L.sheen_generate_scene_ext.argtypes = [I, U, I, I, I, ctypes.POINTER(P)]
+    L.sheen_generate_scene_ext.restype = I
+    L.sheen_owned_ext.argtypes = [P]
+    L.sheen_owned_ext.restype = P
+    L.sheen_scene_create_ext.argtypes = [P, P, I, ctypes.POINTER(P)]
+    L.sheen_scene_create_ext.restype = I
     L.sheen_scene_primary_hits.argtypes = [P, I, I, I, P, P, P]
     L.sheen_scene_profile_stages.argtypes = [P, I, I, I, P, P, ctypes.POINTER(StageProfile)]
     L.sheen_render_batch.argtypes = [ctypes.POINTER(BatchJob), I, P, ctypes.POINTER(RenderStats)]
@@ -187,12 +193,18 @@ def render_rgba(scene, width: int, height: int, aa: int, form: int = FORM_PLAIN)
 
 
 class DeviceScene:
-    """A scene resident in HBM (SheenDeviceScene)."""
+    """A scene resident in HBM (SheenDeviceScene).  With ext, an OwnedScene's
+    extension arrays (sheen_owned_ext) are passed to sheen_scene_create_ext."""
 
-    def __init__(self, scene, form: int = FORM_PLAIN):
+    def __init__(self, scene, form: int = FORM_PLAIN, ext: bool = False):
         ptr, keep = _scene_ptr(scene)
         h = ctypes.c_void_p()
-        _check(lib().sheen_scene_create(ptr, form, ctypes.byref(h)))
+        if ext:
+            if not isinstance(scene, OwnedScene):
+                raise TypeError("scene extensions come from an OwnedScene")
+            _check(lib().sheen_scene_create_ext(ptr, scene.ext_ptr, form, ctypes.byref(h)))
+        else:
+            _check(lib().sheen_scene_create(ptr, form, ctypes.byref(h)))
         del keep
         self.handle = h.value
         self.form = form
@@ -285,6 +297,11 @@ class OwnedScene:
         return SheenScene.from_address(self.view_ptr)
 
     @property
+    def ext_ptr(self) -> int:
+        """Address of the scene's SheenSceneExt (zero-filled when it has none)."""
+        return lib().sheen_owned_ext(self.handle)
+
+    @property
     def settings(self) -> dict:
         s = lib().sheen_owned_settings(self.handle).contents
         return {"width": s.width, "height": s.height, "aa": s.aa, "photons": s.photons,
@@ -309,9 +326,15 @@ def load_scene_file(path: str) -> OwnedScene:
     return OwnedScene(h.value)
 
 
-def generate_scene(config: int, seed: int = 1, detail: int = 0, photons: int = 0) -> OwnedScene:
+def generate_scene(config: int, seed: int = 1, detail: int = 0, photons: int = 0,
+                   extended: bool = False) -> OwnedScene:
+    """A workload scene; extended (config 2): with its extension column
+    (sheen_generate_scene_ext)."""
     h = ctypes.c_void_p()
-    _check(lib().sheen_generate_scene(config, seed, detail, photons, ctypes.byref(h)))
+    if extended:
+        _check(lib().sheen_generate_scene_ext(config, seed, detail, photons, 1, ctypes.byref(h)))
+    else:
+        _check(lib().sheen_generate_scene(config, seed, detail, photons, ctypes.byref(h)))
     return OwnedScene(h.value)
 
 
@@ -349,6 +372,7 @@ def tune_get(key: str) -> int:
 
 
 TUNE_KEYS = ("wave.shadow_kernel", "wave.refill_min", "wave.shadow_blocks_per_sm", "wave.shadow_stack",
+             "wave.tile_w", "wave.mega_samples",
              "wave.inner_min")
 
 
@@ -356,7 +380,7 @@ class TuneResult(ctypes.Structure):
     _fields_ = [("shadow_kernel", ctypes.c_int), ("refill_min", ctypes.c_int),
                 ("shadow_blocks_per_sm", ctypes.c_int), ("candidates", ctypes.c_int),
                 ("best_ms", ctypes.c_double), ("default_ms", ctypes.c_double), ("shadow_stack", ctypes.c_int),
-                ("inner_min", ctypes.c_int)]
+                ("inner_min", ctypes.c_int), ("tile_w", ctypes.c_int), ("mega_samples", ctypes.c_int)]
 
 
 def autotune(scene: "DeviceScene", width: int, height: int, aa: int, reps: int = 3, cache: str | None = None,
@@ -385,7 +409,7 @@ def autotune(scene: "DeviceScene", width: int, height: int, aa: int, reps: int =
     _check(L.sheen_autotune(scene.handle, width, height, aa, reps, ctypes.byref(r)))
     res = {"wave.shadow_kernel": r.shadow_kernel, "wave.refill_min": r.refill_min,
            "wave.shadow_blocks_per_sm": r.shadow_blocks_per_sm, "wave.shadow_stack": r.shadow_stack,
-           "wave.inner_min": r.inner_min,
+           "wave.inner_min": r.inner_min, "wave.tile_w": r.tile_w, "wave.mega_samples": r.mega_samples,
            "candidates": r.candidates,
            "best_ms": r.best_ms, "default_ms": r.default_ms}
     if cache:

@@ -124,12 +124,16 @@ void sheen_cleanup(void) {
 }
 
 int sheen_scene_create(const SheenScene* scene, int form, SheenDeviceScene* out) {
+    return sheen_scene_create_ext(scene, nullptr, form, out);
+}
+
+int sheen_scene_create_ext(const SheenScene* scene, const SheenSceneExt* ext, int form, SheenDeviceScene* out) {
     if (!out) { sheen::set_error("null output handle"); return -1; }
     *out = nullptr;
     if (!scene) { sheen::set_error("null scene"); return -1; }
     if (!scene->num_materials) { sheen::set_error("no materials"); return -1; }
     sheen::DeviceScene* s = nullptr;
-    if (sheen::scene_upload(scene, form, &s) != 0) return -1;
+    if (sheen::scene_upload_ext(scene, ext, form, &s) != 0) return -1;
     {
         std::lock_guard<std::mutex> lk(g_mu);
         g_scenes.insert(s);

@@ -64,6 +64,93 @@ __device__ __forceinline__ void csg_combine(const SpanList& A, const SpanList& B
     }
 }
 
+// Extension leaves (no counterpart in the reference, whose leaves are
+// spheres and superellipsoids).  Both solids are convex, so a ray meets
+// each in one interval, clipped to [t0, t1] like sphere_span.
+__device__ __forceinline__ bool box_span(const Ray& r, float3 lo, float3 hi, float t0, float t1, float& te,
+                                         float& tx) {
+    const float o[3] = {r.o.x, r.o.y, r.o.z}, d[3] = {r.d.x, r.d.y, r.d.z};
+    const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+    float tn = -3.0e38f, tf = 3.0e38f;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float inv = 1.0f / d[a];
+        const float ta = (l[a] - o[a]) * inv, tb = (h[a] - o[a]) * inv;
+        tn = fmaxf(tn, fminf(ta, tb));
+        tf = fminf(tf, fmaxf(ta, tb));
+    }
+    if (!(tn <= tf) || tf < t0 || tn > t1) return false;
+    te = fmaxf(tn, t0);
+    tx = fminf(tf, t1);
+    return te <= tx;
+}
+
+// Capped cone (frustum) from p0 (radius r0) to p1 (radius r1): the axial
+// slab [0, L] intersected with |w|^2 <= (r0 + k h)^2, w the offset from the
+// axis, h the axial coordinate, k = (r1 - r0) / L.
+__device__ __forceinline__ bool cone_span(const Ray& r, float3 p0, float r0, float3 p1, float r1, float t0, float t1,
+                                          float& te, float& tx) {
+    const float3 ax = p1 - p0;
+    const float L = sqrtf(dot(ax, ax));
+    if (!(L > 0.0f)) return false;
+    const float3 a = ax / L;
+    const float3 oc = r.o - p0;
+    const float ho = dot(oc, a), hd = dot(r.d, a);
+    float sa, sb;
+    if (fabsf(hd) > 1e-30f) {
+        sa = (0.0f - ho) / hd;
+        sb = (L - ho) / hd;
+        if (sa > sb) { const float t = sa; sa = sb; sb = t; }
+    } else {
+        if (ho < 0.0f || ho > L) return false;
+        sa = -3.0e38f;
+        sb = 3.0e38f;
+    }
+    const float k = (r1 - r0) / L, rb = r0 + k * ho, rk = k * hd;
+    const float A = dot(r.d, r.d) - hd * hd - rk * rk;
+    const float B = 2.0f * (dot(oc, r.d) - ho * hd - rb * rk);
+    const float C = dot(oc, oc) - ho * ho - rb * rb;
+    float lo = sa, hi = sb;
+    if (fabsf(A) <= 1e-12f * (fabsf(B) + fabsf(C) + 1e-30f)) {
+        if (B == 0.0f) { if (C > 0.0f) return false; }
+        else if (B > 0.0f) hi = fminf(hi, -C / B);
+        else lo = fmaxf(lo, -C / B);
+    } else {
+        const float disc = B * B - 4.0f * A * C;
+        if (A > 0.0f) {
+            if (disc < 0.0f) return false;
+            const float sq = sqrtf(disc);
+            lo = fmaxf(lo, (-B - sq) / (2.0f * A));
+            hi = fminf(hi, (-B + sq) / (2.0f * A));
+        } else if (disc >= 0.0f) {
+            // q <= 0 outside the roots: the piece on the frustum's side of
+            // the apex (radius r0 + k h >= 0 at its middle)
+            const float sq = sqrtf(disc);
+            const float ra = (-B + sq) / (2.0f * A), rbb = (-B - sq) / (2.0f * A);   // ra <= rbb
+            const float l1 = lo, h1 = fminf(hi, ra), l2 = fmaxf(lo, rbb), h2 = hi;
+            const bool ok1 = l1 <= h1, ok2 = l2 <= h2;
+            if (ok1 && ok2) {
+                const float m1 = 0.5f * (fmaxf(l1, -1e30f) + fminf(h1, 1e30f));
+                if (r0 + k * (ho + m1 * hd) >= 0.0f) hi = h1; else lo = l2;
+            } else if (ok1) {
+                hi = h1;
+            } else if (ok2) {
+                lo = l2;
+            } else {
+                return false;
+            }
+        }
+    }
+    if (!(lo <= hi) || hi < t0 || lo > t1) return false;
+    te = fmaxf(lo, t0);
+    tx = fminf(hi, t1);
+    return te <= tx;
+}
+
+__device__ __forceinline__ float se_n2_of(const DevScene& S, int i) {
+    return S.se_n2 ? __ldg(&S.se_n2[i]) : 0.0f;
+}
+
 __device__ __forceinline__ void csg_leaf(const DevScene& S, const CSGNode& nd, const Ray& r, float t0, float t1,
                                          SpanList& out) {
     out.n = 0;
@@ -75,8 +162,17 @@ __device__ __forceinline__ void csg_leaf(const DevScene& S, const CSGNode& nd, c
         sp.mat = o.material_id;
     } else if (nd.leaf_kind == 1) {
         const Superellipsoid se = S.ses[nd.leaf_index];
-        ok = se_span(r, se, t0, t1, sp.te, sp.tx);
+        const float n2 = se_n2_of(S, nd.leaf_index);
+        ok = n2 > 0.0f ? se_span2(r, se, n2, t0, t1, sp.te, sp.tx, nullptr) : se_span(r, se, t0, t1, sp.te, sp.tx);
         sp.mat = se.material_id;
+    } else if (nd.leaf_kind == 2 && S.csg_boxes) {
+        const float4 lo = __ldg(&S.csg_boxes[2 * nd.leaf_index]), hi = __ldg(&S.csg_boxes[2 * nd.leaf_index + 1]);
+        ok = box_span(r, f3(lo.x, lo.y, lo.z), f3(hi.x, hi.y, hi.z), t0, t1, sp.te, sp.tx);
+        sp.mat = __float_as_int(lo.w);
+    } else if (nd.leaf_kind == 3 && S.csg_cones) {
+        const float4 a = __ldg(&S.csg_cones[3 * nd.leaf_index]), b = __ldg(&S.csg_cones[3 * nd.leaf_index + 1]);
+        ok = cone_span(r, f3(a.x, a.y, a.z), a.w, f3(b.x, b.y, b.z), b.w, t0, t1, sp.te, sp.tx);
+        sp.mat = __float_as_int(__ldg(&S.csg_cones[3 * nd.leaf_index + 2]).x);
     }
     if (ok) {
         sp.leaf = nd.leaf_index;
@@ -85,14 +181,48 @@ __device__ __forceinline__ void csg_leaf(const DevScene& S, const CSGNode& nd, c
     }
 }
 
-// integrator/csg.h:142-186: nearest interval of the root -> hit record.
-static __device__ __noinline__ bool csg_test(const DevScene& S, const Ray& r, Hit& h) {
+// Outward normal direction of an extension leaf at p.
+__device__ __forceinline__ float3 csg_ext_normal(const DevScene& S, int kind, int leaf, float3 p) {
+    if (kind == 2) {
+        const float4 lo = __ldg(&S.csg_boxes[2 * leaf]), hi = __ldg(&S.csg_boxes[2 * leaf + 1]);
+        const float c[3] = {0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z)};
+        const float e[3] = {0.5f * (hi.x - lo.x), 0.5f * (hi.y - lo.y), 0.5f * (hi.z - lo.z)};
+        const float q[3] = {p.x - c[0], p.y - c[1], p.z - c[2]};
+        int best = 0;
+        float bd = 3.0e38f;
+        for (int a = 0; a < 3; a++) {
+            const float dd = fabsf(e[a] - fabsf(q[a])) / fmaxf(e[a], 1e-30f);
+            if (dd < bd) { bd = dd; best = a; }
+        }
+        float3 n = f3(0.0f, 0.0f, 0.0f);
+        const float sg = q[best] >= 0.0f ? 1.0f : -1.0f;
+        if (best == 0) n.x = sg; else if (best == 1) n.y = sg; else n.z = sg;
+        return n;
+    }
+    const float4 a4 = __ldg(&S.csg_cones[3 * leaf]), b4 = __ldg(&S.csg_cones[3 * leaf + 1]);
+    const float3 p0 = f3(a4.x, a4.y, a4.z), ax = f3(b4.x, b4.y, b4.z) - p0;
+    const float L = sqrtf(dot(ax, ax));
+    const float3 a = ax / L;
+    const float hh = dot(p - p0, a);
+    const float3 w = (p - p0) - hh * a;
+    const float k = (b4.w - a4.w) / L, rad = a4.w + k * hh, wl = sqrtf(dot(w, w));
+    const float side = fabsf(wl - rad) / fmaxf(fmaxf(a4.w, b4.w), 1e-30f);
+    const float cap0 = fabsf(hh) / L, cap1 = fabsf(hh - L) / L;
+    if (cap0 < side && cap0 <= cap1) return -a;
+    if (cap1 < side) return a;
+    // the side: gradient of |w|^2 - (r0 + k h)^2
+    return wl > 0.0f ? w - (rad * k) * a : a;
+}
+
+// integrator/csg.h:142-186: nearest interval of the tree at `root` -> hit
+// record.
+static __device__ __noinline__ bool csg_tree_test(const DevScene& S, const Ray& r, Hit& h, int root) {
     const float t0 = r.tmin, t1 = r.tmax;
     int node_stack[kCsgMaxDepth + 1];
     unsigned char phase[kCsgMaxDepth + 1];
     SpanList vals[kCsgMaxDepth + 2];
     int nn = 0, nv = 0;
-    node_stack[nn] = S.csg_root; phase[nn] = 0; nn++;
+    node_stack[nn] = root; phase[nn] = 0; nn++;
     while (nn > 0) {
         const int id = node_stack[nn - 1];
         const CSGNode nd = S.csg_nodes[id];
@@ -140,7 +270,10 @@ static __device__ __noinline__ bool csg_test(const DevScene& S, const Ray& r, Hi
         h.n = normalize(h.p - f3(S.objects[sp.leaf].param1));
         h.tan = f3(0.0f, 0.0f, 0.0f);
     } else if (sp.kind == 1) {
-        h.n = normalize(se_gradient(S.ses[sp.leaf], h.p));
+        h.n = normalize(se_normal_dir(S.ses[sp.leaf], se_n2_of(S, sp.leaf), h.p));
+        h.tan = f3(1.0f, 0.0f, 0.0f);
+    } else if (sp.kind == 2 || sp.kind == 3) {
+        h.n = normalize(csg_ext_normal(S, sp.kind, sp.leaf, h.p));
         h.tan = f3(1.0f, 0.0f, 0.0f);
     } else {
         h.n = f3(0.0f, 1.0f, 0.0f);
@@ -150,6 +283,61 @@ static __device__ __noinline__ bool csg_test(const DevScene& S, const Ray& r, Hi
     if (dot(h.n, r.d) > 0.0f) h.n = -h.n;
     return true;
 }
+
+// The scene's own tree (integrator/csg.h: a single root).
+__device__ __forceinline__ bool csg_test(const DevScene& S, const Ray& r, Hit& h) {
+    return csg_tree_test(S, r, h, S.csg_root);
+}
+
+// Extension: the closest hit over the further trees of the scene's CSG
+// forest, walked through the median BVH over their leaf boxes (boxes beyond
+// the closest hit so far are skipped).  Each tree is evaluated over the
+// ray's whole [tmin, tmax], as when it is alone.
+static __device__ __noinline__ bool csg_forest_test(const DevScene& S, const Ray& r, Hit& h) {
+    int stack[64];
+    int sp = 0;
+    stack[sp++] = 0;
+    bool any = false;
+    float best = r.tmax;
+    while (sp > 0) {
+        const int id = stack[--sp];
+        const float4 a = __ldg(&S.csg_root_bvh[id].a), b = __ldg(&S.csg_root_bvh[id].b);
+        Ray rb = r;
+        rb.tmax = best;
+        if (!box_hit_ref(rb, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z))) continue;
+        const int left = __float_as_int(a.w), right = __float_as_int(b.w);
+        if (left < 0) {
+            Hit t;
+            if (csg_tree_test(S, r, t, S.csg_roots[~left]) && t.t < best) { h = t; best = t.t; any = true; }
+            continue;
+        }
+        if (sp > 62) continue;   // cannot happen for the trees built here
+        stack[sp++] = right;
+        stack[sp++] = left;
+    }
+    return any;
+}
+
+// The CSG category with the extension forest: the scene's tree (with
+// cull_box, skipped when the ray misses the box of its leaves), then the
+// further trees; strict '<' keeps the earlier tree on a tie.  Not inlined:
+// scenes without a forest take csg_closest's single-tree path.
+static __device__ __noinline__ bool csg_closest_forest(const DevScene& S, const Ray& r, Hit& h, bool cull_box) {
+    bool any = false;
+    if (S.csg_root >= 0 && (!cull_box || ray_meets_box(r, S.csg_lo, S.csg_hi)) && csg_test(S, r, h)) any = true;
+    Hit t;
+    if (csg_forest_test(S, r, t) && (!any || t.t < h.t)) { h = t; any = true; }
+    return any;
+}
+
+// The CSG category (integrator/csg.h: the scene's single tree, culled by the
+// box of its leaves when cull_box), or with an extension forest every tree.
+__device__ __forceinline__ bool csg_closest(const DevScene& S, const Ray& r, Hit& h, bool cull_box) {
+    if (S.num_csg_roots > 0) return csg_closest_forest(S, r, h, cull_box);
+    return S.csg_root >= 0 && (!cull_box || ray_meets_box(r, S.csg_lo, S.csg_hi)) && csg_test(S, r, h);
+}
+
+__device__ __forceinline__ bool has_csg(const DevScene& S) { return S.csg_root >= 0 || S.num_csg_roots > 0; }
 
 }  // namespace dev
 }  // namespace sheen

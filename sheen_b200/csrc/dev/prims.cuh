@@ -523,6 +523,28 @@ __device__ __forceinline__ float3 se_gradient(const Superellipsoid& s, float3 p)
               s.n * powf(fabsf(qz), s.n - 1.0f) * (qz >= 0.0f ? 1.0f : -1.0f) / s.c);
 }
 
+// Extension (no counterpart in the reference): the two-exponent body
+// (|qx|^n + |qz|^n)^(n2/n) + |qy|^n2 = 1 -- n the east-west exponent,
+// n2 > 0 the north-south one on the y axis; n2 == n is the single-exponent
+// body above.
+__device__ __forceinline__ float se_value2(const Superellipsoid& s, float n2, float3 p) {
+    float qx = (p.x - s.center.x) / s.a, qy = (p.y - s.center.y) / s.b, qz = (p.z - s.center.z) / s.c;
+    const float xz = powf(fabsf(qx), s.n) + powf(fabsf(qz), s.n);
+    return powf(xz, n2 / s.n) + powf(fabsf(qy), n2);
+}
+__device__ __forceinline__ float3 se_gradient2(const Superellipsoid& s, float n2, float3 p) {
+    float qx = (p.x - s.center.x) / s.a, qy = (p.y - s.center.y) / s.b, qz = (p.z - s.center.z) / s.c;
+    const float ax = fabsf(qx), az = fabsf(qz);
+    const float xz = powf(ax, s.n) + powf(az, s.n);
+    const float k = xz > 0.0f ? n2 * powf(xz, n2 / s.n - 1.0f) : 0.0f;
+    return f3(k * powf(ax, s.n - 1.0f) * (qx >= 0.0f ? 1.0f : -1.0f) / s.a,
+              n2 * powf(fabsf(qy), n2 - 1.0f) * (qy >= 0.0f ? 1.0f : -1.0f) / s.b,
+              k * powf(az, s.n - 1.0f) * (qz >= 0.0f ? 1.0f : -1.0f) / s.c);
+}
+__device__ __forceinline__ float3 se_normal_dir(const Superellipsoid& s, float n2, float3 p) {
+    return n2 > 0.0f ? se_gradient2(s, n2, p) : se_gradient(s, p);
+}
+
 // Whether F(p) = |qx|^n + |qy|^n + |qz|^n exceeds 1 -- the only use se_span
 // makes of F -- deciding from two bounds before any powf where they can:
 //   F <= 3 max|q_i|^n, so max|q_i| < (1/3)^(1/n) means inside;
@@ -576,16 +598,17 @@ __device__ __forceinline__ void se_chord(const Ray& r, const Superellipsoid& s, 
 // found by sampling is not refined (its bisection interval is empty), so
 // the entry lies on a sample.
 // SIGN: decide the samples through SeSign (the same decisions, fewer powf).
-template <bool SIGN = false>
-__device__ __forceinline__ bool se_span(const Ray& r, const Superellipsoid& s, float t0, float t1,
-                                        float& te, float& tx, float* te_prev = nullptr) {
+// The march and bisection of se_span over an "outside" predicate.
+// make() builds the predicate once the chord is known to be hit.
+template <class MakeOut>
+__device__ __forceinline__ bool se_span_core(const Ray& r, const Superellipsoid& s, float t0, float t1, float& te,
+                                             float& tx, float* te_prev, MakeOut make) {
     float tA, tB;
     se_chord(r, s, tA, tB);
     if (tB < t0 || tA > t1 || tB < tA) return false;
     t0 = fmaxf(t0, tA);
     t1 = fminf(t1, tB);
-    const SeSign sg(SIGN ? s.n : 0.0f);
-    auto out = [&](float3 p) { return SIGN ? sg.outside(s, p) : se_value(s, p) > 1.0f; };
+    const auto out = make();
     const float step = (t1 - t0) / 32.0f;
     float tp = t0;
     bool inside = !out(r.o + tp * r.d);
@@ -617,6 +640,61 @@ __device__ __forceinline__ bool se_span(const Ray& r, const Superellipsoid& s, f
     if (!found_in) return false;
     if (!found_out) tx = t1;
     return te <= tx;
+}
+
+// Whether the march over [t0, t1] can find an inside sample at all.  The
+// body |qx|^n + |qy|^n + |qz|^n <= 1 lies in the ellipsoid
+// qx^2 + qy^2 + qz^2 <= k^2 with k = 1 for n <= 2 (there sum q^2 <=
+// (sum |q|^n)^(2/n), the power means) and k^2 = 3^(1 - 2/n) for n > 2
+// (sum q^2 / 3 <= (sum |q|^n / 3)^(2/n)).  On a ray that misses that
+// ellipsoid widened by 1e-3, every point has F >= (1 + 1e-3)^min(n, 2) - 1
+// above 1 -- for n >= 0.25 about 2.5e-4, far beyond the rounding of F in
+// FP32 -- so every sample tests outside and the march finds no entry: the
+// result is the march's, without its 33 evaluations.
+__device__ __forceinline__ bool se_may_enter(const Ray& r, const Superellipsoid& s, float t0, float t1) {
+    if (!(s.n >= 0.25f && s.n <= 1e4f)) return true;
+    const float k2 = s.n <= 2.0f ? 1.0f : powf(3.0f, 1.0f - 2.0f / s.n);
+    const float K = k2 * 1.002001f;   // (k (1 + 1e-3))^2
+    const float3 inv = f3(1.0f / s.a, 1.0f / s.b, 1.0f / s.c);
+    const float3 oc = f3((r.o.x - s.center.x) * inv.x, (r.o.y - s.center.y) * inv.y, (r.o.z - s.center.z) * inv.z);
+    const float3 dd = f3(r.d.x * inv.x, r.d.y * inv.y, r.d.z * inv.z);
+    const float A = dot(dd, dd), B = dot(oc, dd), C = dot(oc, oc) - K;
+    const float disc = B * B - A * C;
+    // a generous slack on the FP32 discriminant before declaring a miss
+    if (!(disc < -1e-4f * (B * B + fabsf(A * C)))) {
+        if (!(A > 0.0f) || disc <= 0.0f) return true;
+        const float sq = sqrtf(disc);
+        const float ta = (-B - sq) / A, tb = (-B + sq) / A;
+        const float slack = 1e-3f * (fabsf(ta) + fabsf(tb)) + 1e-6f;
+        return !(tb < t0 - slack || ta > t1 + slack);
+    }
+    return false;
+}
+
+// primitives/superellipsoid.h:41-117: 32 samples of F along the clipped
+// chord, 20 bisection steps for the exit.  As in the reference an entry
+// found by sampling is not refined (its bisection interval is empty), so
+// the entry lies on a sample.
+// SIGN: decide the samples through SeSign (the same decisions, fewer powf),
+// and skip the march of rays that miss the body's bounding ellipsoid
+// (se_may_enter: the same result).
+template <bool SIGN = false>
+__device__ __forceinline__ bool se_span(const Ray& r, const Superellipsoid& s, float t0, float t1,
+                                        float& te, float& tx, float* te_prev = nullptr) {
+    if (SIGN && !se_may_enter(r, s, t0, t1)) return false;
+    return se_span_core(r, s, t0, t1, te, tx, te_prev, [&]() {
+        const SeSign sg(SIGN ? s.n : 0.0f);
+        return [sg, &s](float3 p) { return SIGN ? sg.outside(s, p) : se_value(s, p) > 1.0f; };
+    });
+}
+
+// Extension: the two-exponent body's span (the same march), not inlined so
+// that the kernels' code for the reference's body is unchanged.
+static __device__ __noinline__ bool se_span2(const Ray& r, const Superellipsoid& s, float n2, float t0, float t1,
+                                             float& te, float& tx, float* te_prev) {
+    return se_span_core(r, s, t0, t1, te, tx, te_prev, [&]() {
+        return [&s, n2](float3 p) { return se_value2(s, n2, p) > 1.0f; };
+    });
 }
 
 // Extension (a scene created with "trace.se_polish"; the reference has
@@ -651,6 +729,7 @@ static __device__ __noinline__ float se_polish_entry(const Ray& r, const Superel
 }
 
 // primitives/superellipsoid.h:123-161
+// primitives/superellipsoid.h:123-161
 template <bool SIGN = false>
 __device__ __forceinline__ bool se_test(const Ray& r, const Superellipsoid& s, Hit& h, int polish = 0) {
     float t0, t1;
@@ -664,6 +743,25 @@ __device__ __forceinline__ bool se_test(const Ray& r, const Superellipsoid& s, H
     h.t = te;
     h.p = r.o + te * r.d;
     h.n = normalize(se_gradient(s, h.p));
+    h.tan = f3(1.0f, 0.0f, 0.0f);
+    h.uv = make_float2(h.p.x, h.p.y);
+    if (dot(h.n, r.d) > 0.0f) h.n = -h.n;
+    h.mat = s.material_id;
+    return true;
+}
+
+// Extension: the two-exponent body (n2 > 0; no polish), not inlined.
+static __device__ __noinline__ bool se_test2(const Ray& r, const Superellipsoid& s, float n2, Hit& h) {
+    float t0, t1;
+    se_chord(r, s, t0, t1);
+    if (t1 < r.tmin || t0 > r.tmax || t1 < t0) return false;
+    t0 = fmaxf(t0, r.tmin);
+    t1 = fminf(t1, r.tmax);
+    float te, tx;
+    if (!se_span2(r, s, n2, t0, t1, te, tx, nullptr)) return false;
+    h.t = te;
+    h.p = r.o + te * r.d;
+    h.n = normalize(se_gradient2(s, n2, h.p));
     h.tan = f3(1.0f, 0.0f, 0.0f);
     h.uv = make_float2(h.p.x, h.p.y);
     if (dot(h.n, r.d) > 0.0f) h.n = -h.n;
@@ -690,10 +788,28 @@ __device__ __forceinline__ float hf_noise(float fx, float fz, int seed) {
 }
 
 // primitives/heightfield.h:58-116: height above the tile base.
-__device__ __forceinline__ float hf_height(const HeightField& hf, float x, float z) {
+// Extension (no counterpart in the reference): an FP32 height grid of
+// gw x gh values in [0, 1] replaces the procedural / 8-bit height, sampled
+// bilinearly over the same footprint as the 8-bit image.
+struct HfGrid {
+    const float* h;
+    int w, hgt;
+};
+
+__device__ __forceinline__ float hf_height(const HeightField& hf, float x, float z, HfGrid g = HfGrid{nullptr, 0, 0}) {
     float lx = (x - hf.center.x) / hf.size_x + 0.5f;
     float lz = (z - hf.center.z) / hf.size_z + 0.5f;
     if (lx < 0.0f || lx > 1.0f || lz < 0.0f || lz > 1.0f) return 0.0f;
+    if (g.h) {
+        float fu = lx * (float)(g.w - 1), fv = lz * (float)(g.hgt - 1);
+        int u0 = (int)fu, v0 = (int)fv;
+        int u1 = u0 < g.w - 1 ? u0 + 1 : u0, v1 = v0 < g.hgt - 1 ? v0 + 1 : v0;
+        float tx = fu - (float)u0, ty = fv - (float)v0;
+        const float h00 = __ldg(&g.h[(size_t)v0 * g.w + u0]), h10 = __ldg(&g.h[(size_t)v0 * g.w + u1]);
+        const float h01 = __ldg(&g.h[(size_t)v1 * g.w + u0]), h11 = __ldg(&g.h[(size_t)v1 * g.w + u1]);
+        float hh = h00 * (1.0f - tx) * (1.0f - ty) + h10 * tx * (1.0f - ty) + h01 * (1.0f - tx) * ty + h11 * tx * ty;
+        return hh * hf.height;
+    }
     if (hf.image) {
         if (hf.img_w < 1 || hf.img_h < 1) return 0.0f;
         float fu = lx * (float)(hf.img_w - 1), fv = lz * (float)(hf.img_h - 1);
@@ -720,7 +836,7 @@ __device__ __forceinline__ float hf_height(const HeightField& hf, float x, float
 
 // primitives/heightfield.h:121-183: march (diagonal/64 steps, <= 256) then
 // 10 bisection steps; finite-difference normal.
-__device__ __forceinline__ bool hf_test(const Ray& r, const HeightField& hf, Hit& h) {
+__device__ __forceinline__ bool hf_test(const Ray& r, const HeightField& hf, Hit& h, HfGrid g = HfGrid{nullptr, 0, 0}) {
     const float3 lo = f3(hf.center.x - 0.5f * hf.size_x, hf.center.y, hf.center.z - 0.5f * hf.size_z);
     const float3 hi = f3(hf.center.x + 0.5f * hf.size_x, hf.center.y + hf.height, hf.center.z + 0.5f * hf.size_z);
     float ix = 1.0f / r.d.x, iy = 1.0f / r.d.y, iz = 1.0f / r.d.z;
@@ -740,21 +856,21 @@ __device__ __forceinline__ bool hf_test(const Ray& r, const HeightField& hf, Hit
     bool inside = false;
     for (int i = 0; i < 256; i++) {
         float3 p = r.o + t * r.d;
-        bool below = p.y <= hf_height(hf, p.x, p.z) + hf.center.y;
+        bool below = p.y <= hf_height(hf, p.x, p.z, g) + hf.center.y;
         if (below != inside) {
             float a = t - step, b = t;
             if (a < t0) a = t0;
             for (int k = 0; k < 10; k++) {
                 float mid = 0.5f * (a + b);
                 float3 pm = r.o + mid * r.d;
-                if ((pm.y <= hf_height(hf, pm.x, pm.z) + hf.center.y) == below) b = mid; else a = mid;
+                if ((pm.y <= hf_height(hf, pm.x, pm.z, g) + hf.center.y) == below) b = mid; else a = mid;
             }
             float tt = 0.5f * (a + b);
             float3 P = r.o + tt * r.d;
             if (tt >= r.tmin && tt <= r.tmax) {
                 const float e = fmaxf(hf.size_x, hf.size_z) / 256.0f;
-                float hxp = hf_height(hf, P.x + e, P.z), hxm = hf_height(hf, P.x - e, P.z);
-                float hzp = hf_height(hf, P.x, P.z + e), hzm = hf_height(hf, P.x, P.z - e);
+                float hxp = hf_height(hf, P.x + e, P.z, g), hxm = hf_height(hf, P.x - e, P.z, g);
+                float hzp = hf_height(hf, P.x, P.z + e, g), hzm = hf_height(hf, P.x, P.z - e, g);
                 h.t = tt;
                 h.p = P;
                 h.n = normalize(f3(-(hxp - hxm) / (2.0f * e), 1.0f, -(hzp - hzm) / (2.0f * e)));
@@ -771,6 +887,12 @@ __device__ __forceinline__ bool hf_test(const Ray& r, const HeightField& hf, Hit
         if (t > t1) break;
     }
     return false;
+}
+
+// Extension: hf_test over an FP32 height grid, not inlined so that the
+// kernels' code for the reference's heights is unchanged.
+static __device__ __noinline__ bool hf_test_grid(const Ray& r, const HeightField& hf, Hit& h, HfGrid g) {
+    return hf_test(r, hf, h, g);
 }
 
 }  // namespace dev

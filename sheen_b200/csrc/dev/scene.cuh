@@ -102,6 +102,21 @@ struct DevScene {
     int aa_centered;               // camera samples without jitter (extension; 0: the reference's jitter)
     int se_polish;                 // FP64 Newton polish of superellipsoid entries (extension; 0: off)
     int caustic_knn;               // k-nearest-photon gather (extension; 0: the reference's gather)
+
+    // Scene extensions (SheenSceneExt; no counterpart in the reference).
+    // Null / 0 when the scene has none.
+    const float* se_n2;            // per superellipsoid: north-south exponent (> 0: two-exponent body)
+    const int4* hf_grid;           // per heightfield: {offset into hf_heights (< 0: none), w, h, -}
+    const float* hf_heights;
+    const int4* lathe_bz;          // per lathe: {first span, spans, -, -} (spans 0: tessellated)
+    const float4* lathe_bz_bound;  // per lathe: {R, y_lo, y_hi, -} of its exact surface
+    const int4* prism_bz;          // per prism: {first span, spans, -, -}
+    const float4* bz_spans;        // 2 float4 per cubic span: {a0, b0, a1, b1}, {a2, b2, a3, b3}
+    const int* csg_roots;          // further CSG tree roots (closest hit over all trees)
+    int num_csg_roots;
+    const BvhNode* csg_root_bvh;   // median BVH over the further roots' leaf boxes
+    const float4* csg_boxes;       // leaf_kind 2: {lo, material as int}, {hi, 0}
+    const float4* csg_cones;       // leaf_kind 3: {p0, r0}, {p1, r1}, {material as int, 0, 0, 0}
 };
 
 struct Ray {

@@ -437,9 +437,27 @@ __device__ __forceinline__ bool strands_cull(const DevScene& S, const Ray& r, Hi
     return any;
 }
 
+// Extension scenes (SheenSceneExt) walk their categories in functions of
+// their own, not inlined, so that the kernels' code for the reference's
+// shapes is what it is without extensions.
+template <bool COUNT>
+static __device__ __noinline__ bool hfs_cull_ext(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    bool any = false;
+    float best = r.tmax;
+    dfs_cull<COUNT>(S.hf_bvh, r, best, c, [&](int i) {
+        Hit tmp;
+        const HfGrid g = hf_grid_of(S, i);
+        if ((g.h ? hf_test_grid(r, S.hfs[i], tmp, g) : hf_test(r, S.hfs[i], tmp)) && tmp.t < best) {
+            h = tmp; h.obj = -(i + 1); best = tmp.t; any = true;
+        }
+    });
+    return any;
+}
+
 template <bool COUNT>
 __device__ __forceinline__ bool hfs_cull(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
     if (S.num_hfs == 0) return false;
+    if (S.hf_grid) return hfs_cull_ext<COUNT>(S, r, h, c);
     bool any = false;
     float best = r.tmax;
     dfs_cull<COUNT>(S.hf_bvh, r, best, c, [&](int i) {
@@ -450,8 +468,24 @@ __device__ __forceinline__ bool hfs_cull(const DevScene& S, const Ray& r, Hit& h
 }
 
 template <bool COUNT>
+static __device__ __noinline__ bool ses_cull_ext(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    bool any = false;
+    float best = r.tmax;
+    dfs_cull<COUNT>(S.se_bvh, r, best, c, [&](int i) {
+        Hit tmp;
+        const float n2 = se_n2_of(S, i);
+        if ((n2 > 0.0f ? se_test2(r, S.ses[i], n2, tmp) : se_test<true>(r, S.ses[i], tmp, S.se_polish)) &&
+            tmp.t < best) {
+            h = tmp; h.obj = -(i + 1); best = tmp.t; any = true;
+        }
+    });
+    return any;
+}
+
+template <bool COUNT>
 __device__ __forceinline__ bool ses_cull(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
     if (S.num_ses == 0) return false;
+    if (S.se_n2) return ses_cull_ext<COUNT>(S, r, h, c);
     bool any = false;
     float best = r.tmax;
     dfs_cull<COUNT>(S.se_bvh, r, best, c, [&](int i) {
@@ -464,8 +498,27 @@ __device__ __forceinline__ bool ses_cull(const DevScene& S, const Ray& r, Hit& h
 }
 
 template <bool COUNT>
+static __device__ __noinline__ bool lathes_cull_ext(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    bool any = false;
+    float best = r.tmax;
+    const LatheRay lr(r);
+    dfs_cull<COUNT>(S.lathe_bvh, r, best, c, [&](int i) {
+        Hit tmp;
+        const int2 run = lathe_run_of(S, i);
+        const bool ok = run.y > 0 ? lathe_exact_test(r, S.bz_spans, run, __ldg(&S.lathe_bz_bound[i]),
+                                                     S.lathes[i].material_id, tmp)
+                                  : lathe_test_pre(r, lr, S.lathes[i], S.lathe_seg, __ldg(&S.lathe_bound[i]), tmp);
+        if (ok && tmp.t < best) {
+            h = tmp; h.obj = -(i + 1); best = tmp.t; any = true;
+        }
+    });
+    return any;
+}
+
+template <bool COUNT>
 __device__ __forceinline__ bool lathes_cull(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
     if (S.num_lathes == 0) return false;
+    if (S.lathe_bz) return lathes_cull_ext<COUNT>(S, r, h, c);
     bool any = false;
     float best = r.tmax;
     const LatheRay lr(r);
@@ -479,8 +532,22 @@ __device__ __forceinline__ bool lathes_cull(const DevScene& S, const Ray& r, Hit
 }
 
 template <bool COUNT>
+static __device__ __noinline__ bool prisms_cull_ext(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    bool any = false;
+    float best = r.tmax;
+    dfs_cull<COUNT>(S.prism_bvh, r, best, c, [&](int i) {
+        Hit tmp;
+        if (prism_any_test(S, r, i, tmp) && tmp.t < best) {
+            h = tmp; h.obj = -(i + 1); best = tmp.t; any = true;
+        }
+    });
+    return any;
+}
+
+template <bool COUNT>
 __device__ __forceinline__ bool prisms_cull(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
     if (S.num_prisms == 0) return false;
+    if (S.prism_bz) return prisms_cull_ext<COUNT>(S, r, h, c);
     bool any = false;
     float best = r.tmax;
     dfs_cull<COUNT>(S.prism_bvh, r, best, c, [&](int i) {
@@ -522,7 +589,7 @@ struct FastTracer {
         if ((F & kCatSE) && ses_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
         if ((F & kCatLathe) && lathes_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
         if ((F & kCatPrism) && prisms_cull<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-        if ((F & kCatCSG) && S.csg_root >= 0 && ray_meets_box(r, S.csg_lo, S.csg_hi) && csg_test(S, r, t) && t.t < best) { best = t.t; rec = t; hit = true; }
+        if ((F & kCatCSG) && csg_closest(S, r, t, true) && t.t < best) { best = t.t; rec = t; hit = true; }
         if ((F & kCatPlanes) && planes_scan(S, r, t) && t.t < best) { best = t.t; rec = t; hit = true; }
         return hit;
     }
@@ -536,7 +603,7 @@ struct FastTracer {
         }
         if (((F & kCatHF) && hfs_cull<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_cull<COUNT>(S, r, h, c)) ||
             ((F & kCatLathe) && lathes_cull<COUNT>(S, r, h, c)) || ((F & kCatPrism) && prisms_cull<COUNT>(S, r, h, c)) ||
-            ((F & kCatCSG) && S.csg_root >= 0 && ray_meets_box(r, S.csg_lo, S.csg_hi) && csg_test(S, r, h)) || ((F & kCatPlanes) && planes_scan(S, r, h)))
+            ((F & kCatCSG) && csg_closest(S, r, h, true)) || ((F & kCatPlanes) && planes_scan(S, r, h)))
             return classify_shadow_hit(S, h, mask_aware, sh);
         return kClear;
     }
@@ -555,7 +622,7 @@ struct FastTracer {
         Hit h;
         if (((F & kCatHF) && hfs_cull<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_cull<COUNT>(S, r, h, c)) ||
             ((F & kCatLathe) && lathes_cull<COUNT>(S, r, h, c)) || ((F & kCatPrism) && prisms_cull<COUNT>(S, r, h, c)) ||
-            ((F & kCatCSG) && S.csg_root >= 0 && ray_meets_box(r, S.csg_lo, S.csg_hi) && csg_test(S, r, h)) || ((F & kCatPlanes) && planes_scan(S, r, h)))
+            ((F & kCatCSG) && csg_closest(S, r, h, true)) || ((F & kCatPlanes) && planes_scan(S, r, h)))
             return classify_shadow_hit(S, h, mask_aware, sh);
         return kClear;
     }
@@ -566,7 +633,7 @@ struct FastTracer {
         return ((F & kCatHF) && hfs_cull<COUNT>(S, r, h, c)) || ((F & kCatSE) && ses_cull<COUNT>(S, r, h, c)) ||
                ((F & kCatLathe) && lathes_cull<COUNT>(S, r, h, c)) ||
                ((F & kCatPrism) && prisms_cull<COUNT>(S, r, h, c)) ||
-               ((F & kCatCSG) && S.csg_root >= 0 && ray_meets_box(r, S.csg_lo, S.csg_hi) && csg_test(S, r, h)) || ((F & kCatPlanes) && planes_scan(S, r, h));
+               ((F & kCatCSG) && csg_closest(S, r, h, true)) || ((F & kCatPlanes) && planes_scan(S, r, h));
     }
     __device__ __forceinline__ static float strand_depth(const DevScene& S, const Ray& r, Counters& c) {
         return (F & kCatStrands) ? strands_tau_ref<COUNT>(S, r, c) : 0.0f;

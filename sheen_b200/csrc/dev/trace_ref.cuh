@@ -10,6 +10,7 @@
 // between equal-distance primitives resolve the same way.
 #pragma once
 #include "csg.cuh"
+#include "exact.cuh"
 
 namespace sheen {
 namespace dev {
@@ -95,9 +96,27 @@ __device__ __forceinline__ bool mesh_ref(const DevScene& S, const Ray& r, Hit& h
     return true;
 }
 
+// Extension scenes (SheenSceneExt) walk their categories in functions of
+// their own, not inlined, so that the plain kernel's code for the
+// reference's shapes is what it is without extensions.
+template <bool COUNT>
+static __device__ __noinline__ bool hfs_ref_ext(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    bool any = false;
+    float best = r.tmax;
+    dfs_ref<COUNT>(S.hf_bvh, r, c, [&](int i) {
+        Hit tmp;
+        const HfGrid g = hf_grid_of(S, i);
+        if ((g.h ? hf_test_grid(r, S.hfs[i], tmp, g) : hf_test(r, S.hfs[i], tmp)) && tmp.t < best) {
+            h = tmp; h.obj = -(i + 1); best = tmp.t; any = true;
+        }
+    });
+    return any;
+}
+
 template <bool COUNT>
 __device__ __forceinline__ bool hfs_ref(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
     if (S.num_hfs == 0) return false;
+    if (S.hf_grid) return hfs_ref_ext<COUNT>(S, r, h, c);
     bool any = false;
     float best = r.tmax;
     dfs_ref<COUNT>(S.hf_bvh, r, c, [&](int i) {
@@ -108,8 +127,23 @@ __device__ __forceinline__ bool hfs_ref(const DevScene& S, const Ray& r, Hit& h,
 }
 
 template <bool COUNT>
+static __device__ __noinline__ bool ses_ref_ext(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    bool any = false;
+    float best = r.tmax;
+    dfs_ref<COUNT>(S.se_bvh, r, c, [&](int i) {
+        Hit tmp;
+        const float n2 = se_n2_of(S, i);
+        if ((n2 > 0.0f ? se_test2(r, S.ses[i], n2, tmp) : se_test(r, S.ses[i], tmp, S.se_polish)) && tmp.t < best) {
+            h = tmp; h.obj = -(i + 1); best = tmp.t; any = true;
+        }
+    });
+    return any;
+}
+
+template <bool COUNT>
 __device__ __forceinline__ bool ses_ref(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
     if (S.num_ses == 0) return false;
+    if (S.se_n2) return ses_ref_ext<COUNT>(S, r, h, c);
     bool any = false;
     float best = r.tmax;
     dfs_ref<COUNT>(S.se_bvh, r, c, [&](int i) {
@@ -122,8 +156,22 @@ __device__ __forceinline__ bool ses_ref(const DevScene& S, const Ray& r, Hit& h,
 }
 
 template <bool COUNT>
+static __device__ __noinline__ bool lathes_ref_ext(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    bool any = false;
+    float best = r.tmax;
+    dfs_ref<COUNT>(S.lathe_bvh, r, c, [&](int i) {
+        Hit tmp;
+        if (lathe_any_test(S, r, i, tmp) && tmp.t < best) {
+            h = tmp; h.obj = -(i + 1); best = tmp.t; any = true;
+        }
+    });
+    return any;
+}
+
+template <bool COUNT>
 __device__ __forceinline__ bool lathes_ref(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
     if (S.num_lathes == 0) return false;
+    if (S.lathe_bz) return lathes_ref_ext<COUNT>(S, r, h, c);
     bool any = false;
     float best = r.tmax;
     dfs_ref<COUNT>(S.lathe_bvh, r, c, [&](int i) {
@@ -136,8 +184,22 @@ __device__ __forceinline__ bool lathes_ref(const DevScene& S, const Ray& r, Hit&
 }
 
 template <bool COUNT>
+static __device__ __noinline__ bool prisms_ref_ext(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    bool any = false;
+    float best = r.tmax;
+    dfs_ref<COUNT>(S.prism_bvh, r, c, [&](int i) {
+        Hit tmp;
+        if (prism_any_test(S, r, i, tmp) && tmp.t < best) {
+            h = tmp; h.obj = -(i + 1); best = tmp.t; any = true;
+        }
+    });
+    return any;
+}
+
+template <bool COUNT>
 __device__ __forceinline__ bool prisms_ref(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
     if (S.num_prisms == 0) return false;
+    if (S.prism_bz) return prisms_ref_ext<COUNT>(S, r, h, c);
     bool any = false;
     float best = r.tmax;
     dfs_ref<COUNT>(S.prism_bvh, r, c, [&](int i) {
@@ -176,7 +238,7 @@ __device__ __noinline__ bool closest_ref(const DevScene& S, const Ray& r, Hit& r
     if (ses_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
     if (lathes_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
     if (prisms_ref<COUNT>(S, r, t, c) && t.t < best) { best = t.t; rec = t; hit = true; }
-    if (S.csg_root >= 0 && csg_test(S, r, t) && t.t < best) { best = t.t; rec = t; hit = true; }
+    if (csg_closest(S, r, t, false) && t.t < best) { best = t.t; rec = t; hit = true; }
     if (planes_scan(S, r, t) && t.t < best) { best = t.t; rec = t; hit = true; }
     return hit;
 }
@@ -191,7 +253,7 @@ __device__ __noinline__ bool opaque_ref(const DevScene& S, const Ray& r, Hit& re
     if (ses_ref<COUNT>(S, r, rec, c)) return true;
     if (lathes_ref<COUNT>(S, r, rec, c)) return true;
     if (prisms_ref<COUNT>(S, r, rec, c)) return true;
-    if (S.csg_root >= 0 && csg_test(S, r, rec)) return true;
+    if (csg_closest(S, r, rec, false)) return true;
     return planes_scan(S, r, rec);
 }
 

@@ -103,6 +103,8 @@ struct DeviceScene {
 cudaError_t build_wave_meshes_device(DeviceScene& s, cudaStream_t stream);
 
 int scene_upload(const SheenScene* in, int form, DeviceScene** out);
+// With scene extensions (ext may be null).
+int scene_upload_ext(const SheenScene* in, const SheenSceneExt* ext, int form, DeviceScene** out);
 void release_upload_rings();
 void scene_release(DeviceScene* s);
 
@@ -195,9 +197,10 @@ struct Tuning {
     int aa_centered = 0;            // camera samples: 0 the reference's jitter, 1 cell centres
     int se_polish = 0;              // superellipsoid entries: 0 on a sample (reference), 1 FP64 Newton polish
     int caustic_knn = 0;            // caustic gather: 0 the reference's, k in 1..64 the k nearest photons
-    int shadow_cache = 0;           // refill shadow stage: 1 tests each warp's last occluder leaf first
-    int mega_samples = 0;           // wavefront frames of at most this many samples (tile-padded pixels x spp)
-                                    // run on the BVH4 megakernel (one launch) instead of the queue stages
+    int tile_w = 16;                // wavefront sample order: width of the 128-pixel tiles (8, 16 or 32)
+    int mega_samples = 327680;      // wavefront frames of at most this many samples (tile-padded pixels x spp;
+                                    // a quarter of it for scenes with triangles) run on the BVH4 megakernel
+                                    // (one launch) instead of the queue stages; 0: never
 };
 Tuning tuning();
 int tuning_generation();

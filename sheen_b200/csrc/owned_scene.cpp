@@ -52,6 +52,25 @@ void OwnedScene::finalize() {
     SHEEN_VIEW(media)
 #undef SHEEN_VIEW
     v.csg_root = csg_root;
+    {
+        SheenSceneExt& x = ext_view;
+        std::memset(&x, 0, sizeof(x));
+        auto ptr = [](const auto& vec) { return vec.empty() ? nullptr : vec.data(); };
+        x.lathe_bezier = ptr(lathe_bezier);
+        x.prism_bezier = ptr(prism_bezier);
+        x.bezier_ctrl = ptr(bezier_ctrl);
+        x.num_bezier_ctrl = (int)(bezier_ctrl.size() / 2);
+        x.se_n2 = ptr(se_n2);
+        x.hf_grid = ptr(hf_grid);
+        x.hf_heights = ptr(hf_heights);
+        x.num_hf_heights = (int)hf_heights.size();
+        x.csg_roots = ptr(csg_roots);
+        x.num_csg_roots = (int)csg_roots.size();
+        x.csg_boxes = ptr(csg_boxes);
+        x.num_csg_boxes = (int)csg_boxes.size();
+        x.csg_cones = ptr(csg_cones);
+        x.num_csg_cones = (int)csg_cones.size();
+    }
     v.texture_pixels = tex_ptrs.empty() ? nullptr : tex_ptrs.data();
     v.texture_widths = tex_w.empty() ? nullptr : tex_w.data();
     v.texture_heights = tex_h.empty() ? nullptr : tex_h.data();
@@ -216,6 +235,10 @@ extern "C" {
 
 const SheenScene* sheen_owned_view(SheenOwnedScene s) {
     return s ? &reinterpret_cast<sheen::OwnedScene*>(s)->view : nullptr;
+}
+
+const SheenSceneExt* sheen_owned_ext(SheenOwnedScene s) {
+    return s ? &reinterpret_cast<sheen::OwnedScene*>(s)->ext_view : nullptr;
 }
 
 const SheenSceneSettings* sheen_owned_settings(SheenOwnedScene s) {

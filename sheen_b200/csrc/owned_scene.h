@@ -38,8 +38,19 @@ struct OwnedScene {
     std::vector<Medium> media;
     SheenSceneSettings settings{};
 
-    // C view (rebuilt by finalize()).
+    // Scene extensions (SheenSceneExt; the extended generators fill them).
+    std::vector<SheenBezierRun> lathe_bezier, prism_bezier;
+    std::vector<float> bezier_ctrl;          // (a, b) pairs
+    std::vector<float> se_n2;
+    std::vector<SheenHeightGrid> hf_grid;
+    std::vector<float> hf_heights;
+    std::vector<int> csg_roots;
+    std::vector<SheenCsgBox> csg_boxes;
+    std::vector<SheenCsgCone> csg_cones;
+
+    // C views (rebuilt by finalize()).
     SheenScene view{};
+    SheenSceneExt ext_view{};
     std::vector<const unsigned char*> tex_ptrs;
     std::vector<int> tex_w, tex_h;
 

@@ -98,7 +98,7 @@ cudaError_t launch_mega_bvh4(const DeviceScene& s, int W, int H, int aa, Region 
     const dim3 grid((rg.x1 - rg.x0 + 15) / 16, (rg.y1 - rg.y0 + 7) / 8);
     const dev::DevScene& v = s.view;
     const bool simple = v.num_strands == 0 && v.num_hfs == 0 && v.num_ses == 0 && v.num_lathes == 0 &&
-                        v.num_prisms == 0 && v.csg_root < 0;
+                        v.num_prisms == 0 && v.csg_root < 0 && v.num_csg_roots == 0;
     const bool wt = v.q_all.watertight != 0;
     const bool basic = simple && v.num_tris == 0;
 #define MEGA(C, F) dev::mega_bvh4_kernel<C, F><<<grid, block, 0, stream>>>(v, out, W, H, aa, rg.x0, rg.y0, rg.x1, \

@@ -65,6 +65,7 @@ struct WaveView {
     int nsamples;          // rw * rh * ns
     float pix_angle;
     int count_rays;
+    int tw_log2;           // log2 of the pixel tile's width (tiles of 128 pixels: 8x16, 16x8 or 32x4)
     // Multi-job launches (the MULTI kernels): the job table.  nsamples is
     // then the total over all jobs, npix the total of their padded pixels,
     // and the queues and counters above are shared; every per-frame field
@@ -133,16 +134,18 @@ __device__ __forceinline__ int claim_batch(unsigned int* head) {
     return (int)__shfl_sync(0xffffffffu, b, 0);
 }
 
-// Sample index -> pixel and sample number.  Pixels are walked in 16x8 tiles
-// so a warp's primary rays are coherent.
+// Sample index -> pixel and sample number.  Pixels are walked in tiles of
+// 128 (16x8 by default; the "wave.tile_w" launch parameter picks 8x16 or
+// 32x4) so a warp's primary rays are coherent.
 __device__ __forceinline__ void sample_pixel(const WaveView& V, int i, int& x, int& y, int& s) {
     s = i % V.ns;
     const int p = i / V.ns;
-    const int tiles_x = (V.rw + 15) / 16;
-    const int tile = p / 128, in = p % 128;
+    const int tw = 1 << V.tw_log2;
+    const int tiles_x = (V.rw + tw - 1) >> V.tw_log2;
+    const int tile = p >> 7, in = p & 127;
     const int tx = tile % tiles_x, ty = tile / tiles_x;
-    x = V.x0 + tx * 16 + (in % 16);
-    y = V.y0 + ty * 8 + (in / 16);
+    x = V.x0 + tx * tw + (in & (tw - 1));
+    y = V.y0 + ty * (128 >> V.tw_log2) + (in >> V.tw_log2);
 }
 
 __device__ __forceinline__ bool sample_valid(const WaveView& V, int x, int y) {
@@ -370,19 +373,9 @@ __global__ void __launch_bounds__(128) wave_shadow(DevScene S0, WaveView V0) {
 // local memory, whose scattered stores fill L1 with 32-byte sectors carrying
 // 4 useful bytes; the entry distances (closest-hit walks of the passable set
 // only) stay in local memory.  24 KB per 128-thread block.
-//
-// With `occluder_cache`, each warp remembers the leaf (and the job whose
-// tree it belongs to) where one of its lanes last found a blocking
-// triangle, and a lane starting an any-hit walk of that job's blocking tree
-// tests that leaf's triangles first.  Neighbouring queue entries are
-// neighbouring samples towards the same light, whose occluders are usually
-// the same few triangles.  Any blocking hit before the passable one decides
-// the query, and the cached triangles are in the tree the walk would search
-// (their leaf box holds them), so the result is the walk's: a hit there is
-// one the walk would have found, a miss falls through to the walk.
 template <int F, bool SMEM_STACK, bool MULTI>
 __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveView V0, int refill_min,
-                                                             int inner_min, int occluder_cache) {
+                                                             int inner_min) {
     using T = FastTracer<false, F>;
     constexpr unsigned int kFull = 0xffffffffu;
     constexpr uint32_t kLeafBit = 0x80000000u;
@@ -429,34 +422,6 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveVi
         else return stack_e_local[i];
     };
 
-    __shared__ unsigned long long occ_leaf[4];   // per warp: job << 32 | leaf entry; ~0: none
-    unsigned long long& occ = occ_leaf[threadIdx.x >> 5];
-    if (lane == 0) occ = ~0ull;
-    __syncwarp();
-    // A fresh any-hit walk (wn / wt / t_best set up): the cached leaf first.
-    auto cached_block_hit = [&]() -> bool {
-        if (!occluder_cache) return false;
-        const unsigned long long k = occ;
-        if ((unsigned int)(k >> 32) != (unsigned int)job) return false;
-        const uint32_t le = (uint32_t)k;
-        const int first = (int)((le & 0x7fffffffu) >> 3);
-        const int count = (int)(le & 7u) + 1;
-        for (int i = 0; i < count; i++) {
-            const int s = first + i;
-            const float4 a = __ldg(&wt[3 * s]);
-            const float4 b = __ldg(&wt[3 * s + 1]);
-            const float4 c4 = __ldg(&wt[3 * s + 2]);
-            float t, u, v;
-            if (qtri_test<tri_of<F>()>(q, a, b, c4, q.tmin, tmax, t, u, v, scene().q_all.watertight) &&
-                t < t_best) {
-                t_best = t; wu = u; wv = v;
-                wbest = __float_as_int(a.w);
-                return true;
-            }
-        }
-        return false;
-    };
-
     bool exhausted = false;
     for (;;) {
         // ---- refill idle lanes ------------------------------------------
@@ -499,8 +464,7 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveVi
                 state = kWalkBlock; block_after_pass = true;
                 wn = scene().q_block.nodes; wt = scene().q_block.tris;
                 entry = 0; sp = 0; wbest = -1; t_best = tp;
-                if (cached_block_hit()) state = kEndBlock;
-                res = -3;   // keep walking (or settle the cached hit next round)
+                res = -3;   // keep walking
             } else {
                 if (state == kEndPass) { pass_tri = wbest; tp = t_best; up = wu; vp = wv; }
                 res = (state == kEndBlock && wbest >= 0) ? kBlocked : kClear;
@@ -529,7 +493,6 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveVi
                         } else {
                             state = kWalkBlock; block_after_pass = false;
                             wn = scene().q_all.nodes; wt = scene().q_all.tris;
-                            if (cached_block_hit()) state = kEndBlock;
                         }
                         break;
                     }
@@ -627,11 +590,7 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveVi
                     t < t_best) {
                     t_best = t; wu = u; wv = v;
                     wbest = __float_as_int(a.w);
-                    if (state == kWalkBlock) {
-                        if (occluder_cache) occ = ((unsigned long long)(unsigned int)job << 32) | entry;
-                        ended = true;
-                        break;
-                    }
+                    if (state == kWalkBlock) { ended = true; break; }
                 }
             }
             if (!ended) {
@@ -976,11 +935,10 @@ static cudaError_t run_pipeline(const dev::DevScene& S0, const dev::WaveView& V,
         if (!refill)
             dev::wave_shadow<F, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V);
         else if (smem)
-            dev::wave_shadow_refill<F, true, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V, tu.refill_min, tu.inner_min,
-                                                                                 tu.shadow_cache);
+            dev::wave_shadow_refill<F, true, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V, tu.refill_min, tu.inner_min);
         else
             dev::wave_shadow_refill<F, false, MULTI><<<g_shadow, 128, 0, stream>>>(S0, V, tu.refill_min,
-                                                                                  tu.inner_min, tu.shadow_cache);
+                                                                                  tu.inner_min);
     };
     int mark = 0;
     auto stage_end = [&]() {
@@ -1122,22 +1080,31 @@ static cudaError_t wave_reserve_into(Wave*& w, int L, long long nsamples, int de
     return cudaSuccess;
 }
 
-static long long region_padded(Region rg) {
-    const int rw = rg.x1 - rg.x0, rh = rg.y1 - rg.y0;
-    return (long long)((rw + 15) / 16) * 16 * ((rh + 7) / 8) * 8;
+// The pixel tile of the sample order: log2 of its width (3, 4 or 5; tiles
+// of 128 pixels), read once per frame from the launch parameters.
+static int tile_log2() {
+    const int w = tuning().tile_w;
+    return w == 8 ? 3 : (w == 32 ? 5 : 4);
+}
+
+static long long region_padded(Region rg, int twl) {
+    const long long tw = 1ll << twl, th = 128ll >> twl;
+    const long long rw = rg.x1 - rg.x0, rh = rg.y1 - rg.y0;
+    return (rw + tw - 1) / tw * tw * ((rh + th - 1) / th) * th;
 }
 
 static int clamp_spp(int aa) { return aa < 1 ? 1 : (aa > 64 ? 64 : aa); }
 
 // Queue view of one frame region; the region's pixels are walked in whole
-// 16x8 tiles (sample_pixel), so its sample count is padded to them.
-static dev::WaveView make_view(const DeviceScene& s, const Wave& w, int W, int H, int ns, Region rg) {
+// tiles of 128 (sample_pixel), so its sample count is padded to them.
+static dev::WaveView make_view(const DeviceScene& s, const Wave& w, int W, int H, int ns, Region rg, int twl) {
     dev::WaveView V;
     V.slots = w.slots; V.coef = w.coef; V.shq = w.shq; V.rq = w.rq; V.tq = w.tq; V.ctr = w.ctr;
     V.L = s.view.num_lights;
     V.ns = ns;
     V.W = W; V.H = H; V.x0 = rg.x0; V.y0 = rg.y0; V.rw = rg.x1 - rg.x0; V.rh = rg.y1 - rg.y0;
-    V.nsamples = (int)(region_padded(rg) * ns);
+    V.nsamples = (int)(region_padded(rg, twl) * ns);
+    V.tw_log2 = twl;
     const CameraData& cam = s.view.cam;
     float tan_x = 1.0f;
     if (cam.focal_length > 0.0f) {
@@ -1173,7 +1140,7 @@ static bool watertight_scene(const DeviceScene& s) { return s.view.q_all.waterti
 static bool simple_scene(const DeviceScene& s) {
     const dev::DevScene& sv = s.view;
     return sv.num_strands == 0 && sv.num_hfs == 0 && sv.num_ses == 0 && sv.num_lathes == 0 && sv.num_prisms == 0 &&
-           sv.csg_root < 0;
+           sv.csg_root < 0 && sv.num_csg_roots == 0;
 }
 
 // Small frames run on the BVH4 megakernel: below wave.mega_samples samples
@@ -1190,16 +1157,17 @@ static bool small_frame(const DeviceScene& s, long long nsamples) {
 
 cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
                              bool count_nodes) {
+    const int twl = tile_log2();
     if (!wave_supported(s) || count_nodes) return launch_mega_bvh4(s, W, H, aa, rg, out, stream, count_nodes);
     const int ns = clamp_spp(aa);
-    const long long nsamples = region_padded(rg) * ns;
+    const long long nsamples = region_padded(rg, twl) * ns;
     if (nsamples > (1ll << 30)) return cudaErrorInvalidValue;
     if (small_frame(s, nsamples)) return launch_mega_bvh4(s, W, H, aa, rg, out, stream, false);
     cudaError_t e = wave_reserve_into(s.wave, s.view.num_lights, nsamples, s.device);
     if (e != cudaSuccess) return e;
     Wave* w = s.wave;
-    const dev::WaveView V = make_view(s, *w, W, H, ns, rg);
-    const int npad = (int)region_padded(rg);
+    const dev::WaveView V = make_view(s, *w, W, H, ns, rg, twl);
+    const int npad = (int)region_padded(rg, twl);
     const bool simple = simple_scene(s);
     // Replay the captured frame when the shape and output match.  A shape
     // seen for the first time is launched directly; on its second frame the
@@ -1248,11 +1216,12 @@ bool wave_pipeline_used(const DeviceScene& s) { return wave_supported(s); }
 // differently.  Scratch comes from the library's pool, ordered on `stream`.
 template <int F>
 static cudaError_t batch_pass(const std::vector<BatchItem>& items, cudaStream_t stream, unsigned long long* tally) {
+    const int twl = tile_log2();
     const int n = (int)items.size();
     if (n == 0) return cudaSuccess;
     long long total_samples = 0, total_pix = 0, slot_floats = 0, shadow_entries = 0;
     for (const BatchItem& it : items) {
-        const long long npad = region_padded(it.rg), ns = clamp_spp(it.aa);
+        const long long npad = region_padded(it.rg, twl), ns = clamp_spp(it.aa);
         const int L = it.s->view.num_lights;
         total_samples += npad * ns;
         total_pix += npad;
@@ -1291,11 +1260,11 @@ static cudaError_t batch_pass(const std::vector<BatchItem>& items, cudaStream_t 
         dev::JobDesc& J = jobs[(size_t)j];
         std::memset(&J, 0, sizeof(J));
         J.S = it.s->view;
-        J.V = make_view(*it.s, w, it.W, it.H, ns, it.rg);
+        J.V = make_view(*it.s, w, it.W, it.H, ns, it.rg, twl);
         J.out = it.out;
         J.sample_base = (int)sample_off;
         J.pix_base = (int)pix_off;
-        const long long npad = region_padded(it.rg);
+        const long long npad = region_padded(it.rg, twl);
         sample_off += npad * ns;
         pix_off += npad;
         slot_off += npad * ns * 3 * (it.s->view.num_lights + 2) * 3;
@@ -1339,15 +1308,16 @@ cudaError_t launch_wavefront_batch(const std::vector<BatchItem>& items, cudaStre
 // at the stage boundaries and the ray counters read after every kernel.
 cudaError_t profile_wavefront(DeviceScene& s, int W, int H, int aa, float4* out, cudaStream_t stream,
                               SheenStageProfile* prof) {
+    const int twl = tile_log2();
     if (!wave_supported(s)) return cudaErrorNotSupported;
     const int ns = clamp_spp(aa);
     const Region rg{0, 0, W, H};
-    const long long nsamples = region_padded(rg) * ns;
+    const long long nsamples = region_padded(rg, twl) * ns;
     if (nsamples > (1ll << 30)) return cudaErrorInvalidValue;
     cudaError_t e = wave_reserve_into(s.wave, s.view.num_lights, nsamples, s.device);
     if (e != cudaSuccess) return e;
-    const dev::WaveView V = make_view(s, *s.wave, W, H, ns, rg);
-    const int npad = (int)region_padded(rg);
+    const dev::WaveView V = make_view(s, *s.wave, W, H, ns, rg, twl);
+    const int npad = (int)region_padded(rg, twl);
     cudaEvent_t ev[8] = {nullptr};
     unsigned int* snap = nullptr;
     for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&ev[i]);
@@ -1395,15 +1365,16 @@ cudaError_t profile_wavefront(DeviceScene& s, int W, int H, int aa, float4* out,
 
 cudaError_t launch_wavefront_scratch(DeviceScene& s, void* scratch, size_t scratch_bytes, int W, int H, int aa,
                                      Region rg, float4* out, cudaStream_t stream, unsigned long long* tally) {
+    const int twl = tile_log2();
     if (!wave_supported(s)) return launch_mega_bvh4(s, W, H, aa, rg, out, stream, false, tally);
     const int ns = clamp_spp(aa);
-    const long long nsamples = region_padded(rg) * ns;
+    const long long nsamples = region_padded(rg, twl) * ns;
     if (nsamples > (1ll << 30)) return cudaErrorInvalidValue;
     if (small_frame(s, nsamples)) return launch_mega_bvh4(s, W, H, aa, rg, out, stream, false, tally);
     Wave w;
     if (!wave_carve(w, scratch, scratch_bytes, s.view.num_lights, nsamples)) return cudaErrorInvalidValue;
-    const dev::WaveView V = make_view(s, w, W, H, ns, rg);
-    const int npad = (int)region_padded(rg);
+    const dev::WaveView V = make_view(s, w, W, H, ns, rg, twl);
+    const int npad = (int)region_padded(rg, twl);
     return dispatch_variant(simple_scene(s), watertight_scene(s), [&](auto f) {
         return run_pipeline<decltype(f)::value>(s.view, V, npad, out, stream, tally);
     });
@@ -1424,7 +1395,8 @@ cudaError_t launch_wavefront_scratch(DeviceScene& s, void* scratch, size_t scrat
 // carved from one fixed array in the library's device globals instead.
 //
 // Limits: at most kNoAllocMaxSamples samples per call (the region's pixels
-// rounded up to whole 16x8 tiles, times the samples per pixel -- e.g. a
+// rounded up to whole 128-pixel tiles, 16x8 by default, times the samples
+// per pixel -- e.g. a
 // 128x128 tile at 1 spp or 64x64 at 4 spp) and scenes with at most
 // kNoAllocMaxLights lights.  The array (about 13 MB) is held on every GPU
 // that loads the library until the process exits.  Every call uses the same
@@ -1479,6 +1451,7 @@ void release_noalloc_scratch() {
 extern "C" int sheen_scene_render_region_noalloc(SheenDeviceScene h, int W, int H, int aa, int x0, int y0, int x1,
                                                  int y1, float* out_rgba_device, void* stream) {
     using namespace sheen;
+    const int twl = tile_log2();
     auto* s = reinterpret_cast<DeviceScene*>(h);
     if (!s) { set_error("null scene handle"); return -1; }
     if (W <= 0 || H <= 0 || aa < 1 || aa > 64 || !out_rgba_device) { set_error("bad render params"); return -1; }
@@ -1488,10 +1461,10 @@ extern "C" int sheen_scene_render_region_noalloc(SheenDeviceScene h, int W, int 
         return -1;
     }
     const Region rg{x0, y0, x1, y1};
-    const long long nsamples = region_padded(rg) * aa;
+    const long long nsamples = region_padded(rg, twl) * aa;
     if (nsamples > kNoAllocMaxSamples) {
         set_error("region too large for allocation-free rendering: at most 16384 samples per call "
-                  "(pixels rounded up to whole 16x8 tiles, times samples per pixel)");
+                  "(pixels rounded up to whole 128-pixel tiles, 16x8 by default, times samples per pixel)");
         return -1;
     }
     if (s->view.num_lights > kNoAllocMaxLights) {

@@ -312,18 +312,24 @@ void gen_caustics(OwnedScene& s, uint32_t seed, int photons) {
 }  // namespace
 
 namespace sheen {
-void gen_analytic(OwnedScene& s, uint32_t seed, int detail);
+void gen_analytic(OwnedScene& s, uint32_t seed, int detail, bool extended);
 }
 
 extern "C" int sheen_generate_scene(int config, unsigned int seed, int detail, int photons,
                                     SheenOwnedScene* out) {
+    return sheen_generate_scene_ext(config, seed, detail, photons, 0, out);
+}
+
+extern "C" int sheen_generate_scene_ext(int config, unsigned int seed, int detail, int photons, int extended,
+                                        SheenOwnedScene* out) {
     if (!out) { sheen::set_error("null output handle"); return -1; }
     *out = nullptr;
+    if (extended && config != 2) { sheen::set_error("extended generator exists for config 2 only"); return -1; }
     OwnedScene* s = new OwnedScene();
     switch (config) {
         case 0: gen_spheres(*s, seed); break;
         case 1: gen_mesh(*s, seed, detail > 0 ? detail : 8); break;
-        case 2: sheen::gen_analytic(*s, seed, detail); break;
+        case 2: sheen::gen_analytic(*s, seed, detail, extended != 0); break;
         case 3: gen_caustics(*s, seed, photons > 0 ? photons : 4000000); break;
         default:
             delete s;

@@ -8,6 +8,15 @@
 // paths, one procedural fBm heightfield, and one CSG tree of depth 3 over
 // spheres and superellipsoid boxes (n = 12).  Lathes keep center = 0: the
 // reference's lathe test ignores Lathe.center, so they share the Y axis.
+//
+// extended (the workload's extension column, no counterpart in the
+// reference): the same scene with two-exponent superellipsoids (both
+// exponents 2/e, e uniform in [0.2, 3]), the lathes' and prisms' Bezier
+// control points kept as exact surfaces, a 1024 x 1024 FP32 fBm height grid
+// for the heightfield, and 128 further CSG trees of depth 3 over spheres,
+// boxes and cones.  Its draws come from a second generator stream, so the
+// base geometry is the base scene's.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -43,9 +52,47 @@ std::vector<std::pair<float, float>> bezier_run(const std::vector<std::pair<floa
 }
 }  // namespace
 
-void gen_analytic(OwnedScene& s, uint32_t seed, int detail) {
+// Seeded value-noise fBm on the unit square, normalised to [0, 1] over the
+// grid (the extension's FP32 height grid).
+static void fbm_grid(uint32_t seed, int w, int h, std::vector<float>& out) {
+    auto hash = [seed](int x, int z) {
+        uint32_t v = (uint32_t)x * 0x8da6b343u ^ (uint32_t)z * 0xd8163841u ^ seed * 0xcb1ab31fu;
+        v ^= v >> 15; v *= 0x2c1b3c6du; v ^= v >> 12; v *= 0x297a2d39u; v ^= v >> 15;
+        return (float)(v >> 8) * (1.0f / 16777216.0f);
+    };
+    auto noise = [&](float x, float z) {
+        const int x0 = (int)std::floor(x), z0 = (int)std::floor(z);
+        float tx = x - (float)x0, tz = z - (float)z0;
+        tx = tx * tx * (3.0f - 2.0f * tx);
+        tz = tz * tz * (3.0f - 2.0f * tz);
+        const float a = hash(x0, z0) + (hash(x0 + 1, z0) - hash(x0, z0)) * tx;
+        const float b = hash(x0, z0 + 1) + (hash(x0 + 1, z0 + 1) - hash(x0, z0 + 1)) * tx;
+        return a + (b - a) * tz;
+    };
+    out.assign((size_t)w * h, 0.0f);
+    float lo = 1e30f, hi = -1e30f;
+    for (int v = 0; v < h; v++)
+        for (int u = 0; u < w; u++) {
+            float fx = 6.0f * (float)u / (float)(w - 1), fz = 6.0f * (float)v / (float)(h - 1);
+            float amp = 0.5f, sum = 0.0f;
+            for (int o = 0; o < 6; o++) {
+                sum += amp * noise(fx + 17.0f * o, fz + 31.0f * o);
+                amp *= 0.5f;
+                fx *= 2.0f;
+                fz *= 2.0f;
+            }
+            out[(size_t)v * w + u] = sum;
+            lo = std::min(lo, sum);
+            hi = std::max(hi, sum);
+        }
+    const float span = hi > lo ? hi - lo : 1.0f;
+    for (float& x : out) x = (x - lo) / span;
+}
+
+void gen_analytic(OwnedScene& s, uint32_t seed, int detail, bool extended) {
     (void)detail;
     R rng(seed);
+    R rng2(seed * 2654435761u ^ 0x5bd1e995u);   // the extensions' stream
     {
         CameraData c;
         std::memset(&c, 0, sizeof(c));
@@ -79,6 +126,10 @@ void gen_analytic(OwnedScene& s, uint32_t seed, int detail) {
         se.a = rng.uni(0.3f, 0.8f); se.b = rng.uni(0.3f, 0.8f); se.c = rng.uni(0.3f, 0.8f);
         se.n = 2.0f / rng.uni(0.2f, 2.0f);
         se.material_id = i % 7;
+        if (extended) {
+            se.n = 2.0f / rng2.uni(0.2f, 3.0f);
+            s.se_n2.push_back(2.0f / rng2.uni(0.2f, 3.0f));
+        }
         s.superellipsoids.push_back(se);
     }
     for (int i = 0; i < 64; i++) {
@@ -89,6 +140,10 @@ void gen_analytic(OwnedScene& s, uint32_t seed, int detail) {
             ctrl.push_back({y, rng.uni(0.1f, 1.6f)});
         }
         auto line = bezier_run(ctrl, 8);
+        if (extended) {
+            s.lathe_bezier.push_back({(int)(s.bezier_ctrl.size() / 2), (int)ctrl.size()});
+            for (auto& q : ctrl) { s.bezier_ctrl.push_back(q.first); s.bezier_ctrl.push_back(q.second); }
+        }
         Lathe l;
         std::memset(&l, 0, sizeof(l));
         l.point_offset = (int)s.lathe_points.size();
@@ -111,6 +166,10 @@ void gen_analytic(OwnedScene& s, uint32_t seed, int detail) {
         }
         auto line = bezier_run(ctrl, 8);
         if (!line.empty()) line.push_back(line.front());   // closed contour
+        if (extended) {
+            s.prism_bezier.push_back({(int)(s.bezier_ctrl.size() / 2), (int)ctrl.size()});
+            for (auto& q : ctrl) { s.bezier_ctrl.push_back(q.first); s.bezier_ctrl.push_back(q.second); }
+        }
         Prism p;
         std::memset(&p, 0, sizeof(p));
         p.center = {rng.uni(-18.0f, 18.0f), 0.0f, rng.uni(-4.0f, 16.0f)};
@@ -148,6 +207,13 @@ void gen_analytic(OwnedScene& s, uint32_t seed, int detail) {
         hf.material_id = m_ground;
         s.heightfields.push_back(hf);
         s.height_image_of.push_back(-1);
+        if (extended) {
+            const int gw = 1024, gh = 1024;
+            s.hf_grid.push_back({(int)s.hf_heights.size(), gw, gh});
+            std::vector<float> g;
+            fbm_grid(rng2.g(), gw, gh, g);
+            s.hf_heights.insert(s.hf_heights.end(), g.begin(), g.end());
+        }
     }
     {
         // Depth-3 tree: difference(intersection(box, sphere), union(sphere, box)).
@@ -183,6 +249,59 @@ void gen_analytic(OwnedScene& s, uint32_t seed, int detail) {
         int inter = op(1, a, b);
         int uni = op(0, c, d);
         s.csg_root = op(2, inter, uni);
+        if (extended) {
+            // 128 further trees of depth 3: op(op(leaf, leaf), op(leaf, leaf))
+            // over spheres (Objects of type 1: CSG-only, not drawn as spheres),
+            // boxes and cones
+            auto ext_leaf = [&](float cx, float cy, float cz, float size, int mat) {
+                const int kind = (int)(rng2.u01() * 3.0f) % 3;
+                const float ox = rng2.uni(-0.5f, 0.5f) * size, oy = rng2.uni(-0.5f, 0.5f) * size;
+                const float oz = rng2.uni(-0.5f, 0.5f) * size;
+                if (kind == 0) {
+                    Object o;
+                    std::memset(&o, 0, sizeof(o));
+                    o.type = 1;
+                    o.material_id = mat;
+                    o.param1 = {cx + ox, cy + oy, cz + oz};
+                    o.param2 = rng2.uni(0.35f, 0.7f) * size;
+                    s.objects.push_back(o);
+                    return leaf(0, (int)s.objects.size() - 1);
+                }
+                if (kind == 1) {
+                    SheenCsgBox b;
+                    std::memset(&b, 0, sizeof(b));
+                    const float hx = rng2.uni(0.25f, 0.6f) * size, hy = rng2.uni(0.25f, 0.6f) * size;
+                    const float hz = rng2.uni(0.25f, 0.6f) * size;
+                    b.lo = {cx + ox - hx, cy + oy - hy, cz + oz - hz};
+                    b.hi = {cx + ox + hx, cy + oy + hy, cz + oz + hz};
+                    b.material_id = mat;
+                    s.csg_boxes.push_back(b);
+                    return leaf(2, (int)s.csg_boxes.size() - 1);
+                }
+                SheenCsgCone cn;
+                std::memset(&cn, 0, sizeof(cn));
+                const float hh = rng2.uni(0.4f, 0.9f) * size;
+                float ax = rng2.uni(-0.4f, 0.4f), az = rng2.uni(-0.4f, 0.4f);
+                cn.p0 = {cx + ox - ax * hh, cy + oy - hh, cz + oz - az * hh};
+                cn.p1 = {cx + ox + ax * hh, cy + oy + hh, cz + oz + az * hh};
+                cn.r0 = rng2.uni(0.2f, 0.6f) * size;
+                cn.r1 = rng2.uni(0.0f, 0.4f) * size;
+                cn.material_id = mat;
+                s.csg_cones.push_back(cn);
+                return leaf(3, (int)s.csg_cones.size() - 1);
+            };
+            for (int t = 0; t < 128; t++) {
+                const float cx = rng2.uni(-17.0f, 17.0f), cy = rng2.uni(0.8f, 5.0f), cz = rng2.uni(-5.0f, 17.0f);
+                const float size = rng2.uni(0.5f, 1.1f);
+                const int mat = t % 7;
+                const int l0 = ext_leaf(cx, cy, cz, size, mat), l1 = ext_leaf(cx, cy, cz, size, mat);
+                const int l2 = ext_leaf(cx, cy, cz, size, mat), l3 = ext_leaf(cx, cy, cz, size, mat);
+                const int a0 = op((int)(rng2.u01() * 3.0f) % 3, l0, l1);
+                const int a1 = op((int)(rng2.u01() * 3.0f) % 3, l2, l3);
+                // the top operation keeps some solid: union or intersection-free difference
+                s.csg_roots.push_back(op(rng2.u01() < 0.5f ? 0 : 2, a0, a1));
+            }
+        }
     }
     s.add_plane(0.0f, 1.0f, 0.0f, 0.5f, m_ground);
     for (int k = 0; k < 2; k++) {

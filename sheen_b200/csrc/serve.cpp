@@ -13,7 +13,7 @@
 //     in stream order after the request's last copy:
 //       [ wavefront queues for one tile | tile output (float4) | 8 tallies ]
 //   * the image is rendered in bands of whole rows ("tiles", at most
-//     tile_samples samples each, rows a multiple of 8 except the last); each
+//     tile_samples samples each, rows a multiple of 16 except the last); each
 //     band is copied into the slot's pinned staging image, and the staging
 //     image into the caller's host buffer when the stream reaches the end.
 // Results do not depend on the tiling or on what else runs: every sample's
@@ -162,13 +162,15 @@ void CUDART_CB on_request_done(void* p) {
 // Plans the bands of `r` and its device footprint.
 void plan_request(const Server& sv, Request& r) {
     const int ns = std::min(std::max(r.aa, 1), 64);
-    const long long wpad = (long long)((r.W + 15) / 16) * 16;
+    // queue scratch for a band padded to any of the wavefront sample order's
+    // tile shapes (8x16, 16x8, 32x4: widths up to 32, heights up to 16)
+    const long long wpad = (long long)((r.W + 31) / 32) * 32;
     long long rows = sv.tile_samples / (wpad * ns);
-    rows = std::max<long long>(8, rows / 8 * 8);
+    rows = std::max<long long>(16, rows / 16 * 16);
     if (rows >= r.H) rows = r.H;
     r.rows_per_tile = (int)rows;
     r.tiles = (int)((r.H + rows - 1) / rows);
-    const long long tile_samples = wpad * ((rows + 7) / 8 * 8) * ns;
+    const long long tile_samples = wpad * ((rows + 15) / 16 * 16) * ns;
     const bool queues = sv.form == SHEEN_FORM_WAVEFRONT && wave_pipeline_used(*r.scene);
     r.scratch_bytes = queues ? wave_scratch_bytes(r.scene->view.num_lights, tile_samples) : 0;
     const size_t tile_out = ((size_t)r.W * rows * sizeof(float4) + 255) & ~(size_t)255;

@@ -39,7 +39,7 @@ const Key kKeys[] = {
     {"trace.se_polish", &Tuning::se_polish, 0, 1},
     {"caustic.knn", &Tuning::caustic_knn, 0, 64},
     {"wave.mega_samples", &Tuning::mega_samples, 0, 1 << 30},
-    {"wave.shadow_cache", &Tuning::shadow_cache, 0, 1},
+    {"wave.tile_w", &Tuning::tile_w, 8, 32},
 };
 
 }  // namespace
@@ -56,6 +56,10 @@ int tuning_set(const char* name, int value) {
     for (const Key& k : kKeys) {
         if (std::strcmp(k.name, name) != 0) continue;
         if (value < k.lo || value > k.hi) { set_errorf("tuning value out of range for %s", name); return -1; }
+        if (k.field == &Tuning::tile_w && value != 8 && value != 16 && value != 32) {
+            set_errorf("%s must be 8, 16 or 32", name);
+            return -1;
+        }
         std::lock_guard<std::mutex> lk(g_tune_mu);
         if (g_tuning.*(k.field) != value) {
             g_tuning.*(k.field) = value;
@@ -92,7 +96,7 @@ namespace sheen {
 namespace {
 
 struct Candidate {
-    int shadow_kernel, refill_min, shadow_blocks_per_sm, shadow_stack, inner_min;
+    int shadow_kernel, refill_min, shadow_blocks_per_sm, shadow_stack, inner_min, tile_w, mega_samples;
 };
 
 void apply(const Candidate& c) {
@@ -101,6 +105,8 @@ void apply(const Candidate& c) {
     tuning_set("wave.shadow_blocks_per_sm", c.shadow_blocks_per_sm);
     tuning_set("wave.shadow_stack", c.shadow_stack);
     tuning_set("wave.inner_min", c.inner_min);
+    tuning_set("wave.tile_w", c.tile_w);
+    tuning_set("wave.mega_samples", c.mega_samples);
 }
 
 }  // namespace
@@ -114,13 +120,15 @@ extern "C" int sheen_autotune(SheenDeviceScene h, int W, int H, int aa, int reps
     if (s->form != SHEEN_FORM_WAVEFRONT) { set_error("autotuning applies to SHEEN_FORM_WAVEFRONT scenes"); return -1; }
     if (reps < 1) reps = 3;
     const Tuning t0 = tuning();
+    const Candidate start{t0.shadow_kernel, t0.refill_min, t0.shadow_blocks_per_sm, t0.shadow_stack, t0.inner_min,
+                          t0.tile_w, t0.mega_samples};
     std::vector<Candidate> cands;
-    cands.push_back({t0.shadow_kernel, t0.refill_min, t0.shadow_blocks_per_sm, t0.shadow_stack, t0.inner_min});
-    cands.push_back({0, t0.refill_min, 0, 0, 0});
+    cands.push_back(start);
+    cands.push_back({0, t0.refill_min, 0, 0, 0, t0.tile_w, t0.mega_samples});
     for (int st : {0, 1})
         for (int r : {8, 16, 24})
-            for (int im : {0, 6, 10, 14}) cands.push_back({1, r, 0, st, im});
-    cands.push_back({1, 16, 4, 0, 10});
+            for (int im : {0, 6, 10, 14}) cands.push_back({1, r, 0, st, im, t0.tile_w, t0.mega_samples});
+    cands.push_back({1, 16, 4, 0, 10, t0.tile_w, t0.mega_samples});
     float4* buf = nullptr;
     cudaStream_t st = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -131,25 +139,50 @@ extern "C" int sheen_autotune(SheenDeviceScene h, int W, int H, int aa, int reps
     double best = 1e30, first = 0.0;
     int best_i = 0;
     const Region rg{0, 0, W, H};
-    for (size_t i = 0; i < cands.size() && e == cudaSuccess; i++) {
-        apply(cands[i]);
-        if ((e = launch_wavefront(*s, W, H, aa, rg, buf, st, false)) != cudaSuccess) break;   // warm-up + capture
-        cudaEventRecord(e0, st);
-        for (int k = 0; k < reps && e == cudaSuccess; k++) e = launch_wavefront(*s, W, H, aa, rg, buf, st, false);
-        cudaEventRecord(e1, st);
-        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        const double per = ms / reps;
-        if (i == 0) first = per;
-        if (per < best) { best = per; best_i = (int)i; }
+    auto time_from = [&](size_t from) {
+        for (size_t i = from; i < cands.size() && e == cudaSuccess; i++) {
+            apply(cands[i]);
+            if ((e = launch_wavefront(*s, W, H, aa, rg, buf, st, false)) != cudaSuccess) break;   // warm-up + capture
+            cudaEventRecord(e0, st);
+            for (int k = 0; k < reps && e == cudaSuccess; k++) e = launch_wavefront(*s, W, H, aa, rg, buf, st, false);
+            cudaEventRecord(e1, st);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            const double per = ms / reps;
+            if (i == 0) first = per;
+            if (per < best) { best = per; best_i = (int)i; }
+        }
+    };
+    // 1. the shadow stage's parameters
+    time_from(0);
+    // 2. the pixel tile of the sample order, with the best shadow setting
+    if (e == cudaSuccess) {
+        const size_t from = cands.size();
+        for (int tw : {8, 16, 32}) {
+            if (tw == cands[(size_t)best_i].tile_w) continue;
+            Candidate c = cands[(size_t)best_i];
+            c.tile_w = tw;
+            cands.push_back(c);
+        }
+        time_from(from);
+    }
+    // 3. the small-frame switch: queue stages or the megakernel for this frame
+    if (e == cudaSuccess) {
+        const size_t from = cands.size();
+        for (int m : {0, 1 << 30}) {
+            Candidate c = cands[(size_t)best_i];
+            c.mega_samples = m;
+            cands.push_back(c);
+        }
+        time_from(from);
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (st) cudaStreamDestroy(st);
     dfree(buf);
     if (e != cudaSuccess) {
-        apply({t0.shadow_kernel, t0.refill_min, t0.shadow_blocks_per_sm, t0.shadow_stack, t0.inner_min});
+        apply(start);
         set_error(cudaGetErrorString(e));
         return -1;
     }
@@ -159,6 +192,8 @@ extern "C" int sheen_autotune(SheenDeviceScene h, int W, int H, int aa, int reps
     out->shadow_blocks_per_sm = cands[best_i].shadow_blocks_per_sm;
     out->shadow_stack = cands[best_i].shadow_stack;
     out->inner_min = cands[best_i].inner_min;
+    out->tile_w = cands[best_i].tile_w;
+    out->mega_samples = cands[best_i].mega_samples;
     out->candidates = (int)cands.size();
     out->best_ms = best;
     out->default_ms = first;

@@ -234,7 +234,7 @@ namespace {
 // materials[rec.material_id], integrator/csg.h reads objects / SEs by leaf
 // index), so a scene whose indices leave their arrays is refused here
 // instead of faulting on the GPU.  Returns null or the first problem.
-const char* scene_index_error(const SheenScene* in) {
+const char* scene_index_error(const SheenScene* in, const SheenSceneExt* ext) {
     struct Arr { const void* p; int n; const char* what; };
     const Arr arrays[] = {
         {in->objects, in->num_objects, "objects"}, {in->sweep_points, in->num_sweep_points, "sweep points"},
@@ -275,10 +275,62 @@ const char* scene_index_error(const SheenScene* in) {
     }
     for (int i = 0; i < in->num_planes; i++)
         if (!mat_ok(in->planes[i].material_id)) return "plane material_id out of range";
-    if (in->csg_nodes && in->num_csg_nodes > 0 && in->csg_root >= 0 && in->csg_root < in->num_csg_nodes) {
-        for (int i = 0; i < in->num_csg_nodes; i++) {
-            const CSGNode& c = in->csg_nodes[i];
-            if (c.leaf_kind == 0) {
+    const bool forest = ext && ext->num_csg_roots > 0;
+    if (forest) {
+        if (!ext->csg_roots) return "null CSG root list with a nonzero count";
+        if (!in->csg_nodes || in->num_csg_nodes <= 0) return "CSG roots without CSG nodes";
+        for (int i = 0; i < ext->num_csg_roots; i++)
+            if (ext->csg_roots[i] < 0 || ext->csg_roots[i] >= in->num_csg_nodes) return "CSG root index out of range";
+    }
+    if (ext) {
+        if (ext->num_csg_boxes < 0 || ext->num_csg_cones < 0 || ext->num_bezier_ctrl < 0 || ext->num_hf_heights < 0 ||
+            ext->num_csg_roots < 0)
+            return "negative extension count";
+        if ((ext->num_csg_boxes > 0 && !ext->csg_boxes) || (ext->num_csg_cones > 0 && !ext->csg_cones) ||
+            (ext->num_bezier_ctrl > 0 && !ext->bezier_ctrl) || (ext->num_hf_heights > 0 && !ext->hf_heights))
+            return "null extension array with a nonzero count";
+        for (int i = 0; i < ext->num_csg_boxes; i++)
+            if (!mat_ok(ext->csg_boxes[i].material_id)) return "CSG box material_id out of range";
+        for (int i = 0; i < ext->num_csg_cones; i++) {
+            if (!mat_ok(ext->csg_cones[i].material_id)) return "CSG cone material_id out of range";
+            if (!(ext->csg_cones[i].r0 >= 0.0f && ext->csg_cones[i].r1 >= 0.0f)) return "CSG cone radius negative";
+        }
+        auto bez_ok = [&](const SheenBezierRun* runs, int n) {
+            for (int i = 0; runs && i < n; i++) {
+                const SheenBezierRun& r = runs[i];
+                if (r.ctrl_count == 0) continue;
+                if (r.ctrl_count < 4 || r.ctrl_count % 4 != 0 || !range_ok(r.ctrl_offset, r.ctrl_count, ext->num_bezier_ctrl))
+                    return false;
+            }
+            return true;
+        };
+        if (!bez_ok(ext->lathe_bezier, in->num_lathes)) return "lathe Bezier run out of range (4k control points)";
+        if (!bez_ok(ext->prism_bezier, in->num_prisms)) return "prism Bezier run out of range (4k control points)";
+        for (int i = 0; ext->hf_grid && i < in->num_heightfields; i++) {
+            const SheenHeightGrid& g = ext->hf_grid[i];
+            if (g.offset < 0) continue;
+            if (g.w < 2 || g.h < 2 || !range_ok(g.offset, (int)std::min<long long>((long long)g.w * g.h, 1ll << 30),
+                                                ext->num_hf_heights) || (long long)g.w * g.h > (1ll << 30))
+                return "height grid out of range";
+        }
+    }
+    // CSG nodes reachable from the roots in use (the scene's tree, and the
+    // extension forest when one is given)
+    if (in->csg_nodes && in->num_csg_nodes > 0) {
+        std::vector<int> st;
+        if (in->csg_root >= 0 && in->csg_root < in->num_csg_nodes) st.push_back(in->csg_root);
+        if (forest) st.insert(st.end(), ext->csg_roots, ext->csg_roots + ext->num_csg_roots);
+        std::vector<unsigned char> seen((size_t)in->num_csg_nodes, 0);
+        while (!st.empty()) {
+            const int id = st.back();
+            st.pop_back();
+            if (seen[(size_t)id]) continue;
+            seen[(size_t)id] = 1;
+            const CSGNode& c = in->csg_nodes[id];
+            if (c.leaf_kind == 2 || c.leaf_kind == 3) {
+                const int n = !ext ? 0 : (c.leaf_kind == 2 ? ext->num_csg_boxes : ext->num_csg_cones);
+                if (c.leaf_index < 0 || c.leaf_index >= n) return "CSG box / cone leaf index out of range";
+            } else if (c.leaf_kind == 0) {
                 if (!in->objects || c.leaf_index < 0 || c.leaf_index >= in->num_objects)
                     return "CSG sphere leaf index out of range";
                 if (!mat_ok(in->objects[c.leaf_index].material_id)) return "CSG leaf material_id out of range";
@@ -288,6 +340,8 @@ const char* scene_index_error(const SheenScene* in) {
             } else if (c.leaf_kind < 0) {
                 if (c.left < -1 || c.left >= in->num_csg_nodes || c.right < -1 || c.right >= in->num_csg_nodes)
                     return "CSG child index out of range";
+                if (c.left >= 0) st.push_back(c.left);
+                if (c.right >= 0) st.push_back(c.right);
             } else {
                 return "unknown CSG leaf kind";
             }
@@ -307,12 +361,184 @@ __global__ void k_check_tri_materials(const Triangle* __restrict__ t, int n, int
 
 }  // namespace
 
-int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
+namespace {
+
+// Extension tables (SheenSceneExt) in their device layouts; empty vectors
+// when the scene has no such extension.
+struct ExtTables {
+    std::vector<float> se_n2;           // per superellipsoid
+    std::vector<int4> hf_grid;          // per heightfield {offset, w, h, 0}
+    std::vector<int4> lathe_bz;         // per lathe {first span, spans, 0, 0}
+    std::vector<float4> lathe_bound;    // per lathe {R, y_lo, y_hi, 0}
+    std::vector<int4> prism_bz;         // per prism
+    std::vector<float4> prism_box;      // per prism {x_lo, z_lo, x_hi, z_hi} about its centre
+    std::vector<float4> spans;          // 2 per cubic span
+    std::vector<int> csg_roots;
+    std::vector<HostNode> csg_root_bvh;
+    std::vector<float4> csg_boxes;      // 2 per box
+    std::vector<float4> csg_cones;      // 3 per cone
+};
+
+float4 f4(float x, float y, float z, float w) { return make_float4(x, y, z, w); }
+float int_bits(int i) { float f; std::memcpy(&f, &i, 4); return f; }
+
+// Box of an extension CSG leaf (kind 2 box, 3 cone).
+void csg_ext_leaf_box(const ExtTables& xt, int kind, int idx, float lo[3], float hi[3]) {
+    if (kind == 2) {
+        const float4 a = xt.csg_boxes[2 * (size_t)idx], b = xt.csg_boxes[2 * (size_t)idx + 1];
+        lo[0] = a.x; lo[1] = a.y; lo[2] = a.z;
+        hi[0] = b.x; hi[1] = b.y; hi[2] = b.z;
+        return;
+    }
+    const float4 a = xt.csg_cones[3 * (size_t)idx], b = xt.csg_cones[3 * (size_t)idx + 1];
+    const float r = std::max(a.w, b.w);
+    lo[0] = std::min(a.x, b.x) - r; lo[1] = std::min(a.y, b.y) - r; lo[2] = std::min(a.z, b.z) - r;
+    hi[0] = std::max(a.x, b.x) + r; hi[1] = std::max(a.y, b.y) + r; hi[2] = std::max(a.z, b.z) + r;
+}
+
+// Box of the CSG tree at `root`: the union of its leaves' boxes (the solid
+// lies inside the union of its leaves), widened by 1e-4 relative.
+void csg_tree_box(const SheenScene* in, const ExtTables& xt, int root, float lo[3], float hi[3]) {
+    for (int k = 0; k < 3; k++) { lo[k] = FLT_MAX; hi[k] = -FLT_MAX; }
+    std::vector<int> st{root};
+    int guard = 0;
+    while (!st.empty() && guard++ <= 4 * in->num_csg_nodes + 4) {
+        const int id = st.back();
+        st.pop_back();
+        if (id < 0 || id >= in->num_csg_nodes) continue;
+        const CSGNode& c = in->csg_nodes[id];
+        float a[3], b[3];
+        if (c.leaf_kind < 0) {
+            st.push_back(c.left);
+            st.push_back(c.right);
+            continue;
+        } else if (c.leaf_kind == 0) {
+            const Object& o = in->objects[c.leaf_index];
+            const float r = std::fabs(o.param2);
+            a[0] = o.param1.x - r; a[1] = o.param1.y - r; a[2] = o.param1.z - r;
+            b[0] = o.param1.x + r; b[1] = o.param1.y + r; b[2] = o.param1.z + r;
+        } else if (c.leaf_kind == 1) {
+            const Superellipsoid& e = in->superellipsoids[c.leaf_index];
+            a[0] = e.center.x - std::fabs(e.a); a[1] = e.center.y - std::fabs(e.b); a[2] = e.center.z - std::fabs(e.c);
+            b[0] = e.center.x + std::fabs(e.a); b[1] = e.center.y + std::fabs(e.b); b[2] = e.center.z + std::fabs(e.c);
+        } else {
+            csg_ext_leaf_box(xt, c.leaf_kind, c.leaf_index, a, b);
+        }
+        for (int k = 0; k < 3; k++) { lo[k] = std::min(lo[k], a[k]); hi[k] = std::max(hi[k], b[k]); }
+    }
+    if (!(lo[0] <= hi[0])) { for (int k = 0; k < 3; k++) lo[k] = hi[k] = 0.0f; return; }
+    float scale = 0.0f;
+    for (int k = 0; k < 3; k++) scale = std::max(scale, std::max(std::fabs(lo[k]), std::fabs(hi[k])));
+    const float m = 1e-4f * scale + 1e-6f;
+    for (int k = 0; k < 3; k++) { lo[k] -= m; hi[k] += m; }
+}
+
+void build_ext_tables(const SheenScene* in, const SheenSceneExt* ext, ExtTables& xt) {
+    if (!ext) return;
+    if (ext->se_n2 && in->num_superellipsoids > 0)
+        xt.se_n2.assign(ext->se_n2, ext->se_n2 + in->num_superellipsoids);
+    if (ext->hf_grid && in->num_heightfields > 0) {
+        for (int i = 0; i < in->num_heightfields; i++) {
+            const SheenHeightGrid& g = ext->hf_grid[i];
+            xt.hf_grid.push_back(g.offset >= 0 ? make_int4(g.offset, g.w, g.h, 0) : make_int4(-1, 0, 0, 0));
+        }
+    }
+    // Bezier runs -> cubic spans, consecutive spans joined (and prism
+    // contours closed) by straight spans where their ends differ.
+    auto add_run = [&](const SheenBezierRun& r, bool close, float box[4]) -> int4 {
+        const float* c = ext->bezier_ctrl + 2 * (size_t)r.ctrl_offset;
+        const int first = (int)(xt.spans.size() / 2);
+        auto push = [&](float a0, float b0, float a1, float b1, float a2, float b2, float a3, float b3) {
+            xt.spans.push_back(f4(a0, b0, a1, b1));
+            xt.spans.push_back(f4(a2, b2, a3, b3));
+        };
+        auto line = [&](float pa, float pb, float qa, float qb) {
+            push(pa, pb, pa + (qa - pa) / 3.0f, pb + (qb - pb) / 3.0f, pa + 2.0f * (qa - pa) / 3.0f,
+                 pb + 2.0f * (qb - pb) / 3.0f, qa, qb);
+        };
+        const int ns = r.ctrl_count / 4;
+        for (int k = 0; k < ns; k++) {
+            const float* q = c + 8 * k;
+            if (k > 0 && (q[-2] != q[0] || q[-1] != q[1])) line(q[-2], q[-1], q[0], q[1]);
+            push(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7]);
+        }
+        const float* last = c + 8 * (ns - 1) + 6;
+        if (close && (last[0] != c[0] || last[1] != c[1])) line(last[0], last[1], c[0], c[1]);
+        box[0] = box[2] = c[0];
+        box[1] = box[3] = c[1];
+        for (int k = 0; k < r.ctrl_count; k++) {
+            box[0] = std::min(box[0], c[2 * k]); box[2] = std::max(box[2], c[2 * k]);
+            box[1] = std::min(box[1], c[2 * k + 1]); box[3] = std::max(box[3], c[2 * k + 1]);
+        }
+        return make_int4(first, (int)(xt.spans.size() / 2) - first, 0, 0);
+    };
+    if (ext->lathe_bezier && in->num_lathes > 0) {
+        for (int i = 0; i < in->num_lathes; i++) {
+            const SheenBezierRun& r = ext->lathe_bezier[i];
+            if (r.ctrl_count < 4) {
+                xt.lathe_bz.push_back(make_int4(0, 0, 0, 0));
+                xt.lathe_bound.push_back(f4(0, 0, 0, 0));
+                continue;
+            }
+            float box[4];   // {y_lo, r_lo, y_hi, r_hi}
+            xt.lathe_bz.push_back(add_run(r, false, box));
+            const float R = std::max(std::fabs(box[1]), std::fabs(box[3]));
+            const float m = 1e-6f * (std::max(std::fabs(box[0]), std::fabs(box[2])) + R) + 1e-6f;
+            xt.lathe_bound.push_back(f4(R + m, box[0] - m, box[2] + m, 0.0f));
+        }
+    }
+    if (ext->prism_bezier && in->num_prisms > 0) {
+        for (int i = 0; i < in->num_prisms; i++) {
+            const SheenBezierRun& r = ext->prism_bezier[i];
+            if (r.ctrl_count < 4) {
+                xt.prism_bz.push_back(make_int4(0, 0, 0, 0));
+                xt.prism_box.push_back(f4(0, 0, 0, 0));
+                continue;
+            }
+            float box[4];   // {x_lo, z_lo, x_hi, z_hi}
+            xt.prism_bz.push_back(add_run(r, true, box));
+            const float m = 1e-6f * std::max(std::max(std::fabs(box[0]), std::fabs(box[2])),
+                                             std::max(std::fabs(box[1]), std::fabs(box[3]))) + 1e-6f;
+            xt.prism_box.push_back(f4(box[0] - m, box[1] - m, box[2] + m, box[3] + m));
+        }
+    }
+    for (int i = 0; i < ext->num_csg_boxes; i++) {
+        const SheenCsgBox& b = ext->csg_boxes[i];
+        xt.csg_boxes.push_back(f4(b.lo.x, b.lo.y, b.lo.z, int_bits(b.material_id)));
+        xt.csg_boxes.push_back(f4(b.hi.x, b.hi.y, b.hi.z, 0.0f));
+    }
+    for (int i = 0; i < ext->num_csg_cones; i++) {
+        const SheenCsgCone& c = ext->csg_cones[i];
+        xt.csg_cones.push_back(f4(c.p0.x, c.p0.y, c.p0.z, c.r0));
+        xt.csg_cones.push_back(f4(c.p1.x, c.p1.y, c.p1.z, c.r1));
+        xt.csg_cones.push_back(f4(int_bits(c.material_id), 0.0f, 0.0f, 0.0f));
+    }
+    if (ext->num_csg_roots > 0) {
+        xt.csg_roots.assign(ext->csg_roots, ext->csg_roots + ext->num_csg_roots);
+        std::vector<float> lo, hi;
+        std::vector<int> prims;
+        for (int k = 0; k < ext->num_csg_roots; k++) {
+            float a[3], b[3];
+            csg_tree_box(in, xt, ext->csg_roots[k], a, b);
+            push_box(lo, hi, a, b);
+            prims.push_back(k);
+        }
+        build_median_bvh(lo, hi, prims, true, xt.csg_root_bvh);
+    }
+}
+
+}  // namespace
+
+int scene_upload(const SheenScene* in, int form, DeviceScene** out) { return scene_upload_ext(in, nullptr, form, out); }
+
+int scene_upload_ext(const SheenScene* in, const SheenSceneExt* ext, int form, DeviceScene** out) {
     *out = nullptr;
     if (!in) { set_error("null scene"); return -1; }
     if (form != SHEEN_FORM_PLAIN && form != SHEEN_FORM_WAVEFRONT) { set_error("unknown renderer form"); return -1; }
     if (in->num_materials <= 0 || !in->materials) { set_error("no materials"); return -1; }
-    if (const char* why = scene_index_error(in)) { set_error(why); return -1; }
+    if (const char* why = scene_index_error(in, ext)) { set_error(why); return -1; }
+    ExtTables xt;
+    build_ext_tables(in, ext, xt);
     DeviceScene* s = new DeviceScene();
     s->form = form;
     cudaGetDevice(&s->device);
@@ -399,6 +625,14 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     lo.clear(); hi.clear(); prims.clear();
     for (int i = 0; i < in->num_lathes; i++) {   // bvh.h:394-407 (x/z start at +-1e30 about the centre)
         const Lathe& l = in->lathes[i];
+        if (!xt.lathe_bz.empty() && xt.lathe_bz[(size_t)i].y > 0) {
+            // exact surface (extension): its box about the world Y axis
+            const float4 b4 = xt.lathe_bound[(size_t)i];
+            float a[3] = {-b4.x, b4.y, -b4.x}, b[3] = {b4.x, b4.z, b4.x};
+            push_box(lo, hi, a, b);
+            prims.push_back(i);
+            continue;
+        }
         float a[3] = {l.center.x - 1e30f, 1e30f, l.center.z - 1e30f};
         float b[3] = {l.center.x + 1e30f, -1e30f, l.center.z + 1e30f};
         for (int k = 0; k < l.point_count; k++) {
@@ -418,6 +652,15 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     lo.clear(); hi.clear(); prims.clear();
     for (int i = 0; i < in->num_prisms; i++) {   // bvh.h:321-332
         const Prism& p = in->prisms[i];
+        if (!xt.prism_bz.empty() && xt.prism_bz[(size_t)i].y > 0) {
+            // exact contour (extension): the hull of its control points
+            const float4 b4 = xt.prism_box[(size_t)i];
+            float a[3] = {p.center.x + b4.x, p.center.y + p.y_min, p.center.z + b4.y};
+            float b[3] = {p.center.x + b4.z, p.center.y + p.y_max, p.center.z + b4.w};
+            push_box(lo, hi, a, b);
+            prims.push_back(i);
+            continue;
+        }
         float a[3] = {1e30f, p.center.y + p.y_min, 1e30f}, b[3] = {-1e30f, p.center.y + p.y_max, -1e30f};
         for (int k = 0; k < p.point_count; k++) {
             const PrismPoint& q = in->prism_points[p.point_offset + k];
@@ -534,6 +777,19 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
                               : (size_t)-1;   // zero-filled; set by lathe_segments_kernel
     const size_t o_lbnd = (o_lseg != (size_t)-1) ? ar.add(nullptr, (size_t)in->num_lathes * sizeof(float4))
                                                  : (size_t)-1;
+    const size_t o_sen2 = add_vec(xt.se_n2);
+    const size_t o_hfg = add_vec(xt.hf_grid);
+    const size_t o_hfh = (ext && ext->hf_grid && ext->num_hf_heights > 0)
+                             ? ar.add(ext->hf_heights, (size_t)ext->num_hf_heights * sizeof(float))
+                             : (size_t)-1;
+    const size_t o_lbz = add_vec(xt.lathe_bz);
+    const size_t o_lbzb = add_vec(xt.lathe_bound);
+    const size_t o_pbz = add_vec(xt.prism_bz);
+    const size_t o_spans = add_vec(xt.spans);
+    const size_t o_croots = add_vec(xt.csg_roots);
+    const size_t o_crbvh = add_vec(xt.csg_root_bvh);
+    const size_t o_cbox = add_vec(xt.csg_boxes);
+    const size_t o_ccone = add_vec(xt.csg_cones);
     ar.size = (ar.size + 255) & ~(size_t)255;
 
     cudaError_t e = dmalloc(&s->arena, ar.size);
@@ -598,31 +854,15 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     v.csg_root = (in->csg_nodes && in->num_csg_nodes > 0 && in->csg_root >= 0 && in->csg_root < in->num_csg_nodes)
                      ? in->csg_root : -1;
     {
-        // the CSG leaves' box (the leaf indices were checked at the start)
-        float lo3[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi3[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-        for (int i = 0; v.csg_root >= 0 && i < in->num_csg_nodes; i++) {
-            const CSGNode& c = in->csg_nodes[i];
-            float cen[3], ext[3];
-            if (c.leaf_kind == 0) {
-                const Object& o = in->objects[c.leaf_index];
-                cen[0] = o.param1.x; cen[1] = o.param1.y; cen[2] = o.param1.z;
-                ext[0] = ext[1] = ext[2] = std::fabs(o.param2);
-            } else if (c.leaf_kind == 1) {
-                const Superellipsoid& se = in->superellipsoids[c.leaf_index];
-                cen[0] = se.center.x; cen[1] = se.center.y; cen[2] = se.center.z;
-                ext[0] = std::fabs(se.a); ext[1] = std::fabs(se.b); ext[2] = std::fabs(se.c);
-            } else {
-                continue;
-            }
-            for (int k = 0; k < 3; k++) {
-                lo3[k] = std::min(lo3[k], cen[k] - ext[k]);
-                hi3[k] = std::max(hi3[k], cen[k] + ext[k]);
-            }
+        // the box of the tree's leaves (the leaf indices were checked at the
+        // start), widened by 1e-4 relative
+        float lo3[3], hi3[3];
+        if (v.csg_root >= 0) {
+            csg_tree_box(in, xt, v.csg_root, lo3, hi3);
+        } else {
+            for (int k = 0; k < 3; k++) { lo3[k] = FLT_MAX; hi3[k] = -FLT_MAX; }
         }
-        float scale = 0.0f;
-        for (int k = 0; k < 3; k++) scale = std::max(scale, std::max(std::fabs(lo3[k]), std::fabs(hi3[k])));
-        const float m = lo3[0] <= hi3[0] ? 1e-4f * scale + 1e-6f : 0.0f;
-        for (int k = 0; k < 3; k++) { v.csg_lo[k] = lo3[k] - m; v.csg_hi[k] = hi3[k] + m; }
+        for (int k = 0; k < 3; k++) { v.csg_lo[k] = lo3[k]; v.csg_hi[k] = hi3[k]; }
     }
     v.planes = (const Plane*)dptr(o_pla); v.num_planes = in->num_planes;
     v.materials = (const Material*)dptr(o_mat); v.num_materials = in->num_materials;
@@ -646,6 +886,18 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out) {
     v.aa_centered = tuning().aa_centered;
     v.se_polish = tuning().se_polish;
     v.caustic_knn = tuning().caustic_knn;
+    v.se_n2 = (const float*)dptr(o_sen2);
+    v.hf_grid = (const int4*)dptr(o_hfg);
+    v.hf_heights = (const float*)dptr(o_hfh);
+    v.lathe_bz = (const int4*)dptr(o_lbz);
+    v.lathe_bz_bound = (const float4*)dptr(o_lbzb);
+    v.prism_bz = (const int4*)dptr(o_pbz);
+    v.bz_spans = (const float4*)dptr(o_spans);
+    v.csg_roots = (const int*)dptr(o_croots);
+    v.num_csg_roots = (int)xt.csg_roots.size();
+    v.csg_root_bvh = (const dev::BvhNode*)dptr(o_crbvh);
+    v.csg_boxes = (const float4*)dptr(o_cbox);
+    v.csg_cones = (const float4*)dptr(o_ccone);
     s->d_tally = (unsigned long long*)dptr(o_tally);
     s->wave_depth = std::max(q_all.max_depth, std::max(q_block.max_depth, q_pass.max_depth));
     s->build_ms = t1 - t0;

@@ -34,6 +34,8 @@ class Oracle:
         L = self.lib
         L.oracle_scene_create.argtypes = [P]
         L.oracle_scene_create.restype = P
+        L.oracle_scene_create_ext.argtypes = [P, P]
+        L.oracle_scene_create_ext.restype = P
         L.oracle_scene_destroy.argtypes = [P]
         L.oracle_scene_photon_count.argtypes = [P]
         L.oracle_scene_photon_count.restype = I
@@ -52,8 +54,10 @@ class Oracle:
         L.oracle_render_region.argtypes = [P, I, I, I, I, I, I, I, P, I, P]
         L.oracle_render_region.restype = I
 
-    def scene(self, view_ptr: int, centered: bool = False, knn: int = 0):
-        h = _Handle(self.lib, self.lib.oracle_scene_create(view_ptr), self.lib.oracle_scene_destroy)
+    def scene(self, view_ptr: int, centered: bool = False, knn: int = 0, ext_ptr: int | None = None):
+        ptr = (self.lib.oracle_scene_create_ext(view_ptr, ext_ptr) if ext_ptr
+               else self.lib.oracle_scene_create(view_ptr))
+        h = _Handle(self.lib, ptr, self.lib.oracle_scene_destroy)
         if centered:
             self.lib.oracle_scene_set_centered(h.ptr, 1)
         if knn:

@@ -203,3 +203,27 @@ def test_srgb_thresholds_are_the_host_conversion_steps(tmp_path):
     assert np.array_equal(got[:, 1], by_table(vals[::-1]))
     assert np.array_equal(got[:255, 0], np.arange(1, 256, dtype=np.uint8))   # each threshold: its byte
     assert np.array_equal(got[255:510, 0], np.arange(0, 255, dtype=np.uint8))  # one ulp below: the byte before
+
+
+def test_contract_fixture_is_the_addons_layout(reference_tree):
+    """golden/contract_scene.npz holds what the reference's ctypes contract
+    (c_api_contract.py) builds for its scene: regenerated here byte for byte
+    (pointer fields excepted, which hold this process's addresses)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "make_contract_fixture", os.path.join(os.path.dirname(__file__), "golden", "make_contract_fixture.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    sc, keep = mod.build()
+    f = np.load(os.path.join(os.path.dirname(__file__), "golden", "contract_scene.npz"))
+    now = np.frombuffer(ctypes.string_at(ctypes.addressof(sc), ctypes.sizeof(sc)), np.uint8).copy()
+    rec = f["scene_bytes"].copy()
+    for k in f.files:
+        if k.startswith("ptr_"):
+            o = int(f[k])
+            now[o:o + 8] = 0
+            rec[o:o + 8] = 0
+            arr = keep[k[4:]]
+            assert bytes(f["arr_" + k[4:]]) == ctypes.string_at(ctypes.addressof(arr), ctypes.sizeof(arr))
+    assert np.array_equal(now, rec)
+    assert int(f["sizeof_HeightField"]) == 72 and int(f["sizeof_SheenScene"]) == 344
