@@ -174,6 +174,13 @@ WORKLOADS = {
 }
 
 
+EXT_WORKLOADS = {
+    1: "reflect + refract recursion to 4 bounces (BVH4 megakernel)",
+    2: "exact cubic-Bezier lathes and prisms (FP64 root isolation), two-exponent superellipsoids, "
+       "1024x1024 FP32 height grid, 128 more CSG trees over spheres, boxes and cones",
+}
+
+
 def make_scene(args):
     """The workload's scene; sets the frame size and spp from the generator."""
     import sheen_b200 as sb
@@ -339,7 +346,7 @@ def run_ours(args):
     # counting megakernel's shadow-query counters (same walks).  Plain: the
     # single megakernel launch, timed above.
     stages = None
-    mega = form == sb.FORM_WAVEFRONT and uses_megakernel(scene, W, H, SPP)
+    mega = form == sb.FORM_WAVEFRONT and uses_megakernel(ds, W, H, SPP)
     if form == sb.FORM_WAVEFRONT and not mega:
         profs = []
         for i in range(max(3, args.steps // 2)):
@@ -371,11 +378,14 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(frame_ms, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generator)",
-        "config": {"workload": WORKLOADS.get(args.config, f"config {args.config}"),
+        "config": {"workload": WORKLOADS.get(args.config, f"config {args.config}")
+                   + (" + extension column: " + EXT_WORKLOADS[args.config] if args.extended else ""),
                    "triangles": scene.view.num_triangles, "width": W, "height": H, "spp": SPP,
                    "form": args.form, "parallelism": f"replicas{world}",
                    "frame": (f"{args.tiles} uneven tiles in one batched pass" if args.tiles > 0
-                             else "whole frame, one megakernel launch (small frame)" if mega
+                             else "whole frame, one BVH4 megakernel launch (%s)" % (
+                                 "reflect + refract recursion runs outside the queue stages"
+                                 if args.extended and args.config == 1 else "small frame") if mega
                              else "whole frame, captured CUDA graph"),
                    "l2": "256 MB buffer written between timed frames; scene arrays exceed L2",
                    "rays_per_frame": rays, "box_tests_per_frame": nodes, "prim_tests_per_frame": prims,
@@ -437,15 +447,12 @@ def uneven_tiles(W, H, n, seed):
     return tiles
 
 
-def uses_megakernel(scene, W, H, spp):
-    """The library's small-frame rule (wave.mega_samples): a frame of at most
-    that many samples -- pixels padded to whole 16x8 tiles, times spp; a
-    quarter of it for scenes with triangles -- runs on the BVH4 megakernel."""
+def uses_megakernel(ds, W, H, spp):
+    """True when the library renders this frame of a wavefront-form scene on
+    the BVH4 megakernel (sheen_scene_frame_path): small frames (the
+    wave.mega_samples rule) and scenes outside the queue pipeline."""
     import sheen_b200 as sb
-    m = sb.tune_get("wave.mega_samples")
-    samples = ((W + 15) // 16 * 16) * ((H + 7) // 8 * 8) * max(1, min(spp, 64))
-    limit = m // 4 if scene.view.num_triangles > 0 else m
-    return m > 0 and samples <= limit
+    return ds.frame_path(W, H, spp) == sb.PATH_MEGAKERNEL
 
 
 def launches_per_frame(form):
@@ -789,9 +796,10 @@ def main():
                     help="requests of the short serving run in the default bench line (0: skip)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form denominator")
     ap.add_argument("--extended", action="store_true",
-                    help="config 2 with its extension column (exact Bezier lathes and prisms, two-exponent "
-                         "superellipsoids, FP32 height grid, 128 CSG trees); the reference has none of these, "
-                         "so the line carries no reference or host-array legs")
+                    help="the workload's extension column -- config 1: reflect + refract recursion to 4 "
+                         "bounces; config 2: exact Bezier lathes and prisms, two-exponent superellipsoids, "
+                         "FP32 height grid, 128 CSG trees; the reference has none of these, so the line "
+                         "carries no reference or host-array legs")
     ap.add_argument("--capture", choices=sorted(CAPTURE_CASES),
                     help="render one small frame of a named case and exit (for profiler captures)")
     args = ap.parse_args()
@@ -801,8 +809,8 @@ def main():
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.extended:
-        if args.config != 2:
-            ap.error("--extended applies to --config 2")
+        if args.config not in (1, 2):
+            ap.error("--extended applies to --config 1 and 2")
         args.no_cpu = args.no_ref_gpu = args.no_plain = True
         args.serve_requests = 0
     if args.tune:

@@ -240,6 +240,16 @@ typedef struct SheenSceneExt {
     int num_csg_boxes;
     const SheenCsgCone* csg_cones;
     int num_csg_cones;
+    /* Reflect + refract recursion to max_depth bounces (2..8; 0 or 1: the
+     * reference's depth-1 mirror ray and up-to-three-face refraction;
+     * outside 0..8 the create fails).  Every hit below the limit blends as
+     * the reference's primary hit does (lighting x (1 - wr)(1 - wt), a
+     * mirror ray x wr (1 - wt), a refracted ray x the face's transmission;
+     * wr = min(reflect, 1), wt = min(transmission, 1)); a hit at the limit
+     * contributes its lighting alone.  Media act on every segment, beams on
+     * the primary ray only.  Such scenes render on the BVH4 megakernel
+     * (wavefront form) or the plain kernel. */
+    int max_depth;
 } SheenSceneExt;
 
 /* sheen_scene_create with extensions (ext may be NULL).  Fails with a
@@ -247,6 +257,19 @@ typedef struct SheenSceneExt {
 int  sheen_scene_create_ext(const SheenScene* scene, const SheenSceneExt* ext, int form, SheenDeviceScene* out);
 unsigned long long sheen_scene_device_bytes(SheenDeviceScene scene);
 int  sheen_scene_form(SheenDeviceScene scene);
+
+/* Which kernels render a whole width x height frame of the scene at
+ * aa_samples spp: SHEEN_PATH_PLAIN (a SHEEN_FORM_PLAIN scene: the
+ * reference-order kernel), SHEEN_PATH_QUEUES (the wavefront queue stages)
+ * or SHEEN_PATH_MEGAKERNEL (the BVH4 megakernel: frames at most
+ * wave.mega_samples samples, and scenes outside the queue pipeline --
+ * beams, media, shadow-debug materials, more than 16 lights, reflect +
+ * refract recursion).  Follows the current tuning; -1 on a null handle or
+ * bad sizes.  No counterpart in the reference (one megakernel). */
+#define SHEEN_PATH_PLAIN 0
+#define SHEEN_PATH_QUEUES 1
+#define SHEEN_PATH_MEGAKERNEL 2
+int  sheen_scene_frame_path(SheenDeviceScene scene, int width, int height, int aa_samples);
 
 /* Render a resident scene into a DEVICE buffer (width*height float4) on the
  * given CUDA stream (cudaStream_t passed as void*, NULL = legacy default
@@ -360,7 +383,8 @@ typedef struct SheenBatchJob {
  * the blocks from shared queues.  Each job's pixels are exactly those of
  * rendering it alone.  Jobs on SHEEN_FORM_PLAIN scenes, or whose frames run
  * on the megakernel (beams, media, shadow-debug materials, more than 16
- * lights), are rendered one by one on the same stream first.  Asynchronous on
+ * lights, reflect + refract recursion), are rendered one by one on the same
+ * stream first.  Asynchronous on
  * `stream` unless stats is non-NULL (then it synchronises and fills the ray
  * counts and render_ms).  No counterpart in the reference (one frame per
  * launch, render_kernel.cu:438-814).  0 / -1. */
@@ -379,7 +403,7 @@ typedef struct SheenStageProfile {
 /* One full frame of a SHEEN_FORM_WAVEFRONT scene into a DEVICE buffer
  * (width*height float4) with the stage profile above; synchronous.  Scenes
  * whose frames run on the megakernel (beams, media, shadow-debug materials,
- * more than 16 lights) have no stages: -1. */
+ * more than 16 lights, reflect + refract recursion) have no stages: -1. */
 int sheen_scene_profile_stages(SheenDeviceScene scene, int width, int height, int aa_samples,
                                float* out_rgba_device, void* stream, SheenStageProfile* out);
 
@@ -508,14 +532,16 @@ int sheen_generate_scene(int config, unsigned int seed, int detail, int photons,
                          SheenOwnedScene* out);
 
 /* The workload generators with their extension column (no counterpart in
- * the reference).  extended != 0, config 2: the same scene with
+ * the reference).  extended != 0, config 1: the same scene with reflect +
+ * refract recursion to 4 bounces (SheenSceneExt.max_depth).  Config 2: the
+ * same scene with
  * two-exponent superellipsoids (both exponents 2/e, e uniform in [0.2, 3]),
  * the lathes' and prisms' Bezier control points as exact surfaces, a
  * 1024 x 1024 FP32 height grid (heights in [0, 2]) for the heightfield, and
  * 128 further CSG trees of depth 3 over spheres, boxes and cones.  The
  * extensions are read with sheen_owned_ext() and passed to
  * sheen_scene_create_ext(); the SheenScene view alone is the reference's
- * scene.  Other configs: extended must be 0. */
+ * scene.  Configs 0 and 3: extended must be 0. */
 int sheen_generate_scene_ext(int config, unsigned int seed, int detail, int photons, int extended,
                              SheenOwnedScene* out);
 

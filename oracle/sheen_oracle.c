@@ -133,6 +133,7 @@ struct OracleScene {
     int* csg_roots; int ncsg_roots;
     SheenCsgBox* csg_boxes; int ncsg_boxes;
     SheenCsgCone* csg_cones; int ncsg_cones;
+    int bounces;                        /* reflect + refract recursion depth (> 1: render_deep) */
 };
 
 static void sample_pos(const OracleScene* S, int s, int n, int x, int y, real* ox, real* oy) {
@@ -1777,6 +1778,125 @@ static V media_march(const OracleScene* S, const Ray* ray, real t_surf, uint32_t
     return ins;
 }
 
+/* render_kernel.cu:560-652 -- visible spot-light cones along one ray */
+static V beams(const OracleScene* S, const Ray* ray, int hit, real t_hit, uint32_t seed) {
+    V total = v3(0, 0, 0);
+    for (int i = 0; i < S->s.num_lights; i++) {
+        const Light* L = &S->lights[i];
+        if (L->type != 3 || L->beam <= 0) continue;
+        real t_end = hit ? rfmin(t_hit, 30) : R(30);
+        if (t_end <= 0) continue;
+        const int STEPS = 6;
+        real dt = t_end / (real)STEPS, ch = (real)cos(L->angle);
+        real bl = rfmin(rfmax(L->blend, 0), 1), cs = (real)cos(L->angle * (1 - bl));
+        V bacc = v3(0, 0, 0);
+        for (int k = 0; k < STEPS; k++) {
+            real t = ((real)k + R(0.5)) * dt;
+            V p = add(ray->o, mul(ray->d, t));
+            V vv = sub(p, fv(L->position));
+            real d2 = rfmax(dot(vv, vv), R(1e-4));
+            real c = dot(vv, fv(L->direction)) * (R(1) / sqrt(d2));
+            if (c <= ch) continue;
+            real w = 1;
+            if (cs > ch + R(1e-4)) w = rfmin((c - ch) / (cs - ch), 1);
+            real dens = L->beam * L->intensity * R(1e-3) / (1 + R(0.25) * d2);
+            V target = fv(L->position);
+            if (L->radius > 0) {
+                V axis = nrm(neg(vv)), up = up_for(axis);
+                V t1 = nrm(cross(axis, up)), t2 = cross(axis, t1);
+                real rr = sqrt(aa_rand(seed ^ ((uint32_t)k * 2654435761u) ^ 0x85ebca6bu)) * L->radius;
+                real ph = R(6.2831853) * aa_rand(seed ^ ((uint32_t)k * 2246822519u) ^ 0xc2b2ae35u);
+                target = add(add(fv(L->position), mul(t1, cos(ph) * rr)), mul(t2, sin(ph) * rr));
+            }
+            V tl = sub(target, p);
+            real ld = sqrt(rfmax(dot(tl, tl), R(1e-8)));
+            V ldir = v3(tl.x / ld, tl.y / ld, tl.z / ld);
+            real remain = ld * R(0.999);
+            Ray sr;
+            sr.o = p; sr.d = ldir; sr.tmin = R(0.002); sr.tmax = remain;
+            int blocked = 0;
+            for (int pass = 0; pass < 3; pass++) {
+                Hit sh;
+                if (!scene_hit_opaque(S, &sr, &sh)) { blocked = 0; break; }
+                if (S->mats[sh.mat].transmission > R(0.5)) {
+                    remain -= sh.t + R(0.002);
+                    if (remain <= 0) { blocked = 0; break; }
+                    sr.o = add(sh.p, mul(ldir, R(0.002)));
+                    sr.tmax = remain;
+                    continue;
+                }
+                blocked = 1;
+                break;
+            }
+            if (blocked) continue;
+            bacc = add(bacc, mul(fv(L->color), dens * w * dt));
+        }
+        total = add(total, bacc);
+    }
+    return total;
+}
+
+/* Extension, no counterpart in the reference: reflect + refract recursion to
+ * S->bounces bounces.  Below the limit every hit blends as the reference's
+ * primary hit does (render_kernel.cu:730-731, 805): its lighting times
+ * (1 - wr)(1 - wt), a mirror ray times wr (1 - wt), a refracted ray times the
+ * face's transmission (wr = min(reflect, 1), wt = min(transmission, 1)); at
+ * the limit a hit gives its lighting alone.  A refracted ray crosses the face
+ * (exit eta = ior after an entry); a mirror ray and a totally reflected ray
+ * stay on their side.  Media act on every segment, beams on the primary ray
+ * only.  Paths are summed depth first in the order a stack gives (the mirror
+ * child is pushed last, so it is walked first), the device's order. */
+typedef struct { V o, d, w; int depth, inside; } DeepNode;
+
+static V render_deep(const OracleScene* S, Ray ray0, real pix, uint32_t seed) {
+    DeepNode st[10];
+    int sp = 0;
+    const int D = S->bounces < 8 ? S->bounces : 8;
+    st[sp].o = ray0.o; st[sp].d = ray0.d; st[sp].w = v3(1, 1, 1); st[sp].depth = 0; st[sp].inside = 0; sp++;
+    V color = v3(0, 0, 0);
+    while (sp > 0) {
+        const DeepNode nd = st[--sp];
+        Ray r;
+        r.o = nd.o; r.d = nd.d; r.tmin = R(0.001); r.tmax = R(1e10);
+        Hit h;
+        int hit = scene_hit(S, &r, &h);
+        V local = hit ? lighting(S, &h, neg(r.d), h.t * pix, seed) : sky(r.d);
+        if (nd.depth == 0) local = add(local, beams(S, &r, hit, hit ? h.t : 0, seed));
+        if (S->s.num_media > 0) {
+            real tau = 0;
+            V ins = media_march(S, &r, hit ? h.t : R(1e9), seed, &tau);
+            local = add(mul(local, (real)exp(-tau)), ins);
+        }
+        if (!hit || nd.depth >= D) { color = add(color, vmul(nd.w, local)); continue; }
+        const Material* m = &S->mats[h.mat];
+        real wr = m->reflect > 0 ? rfmin(m->reflect, 1) : 0;
+        real gtr = hit_transmission(S, &h, m);
+        real wt = gtr > 0 ? rfmin(gtr, 1) : 0;
+        color = add(color, mul(vmul(nd.w, local), (1 - wr) * (1 - wt)));
+        if (gtr > 0 && sp < 10) {
+            real ior = rfmax(hit_ior(S, &h, m), 1);
+            real eta = nd.inside ? ior : R(1) / ior;
+            real cosi = rfmax(-dot(r.d, h.n), R(1e-4));
+            real k = 1 - eta * eta * (1 - cosi * cosi);
+            V td = k < 0 ? nrm(add(r.d, mul(h.n, R(2) * cosi)))
+                         : nrm(add(mul(r.d, eta), mul(h.n, eta * cosi - sqrt(k))));
+            DeepNode c;
+            c.o = add(h.p, mul(td, R(0.002))); c.d = td; c.w = mul(nd.w, gtr);
+            c.depth = nd.depth + 1; c.inside = k < 0 ? nd.inside : !nd.inside;
+            st[sp++] = c;
+        }
+        if (wr > 0 && sp < 10) {
+            DeepNode c;
+            c.o = add(h.p, mul(h.n, R(0.002)));
+            c.d = nrm(sub(r.d, mul(h.n, R(2) * dot(r.d, h.n))));
+            c.w = mul(nd.w, wr * (1 - wt));
+            c.depth = nd.depth + 1; c.inside = nd.inside;
+            st[sp++] = c;
+        }
+    }
+    return color;
+}
+
 /* render_kernel.cu:438-814 -- one pixel */
 static void render_pixel(const OracleScene* S, int x, int y, int W, int H, int aa, float* out) {
     const CameraData* cam = &S->s.camera;
@@ -1801,61 +1921,11 @@ static void render_pixel(const OracleScene* S, int x, int y, int W, int H, int a
         ray.tmin = R(0.001);
         ray.tmax = R(1e10);
         const real pix = R(2) * tan_x / (real)W;
+        if (S->bounces > 1) { acc = add(acc, render_deep(S, ray, pix, seed)); continue; }
         Hit rec;
         int hit = scene_hit(S, &ray, &rec);
         V color = hit ? lighting(S, &rec, neg(ray.d), rec.t * pix, seed) : sky(ray.d);
-        for (int i = 0; i < S->s.num_lights; i++) {
-            const Light* L = &S->lights[i];
-            if (L->type != 3 || L->beam <= 0) continue;
-            real t_end = hit ? rfmin(rec.t, 30) : R(30);
-            if (t_end <= 0) continue;
-            const int STEPS = 6;
-            real dt = t_end / (real)STEPS, ch = (real)cos(L->angle);
-            real bl = rfmin(rfmax(L->blend, 0), 1), cs = (real)cos(L->angle * (1 - bl));
-            V bacc = v3(0, 0, 0);
-            for (int k = 0; k < STEPS; k++) {
-                real t = ((real)k + R(0.5)) * dt;
-                V p = add(ray.o, mul(ray.d, t));
-                V vv = sub(p, fv(L->position));
-                real d2 = rfmax(dot(vv, vv), R(1e-4));
-                real c = dot(vv, fv(L->direction)) * (R(1) / sqrt(d2));
-                if (c <= ch) continue;
-                real w = 1;
-                if (cs > ch + R(1e-4)) w = rfmin((c - ch) / (cs - ch), 1);
-                real dens = L->beam * L->intensity * R(1e-3) / (1 + R(0.25) * d2);
-                V target = fv(L->position);
-                if (L->radius > 0) {
-                    V axis = nrm(neg(vv)), up = up_for(axis);
-                    V t1 = nrm(cross(axis, up)), t2 = cross(axis, t1);
-                    real rr = sqrt(aa_rand(seed ^ ((uint32_t)k * 2654435761u) ^ 0x85ebca6bu)) * L->radius;
-                    real ph = R(6.2831853) * aa_rand(seed ^ ((uint32_t)k * 2246822519u) ^ 0xc2b2ae35u);
-                    target = add(add(fv(L->position), mul(t1, cos(ph) * rr)), mul(t2, sin(ph) * rr));
-                }
-                V tl = sub(target, p);
-                real ld = sqrt(rfmax(dot(tl, tl), R(1e-8)));
-                V ldir = v3(tl.x / ld, tl.y / ld, tl.z / ld);
-                real remain = ld * R(0.999);
-                Ray sr;
-                sr.o = p; sr.d = ldir; sr.tmin = R(0.002); sr.tmax = remain;
-                int blocked = 0;
-                for (int pass = 0; pass < 3; pass++) {
-                    Hit sh;
-                    if (!scene_hit_opaque(S, &sr, &sh)) { blocked = 0; break; }
-                    if (S->mats[sh.mat].transmission > R(0.5)) {
-                        remain -= sh.t + R(0.002);
-                        if (remain <= 0) { blocked = 0; break; }
-                        sr.o = add(sh.p, mul(ldir, R(0.002)));
-                        sr.tmax = remain;
-                        continue;
-                    }
-                    blocked = 1;
-                    break;
-                }
-                if (blocked) continue;
-                bacc = add(bacc, mul(fv(L->color), dens * w * dt));
-            }
-            color = add(color, bacc);
-        }
+        color = add(color, beams(S, &ray, hit, hit ? rec.t : 0, seed));
         if (S->s.num_media > 0) {
             real tau = 0;
             V ins = media_march(S, &ray, hit ? rec.t : R(1e9), seed, &tau);
@@ -2120,6 +2190,7 @@ OracleScene* oracle_scene_create_ext(const SheenScene* in, const SheenSceneExt* 
     if (x->num_csg_roots > 0) { S->csg_roots = (int*)dup(x->csg_roots, sizeof(int) * (size_t)x->num_csg_roots); S->ncsg_roots = x->num_csg_roots; }
     if (x->num_csg_boxes > 0) { S->csg_boxes = (SheenCsgBox*)dup(x->csg_boxes, sizeof(SheenCsgBox) * (size_t)x->num_csg_boxes); S->ncsg_boxes = x->num_csg_boxes; }
     if (x->num_csg_cones > 0) { S->csg_cones = (SheenCsgCone*)dup(x->csg_cones, sizeof(SheenCsgCone) * (size_t)x->num_csg_cones); S->ncsg_cones = x->num_csg_cones; }
+    S->bounces = x->max_depth > 1 ? (x->max_depth < 8 ? x->max_depth : 8) : 0;
     return S;
 }
 

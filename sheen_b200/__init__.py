@@ -29,6 +29,7 @@ LIB_PATH = os.path.join(_HERE, "libsheen_c_api.so")
 
 FORM_PLAIN = 0
 FORM_WAVEFRONT = 1
+PATH_PLAIN, PATH_QUEUES, PATH_MEGAKERNEL = 0, 1, 2   # sheen_scene_frame_path
 RENDER_COUNT_RAYS = 1
 RENDER_COUNT_NODES = 2
 
@@ -105,6 +106,8 @@ def lib():
     L.sheen_scene_device_bytes.restype = ctypes.c_ulonglong
     L.sheen_scene_form.argtypes = [P]
     L.sheen_scene_form.restype = I
+    L.sheen_scene_frame_path.argtypes = [P, I, I, I]
+    L.sheen_scene_frame_path.restype = I
     L.sheen_scene_render_device.argtypes = [P, I, I, I, P, P, I, ctypes.POINTER(RenderStats)]
     L.sheen_scene_render_device.restype = I
     L.sheen_scene_render_region.argtypes = [P, I, I, I, I, I, I, I, P, P, I, ctypes.POINTER(RenderStats)]
@@ -193,13 +196,16 @@ def render_rgba(scene, width: int, height: int, aa: int, form: int = FORM_PLAIN)
 
 
 class DeviceScene:
-    """A scene resident in HBM (SheenDeviceScene).  With ext, an OwnedScene's
-    extension arrays (sheen_owned_ext) are passed to sheen_scene_create_ext."""
+    """A scene resident in HBM (SheenDeviceScene).  With ext=True, an
+    OwnedScene's extension arrays (sheen_owned_ext) are passed to
+    sheen_scene_create_ext; ext may also be a contract.SheenSceneExt."""
 
-    def __init__(self, scene, form: int = FORM_PLAIN, ext: bool = False):
+    def __init__(self, scene, form: int = FORM_PLAIN, ext=False):
         ptr, keep = _scene_ptr(scene)
         h = ctypes.c_void_p()
-        if ext:
+        if isinstance(ext, contract.SheenSceneExt):
+            _check(lib().sheen_scene_create_ext(ptr, ctypes.addressof(ext), form, ctypes.byref(h)))
+        elif ext:
             if not isinstance(scene, OwnedScene):
                 raise TypeError("scene extensions come from an OwnedScene")
             _check(lib().sheen_scene_create_ext(ptr, scene.ext_ptr, form, ctypes.byref(h)))
@@ -208,6 +214,14 @@ class DeviceScene:
         del keep
         self.handle = h.value
         self.form = form
+
+    def frame_path(self, width, height, aa) -> int:
+        """PATH_PLAIN, PATH_QUEUES or PATH_MEGAKERNEL: the kernels that render
+        a whole frame of this size (sheen_scene_frame_path)."""
+        r = lib().sheen_scene_frame_path(self.handle, width, height, aa)
+        if r < 0:
+            raise RuntimeError(last_error())
+        return r
 
     @property
     def device_bytes(self) -> int:
@@ -328,8 +342,9 @@ def load_scene_file(path: str) -> OwnedScene:
 
 def generate_scene(config: int, seed: int = 1, detail: int = 0, photons: int = 0,
                    extended: bool = False) -> OwnedScene:
-    """A workload scene; extended (config 2): with its extension column
-    (sheen_generate_scene_ext)."""
+    """A workload scene; extended: with its extension column
+    (sheen_generate_scene_ext) -- config 1 with reflect + refract recursion
+    to 4 bounces, config 2 with the extension shapes."""
     h = ctypes.c_void_p()
     if extended:
         _check(lib().sheen_generate_scene_ext(config, seed, detail, photons, 1, ctypes.byref(h)))

@@ -133,6 +133,20 @@ assert ctypes.sizeof(SheenScene) == 352
 assert SheenScene.photons.offset == 316 and SheenScene.media.offset == 328
 
 
+class SheenSceneExt(ctypes.Structure):
+    """ctypes view of this library's ``SheenSceneExt`` (scene extensions, no
+    counterpart in the reference's contract).  Pointer fields are untyped."""
+    _fields_ = [
+        ("lathe_bezier", _P), ("prism_bezier", _P), ("bezier_ctrl", _P), ("num_bezier_ctrl", _I),
+        ("se_n2", _P),
+        ("hf_grid", _P), ("hf_heights", _P), ("num_hf_heights", _I),
+        ("csg_roots", _P), ("num_csg_roots", _I),
+        ("csg_boxes", _P), ("num_csg_boxes", _I),
+        ("csg_cones", _P), ("num_csg_cones", _I),
+        ("max_depth", _I),
+    ]
+
+
 def _ptr(a):
     return a.ctypes.data if a is not None and len(a) else None
 

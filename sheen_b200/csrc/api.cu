@@ -163,6 +163,13 @@ int sheen_scene_form(SheenDeviceScene h) {
     return s ? s->form : -1;
 }
 
+int sheen_scene_frame_path(SheenDeviceScene h, int W, int H, int aa) {
+    auto* s = reinterpret_cast<sheen::DeviceScene*>(h);
+    if (!s) { sheen::set_error("null scene handle"); return -1; }
+    if (W <= 0 || H <= 0 || aa < 1 || aa > 64) { sheen::set_error("bad render params"); return -1; }
+    return sheen::frame_path(*s, W, H, aa);
+}
+
 int sheen_scene_render_device(SheenDeviceScene h, int W, int H, int aa, float* out, void* stream, int flags,
                               SheenRenderStats* stats) {
     auto* s = reinterpret_cast<sheen::DeviceScene*>(h);

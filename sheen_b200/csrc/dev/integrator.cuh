@@ -292,5 +292,74 @@ __device__ float3 render_sample(const DevScene& S, int x, int y, int s, int ns, 
     return color;
 }
 
+// Extension (no counterpart in the reference, whose mirror ray stops at
+// depth 1 and whose refraction follows at most three faces): reflect +
+// refract recursion to S.bounces bounces.  Every hit below the depth
+// limit blends as the reference's primary hit does (render_kernel.cu:
+// 730-731, 805) -- its lighting weighted by (1 - wr)(1 - wt), a mirror ray by
+// wr (1 - wt) and a refracted ray by the face's transmission, wr =
+// min(reflect, 1), wt = min(transmission, 1) -- and a hit at the limit
+// contributes its lighting alone, as the reference's depth-1 mirror hit
+// does.  A refracted ray crosses the face (the next glass face it meets is
+// an exit: eta = ior, then an entry again); a mirror ray, and a ray turned
+// back by total internal reflection, stays on its side.  Media act on every
+// segment (the reference marches them on the primary and the mirror ray),
+// beams on the primary ray only.  Paths are walked depth first with an
+// explicit stack (at most one pending sibling per bounce); the sum runs in
+// that fixed order.
+template <class T, bool COUNT>
+__device__ __noinline__ float3 render_sample_deep(const DevScene& S, int x, int y, int s, int ns, int W, int H,
+                                                  RayTally& rt, Counters& c) {
+    struct Node {
+        float3 o, d, w;
+        int depth, inside;
+    };
+    float pix;
+    const Ray ray0 = camera_ray(S.cam, x, y, s, ns, W, H, pix, S.aa_centered);
+    const uint32_t seed = sample_seed(x, y, s);
+    const int D = S.bounces < kMaxDeepBounces ? S.bounces : kMaxDeepBounces;
+    Node st[kMaxDeepBounces + 2];
+    int sp = 0;
+    st[sp++] = Node{ray0.o, ray0.d, f3(1.0f, 1.0f, 1.0f), 0, 0};
+    float3 color = f3(0.0f, 0.0f, 0.0f);
+    while (sp > 0) {
+        const Node nd = st[--sp];
+        Ray r;
+        r.o = nd.o; r.d = nd.d; r.tmin = 0.001f; r.tmax = 1.0e10f;
+        Hit h;
+        if (nd.depth == 0) rt.primary++;
+        else rt.secondary++;
+        const bool hit = T::closest(S, r, h, c);
+        float3 local = hit ? lighting<T, COUNT>(S, h, -r.d, h.t * pix, seed, rt, c) : sky(r.d);
+        if (nd.depth == 0) local += beams<T, COUNT>(S, r, hit, hit ? h.t : 0.0f, seed, rt, c);
+        if (S.num_media > 0) {
+            float tau = 0.0f;
+            const float3 ins = media_march<T, COUNT>(S, r, hit ? h.t : 1.0e9f, seed, tau, rt, c);
+            local = local * expf(-tau) + ins;
+        }
+        if (!hit || nd.depth >= D) { color += nd.w * local; continue; }
+        const Material m = S.materials[h.mat];
+        const float wr = m.reflect > 0.0f ? fminf(m.reflect, 1.0f) : 0.0f;
+        const float gtr = transmission_at(S, m, h.uv);
+        const float wt = gtr > 0.0f ? fminf(gtr, 1.0f) : 0.0f;
+        color += nd.w * local * ((1.0f - wr) * (1.0f - wt));
+        if (gtr > 0.0f && sp < kMaxDeepBounces + 2) {
+            const float ior = fmaxf(ior_at(S, m, h.uv), 1.0f);
+            const float eta = nd.inside ? ior : 1.0f / ior;
+            const float cosi = fmaxf(-dot(r.d, h.n), 1.0e-4f);
+            const float k = 1.0f - eta * eta * (1.0f - cosi * cosi);
+            const float3 td = k < 0.0f ? normalize(r.d + 2.0f * cosi * h.n)
+                                       : normalize(eta * r.d + (eta * cosi - sqrtf(k)) * h.n);
+            st[sp++] = Node{h.p + td * 0.002f, td, nd.w * gtr, nd.depth + 1, k < 0.0f ? nd.inside : !nd.inside};
+        }
+        if (wr > 0.0f && sp < kMaxDeepBounces + 2) {
+            const float3 rd = normalize(r.d - h.n * (2.0f * dot(r.d, h.n)));
+            st[sp++] = Node{h.p + h.n * 0.002f, rd, nd.w * (wr * (1.0f - wt)), nd.depth + 1, nd.inside};
+        }
+    }
+    return color;
+}
+
 }  // namespace dev
 }  // namespace sheen
+

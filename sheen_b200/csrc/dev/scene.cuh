@@ -58,6 +58,9 @@ struct QMesh {
     int watertight;
 };
 
+// Reflect + refract recursion depth limit of the extension scenes.
+constexpr int kMaxDeepBounces = 8;
+
 struct DevScene {
     CameraData cam;
 
@@ -117,6 +120,7 @@ struct DevScene {
     const BvhNode* csg_root_bvh;   // median BVH over the further roots' leaf boxes
     const float4* csg_boxes;       // leaf_kind 2: {lo, material as int}, {hi, 0}
     const float4* csg_cones;       // leaf_kind 3: {p0, r0}, {p1, r1}, {material as int, 0, 0, 0}
+    int bounces;                   // reflect + refract bounces (> 1: the recursion of render_sample_deep)
 };
 
 struct Ray {

@@ -160,6 +160,8 @@ cudaError_t launch_wavefront_scratch(DeviceScene& s, void* scratch, size_t scrat
                                      Region rg, float4* out, cudaStream_t stream, unsigned long long* tally);
 size_t wave_scratch_bytes(int L, long long nsamples);
 bool wave_pipeline_used(const DeviceScene& s);
+// Which kernels render a whole W x H frame at aa spp (SHEEN_PATH_*).
+int frame_path(const DeviceScene& s, int W, int H, int aa);
 
 // One job of a multi-job wavefront launch: region rg of a W x H frame of
 // scene s at aa samples per pixel into the device image `out` (W*H float4).

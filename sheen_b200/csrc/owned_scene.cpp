@@ -70,6 +70,7 @@ void OwnedScene::finalize() {
         x.num_csg_boxes = (int)csg_boxes.size();
         x.csg_cones = ptr(csg_cones);
         x.num_csg_cones = (int)csg_cones.size();
+        x.max_depth = max_depth;
     }
     v.texture_pixels = tex_ptrs.empty() ? nullptr : tex_ptrs.data();
     v.texture_widths = tex_w.empty() ? nullptr : tex_w.data();

@@ -47,6 +47,7 @@ struct OwnedScene {
     std::vector<int> csg_roots;
     std::vector<SheenCsgBox> csg_boxes;
     std::vector<SheenCsgCone> csg_cones;
+    int max_depth = 0;                       // reflect + refract recursion (SheenSceneExt.max_depth)
 
     // C views (rebuilt by finalize()).
     SheenScene view{};

@@ -28,7 +28,12 @@ __global__ void __launch_bounds__(128) mega_bvh4_kernel(DevScene S, float4* __re
     if (x < x1 && y < y1) {
         const int ns = aa < 1 ? 1 : (aa > 64 ? 64 : aa);
         float3 acc = f3(0.0f, 0.0f, 0.0f);
-        for (int s = 0; s < ns; s++) acc += render_sample<FastTracer<COUNT, F>, COUNT>(S, x, y, s, ns, W, H, rt, c);
+        if (S.bounces > 1) {   // extension: reflect + refract recursion
+            for (int s = 0; s < ns; s++)
+                acc += render_sample_deep<FastTracer<COUNT, F>, COUNT>(S, x, y, s, ns, W, H, rt, c);
+        } else {
+            for (int s = 0; s < ns; s++) acc += render_sample<FastTracer<COUNT, F>, COUNT>(S, x, y, s, ns, W, H, rt, c);
+        }
         const float inv = 1.0f / float(ns);
         out[(size_t)y * W + x] = make_float4(acc.x * inv, acc.y * inv, acc.z * inv, 1.0f);
     }

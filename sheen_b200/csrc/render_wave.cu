@@ -27,8 +27,9 @@
 // so uneven work (glass, empty sky) balances across the SMs.
 //
 // Frames the queue pipeline does not cover -- visible spot beams, media, a
-// material in the shadow-debug mode (shininess < 0), or more than 16
-// lights -- run on the BVH4 megakernel with identical results.
+// material in the shadow-debug mode (shininess < 0), more than 16 lights,
+// or reflect + refract recursion (an extension scene's max_depth > 1) --
+// run on the BVH4 megakernel with identical results.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -1044,7 +1045,7 @@ void wave_release(DeviceScene& s) {
 
 static bool wave_supported(const DeviceScene& s) {
     const dev::DevScene& v = s.view;
-    if (v.num_media > 0 || v.num_lights > dev::kMaxWaveLights) return false;
+    if (v.num_media > 0 || v.num_lights > dev::kMaxWaveLights || v.bounces > 1) return false;
     return !s.wave_fallback;
 }
 
@@ -1202,6 +1203,13 @@ cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, fl
 }
 
 bool wave_pipeline_used(const DeviceScene& s) { return wave_supported(s); }
+
+int frame_path(const DeviceScene& s, int W, int H, int aa) {
+    if (s.form != SHEEN_FORM_WAVEFRONT) return SHEEN_PATH_PLAIN;
+    if (!wave_supported(s)) return SHEEN_PATH_MEGAKERNEL;
+    const long long nsamples = region_padded(Region{0, 0, W, H}, tile_log2()) * clamp_spp(aa);
+    return small_frame(s, nsamples) ? SHEEN_PATH_MEGAKERNEL : SHEEN_PATH_QUEUES;
+}
 
 // Many frames, regions and scenes in one pass of the queue kernels: every
 // stage is one persistent launch over the samples of all jobs, whose work

@@ -324,11 +324,17 @@ extern "C" int sheen_generate_scene_ext(int config, unsigned int seed, int detai
                                         SheenOwnedScene* out) {
     if (!out) { sheen::set_error("null output handle"); return -1; }
     *out = nullptr;
-    if (extended && config != 2) { sheen::set_error("extended generator exists for config 2 only"); return -1; }
+    if (extended && config != 1 && config != 2) {
+        sheen::set_error("extended generator exists for configs 1 and 2 only");
+        return -1;
+    }
     OwnedScene* s = new OwnedScene();
     switch (config) {
         case 0: gen_spheres(*s, seed); break;
-        case 1: gen_mesh(*s, seed, detail > 0 ? detail : 8); break;
+        case 1:
+            gen_mesh(*s, seed, detail > 0 ? detail : 8);
+            if (extended) s->max_depth = 4;   // reflect + refract recursion to 4 bounces
+            break;
         case 2: sheen::gen_analytic(*s, seed, detail, extended != 0); break;
         case 3: gen_caustics(*s, seed, photons > 0 ? photons : 4000000); break;
         default:

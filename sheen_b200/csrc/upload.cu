@@ -286,6 +286,7 @@ const char* scene_index_error(const SheenScene* in, const SheenSceneExt* ext) {
         if (ext->num_csg_boxes < 0 || ext->num_csg_cones < 0 || ext->num_bezier_ctrl < 0 || ext->num_hf_heights < 0 ||
             ext->num_csg_roots < 0)
             return "negative extension count";
+        if (ext->max_depth < 0 || ext->max_depth > dev::kMaxDeepBounces) return "max_depth outside 0..8";
         if ((ext->num_csg_boxes > 0 && !ext->csg_boxes) || (ext->num_csg_cones > 0 && !ext->csg_cones) ||
             (ext->num_bezier_ctrl > 0 && !ext->bezier_ctrl) || (ext->num_hf_heights > 0 && !ext->hf_heights))
             return "null extension array with a nonzero count";
@@ -898,6 +899,7 @@ int scene_upload_ext(const SheenScene* in, const SheenSceneExt* ext, int form, D
     v.csg_root_bvh = (const dev::BvhNode*)dptr(o_crbvh);
     v.csg_boxes = (const float4*)dptr(o_cbox);
     v.csg_cones = (const float4*)dptr(o_ccone);
+    v.bounces = ext && ext->max_depth > 1 ? std::min(ext->max_depth, (int)dev::kMaxDeepBounces) : 0;
     s->d_tally = (unsigned long long*)dptr(o_tally);
     s->wave_depth = std::max(q_all.max_depth, std::max(q_block.max_depth, q_pass.max_depth));
     s->build_ms = t1 - t0;

@@ -39,10 +39,14 @@ def _render(ds, W, H, aa, mega):
 def test_default_rule_picks_the_megakernel_for_small_frames():
     assert sb.tune_get("wave.mega_samples") == 327680
     spheres = sb.DeviceScene(sb.generate_scene(0, 1), sb.FORM_WAVEFRONT)
+    assert spheres.frame_path(640, 480, 1) == sb.PATH_MEGAKERNEL
+    assert spheres.frame_path(1920, 1080, 1) == sb.PATH_QUEUES
     d = _render(spheres, 640, 480, 1, None)
     assert np.array_equal(d, _render(spheres, 640, 480, 1, True))
     spheres.close()
     mesh = sb.DeviceScene(sb.generate_scene(1, 1, 4), sb.FORM_WAVEFRONT)
+    assert mesh.frame_path(640, 480, 1) == sb.PATH_QUEUES
+    assert mesh.frame_path(320, 240, 1) == sb.PATH_MEGAKERNEL
     d = _render(mesh, 640, 480, 1, None)           # 307200 samples > 327680 / 4
     assert np.array_equal(d, _render(mesh, 640, 480, 1, False))
     d = _render(mesh, 320, 240, 1, None)           # 76800 samples <= 81920
