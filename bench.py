@@ -175,10 +175,26 @@ WORKLOADS = {
 
 
 EXT_WORKLOADS = {
-    1: "reflect + refract recursion to 4 bounces (BVH4 megakernel)",
+    1: "16 tori as instances of one 50,000-triangle mesh (two-level BVH), reflect + refract recursion to 4 "
+       "bounces (BVH4 megakernel)",
     2: "exact cubic-Bezier lathes and prisms (FP64 root isolation), two-exponent superellipsoids, "
        "1024x1024 FP32 height grid, 128 more CSG trees over spheres, boxes and cones",
 }
+
+
+def scene_ext(scene, args):
+    """The extension handed to sheen_scene_create_ext: False without
+    --extended, the generator's own (True), or a copy with --max-depth."""
+    import ctypes
+
+    from sheen_b200 import contract as C
+    if not args.extended:
+        return False
+    if args.max_depth < 0:
+        return True
+    x = C.SheenSceneExt.from_buffer_copy(ctypes.string_at(scene.ext_ptr, ctypes.sizeof(C.SheenSceneExt)))
+    x.max_depth = args.max_depth
+    return x
 
 
 def make_scene(args):
@@ -219,13 +235,14 @@ def run_ours(args):
     # the drop-in caller's situation.
     # (scenes with extensions: sheen_scene_create_ext + render to a host
     # buffer + destroy, the extension's public path)
+    ext_arg = scene_ext(scene, args)
     img = np.empty((H, W, 4), np.float32)
     e2e_steps = max(1, min(args.steps, 3))
 
     def one_call():
         if not args.extended:
             return sb.render_rgba(scene, W, H, SPP, form)
-        d = sb.DeviceScene(scene, form, ext=True)
+        d = sb.DeviceScene(scene, form, ext=ext_arg)
         out_img, out_st = d.render_host(W, H, SPP)
         d.close()
         return out_img, out_st
@@ -241,7 +258,7 @@ def run_ours(args):
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
 
     t0 = time.perf_counter()
-    ds = sb.DeviceScene(scene, form, ext=args.extended)
+    ds = sb.DeviceScene(scene, form, ext=ext_arg)
     create_s = time.perf_counter() - t0
     out = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # > 126 MB L2
@@ -379,13 +396,15 @@ def run_ours(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generator)",
         "config": {"workload": WORKLOADS.get(args.config, f"config {args.config}")
-                   + (" + extension column: " + EXT_WORKLOADS[args.config] if args.extended else ""),
+                   + (" + extension column: " + EXT_WORKLOADS[args.config] if args.extended else "")
+                   + (" (max_depth %d)" % args.max_depth if args.extended and args.max_depth >= 0 else ""),
                    "triangles": scene.view.num_triangles, "width": W, "height": H, "spp": SPP,
                    "form": args.form, "parallelism": f"replicas{world}",
                    "frame": (f"{args.tiles} uneven tiles in one batched pass" if args.tiles > 0
                              else "whole frame, one BVH4 megakernel launch (%s)" % (
                                  "reflect + refract recursion runs outside the queue stages"
-                                 if args.extended and args.config == 1 else "small frame") if mega
+                                 if args.extended and args.config == 1 and args.max_depth != 0 and
+                                 args.max_depth != 1 else "small frame") if mega
                              else "whole frame, captured CUDA graph"),
                    "l2": "256 MB buffer written between timed frames; scene arrays exceed L2",
                    "rays_per_frame": rays, "box_tests_per_frame": nodes, "prim_tests_per_frame": prims,
@@ -738,11 +757,14 @@ def run_serving(args):
 
 
 CAPTURE_CASES = {
-    # name: (generator config, detail, photons, width, height, spp, form, small-frame switch on)
-    "wave": (1, 8, 0, 640, 360, 4, "wavefront", False),
-    "plain": (1, 8, 0, 640, 360, 4, "plain", False),
-    "mega": (0, 0, 0, 640, 480, 1, "wavefront", True),
-    "photon": (3, 0, 1000000, 320, 180, 1, "wavefront", True),
+    # name: (generator config, detail, photons, width, height, spp, form, small-frame switch on,
+    #        extension max_depth or None for no extension)
+    "wave": (1, 8, 0, 640, 360, 4, "wavefront", False, None),
+    "plain": (1, 8, 0, 640, 360, 4, "plain", False, None),
+    "mega": (0, 0, 0, 640, 480, 1, "wavefront", True, None),
+    "photon": (3, 0, 1000000, 320, 180, 1, "wavefront", True, None),
+    "wave_inst": (1, 8, 0, 640, 360, 4, "wavefront", False, 0),
+    "mega_deep": (1, 8, 0, 640, 360, 4, "wavefront", True, 4),
 }
 
 
@@ -751,16 +773,22 @@ def run_capture(name):
     wave / plain: the mesh workload at 640x360 4 spp through the queue stages
     or the plain form; mega: the spheres workload at 640x480 1 spp (the
     small-frame megakernel); photon: the caustics workload with 1M photons
-    per light (its scene build runs the photon emission)."""
+    per light (its scene build runs the photon emission); wave_inst: the mesh
+    workload with instanced tori at 640x360 4 spp through the queue stages;
+    mega_deep: the same with reflect + refract recursion to 4 bounces (BVH4
+    megakernel)."""
     import torch
 
     import sheen_b200 as sb
-    cfg, detail, photons, w, h, spp, form, mega = CAPTURE_CASES[name]
+    cfg, detail, photons, w, h, spp, form, mega, depth = CAPTURE_CASES[name]
     sb.init(0, 100)
     if not mega:
         sb.tune_set("wave.mega_samples", 0)
-    ds = sb.DeviceScene(sb.generate_scene(cfg, 1, detail, photons),
-                        sb.FORM_WAVEFRONT if form == "wavefront" else sb.FORM_PLAIN)
+    scene = sb.generate_scene(cfg, 1, detail, photons, extended=depth is not None)
+    ext = False
+    if depth is not None:
+        ext = scene_ext(scene, argparse.Namespace(extended=True, max_depth=depth))
+    ds = sb.DeviceScene(scene, sb.FORM_WAVEFRONT if form == "wavefront" else sb.FORM_PLAIN, ext=ext)
     out = torch.empty((h, w, 4), dtype=torch.float32, device="cuda")
     ds.render_device(w, h, spp, out.data_ptr(), torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
@@ -800,6 +828,9 @@ def main():
                          "bounces; config 2: exact Bezier lathes and prisms, two-exponent superellipsoids, "
                          "FP32 height grid, 128 CSG trees; the reference has none of these, so the line "
                          "carries no reference or host-array legs")
+    ap.add_argument("--max-depth", type=int, default=-1,
+                    help="with --extended: the extension's reflect + refract depth instead of the generator's "
+                         "(0: the reference's depth-1 rules)")
     ap.add_argument("--capture", choices=sorted(CAPTURE_CASES),
                     help="render one small frame of a named case and exit (for profiler captures)")
     args = ap.parse_args()

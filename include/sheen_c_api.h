@@ -200,6 +200,22 @@ typedef struct SheenHeightGrid {    /* w x h FP32 heights in [0, 1], row-major, 
     int w, h;
 } SheenHeightGrid;
 
+/* One mesh of the instanced geometry: a run of SheenSceneExt.mesh_triangles. */
+typedef struct SheenMesh {
+    int tri_offset;
+    int tri_count;
+} SheenMesh;
+
+/* One placement of a mesh: xform is the 3x4 affine map from the mesh's
+ * object space to the world, row-major (world = xform[:, 0:3] p +
+ * xform[:, 3]); it must be invertible.  The instance draws every triangle
+ * of the mesh with material_id. */
+typedef struct SheenInstance {
+    float xform[12];
+    int mesh;
+    int material_id;
+} SheenInstance;
+
 typedef struct SheenSceneExt {
     /* Exact cubic-Bezier surfaces, replacing the tessellation the reference
      * renders (its loader turns Bezier profiles into polylines on the
@@ -250,6 +266,24 @@ typedef struct SheenSceneExt {
      * the primary ray only.  Such scenes render on the BVH4 megakernel
      * (wavefront form) or the plain kernel. */
     int max_depth;
+    /* Instanced meshes in a two-level BVH: mesh_triangles hold every mesh's
+     * object-space triangles (their material_id is not used), meshes[i] a
+     * run of them, instances[j] one placement.  A BVH4 is built per mesh
+     * in object space and a BVH over the instances' world boxes; a query
+     * enters a mesh through the instance's inverse map (t is the same in
+     * both spaces).  Instanced triangles belong to the mesh category like
+     * the scene's own (a query's mesh hit is the closest over both), and a
+     * hit on triangle k of instance j reports the object id
+     * -(num_triangles + 1 + base_j + k), base_j the triangles of the
+     * instances before j: the index it would have with the instances
+     * flattened after the scene's triangles.  At most 2^31 - 1 triangles
+     * flattened. */
+    const Triangle* mesh_triangles;
+    int num_mesh_triangles;
+    const SheenMesh* meshes;
+    int num_meshes;
+    const SheenInstance* instances;
+    int num_instances;
 } SheenSceneExt;
 
 /* sheen_scene_create with extensions (ext may be NULL).  Fails with a
@@ -532,8 +566,9 @@ int sheen_generate_scene(int config, unsigned int seed, int detail, int photons,
                          SheenOwnedScene* out);
 
 /* The workload generators with their extension column (no counterpart in
- * the reference).  extended != 0, config 1: the same scene with reflect +
- * refract recursion to 4 bounces (SheenSceneExt.max_depth).  Config 2: the
+ * the reference).  extended != 0, config 1: the same scene with its 16 tori
+ * as instances of one 50,000-triangle mesh (SheenSceneExt.instances) and
+ * reflect + refract recursion to 4 bounces (SheenSceneExt.max_depth).  Config 2: the
  * same scene with
  * two-exponent superellipsoids (both exponents 2/e, e uniform in [0.2, 3]),
  * the lathes' and prisms' Bezier control points as exact surfaces, a

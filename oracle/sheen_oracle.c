@@ -2174,8 +2174,71 @@ static void add_runs(OracleScene* S, const SheenSceneExt* x, const SheenBezierRu
     }
 }
 
+/* Instanced meshes (extension): flattened after the scene's own triangles,
+ * instance by instance, so that triangle k of instance j has the index
+ * num_triangles + base_j + k the library reports.  Positions go through the
+ * object-to-world map and vertex normals through its inverse transpose,
+ * both in double and rounded once; the triangles take the instance's
+ * material. */
+static Triangle* flatten_instances(const SheenScene* in, const SheenSceneExt* x, int* count) {
+    long long n = in->num_triangles > 0 ? in->num_triangles : 0;
+    for (int j = 0; j < x->num_instances; j++) n += x->meshes[x->instances[j].mesh].tri_count;
+    Triangle* out = (Triangle*)calloc((size_t)(n > 0 ? n : 1), sizeof(Triangle));
+    if (in->num_triangles > 0) memcpy(out, in->triangles, sizeof(Triangle) * (size_t)in->num_triangles);
+    long long k = in->num_triangles > 0 ? in->num_triangles : 0;
+    for (int j = 0; j < x->num_instances; j++) {
+        const SheenInstance* I = &x->instances[j];
+        const float* f = I->xform;
+        double M[3][3], T[3], A[3][3];
+        for (int r = 0; r < 3; r++) { for (int c = 0; c < 3; c++) M[r][c] = f[4 * r + c]; T[r] = f[4 * r + 3]; }
+        double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                     M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+        /* inverse transpose = cofactor matrix / det */
+        A[0][0] = (M[1][1] * M[2][2] - M[1][2] * M[2][1]) / det;
+        A[0][1] = (M[1][2] * M[2][0] - M[1][0] * M[2][2]) / det;
+        A[0][2] = (M[1][0] * M[2][1] - M[1][1] * M[2][0]) / det;
+        A[1][0] = (M[0][2] * M[2][1] - M[0][1] * M[2][2]) / det;
+        A[1][1] = (M[0][0] * M[2][2] - M[0][2] * M[2][0]) / det;
+        A[1][2] = (M[0][1] * M[2][0] - M[0][0] * M[2][1]) / det;
+        A[2][0] = (M[0][1] * M[1][2] - M[0][2] * M[1][1]) / det;
+        A[2][1] = (M[0][2] * M[1][0] - M[0][0] * M[1][2]) / det;
+        A[2][2] = (M[0][0] * M[1][1] - M[0][1] * M[1][0]) / det;
+        const SheenMesh* me = &x->meshes[I->mesh];
+        for (int t = 0; t < me->tri_count; t++, k++) {
+            Triangle tr = x->mesh_triangles[me->tri_offset + t];
+            sheen_float3* vs[3] = {&tr.v0, &tr.v1, &tr.v2};
+            sheen_float3* ns[3] = {&tr.n0, &tr.n1, &tr.n2};
+            for (int v = 0; v < 3; v++) {
+                const double p[3] = {vs[v]->x, vs[v]->y, vs[v]->z}, q[3] = {ns[v]->x, ns[v]->y, ns[v]->z};
+                double w[3], m[3];
+                for (int r = 0; r < 3; r++) {
+                    w[r] = M[r][0] * p[0] + M[r][1] * p[1] + M[r][2] * p[2] + T[r];
+                    m[r] = A[r][0] * q[0] + A[r][1] * q[1] + A[r][2] * q[2];
+                }
+                vs[v]->x = (float)w[0]; vs[v]->y = (float)w[1]; vs[v]->z = (float)w[2];
+                ns[v]->x = (float)m[0]; ns[v]->y = (float)m[1]; ns[v]->z = (float)m[2];
+            }
+            tr.material_id = I->material_id;
+            out[k] = tr;
+        }
+    }
+    *count = (int)n;
+    return out;
+}
+
 OracleScene* oracle_scene_create_ext(const SheenScene* in, const SheenSceneExt* x) {
-    OracleScene* S = oracle_scene_create(in);
+    OracleScene* S;
+    if (in && x && x->num_instances > 0) {
+        SheenScene flat = *in;
+        int n = 0;
+        Triangle* tris = flatten_instances(in, x, &n);
+        flat.triangles = tris;
+        flat.num_triangles = n;
+        S = oracle_scene_create(&flat);
+        free(tris);
+    } else {
+        S = oracle_scene_create(in);
+    }
     if (!S || !x) return S;
     if (x->se_n2 && in->num_superellipsoids > 0) S->se_n2 = (float*)dup(x->se_n2, sizeof(float) * (size_t)in->num_superellipsoids);
     if (x->hf_grid && in->num_heightfields > 0) {

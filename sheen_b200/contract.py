@@ -144,7 +144,20 @@ class SheenSceneExt(ctypes.Structure):
         ("csg_boxes", _P), ("num_csg_boxes", _I),
         ("csg_cones", _P), ("num_csg_cones", _I),
         ("max_depth", _I),
+        ("mesh_triangles", _P), ("num_mesh_triangles", _I),
+        ("meshes", _P), ("num_meshes", _I),
+        ("instances", _P), ("num_instances", _I),
     ]
+
+
+class SheenInstance(ctypes.Structure):
+    """ctypes view of ``SheenInstance``: a mesh placed by a row-major 3x4
+    object-to-world map."""
+    _fields_ = [("xform", ctypes.c_float * 12), ("mesh", _I), ("material_id", _I)]
+
+
+class SheenMesh(ctypes.Structure):
+    _fields_ = [("tri_offset", _I), ("tri_count", _I)]
 
 
 def _ptr(a):

@@ -10,7 +10,7 @@
 //   strand_depth(S, r, c)                 strand_bvh_tau (bvh.h:928-960)
 #pragma once
 #include "shade.cuh"
-#include "trace_ref.cuh"
+#include "trace_bvh4.cuh"   // both query policies, instanced meshes
 
 namespace sheen {
 namespace dev {

@@ -58,6 +58,12 @@ struct QMesh {
     int watertight;
 };
 
+// float4 per instance record: world-to-object rows (3), object-to-world
+// rows (3), {mesh, material, base - first triangle of the mesh, passable},
+// {base, triangles, first triangle of the mesh, 0} (ints); base = the
+// triangles of the instances before it.
+constexpr int kInstRecord = 8;
+
 // Reflect + refract recursion depth limit of the extension scenes.
 constexpr int kMaxDeepBounces = 8;
 
@@ -121,6 +127,15 @@ struct DevScene {
     const float4* csg_boxes;       // leaf_kind 2: {lo, material as int}, {hi, 0}
     const float4* csg_cones;       // leaf_kind 3: {p0, r0}, {p1, r1}, {material as int, 0, 0, 0}
     int bounces;                   // reflect + refract bounces (> 1: the recursion of render_sample_deep)
+    // Instanced meshes (two-level BVH); num_instances 0 without.
+    const Triangle* inst_tris;     // every mesh's object-space triangles
+    const QMesh* inst_mesh;        // per mesh: its BVH4 in object space
+    const float4* inst_xf;         // per instance kInstRecord float4 (dev/instances.cuh)
+    const QNode4* tlas_nodes;      // BVH4 over the instances' world boxes (root node 0)
+    const int* tlas_items;         // per top-level leaf slot: instance (num_instances: the scene's triangles)
+    int num_instances;
+    int inst_tri_total;            // triangles of all instances (flattened count)
+    int inst_flat_leaf;            // 1: top-level leaf num_instances is the scene's own triangles
 };
 
 struct Ray {

@@ -93,6 +93,59 @@ struct ShadePoint {
     int mat;
 };
 
+// Texture footprint scale and tangent frame of a triangle hit from its
+// world edges and uv deltas (render_kernel.cu:82-114).
+__device__ __forceinline__ void tri_lod(float3 e1, float3 e2, sheen_float2 uv0, sheen_float2 uv1, sheen_float2 uv2,
+                                        float3 n, float footprint, float& uv_fp, float3& tu, float3& tv) {
+    float2 d1 = make_float2(uv1.x - uv0.x, uv1.y - uv0.y);
+    float2 d2 = make_float2(uv2.x - uv0.x, uv2.y - uv0.y);
+    float w1 = sqrtf(dot(e1, e1)), w2 = sqrtf(dot(e2, e2));
+    float u1 = sqrtf(d1.x * d1.x + d1.y * d1.y), u2 = sqrtf(d2.x * d2.x + d2.y * d2.y);
+    float a1 = w1 > 1.0e-6f ? u1 / w1 : 0.0f, a2 = w2 > 1.0e-6f ? u2 / w2 : 0.0f;
+    float dens = a1 > a2 ? a1 : a2;
+    if (dens > 1.0e-6f) uv_fp = footprint * dens;
+    float det = d1.x * d2.y - d2.x * d1.y;
+    if (fabsf(det) > 1.0e-8f) {
+        float3 du = (e1 * d2.y - e2 * d1.y) / det;
+        float3 dv = (e2 * d1.x - e1 * d2.x) / det;
+        du = du - n * dot(du, n);
+        dv = dv - n * dot(dv, n);
+        float lu = dot(du, du);
+        if (lu > 1.0e-12f) {
+            tu = du * rsqrtf(lu);
+            dv = dv - tu * dot(dv, tu);
+            float lv = dot(dv, dv);
+            if (lv > 1.0e-12f) tv = dv * rsqrtf(lv);
+        }
+    }
+}
+
+// tri_lod of flattened triangle index ti when it is an instanced one
+// (ti - num_tris among the instances' triangles, instance by instance):
+// the mesh triangle's edges through the instance's object-to-world map.
+static __device__ __noinline__ void inst_tri_lod(const DevScene& S, int ti, float3 n, float footprint, float& uv_fp,
+                                                 float3& tu, float3& tv) {
+    const int k = ti - S.num_tris;
+    if (k < 0 || k >= S.inst_tri_total) return;
+    int lo = 0, hi = S.num_instances - 1;   // last instance whose base <= k
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int4 m2 = __ldg(reinterpret_cast<const int4*>(S.inst_xf + (size_t)kInstRecord * mid + 7));
+        if (m2.x <= k) lo = mid;
+        else hi = mid - 1;
+    }
+    const float4* xf = S.inst_xf + (size_t)kInstRecord * lo;
+    const int4 m2 = __ldg(reinterpret_cast<const int4*>(xf + 7));
+    const Triangle& tr = S.inst_tris[m2.z + (k - m2.x)];
+    const float4 fa = __ldg(&xf[3]), fb = __ldg(&xf[4]), fc = __ldg(&xf[5]);
+    auto lin = [&](float3 d) {
+        return f3(fa.x * d.x + fa.y * d.y + fa.z * d.z, fb.x * d.x + fb.y * d.y + fb.z * d.z,
+                  fc.x * d.x + fc.y * d.y + fc.z * d.z);
+    };
+    tri_lod(lin(f3(tr.v1) - f3(tr.v0)), lin(f3(tr.v2) - f3(tr.v0)), tr.uv0, tr.uv1, tr.uv2, n, footprint, uv_fp, tu,
+            tv);
+}
+
 // render_kernel.cu:67-150
 __device__ __forceinline__ ShadePoint shade_prepare(const DevScene& S, const Hit& h, float3 view, float footprint) {
     ShadePoint sp;
@@ -107,30 +160,12 @@ __device__ __forceinline__ ShadePoint shade_prepare(const DevScene& S, const Hit
         int ti = -h.obj - 1;
         if (ti >= 0 && ti < S.num_tris) {
             const Triangle& tr = S.tris[ti];
-            float3 e1 = f3(tr.v1) - f3(tr.v0), e2 = f3(tr.v2) - f3(tr.v0);
-            float2 d1 = make_float2(tr.uv1.x - tr.uv0.x, tr.uv1.y - tr.uv0.y);
-            float2 d2 = make_float2(tr.uv2.x - tr.uv0.x, tr.uv2.y - tr.uv0.y);
-            float w1 = sqrtf(dot(e1, e1)), w2 = sqrtf(dot(e2, e2));
-            float u1 = sqrtf(d1.x * d1.x + d1.y * d1.y), u2 = sqrtf(d2.x * d2.x + d2.y * d2.y);
-            float a1 = w1 > 1.0e-6f ? u1 / w1 : 0.0f, a2 = w2 > 1.0e-6f ? u2 / w2 : 0.0f;
-            float dens = a1 > a2 ? a1 : a2;
-            if (dens > 1.0e-6f) uv_fp = footprint * dens;
-            float det = d1.x * d2.y - d2.x * d1.y;
-            if (fabsf(det) > 1.0e-8f) {
-                float3 du = (e1 * d2.y - e2 * d1.y) / det;
-                float3 dv = (e2 * d1.x - e1 * d2.x) / det;
-                du = du - h.n * dot(du, h.n);
-                dv = dv - h.n * dot(dv, h.n);
-                float lu = dot(du, du);
-                if (lu > 1.0e-12f) {
-                    tu = du * rsqrtf(lu);
-                    dv = dv - tu * dot(dv, tu);
-                    float lv = dot(dv, dv);
-                    if (lv > 1.0e-12f) tv = dv * rsqrtf(lv);
-                }
-            }
+            tri_lod(f3(tr.v1) - f3(tr.v0), f3(tr.v2) - f3(tr.v0), tr.uv0, tr.uv1, tr.uv2, h.n, footprint, uv_fp, tu,
+                    tv);
         }
     }
+    // instanced triangles: read as their flattened copies
+    if (h.obj < 0 && S.num_instances > 0) inst_tri_lod(S, -h.obj - 1, h.n, footprint, uv_fp, tu, tv);
     sp.uv_fp = uv_fp;
     if (m.normal_id >= 0 && m.normal_id < S.num_textures) {
         const TextureRef& nt = S.textures[m.normal_id];

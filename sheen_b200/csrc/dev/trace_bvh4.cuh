@@ -277,9 +277,20 @@ __device__ __forceinline__ int qmesh_trace(const QMesh& m, const QRay& r, float 
     }
 }
 
+// Scenes with instanced meshes add them to the mesh category in functions
+// of their own (dev/instances.cuh).
+template <bool COUNT, int TRI>
+__device__ __noinline__ bool mesh_q_inst(const DevScene& S, const Ray& r, Hit& h, Counters& c);
+template <bool COUNT, int TRI>
+__device__ __noinline__ int mesh_shadow_q_inst(const DevScene& S, const Ray& r, bool mask_aware, ShadowHit& sh,
+                                               Counters& c);
+template <bool COUNT, int TRI>
+__device__ __noinline__ bool mesh_any_q_inst(const DevScene& S, const Ray& r, Counters& c);
+
 // Closest mesh hit over q_all as a hit record (mesh_ref's result).
 template <bool COUNT, int TRI>
 __device__ __forceinline__ bool mesh_q(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    if (S.num_instances > 0) return mesh_q_inst<COUNT, TRI>(S, r, h, c);
     if (!S.q_all.nodes) return false;
     const QRay q = make_qray(r);
     float t = r.tmax, u = 0.0f, v = 0.0f;
@@ -299,6 +310,7 @@ __device__ __forceinline__ bool mesh_q(const DevScene& S, const Ray& r, Hit& h, 
 template <bool COUNT, int TRI>
 __device__ __forceinline__ int mesh_shadow_q(const DevScene& S, const Ray& r, bool mask_aware, ShadowHit& sh,
                                              Counters& c) {
+    if (S.num_instances > 0) return mesh_shadow_q_inst<COUNT, TRI>(S, r, mask_aware, sh, c);
     if (!S.q_all.nodes) return kClear;
     const QRay q = make_qray(r);
     if (!S.q_pass.nodes) {
@@ -322,6 +334,7 @@ __device__ __forceinline__ int mesh_shadow_q(const DevScene& S, const Ray& r, bo
 // Any hit in the opaque categories (render_kernel.cu:413-422, media rays).
 template <bool COUNT, int TRI>
 __device__ __forceinline__ bool mesh_any_q(const DevScene& S, const Ray& r, Counters& c) {
+    if (S.num_instances > 0) return mesh_any_q_inst<COUNT, TRI>(S, r, c);
     if (!S.q_all.nodes) return false;
     const QRay q = make_qray(r);
     float t = r.tmax, u, v;
@@ -642,3 +655,5 @@ struct FastTracer {
 
 }  // namespace dev
 }  // namespace sheen
+
+#include "instances.cuh"

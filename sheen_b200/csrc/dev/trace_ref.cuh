@@ -78,7 +78,7 @@ __device__ __forceinline__ bool strands_ref(const DevScene& S, const Ray& r, Hit
 }
 
 template <bool COUNT>
-__device__ __forceinline__ bool mesh_ref(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+__device__ __forceinline__ bool mesh_ref_flat(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
     if (S.num_tris == 0) return false;
     float best = r.tmax, bu = 0.0f, bv = 0.0f;
     int bi = -1;
@@ -94,6 +94,16 @@ __device__ __forceinline__ bool mesh_ref(const DevScene& S, const Ray& r, Hit& h
     tri_finish(r, S.tris[bi], best, bu, bv, h);
     h.obj = -(bi + 1);
     return true;
+}
+
+// Scenes with instanced meshes (dev/instances.cuh) add them to the category.
+template <bool COUNT>
+__device__ __noinline__ bool mesh_ref_inst(const DevScene& S, const Ray& r, Hit& h, Counters& c);
+
+template <bool COUNT>
+__device__ __forceinline__ bool mesh_ref(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    if (S.num_instances > 0) return mesh_ref_inst<COUNT>(S, r, h, c);
+    return mesh_ref_flat<COUNT>(S, r, h, c);
 }
 
 // Extension scenes (SheenSceneExt) walk their categories in functions of

@@ -71,6 +71,12 @@ void OwnedScene::finalize() {
         x.csg_cones = ptr(csg_cones);
         x.num_csg_cones = (int)csg_cones.size();
         x.max_depth = max_depth;
+        x.mesh_triangles = ptr(mesh_triangles);
+        x.num_mesh_triangles = (int)mesh_triangles.size();
+        x.meshes = ptr(meshes);
+        x.num_meshes = (int)meshes.size();
+        x.instances = ptr(instances);
+        x.num_instances = (int)instances.size();
     }
     v.texture_pixels = tex_ptrs.empty() ? nullptr : tex_ptrs.data();
     v.texture_widths = tex_w.empty() ? nullptr : tex_w.data();

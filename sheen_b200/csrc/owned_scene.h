@@ -48,6 +48,9 @@ struct OwnedScene {
     std::vector<SheenCsgBox> csg_boxes;
     std::vector<SheenCsgCone> csg_cones;
     int max_depth = 0;                       // reflect + refract recursion (SheenSceneExt.max_depth)
+    std::vector<Triangle> mesh_triangles;    // instanced meshes (object space)
+    std::vector<SheenMesh> meshes;
+    std::vector<SheenInstance> instances;
 
     // C views (rebuilt by finalize()).
     SheenScene view{};

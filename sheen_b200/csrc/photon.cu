@@ -25,7 +25,7 @@ namespace dev {
 // T: the scene's query policy (the plain form's reference-order walks, or
 // the wavefront form's BVH4s: same closest hits except exact ties).
 template <class T>
-__global__ void photon_emit_kernel(DevScene S, int per_light, int total, float4* pos, float4* nrm, float4* flux,
+__global__ void photon_emit_kernel(const __grid_constant__ DevScene S, int per_light, int total, float4* pos, float4* nrm, float4* flux,
                                    int* valid) {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= total) return;

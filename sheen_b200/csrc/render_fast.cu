@@ -19,7 +19,7 @@ __device__ __forceinline__ void warp_add_fast(unsigned long long* dst, unsigned 
 // so a scene of spheres, triangles and planes does not carry the other
 // categories' code and registers.
 template <bool COUNT, int F = kCatAll>
-__global__ void __launch_bounds__(128) mega_bvh4_kernel(DevScene S, float4* __restrict__ out, int W, int H, int aa,
+__global__ void __launch_bounds__(128) mega_bvh4_kernel(const __grid_constant__ DevScene S, float4* __restrict__ out, int W, int H, int aa,
                                                         int x0, int y0, int x1, int y1, unsigned long long* tally) {
     const int x = x0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
     const int y = y0 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(128) mega_bvh4_kernel(DevScene S, float4* __re
     }
 }
 
-__global__ void primary_hits_bvh4_kernel(DevScene S, int W, int H, int ns, int* obj, int* mat, float* tt) {
+__global__ void primary_hits_bvh4_kernel(const __grid_constant__ DevScene S, int W, int H, int ns, int* obj, int* mat, float* tt) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;
@@ -68,7 +68,7 @@ __global__ void primary_hits_bvh4_kernel(DevScene S, int W, int H, int ns, int* 
 // Closest hits of arbitrary rays (sheen_scene_trace): rays[2i] = {origin,
 // tmin}, rays[2i+1] = {direction, tmax}; T is the scene form's query policy.
 template <class T>
-__global__ void trace_rays_kernel(DevScene S, const float4* __restrict__ rays, int n, int* obj, int* mat, float* tt) {
+__global__ void trace_rays_kernel(const __grid_constant__ DevScene S, const float4* __restrict__ rays, int n, int* obj, int* mat, float* tt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 a = rays[2 * (size_t)i], b = rays[2 * (size_t)i + 1];
@@ -105,7 +105,7 @@ cudaError_t launch_mega_bvh4(const DeviceScene& s, int W, int H, int aa, Region 
     const bool simple = v.num_strands == 0 && v.num_hfs == 0 && v.num_ses == 0 && v.num_lathes == 0 &&
                         v.num_prisms == 0 && v.csg_root < 0 && v.num_csg_roots == 0;
     const bool wt = v.q_all.watertight != 0;
-    const bool basic = simple && v.num_tris == 0;
+    const bool basic = simple && v.num_tris == 0 && v.num_instances == 0;
 #define MEGA(C, F) dev::mega_bvh4_kernel<C, F><<<grid, block, 0, stream>>>(v, out, W, H, aa, rg.x0, rg.y0, rg.x1, \
                                                                           rg.y1, tally)
     if (count_nodes) MEGA(true, dev::kCatAll);

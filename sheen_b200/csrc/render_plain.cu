@@ -27,7 +27,7 @@ __device__ __forceinline__ void warp_add(unsigned long long* dst, unsigned long 
 // frame, 1080p 4 spp): 135.8 ms at the default 168 registers (3 blocks),
 // 113.0 ms at 4 blocks, 79.4 ms at 8.
 template <bool COUNT>
-__global__ void __launch_bounds__(128, 8) plain_kernel(DevScene S, float4* __restrict__ out, int W, int H, int aa,
+__global__ void __launch_bounds__(128, 8) plain_kernel(const __grid_constant__ DevScene S, float4* __restrict__ out, int W, int H, int aa,
                                                     int x0, int y0, int x1, int y1, unsigned long long* tally) {
     const int x = x0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
     const int y = y0 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(128, 8) plain_kernel(DevScene S, float4* __res
 // Primary closest hit of every sample (camera ray of render_kernel.cu:491-518
 // and scene_intersect), for hit-identity parity checks.
 template <class T>
-__global__ void primary_hits_kernel(DevScene S, int W, int H, int ns, int* obj, int* mat, float* tt) {
+__global__ void primary_hits_kernel(const __grid_constant__ DevScene S, int W, int H, int ns, int* obj, int* mat, float* tt) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;

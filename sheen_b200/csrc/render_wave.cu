@@ -281,7 +281,7 @@ __device__ __forceinline__ void primary_item(const DevScene& S, const WaveView& 
 // MULTI: samples of every job in the launch's table (V0.jobs), one claim
 // counter over their global order; otherwise the single frame S0 / V0.
 template <int F, bool MULTI>
-__global__ void __launch_bounds__(128, 8) wave_primary(DevScene S0, WaveView V0) {
+__global__ void __launch_bounds__(128, 8) wave_primary(const __grid_constant__ DevScene S0, WaveView V0) {
     Counters c;
     while (true) {
         const int base = claim_batch(&V0.ctr[kPrimHead]);
@@ -331,7 +331,7 @@ __device__ __forceinline__ unsigned int shadow_item(const DevScene& S, const Wav
 }
 
 template <int F, bool MULTI>
-__global__ void __launch_bounds__(128) wave_shadow(DevScene S0, WaveView V0) {
+__global__ void __launch_bounds__(128) wave_shadow(const __grid_constant__ DevScene S0, WaveView V0) {
     Counters c;
     const unsigned int n = V0.ctr[kShadowCount];
     while (true) {
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(128) wave_shadow(DevScene S0, WaveView V0) {
 // 4 useful bytes; the entry distances (closest-hit walks of the passable set
 // only) stay in local memory.  24 KB per 128-thread block.
 template <int F, bool SMEM_STACK, bool MULTI>
-__global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveView V0, int refill_min,
+__global__ void __launch_bounds__(128, 8) wave_shadow_refill(const __grid_constant__ DevScene S0, WaveView V0, int refill_min,
                                                              int inner_min) {
     using T = FastTracer<false, F>;
     constexpr unsigned int kFull = 0xffffffffu;
@@ -389,9 +389,10 @@ __global__ void __launch_bounds__(128, 8) wave_shadow_refill(DevScene S0, WaveVi
     const int lane = threadIdx.x & 31;
     // the lane's job (MULTI): its scene and frame
     int job = 0;
+    const DevScene* const s0 = &S0;
     auto scene = [&]() -> const DevScene& {
         if constexpr (MULTI) return V0.jobs[job].S;
-        else return S0;
+        else return *s0;
     };
     auto view = [&]() -> const WaveView& {
         if constexpr (MULTI) return V0.jobs[job].V;
@@ -636,7 +637,7 @@ __device__ __forceinline__ void reflect_item(const DevScene& S, const WaveView& 
 }
 
 template <int F, bool MULTI>
-__global__ void __launch_bounds__(128, 8) wave_reflect(DevScene S0, WaveView V0) {
+__global__ void __launch_bounds__(128, 8) wave_reflect(const __grid_constant__ DevScene S0, WaveView V0) {
     Counters c;
     const unsigned int n = V0.ctr[kReflCount];
     while (true) {
@@ -711,7 +712,7 @@ __device__ __forceinline__ void refract_item(const DevScene& S, const WaveView& 
 }
 
 template <int F, bool MULTI>
-__global__ void __launch_bounds__(128, 8) wave_refract(DevScene S0, WaveView V0) {
+__global__ void __launch_bounds__(128, 8) wave_refract(const __grid_constant__ DevScene S0, WaveView V0) {
     Counters c;
     const unsigned int n = V0.ctr[kRefrCount];
     while (true) {
@@ -927,7 +928,10 @@ static cudaError_t run_pipeline(const dev::DevScene& S0, const dev::WaveView& V,
     const StageGrids grids = stage_grids<F, MULTI>();
     const int sms = grids.sms, g_primary = grids.primary, g_reflect = grids.reflect, g_refract = grids.refract;
     const Tuning tu = tuning();
-    const bool refill = tu.shadow_kernel == 1;
+    // instanced meshes: the refill kernel walks the scene's own BVH4s lane by
+    // lane and has no top level; such scenes take the per-ray shadow kernel
+    // (batches group them apart)
+    const bool refill = tu.shadow_kernel == 1 && S0.num_instances == 0;
     const bool smem = tu.shadow_stack == 1;
     const int g_shadow = !refill ? shadow_grid(dev::wave_shadow<F, MULTI>, sms, tu.shadow_blocks_per_sm)
                          : smem  ? shadow_grid(dev::wave_shadow_refill<F, true, MULTI>, sms, tu.shadow_blocks_per_sm)
@@ -1153,7 +1157,7 @@ static bool simple_scene(const DeviceScene& s) {
 // arithmetic.
 static bool small_frame(const DeviceScene& s, long long nsamples) {
     const long long m = tuning().mega_samples;
-    return m > 0 && nsamples <= (s.view.num_tris > 0 ? m / 4 : m);
+    return m > 0 && nsamples <= (s.view.num_tris > 0 || s.view.num_instances > 0 ? m / 4 : m);
 }
 
 cudaError_t launch_wavefront(DeviceScene& s, int W, int H, int aa, Region rg, float4* out, cudaStream_t stream,
@@ -1297,16 +1301,18 @@ static cudaError_t batch_pass(const std::vector<BatchItem>& items, cudaStream_t 
 
 cudaError_t launch_wavefront_batch(const std::vector<BatchItem>& items, cudaStream_t stream,
                                    unsigned long long* tally) {
-    // one pass per kernel variant: category set x triangle test
-    std::vector<BatchItem> groups[4];
+    // one pass per kernel variant: category set x triangle test, and scenes
+    // with instanced meshes apart (their shadow stage is the per-ray kernel)
+    std::vector<BatchItem> groups[8];
     for (const BatchItem& it : items) {
         if (!it.s || it.s->form != SHEEN_FORM_WAVEFRONT || !wave_supported(*it.s)) return cudaErrorInvalidValue;
-        groups[(simple_scene(*it.s) ? 0 : 2) + (watertight_scene(*it.s) ? 1 : 0)].push_back(it);
+        groups[(simple_scene(*it.s) ? 0 : 2) + (watertight_scene(*it.s) ? 1 : 0) +
+               (it.s->view.num_instances > 0 ? 4 : 0)].push_back(it);
     }
     cudaError_t e = cudaSuccess;
-    for (int g = 0; g < 4 && e == cudaSuccess; g++)
+    for (int g = 0; g < 8 && e == cudaSuccess; g++)
         if (!groups[g].empty())
-            e = dispatch_variant(g < 2, (g & 1) != 0, [&](auto f) {
+            e = dispatch_variant((g & 2) == 0, (g & 1) != 0, [&](auto f) {
                 return batch_pass<decltype(f)::value>(groups[g], stream, tally);
             });
     return e;

@@ -224,7 +224,10 @@ void gen_spheres(OwnedScene& s, uint32_t seed) {
 // with seeded orientations, flattened into one triangle list; 4 point
 // lights; every 4th torus is glass (transmission 1, ior 1.5), everything
 // else Blinn-Phong with reflect 0.2; a ground plane.
-void gen_mesh(OwnedScene& s, uint32_t seed, int level) {
+// instanced: the tori as instances of one mesh (scene extension) instead
+// of 16 flattened copies; the same draws, so the same scene up to the
+// rounding of the transforms.
+void gen_mesh(OwnedScene& s, uint32_t seed, int level, bool instanced = false) {
     Rng rng(seed);
     s.camera = look_at(V3{0.0f, 7.0f, -26.0f}, V3{0.0f, 0.0f, 0.0f}, 60.0f);
     int m_sphere = s.add_material(0.75f, 0.55f, 0.4f, 0.4f, 48.0f, 0.05f);
@@ -252,11 +255,35 @@ void gen_mesh(OwnedScene& s, uint32_t seed, int level) {
     if (level < 8) { int d = 1 << (8 - level); nu = std::max(10, nu / d); nv = std::max(6, nv / d); }
     Mesh tor = torus(nu, nv, 1.5f, 0.5f);
     displace(tor, 0.06f, 3.0f, seed ^ 0x7654321u);
+    if (instanced) {
+        const size_t first = s.triangles.size();
+        tor.emit(s, m_glass);
+        s.mesh_triangles.assign(s.triangles.begin() + (long)first, s.triangles.end());
+        s.triangles.resize(first);
+        s.meshes.push_back(SheenMesh{0, (int)s.mesh_triangles.size()});
+    }
     for (int k = 0; k < 16; k++) {
         float ang = 6.28318530718f * (float)k / 16.0f + rng.uni(-0.08f, 0.08f);
         V3 centre{9.5f * std::cos(ang), rng.uni(-1.5f, 1.5f), 9.5f * std::sin(ang)};
         V3 axis = norm(V3{rng.uni(-1.0f, 1.0f), rng.uni(-1.0f, 1.0f), rng.uni(-1.0f, 1.0f)});
         float rot = rng.uni(0.0f, 3.14159265f);
+        if (instanced) {
+            // rotate()'s map as a matrix: c I + s [axis]x + (1 - c) axis axis^T
+            const double c = std::cos(rot), sn = std::sin(rot), a[3] = {axis.x, axis.y, axis.z};
+            const double cx[3][3] = {{0.0, -a[2], a[1]}, {a[2], 0.0, -a[0]}, {-a[1], a[0], 0.0}};
+            const double t[3] = {centre.x, centre.y, centre.z};
+            SheenInstance in;
+            std::memset(&in, 0, sizeof(in));
+            for (int r = 0; r < 3; r++) {
+                for (int q = 0; q < 3; q++)
+                    in.xform[4 * r + q] = (float)((r == q ? c : 0.0) + sn * cx[r][q] + (1.0 - c) * a[r] * a[q]);
+                in.xform[4 * r + 3] = (float)t[r];
+            }
+            in.mesh = 0;
+            in.material_id = (k % 4 == 0) ? m_glass : m_torus[k % 4];
+            s.instances.push_back(in);
+            continue;
+        }
         Mesh inst = tor;
         for (size_t i = 0; i < inst.v.size(); i++) {
             inst.v[i] = rotate(tor.v[i], axis, rot) + centre;
@@ -332,7 +359,7 @@ extern "C" int sheen_generate_scene_ext(int config, unsigned int seed, int detai
     switch (config) {
         case 0: gen_spheres(*s, seed); break;
         case 1:
-            gen_mesh(*s, seed, detail > 0 ? detail : 8);
+            gen_mesh(*s, seed, detail > 0 ? detail : 8, extended != 0);
             if (extended) s->max_depth = 4;   // reflect + refract recursion to 4 bounces
             break;
         case 2: sheen::gen_analytic(*s, seed, detail, extended != 0); break;

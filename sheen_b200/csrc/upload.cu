@@ -7,6 +7,8 @@
 // keeps it resident until the handle is released.  The wavefront form also
 // gets the SAH BVH4 with quantised child boxes over the triangles.
 #include <algorithm>
+#include <cfloat>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -307,6 +309,33 @@ const char* scene_index_error(const SheenScene* in, const SheenSceneExt* ext) {
         };
         if (!bez_ok(ext->lathe_bezier, in->num_lathes)) return "lathe Bezier run out of range (4k control points)";
         if (!bez_ok(ext->prism_bezier, in->num_prisms)) return "prism Bezier run out of range (4k control points)";
+        if (ext->num_mesh_triangles < 0 || ext->num_meshes < 0 || ext->num_instances < 0)
+            return "negative instance count";
+        if ((ext->num_mesh_triangles > 0 && !ext->mesh_triangles) || (ext->num_meshes > 0 && !ext->meshes) ||
+            (ext->num_instances > 0 && !ext->instances))
+            return "null instance array with a nonzero count";
+        for (int i = 0; i < ext->num_meshes; i++) {
+            const SheenMesh& m = ext->meshes[i];
+            if (m.tri_count <= 0 || !range_ok(m.tri_offset, m.tri_count, ext->num_mesh_triangles))
+                return "mesh triangles out of range";
+        }
+        long long flat = std::max(in->num_triangles, 0);
+        for (int i = 0; i < ext->num_instances; i++) {
+            const SheenInstance& x = ext->instances[i];
+            if (x.mesh < 0 || x.mesh >= ext->num_meshes) return "instance mesh out of range";
+            if (!mat_ok(x.material_id)) return "instance material_id out of range";
+            for (float f : x.xform)
+                if (!std::isfinite(f)) return "instance transform not finite";
+            const float* m = x.xform;
+            const double det = (double)m[0] * ((double)m[5] * m[10] - (double)m[6] * m[9]) -
+                               (double)m[1] * ((double)m[4] * m[10] - (double)m[6] * m[8]) +
+                               (double)m[2] * ((double)m[4] * m[9] - (double)m[5] * m[8]);
+            double scale = 0.0;
+            for (int k : {0, 1, 2, 4, 5, 6, 8, 9, 10}) scale = std::max(scale, std::fabs((double)m[k]));
+            if (!(std::fabs(det) > 1e-9 * scale * scale * scale)) return "instance transform not invertible";
+            flat += ext->meshes[x.mesh].tri_count;
+            if (flat > 2147483646ll) return "more than 2^31 - 1 triangles with the instances flattened";
+        }
         for (int i = 0; ext->hf_grid && i < in->num_heightfields; i++) {
             const SheenHeightGrid& g = ext->hf_grid[i];
             if (g.offset < 0) continue;
@@ -378,6 +407,15 @@ struct ExtTables {
     std::vector<HostNode> csg_root_bvh;
     std::vector<float4> csg_boxes;      // 2 per box
     std::vector<float4> csg_cones;      // 3 per cone
+    // instanced meshes
+    std::vector<QBvh> meshes;           // per mesh: BVH4 in object space
+    std::vector<float4> inst_xf;        // kInstRecord per instance
+    std::vector<dev::QNode4> tlas_nodes;  // top-level BVH4 over the instances (and the scene's triangles)
+    std::vector<int> tlas_items;        // per top-level leaf slot: instance (num_instances: the scene's triangles)
+    int tlas_depth = 0;
+    int inst_tri_total = 0;
+    int mesh_depth = 0;                 // deepest mesh BVH4
+    int inst_flat_leaf = 0;             // the scene's triangles are a top-level leaf
 };
 
 float4 f4(float x, float y, float z, float w) { return make_float4(x, y, z, w); }
@@ -434,7 +472,152 @@ void csg_tree_box(const SheenScene* in, const ExtTables& xt, int root, float lo[
     for (int k = 0; k < 3; k++) { lo[k] -= m; hi[k] += m; }
 }
 
-void build_ext_tables(const SheenScene* in, const SheenSceneExt* ext, ExtTables& xt) {
+// Instanced meshes: a BVH4 per mesh over its object-space triangles (the
+// records keep indices into mesh_triangles), one record per instance with
+// both maps (the inverse in double, rounded once), and a BVH4 over the
+// instances' world boxes (the mesh box's corners through the map, widened
+// by 1e-5 of the box's largest coordinate).
+void build_instance_tables(const SheenScene* in, const SheenSceneExt* ext, bool flat_leaf, ExtTables& xt) {
+    const bool wt = tuning().watertight != 0;
+    const int nm = ext->num_meshes;
+    xt.meshes.resize((size_t)nm);
+    std::vector<std::array<double, 6>> mbox((size_t)nm);
+    std::vector<std::thread> workers;
+    for (int m = 0; m < nm; m++) {
+        workers.emplace_back([&, m] {
+            const SheenMesh& me = ext->meshes[m];
+            std::vector<int> sub((size_t)me.tri_count);
+            std::array<double, 6> b = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
+            for (int k = 0; k < me.tri_count; k++) {
+                sub[(size_t)k] = me.tri_offset + k;
+                const Triangle& t = ext->mesh_triangles[me.tri_offset + k];
+                for (const sheen_float3& v : {t.v0, t.v1, t.v2}) {
+                    const double c[3] = {v.x, v.y, v.z};
+                    for (int a = 0; a < 3; a++) { b[a] = std::min(b[a], c[a]); b[3 + a] = std::max(b[3 + a], c[a]); }
+                }
+            }
+            mbox[(size_t)m] = b;
+            build_qbvh4(ext->mesh_triangles, sub, xt.meshes[(size_t)m], wt);
+        });
+        if (workers.size() == 8 || m == nm - 1) {
+            for (auto& w : workers) w.join();
+            workers.clear();
+        }
+    }
+    for (const QBvh& q : xt.meshes) xt.mesh_depth = std::max(xt.mesh_depth, q.max_depth);
+    std::vector<float> lo, hi;
+    std::vector<int> prims;
+    int base = 0;
+    for (int i = 0; i < ext->num_instances; i++) {
+        const SheenInstance& x = ext->instances[i];
+        const float* f = x.xform;
+        const double M[3][3] = {{f[0], f[1], f[2]}, {f[4], f[5], f[6]}, {f[8], f[9], f[10]}};
+        const double T[3] = {f[3], f[7], f[11]};
+        const double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) -
+                           M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                           M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+        double I[3][3];
+        I[0][0] = (M[1][1] * M[2][2] - M[1][2] * M[2][1]) / det;
+        I[0][1] = (M[0][2] * M[2][1] - M[0][1] * M[2][2]) / det;
+        I[0][2] = (M[0][1] * M[1][2] - M[0][2] * M[1][1]) / det;
+        I[1][0] = (M[1][2] * M[2][0] - M[1][0] * M[2][2]) / det;
+        I[1][1] = (M[0][0] * M[2][2] - M[0][2] * M[2][0]) / det;
+        I[1][2] = (M[0][2] * M[1][0] - M[0][0] * M[1][2]) / det;
+        I[2][0] = (M[1][0] * M[2][1] - M[1][1] * M[2][0]) / det;
+        I[2][1] = (M[0][1] * M[2][0] - M[0][0] * M[2][1]) / det;
+        I[2][2] = (M[0][0] * M[1][1] - M[0][1] * M[1][0]) / det;
+        for (int r = 0; r < 3; r++) {
+            const double ti = -(I[r][0] * T[0] + I[r][1] * T[1] + I[r][2] * T[2]);
+            xt.inst_xf.push_back(f4((float)I[r][0], (float)I[r][1], (float)I[r][2], (float)ti));
+        }
+        for (int r = 0; r < 3; r++) xt.inst_xf.push_back(f4(f[4 * r], f[4 * r + 1], f[4 * r + 2], f[4 * r + 3]));
+        const SheenMesh& me = ext->meshes[x.mesh];
+        const Material& mat = in->materials[x.material_id];
+        const int passable = mat.transmission > 0.5f ? 1 : 0;
+        xt.inst_xf.push_back(f4(int_bits(x.mesh), int_bits(x.material_id), int_bits(base - me.tri_offset),
+                                int_bits(passable)));
+        xt.inst_xf.push_back(f4(int_bits(base), int_bits(me.tri_count), int_bits(me.tri_offset), int_bits(0)));
+        // world box
+        const std::array<double, 6>& b = mbox[(size_t)x.mesh];
+        double wl[3] = {1e300, 1e300, 1e300}, wh[3] = {-1e300, -1e300, -1e300}, big = 0.0;
+        for (int corner = 0; corner < 8; corner++) {
+            const double p[3] = {b[(corner & 1) ? 3 : 0], b[(corner & 2) ? 4 : 1], b[(corner & 4) ? 5 : 2]};
+            for (int r = 0; r < 3; r++) {
+                const double w = M[r][0] * p[0] + M[r][1] * p[1] + M[r][2] * p[2] + T[r];
+                wl[r] = std::min(wl[r], w);
+                wh[r] = std::max(wh[r], w);
+                big = std::max(big, std::fabs(w));
+            }
+        }
+        float a[3], c[3];
+        for (int r = 0; r < 3; r++) {
+            a[r] = (float)(wl[r] - 1e-5 * big - 1e-6);
+            c[r] = (float)(wh[r] + 1e-5 * big + 1e-6);
+        }
+        push_box(lo, hi, a, c);
+        prims.push_back(i);
+        base += me.tri_count;
+    }
+    xt.inst_tri_total = base;
+    // Wavefront form: the scene's own triangles as one more leaf (index
+    // num_instances, identity maps, mesh -1), so that the top-level walk
+    // orders them with the instances by entry distance and a hit in either
+    // culls the other.
+    if (flat_leaf) {
+        float a[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, c[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+        for (int t = 0; t < in->num_triangles; t++) {
+            const Triangle& tr = in->triangles[t];
+            for (const sheen_float3& v : {tr.v0, tr.v1, tr.v2}) {
+                a[0] = std::min(a[0], v.x); a[1] = std::min(a[1], v.y); a[2] = std::min(a[2], v.z);
+                c[0] = std::max(c[0], v.x); c[1] = std::max(c[1], v.y); c[2] = std::max(c[2], v.z);
+            }
+        }
+        for (int r = 0; r < 3; r++) {
+            const float pad = 1e-5f * std::max(std::fabs(a[r]), std::fabs(c[r])) + 1e-6f;
+            a[r] -= pad;
+            c[r] += pad;
+        }
+        for (int r = 0; r < 3; r++) {
+            float4 row = f4(0.0f, 0.0f, 0.0f, 0.0f);
+            (&row.x)[r] = 1.0f;
+            xt.inst_xf.push_back(row);
+        }
+        for (int r = 0; r < 3; r++) xt.inst_xf.push_back(xt.inst_xf[xt.inst_xf.size() - 3]);
+        xt.inst_xf.push_back(f4(int_bits(-1), int_bits(-1), int_bits(0), int_bits(0)));
+        xt.inst_xf.push_back(f4(int_bits(base), int_bits(0), int_bits(0), int_bits(0)));
+        push_box(lo, hi, a, c);
+        prims.push_back(ext->num_instances);
+        xt.inst_flat_leaf = 1;
+    }
+    // Top level: the BVH4 builder over one stand-in triangle per leaf item
+    // whose box is the item's (corners lo and hi, third vertex the centre),
+    // so the top level is walked with the same 4-wide quantised nodes; each
+    // leaf slot maps to its item.
+    const size_t n = prims.size();
+    std::vector<Triangle> proxy(n);
+    std::vector<int> sub(n);
+    for (size_t k = 0; k < n; k++) {
+        Triangle& t = proxy[k];
+        std::memset(&t, 0, sizeof(t));
+        t.v0 = sheen_float3{lo[3 * k], lo[3 * k + 1], lo[3 * k + 2]};
+        t.v1 = sheen_float3{hi[3 * k], hi[3 * k + 1], hi[3 * k + 2]};
+        t.v2 = sheen_float3{0.5f * (lo[3 * k] + hi[3 * k]), 0.5f * (lo[3 * k + 1] + hi[3 * k + 1]),
+                            0.5f * (lo[3 * k + 2] + hi[3 * k + 2])};
+        sub[k] = (int)k;
+    }
+    QBvh top;
+    build_qbvh4(proxy.data(), sub, top, false);
+    xt.tlas_nodes = std::move(top.nodes);
+    xt.tlas_items.resize(top.tris.size() / 3);
+    for (size_t slot = 0; slot < xt.tlas_items.size(); slot++) {
+        int k;
+        std::memcpy(&k, &top.tris[3 * slot].w, 4);
+        xt.tlas_items[slot] = prims[(size_t)k];
+    }
+    xt.tlas_depth = top.max_depth;
+}
+
+void build_ext_tables(const SheenScene* in, const SheenSceneExt* ext, int form, ExtTables& xt) {
     if (!ext) return;
     if (ext->se_n2 && in->num_superellipsoids > 0)
         xt.se_n2.assign(ext->se_n2, ext->se_n2 + in->num_superellipsoids);
@@ -526,6 +709,8 @@ void build_ext_tables(const SheenScene* in, const SheenSceneExt* ext, ExtTables&
         }
         build_median_bvh(lo, hi, prims, true, xt.csg_root_bvh);
     }
+    if (ext->num_instances > 0)
+        build_instance_tables(in, ext, form == SHEEN_FORM_WAVEFRONT && in->num_triangles > 0, xt);
 }
 
 }  // namespace
@@ -539,7 +724,7 @@ int scene_upload_ext(const SheenScene* in, const SheenSceneExt* ext, int form, D
     if (in->num_materials <= 0 || !in->materials) { set_error("no materials"); return -1; }
     if (const char* why = scene_index_error(in, ext)) { set_error(why); return -1; }
     ExtTables xt;
-    build_ext_tables(in, ext, xt);
+    build_ext_tables(in, ext, form, xt);
     DeviceScene* s = new DeviceScene();
     s->form = form;
     cudaGetDevice(&s->device);
@@ -791,6 +976,25 @@ int scene_upload_ext(const SheenScene* in, const SheenSceneExt* ext, int form, D
     const size_t o_crbvh = add_vec(xt.csg_root_bvh);
     const size_t o_cbox = add_vec(xt.csg_boxes);
     const size_t o_ccone = add_vec(xt.csg_cones);
+    // instanced meshes: per-mesh BVH4s, their QMesh descriptors (patched
+    // below), the object-space triangles, instance records, the top BVH
+    const size_t nmesh = xt.meshes.size();
+    std::vector<size_t> o_mnodes(nmesh), o_mtris(nmesh);
+    for (size_t m = 0; m < nmesh; m++) {
+        o_mnodes[m] = add_vec(xt.meshes[m].nodes);
+        o_mtris[m] = add_vec(xt.meshes[m].tris);
+    }
+    std::vector<dev::QMesh> inst_qm(nmesh);
+    const size_t o_iqm = nmesh ? ar.add(nullptr, nmesh * sizeof(dev::QMesh)) : (size_t)-1;
+    const size_t o_itri = nmesh ? add_raw(ext->mesh_triangles, ext->num_mesh_triangles, sizeof(Triangle)) : (size_t)-1;
+    const size_t o_ixf = add_vec(xt.inst_xf);
+    const size_t o_tln = add_vec(xt.tlas_nodes);
+    const size_t o_tli = add_vec(xt.tlas_items);
+    if (3 * std::max(xt.mesh_depth, xt.tlas_depth) + 1 > 48) {
+        set_error("instanced mesh BVH too deep for the traversal stack");
+        delete s;
+        return -1;
+    }
     ar.size = (ar.size + 255) & ~(size_t)255;
 
     cudaError_t e = dmalloc(&s->arena, ar.size);
@@ -802,9 +1006,17 @@ int scene_upload_ext(const SheenScene* in, const SheenSceneExt* ext, int form, D
     // Patch device pointers into the host copies that reference other arrays.
     for (size_t i = 0; i < texrefs.size(); i++) texrefs[i].pixels = (const unsigned char*)dptr(o_chain[i]);
     for (size_t i = 0; i < hfs.size(); i++) hfs[i].image = (const unsigned char*)dptr(o_img[i]);
+    for (size_t m = 0; m < nmesh; m++) {
+        inst_qm[m].nodes = (const dev::QNode4*)dptr(o_mnodes[m]);
+        inst_qm[m].tris = (const float4*)dptr(o_mtris[m]);
+        inst_qm[m].num_nodes = (int)xt.meshes[m].nodes.size();
+        inst_qm[m].num_tris = (int)(xt.meshes[m].tris.size() / 3);
+        inst_qm[m].watertight = xt.meshes[m].vertices ? 1 : 0;
+    }
     for (auto& it : ar.items) {
         if (it.off == o_tex) it.src = texrefs.data();
         if (it.off == o_hf) it.src = hfs.data();
+        if (it.off == o_iqm) it.src = inst_qm.data();
     }
 
     // Every array straight from its host source through the pinned ring.
@@ -900,6 +1112,14 @@ int scene_upload_ext(const SheenScene* in, const SheenSceneExt* ext, int form, D
     v.csg_boxes = (const float4*)dptr(o_cbox);
     v.csg_cones = (const float4*)dptr(o_ccone);
     v.bounces = ext && ext->max_depth > 1 ? std::min(ext->max_depth, (int)dev::kMaxDeepBounces) : 0;
+    v.inst_tris = (const Triangle*)dptr(o_itri);
+    v.inst_mesh = (const dev::QMesh*)dptr(o_iqm);
+    v.inst_xf = (const float4*)dptr(o_ixf);
+    v.tlas_nodes = (const dev::QNode4*)dptr(o_tln);
+    v.tlas_items = (const int*)dptr(o_tli);
+    v.num_instances = nmesh ? ext->num_instances : 0;
+    v.inst_tri_total = xt.inst_tri_total;
+    v.inst_flat_leaf = xt.inst_flat_leaf;
     s->d_tally = (unsigned long long*)dptr(o_tally);
     s->wave_depth = std::max(q_all.max_depth, std::max(q_block.max_depth, q_pass.max_depth));
     s->build_ms = t1 - t0;
@@ -921,6 +1141,9 @@ int scene_upload_ext(const SheenScene* in, const SheenSceneExt* ext, int form, D
         }
         s->build_ms += now_ms() - tb;
     }
+    // the kernels pick their triangle test from q_all's flag: with
+    // instances and no triangles of the scene's own, the meshes' flag
+    if (!v.q_all.nodes && v.num_instances > 0) v.q_all.watertight = tuning().watertight != 0 ? 1 : 0;
 
     if (in->photons > 0 && in->num_lights > 0) {
         const double tp = now_ms();

@@ -1,17 +1,18 @@
 """Reflect + refract recursion (SheenSceneExt.max_depth; an extension with no
 counterpart in the reference, whose mirror ray stops at depth 1).
 
-The mesh workload's extended form (config 1, max_depth 4: every surface but
-the glass reflects 0.2, the glass tori refract) is rendered by both renderer
-forms and compared with the oracle's restatement of the same rules
-(oracle/sheen_oracle.c, render_deep).
+The mesh workload's extended form (config 1: its tori instanced, max_depth
+4; every surface but the glass reflects 0.2, the glass tori refract) is
+rendered by both renderer forms and compared with the oracle's restatement
+of the same rules (oracle/sheen_oracle.c, render_deep).  The depth-1
+baseline is the same extension with max_depth 0.
 
 CPU: the ctypes view of SheenSceneExt against the C header, the range check
 on max_depth (run before any device call), and properties of the oracle's
 recursion -- depth 1 is the reference's path bit for bit, sky pixels keep
 their colour, deeper paths change the image, FP32 and FP64 agree.
-GPU: images and ray counts against the oracle, depth 1 equal to the plain
-create, batch jobs of such scenes equal to their single renders.
+GPU: images and ray counts against the oracle, depth 1 equal to depth 0,
+batch jobs of such scenes equal to their single renders.
 """
 import ctypes
 import os
@@ -91,17 +92,18 @@ def test_depth_outside_range_is_refused(deep_scene, depth):
 
 
 def test_oracle_depth_one_is_the_reference_path(deep_scene):
-    base = _oracle_render(deep_scene, None, w=64, h=36, aa=1)
+    base = _oracle_render(deep_scene, _ext(deep_scene, 0), w=64, h=36, aa=1)
     one = _oracle_render(deep_scene, _ext(deep_scene, 1), w=64, h=36, aa=1)
     assert np.array_equal(base, one)
 
 
 def test_oracle_recursion_changes_bouncing_pixels_only(deep_scene):
     w, h = 64, 36
-    base = _oracle_render(deep_scene, None, w=w, h=h, aa=1)
+    base = _oracle_render(deep_scene, _ext(deep_scene, 0), w=w, h=h, aa=1)
     deep = _oracle_render(deep_scene, _ext(deep_scene, 4), w=w, h=h, aa=1)
     o = Oracle()
-    hd = o.scene(deep_scene.view_ptr)
+    x0 = _ext(deep_scene, 0)
+    hd = o.scene(deep_scene.view_ptr, ext_ptr=ctypes.addressof(x0))
     cat, _, _ = o.primary_hits(hd, w, h, 1)
     hd.close()
     sky = (cat.reshape(h, w) < 0)
@@ -144,7 +146,7 @@ def test_recursion_matches_oracle(device, deep_scene, form, depth):
     err = image_error(img, ref)
     assert st["primary_rays"] == W * H * AA
     assert err["mean_abs"] <= 1e-3 and err["frac_px_over_1e-2"] <= 0.01, err
-    base, _ = sb.DeviceScene(deep_scene, form).render_host(W, H, AA)
+    base, _ = sb.DeviceScene(deep_scene, form, ext=_ext(deep_scene, 0)).render_host(W, H, AA)
     assert image_error(img, base)["mean_abs"] > 1e-3
 
 
@@ -164,7 +166,7 @@ def test_recursion_ray_count_matches_oracle(device, deep_scene, form):
     hd.close()
     assert abs(st["total_rays"] - queries) <= max(2, 1e-3 * queries), (st, queries)
     # more secondary rays than the reference's depth-1 rules issue
-    base = sb.DeviceScene(deep_scene, form)
+    base = sb.DeviceScene(deep_scene, form, ext=_ext(deep_scene, 0))
     bst = base.render_region(W, H, AA, 0, 0, W, H, out.data_ptr(), 0, count_rays=True)
     torch.cuda.synchronize()
     base.close()
@@ -173,8 +175,8 @@ def test_recursion_ray_count_matches_oracle(device, deep_scene, form):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("form", FORMS, ids=FORM_IDS)
-def test_depth_one_equals_plain_create(device, deep_scene, form):
-    a, _ = sb.DeviceScene(deep_scene, form).render_host(64, 36, 1)
+def test_depth_one_equals_depth_zero(device, deep_scene, form):
+    a, _ = sb.DeviceScene(deep_scene, form, ext=_ext(deep_scene, 0)).render_host(64, 36, 1)
     b, _ = sb.DeviceScene(deep_scene, form, ext=_ext(deep_scene, 1)).render_host(64, 36, 1)
     assert np.array_equal(a, b)
 
@@ -182,7 +184,7 @@ def test_depth_one_equals_plain_create(device, deep_scene, form):
 @pytest.mark.gpu
 def test_frame_path_reports_the_megakernel(device, deep_scene):
     deep = sb.DeviceScene(deep_scene, sb.FORM_WAVEFRONT, ext=_ext(deep_scene, 4))
-    flat = sb.DeviceScene(deep_scene, sb.FORM_WAVEFRONT)
+    flat = sb.DeviceScene(deep_scene, sb.FORM_WAVEFRONT, ext=_ext(deep_scene, 0))
     plain = sb.DeviceScene(deep_scene, sb.FORM_PLAIN, ext=_ext(deep_scene, 4))
     assert deep.frame_path(1920, 1080, 4) == sb.PATH_MEGAKERNEL
     assert flat.frame_path(1920, 1080, 4) == sb.PATH_QUEUES
@@ -197,7 +199,7 @@ def test_frame_path_reports_the_megakernel(device, deep_scene):
 def test_batch_renders_recursion_scenes_alone(device, deep_scene):
     import torch
     deep = sb.DeviceScene(deep_scene, sb.FORM_WAVEFRONT, ext=_ext(deep_scene, 4))
-    flat = sb.DeviceScene(deep_scene, sb.FORM_WAVEFRONT)
+    flat = sb.DeviceScene(deep_scene, sb.FORM_WAVEFRONT, ext=_ext(deep_scene, 0))
     outs = [torch.zeros((H, W, 4), dtype=torch.float32, device="cuda") for _ in range(2)]
     sb.render_batch([(deep, W, H, AA, None, outs[0].data_ptr()), (flat, W, H, AA, None, outs[1].data_ptr())])
     torch.cuda.synchronize()
