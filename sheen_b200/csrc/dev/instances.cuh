@@ -51,7 +51,7 @@ __device__ __forceinline__ int4 inst_meta(const DevScene& S, int i) {
 // order for ANY walks; near to far for closest-hit walks, the nearer pushed
 // last) and entry distances.  Returns the child to visit next and its entry
 // distance in `next_t`.
-template <bool ANY>
+template <bool ANY, int CAP = kQStack>
 __device__ __forceinline__ uint32_t qnode_push(int mask, const float tn[4], const uint4& ch, uint32_t* stack_e,
                                                float* stack_t, int& sp, float& next_t) {
     const uint32_t cid[4] = {ch.x, ch.y, ch.z, ch.w};
@@ -61,7 +61,7 @@ __device__ __forceinline__ uint32_t qnode_push(int mask, const float tn[4], cons
         for (int k = 0; k < 4; k++) {
             if (!(mask & (1 << k))) continue;
             if (first < 0) first = k;
-            else if (sp < kQStack) stack_e[sp++] = cid[k];
+            else if (sp < CAP) stack_e[sp++] = cid[k];
         }
         next_t = tn[first];
         return cid[first];
@@ -77,7 +77,7 @@ __device__ __forceinline__ uint32_t qnode_push(int mask, const float tn[4], cons
         else if (n == 4) { CSWAP(0, 1) CSWAP(2, 3) CSWAP(0, 2) CSWAP(1, 3) CSWAP(1, 2) }
 #undef CSWAP
         for (int k = n - 1; k >= 1; k--) {
-            if (sp < kQStack) {
+            if (sp < CAP) {
                 stack_e[sp] = cid[key[k] & 3u];
                 stack_t[sp] = tn[key[k] & 3u];
                 sp++;
@@ -88,6 +88,11 @@ __device__ __forceinline__ uint32_t qnode_push(int mask, const float tn[4], cons
     }
 }
 
+// Stack entries of the two-level walk: at most 3 per level of either tree,
+// the marker between them, and a top-level leaf's remainder.
+constexpr int kInstStack = 72;
+constexpr uint32_t kInstMarker = 0x7fffffffu;   // never an inner node id
+
 // Closest instanced triangle strictly below `best` (in/out) among the
 // instances WANT selects (0 all, 1 passable, 2 blocking; the scene's own
 // triangles, when they are a top-level leaf: q_all, q_pass, or q_block --
@@ -95,137 +100,95 @@ __device__ __forceinline__ uint32_t qnode_push(int mask, const float tn[4], cons
 // instance (num_instances: the scene's triangles; -1: no hit) with the
 // triangle and its barycentrics.
 //
-// One loop walks both levels, one BVH4 node per iteration: the top level
-// (the instances' world boxes, in the world) or the current instance's
-// mesh (in its object space), with qmesh_trace's child order, culling and
-// triangle test.  A top-level leaf of several items visits the first and
-// puts the rest back on the top-level stack.  Nesting the mesh walk inside
-// a top-level walk instead left the lanes of a warp at different loop
-// levels, the ones between instances waiting for the ones inside a mesh.
+// One loop and one stack walk both levels, one BVH4 node per iteration:
+// the inner-node step is the same code for the top level (the instances'
+// world boxes, world ray) and a mesh (object-space ray), so the lanes of a
+// warp stay together whichever level each is in.  Entering an item pushes
+// a marker; popping the marker restores the world ray and the top level.
+// A top-level leaf of several items visits the first and pushes the rest.
+// Child order, culling and the triangle test are qmesh_trace's.
 template <bool ANY, bool COUNT, int TRI, int WANT>
 __device__ __forceinline__ int inst_walk(const DevScene& S, const Ray& r, float& best, int& tri, float& bu,
                                          float& bv, Counters& c) {
     constexpr uint32_t kLeaf = 0x80000000u;
-    const QRay qw = make_qray(r);
-    uint32_t tstack_e[kQStack];
-    float tstack_t[ANY ? 1 : kQStack];
-    int tsp = 0;
-    uint32_t tentry = 0;    // top-level root (inner)
-    float tentry_t = 0.0f;
-    uint32_t stack_e[kQStack];
-    float stack_t[ANY ? 1 : kQStack];
+    uint32_t stack_e[kInstStack];
+    float stack_t[ANY ? 1 : kInstStack];
     int sp = 0;
     int found = -1;
-    int inst = -1;          // item whose mesh is being walked (-1: the top level)
-    QRay q{};
-    const QNode4* mnodes = nullptr;
-    const float4* mtris = nullptr;
-    int mwt = 0;
-    uint32_t entry = 0;
+    int item = -1;                   // item whose mesh is being walked (-1: the top level)
+    QRay q = make_qray(r);           // the current level's ray
+    const QNode4* nodes = S.tlas_nodes;
+    const float4* tris = nullptr;
+    int wt = 0;
+    uint32_t e = 0;                  // top-level root (inner)
+    float et = 0.0f;                 // entry distance of e
     while (true) {
-        if (inst < 0) {
-            // ---- top level ---------------------------------------------------
-            bool pop = false;
-            if (!(tentry & kLeaf)) {
-                float tn[4];
-                uint4 ch;
-                if (COUNT) c.nodes++;
-                const int mask = qnode_children(S.tlas_nodes, (int)tentry, qw, best, tn, ch);
-                if (mask != 0) tentry = qnode_push<ANY>(mask, tn, ch, tstack_e, tstack_t, tsp, tentry_t);
-                else pop = true;
-            } else {
-                const int first = (int)((tentry & 0x7fffffffu) >> 3);
-                const int count = (int)(tentry & 7u) + 1;
-                const int i = __ldg(&S.tlas_items[first]);
-                if (count > 1 && tsp < kQStack) {     // the leaf's other items, same entry distance
-                    tstack_e[tsp] = kLeaf | ((uint32_t)(first + 1) << 3) | (uint32_t)(count - 2);
-                    if (!ANY) tstack_t[tsp] = tentry_t;
-                    tsp++;
-                }
-                const int4 meta = inst_meta(S, i);
-                QMesh m;
-                m.nodes = nullptr;
-                if (meta.x < 0) {
-                    // the scene's own triangles (wavefront form), in world space
-                    m = WANT == 0 ? S.q_all : (WANT == 1 ? S.q_pass : (S.q_pass.nodes ? S.q_block : S.q_all));
-                    q = qw;
-                } else if (!((WANT == 1 && !meta.w) || (WANT == 2 && meta.w))) {
-                    m = S.inst_mesh[meta.x];
-                    q = make_qray(inst_ray(S, i, r));
-                }
-                if (m.nodes) {
-                    if (COUNT) c.prims++;
-                    mnodes = m.nodes; mtris = m.tris; mwt = m.watertight;
-                    inst = i; entry = 0; sp = 0;
-                    continue;
-                }
-                pop = true;
-            }
-            if (pop) {
-                if constexpr (ANY) {
-                    if (tsp == 0) return found;
-                    tentry = tstack_e[--tsp];
-                } else {
-                    while (true) {
-                        if (tsp == 0) return found;
-                        --tsp;
-                        if (tstack_t[tsp] <= best) { tentry = tstack_e[tsp]; tentry_t = tstack_t[tsp]; break; }
-                    }
-                }
-            }
-            continue;
-        }
-        // ---- bottom level: one node of the item's mesh ------------------------
-        if (!(entry & kLeaf)) {
+        if (!(e & kLeaf)) {
             float tn[4];
             uint4 ch;
             if (COUNT) c.nodes++;
-            const int mask = qnode_children(mnodes, (int)entry, q, best, tn, ch);
+            const int mask = qnode_children(nodes, (int)e, q, best, tn, ch);
             if (mask != 0) {
-                float nt;
-                entry = qnode_push<ANY>(mask, tn, ch, stack_e, stack_t, sp, nt);
+                e = qnode_push<ANY, kInstStack>(mask, tn, ch, stack_e, stack_t, sp, et);
+                continue;
+            }
+        } else if (item < 0) {
+            // top-level leaf: enter its first item
+            const int first = (int)((e & 0x7fffffffu) >> 3);
+            const int count = (int)(e & 7u) + 1;
+            const int i = __ldg(&S.tlas_items[first]);
+            if (count > 1 && sp < kInstStack) {      // the leaf's other items, same entry distance
+                stack_e[sp] = kLeaf | ((uint32_t)(first + 1) << 3) | (uint32_t)(count - 2);
+                if (!ANY) stack_t[sp] = et;
+                sp++;
+            }
+            const int4 meta = inst_meta(S, i);
+            QMesh m;
+            m.nodes = nullptr;
+            if (meta.x < 0) m = WANT == 0 ? S.q_all : (WANT == 1 ? S.q_pass : (S.q_pass.nodes ? S.q_block : S.q_all));
+            else if (!((WANT == 1 && !meta.w) || (WANT == 2 && meta.w))) m = S.inst_mesh[meta.x];
+            if (m.nodes && sp < kInstStack) {
+                if (COUNT) c.prims++;
+                stack_e[sp] = kInstMarker;
+                if (!ANY) stack_t[sp] = -INFINITY;
+                sp++;
+                if (meta.x >= 0) q = make_qray(inst_ray(S, i, r));
+                nodes = m.nodes; tris = m.tris; wt = m.watertight;
+                item = i; e = 0;
                 continue;
             }
         } else {
-            const int first = (int)((entry & 0x7fffffffu) >> 3);
-            const int count = (int)(entry & 7u) + 1;
+            const int first = (int)((e & 0x7fffffffu) >> 3);
+            const int count = (int)(e & 7u) + 1;
             for (int k = 0; k < count; k++) {
                 const int slot = first + k;
-                const float4 a = __ldg(&mtris[3 * slot]);
-                const float4 b = __ldg(&mtris[3 * slot + 1]);
-                const float4 cc = __ldg(&mtris[3 * slot + 2]);
+                const float4 a = __ldg(&tris[3 * slot]);
+                const float4 b = __ldg(&tris[3 * slot + 1]);
+                const float4 cc = __ldg(&tris[3 * slot + 2]);
                 if (COUNT) c.prims++;
                 float t, u, v;
-                if (qtri_test<TRI>(q, a, b, cc, q.tmin, r.tmax, t, u, v, mwt) && t < best) {
+                if (qtri_test<TRI>(q, a, b, cc, q.tmin, r.tmax, t, u, v, wt) && t < best) {
                     best = t; bu = u; bv = v;
                     tri = __float_as_int(a.w);
-                    found = inst;
+                    found = item;
                     if (ANY) return found;
                 }
             }
         }
-        // pop within the mesh; an empty stack returns to the top level
-        if constexpr (ANY) {
-            if (sp == 0) inst = -1;
-            else entry = stack_e[--sp];
-        } else {
-            while (true) {
-                if (sp == 0) { inst = -1; break; }
-                --sp;
-                if (stack_t[sp] <= best) { entry = stack_e[sp]; break; }
+        // next entry; the marker returns to the top level
+        while (true) {
+            if (sp == 0) return found;
+            --sp;
+            if (stack_e[sp] == kInstMarker) {
+                item = -1;
+                q = make_qray(r);
+                nodes = S.tlas_nodes;
+                continue;
             }
-        }
-        if (inst < 0) {
-            // back at the top level: its next entry
-            if constexpr (ANY) {
-                if (tsp == 0) return found;
-                tentry = tstack_e[--tsp];
-            } else {
-                while (true) {
-                    if (tsp == 0) return found;
-                    --tsp;
-                    if (tstack_t[tsp] <= best) { tentry = tstack_e[tsp]; tentry_t = tstack_t[tsp]; break; }
-                }
+            if (ANY || stack_t[sp] <= best) {
+                e = stack_e[sp];
+                if (!ANY) et = stack_t[sp];
+                break;
             }
         }
     }

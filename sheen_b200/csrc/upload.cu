@@ -990,7 +990,9 @@ int scene_upload_ext(const SheenScene* in, const SheenSceneExt* ext, int form, D
     const size_t o_ixf = add_vec(xt.inst_xf);
     const size_t o_tln = add_vec(xt.tlas_nodes);
     const size_t o_tli = add_vec(xt.tlas_items);
-    if (3 * std::max(xt.mesh_depth, xt.tlas_depth) + 1 > 48) {
+    // the two-level walk's stack (dev/instances.cuh: 72 entries) holds 3 per
+    // level of both trees, a marker and a top-level leaf's remainder
+    if (3 * xt.mesh_depth + 1 > 48 || 3 * (xt.mesh_depth + xt.tlas_depth) + 2 > 72) {
         set_error("instanced mesh BVH too deep for the traversal stack");
         delete s;
         return -1;
@@ -1140,6 +1142,11 @@ int scene_upload_ext(const SheenScene* in, const SheenSceneExt* ext, int form, D
             return -1;
         }
         s->build_ms += now_ms() - tb;
+    }
+    if (v.inst_flat_leaf && 3 * (s->wave_depth + xt.tlas_depth) + 2 > 72) {
+        set_error("triangle BVH too deep for the instanced walk's stack");
+        scene_release(s);
+        return -1;
     }
     // the kernels pick their triangle test from q_all's flag: with
     // instances and no triangles of the scene's own, the meshes' flag
