@@ -321,6 +321,75 @@ struct LatheRay {
     }
 };
 
+// One profile segment p of a tessellated lathe (cone_test on the
+// precomputed constants) against the ray: lowers `best` and fills h on a
+// closer hit.  The ray's squared distance to the Y axis, q(t) = axz t^2 +
+// 2 bxz t + cxz, is convex: the segment is skipped when q stays above its
+// largest radius squared over the ray's t-range inside the segment's y-slab
+// (1e-4 relative margins in space, 1e-5 relative slack in t and q, far
+// above the rounding of a hit cone_test accepts, cancellation included).
+__device__ __forceinline__ bool lathe_seg_hit(const Ray& r, const LatheRay& lr, const float4* __restrict__ seg, int p,
+                                              float& best, Hit& h) {
+    const float idy = lr.inv[1];
+    const float axz = lr.axz, bxz = lr.bxz, cxz = lr.cxz, tstar = lr.tstar;
+    const float4 s1 = __ldg(&seg[2 * (size_t)p + 1]);
+    if (s1.w == 0.0f) return false;
+    const float4 s0 = __ldg(&seg[2 * (size_t)p]);
+    {
+        const float rs = fmaxf(fabsf(s0.y), fabsf(s1.z));
+        const float m = 1e-4f * (fabsf(s0.x) + fabsf(s1.y) + rs) + 1e-6f;
+        const float ylo = fminf(s0.x, s1.y) - m, yhi = fmaxf(s0.x, s1.y) + m;
+        float ta = r.tmin, tb = r.tmax;
+        if (r.d.y != 0.0f) {
+            const float u0 = (ylo - r.o.y) * idy, u1 = (yhi - r.o.y) * idy;
+            ta = fmaxf(ta, fminf(u0, u1));
+            tb = fminf(tb, fmaxf(u0, u1));
+        } else if (r.o.y < ylo || r.o.y > yhi) {
+            return false;
+        }
+        if (ta > tb + 1e-5f * (fabsf(ta) + fabsf(tb)) + 1e-6f) return false;
+        if (ta <= tb) {
+            const float tc = fminf(fmaxf(tstar, ta), tb);
+            const float q = axz * tc * tc + 2.0f * bxz * tc + cxz;
+            const float rr = rs + m;
+            const float tol = 1e-5f * (axz * tc * tc + 2.0f * fabsf(bxz * tc) + cxz) + 1e-4f * rr * rr;
+            if (q > rr * rr + tol) return false;
+        }
+    }
+    const float3 p0 = f3(0.0f, s0.x, 0.0f);
+    const float r0 = s0.y, k = s0.z, L = s0.w;
+    const float3 da = f3(0.0f, s1.x, 0.0f);
+    const float3 Q = r.o - p0;
+    const float u = dot(r.d, da), v = dot(Q, da);
+    const float3 Dp = r.d - u * da, Qp = Q - v * da;
+    const float A = dot(Dp, Dp) - k * k * u * u;
+    const float B = 2.0f * (dot(Dp, Qp) - k * r0 * u - k * k * v * u);
+    const float C = dot(Qp, Qp) - k * k * v * v - 2.0f * k * r0 * v - r0 * r0;
+    const float disc = B * B - 4.0f * A * C;
+    if (disc < 0.0f) return false;
+    const float sq = sqrtf(disc);
+    const float i2a = 1.0f / (2.0f * A);
+    const float s1r = (-B - sq) * i2a, s2r = (-B + sq) * i2a;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        const float sr = j == 0 ? s1r : s2r;
+        if (sr < r.tmin || sr > r.tmax) continue;
+        const float tp = v + sr * u;
+        if (tp < 0.0f || tp > L) continue;
+        if (sr < best) {
+            h.t = sr;
+            h.n = normalize(Qp + sr * Dp);
+            h.tan = da;
+            if (dot(h.n, r.d) > 0.0f) h.n = -h.n;
+            h.p = r.o + sr * r.d;
+            best = sr;
+            return true;
+        }
+        return false;   // cone_test reports its first root in range
+    }
+    return false;
+}
+
 // lathe_test with the segment constants precomputed (lathe_segments_kernel):
 // cone_test's steps after its axis, L, da and k, so the same hits and
 // records, without a square root and four divisions per segment.
@@ -342,73 +411,9 @@ __device__ __forceinline__ bool lathe_test_pre(const Ray& r, const LatheRay& lr,
         }
         if (tn > tf + 1e-5f * (fabsf(tn) + fabsf(tf)) + 1e-6f) return false;
     }
-    // The ray's squared distance to the Y axis, q(t) = axz t^2 + 2 bxz t +
-    // cxz, is convex: a segment is skipped when q stays above its largest
-    // radius squared over the ray's t-range inside the segment's y-slab
-    // (1e-4 relative margins in space, 1e-5 relative slack in t and q, far
-    // above the rounding of a hit cone_test accepts, cancellation included).
-    const float idy = lr.inv[1];
-    const float axz = lr.axz, bxz = lr.bxz, cxz = lr.cxz, tstar = lr.tstar;
     bool any = false;
     float best = r.tmax;
-    for (int i = 0; i < l.point_count - 1; i++) {
-        const int p = l.point_offset + i;
-        const float4 s1 = __ldg(&seg[2 * (size_t)p + 1]);
-        if (s1.w == 0.0f) continue;
-        const float4 s0 = __ldg(&seg[2 * (size_t)p]);
-        {
-            const float rs = fmaxf(fabsf(s0.y), fabsf(s1.z));
-            const float m = 1e-4f * (fabsf(s0.x) + fabsf(s1.y) + rs) + 1e-6f;
-            const float ylo = fminf(s0.x, s1.y) - m, yhi = fmaxf(s0.x, s1.y) + m;
-            float ta = r.tmin, tb = r.tmax;
-            if (r.d.y != 0.0f) {
-                const float u0 = (ylo - r.o.y) * idy, u1 = (yhi - r.o.y) * idy;
-                ta = fmaxf(ta, fminf(u0, u1));
-                tb = fminf(tb, fmaxf(u0, u1));
-            } else if (r.o.y < ylo || r.o.y > yhi) {
-                continue;
-            }
-            if (ta > tb + 1e-5f * (fabsf(ta) + fabsf(tb)) + 1e-6f) continue;
-            if (ta <= tb) {
-                const float tc = fminf(fmaxf(tstar, ta), tb);
-                const float q = axz * tc * tc + 2.0f * bxz * tc + cxz;
-                const float rr = rs + m;
-                const float tol = 1e-5f * (axz * tc * tc + 2.0f * fabsf(bxz * tc) + cxz) + 1e-4f * rr * rr;
-                if (q > rr * rr + tol) continue;
-            }
-        }
-        const float3 p0 = f3(0.0f, s0.x, 0.0f);
-        const float r0 = s0.y, k = s0.z, L = s0.w;
-        const float3 da = f3(0.0f, s1.x, 0.0f);
-        const float3 Q = r.o - p0;
-        const float u = dot(r.d, da), v = dot(Q, da);
-        const float3 Dp = r.d - u * da, Qp = Q - v * da;
-        const float A = dot(Dp, Dp) - k * k * u * u;
-        const float B = 2.0f * (dot(Dp, Qp) - k * r0 * u - k * k * v * u);
-        const float C = dot(Qp, Qp) - k * k * v * v - 2.0f * k * r0 * v - r0 * r0;
-        const float disc = B * B - 4.0f * A * C;
-        if (disc < 0.0f) continue;
-        const float sq = sqrtf(disc);
-        const float i2a = 1.0f / (2.0f * A);
-        const float s1r = (-B - sq) * i2a, s2r = (-B + sq) * i2a;
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-            const float s = j == 0 ? s1r : s2r;
-            if (s < r.tmin || s > r.tmax) continue;
-            const float tp = v + s * u;
-            if (tp < 0.0f || tp > L) continue;
-            if (s < best) {
-                h.t = s;
-                h.n = normalize(Qp + s * Dp);
-                h.tan = da;
-                if (dot(h.n, r.d) > 0.0f) h.n = -h.n;
-                h.p = r.o + s * r.d;
-                best = s;
-                any = true;
-            }
-            break;   // cone_test reports its first root in range
-        }
-    }
+    for (int i = 0; i < l.point_count - 1; i++) any |= lathe_seg_hit(r, lr, seg, l.point_offset + i, best, h);
     if (any) { h.mat = l.material_id; h.uv = make_float2(0.0f, 0.0f); }
     return any;
 }
@@ -600,7 +605,13 @@ __device__ __forceinline__ void se_chord(const Ray& r, const Superellipsoid& s, 
 // SIGN: decide the samples through SeSign (the same decisions, fewer powf).
 // The march and bisection of se_span over an "outside" predicate.
 // make() builds the predicate once the chord is known to be hit.
-template <class MakeOut>
+// ENTRY_ONLY (the closest-hit test, whose result is the entry alone): stop
+// at the entry sample.  The exit the march would go on to find lies at or
+// after the entry (it is bisected after an inside sample at or after the
+// entry, and clamped to t1 >= entry), so the reference's final check
+// entry <= exit always holds and the exit never changes the hit; tx is
+// then t1.
+template <bool ENTRY_ONLY = false, class MakeOut>
 __device__ __forceinline__ bool se_span_core(const Ray& r, const Superellipsoid& s, float t0, float t1, float& te,
                                              float& tx, float* te_prev, MakeOut make) {
     float tA, tB;
@@ -616,6 +627,7 @@ __device__ __forceinline__ bool se_span_core(const Ray& r, const Superellipsoid&
     te = inside ? t0 : -1e30f;
     if (te_prev) *te_prev = te;   // the last sample outside before the entry (te itself: no bracket)
     tx = -1e30f;
+    if (ENTRY_ONLY && inside) { tx = t1; return true; }
     for (int i = 1; i <= 32 && !found_out; i++) {
         float t = fminf(t0 + step * (float)i, t1);
         const bool o = out(r.o + t * r.d);
@@ -632,6 +644,7 @@ __device__ __forceinline__ bool se_span_core(const Ray& r, const Superellipsoid&
         if (!inside && !o) {
             te = fmaxf(t, t0);   // bisection over [t, t] in the reference
             if (te_prev) *te_prev = tp;
+            if (ENTRY_ONLY) { tx = t1; return true; }
             found_in = true;
             inside = true;
         }
@@ -678,11 +691,11 @@ __device__ __forceinline__ bool se_may_enter(const Ray& r, const Superellipsoid&
 // SIGN: decide the samples through SeSign (the same decisions, fewer powf),
 // and skip the march of rays that miss the body's bounding ellipsoid
 // (se_may_enter: the same result).
-template <bool SIGN = false>
+template <bool SIGN = false, bool ENTRY_ONLY = false>
 __device__ __forceinline__ bool se_span(const Ray& r, const Superellipsoid& s, float t0, float t1,
                                         float& te, float& tx, float* te_prev = nullptr) {
     if (SIGN && !se_may_enter(r, s, t0, t1)) return false;
-    return se_span_core(r, s, t0, t1, te, tx, te_prev, [&]() {
+    return se_span_core<ENTRY_ONLY>(r, s, t0, t1, te, tx, te_prev, [&]() {
         const SeSign sg(SIGN ? s.n : 0.0f);
         return [sg, &s](float3 p) { return SIGN ? sg.outside(s, p) : se_value(s, p) > 1.0f; };
     });
@@ -691,10 +704,10 @@ __device__ __forceinline__ bool se_span(const Ray& r, const Superellipsoid& s, f
 // Extension: the two-exponent body's span (the same march), not inlined so
 // that the kernels' code for the reference's body is unchanged.
 static __device__ __noinline__ bool se_span2(const Ray& r, const Superellipsoid& s, float n2, float t0, float t1,
-                                             float& te, float& tx, float* te_prev) {
-    return se_span_core(r, s, t0, t1, te, tx, te_prev, [&]() {
-        return [&s, n2](float3 p) { return se_value2(s, n2, p) > 1.0f; };
-    });
+                                             float& te, float& tx, float* te_prev, bool entry_only = false) {
+    auto make = [&]() { return [&s, n2](float3 p) { return se_value2(s, n2, p) > 1.0f; }; };
+    return entry_only ? se_span_core<true>(r, s, t0, t1, te, tx, te_prev, make)
+                      : se_span_core<false>(r, s, t0, t1, te, tx, te_prev, make);
 }
 
 // Extension (a scene created with "trace.se_polish"; the reference has
@@ -738,7 +751,7 @@ __device__ __forceinline__ bool se_test(const Ray& r, const Superellipsoid& s, H
     t0 = fmaxf(t0, r.tmin);
     t1 = fminf(t1, r.tmax);
     float te, tx, te_prev;
-    if (!se_span<SIGN>(r, s, t0, t1, te, tx, &te_prev)) return false;
+    if (!se_span<SIGN, true>(r, s, t0, t1, te, tx, &te_prev)) return false;
     if (polish && te_prev < te) te = se_polish_entry(r, s, te_prev, te);
     h.t = te;
     h.p = r.o + te * r.d;
@@ -758,7 +771,7 @@ static __device__ __noinline__ bool se_test2(const Ray& r, const Superellipsoid&
     t0 = fmaxf(t0, r.tmin);
     t1 = fminf(t1, r.tmax);
     float te, tx;
-    if (!se_span2(r, s, n2, t0, t1, te, tx, nullptr)) return false;
+    if (!se_span2(r, s, n2, t0, t1, te, tx, nullptr, true)) return false;
     h.t = te;
     h.p = r.o + te * r.d;
     h.n = normalize(se_gradient2(s, n2, h.p));

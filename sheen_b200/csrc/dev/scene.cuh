@@ -127,6 +127,16 @@ struct DevScene {
     const float4* csg_boxes;       // leaf_kind 2: {lo, material as int}, {hi, 0}
     const float4* csg_cones;       // leaf_kind 3: {p0, r0}, {p1, r1}, {material as int, 0, 0, 0}
     int bounces;                   // reflect + refract bounces (> 1: the recursion of render_sample_deep)
+    // Wavefront form, tessellated lathes: their profile segments bucketed by
+    // height over the union of the lathes (all turn about the world Y axis):
+    // {y0, 1 / bucket height, radius bound, buckets as int}; bucket b's items
+    // in [start[b], start[b + 1]), each a profile point p (low 24 bits) with
+    // the first bucket listing it (high 8 bits); the lathe of each point.
+    // Null without lathes or with exact Bezier ones.
+    const float4* lathe_grid;
+    const int* lathe_grid_start;
+    const int* lathe_grid_items;
+    const int* lathe_of_point;
     // Instanced meshes (two-level BVH); num_instances 0 without.
     const Triangle* inst_tris;     // every mesh's object-space triangles
     const QMesh* inst_mesh;        // per mesh: its BVH4 in object space

@@ -528,10 +528,74 @@ static __device__ __noinline__ bool lathes_cull_ext(const DevScene& S, const Ray
     return any;
 }
 
+// Tessellated lathes through the height buckets (DevScene.lathe_grid): the
+// ray's t-range inside the cylinder about the Y axis that holds every
+// lathe, cut to the buckets' height range, gives the buckets it can meet;
+// each segment listed there is tested once (in the first of those buckets
+// that lists it), with lathe_test_pre's per-segment test.  The closest hit
+// over all lathes is the per-lathe walk's (exact ties between two lathes
+// may resolve the other way).
+template <bool COUNT>
+__device__ __forceinline__ bool lathes_grid(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
+    const float4 g = __ldg(&S.lathe_grid[0]);
+    const int nb = __float_as_int(g.w);
+    const LatheRay lr(r);
+    // inside the cylinder x^2 + z^2 <= R^2 (q(t) = axz t^2 + 2 bxz t + cxz)
+    float ta = r.tmin, tb = r.tmax;
+    const float R2 = g.z * g.z;
+    if (lr.axz > 0.0f) {
+        const float disc = lr.bxz * lr.bxz - lr.axz * (lr.cxz - R2);
+        if (!(disc >= 0.0f)) return false;
+        const float sq = sqrtf(disc);
+        const float c0 = (-lr.bxz - sq) / lr.axz, c1 = (-lr.bxz + sq) / lr.axz;
+        const float slack = 1e-5f * (fabsf(c0) + fabsf(c1)) + 1e-6f;
+        ta = fmaxf(ta, c0 - slack);
+        tb = fminf(tb, c1 + slack);
+    } else if (lr.cxz > R2) {
+        return false;
+    }
+    // and inside the buckets' height range
+    const float y_lo = g.x, y_hi = g.x + (float)nb / g.y;
+    if (r.d.y != 0.0f) {
+        const float u0 = (y_lo - r.o.y) * lr.inv[1], u1 = (y_hi - r.o.y) * lr.inv[1];
+        ta = fmaxf(ta, fminf(u0, u1));
+        tb = fminf(tb, fmaxf(u0, u1));
+    } else if (r.o.y < y_lo || r.o.y > y_hi) {
+        return false;
+    }
+    if (ta > tb + 1e-5f * (fabsf(ta) + fabsf(tb)) + 1e-6f) return false;
+    const float ya = r.o.y + ta * r.d.y, yb = r.o.y + tb * r.d.y;
+    const float ylo = fminf(ya, yb), yhi = fmaxf(ya, yb);
+    const float m = 1e-4f * (fabsf(ylo) + fabsf(yhi)) + 1e-5f;
+    const int b0 = max(0, min(nb - 1, (int)floorf((ylo - m - g.x) * g.y)));
+    const int b1 = max(0, min(nb - 1, (int)floorf((yhi + m - g.x) * g.y)));
+    bool any = false;
+    float best = r.tmax;
+    int lathe = -1;
+    for (int b = b0; b <= b1; b++) {
+        const int k0 = __ldg(&S.lathe_grid_start[b]), k1 = __ldg(&S.lathe_grid_start[b + 1]);
+        for (int k = k0; k < k1; k++) {
+            const int it = __ldg(&S.lathe_grid_items[k]);
+            const int first = (int)((unsigned)it >> 24);
+            if (max(first, b0) != b) continue;
+            const int p = it & 0xffffff;
+            if (COUNT) c.prims++;
+            if (lathe_seg_hit(r, lr, S.lathe_seg, p, best, h)) { any = true; lathe = p; }
+        }
+    }
+    if (!any) return false;
+    const int li = __ldg(&S.lathe_of_point[lathe]);
+    h.mat = S.lathes[li].material_id;
+    h.uv = make_float2(0.0f, 0.0f);
+    h.obj = -(li + 1);
+    return true;
+}
+
 template <bool COUNT>
 __device__ __forceinline__ bool lathes_cull(const DevScene& S, const Ray& r, Hit& h, Counters& c) {
     if (S.num_lathes == 0) return false;
     if (S.lathe_bz) return lathes_cull_ext<COUNT>(S, r, h, c);
+    if (S.lathe_grid) return lathes_grid<COUNT>(S, r, h, c);
     bool any = false;
     float best = r.tmax;
     const LatheRay lr(r);

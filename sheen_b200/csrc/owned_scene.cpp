@@ -55,6 +55,12 @@ void OwnedScene::finalize() {
     {
         SheenSceneExt& x = ext_view;
         std::memset(&x, 0, sizeof(x));
+        // per-primitive extension arrays cover every primitive (the library
+        // reads one entry per superellipsoid / heightfield / lathe / prism)
+        if (!se_n2.empty()) se_n2.resize(superellipsoids.size(), 0.0f);
+        if (!hf_grid.empty()) hf_grid.resize(heightfields.size(), SheenHeightGrid{-1, 0, 0});
+        if (!lathe_bezier.empty()) lathe_bezier.resize(lathes.size(), SheenBezierRun{0, 0});
+        if (!prism_bezier.empty()) prism_bezier.resize(prisms.size(), SheenBezierRun{0, 0});
         auto ptr = [](const auto& vec) { return vec.empty() ? nullptr : vec.data(); };
         x.lathe_bezier = ptr(lathe_bezier);
         x.prism_bezier = ptr(prism_bezier);

@@ -226,6 +226,9 @@ void gen_analytic(OwnedScene& s, uint32_t seed, int detail, bool extended) {
             std::memset(&se, 0, sizeof(se));
             se.center = {x, y, z}; se.a = a; se.b = b; se.c = c; se.n = 12.0f; se.material_id = 7;
             s.superellipsoids.push_back(se);
+            // the extension's array has one entry per superellipsoid: the
+            // tree's boxes keep the single-exponent body
+            if (extended) s.se_n2.push_back(0.0f);
             return (int)s.superellipsoids.size() - 1;
         };
         auto leaf = [&](int kind, int idx) {

@@ -416,6 +416,9 @@ struct ExtTables {
     int inst_tri_total = 0;
     int mesh_depth = 0;                 // deepest mesh BVH4
     int inst_flat_leaf = 0;             // the scene's triangles are a top-level leaf
+    // tessellated lathes' height buckets (wavefront form)
+    std::vector<float4> lathe_grid;
+    std::vector<int> lathe_grid_start, lathe_grid_items, lathe_of_point;
 };
 
 float4 f4(float x, float y, float z, float w) { return make_float4(x, y, z, w); }
@@ -617,7 +620,54 @@ void build_instance_tables(const SheenScene* in, const SheenSceneExt* ext, bool 
     xt.tlas_depth = top.max_depth;
 }
 
+// Height buckets over the tessellated lathes' profile segments (wavefront
+// form; all lathes turn about the world Y axis, so their boxes coincide and
+// a per-lathe BVH cannot separate them): each segment is listed in every
+// bucket its height range meets, widened by 1e-3 relative -- ten times the
+// device's own per-segment margin -- so a segment is listed wherever the
+// device test could accept a hit.
+void build_lathe_grid(const SheenScene* in, ExtTables& xt) {
+    struct SegBox { int p; float ylo, yhi; };
+    std::vector<SegBox> segs;
+    float Y0 = FLT_MAX, Y1 = -FLT_MAX, R = 0.0f;
+    xt.lathe_of_point.assign((size_t)in->num_lathe_points, -1);
+    for (int i = 0; i < in->num_lathes; i++) {
+        const Lathe& l = in->lathes[i];
+        for (int j = 0; j + 1 < l.point_count; j++) {
+            const int p = l.point_offset + j;
+            xt.lathe_of_point[(size_t)p] = i;
+            const LathePoint a = in->lathe_points[p], b = in->lathe_points[p + 1];
+            if (a.radius <= 0.0f && b.radius <= 0.0f) continue;
+            const float rs = std::max(std::fabs(a.radius), std::fabs(b.radius));
+            const float ylo = std::min(a.y, b.y), yhi = std::max(a.y, b.y);
+            const float m = 1e-3f * (std::fabs(ylo) + std::fabs(yhi) + rs) + 1e-5f;
+            segs.push_back({p, ylo - m, yhi + m});
+            Y0 = std::min(Y0, ylo - m);
+            Y1 = std::max(Y1, yhi + m);
+            R = std::max(R, rs + m);
+        }
+    }
+    if (segs.empty() || !(Y1 > Y0)) { xt.lathe_of_point.clear(); return; }
+    const int nb = (int)std::max<size_t>(1, std::min<size_t>(128, segs.size() / 8));
+    const float inv_h = (float)nb / (Y1 - Y0);
+    auto bucket = [&](float y) { return std::max(0, std::min(nb - 1, (int)std::floor((y - Y0) * inv_h))); };
+    std::vector<std::vector<int>> lists((size_t)nb);
+    for (const SegBox& sb : segs) {
+        const int b0 = bucket(sb.ylo), b1 = bucket(sb.yhi);
+        for (int b = b0; b <= b1; b++) lists[(size_t)b].push_back(sb.p | (b0 << 24));
+    }
+    xt.lathe_grid = {f4(Y0, inv_h, R * 1.001f, int_bits(nb))};
+    xt.lathe_grid_start.push_back(0);
+    for (const auto& lst : lists) {
+        xt.lathe_grid_items.insert(xt.lathe_grid_items.end(), lst.begin(), lst.end());
+        xt.lathe_grid_start.push_back((int)xt.lathe_grid_items.size());
+    }
+}
+
 void build_ext_tables(const SheenScene* in, const SheenSceneExt* ext, int form, ExtTables& xt) {
+    if (form == SHEEN_FORM_WAVEFRONT && in->num_lathes > 0 && in->num_lathe_points < (1 << 24) &&
+        !(ext && ext->lathe_bezier))
+        build_lathe_grid(in, xt);
     if (!ext) return;
     if (ext->se_n2 && in->num_superellipsoids > 0)
         xt.se_n2.assign(ext->se_n2, ext->se_n2 + in->num_superellipsoids);
@@ -988,6 +1038,10 @@ int scene_upload_ext(const SheenScene* in, const SheenSceneExt* ext, int form, D
     const size_t o_iqm = nmesh ? ar.add(nullptr, nmesh * sizeof(dev::QMesh)) : (size_t)-1;
     const size_t o_itri = nmesh ? add_raw(ext->mesh_triangles, ext->num_mesh_triangles, sizeof(Triangle)) : (size_t)-1;
     const size_t o_ixf = add_vec(xt.inst_xf);
+    const size_t o_lg = add_vec(xt.lathe_grid);
+    const size_t o_lgs = add_vec(xt.lathe_grid_start);
+    const size_t o_lgi = add_vec(xt.lathe_grid_items);
+    const size_t o_lop = add_vec(xt.lathe_of_point);
     const size_t o_tln = add_vec(xt.tlas_nodes);
     const size_t o_tli = add_vec(xt.tlas_items);
     // the two-level walk's stack (dev/instances.cuh: 72 entries) holds 3 per
@@ -1117,6 +1171,10 @@ int scene_upload_ext(const SheenScene* in, const SheenSceneExt* ext, int form, D
     v.inst_tris = (const Triangle*)dptr(o_itri);
     v.inst_mesh = (const dev::QMesh*)dptr(o_iqm);
     v.inst_xf = (const float4*)dptr(o_ixf);
+    v.lathe_grid = (const float4*)dptr(o_lg);
+    v.lathe_grid_start = (const int*)dptr(o_lgs);
+    v.lathe_grid_items = (const int*)dptr(o_lgi);
+    v.lathe_of_point = (const int*)dptr(o_lop);
     v.tlas_nodes = (const dev::QNode4*)dptr(o_tln);
     v.tlas_items = (const int*)dptr(o_tli);
     v.num_instances = nmesh ? ext->num_instances : 0;

@@ -52,3 +52,24 @@ def test_bvh4_structure():
         s = sb.generate_scene(1, 3, detail)
         d = L.sheen_selfcheck_bvh4(s.view_ptr)
         assert 1 <= d <= 15, d
+
+
+def test_extended_per_primitive_arrays_cover_every_primitive():
+    """SheenSceneExt's per-primitive arrays hold one entry per primitive (the
+    library and the oracle read that many): the analytic workload's CSG-leaf
+    superellipsoids carry n2 = 0 (single-exponent body), and two generations
+    give the same bytes over the whole array."""
+    import ctypes
+
+    from sheen_b200 import contract as C
+
+    def n2_bytes():
+        s = sb.generate_scene(2, 1, 0, 0, extended=True)
+        x = C.SheenSceneExt.from_buffer_copy(ctypes.string_at(s.ext_ptr, ctypes.sizeof(C.SheenSceneExt)))
+        n = s.view.num_superellipsoids
+        return np.frombuffer(ctypes.string_at(x.se_n2, 4 * n), np.float32).copy(), n
+
+    a, n = n2_bytes()
+    b, _ = n2_bytes()
+    assert n == 258 and np.array_equal(a, b)
+    assert (a[:256] > 0).all() and (a[256:] == 0).all()
