@@ -185,6 +185,31 @@ __device__ __forceinline__ bool cap_test(const Ray& r, float3 c, float rad, floa
 
 // primitives/sweep.h:13-90: a strand = caps at both ends + cone pieces with
 // caps at the joints; closest of all against the unchanged ray range.
+// Whether the ray's line comes within R = half + rmax of the point m.  A
+// miss is declared only beyond R by 1e-3 relative plus the cancellation
+// error of the squared distance (1e-5 of |w|^2 + R^2), so the pieces it
+// skips are ones whose tests report no hit (or no depth):
+//   - a piece from a to b with radii up to rmax (its cone and end caps) lies
+//     within |b - a| / 2 + rmax of its midpoint;
+//   - piece_tau measures the distance between the points o - v t (t >= 0)
+//     and a - u s (s in [0, 1]) -- its w = o - a with the reference's signs
+//     -- so the depth it can report comes from the segment a .. 2a - b:
+//     centre a - u / 2, the same half length.
+__device__ __forceinline__ bool piece_in_reach(const Ray& r, float3 m, float half, float rmax) {
+    const float R = half + fabsf(rmax);
+    const float3 w = m - r.o;
+    const float dd = dot(r.d, r.d);
+    if (!(dd > 0.0f)) return true;
+    const float p = dot(w, r.d);
+    const float ww = dot(w, w);
+    const float d2 = ww - p * p / dd;
+    const float R2 = R * R;
+    return !(d2 > R2 * 1.002001f + 1e-5f * (ww + R2));
+}
+
+// CULL (the wavefront form): pieces out of reach (piece_in_reach) skip
+// their tests; the hits are the same.
+template <bool CULL = false>
 __device__ __forceinline__ bool strand_test(const Ray& r, const SweepStrand& st, const SweepPoint* pts, Hit& h) {
     const int n = st.point_count;
     if (n < 2) return false;
@@ -192,10 +217,16 @@ __device__ __forceinline__ bool strand_test(const Ray& r, const SweepStrand& st,
     bool any = false;
     float best = r.tmax;
     Hit tmp;
-    if (cap_test(r, f3(P[0].position), P[0].radius, normalize(f3(P[0].position) - f3(P[1].position)), tmp) &&
+    auto reach = [&](float3 a, float3 b, float ra, float rb) {
+        const float3 u = b - a;
+        return piece_in_reach(r, 0.5f * (a + b), 0.5f * sqrtf(dot(u, u)), fmaxf(fabsf(ra), fabsf(rb)));
+    };
+    const bool reach0 = !CULL || reach(f3(P[0].position), f3(P[1].position), P[0].radius, P[1].radius);
+    if (reach0 && cap_test(r, f3(P[0].position), P[0].radius, normalize(f3(P[0].position) - f3(P[1].position)), tmp) &&
         tmp.t < best) { h = tmp; best = tmp.t; any = true; }
     for (int i = 0; i < n - 1; i++) {
         float3 a = f3(P[i].position), b = f3(P[i + 1].position);
+        if (CULL && !reach(a, b, P[i].radius, P[i + 1].radius)) continue;
         if (cone_test(r, a, P[i].radius, b, P[i + 1].radius, tmp) && tmp.t < best) { h = tmp; best = tmp.t; any = true; }
         if (i < n - 2) {
             float3 ax = normalize(f3(P[i + 2].position) - b);
@@ -203,7 +234,10 @@ __device__ __forceinline__ bool strand_test(const Ray& r, const SweepStrand& st,
         }
     }
     float3 pl = f3(P[n - 1].position), pp = f3(P[n - 2].position);
-    if (cap_test(r, pl, P[n - 1].radius, normalize(pl - pp), tmp) && tmp.t < best) { h = tmp; best = tmp.t; any = true; }
+    const bool reach1 = !CULL || reach(pp, pl, P[n - 2].radius, P[n - 1].radius);
+    if (reach1 && cap_test(r, pl, P[n - 1].radius, normalize(pl - pp), tmp) && tmp.t < best) {
+        h = tmp; best = tmp.t; any = true;
+    }
     if (any) { h.mat = st.material_id; h.uv = make_float2(0.0f, 0.0f); }
     return any;
 }
@@ -229,10 +263,20 @@ __device__ __forceinline__ float piece_tau(const Ray& r, const SweepPoint& a, co
     return sigma * (2.0f * sqrtf(fmaxf(r2 - d2, 0.0f)));
 }
 
+template <bool CULL = false>
 __device__ __forceinline__ float strand_tau(const Ray& r, const SweepStrand& st, const SweepPoint* pts, float sigma) {
     float tau = 0.0f;
     for (int i = 0; i < st.point_count - 1; i++) {
-        tau += piece_tau(r, pts[st.point_offset + i], pts[st.point_offset + i + 1], sigma);
+        const SweepPoint& a = pts[st.point_offset + i];
+        const SweepPoint& b = pts[st.point_offset + i + 1];
+        // a piece out of reach adds exactly 0 (piece_tau's segment is a .. 2a - b)
+        if (CULL) {
+            const float3 u = f3(b.position) - f3(a.position);
+            if (!piece_in_reach(r, f3(a.position) - 0.5f * u, 0.5f * sqrtf(dot(u, u)),
+                                fmaxf(fabsf(a.radius), fabsf(b.radius))))
+                continue;
+        }
+        tau += piece_tau(r, a, b, sigma);
         if (tau > 6.0f) break;
     }
     return tau;

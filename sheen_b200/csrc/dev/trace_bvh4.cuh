@@ -443,7 +443,7 @@ __device__ __forceinline__ bool strands_cull(const DevScene& S, const Ray& r, Hi
     float best = r.tmax;
     dfs_cull<COUNT>(S.strand_bvh, r, best, c, [&](int i) {
         Hit tmp;
-        if (strand_test(r, S.strands[i], S.sweep_points, tmp) && tmp.t < best) {
+        if (strand_test<true>(r, S.strands[i], S.sweep_points, tmp) && tmp.t < best) {
             h = tmp; h.obj = -(i + 1); best = tmp.t; any = true;
         }
     });
@@ -713,7 +713,7 @@ struct FastTracer {
                ((F & kCatCSG) && csg_closest(S, r, h, true)) || ((F & kCatPlanes) && planes_scan(S, r, h));
     }
     __device__ __forceinline__ static float strand_depth(const DevScene& S, const Ray& r, Counters& c) {
-        return (F & kCatStrands) ? strands_tau_ref<COUNT>(S, r, c) : 0.0f;
+        return (F & kCatStrands) ? strands_tau_ref<COUNT, true>(S, r, c) : 0.0f;
     }
 };
 

@@ -269,7 +269,7 @@ __device__ __noinline__ bool opaque_ref(const DevScene& S, const Ray& r, Hit& re
 
 // bvh.h:928-960: strand optical depth along a shadow ray, stopping once
 // tau exceeds 6.
-template <bool COUNT>
+template <bool COUNT, bool CULL = false>
 __device__ __noinline__ float strands_tau_ref(const DevScene& S, const Ray& r, Counters& c) {
     if (S.num_strands == 0) return 0.0f;
     float tau = 0.0f;
@@ -284,7 +284,7 @@ __device__ __noinline__ float strands_tau_ref(const DevScene& S, const Ray& r, C
         const int left = __float_as_int(a.w), right = __float_as_int(b.w);
         if (left < 0) {
             if (COUNT) c.prims++;
-            tau += strand_tau(r, S.strands[~left], S.sweep_points, 6.0f);
+            tau += strand_tau<CULL>(r, S.strands[~left], S.sweep_points, 6.0f);
             if (tau > 6.0f) return tau;
         } else if (sp <= kRefStack - 2) {
             stack[sp++] = left;

@@ -165,3 +165,31 @@ def test_csg_box_hits_equal_plain_form(analytic):
     assert np.array_equal(o0, o1) and np.array_equal(m0, m1)
     assert np.array_equal(t0, t1)
     assert np.abs(i0 - i1).mean() <= 1e-3
+
+
+@pytest.mark.gpu
+def test_strand_reach_cull_equals_plain_form(analytic):
+    """The wavefront form skips the tests of strand pieces whose bounding
+    sphere the ray's line misses (in the closest-hit test and in the
+    optical depth of shadow rays); on a scene of the strands and the ground
+    plane its primary hits equal the plain form's bit for bit, and the
+    images, whose shadow rays carry the strands' optical depth, agree to the
+    last bits of the two forms' separately compiled shading."""
+    sb.init(0, 100)
+    v = _copy(analytic)
+    for k in ("num_objects", "num_superellipsoids", "num_triangles", "num_heightfields", "num_lathes",
+              "num_prisms"):
+        setattr(v, k, 0)
+    v.csg_root = -1
+    assert v.num_sweep_strands > 0
+    res = []
+    for form in (sb.FORM_PLAIN, sb.FORM_WAVEFRONT):
+        ds = sb.DeviceScene(v, form)
+        o, m, t = ds.primary_hits(640, 360, 1)
+        img, _ = ds.render_host(320, 180, 1)
+        ds.close()
+        res.append((o, m, t, img))
+    (o0, m0, t0, i0), (o1, m1, t1, i1) = res
+    assert (o0 < 0).sum() > 1000                    # strand hits present
+    assert np.array_equal(o0, o1) and np.array_equal(m0, m1) and np.array_equal(t0, t1)
+    assert np.abs(i0 - i1).mean() <= 1e-5
