@@ -764,6 +764,7 @@ CAPTURE_CASES = {
     "mega": (0, 0, 0, 640, 480, 1, "wavefront", True, None),
     "photon": (3, 0, 1000000, 320, 180, 1, "wavefront", True, None),
     "wave_inst": (1, 8, 0, 640, 360, 4, "wavefront", False, 0),
+    "analytic": (2, 0, 0, 640, 360, 4, "wavefront", False, None),
     "mega_deep": (1, 8, 0, 640, 360, 4, "wavefront", True, 4),
 }
 
@@ -775,6 +776,8 @@ def run_capture(name):
     small-frame megakernel); photon: the caustics workload with 1M photons
     per light (its scene build runs the photon emission); wave_inst: the mesh
     workload with instanced tori at 640x360 4 spp through the queue stages;
+    analytic: the analytic + CSG workload at 640x360 4 spp through the queue
+    stages;
     mega_deep: the same with reflect + refract recursion to 4 bounces (BVH4
     megakernel)."""
     import torch
