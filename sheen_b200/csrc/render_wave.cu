@@ -331,7 +331,7 @@ __device__ __forceinline__ unsigned int shadow_item(const DevScene& S, const Wav
 }
 
 template <int F, bool MULTI>
-__global__ void __launch_bounds__(128, 4) wave_shadow(const __grid_constant__ DevScene S0, WaveView V0) {
+__global__ void __launch_bounds__(128, 8) wave_shadow(const __grid_constant__ DevScene S0, WaveView V0) {
     Counters c;
     const unsigned int n = V0.ctr[kShadowCount];
     while (true) {
