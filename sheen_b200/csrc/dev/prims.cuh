@@ -655,18 +655,24 @@ __device__ __forceinline__ void se_chord(const Ray& r, const Superellipsoid& s, 
 // entry, and clamped to t1 >= entry), so the reference's final check
 // entry <= exit always holds and the exit never changes the hit; tx is
 // then t1.
+// [wa, wb]: a window outside which every point of the ray is known to be
+// outside the body (se_may_enter's widened bounding-ellipsoid chord); a
+// sample or bisection point outside it is decided without evaluating F,
+// and once no entry was found and the samples pass wb none can follow.
 template <bool ENTRY_ONLY = false, class MakeOut>
 __device__ __forceinline__ bool se_span_core(const Ray& r, const Superellipsoid& s, float t0, float t1, float& te,
-                                             float& tx, float* te_prev, MakeOut make) {
+                                             float& tx, float* te_prev, MakeOut make,
+                                             float wa = -INFINITY, float wb = INFINITY) {
     float tA, tB;
     se_chord(r, s, tA, tB);
     if (tB < t0 || tA > t1 || tB < tA) return false;
     t0 = fmaxf(t0, tA);
     t1 = fminf(t1, tB);
-    const auto out = make();
+    const auto out0 = make();
+    const auto out = [&](float t) { return (t < wa || t > wb) ? true : out0(r.o + t * r.d); };
     const float step = (t1 - t0) / 32.0f;
     float tp = t0;
-    bool inside = !out(r.o + tp * r.d);
+    bool inside = !out(tp);
     bool found_in = inside, found_out = false;
     te = inside ? t0 : -1e30f;
     if (te_prev) *te_prev = te;   // the last sample outside before the entry (te itself: no bracket)
@@ -674,12 +680,13 @@ __device__ __forceinline__ bool se_span_core(const Ray& r, const Superellipsoid&
     if (ENTRY_ONLY && inside) { tx = t1; return true; }
     for (int i = 1; i <= 32 && !found_out; i++) {
         float t = fminf(t0 + step * (float)i, t1);
-        const bool o = out(r.o + t * r.d);
+        if (!inside && t > wb) break;   // every later sample is outside too
+        const bool o = out(t);
         if (inside && o) {
             float lo = tp, hi = t;
             for (int b = 0; b < 20; b++) {
                 float mid = 0.5f * (lo + hi);
-                if (out(r.o + mid * r.d)) hi = mid; else lo = mid;
+                if (out(mid)) hi = mid; else lo = mid;
             }
             tx = fminf(0.5f * (lo + hi), t1);
             found_out = true;
@@ -708,7 +715,12 @@ __device__ __forceinline__ bool se_span_core(const Ray& r, const Superellipsoid&
 // above 1 -- for n >= 0.25 about 2.5e-4, far beyond the rounding of F in
 // FP32 -- so every sample tests outside and the march finds no entry: the
 // result is the march's, without its 33 evaluations.
-__device__ __forceinline__ bool se_may_enter(const Ray& r, const Superellipsoid& s, float t0, float t1) {
+// The widened chord [wa, wb] is returned as se_span_core's window (left
+// unbounded where no chord is computed).
+__device__ __forceinline__ bool se_may_enter(const Ray& r, const Superellipsoid& s, float t0, float t1, float& wa,
+                                             float& wb) {
+    wa = -INFINITY;
+    wb = INFINITY;
     if (!(s.n >= 0.25f && s.n <= 1e4f)) return true;
     const float k2 = s.n <= 2.0f ? 1.0f : powf(3.0f, 1.0f - 2.0f / s.n);
     const float K = k2 * 1.002001f;   // (k (1 + 1e-3))^2
@@ -723,6 +735,8 @@ __device__ __forceinline__ bool se_may_enter(const Ray& r, const Superellipsoid&
         const float sq = sqrtf(disc);
         const float ta = (-B - sq) / A, tb = (-B + sq) / A;
         const float slack = 1e-3f * (fabsf(ta) + fabsf(tb)) + 1e-6f;
+        wa = ta - slack;
+        wb = tb + slack;
         return !(tb < t0 - slack || ta > t1 + slack);
     }
     return false;
@@ -738,11 +752,12 @@ __device__ __forceinline__ bool se_may_enter(const Ray& r, const Superellipsoid&
 template <bool SIGN = false, bool ENTRY_ONLY = false>
 __device__ __forceinline__ bool se_span(const Ray& r, const Superellipsoid& s, float t0, float t1,
                                         float& te, float& tx, float* te_prev = nullptr) {
-    if (SIGN && !se_may_enter(r, s, t0, t1)) return false;
+    float wa = -INFINITY, wb = INFINITY;
+    if (SIGN && !se_may_enter(r, s, t0, t1, wa, wb)) return false;
     return se_span_core<ENTRY_ONLY>(r, s, t0, t1, te, tx, te_prev, [&]() {
         const SeSign sg(SIGN ? s.n : 0.0f);
         return [sg, &s](float3 p) { return SIGN ? sg.outside(s, p) : se_value(s, p) > 1.0f; };
-    });
+    }, wa, wb);
 }
 
 // Extension: the two-exponent body's span (the same march), not inlined so
