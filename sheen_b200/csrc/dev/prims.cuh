@@ -603,9 +603,14 @@ __device__ __forceinline__ float3 se_normal_dir(const Superellipsoid& s, float n
 // The thresholds carry a 1e-4 relative margin, far above the few-ulp error
 // of powf and the sum, so every decision equals se_value(s, p) > 1; any
 // other point (or a NaN) is evaluated exactly with se_value's arithmetic.
+// The bounds are evaluated on q from multiplications by 1 / a, 1 / b, 1 / c
+// (a few ulp from the quotients, far inside the 1e-4 margins); only a point
+// they leave undecided computes the quotients and F with se_value's
+// arithmetic.
 struct SeSign {
     float thr_in, thr_out;   // on max|q_i| and on sum|q_i|; -1 / +inf: no shortcut
-    __device__ __forceinline__ explicit SeSign(float n) {
+    float ia, ib, ic;
+    __device__ __forceinline__ SeSign(float n, const Superellipsoid& s) {
         if (n >= 0.25f && n <= 1e4f) {
             thr_in = powf(1.0f / 3.0f, 1.0f / n) * (1.0f - 1e-4f);
             thr_out = (n >= 1.0f ? powf(3.0f, 1.0f - 1.0f / n) : 1.0f) * (1.0f + 1e-4f);
@@ -613,15 +618,21 @@ struct SeSign {
             thr_in = -1.0f;
             thr_out = __int_as_float(0x7f800000);
         }
+        ia = 1.0f / s.a;
+        ib = 1.0f / s.b;
+        ic = 1.0f / s.c;
     }
     __device__ __forceinline__ bool outside(const Superellipsoid& s, float3 p) const {
-        const float qx = (p.x - s.center.x) / s.a, qy = (p.y - s.center.y) / s.b, qz = (p.z - s.center.z) / s.c;
-        const float ax = fabsf(qx), ay = fabsf(qy), az = fabsf(qz);
-        const float sum = ax + ay + az;
-        if (sum == sum) {
-            if (fmaxf(fmaxf(ax, ay), az) < thr_in) return false;
-            if (sum > thr_out) return true;
+        const float dx = p.x - s.center.x, dy = p.y - s.center.y, dz = p.z - s.center.z;
+        {
+            const float ax = fabsf(dx * ia), ay = fabsf(dy * ib), az = fabsf(dz * ic);
+            const float sum = ax + ay + az;
+            if (sum == sum) {
+                if (fmaxf(fmaxf(ax, ay), az) < thr_in) return false;
+                if (sum > thr_out) return true;
+            }
         }
+        const float ax = fabsf(dx / s.a), ay = fabsf(dy / s.b), az = fabsf(dz / s.c);
         return powf(ax, s.n) + powf(ay, s.n) + powf(az, s.n) > 1.0f;
     }
 };
@@ -755,7 +766,7 @@ __device__ __forceinline__ bool se_span(const Ray& r, const Superellipsoid& s, f
     float wa = -INFINITY, wb = INFINITY;
     if (SIGN && !se_may_enter(r, s, t0, t1, wa, wb)) return false;
     return se_span_core<ENTRY_ONLY>(r, s, t0, t1, te, tx, te_prev, [&]() {
-        const SeSign sg(SIGN ? s.n : 0.0f);
+        const SeSign sg(SIGN ? s.n : 0.0f, s);
         return [sg, &s](float3 p) { return SIGN ? sg.outside(s, p) : se_value(s, p) > 1.0f; };
     }, wa, wb);
 }
