@@ -233,3 +233,51 @@ def test_batch_with_instanced_scenes(device, inst_scene, flat_scene):
     assert np.array_equal(outs[0].cpu().numpy(), ia)
     assert np.array_equal(outs[1].cpu().numpy(), ib)
     assert np.array_equal(outs[2].cpu().numpy()[:, :W // 2], ic[:, :W // 2])
+
+
+def _affine_ext(scene):
+    """The extension with non-rigid maps: every instance scaled non-uniformly
+    about its centre, every other one mirrored (negative determinant)."""
+    x = _ext(scene)
+    inst = _instances(x)
+    for j, it in enumerate(inst):
+        sx, sy, sz = 1.3, 0.8, (-1.1 if j % 2 else 1.1)
+        for r in range(3):
+            it.xform[4 * r + 0] *= sx
+            it.xform[4 * r + 1] *= sy
+            it.xform[4 * r + 2] *= sz
+    x.instances = ctypes.addressof(inst)
+    return x, inst
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", FORMS, ids=FORM_IDS)
+def test_non_rigid_instances_match_oracle(device, inst_scene, form):
+    """Scaled and mirrored instances: t is shared by both spaces, normals go
+    through the inverse transpose, facing survives a mirror -- against the
+    oracle, which flattens the same maps in double."""
+    x, keep = _affine_ext(inst_scene)
+    ds = sb.DeviceScene(inst_scene, form, ext=x)
+    img, _ = ds.render_host(W, H, AA)
+    rays = _torus_rays(inst_scene, 10000, seed=8)
+    obj, mat, t = ds.trace(rays)
+    ds.close()
+    o = Oracle()
+    h = o.scene(inst_scene.view_ptr, ext_ptr=ctypes.addressof(x))
+    ref = o.render(h, W, H, AA)
+    h.close()
+    err = image_error(img, ref)
+    assert err["mean_abs"] <= 1e-3 and err["frac_px_over_1e-2"] <= 0.01, err
+    o64 = Oracle(fp64=True)
+    h = o64.scene(inst_scene.view_ptr, ext_ptr=ctypes.addressof(x))
+    cat, prim, t64 = o64.trace(h, np.c_[rays[:, 0:3], rays[:, 4:7]].astype(np.float64))
+    h.close()
+    want = np.where(cat == 0, prim, -(prim + 1))
+    same = (cat >= 0) & (obj == want)
+    both = (cat >= 0) & (obj != MISS)
+    assert same.sum() >= 0.99 * both.sum()
+    sel = same & (obj < -inst_scene.view.num_triangles)
+    assert sel.sum() > 1000
+    rel = np.abs(t[sel].astype(np.float64) - t64[sel]) / np.abs(t64[sel])
+    assert np.quantile(rel, 0.99) <= 1e-5, np.quantile(rel, 0.99)
+    del keep
