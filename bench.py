@@ -645,9 +645,12 @@ def serve_stream(n_requests, rate, inflight, seed, warmup, serial_k=0, local=0):
     t0 = time.perf_counter()
     sid = {k: srv.add_scene(host_scenes[k]) for k in keys}
     add_s = time.perf_counter() - t0
-    # warm-up: one small request per scene (kernels loaded, pool primed)
+    # warm-up: one small request per scene (kernels loaded), then one
+    # 1080p 4-spp request per generator (the pool primed to a full row band)
     for k in keys:
         srv.submit(sid[k], 256, 256, 1).wait()
+    for cfg in sorted({k[0] for k in keys}):
+        srv.submit(sid[next(k for k in keys if k[0] == cfg)], 1920, 1080, 4).wait()
     for _ in range(max(0, warmup - 1)):
         srv.submit(sid[keys[0]], 512, 512, 4).wait()
 
