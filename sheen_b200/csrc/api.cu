@@ -103,6 +103,8 @@ int sheen_init(int device_id, int cuda_arch) {
     if (e != cudaSuccess) return fail_cuda(e);
     e = cudaFree(0);
     if (e != cudaSuccess) return fail_cuda(e);
+    e = sheen::prewarm_device(sheen::tuning().prewarm_mb);
+    if (e != cudaSuccess) return fail_cuda(e);
     return 0;
 }
 

@@ -106,6 +106,9 @@ int scene_upload(const SheenScene* in, int form, DeviceScene** out);
 // With scene extensions (ext may be null).
 int scene_upload_ext(const SheenScene* in, const SheenSceneExt* ext, int form, DeviceScene** out);
 void release_upload_rings();
+// sheen_init's warm-up of the current device: `mb` of device memory mapped
+// into the library's pool, and the pinned upload ring.
+cudaError_t prewarm_device(int mb);
 void scene_release(DeviceScene* s);
 
 // Pixel rectangle [x0, x1) x [y0, y1) of a W x H image; the output buffer
@@ -195,6 +198,7 @@ struct Tuning {
     int build_device = 1;           // wavefront triangle BVH4s: 1 built on the device, 0 on the host
     int build_concurrent = 1;       // device build: the subset trees beside the full tree (2 host threads)
     int pool_keep_mb = 16384;       // freed device memory the library's pool keeps for reuse
+    int prewarm_mb = 2048;          // device memory sheen_init maps into the pool up front (0: none)
     int watertight = 0;             // wavefront triangle test: 0 Moller-Trumbore (the reference's), 1 watertight
     int aa_centered = 0;            // camera samples: 0 the reference's jitter, 1 cell centres
     int se_polish = 0;              // superellipsoid entries: 0 on a sample (reference), 1 FP64 Newton polish

@@ -34,6 +34,7 @@ const Key kKeys[] = {
     {"build.device", &Tuning::build_device, 0, 1},
     {"build.concurrent", &Tuning::build_concurrent, 0, 1},
     {"mem.pool_keep_mb", &Tuning::pool_keep_mb, 0, 1 << 20},
+    {"mem.prewarm_mb", &Tuning::prewarm_mb, 0, 1 << 20},
     {"trace.watertight", &Tuning::watertight, 0, 1},
     {"camera.centered", &Tuning::aa_centered, 0, 1},
     {"trace.se_polish", &Tuning::se_polish, 0, 1},

@@ -1222,6 +1222,29 @@ int scene_upload_ext(const SheenScene* in, const SheenSceneExt* ext, int form, D
     return 0;
 }
 
+// The first render of a process used to pay the pool's growth (hundreds of
+// MB mapped by the driver) and the pinned ring's allocation: about 220 ms
+// for each of the first two host-array calls of the mesh workload against
+// 43 ms after.  sheen_init maps `mb` into the pool (an allocation freed back
+// to it; the pool keeps freed memory mapped up to mem.pool_keep_mb) and
+// allocates the ring.
+cudaError_t prewarm_device(int mb) {
+    if (mb > 0) {
+        void* p = nullptr;
+        cudaError_t e = dmalloc(&p, (size_t)mb << 20);
+        if (e != cudaSuccess) {
+            cudaGetLastError();   // not enough memory: no warm-up
+        } else {
+            dfree(p);
+        }
+    }
+    int dev_id = 0;
+    cudaError_t e = cudaGetDevice(&dev_id);
+    if (e != cudaSuccess || dev_id < 0 || dev_id >= kUpMaxDevices) return e;
+    std::lock_guard<std::mutex> lk(g_up_mu);
+    return ring_init(g_up[dev_id]);
+}
+
 // Frees the pinned upload rings (sheen_cleanup, before the device reset).
 void release_upload_rings() {
     std::lock_guard<std::mutex> lk(g_up_mu);
