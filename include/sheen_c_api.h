@@ -463,6 +463,9 @@ int sheen_scene_profile_stages(SheenDeviceScene scene, int width, int height, in
  *                                   beside the full one (two host threads)
  *   "mem.pool_keep_mb"           0..1048576 (default 16384): freed device
  *                                   memory the library keeps for reuse
+ *   "mem.prewarm_mb"             0..1048576 (default 2048): device memory
+ *                                   sheen_init maps into that pool up front
+ *                                   (set before sheen_init; 0: none)
  *   "trace.watertight"           0 (default): the wavefront form tests
  *                                   triangles with the reference's
  *                                   Moller-Trumbore; 1: a watertight
