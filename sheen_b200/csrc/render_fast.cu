@@ -20,10 +20,12 @@ __device__ __forceinline__ void warp_add_fast(unsigned long long* dst, unsigned 
 // categories' code and registers.  Those smaller variants run 8 blocks of
 // 128 threads per SM (64 registers): measured on a B200, the spheres frame
 // 0.140 -> 0.126 ms and the mesh workload at depth 4 with instanced tori
-// 119.1 -> 101.7 ms against the unbounded 168-register build; the
-// all-categories variant keeps its registers.
+// 119.1 -> 101.7 ms against the unbounded 168-register build.  The
+// all-categories variant runs 4 blocks (128 registers): 640x360 1-spp
+// frames of the analytic workload 2.59 -> 2.54 ms and of the caustics
+// workload 6.63 -> 5.81 ms against its unbounded build.
 template <bool COUNT, int F = kCatAll>
-__global__ void __launch_bounds__(128, ((F & kCatAll) == kCatAll) ? 1 : 8) mega_bvh4_kernel(const __grid_constant__ DevScene S, float4* __restrict__ out, int W, int H, int aa,
+__global__ void __launch_bounds__(128, ((F & kCatAll) == kCatAll) ? 4 : 8) mega_bvh4_kernel(const __grid_constant__ DevScene S, float4* __restrict__ out, int W, int H, int aa,
                                                         int x0, int y0, int x1, int y1, unsigned long long* tally) {
     const int x = x0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
     const int y = y0 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
