@@ -256,3 +256,46 @@ def make_light(kind, **kw):
     for k, v in kw.items():
         l[k] = v
     return l
+
+
+@dataclass
+class InstanceArrays:
+    """Owns the arrays of an instancing / recursion extension and builds the
+    C ``SheenSceneExt`` (the other extension fields left empty).
+
+    mesh_triangles: object-space triangles (TRIANGLE dtype) of every mesh;
+    meshes: (n, 2) int32 rows of (first triangle, triangle count);
+    xforms: (k, 3, 4) float32 object-to-world maps; inst_mesh / inst_material:
+    per-instance mesh index and material id; max_depth: reflect + refract
+    recursion (0: the reference's depth-1 rules)."""
+    mesh_triangles: np.ndarray = field(default_factory=lambda: np.zeros(0, TRIANGLE))
+    meshes: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.int32))
+    xforms: np.ndarray = field(default_factory=lambda: np.zeros((0, 3, 4), np.float32))
+    inst_mesh: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    inst_material: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    max_depth: int = 0
+
+    def view(self) -> SheenSceneExt:
+        """C view; valid while this object (and its arrays) is alive."""
+        k = len(self.xforms)
+        assert len(self.inst_mesh) == k and len(self.inst_material) == k
+        self._tris = np.ascontiguousarray(self.mesh_triangles, dtype=TRIANGLE)
+        self._meshes = (SheenMesh * max(len(self.meshes), 1))(
+            *[SheenMesh(int(a), int(b)) for a, b in np.asarray(self.meshes, np.int32).reshape(-1, 2)])
+        inst = (SheenInstance * max(k, 1))()
+        xf = np.asarray(self.xforms, np.float32).reshape(k, 12)
+        for j in range(k):
+            for q in range(12):
+                inst[j].xform[q] = float(xf[j, q])
+            inst[j].mesh = int(self.inst_mesh[j])
+            inst[j].material_id = int(self.inst_material[j])
+        self._inst = inst
+        x = SheenSceneExt()
+        x.mesh_triangles = _ptr(self._tris)
+        x.num_mesh_triangles = len(self._tris)
+        x.meshes = ctypes.addressof(self._meshes) if len(self.meshes) else None
+        x.num_meshes = len(self.meshes)
+        x.instances = ctypes.addressof(inst) if k else None
+        x.num_instances = k
+        x.max_depth = int(self.max_depth)
+        return x

@@ -281,3 +281,27 @@ def test_non_rigid_instances_match_oracle(device, inst_scene, form):
     rel = np.abs(t[sel].astype(np.float64) - t64[sel]) / np.abs(t64[sel])
     assert np.quantile(rel, 0.99) <= 1e-5, np.quantile(rel, 0.99)
     del keep
+
+
+def test_instance_arrays_build_the_generators_extension(inst_scene):
+    """contract.InstanceArrays (numpy-owned meshes, maps and materials) gives
+    the oracle the same scene as the generator's own extension."""
+    x = _ext(inst_scene)
+    inst = _instances(x)
+    meshes = (C.SheenMesh * x.num_meshes).from_address(x.meshes)
+    tris = np.frombuffer(ctypes.string_at(x.mesh_triangles, C.TRIANGLE.itemsize * x.num_mesh_triangles),
+                         C.TRIANGLE).copy()
+    arrays = C.InstanceArrays(
+        mesh_triangles=tris,
+        meshes=np.array([[m.tri_offset, m.tri_count] for m in meshes], np.int32),
+        xforms=np.array([list(i.xform) for i in inst], np.float32).reshape(-1, 3, 4),
+        inst_mesh=np.array([i.mesh for i in inst], np.int32),
+        inst_material=np.array([i.material_id for i in inst], np.int32))
+    mine = arrays.view()
+    o = Oracle()
+    imgs = []
+    for ext in (x, mine):
+        h = o.scene(inst_scene.view_ptr, ext_ptr=ctypes.addressof(ext))
+        imgs.append(o.render(h, 48, 27, 1))
+        h.close()
+    assert np.array_equal(imgs[0], imgs[1])
